@@ -1,0 +1,791 @@
+/*
+ * ms_oracle.c -- FP64 CPU restatement of the matchSeries registration path.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the CUDA path, never the product.
+ * Each function follows the reference file:line given beside it, including
+ * the order of floating-point operations where that order is observable in
+ * FP64 (sums are accumulated in the reference's loop order), so that the
+ * restatement agrees with the reference's own templates to rounding.
+ */
+#include "ms_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* 1-D Gauss points of GaussQuadrature<double,QC_1D,3> (baseFunctionSet.h:1538-1545) */
+#define GP0 0.2113248654051871
+#define GP1 0.7886751345948129
+
+static int lvl_n(int level) { return (1 << level) + 1; }
+static double lvl_h(int level) { return 1.0 / (double)(1 << level); }
+static double sqr(double x) { return x * x; }
+
+/* Quadrature tables of BaseFunctionSetMultiLin<double,QC_2D,Gauss3>
+ * (baseFunctionSet.h:58-65, 128-195, Quadrature2D 1443-1454).            */
+typedef struct {
+  double rc[4][2];       /* reference coordinates of the 4 quad points   */
+  double bq[4][4];       /* basis value  [basis][quad]                   */
+  double gq[4][4][2];    /* basis gradient / h [basis][quad][comp]       */
+  double w;              /* quad weight (0.5 * 0.5)                      */
+} quad_t;
+
+static void basis_grad(int b, double x, double y, double h, double g[2]) {
+  switch (b) {
+    case 0: g[0] = (y - 1.0) / h; g[1] = (x - 1.0) / h; break;
+    case 1: g[0] = (1.0 - y) / h; g[1] = (-x) / h; break;
+    case 2: g[0] = (-y) / h; g[1] = (1.0 - x) / h; break;
+    default: g[0] = y / h; g[1] = x / h; break;
+  }
+}
+
+static double basis_val(int b, double x, double y) {
+  switch (b) {
+    case 0: return (1.0 - x) * (1.0 - y);
+    case 1: return x * (1.0 - y);
+    case 2: return (1.0 - x) * y;
+    default: return x * y;
+  }
+}
+
+static void quad_init(quad_t* Q, double h) {
+  const double g[2] = {GP0, GP1};
+  for (int i = 0, k = 0; i < 2; ++i)
+    for (int j = 0; j < 2; ++j, ++k) { Q->rc[k][0] = g[i]; Q->rc[k][1] = g[j]; }
+  for (int b = 0; b < 4; ++b)
+    for (int q = 0; q < 4; ++q) {
+      Q->bq[b][q] = basis_val(b, Q->rc[q][0], Q->rc[q][1]);
+      basis_grad(b, Q->rc[q][0], Q->rc[q][1], h, Q->gq[b][q]);
+    }
+  Q->w = 0.5 * 0.5;
+}
+
+/* global node index of local dof b of element (ex, ey) (indexMapper.h:410-414) */
+static int dof(int n, int ex, int ey, int b) {
+  return ex + ey * n + ((b & 1) ? 1 : 0) + ((b & 2) ? n : 0);
+}
+
+/* DiscreteFunctionDefault::evaluateAtQuadPoint (discreteFunction.h:239-246) */
+static double eval_at_quad(const quad_t* Q, const double* f, int n, int ex, int ey, int q) {
+  double w = 0.;
+  for (int b = 0; b < 4; ++b) w += f[dof(n, ex, ey, b)] * Q->bq[b][q];
+  return w;
+}
+
+/* DiscreteFunctionDefault::evaluate (discreteFunction.h:230-237) */
+static double eval_local(const double* f, int n, int ex, int ey, double x, double y) {
+  double w = 0.;
+  for (int b = 0; b < 4; ++b) w += f[dof(n, ex, ey, b)] * basis_val(b, x, y);
+  return w;
+}
+
+/* DiscreteFunctionDefault::evaluateGradient (discreteFunction.h:259-269) */
+static void eval_grad_local(const double* f, int n, int ex, int ey, double x, double y,
+                            double h, double g[2]) {
+  g[0] = 0.; g[1] = 0.;
+  for (int b = 0; b < 4; ++b) {
+    double v[2];
+    basis_grad(b, x, y, h, v);
+    const double d = f[dof(n, ex, ey, b)];
+    v[0] *= d; v[1] *= d;
+    g[0] += v[0]; g[1] += v[1];
+  }
+}
+
+/* transformAndClipCoord (deformations.h:765-817) followed by
+ * getLocalCoordsRegularRectangularGrid (configurators.h:34-51).            */
+typedef struct { int el[2]; double loc[2]; int within[2]; } tcoord_t;
+
+static void transform_and_clip(const quad_t* Q, int n, double h, int ex, int ey, int q,
+                               double off_x, double off_y, tcoord_t* t) {
+  double coord[2];
+  coord[0] = ((double)ex + Q->rc[q][0]) * h;
+  coord[1] = ((double)ey + Q->rc[q][1]) * h;
+  coord[0] += off_x;
+  coord[1] += off_y;
+  for (int c = 0; c < 2; ++c) {
+    const int width = (int)((double)(n - 1) * h);
+    t->within[c] = 1;
+    if (coord[c] < 0.) {
+      coord[c] = 0.;
+      t->within[c] = 0;
+    } else if (coord[c] >= width) {
+      coord[c] = width - DBL_EPSILON;
+      t->within[c] = 0;
+    }
+    const double sc = coord[c] / h;
+    int e = (short)sc;
+    double l = sc - e;
+    if (e == n - 1 && fabs(l - 0.) < 1e-15) { e = n - 2; l = 1; }
+    t->el[c] = e;
+    t->loc[c] = l;
+  }
+}
+
+/* ---------------------------------------------------------------------- */
+
+double msor_ssd_energy(int level, const double* R, const double* T,
+                       const double* phix, const double* phiy) {
+  const int n = lvl_n(level);
+  const double h = lvl_h(level);
+  const double vol = sqr(h);
+  quad_t Q;
+  quad_init(&Q, h);
+  double res = 0.;
+  for (int ey = 0; ey < n - 1; ++ey)
+    for (int ex = 0; ex < n - 1; ++ex) {
+      double a = 0.;
+      for (int q = 0; q < 4; ++q) {
+        const double ox = eval_at_quad(&Q, phix, n, ex, ey, q);
+        const double oy = eval_at_quad(&Q, phiy, n, ex, ey, q);
+        tcoord_t t;
+        transform_and_clip(&Q, n, h, ex, ey, q, ox, oy, &t);
+        const double tv = eval_local(T, n, t.el[0], t.el[1], t.loc[0], t.loc[1]);
+        const double rv = eval_at_quad(&Q, R, n, ex, ey, q);
+        a += (0.5 * sqr(tv - rv)) * Q.w;
+      }
+      a *= vol;
+      res += a;
+    }
+  return 0. + res;
+}
+
+void msor_ssd_force(int level, const double* R, const double* T,
+                    const double* phix, const double* phiy, double* gx, double* gy) {
+  const int n = lvl_n(level);
+  const double h = lvl_h(level);
+  const double vol = sqr(h);
+  quad_t Q;
+  quad_init(&Q, h);
+  memset(gx, 0, sizeof(double) * n * n);
+  memset(gy, 0, sizeof(double) * n * n);
+  for (int ey = 0; ey < n - 1; ++ey)
+    for (int ex = 0; ex < n - 1; ++ex) {
+      double nl[4][2];
+      for (int q = 0; q < 4; ++q) {
+        const double ox = eval_at_quad(&Q, phix, n, ex, ey, q);
+        const double oy = eval_at_quad(&Q, phiy, n, ex, ey, q);
+        tcoord_t t;
+        transform_and_clip(&Q, n, h, ex, ey, q, ox, oy, &t);
+        const double td = eval_local(T, n, t.el[0], t.el[1], t.loc[0], t.loc[1]);
+        const double rv = eval_at_quad(&Q, R, n, ex, ey, q);
+        eval_grad_local(T, n, t.el[0], t.el[1], t.loc[0], t.loc[1], h, nl[q]);
+        for (int c = 0; c < 2; ++c) nl[q][c] = t.within[c] ? nl[q][c] * (td - rv) : 0;
+      }
+      for (int b = 0; b < 4; ++b) {
+        double a0 = 0., a1 = 0.;
+        for (int q = 0; q < 4; ++q) {
+          const double f = Q.bq[b][q] * Q.w;
+          a0 += nl[q][0] * f;
+          a1 += nl[q][1] * f;
+        }
+        const int g = dof(n, ex, ey, b);
+        gx[g] += vol * a0;
+        gy[g] += vol * a1;
+      }
+    }
+}
+
+/* Assembled Q1 stiffness in the 3x3-per-row layout of FastUniformGridMatrix
+ * (fastUniformGridMatrix.h:313-470): local matrix by quadrature
+ * (FEOpInterface.h:1362-1395), added once per entry in element order
+ * (LocalAssemblyHelper<QUOC_GRID_INDEX_MODE>::doLocalAssembly,
+ * FEOpInterface.h:65-88).                                                 */
+static double* stiff_build(int level) {
+  const int n = lvl_n(level);
+  const double h = lvl_h(level);
+  const double vol = sqr(h);
+  quad_t Q;
+  quad_init(&Q, h);
+  double L[4][4];
+  for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) L[i][j] = 0.;
+  for (int q = 0; q < 4; ++q) {
+    const double coeff = 1.;
+    for (int i = 0; i < 4; ++i)
+      for (int j = i; j < 4; ++j) {
+        double dot = 0;
+        dot += Q.gq[i][q][0] * Q.gq[j][q][0];
+        dot += Q.gq[i][q][1] * Q.gq[j][q][1];
+        L[i][j] += dot * coeff * Q.w;
+      }
+  }
+  for (int i = 0; i < 4; ++i)
+    for (int j = i; j < 4; ++j) L[j][i] = L[i][j] = L[i][j] * vol;
+  double* st = (double*)calloc((size_t)n * n * 9, sizeof(double));
+  for (int ey = 0; ey < n - 1; ++ey)
+    for (int ex = 0; ex < n - 1; ++ex)
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) {
+          const int gi = dof(n, ex, ey, i), gj = dof(n, ex, ey, j);
+          const int dx = (gj % n) - (gi % n), dy = (gj / n) - (gi / n);
+          double* e = &st[(size_t)gi * 9 + (dy + 1) * 3 + (dx + 1)];
+          *e += 1.0 * L[i][j];
+        }
+  return st;
+}
+
+static void stiff_apply_with(const double* st, int level, const double* u, double* Lu) {
+  const int n = lvl_n(level);
+  for (int r = 0; r < n * n; ++r) {
+    const int x = r % n, y = r / n;
+    double d = 0.;
+    for (int j = -1; j <= 1; ++j)
+      for (int i = -1; i <= 1; ++i) {
+        const int X = x + i, Y = y + j;
+        if (X >= 0 && X < n && Y >= 0 && Y < n)
+          d += st[(size_t)r * 9 + (j + 1) * 3 + (i + 1)] * u[X + Y * n];
+      }
+    Lu[r] = d;
+  }
+}
+
+void msor_stiff_apply(int level, const double* u, double* Lu) {
+  double* st = stiff_build(level);
+  stiff_apply_with(st, level, u, Lu);
+  free(st);
+}
+
+static double dot(const double* a, const double* b, int N) {
+  double r = 0;
+  for (int i = 0; i < N; ++i) r += a[i] * b[i];
+  return r;
+}
+
+/* DisplacementLengthEnergy::apply (hyperelastic.h:178-183) */
+static double reg_energy_with(const double* st, int level, const double* phix, const double* phiy) {
+  const int n = lvl_n(level), N = n * n;
+  double* tmp = (double*)malloc(sizeof(double) * N * 2);
+  stiff_apply_with(st, level, phix, tmp);
+  stiff_apply_with(st, level, phiy, tmp + N);
+  double d = 0;
+  d += dot(phix, tmp, N);
+  d += dot(phiy, tmp + N, N);
+  free(tmp);
+  return 0.5 * d;
+}
+
+static double energy_with(const double* st, int level, const double* R, const double* T,
+                          const double* phix, const double* phiy, double lambda, double* ereg) {
+  double e = 0.;
+  e += msor_ssd_energy(level, R, T, phix, phiy);
+  const double r = reg_energy_with(st, level, phix, phiy);
+  if (ereg) *ereg = r;
+  if (lambda != 1.0) e += lambda * r; else e += r;
+  return e;
+}
+
+double msor_energy(int level, const double* R, const double* T, const double* phix,
+                   const double* phiy, double lambda, double* ereg) {
+  double* st = stiff_build(level);
+  const double e = energy_with(st, level, R, T, phix, phiy, lambda, ereg);
+  free(st);
+  return e;
+}
+
+static void denergy_with(const double* st, int level, const double* R, const double* T,
+                         const double* phix, const double* phiy, double lambda,
+                         double* gx, double* gy) {
+  const int n = lvl_n(level), N = n * n;
+  msor_ssd_force(level, R, T, phix, phiy, gx, gy);
+  double* tmp = (double*)malloc(sizeof(double) * N);
+  stiff_apply_with(st, level, phix, tmp);
+  for (int i = 0; i < N; ++i) gx[i] += (lambda != 1.0) ? lambda * tmp[i] : tmp[i];
+  stiff_apply_with(st, level, phiy, tmp);
+  for (int i = 0; i < N; ++i) gy[i] += (lambda != 1.0) ? lambda * tmp[i] : tmp[i];
+  free(tmp);
+}
+
+void msor_denergy(int level, const double* R, const double* T, const double* phix,
+                  const double* phiy, double lambda, double* gx, double* gy) {
+  double* st = stiff_build(level);
+  denergy_with(st, level, R, T, phix, phiy, lambda, gx, gy);
+  free(st);
+}
+
+/* --- multigrid heat smoother (linearSmoothOp.cpp) --------------------- */
+
+/* HeatEquation2DFD::apply (linearSmoothOp.cpp:61-146) */
+static void heat_apply(int level, double tau, const double* A, double* D) {
+  const int w = lvl_n(level);
+  const double hsq = tau * (double)((w - 1) * (w - 1));
+#define AG(X, Y) A[(X) + (Y) * w]
+#define DS(X, Y, V) D[(X) + (Y) * w] = (V)
+  for (int X = 1; X < w - 1; ++X)
+    for (int Y = 1; Y < w - 1; ++Y) {
+      const double a = AG(X, Y) * 4;
+      double b = 0.0;
+      b -= AG(X + 1, Y);
+      b -= AG(X - 1, Y);
+      b -= AG(X, Y + 1);
+      b -= AG(X, Y - 1);
+      DS(X, Y, AG(X, Y) + hsq * (a + b));
+    }
+  const int e = w - 1;
+  const int cs[4][2] = {{0, 0}, {e, 0}, {0, e}, {e, e}};
+  const int co[4][2] = {{1, 1}, {-1, 1}, {1, -1}, {-1, -1}};
+  for (int i = 0; i < 4; ++i) {
+    const int cx = cs[i][0], cy = cs[i][1];
+    const double a = AG(cx, cy) * 4;
+    const double b = -AG(cx + co[i][0], cy) - AG(cx, cy + co[i][1]);
+    DS(cx, cy, AG(cx, cy) + hsq * (a + 2 * b));
+  }
+  for (int X = 1; X < w - 1; ++X) {
+    double a = AG(X, e) * 4;
+    double b = -2 * (AG(X, e - 1));
+    b -= AG(X + 1, e);
+    b -= AG(X - 1, e);
+    DS(X, e, AG(X, e) + hsq * (a + b));
+    a = AG(X, 0) * 4;
+    b = -2 * (AG(X, 1));
+    b -= AG(X + 1, 0);
+    b -= AG(X - 1, 0);
+    DS(X, 0, AG(X, 0) + hsq * (a + b));
+  }
+  for (int X = 1; X < w - 1; ++X) {
+    double a = AG(e, X) * 4;
+    double b = -2 * (AG(e - 1, X));
+    b -= AG(e, X + 1);
+    b -= AG(e, X - 1);
+    DS(e, X, AG(e, X) + hsq * (a + b));
+    a = AG(0, X) * 4;
+    b = -2 * (AG(1, X));
+    b -= AG(0, X + 1);
+    b -= AG(0, X - 1);
+    DS(0, X, AG(0, X) + hsq * (a + b));
+  }
+#undef AG
+#undef DS
+}
+
+/* HeatMultigrid::jacobi (linearSmoothOp.cpp:556-580) */
+static void jacobi(int level, double tau, double* X, const double* rhs, double* dummy) {
+  const int w = lvl_n(level);
+  const double diag = 1 + 4 * tau * (double)((w - 1) * (w - 1));
+  const double relax = 1.0;
+  heat_apply(level, tau, X, dummy);
+  for (int l = 0; l < w * w; ++l) {
+    const double v = rhs[l] - dummy[l];
+    X[l] += relax * v / diag;
+  }
+}
+
+typedef struct { double* x[16]; double* rhs[16]; double* dummy[16]; double* res[16]; } mg_t;
+
+/* MDMultigrid::solve (linearSmoothOp.cpp:451-494) */
+static void mg_solve(mg_t* M, int level, double tau) {
+  const int w = lvl_n(level);
+  if (level == 0) {
+    for (int i = 0; i < 100; ++i) jacobi(level, tau, M->x[level], M->rhs[level], M->dummy[level]);
+    return;
+  }
+  for (int i = 0; i < 2; ++i) jacobi(level, tau, M->x[level], M->rhs[level], M->dummy[level]);
+  heat_apply(level, tau, M->x[level], M->dummy[level]);
+  for (int l = 0; l < w * w; ++l) M->res[level][l] = M->rhs[level][l] - M->dummy[level][l];
+  msor_restrict(level, M->res[level], M->rhs[level - 1]);
+  const int wc = lvl_n(level - 1);
+  memset(M->x[level - 1], 0, sizeof(double) * wc * wc);
+  mg_solve(M, level - 1, tau);
+  msor_prolong(level - 1, M->x[level - 1], M->dummy[level]);
+  for (int l = 0; l < w * w; ++l) M->x[level][l] += M->dummy[level][l];
+  for (int i = 0; i < 2; ++i) jacobi(level, tau, M->x[level], M->rhs[level], M->dummy[level]);
+}
+
+void msor_smooth_tau(int level, double tau, const double* in, double* out) {
+  mg_t M = {{0}, {0}, {0}, {0}};
+  for (int l = 0; l <= level; ++l) {
+    const int w = lvl_n(l);
+    M.x[l] = (double*)calloc((size_t)w * w, sizeof(double));
+    M.rhs[l] = (double*)calloc((size_t)w * w, sizeof(double));
+    M.dummy[l] = (double*)calloc((size_t)w * w, sizeof(double));
+    M.res[l] = (double*)calloc((size_t)w * w, sizeof(double));
+  }
+  const int w = lvl_n(level);
+  memcpy(M.rhs[level], in, sizeof(double) * w * w);
+  mg_solve(&M, level, tau);
+  memcpy(out, M.x[level], sizeof(double) * w * w);
+  for (int l = 0; l <= level; ++l) { free(M.x[l]); free(M.rhs[l]); free(M.dummy[l]); free(M.res[l]); }
+}
+
+/* LinearSmoothOp::setSigma: tau = 0.5f * sigma^2 (linearSmoothOp.h:50-52) */
+void msor_smooth(int level, double sigma, const double* in, double* out) {
+  msor_smooth_tau(level, 0.5f * sqr(sigma), in, out);
+}
+
+/* --- level transfer ----------------------------------------------------- */
+
+void msor_restrict(int fine_level, const double* fine, double* coarse) {
+  const int cw = lvl_n(fine_level - 1), fw = lvl_n(fine_level);
+#define F(X, Y) fine[(X) + (Y) * fw]
+#define C(X, Y) coarse[(X) + (Y) * cw]
+  for (int X = 0; X < cw; ++X)
+    for (int Y = 0; Y < cw; ++Y) C(X, Y) = F(2 * X, 2 * Y) / 4;
+  for (int X = 0; X < cw - 1; ++X)
+    for (int Y = 0; Y < cw - 1; ++Y) {
+      const double v = F(2 * X + 1, 2 * Y + 1) / 16;
+      C(X, Y) += v; C(X + 1, Y) += v; C(X, Y + 1) += v; C(X + 1, Y + 1) += v;
+    }
+  for (int X = 0; X < cw - 1; ++X)
+    for (int Y = 0; Y < cw; ++Y) {
+      const double v = F(2 * X + 1, 2 * Y) / 8;
+      C(X, Y) += v; C(X + 1, Y) += v;
+    }
+  for (int X = 0; X < cw; ++X)
+    for (int Y = 0; Y < cw - 1; ++Y) {
+      const double v = F(2 * X, 2 * Y + 1) / 8;
+      C(X, Y + 1) += v; C(X, Y) += v;
+    }
+  for (int X = 1; X < cw - 1; ++X) {
+    C(X, 0) = 4 * (C(X, 0) / 3);
+    C(X, cw - 1) = 4 * (C(X, cw - 1) / 3);
+    C(0, X) = 4 * (C(0, X) / 3);
+    C(cw - 1, X) = 4 * (C(cw - 1, X) / 3);
+  }
+  C(0, 0) = 16 * (C(0, 0) / 9);
+  C(cw - 1, 0) = 16 * (C(cw - 1, 0) / 9);
+  C(0, cw - 1) = 16 * (C(0, cw - 1) / 9);
+  C(cw - 1, cw - 1) = 16 * (C(cw - 1, cw - 1) / 9);
+#undef F
+#undef C
+}
+
+void msor_prolong(int coarse_level, const double* coarse, double* fine) {
+  const int cw = lvl_n(coarse_level) - 1, fw = lvl_n(coarse_level + 1);
+  int cc = 0, fc = 0;
+  for (int y = 0; y <= cw; ++y) {
+    double u = coarse[cc++];
+    for (int x = 0; x < cw; ++x) {
+      const double w = coarse[cc++];
+      fine[fc++] = u;
+      fine[fc++] = (u + w) / 2;
+      u = w;
+    }
+    fine[fc++] = u;
+    fc += fw;
+  }
+  fc = fw;
+  int tc = 0;
+  cc = fw << 1;
+  for (int y = 0; y < cw; ++y) {
+    for (int x = 0; x < fw; ++x) fine[fc++] = (fine[tc++] + fine[cc++]) / 2;
+    fc += fw; tc += fw; cc += fw;
+  }
+}
+
+/* ScalarArray<QC_2D>::interpolate (scalarArray.h:499-525) */
+static double interp(const double* img, int n, double X, double Y) {
+  int xL = (int)X, yL = (int)Y;
+  if (X >= (double)(n - 1)) xL = n - 2;
+  if (Y >= (double)(n - 1)) yL = n - 2;
+  if (X < 0.) xL = 0;
+  if (Y < 0.) yL = 0;
+  X -= xL;
+  Y -= yL;
+  const int xU = xL + 1, yU = yL + 1;
+  const double v0 = img[xL + yL * n], v1 = img[xU + yL * n], v2 = img[xL + yU * n], v3 = img[xU + yU * n];
+  if (Y == 0) return (1 - X) * v0 + X * v1;
+  return (1 - X) * (1 - Y) * v0 + X * (1 - Y) * v1 + (1 - X) * Y * v2 + X * Y * v3;
+}
+
+void msor_resample(int src_level, const double* src, int dst_level, double* dst) {
+  const int ns = lvl_n(src_level), nd = lvl_n(dst_level);
+  const long double hx = (long double)(ns - 1) / (nd - 1);
+  for (int y = 0; y < nd; ++y)
+    for (int x = 0; x < nd; ++x) {
+      const double sx = (double)(x * hx), sy = (double)(y * hx);
+      dst[x + y * nd] = interp(src, ns, sx, sy);
+    }
+}
+
+void msor_deform_image(int level, const double* img, const double* phix, const double* phiy,
+                       double ext_value, double* out) {
+  const int n = lvl_n(level);
+  const double h = lvl_h(level);
+  for (int y = 0; y < n; ++y)
+    for (int x = 0; x < n; ++x) {
+      const int i = x + y * n;
+      const double ds0 = x + phix[i] / h, ds1 = y + phiy[i] / h;
+      int inside = 1;
+      if (ds0 < 0. || ds0 > (double)(n - 1) || isnan(ds0)) inside = 0;
+      if (ds1 < 0. || ds1 > (double)(n - 1) || isnan(ds1)) inside = 0;
+      out[i] = inside ? interp(img, n, ds0, ds1) : ext_value;
+    }
+}
+
+static int cmp_double(const void* a, const void* b) {
+  const double x = *(const double*)a, y = *(const double*)b;
+  return (x < y) ? -1 : (x > y) ? 1 : 0;
+}
+
+void msor_normalize(double* img, int count, double sat, int min_to_zero) {
+  if (sat >= 0) {
+    double* tmp = (double*)malloc(sizeof(double) * count);
+    memcpy(tmp, img, sizeof(double) * count);
+    qsort(tmp, count, sizeof(double), cmp_double);
+    const int m1 = count - 1;
+    int il = (int)(sat / 200 * m1), ih = (int)((1 - sat / 200) * m1);
+    il = il < 0 ? 0 : (il > m1 ? m1 : il);
+    ih = ih < 0 ? 0 : (ih > m1 ? m1 : ih);
+    const double lo = tmp[il], hi = tmp[ih];
+    free(tmp);
+    for (int i = 0; i < count; ++i) img[i] = img[i] < lo ? lo : (img[i] > hi ? hi : img[i]);
+    double mn = img[0];
+    for (int i = 1; i < count; ++i) if (img[i] < mn) mn = img[i];
+    const double s = -1 * mn;
+    for (int i = 0; i < count; ++i) img[i] += s;
+    double mx = img[0];
+    for (int i = 1; i < count; ++i) if (img[i] > mx) mx = img[i];
+    if (mx != 0) for (int i = 0; i < count; ++i) img[i] /= mx;
+  } else {
+    double mn = img[0];
+    for (int i = 1; i < count; ++i) if (img[i] < mn) mn = img[i];
+    if (mn < 0. || min_to_zero) for (int i = 0; i < count; ++i) img[i] += -mn;
+    double mx = img[0];
+    for (int i = 1; i < count; ++i) if (img[i] > mx) mx = img[i];
+    if (mx != 0.) for (int i = 0; i < count; ++i) img[i] /= mx;
+  }
+}
+
+/* --- gradient flow ------------------------------------------------------ */
+
+typedef struct {
+  int level, N;
+  const double *R, *T;
+  const double* st;
+  double lambda;
+  /* ring buffer of the last two Armijo evaluations (gradientDescent.h:56-59) */
+  double rb_tau[2], rb_e[2];
+  int rb_pos;
+  int evals;
+  double e_at_pos;
+  double *tx, *ty;  /* scratch position */
+} gd_ctx;
+
+/* ArmijoLineSearchHelpFunction_evaluate (gradientDescent.h:168-187) */
+static double armijo_eval(gd_ctx* C, const double* px, const double* py, const double* dx,
+                          const double* dy, double tw) {
+  if (tw == 0) return C->e_at_pos;
+  for (int i = 0; i < C->N; ++i) { C->tx[i] = px[i]; C->tx[i] += tw * dx[i]; }
+  for (int i = 0; i < C->N; ++i) { C->ty[i] = py[i]; C->ty[i] += tw * dy[i]; }
+  const double e = energy_with(C->st, C->level, C->R, C->T, C->tx, C->ty, C->lambda, NULL);
+  C->rb_tau[C->rb_pos] = tw;
+  C->rb_e[C->rb_pos] = e;
+  C->rb_pos ^= 1;
+  C->evals++;
+  return e;
+}
+
+static int finite(double x) { return !isnan(x) && !isinf(x); }
+
+/* getTimestepWidthWithArmijoLineSearch (ArmijoSearch.h:118-200) */
+static double armijo(gd_ctx* C, const double* px, const double* py, const double* dx,
+                     const double* dy, const double* DEx, const double* DEy, double old_tau) {
+  const double sigma = 0.5, tau_min = pow(2., -30.), tau_max = pow(2., 25.);
+  double tau = old_tau < tau_min ? tau_min : (old_tau > tau_max ? tau_max : old_tau);
+  const double f = armijo_eval(C, px, py, dx, dy, 0.);
+  double fnew = armijo_eval(C, px, py, dx, dy, tau);
+  double Df = 0;
+  Df += dot(DEx, dx, C->N);
+  Df += dot(DEy, dy, C->N);
+  double G = (fnew - f) / (Df * tau);
+  if (Df >= 0) return 0;
+  if (!finite(f)) return 0;
+  if (G >= sigma && f >= fnew) {
+    do {
+      tau *= 2.;
+      fnew = armijo_eval(C, px, py, dx, dy, tau);
+      G = (fnew - f) / (Df * tau);
+    } while (G >= sigma && f >= fnew && tau <= tau_max);
+    tau *= 0.5;
+  } else {
+    do {
+      if (tau > tau_min) tau *= 0.5;
+      fnew = armijo_eval(C, px, py, dx, dy, tau);
+      G = (fnew - f) / (Df * tau);
+    } while ((!finite(fnew) || (G < sigma || f < fnew)) && (tau > tau_min));
+  }
+  return (tau > tau_min) ? tau : 0.;
+}
+
+int msor_gd_level(int level, const double* R, const double* T, double* phix, double* phiy,
+                  double lambda, int max_iter, double stop_eps, double* energy_out,
+                  msor_step* trace, int trace_cap) {
+  const int n = lvl_n(level), N = n * n;
+  double* st = stiff_build(level);
+  gd_ctx C;
+  memset(&C, 0, sizeof(C));
+  C.level = level; C.N = N; C.R = R; C.T = T; C.st = st; C.lambda = lambda;
+  C.rb_tau[0] = C.rb_tau[1] = NAN;
+  double* buf = (double*)calloc((size_t)N * 12, sizeof(double));
+  double *dx = buf, *dy = buf + N;            /* descent direction           */
+  double *ogx = buf + 2 * N, *ogy = buf + 3 * N; /* OldGradient              */
+  double *odx = buf + 4 * N, *ody = buf + 5 * N; /* OldDirection             */
+  double *DEx = buf + 6 * N, *DEy = buf + 7 * N; /* cached DE                */
+  C.tx = buf + 8 * N; C.ty = buf + 9 * N;
+  double *sx = buf + 10 * N, *sy = buf + 11 * N;
+
+  double tau = 1.0;              /* startTau (registration.h:52) */
+  double sigma = 1.0;            /* GradientDescentWithAutomaticFilterWidth (gradientDescent.h:688) */
+  const double stop_sigma = 0.0001, sigma_tol = 0.00001;
+  double energy = energy_with(st, level, R, T, phix, phiy, lambda, NULL);
+  double energy_new = energy;
+  int iter = 0, n_trace = 0;
+  if (max_iter <= 0) {
+    if (energy_out) *energy_out = energy_new;
+    free(buf); free(st);
+    return 0;
+  }
+  int go;
+  do {
+    iter++;
+    energy = energy_new;
+    C.e_at_pos = energy;
+    C.evals = 0;
+    const double sigma_used = sigma;
+    /* calcTaudAndDescentDir (gradientDescent.h:200-236) */
+    denergy_with(st, level, R, T, phix, phiy, lambda, DEx, DEy);
+    for (int i = 0; i < N; ++i) { dx[i] = DEx[i] * -1.; dy[i] = DEy[i] * -1.; }
+    msor_smooth(level, sigma, dx, sx); memcpy(dx, sx, sizeof(double) * N);
+    msor_smooth(level, sigma, dy, sy); memcpy(dy, sy, sizeof(double) * N);
+    double beta = 0.;
+    if ((iter - 1) % 10) {
+      double a = 0, b = 0;
+      a += dot(dx, dx, N); a += dot(dy, dy, N);
+      b += dot(ogx, ogx, N); b += dot(ogy, ogy, N);
+      beta = a / b;
+    }
+    memcpy(ogx, dx, sizeof(double) * N); memcpy(ogy, dy, sizeof(double) * N);
+    for (int i = 0; i < N; ++i) { dx[i] += beta * odx[i]; dy[i] += beta * ody[i]; }
+    memcpy(odx, dx, sizeof(double) * N); memcpy(ody, dy, sizeof(double) * N);
+    tau = armijo(&C, phix, phiy, dx, dy, DEx, DEy, tau);
+    for (int i = 0; i < N; ++i) { dx[i] *= tau; dy[i] *= tau; }
+    if (tau == 0) {
+      memcpy(dx, ogx, sizeof(double) * N); memcpy(dy, ogy, sizeof(double) * N);
+      memset(odx, 0, sizeof(double) * N); memset(ody, 0, sizeof(double) * N);
+      tau = armijo(&C, phix, phiy, dx, dy, DEx, DEy, tau);
+      for (int i = 0; i < N; ++i) { dx[i] *= tau; dy[i] *= tau; }
+    }
+    /* energy at the new position (gradientDescent.h:356-395) */
+    double enew = NAN;
+    if (C.rb_tau[0] == tau) enew = C.rb_e[0];
+    else if (C.rb_tau[1] == tau) enew = C.rb_e[1];
+    else if (tau == 0) enew = energy;
+    if (tau != 0) {
+      for (int i = 0; i < N; ++i) { phix[i] += dx[i]; phiy[i] += dy[i]; }
+    }
+    if (isnan(enew)) enew = energy_with(st, level, R, T, phix, phiy, lambda, NULL);
+    energy_new = enew;
+    if (trace && n_trace < trace_cap) {
+      trace[n_trace].iter = iter; trace[n_trace].energy = energy_new; trace[n_trace].tau = tau;
+      trace[n_trace].sigma = sigma_used; trace[n_trace].evals = C.evals; n_trace++;
+    }
+    /* stopping and filter-width schedule (gradientDescent.h:416-439) */
+    go = ((energy - energy_new) > stop_eps) && (iter < max_iter);
+    if ((0.5 * sigma > stop_sigma) && ((energy - energy_new) < sigma_tol)) {
+      sigma *= 0.5;
+      tau = 1.;
+      go = (sigma > stop_sigma) && (iter < max_iter);
+    }
+  } while (go);
+  if (energy_out) *energy_out = energy_new;
+  free(buf);
+  free(st);
+  return iter;
+}
+
+/* --- multilevel driver ------------------------------------------------- */
+
+/* The displacement components of the multilevel descent are qc::Array
+ * (aol::Vector) objects, so resampleInsteadOfProlongateDeformation resamples
+ * the flattened node vector linearly in 1-D: aol::Vector::resampleFrom and
+ * aol::Vector::interpolate (vec.h:461-472, 565-570), as called from
+ * RegistrationMultilevelDescentInterface::prolongate (registration.h:510-521). */
+static void resample_flat(const double* src, int ns, double* dst, int nd) {
+  const double s = (ns - 1) / (double)(nd - 1);
+  for (int i = 0; i < nd; ++i) {
+    const double pos = i * s;
+    const int p = (int)pos;
+    const double pf = pos - p;
+    dst[i] = (p == ns - 1) ? src[p] : (1 - pf) * src[p] + pf * src[p + 1];
+  }
+}
+
+static void phi_up(int level, int resample, double* const* Px, double* const* Py) {
+  if (resample) {
+    const int ns = lvl_n(level) * lvl_n(level), nd = lvl_n(level + 1) * lvl_n(level + 1);
+    resample_flat(Px[level], ns, Px[level + 1], nd);
+    resample_flat(Py[level], ns, Py[level + 1], nd);
+  } else {
+    msor_prolong(level, Px[level], Px[level + 1]);
+    msor_prolong(level, Py[level], Py[level + 1]);
+  }
+}
+
+double msor_register(int max_level, int start_level, int stop_level, const double* R,
+                     const double* T, double* phix, double* phiy, double lambda,
+                     double lambda_factor, int max_iter, double stop_eps, int resample_phi,
+                     int* steps_per_level) {
+  double *Rl[16] = {0}, *Tl[16] = {0}, *Px[16] = {0}, *Py[16] = {0};
+  for (int l = 0; l <= max_level; ++l) {
+    const int n = lvl_n(l);
+    Rl[l] = (double*)calloc((size_t)n * n, sizeof(double));
+    Tl[l] = (double*)calloc((size_t)n * n, sizeof(double));
+    Px[l] = (double*)calloc((size_t)n * n, sizeof(double));
+    Py[l] = (double*)calloc((size_t)n * n, sizeof(double));
+  }
+  const int nm = lvl_n(max_level);
+  memcpy(Rl[max_level], R, sizeof(double) * nm * nm);
+  memcpy(Tl[max_level], T, sizeof(double) * nm * nm);
+  memcpy(Px[max_level], phix, sizeof(double) * nm * nm);
+  memcpy(Py[max_level], phiy, sizeof(double) * nm * nm);
+  /* MultilevelArray::levRestrict (multilevelArray.h:94-110) */
+  for (int l = max_level; l > 0; --l) {
+    msor_restrict(l, Rl[l], Rl[l - 1]);
+    msor_restrict(l, Tl[l], Tl[l - 1]);
+    msor_restrict(l, Px[l], Px[l - 1]);
+    msor_restrict(l, Py[l], Py[l - 1]);
+  }
+  double energy = NAN;
+  int cur = start_level;
+  if (start_level <= stop_level) {
+    for (int level = start_level; level <= stop_level; ++level) {
+      /* getRegularizationWeight (registration.h:523-526) */
+      const double lam = (double)pow(lambda_factor, stop_level - level) * lambda;
+      const int steps = msor_gd_level(level, Rl[level], Tl[level], Px[level], Py[level], lam,
+                                      max_iter, stop_eps, &energy, NULL, 0);
+      if (steps_per_level) steps_per_level[level - start_level] = steps;
+      if (level < stop_level) {
+        phi_up(level, resample_phi, Px, Py);
+        cur = level + 1;
+      }
+    }
+  }
+  for (; cur < max_level; ++cur) phi_up(cur, resample_phi, Px, Py);
+  memcpy(phix, Px[max_level], sizeof(double) * nm * nm);
+  memcpy(phiy, Py[max_level], sizeof(double) * nm * nm);
+  for (int l = 0; l <= max_level; ++l) { free(Rl[l]); free(Tl[l]); free(Px[l]); free(Py[l]); }
+  return energy;
+}
+
+void msor_warp_mean(int level, int F, const double* frames, const double* phis, double* mean,
+                    double* count) {
+  const int n = lvl_n(level), N = n * n;
+  double* def = (double*)malloc(sizeof(double) * (size_t)N * F);
+  for (int f = 0; f < F; ++f)
+    msor_deform_image(level, frames + (size_t)f * N, phis + (size_t)2 * f * N,
+                      phis + (size_t)(2 * f + 1) * N, INFINITY, def + (size_t)f * N);
+  double last_mean = 0;
+  for (int i = 0; i < N; ++i) last_mean += frames[(size_t)(F - 1) * N + i];
+  last_mean /= N;
+  for (int j = 0; j < N; ++j) {
+    double a = 0;
+    int k = 0;
+    for (int f = 0; f < F; ++f) {
+      const double v = def[(size_t)f * N + j];
+      if (v != INFINITY) { a += v; ++k; }
+    }
+    mean[j] = (k > 0) ? a / k : last_mean;
+    count[j] = k;
+  }
+  free(def);
+}

@@ -1,0 +1,266 @@
+"""ctypes binding of the FP64 CPU restatement (oracle/libmsoracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by the smoke check and by the
+CPU-baseline leg of bench.py, as the checker.  The product never imports it.
+Also wraps the reference driver oracle/_ref/ms_ref when it has been built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmsoracle.so")
+REF_BIN = os.path.join(HERE, "_ref", "ms_ref")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class Step(ctypes.Structure):
+    _fields_ = [("iter", ctypes.c_int), ("energy", ctypes.c_double), ("tau", ctypes.c_double),
+                ("sigma", ctypes.c_double), ("evals", ctypes.c_int)]
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-f", os.path.join(HERE, "Makefile")], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        L.msor_ssd_energy.restype = ctypes.c_double
+        L.msor_energy.restype = ctypes.c_double
+        L.msor_register.restype = ctypes.c_double
+        L.msor_gd_level.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_dp)
+
+
+def n_of(level: int) -> int:
+    return (1 << level) + 1
+
+
+def _c(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def ssd_energy(level, R, T, px, py):
+    return lib().msor_ssd_energy(level, _p(_c(R)), _p(_c(T)), _p(_c(px)), _p(_c(py)))
+
+
+def energy(level, R, T, px, py, lam):
+    ereg = ctypes.c_double()
+    e = lib().msor_energy(level, _p(_c(R)), _p(_c(T)), _p(_c(px)), _p(_c(py)),
+                          ctypes.c_double(lam), ctypes.byref(ereg))
+    return e, ereg.value
+
+
+def denergy(level, R, T, px, py, lam):
+    n = n_of(level)
+    gx = np.zeros(n * n)
+    gy = np.zeros(n * n)
+    lib().msor_denergy(level, _p(_c(R)), _p(_c(T)), _p(_c(px)), _p(_c(py)), ctypes.c_double(lam),
+                       _p(gx), _p(gy))
+    return gx, gy
+
+
+def ssd_force(level, R, T, px, py):
+    n = n_of(level)
+    gx = np.zeros(n * n)
+    gy = np.zeros(n * n)
+    lib().msor_ssd_force(level, _p(_c(R)), _p(_c(T)), _p(_c(px)), _p(_c(py)), _p(gx), _p(gy))
+    return gx, gy
+
+
+def stiff_apply(level, u):
+    out = np.zeros(n_of(level) ** 2)
+    lib().msor_stiff_apply(level, _p(_c(u)), _p(out))
+    return out
+
+
+def smooth(level, sigma, x):
+    out = np.zeros(n_of(level) ** 2)
+    lib().msor_smooth(level, ctypes.c_double(sigma), _p(_c(x)), _p(out))
+    return out
+
+
+def restrict(fine_level, x):
+    out = np.zeros(n_of(fine_level - 1) ** 2)
+    lib().msor_restrict(fine_level, _p(_c(x)), _p(out))
+    return out
+
+
+def prolong(coarse_level, x):
+    out = np.zeros(n_of(coarse_level + 1) ** 2)
+    lib().msor_prolong(coarse_level, _p(_c(x)), _p(out))
+    return out
+
+
+def resample(src_level, x, dst_level):
+    out = np.zeros(n_of(dst_level) ** 2)
+    lib().msor_resample(src_level, _p(_c(x)), dst_level, _p(out))
+    return out
+
+
+def deform_image(level, img, px, py, ext=np.inf):
+    out = np.zeros(n_of(level) ** 2)
+    lib().msor_deform_image(level, _p(_c(img)), _p(_c(px)), _p(_c(py)), ctypes.c_double(ext), _p(out))
+    return out
+
+
+def normalize(img, sat=0.15, min_to_zero=1):
+    a = _c(img).copy()
+    lib().msor_normalize(_p(a), a.size, ctypes.c_double(sat), min_to_zero)
+    return a
+
+
+def gd_level(level, R, T, px, py, lam, max_iter, stop_eps=0.0, trace_cap=4096):
+    px = _c(px).copy()
+    py = _c(py).copy()
+    tr = (Step * trace_cap)()
+    e = ctypes.c_double()
+    steps = lib().msor_gd_level(level, _p(_c(R)), _p(_c(T)), _p(px), _p(py), ctypes.c_double(lam),
+                                max_iter, ctypes.c_double(stop_eps), ctypes.byref(e), tr, trace_cap)
+    trace = [(tr[i].iter, tr[i].energy, tr[i].tau, tr[i].sigma, tr[i].evals) for i in range(min(steps, trace_cap))]
+    return px, py, e.value, steps, trace
+
+
+def register(max_level, start, stop, R, T, px=None, py=None, lam=0.1, lam_factor=1.0,
+             max_iter=20, stop_eps=0.0, resample_phi=False):
+    N = n_of(max_level) ** 2
+    px = np.zeros(N) if px is None else _c(px).copy()
+    py = np.zeros(N) if py is None else _c(py).copy()
+    steps = (ctypes.c_int * max(1, stop - start + 1))()
+    e = lib().msor_register(max_level, start, stop, _p(_c(R)), _p(_c(T)), _p(px), _p(py),
+                            ctypes.c_double(lam), ctypes.c_double(lam_factor), max_iter,
+                            ctypes.c_double(stop_eps), int(bool(resample_phi)), steps)
+    return px, py, e, list(steps)
+
+
+def warp_mean(level, frames, phis):
+    n = n_of(level)
+    F = frames.shape[0]
+    mean = np.zeros(n * n)
+    count = np.zeros(n * n)
+    lib().msor_warp_mean(level, F, _p(_c(frames).reshape(-1)), _p(_c(phis).reshape(-1)), _p(mean), _p(count))
+    return mean, count
+
+
+# --- reference driver (oracle/_ref/ms_ref) ---------------------------------
+
+def have_ref() -> bool:
+    return os.path.exists(REF_BIN)
+
+
+class RefRunner:
+    """Runs the reference's own templates through oracle/_ref/ms_ref."""
+
+    def __init__(self):
+        self.dir = tempfile.mkdtemp(prefix="msref_")
+
+    def _w(self, name, a):
+        p = os.path.join(self.dir, name)
+        _c(a).tofile(p)
+        return p
+
+    def _r(self, name, count=None):
+        a = np.fromfile(os.path.join(self.dir, name), dtype=np.float64)
+        return a if count is None else a[:count]
+
+    def run(self, *args):
+        subprocess.run([REF_BIN, *map(str, args)], check=True, stdout=subprocess.DEVNULL,
+                       stderr=subprocess.DEVNULL)
+
+    def energy(self, level, R, T, px, py, lam):
+        N = n_of(level) ** 2
+        self.run("energy", level, self._w("R", R), self._w("T", T), self._w("px", px), self._w("py", py),
+                 repr(float(lam)), os.path.join(self.dir, "e"))
+        essd, ereg, etot = map(float, open(os.path.join(self.dir, "e.txt")).read().split())
+        de = self._r("e_de.bin")
+        return dict(essd=essd, ereg=ereg, e=etot, dex=de[:N], dey=de[N:2 * N], fx=de[2 * N:3 * N], fy=de[3 * N:])
+
+    def smooth(self, level, sigma, x):
+        self.run("smooth", level, repr(float(sigma)), self._w("in", x), os.path.join(self.dir, "out"))
+        return self._r("out")
+
+    def restrict(self, fine_level, x):
+        self.run("restrict", fine_level, self._w("in", x), os.path.join(self.dir, "out"))
+        return self._r("out")
+
+    def prolong(self, coarse_level, x):
+        self.run("prolong", coarse_level, self._w("in", x), os.path.join(self.dir, "out"))
+        return self._r("out")
+
+    def resample(self, src_level, x, dst_level):
+        self.run("resample", src_level, self._w("in", x), dst_level, os.path.join(self.dir, "out"))
+        return self._r("out")
+
+    def deform(self, level, img, px, py):
+        self.run("deform", level, self._w("img", img), self._w("px", px), self._w("py", py),
+                 os.path.join(self.dir, "out"))
+        return self._r("out")
+
+    def normalize(self, level, img, sat=0.15, min_to_zero=1):
+        self.run("normalize", level, self._w("img", img), repr(float(sat)), min_to_zero,
+                 os.path.join(self.dir, "out"))
+        return self._r("out")
+
+    def gd_level(self, level, R, T, px, py, lam, max_iter, stop_eps=0.0):
+        N = n_of(level) ** 2
+        self.run("gdlevel", level, self._w("R", R), self._w("T", T), self._w("px", px), self._w("py", py),
+                 repr(float(lam)), max_iter, repr(float(stop_eps)), os.path.join(self.dir, "phi"),
+                 os.path.join(self.dir, "trace.txt"))
+        phi = self._r("phi")
+        lines = open(os.path.join(self.dir, "trace.txt")).read().splitlines()
+        head = lines[0].split()
+        final_e = float(head[head.index("final") + 1])
+        steps = int(head[head.index("steps") + 1])
+        rows = [l.split() for l in lines[1:]]
+        trace = [(int(r[0]), float(r[1]), float(r[2]), float(r[3]), int(r[4])) for r in rows]
+        return phi[:N], phi[N:], final_e, steps, trace
+
+    def register(self, max_level, start, stop, R, T, px=None, py=None, lam=0.1, lam_factor=1.0,
+                 max_iter=20, stop_eps=0.0, resample_phi=False):
+        N = n_of(max_level) ** 2
+        px = np.zeros(N) if px is None else px
+        py = np.zeros(N) if py is None else py
+        self.run("register", max_level, start, stop, self._w("R", R), self._w("T", T), self._w("px", px),
+                 self._w("py", py), repr(float(lam)), repr(float(lam_factor)), max_iter, repr(float(stop_eps)),
+                 int(bool(resample_phi)), os.path.join(self.dir, "phi"), os.path.join(self.dir, "e.txt"))
+        phi = self._r("phi")
+        return phi[:N], phi[N:], float(open(os.path.join(self.dir, "e.txt")).read())
+
+    def series(self, max_level, start, stop, frames, lam, lam_factor, max_iter, stop_eps=0.0, sat=0.15,
+               min_to_zero=1):
+        F = frames.shape[0]
+        N = n_of(max_level) ** 2
+        self.run("series", max_level, start, stop, repr(float(lam)), repr(float(lam_factor)), max_iter,
+                 repr(float(stop_eps)), repr(float(sat)), min_to_zero, F, self._w("frames", frames),
+                 os.path.join(self.dir, "phis"), os.path.join(self.dir, "mean"), os.path.join(self.dir, "s.txt"))
+        phis = self._r("phis").reshape(F, 2, N)
+        mean = self._r("mean")
+        info = {}
+        energies = {}
+        for line in open(os.path.join(self.dir, "s.txt")):
+            t = line.split()
+            if t[0] == "energy":
+                energies[int(t[1])] = float(t[2])
+            else:
+                info[t[0]] = float(t[1])
+        info["energies"] = [energies[i] for i in range(F)]
+        return phis, mean, info

@@ -1,0 +1,337 @@
+// ref_driver.cpp -- command-line driver over the reference's OWN templates.
+//
+// TEST INFRASTRUCTURE ONLY.  Compiled by oracle/Makefile.ref against the
+// quocmesh sources (their headers and .cpp files, left where they are) into
+// oracle/_ref/ms_ref.  It pins the CPU restatement (oracle/ms_oracle.c) and is
+// the CPU baseline that the benchmark times.  No reference source is copied:
+// every operator below is instantiated from the reference headers.
+//
+// Arrays are raw little-endian float64 files, x fastest (quoc ILex order).
+// The configurator is the dyadic 2^l+1 grid with Q1 elements and 2x2 Gauss
+// quadrature (QuocConfiguratorTraitMultiLin, configurators.h:218-330), with the
+// SSD data term (registration.h:1257-1273), the Dirichlet regulariser
+// (registration.h:677-710) and the H1 gradient flow with automatic filter
+// width (gradientDescent.h:632-709).
+#include <registration.h>
+#include <configurators.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <fstream>
+#include <sys/time.h>
+#include <vector>
+
+typedef double RealType;
+typedef qc::QuocConfiguratorTraitMultiLin<RealType, qc::QC_2D, aol::GaussQuadrature<RealType, qc::QC_2D, 3> > ConfType;
+typedef qc::ScalarArray<RealType, qc::QC_2D> ArrayType;
+typedef qc::StandardRegistrationMultilevelDescent<ConfType, qc::SSDRegistrationConfigurator<ConfType> > RegisType;
+typedef aol::H1GradientDescent<ConfType, aol::MultiVector<RealType>, qc::LinearSmoothOp<RealType> > H1Type;
+typedef aol::GradientDescentWithAutomaticFilterWidth<ConfType, aol::MultiVector<RealType>, H1Type> GDType;
+
+static int lvlN ( int l ) { return ( 1 << l ) + 1; }
+
+static void readBin ( const char *path, RealType *dst, size_t count ) {
+  FILE *f = fopen ( path, "rb" );
+  if ( !f ) { fprintf ( stderr, "cannot open %s\n", path ); exit ( 2 ); }
+  if ( fread ( dst, sizeof ( RealType ), count, f ) != count ) { fprintf ( stderr, "short read %s\n", path ); exit ( 2 ); }
+  fclose ( f );
+}
+
+static void writeBin ( const char *path, const RealType *src, size_t count ) {
+  FILE *f = fopen ( path, "wb" );
+  if ( !f ) { fprintf ( stderr, "cannot write %s\n", path ); exit ( 2 ); }
+  fwrite ( src, sizeof ( RealType ), count, f );
+  fclose ( f );
+}
+
+static double wallSeconds ( ) {
+  struct timeval tv;
+  gettimeofday ( &tv, NULL );
+  return tv.tv_sec + 1e-6 * tv.tv_usec;
+}
+
+// A GD solver that records, per step, the accepted tau, the filter width used
+// and the energy after the step.  Only observation hooks are overridden; the
+// descent itself is the reference's applySingle.
+class TracingGD : public GDType {
+public:
+  mutable std::vector<double> energies, taus, sigmas;
+  mutable std::vector<int> evals;
+  mutable int evalCount;
+  mutable double lastTau, lastSigma;
+  TracingGD ( const qc::GridDefinition &Grid, const aol::Op<aol::MultiVector<double>, aol::Scalar<double> > &E,
+              const aol::Op<aol::MultiVector<double> > &DE, int MaxIter, double StopEps )
+    : GDType ( Grid, E, DE, MaxIter, 1., StopEps ), evalCount ( 0 ), lastTau ( 0 ), lastSigma ( 0 ) {}
+  void writeEnergy ( const double CurrentEnergy ) const {
+    if ( this->_iterations == 0 ) { energies.push_back ( CurrentEnergy ); taus.push_back ( 0 ); sigmas.push_back ( 0 ); evals.push_back ( 0 ); return; }
+    energies.push_back ( CurrentEnergy ); taus.push_back ( lastTau ); sigmas.push_back ( lastSigma ); evals.push_back ( evalCount );
+    evalCount = 0;
+  }
+protected:
+  void getTauAndUpdateDescentDir ( aol::MultiVector<double> &DescentDir, const aol::MultiVector<double> &CurrentPosition, aol::Vector<double> &Tau ) const {
+    lastSigma = this->_filterWidth;
+    GDType::getTauAndUpdateDescentDir ( DescentDir, CurrentPosition, Tau );
+    lastTau = Tau[0];
+  }
+  double ArmijoLineSearchHelpFunction_evaluate ( const aol::MultiVector<double> &DescentDir, const aol::MultiVector<double> &CurrentPosition, const double TimestepWidth ) const {
+    if ( TimestepWidth != 0 ) ++evalCount;
+    return GDType::ArmijoLineSearchHelpFunction_evaluate ( DescentDir, CurrentPosition, TimestepWidth );
+  }
+};
+
+static aol::ParameterParser* makeParser ( int maxLevel, int start, int stop, double lambda, double lambdaFactor,
+                                          int maxIter, double stopEps, int resample, double sat, int minToZero ) {
+  aol::ParameterParser *p = new aol::ParameterParser;
+  p->addVariable ( "precisionLevel", maxLevel );
+  p->addVariable ( "startLevel", start );
+  p->addVariable ( "stopLevel", stop );
+  p->addVariable ( "lambda", aol::strprintf ( "%.17g", lambda ).c_str() );
+  p->addVariable ( "lambdaFactor", aol::strprintf ( "%.17g", lambdaFactor ).c_str() );
+  p->addVariable ( "maxGDIterations", maxIter );
+  p->addVariable ( "stopEpsilon", aol::strprintf ( "%.17g", stopEps ).c_str() );
+  if ( resample ) p->addVariable ( "resampleInsteadOfProlongateDeformation", 1 );
+  if ( sat >= 0 ) p->addVariable ( "enhanceContrastSaturationPercentage", aol::strprintf ( "%.17g", sat ).c_str() );
+  p->addVariable ( "normalizeMinToZero", minToZero );
+  return p;
+}
+
+static int usage ( ) {
+  fprintf ( stderr,
+    "ms_ref energy L R T px py lambda outPrefix\n"
+    "ms_ref smooth L sigma in out\n"
+    "ms_ref restrict Lfine in out | prolong Lcoarse in out | resample Lsrc in Ldst out\n"
+    "ms_ref deform L img px py out\n"
+    "ms_ref gdlevel L R T px py lambda maxIter stopEps outPhi outTrace\n"
+    "ms_ref register maxL start stop R T px py lambda lambdaFactor maxIter stopEps resample outPhi outTxt\n"
+    "ms_ref normalize L in sat minToZero out\n"
+    "ms_ref series maxL start stop lambda lambdaFactor maxIter stopEps sat minToZero F framesBin outPhis outMean outTxt\n" );
+  return 1;
+}
+
+int main ( int argc, char **argv ) {
+  if ( argc < 2 ) return usage ( );
+  const std::string cmd = argv[1];
+  try {
+    if ( cmd == "energy" && argc == 9 ) {
+      const int L = atoi ( argv[2] ), n = lvlN ( L ), N = n * n;
+      qc::GridDefinition grid ( L, qc::QC_2D );
+      ArrayType R ( grid ), T ( grid );
+      aol::MultiVector<RealType> phi ( 2, N ), de ( 2, N );
+      readBin ( argv[3], R.getData ( ), N ); readBin ( argv[4], T.getData ( ), N );
+      readBin ( argv[5], phi[0].getData ( ), N ); readBin ( argv[6], phi[1].getData ( ), N );
+      const RealType lambda = atof ( argv[7] );
+      qc::SSDEnergy<ConfType> ssd ( grid, R, T );
+      qc::SSDForce<ConfType> force ( grid, R, T );
+      qc::DirichletRegularizationConfigurator<ConfType> regul ( grid );
+      aol::LinCombOp<aol::MultiVector<RealType>, aol::Scalar<RealType> > E;
+      E.appendReference ( ssd ); E.appendReference ( regul.getRegERef ( ), lambda );
+      aol::LinCombOp<aol::MultiVector<RealType> > DE;
+      DE.appendReference ( force ); DE.appendReference ( regul.getRegDERef ( ), lambda );
+      aol::Scalar<RealType> essd, ereg, etot;
+      ssd.apply ( phi, essd ); regul.getRegERef ( ).apply ( phi, ereg ); E.apply ( phi, etot );
+      DE.apply ( phi, de );
+      aol::MultiVector<RealType> fo ( 2, N );
+      force.apply ( phi, fo );
+      std::vector<RealType> out ( 4 * N );
+      memcpy ( &out[0], de[0].getData ( ), N * sizeof ( RealType ) );
+      memcpy ( &out[N], de[1].getData ( ), N * sizeof ( RealType ) );
+      memcpy ( &out[2 * N], fo[0].getData ( ), N * sizeof ( RealType ) );
+      memcpy ( &out[3 * N], fo[1].getData ( ), N * sizeof ( RealType ) );
+      writeBin ( ( std::string ( argv[8] ) + "_de.bin" ).c_str ( ), &out[0], 4 * N );
+      FILE *f = fopen ( ( std::string ( argv[8] ) + ".txt" ).c_str ( ), "w" );
+      fprintf ( f, "%.17g %.17g %.17g\n", essd[0], ereg[0], etot[0] );
+      fclose ( f );
+      return 0;
+    }
+    if ( cmd == "smooth" && argc == 6 ) {
+      const int L = atoi ( argv[2] ), n = lvlN ( L ), N = n * n;
+      qc::GridDefinition grid ( L, qc::QC_2D );
+      aol::Vector<RealType> in ( N ), out ( N );
+      readBin ( argv[4], in.getData ( ), N );
+      qc::LinearSmoothOp<RealType> smooth ( grid );
+      smooth.setSigma ( atof ( argv[3] ) );
+      smooth.apply ( in, out );
+      writeBin ( argv[5], out.getData ( ), N );
+      return 0;
+    }
+    if ( cmd == "restrict" && argc == 5 ) {
+      const int L = atoi ( argv[2] );
+      qc::GridDefinition fine ( L, qc::QC_2D ), coarse ( L - 1, qc::QC_2D );
+      aol::Vector<RealType> in ( fine.getNumberOfNodes ( ) ), out ( coarse.getNumberOfNodes ( ) );
+      readBin ( argv[3], in.getData ( ), in.size ( ) );
+      qc::RestrictOp<RealType, qc::STD_QUOC_RESTRICT> r ( coarse, fine );
+      r.apply ( in, out );
+      writeBin ( argv[4], out.getData ( ), out.size ( ) );
+      return 0;
+    }
+    if ( cmd == "prolong" && argc == 5 ) {
+      const int L = atoi ( argv[2] );
+      qc::GridDefinition coarse ( L, qc::QC_2D ), fine ( L + 1, qc::QC_2D );
+      aol::Vector<RealType> in ( coarse.getNumberOfNodes ( ) ), out ( fine.getNumberOfNodes ( ) );
+      readBin ( argv[3], in.getData ( ), in.size ( ) );
+      qc::ProlongOp<RealType> p ( coarse, fine );
+      p.apply ( in, out );
+      writeBin ( argv[4], out.getData ( ), out.size ( ) );
+      return 0;
+    }
+    if ( cmd == "resample" && argc == 6 ) {
+      const int Ls = atoi ( argv[2] ), Ld = atoi ( argv[4] );
+      qc::GridDefinition gs ( Ls, qc::QC_2D ), gd ( Ld, qc::QC_2D );
+      ArrayType src ( gs ), dst ( gd );
+      readBin ( argv[3], src.getData ( ), src.size ( ) );
+      dst.resampleFrom ( src );
+      writeBin ( argv[5], dst.getData ( ), dst.size ( ) );
+      return 0;
+    }
+    if ( cmd == "deform" && argc == 7 ) {
+      const int L = atoi ( argv[2] ), n = lvlN ( L ), N = n * n;
+      qc::GridDefinition grid ( L, qc::QC_2D );
+      aol::Vector<RealType> img ( N ), out ( N );
+      aol::MultiVector<RealType> phi ( 2, N );
+      readBin ( argv[3], img.getData ( ), N );
+      readBin ( argv[4], phi[0].getData ( ), N ); readBin ( argv[5], phi[1].getData ( ), N );
+      qc::DeformImage<ConfType> ( img, grid, out, phi, true, aol::NumberTrait<RealType>::Inf, false );
+      writeBin ( argv[6], out.getData ( ), N );
+      return 0;
+    }
+    if ( cmd == "gdlevel" && argc == 12 ) {
+      const int L = atoi ( argv[2] ), n = lvlN ( L ), N = n * n;
+      qc::GridDefinition grid ( L, qc::QC_2D );
+      ArrayType R ( grid ), T ( grid );
+      aol::MultiVector<RealType> phi ( 2, N );
+      readBin ( argv[3], R.getData ( ), N ); readBin ( argv[4], T.getData ( ), N );
+      readBin ( argv[5], phi[0].getData ( ), N ); readBin ( argv[6], phi[1].getData ( ), N );
+      const RealType lambda = atof ( argv[7] );
+      const int maxIter = atoi ( argv[8] );
+      const RealType stopEps = atof ( argv[9] );
+      // StandardRegistration::findTransformation + updateTransformationWithGD (registration.h:967-1021)
+      qc::SSDEnergy<ConfType> ssd ( grid, R, T );
+      qc::SSDForce<ConfType> force ( grid, R, T );
+      qc::DirichletRegularizationConfigurator<ConfType> regul ( grid );
+      aol::LinCombOp<aol::MultiVector<RealType>, aol::Scalar<RealType> > E;
+      E.appendReference ( ssd ); E.appendReference ( regul.getRegERef ( ), lambda );
+      aol::LinCombOp<aol::MultiVector<RealType> > DE;
+      DE.appendReference ( force ); DE.appendReference ( regul.getRegDERef ( ), lambda );
+      TracingGD gd ( grid, E, DE, maxIter, stopEps );
+      gd.setConfigurationFlags ( GDType::USE_NONLINEAR_CG | GDType::DO_NOT_WRITE_CONSOLE_OUTPUT );
+      gd.applySingle ( phi );
+      std::vector<RealType> out ( 2 * N );
+      memcpy ( &out[0], phi[0].getData ( ), N * sizeof ( RealType ) );
+      memcpy ( &out[N], phi[1].getData ( ), N * sizeof ( RealType ) );
+      writeBin ( argv[10], &out[0], 2 * N );
+      FILE *f = fopen ( argv[11], "w" );
+      fprintf ( f, "# iter energy tau sigma evals ; final %.17g steps %d\n", gd.getEnergyAtLastPosition ( ), gd.getIterations ( ) );
+      for ( size_t i = 0; i < gd.energies.size ( ); ++i )
+        fprintf ( f, "%d %.17g %.17g %.17g %d\n", ( int ) i, gd.energies[i], gd.taus[i], gd.sigmas[i], gd.evals[i] );
+      fclose ( f );
+      return 0;
+    }
+    if ( cmd == "register" && argc == 16 ) {
+      const int maxL = atoi ( argv[2] ), start = atoi ( argv[3] ), stop = atoi ( argv[4] );
+      const int n = lvlN ( maxL ), N = n * n;
+      aol::ParameterParser *parser = makeParser ( maxL, start, stop, atof ( argv[9] ), atof ( argv[10] ), atoi ( argv[11] ),
+                                                  atof ( argv[12] ), atoi ( argv[13] ), -1, 0 );
+      RegisType regis ( *parser );
+      qc::GridDefinition grid ( maxL, qc::QC_2D );
+      ArrayType R ( grid ), T ( grid );
+      readBin ( argv[5], R.getData ( ), N ); readBin ( argv[6], T.getData ( ), N );
+      regis.initRefOrTemplate ( R, qc::REFERENCE, true );
+      regis.initRefOrTemplate ( T, qc::TEMPLATE, true );
+      qc::MultiArray<RealType, qc::QC_2D> phi ( grid );
+      readBin ( argv[7], phi[0].getData ( ), N ); readBin ( argv[8], phi[1].getData ( ), N );
+      regis.setTransformation ( phi );
+      regis.solveAndProlongToMaxDepth ( );
+      regis.getTransformation ( phi );
+      std::vector<RealType> out ( 2 * N );
+      memcpy ( &out[0], phi[0].getData ( ), N * sizeof ( RealType ) );
+      memcpy ( &out[N], phi[1].getData ( ), N * sizeof ( RealType ) );
+      writeBin ( argv[14], &out[0], 2 * N );
+      FILE *f = fopen ( argv[15], "w" );
+      fprintf ( f, "%.17g\n", regis.getEnergyOfLastSolution ( ) );
+      fclose ( f );
+      delete parser;
+      return 0;
+    }
+    if ( cmd == "normalize" && argc == 7 ) {
+      const int L = atoi ( argv[2] ), n = lvlN ( L ), N = n * n;
+      aol::ParameterParser *parser = makeParser ( L, L, L, 1, 1, 1, 0, 0, atof ( argv[4] ), atoi ( argv[5] ) );
+      RegisType regis ( *parser );
+      qc::GridDefinition grid ( L, qc::QC_2D );
+      ArrayType img ( grid );
+      readBin ( argv[3], img.getData ( ), N );
+      regis.initRefOrTemplate ( img, qc::REFERENCE, false );
+      writeBin ( argv[6], regis.getRefImageReference ( ).getData ( ), N );
+      delete parser;
+      return 0;
+    }
+    if ( cmd == "series" && argc == 16 ) {
+      // One stage of series matching with a fixed reference: every frame is
+      // prepared (normalised), registered to the reference from a zero
+      // displacement, and the raw frames are averaged after warping
+      // (matchSeries.h:141-155, 385-425).  Frame 0 of framesBin is the reference.
+      const int maxL = atoi ( argv[2] ), start = atoi ( argv[3] ), stop = atoi ( argv[4] );
+      const int n = lvlN ( maxL ), N = n * n;
+      const int F = atoi ( argv[11] );
+      aol::ParameterParser *parser = makeParser ( maxL, start, stop, atof ( argv[5] ), atof ( argv[6] ), atoi ( argv[7] ),
+                                                  atof ( argv[8] ), 0, atof ( argv[9] ), atoi ( argv[10] ) );
+      RegisType regis ( *parser );
+      qc::GridDefinition grid ( maxL, qc::QC_2D );
+      std::vector<RealType> frames ( ( size_t ) N * F );
+      readBin ( argv[12], &frames[0], ( size_t ) N * F );
+      ArrayType ref ( grid );
+      memcpy ( ref.getData ( ), &frames[0], N * sizeof ( RealType ) );
+      const double t0 = wallSeconds ( );
+      regis.initRefOrTemplate ( ref, qc::REFERENCE, false );
+      std::vector<RealType> phis ( ( size_t ) 2 * N * F, 0. );
+      std::vector<double> energies ( F, 0. );
+      qc::MultiArray<RealType, qc::QC_2D> phi ( grid );
+      for ( int f = 1; f < F; ++f ) {
+        ArrayType tpl ( grid );
+        memcpy ( tpl.getData ( ), &frames[( size_t ) f * N], N * sizeof ( RealType ) );
+        regis.initRefOrTemplate ( tpl, qc::TEMPLATE, false );
+        regis.setTransformationToZero ( );
+        regis.solveAndProlongToMaxDepth ( );
+        regis.getTransformation ( phi );
+        energies[f] = regis.getEnergyOfLastSolution ( );
+        memcpy ( &phis[( size_t ) 2 * f * N], phi[0].getData ( ), N * sizeof ( RealType ) );
+        memcpy ( &phis[( size_t ) ( 2 * f + 1 ) * N], phi[1].getData ( ), N * sizeof ( RealType ) );
+      }
+      const double t1 = wallSeconds ( );
+      // averageSeries: DeformImage with Inf extension, mean over finite samples.
+      std::vector<RealType> mean ( N, 0. );
+      {
+        aol::MultiVector<RealType> deformed ( F, N );
+        for ( int f = 0; f < F; ++f ) {
+          aol::Vector<RealType> img ( &frames[( size_t ) f * N], N, aol::FLAT_COPY );
+          aol::MultiVector<RealType> p ( 2, N );
+          memcpy ( p[0].getData ( ), &phis[( size_t ) 2 * f * N], N * sizeof ( RealType ) );
+          memcpy ( p[1].getData ( ), &phis[( size_t ) ( 2 * f + 1 ) * N], N * sizeof ( RealType ) );
+          qc::DeformImage<ConfType> ( img, grid, deformed[f], p, true, aol::NumberTrait<RealType>::Inf, false );
+        }
+        aol::Vector<RealType> last ( &frames[( size_t ) ( F - 1 ) * N], N, aol::FLAT_COPY );
+        const RealType lastMean = last.getMeanValue ( );
+        for ( int j = 0; j < N; ++j ) {
+          RealType a = 0; int k = 0;
+          for ( int f = 0; f < F; ++f )
+            if ( deformed[f][j] != aol::NumberTrait<RealType>::Inf ) { a += deformed[f][j]; ++k; }
+          mean[j] = ( k > 0 ) ? a / k : lastMean;
+        }
+      }
+      const double t2 = wallSeconds ( );
+      writeBin ( argv[13], &phis[0], ( size_t ) 2 * N * F );
+      writeBin ( argv[14], &mean[0], N );
+      FILE *f = fopen ( argv[15], "w" );
+      fprintf ( f, "registration_seconds %.6f\naverage_seconds %.6f\n", t1 - t0, t2 - t1 );
+      for ( int i = 0; i < F; ++i ) fprintf ( f, "energy %d %.17g\n", i, energies[i] );
+      fclose ( f );
+      delete parser;
+      return 0;
+    }
+  } catch ( aol::Exception &e ) {
+    e.dump ( );
+    return 3;
+  }
+  return usage ( );
+}
