@@ -1,0 +1,401 @@
+#!/usr/bin/env python
+"""Benchmark: registered frames/s for one stage of series matching at 513^2.
+
+Workload (per GPU): 20 frames of a hexagonal Gaussian-column lattice, 513x513
+(level 9), Poisson peak 30, smooth displacements <= 3 px plus 0.7 px row
+jitter, registered to a reference frame of the same series on levels 5..9
+(maxGDIterations 30, lambda 0.1, reference preprocessing with saturation
+0.15 %), followed by the warped-frame average.  One bench step = one such
+stage (all 20 registrations + the average).  Seeded synthetic data.
+
+  value : frames/s with the images resident in HBM (device entry point)
+  e2e   : frames/s through the host entry point msgpu_match_series_stage with
+          pinned host buffers (uploads and downloads inside the timed region)
+
+--impl reference times the reference's own CPU code (oracle/_ref/ms_ref, the
+quocmesh templates built from the reference sources) on a bounded sample of
+the same workload, one process per host core.
+
+Multi-GPU (torchrun): weak scaling; every rank registers its own series.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "match-series_b200"))
+
+METRIC = "registered frames/s at 513² to stated energy tol: warm-start+batched vs plain GPU"
+UNIT = "frames/s"
+LEVEL, START, FRAMES, MAX_ITER, LAMBDA = 9, 5, 20, 30, 0.1
+
+
+def workload(rank: int):
+    from msgpu import synthetic as syn
+    n = (1 << LEVEL) + 1
+    frames, clean, _ = syn.make_series(n, FRAMES + 1, syn.HEX_513, seed=2000 + 1000 * rank)
+    ref = frames[FRAMES].reshape(-1).copy()   # the reference frame of the stage
+    tmpl = frames[:FRAMES].reshape(FRAMES, -1).copy()
+    return ref, tmpl, clean[FRAMES]
+
+
+def params(fp64: bool):
+    import msgpu
+    return msgpu.default_params(precision_level=LEVEL, input_level=LEVEL, start_level=START, stop_level=LEVEL,
+                                max_gd_iterations=MAX_ITER, use_fp64=int(fp64))
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                t = [x.strip() for x in line.split(",")]
+                if len(t) >= 9 and t[1].replace(".", "").isdigit():
+                    rows.append(t)
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows]
+        mx = max(float(r[2]) for r in rows)
+        load = [s for s in sm if s > 0.5 * mx] or sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def level_traffic(fp64: bool):
+    """DRAM bytes per launch of the finest-level kernel from the committed ncu summary (or None)."""
+    try:
+        d = json.load(open(os.path.join(ROOT, "profiles", "level_kernel_traffic.json")))
+        return d.get("f64" if fp64 else "f32", {}).get("bytes_per_launch_513x20")
+    except Exception:
+        return None
+
+
+def algorithmic_bytes(steps: int, evals: int, real_bytes: int) -> float:
+    """Per-level algorithmic bytes: per node and frame 24 B per energy trial,
+    24 B gradient + 20 B NCG/update per step, 96 B per V-cycle component with
+    2 components per step (FP32 figures, scaled by the word size)."""
+    n = (1 << LEVEL) + 1
+    return n * n * (24.0 * evals + (24.0 + 20.0 + 2 * 96.0) * steps) * (real_bytes / 4.0)
+
+
+# --- CPU baseline: the reference binary on a bounded sample ------------------
+
+def run_reference_sample(ref, tmpl, procs: int, workdir: str):
+    """Registers `procs` templates with the reference (one process each, in
+    parallel); returns (frames, seconds, phis, energies, kind)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import msor
+    n = (1 << LEVEL) + 1
+    N = n * n
+    if msor.have_ref():
+        jobs = []
+        for i in range(procs):
+            d = os.path.join(workdir, f"r{i}")
+            os.makedirs(d, exist_ok=True)
+            fr = np.stack([ref, tmpl[i]])
+            fr.tofile(os.path.join(d, "frames.bin"))
+            cmd = [msor.REF_BIN, "series", str(LEVEL), str(START), str(LEVEL), repr(LAMBDA), "1.0", str(MAX_ITER),
+                   "0.0", "0.15", "1", "2", os.path.join(d, "frames.bin"), os.path.join(d, "phis.bin"),
+                   os.path.join(d, "mean.bin"), os.path.join(d, "info.txt")]
+            jobs.append(subprocess.Popen(cmd, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL))
+        t0 = time.perf_counter()
+        for j in jobs:
+            j.wait()
+        wall = time.perf_counter() - t0
+        secs, phis, energies = [], [], []
+        for i in range(procs):
+            d = os.path.join(workdir, f"r{i}")
+            info = {}
+            for line in open(os.path.join(d, "info.txt")):
+                t = line.split()
+                info[t[0] + (t[1] if t[0] == "energy" else "")] = float(t[-1])
+            secs.append(info["registration_seconds"])
+            phis.append(np.fromfile(os.path.join(d, "phis.bin")).reshape(2, 2, N)[1])
+            energies.append(info["energy1"])
+        # registration phase only (the driver's own clock, file I/O excluded)
+        return procs, max(secs), np.array(phis), np.array(energies), "reference", wall
+    # the CPU restatement when the reference binary is not available here
+    import multiprocessing as mp
+    msor.lib()
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        res = pool.starmap(_oracle_one, [(ref, tmpl[i]) for i in range(procs)])
+    wall = time.perf_counter() - t0
+    phis = np.array([[r[0], r[1]] for r in res])
+    energies = np.array([r[2] for r in res])
+    return procs, wall, phis, energies, "port", wall
+
+
+def _oracle_one(ref, tpl):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import msor
+    R = msor.normalize(ref)
+    T = msor.normalize(tpl)
+    px, py, e, _ = msor.register(LEVEL, START, LEVEL, R, T, lam=LAMBDA, max_iter=MAX_ITER)
+    return px, py, e
+
+
+def cpu_procs():
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except Exception:
+        return max(1, os.cpu_count() or 1)
+
+
+# --- main ---------------------------------------------------------------------
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def allreduce_max(x: float, world: int):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return 0
+    ref, tmpl, _ = workload(0)
+    procs = min(cpu_procs(), FRAMES)
+    values = []
+    kind = None
+    with tempfile.TemporaryDirectory() as wd:
+        for it in range(args.warmup + args.steps):
+            nfr, secs, _, _, kind, _ = run_reference_sample(ref, tmpl, procs, wd)
+            if it >= args.warmup:
+                values.append(nfr / secs)
+    v = statistics.mean(values)
+    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * procs / v,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": f"stage registration of {procs} of the 20 hex-lattice frames 513x513 (level 9) "
+                                  f"to a reference frame, levels {START}-{LEVEL}, maxGDIterations {MAX_ITER}, "
+                                  f"lambda {LAMBDA}; one process per host core", "frames_per_step": procs},
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": procs, "kind": kind,
+                            "sample": f"{procs} frames 513x513 per step, one per process"},
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--fp32", action="store_true", help="FP32 bulk with FP64 reductions (outside the energy tol)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        return run_reference_arm(args, world, rank)
+
+    import numpy as np
+    import torch
+    import msgpu
+    from msgpu import build as mbuild
+    from msgpu import synthetic as syn
+
+    torch.cuda.set_device(local)
+    mbuild.build()
+    fp64 = not args.fp32
+    p = params(fp64)
+    ref, tmpl, clean_ref = workload(rank)
+    n = (1 << LEVEL) + 1
+    N = n * n
+    nlev = LEVEL - START + 1
+    ctx = msgpu.Context(local)
+    dev = torch.device("cuda", local)
+    d_ref = torch.from_numpy(ref).to(dev)
+    d_tmpl = torch.from_numpy(tmpl).to(dev)
+    d_phis = torch.empty((FRAMES, 2, N), dtype=torch.float64, device=dev)
+    d_e = torch.empty(FRAMES, dtype=torch.float64, device=dev)
+    d_s = torch.empty((FRAMES, nlev), dtype=torch.int32, device=dev)
+    d_mean = torch.empty(N, dtype=torch.float64, device=dev)
+    d_count = torch.empty(N, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        ctx.match_series_stage_device(p, d_ref.data_ptr(), d_tmpl.data_ptr(), FRAMES, d_phis.data_ptr(),
+                                      d_e.data_ptr(), d_s.data_ptr(), d_mean.data_ptr(), d_count.data_ptr(),
+                                      stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    # ---- device-resident timed region (profiling events per level launch)
+    ctx.set_profiling(True)
+    lvl_ms, lvl_steps, lvl_evals, launches = [], [], [], 0
+    start_ev = torch.cuda.Event(enable_timing=True)
+    stop_ev = torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clocks:
+        start_ev.record(stream)
+        for _ in range(args.steps):
+            step()
+            st = ctx.stats()
+            lvl_ms.append(st["level_ms"][-1])
+            lvl_steps.append(st["level_steps"][-1])
+            lvl_evals.append(st["level_evals"][-1])
+            launches += st["kernel_launches"]
+        stop_ev.record(stream)
+        torch.cuda.synchronize(dev)
+    barrier(world)
+    ctx.set_profiling(False)
+    elapsed_ms = allreduce_max(start_ev.elapsed_time(stop_ev), world)
+    ms_per_step = elapsed_ms / args.steps
+    value = world * FRAMES * args.steps / (elapsed_ms / 1000.0)
+    phis = d_phis.cpu().numpy()
+    energies = d_e.cpu().numpy()
+    mean = d_mean.cpu().numpy()
+    steps_per_level = d_s.cpu().numpy()
+
+    # ---- end to end through the host entry point, pinned host buffers
+    h_ref = torch.from_numpy(ref).pin_memory().numpy()
+    h_tmpl = torch.from_numpy(tmpl).pin_memory().numpy()
+    outs = (torch.zeros((FRAMES, 2, N), dtype=torch.float64).pin_memory().numpy(),
+            torch.zeros(FRAMES, dtype=torch.float64).pin_memory().numpy(),
+            torch.zeros((FRAMES, nlev), dtype=torch.int32).pin_memory().numpy(),
+            torch.zeros(N, dtype=torch.float64).pin_memory().numpy(),
+            torch.zeros(N, dtype=torch.float64).pin_memory().numpy())
+    ctx.match_series_stage(p, h_ref, h_tmpl, out=outs)
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ctx.match_series_stage(p, h_ref, h_tmpl, out=outs)
+    e2e_s = allreduce_max(time.perf_counter() - t0, world)
+    e2e_value = world * FRAMES * args.steps / e2e_s
+    h2d = (1 + FRAMES) * N * 8
+    d2h = (2 * FRAMES * N + 2 * N + FRAMES) * 8 + FRAMES * nlev * 4
+
+    out = None
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        real_bytes = 8 if fp64 else 4
+        avg_ms = statistics.mean(lvl_ms)
+        alg = statistics.mean(algorithmic_bytes(s, e, real_bytes) for s, e in zip(lvl_steps, lvl_evals))
+        achieved = alg / (avg_ms / 1000.0) / 1e9
+        traffic = level_traffic(fp64)
+        clk = clocks.summary()
+        cpu = None
+        accuracy = None
+        if world == 1 and not args.no_cpu_baseline:
+            procs = min(cpu_procs(), FRAMES)
+            with tempfile.TemporaryDirectory() as wd:
+                nfr, secs, rphis, renergies, kind, wall = run_reference_sample(ref, tmpl, procs, wd)
+            cpu = {"value": nfr / secs, "unit": UNIT, "cores": procs, "kind": kind,
+                   "sample": f"{nfr} of the 20 frames (513x513, levels {START}-{LEVEL}), one process per core, "
+                             f"registration phase {secs:.1f} s"}
+            dphi = float(np.abs(phis[:nfr] - rphis).max()) * (n - 1)
+            rel = float(np.max(np.abs(energies[:nfr] - renergies) / np.abs(renergies)))
+            accuracy = {"frames_checked": nfr, "max_dphi_px": dphi, "max_rel_energy": rel,
+                        "tolerance": {"dphi_px": 1e-3, "rel_energy": 1e-6},
+                        "within_tolerance": bool(dphi <= 1e-3 and rel <= 1e-6)}
+        psnr = syn.psnr(mean.reshape(n, n), clean_ref)
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if fp64 else "f32+f64-reductions", "data": "synthetic",
+            "config": {"workload": f"stage registration: {FRAMES} hex-lattice frames 513x513 (level {LEVEL}) to a "
+                                   f"reference frame, levels {START}-{LEVEL}, maxGDIterations {MAX_ITER}, "
+                                   f"lambda {LAMBDA}, saturation 0.15%, plus warped-frame average",
+                       "frames_per_gpu": FRAMES, "level": LEVEL, "start_level": START,
+                       "max_gd_iterations": MAX_ITER, "lambda": LAMBDA,
+                       "l2": "no flush: per-step working set (~0.6 GB) exceeds the 126 MB L2",
+                       "parallelism": f"weak, {world} independent series"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": f"level_kernel<{'double' if fp64 else 'float'}> level {LEVEL}",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
+                         "steps_per_launch": statistics.mean(lvl_steps),
+                         "energy_evals_per_launch": statistics.mean(lvl_evals)},
+            "cpu_baseline": cpu,
+            "accuracy": accuracy,
+            "reconstruction_psnr_db": psnr,
+            "steps_per_level_frame0": steps_per_level[0].tolist(),
+            "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        }
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,141 @@
+/*
+ * msgpu.h -- C ABI of the B200 implementation of matchSeries' multilevel
+ * SSD + Dirichlet H1 gradient-flow registration and warped-frame average.
+ *
+ * Plain pointers and sizes only.  Every function returns an msgpu_status;
+ * on failure msgpu_last_error() gives the message (the reference throws
+ * aol::Exception with file and line; a C++ adapter rethrows this text).
+ * A context is bound to one CUDA device and is not shared between threads.
+ * Host-pointer entry points are synchronous.  Images are (2^l+1)^2 float64
+ * arrays, x fastest (quoc ILex order); displacements are in domain units
+ * (pixel shift = phi * 2^l) and stored as [phi_x, phi_y] per frame.
+ */
+#ifndef MSGPU_H
+#define MSGPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  MSGPU_OK = 0,
+  MSGPU_ERR_INVALID_ARG = 1,   /* null pointer, bad level range, ...        */
+  MSGPU_ERR_SIZE = 2,          /* input size does not match the grid        */
+  MSGPU_ERR_CUDA = 3,          /* CUDA runtime or launch failure            */
+  MSGPU_ERR_UNSUPPORTED = 4    /* option not provided by this build         */
+} msgpu_status;
+
+typedef struct msgpu_context msgpu_context;
+
+/* The parameter-file keys of the registration path (names as in the
+ * reference's .par files; see msgpu_params_default for the defaults).       */
+typedef struct {
+  int precision_level;         /* precisionLevel: images are (2^l+1)^2      */
+  int input_level;             /* level of the input images (>= precision)  */
+  int start_level;             /* startLevel                                 */
+  int stop_level;              /* stopLevel                                  */
+  double lambda;               /* lambda                                     */
+  double lambda_factor;        /* lambdaFactor (1 when absent)               */
+  int max_gd_iterations;       /* maxGDIterations                            */
+  double stop_epsilon;         /* stopEpsilon (0 when absent)                */
+  double saturation_percent;   /* enhanceContrastSaturationPercentage; <0 = absent */
+  int normalize_min_to_zero;   /* normalizeMinToZero                         */
+  int dont_normalize_input;    /* dontNormalizeInputImages                   */
+  int resample_deformation;    /* resampleInsteadOfProlongateDeformation     */
+  int use_fp64;                /* 0: FP32 bulk + FP64 reductions; 1: FP64   */
+} msgpu_params;
+
+void msgpu_params_default(msgpu_params* p);
+int  msgpu_abi_version(void);
+
+int  msgpu_create(int device, msgpu_context** out);
+int  msgpu_destroy(msgpu_context* ctx);
+const char* msgpu_last_error(const msgpu_context* ctx);
+
+/* One stage of series matching against a fixed reference: every template is
+ * prepared like the reference image (prepareMultilevelArray,
+ * registration.h:331-367), registered from initial_phis (NULL = zero,
+ * setTransformationToZero registration.h:570-574) by
+ * solveAndProlongToMaxDepth (registration.h:462-467), and returned at the
+ * precision level.  Replaces the per-frame loop of SeriesMatching::matchSeries
+ * (matchSeries.h:141-155, 223-245) for all frames of the stage at once.
+ *   reference  : (2^input_level+1)^2 doubles
+ *   templates  : num_templates such images
+ *   phis_out   : num_templates * 2 * (2^precision_level+1)^2 doubles
+ *   energies_out (nullable): energy of the last level solve per template
+ *                (getEnergyOfLastSolution, registration.h:1117-1119)
+ *   steps_out  (nullable): num_templates * (stop-start+1) gradient steps     */
+int msgpu_register_batch(msgpu_context* ctx, const msgpu_params* p, const double* reference,
+                         const double* templates, int num_templates, const double* initial_phis,
+                         double* phis_out, double* energies_out, int* steps_out);
+
+/* Same with device pointers, enqueued on the CUDA stream `stream`
+ * (a cudaStream_t; NULL = legacy default stream); returns after enqueueing.
+ * energies_out/steps_out are device pointers too (nullable).               */
+int msgpu_register_batch_device(msgpu_context* ctx, const msgpu_params* p, const double* d_reference,
+                                const double* d_templates, int num_templates, const double* d_initial_phis,
+                                double* d_phis_out, double* d_energies_out, int* d_steps_out,
+                                void* stream);
+
+/* averageSeries (matchSeries.h:385-425): each frame is warped by its
+ * displacement with DeformImage and Inf extension (deformations.h:62-101,
+ * registration.h:595-610); mean over the finite samples per pixel, pixels
+ * without samples take the last frame's mean; count = number of samples.   */
+int msgpu_warp_mean(msgpu_context* ctx, int level, const double* frames, const double* phis,
+                    int num_frames, double* mean_out, double* count_out);
+int msgpu_warp_mean_device(msgpu_context* ctx, int level, const double* d_frames, const double* d_phis,
+                           int num_frames, double* d_mean_out, double* d_count_out, void* stream);
+
+/* One stage of series matching in one call: msgpu_register_batch followed by
+ * msgpu_warp_mean of the raw templates with their displacements (the stage
+ * loop of matchSeries<>(), matchSeries.h:1284-1316, with averageSeries).
+ * One upload of the images, one download of the results.                  */
+int msgpu_match_series_stage(msgpu_context* ctx, const msgpu_params* p, const double* reference,
+                             const double* templates, int num_templates, double* phis_out,
+                             double* energies_out, int* steps_out, double* mean_out, double* count_out);
+int msgpu_match_series_stage_device(msgpu_context* ctx, const msgpu_params* p, const double* d_reference,
+                                    const double* d_templates, int num_templates, double* d_phis_out,
+                                    double* d_energies_out, int* d_steps_out, double* d_mean_out,
+                                    double* d_count_out, void* stream);
+
+/* Per-call statistics (no counterpart in the reference; used for the roofline).
+ * With profiling on, every batch call records CUDA events around each level
+ * launch on its stream and waits for them at the end of the call.          */
+typedef struct {
+  int kernel_launches;          /* kernels launched by the last batch call  */
+  int num_levels;               /* start..stop of the last batch call       */
+  int first_level;
+  float level_ms[16];           /* device time of each level launch         */
+  long long level_steps[16];    /* gradient steps summed over the frames    */
+  long long level_evals[16];    /* energy evaluations summed over the frames */
+} msgpu_stats;
+int msgpu_set_profiling(msgpu_context* ctx, int on);
+int msgpu_get_stats(const msgpu_context* ctx, msgpu_stats* out);
+
+/* --- single operators of the path (parity entry points) ----------------- */
+/* E = SSDEnergy + lambda * DisplacementLengthEnergy and DE = SSDForce +
+ * lambda * L phi (registration.h:971-982, 1584-1667).  de_out: 2*N doubles. */
+int msgpu_energy(msgpu_context* ctx, int level, const double* R, const double* T, const double* phix,
+                 const double* phiy, double lambda, int use_fp64, double* energy_out, double* de_out);
+/* LinearSmoothOp::apply with sigma (linearSmoothOp.cpp:591-612).          */
+int msgpu_smooth(msgpu_context* ctx, int level, double sigma, int use_fp64, const double* in, double* out);
+/* RestrictOp<STD_QUOC_RESTRICT>::apply, fine level -> fine level - 1.      */
+int msgpu_restrict(msgpu_context* ctx, int fine_level, const double* in, double* out);
+/* ProlongOp::apply, coarse level -> coarse level + 1.                      */
+int msgpu_prolong(msgpu_context* ctx, int coarse_level, const double* in, double* out);
+/* Image preparation (normalisation only, registration.h:335-346).         */
+int msgpu_normalize(msgpu_context* ctx, const double* in, int count, double saturation_percent,
+                    int normalize_min_to_zero, double* out);
+/* One level solve, StandardRegistration::findTransformation
+ * (registration.h:967-1021): phix/phiy are updated in place.  trace
+ * (nullable) receives up to max_trace rows of (energy, tau, sigma, evals).  */
+int msgpu_gd_level(msgpu_context* ctx, int level, const double* R, const double* T, double* phix,
+                   double* phiy, double lambda, int max_iter, double stop_eps, int use_fp64,
+                   double* energy_out, int* steps_out, double* trace, int max_trace);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1164 @@
+// msgpu.cu -- C ABI and batch pipeline of the B200 registration path.
+//
+// Pipeline of msgpu_register_batch (one stage of series matching, all frames
+// at once):
+//   1. image preparation: exact saturated min/max by radix selection, clamp,
+//      scale to [0,1] (registration.h:335-346, vec.h:864-871, 1084-1089)
+//   2. image pyramid by RestrictOp<STD_QUOC_RESTRICT> (multilevelArray.h:94-110)
+//   3. per level: ONE persistent launch (msgpu_level.cuh) solving every frame's
+//      gradient flow, then prolongation of the displacements
+//      (quocDescent.h:83-105, registration.h:510-521)
+//   4. prolongation to the precision level (registration.h:462-467)
+// and msgpu_warp_mean the warped-frame average (matchSeries.h:385-425).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/msgpu.h"
+#include "msgpu_level.cuh"
+
+using namespace msg;
+
+struct msgpu_context {
+  int device = 0;
+  int sm_count = 0;
+  std::string err;
+  cudaStream_t stream = nullptr;
+  // growable device buffers
+  struct Buf { void* p = nullptr; size_t cap = 0; };
+  Buf arena, shared_real, dscratch, small, phis_d, io[6];
+  // statistics of the last batch call
+  bool profiling = false;
+  msgpu_stats stats{};
+  cudaEvent_t ev[32] = {};
+  bool ev_ready = false;
+};
+
+namespace {
+
+constexpr int kAbiVersion = 1;
+
+int fail(msgpu_context* ctx, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (ctx) ctx->err = buf;
+  return code;
+}
+
+#define CK(call)                                                                                  \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess)                                                                        \
+      return fail(ctx, MSGPU_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),   \
+                  __FILE__, __LINE__);                                                            \
+  } while (0)
+
+int ensure(msgpu_context* ctx, msgpu_context::Buf& b, size_t bytes) {
+  if (b.cap >= bytes) return MSGPU_OK;
+  if (b.p) CK(cudaFree(b.p));
+  b.p = nullptr;
+  b.cap = 0;
+  CK(cudaMalloc(&b.p, bytes));
+  b.cap = bytes;
+  return MSGPU_OK;
+}
+
+__host__ __device__ inline int lvl_n(int l) { return (1 << l) + 1; }
+__host__ __device__ inline size_t lvl_N(int l) { return (size_t)lvl_n(l) * lvl_n(l); }
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Q1 tables and assembled stiffness stencil per node class, computed in double
+// the way the reference assembles StiffOp (FEOpInterface.h:65-88, 1362-1395).
+// The values do not depend on the level: h enters only through exact powers of
+// two that cancel between the gradients and the element volume.
+bool g_tables_ready[64] = {false};
+
+void host_basis_grad(int b, double x, double y, double h, double g[2]) {
+  switch (b) {
+    case 0: g[0] = (y - 1.0) / h; g[1] = (x - 1.0) / h; break;
+    case 1: g[0] = (1.0 - y) / h; g[1] = (-x) / h; break;
+    case 2: g[0] = (-y) / h; g[1] = (1.0 - x) / h; break;
+    default: g[0] = y / h; g[1] = x / h; break;
+  }
+}
+double host_basis_val(int b, double x, double y) {
+  switch (b) {
+    case 0: return (1.0 - x) * (1.0 - y);
+    case 1: return x * (1.0 - y);
+    case 2: return (1.0 - x) * y;
+    default: return x * y;
+  }
+}
+
+void host_fe_tables(FeTables& t) {
+  const double g[2] = {0.2113248654051871, 0.7886751345948129};
+  for (int i = 0, k = 0; i < 2; ++i)
+    for (int j = 0; j < 2; ++j, ++k) { t.rc[k][0] = g[i]; t.rc[k][1] = g[j]; }
+  const double h = 0.25, vol = h * h;
+  double gq[4][4][2];
+  for (int b = 0; b < 4; ++b)
+    for (int q = 0; q < 4; ++q) {
+      t.bq[b][q] = host_basis_val(b, t.rc[q][0], t.rc[q][1]);
+      host_basis_grad(b, t.rc[q][0], t.rc[q][1], h, gq[b][q]);
+    }
+  t.w = 0.5 * 0.5;
+  double L[4][4];
+  for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) L[i][j] = 0.;
+  for (int q = 0; q < 4; ++q)
+    for (int i = 0; i < 4; ++i)
+      for (int j = i; j < 4; ++j) {
+        double d = 0;
+        d += gq[i][q][0] * gq[j][q][0];
+        d += gq[i][q][1] * gq[j][q][1];
+        L[i][j] += d * 1. * t.w;
+      }
+  for (int i = 0; i < 4; ++i)
+    for (int j = i; j < 4; ++j) L[j][i] = L[i][j] = L[i][j] * vol;
+  // assemble on a 5x5 node grid in element order and read the 9 node classes
+  const int n = 5;
+  std::vector<double> st((size_t)n * n * 9, 0.0);
+  for (int ey = 0; ey < n - 1; ++ey)
+    for (int ex = 0; ex < n - 1; ++ex)
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) {
+          const int gi = ex + ey * n + ((i & 1) ? 1 : 0) + ((i & 2) ? n : 0);
+          const int gj = ex + ey * n + ((j & 1) ? 1 : 0) + ((j & 2) ? n : 0);
+          const int dx = (gj % n) - (gi % n), dy = (gj / n) - (gi / n);
+          st[(size_t)gi * 9 + (dy + 1) * 3 + (dx + 1)] += 1.0 * L[i][j];
+        }
+  const int rep[3] = {0, 2, 4};
+  for (int cy = 0; cy < 3; ++cy)
+    for (int cx = 0; cx < 3; ++cx) {
+      const int node = rep[cx] + rep[cy] * n;
+      for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) t.st[cx + 3 * cy][j][i] = st[(size_t)node * 9 + j * 3 + i];
+    }
+}
+
+int ensure_tables(msgpu_context* ctx) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 64 && g_tables_ready[dev]) return MSGPU_OK;
+  FeTables t;
+  host_fe_tables(t);
+  CK(cudaMemcpyToSymbol(c_fe, &t, sizeof(t)));
+  if (dev < 64) g_tables_ready[dev] = true;
+  return MSGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Kernels of the batch pipeline.
+
+// Order-preserving 64-bit key of a double.
+__device__ __forceinline__ unsigned long long dkey(double v) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double dkey_inv(unsigned long long k) {
+  const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+  return __longlong_as_double((long long)b);
+}
+
+// Exact order statistics of every image (the entries a sort would put at
+// positions rank_lo and rank_hi, vec.h:864-871) by MSD radix selection with
+// 8-bit digits; one CTA per image, both ranks selected together.
+constexpr int kSelThreads = 1024;
+__global__ void __launch_bounds__(kSelThreads) k_select2(const double* __restrict__ img, size_t stride, int count,
+                                                       int rank_lo, int rank_hi, double* out /* [2*i] */) {
+  __shared__ unsigned int hist[2][256];
+  __shared__ unsigned long long prefix[2];
+  __shared__ int kk[2];
+  const double* a = img + (size_t)blockIdx.x * stride;
+  if (threadIdx.x == 0) {
+    prefix[0] = prefix[1] = 0ull;
+    kk[0] = rank_lo;
+    kk[1] = rank_hi;
+  }
+  for (int pass = 0; pass < 8; ++pass) {
+    const int shift = 56 - 8 * pass;
+    for (int i = threadIdx.x; i < 512; i += kSelThreads) (&hist[0][0])[i] = 0u;
+    __syncthreads();
+    const unsigned long long mask = (pass == 0) ? 0ull : (~0ull << (shift + 8));
+    const unsigned long long p0 = prefix[0], p1 = prefix[1];
+    for (int i = threadIdx.x; i < count; i += kSelThreads) {
+      const unsigned long long k = dkey(a[i]);
+      const unsigned d = (unsigned)((k >> shift) & 0xffu);
+      if ((k & mask) == p0) atomicAdd(&hist[0][d], 1u);
+      if ((k & mask) == p1) atomicAdd(&hist[1][d], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+      const int s = threadIdx.x;
+      int k = kk[s];
+      unsigned acc = 0;
+      int b = 0;
+      for (; b < 256; ++b) {
+        if (acc + hist[s][b] > (unsigned)k) break;
+        acc += hist[s][b];
+      }
+      kk[s] = k - (int)acc;
+      prefix[s] |= ((unsigned long long)b) << shift;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x < 2) out[2 * blockIdx.x + threadIdx.x] = dkey_inv(prefix[threadIdx.x]);
+}
+
+// min and max of every image (deterministic: min/max are order independent).
+__global__ void __launch_bounds__(1024) k_minmax(const double* __restrict__ img, size_t stride, int count,
+                                                 double* out) {
+  __shared__ double smn[32], smx[32];
+  const double* a = img + (size_t)blockIdx.x * stride;
+  double mn = INFINITY, mx = -INFINITY;
+  for (int i = threadIdx.x; i < count; i += blockDim.x) {
+    const double v = a[i];
+    mn = fmin(mn, v);
+    mx = fmax(mx, v);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  if ((threadIdx.x & 31) == 0) { smn[threadIdx.x >> 5] = mn; smx[threadIdx.x >> 5] = mx; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) { mn = fmin(mn, smn[w]); mx = fmax(mx, smx[w]); }
+    mn = fmin(mn, smn[0]);
+    mx = fmax(mx, smx[0]);
+    out[2 * blockIdx.x] = mn;
+    out[2 * blockIdx.x + 1] = mx;
+  }
+}
+
+// prepareMultilevelArray scaling (registration.h:335-346).
+//   sat >= 0 : x = clamp(x, lo, hi); x += -lo; x /= (hi + -lo) unless 0
+//   sat <  0 : if (mn < 0 || min_to_zero) x += -mn; x /= max unless 0
+__global__ void k_normalize(double* img, size_t stride, int count, const double* mm, int sat_mode,
+                            int min_to_zero) {
+  const int b = blockIdx.y;
+  double* a = img + (size_t)b * stride;
+  const double lo = mm[2 * b], hi = mm[2 * b + 1];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    double v = a[i];
+    if (sat_mode) {
+      v = v < lo ? lo : (v > hi ? hi : v);
+      const double s = -1 * lo;
+      v += s;
+      const double mx = hi + s;
+      if (mx != 0) v /= mx;
+    } else {
+      double mx = hi;
+      if (lo < 0. || min_to_zero) {
+        v += -lo;
+        mx = hi + -lo;
+      }
+      if (mx != 0.) v /= mx;
+    }
+    a[i] = v;
+  }
+}
+
+// One restriction step for a batch of images: coarse[b] = R fine[b].
+template <typename T>
+__global__ void k_restrict(const T* __restrict__ fine, size_t fstride, T* coarse, size_t cstride, int fine_level) {
+  const int fw = lvl_n(fine_level), cw = lvl_n(fine_level - 1);
+  const T* f = fine + (size_t)blockIdx.y * fstride;
+  T* c = coarse + (size_t)blockIdx.y * cstride;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cw * cw; i += gridDim.x * blockDim.x) {
+    c[i] = restrict_node<T>(i % cw, i / cw, cw, [&](int x, int y) { return f[(size_t)y * fw + x]; });
+  }
+}
+
+template <typename T>
+__global__ void k_prolong(const T* __restrict__ coarse, size_t cstride, T* fine, size_t fstride, int coarse_level) {
+  const int cw = lvl_n(coarse_level), fw = lvl_n(coarse_level + 1);
+  const T* c = coarse + (size_t)blockIdx.y * cstride;
+  T* f = fine + (size_t)blockIdx.y * fstride;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < fw * fw; i += gridDim.x * blockDim.x) {
+    f[i] = prolong_node<T>(i % fw, i / fw, [&](int x, int y) { return c[(size_t)y * cw + x]; });
+  }
+}
+
+template <typename Src, typename Dst>
+__global__ void k_convert(const Src* __restrict__ src, size_t sstride, Dst* dst, size_t dstride, size_t count) {
+  const Src* s = src + (size_t)blockIdx.y * sstride;
+  Dst* d = dst + (size_t)blockIdx.y * dstride;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x)
+    d[i] = (Dst)s[i];
+}
+
+// Displacement transfer to the next level for every instance: reads the
+// buffer bin[i], writes buffer bin[i]^1 and records it in bout[i].
+// mode 0: ProlongOp (prolongation.cpp:195-232); mode 1: 1-D resampling of the
+// flattened node vector (vec.h:461-472, 565-570; registration.h:510-516).
+template <typename Real>
+__global__ void k_phi_up(Real* arena, size_t inst_stride, size_t off0, size_t off1, size_t comp_stride_src,
+                         size_t comp_stride_dst, int coarse_level, const int* bin, int* bout, int mode) {
+  const int inst = blockIdx.y;
+  const int b = bin[inst];
+  Real* base = arena + (size_t)inst * inst_stride;
+  const Real* src = base + (b ? off1 : off0);
+  Real* dst = base + (b ? off0 : off1);
+  const int cw = lvl_n(coarse_level), fw = lvl_n(coarse_level + 1);
+  const int ns = cw * cw, nd = fw * fw;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nd; i += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const Real* s = src + (size_t)c * comp_stride_src;
+      Real v;
+      if (mode == 0) {
+        v = prolong_node<Real>(i % fw, i / fw, [&](int x, int y) { return s[(size_t)y * cw + x]; });
+      } else {
+        const double sc = (ns - 1) / (double)(nd - 1);
+        const double pos = i * sc;
+        const int p = (int)pos;
+        const double pf = pos - p;
+        v = (p == ns - 1) ? s[p] : (Real)((1 - pf) * (double)s[p] + pf * (double)s[p + 1]);
+      }
+      dst[(size_t)c * comp_stride_dst + i] = v;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) bout[inst] = b ^ 1;
+}
+
+template <typename Real>
+__global__ void k_set_buf(int* buf, int n, int v) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) buf[i] = v;
+}
+
+// phi of every instance at the given level -> double output (F x 2 x N).
+template <typename Real>
+__global__ void k_phi_out(const Real* arena, size_t inst_stride, size_t off0, size_t off1, size_t comp_stride,
+                          const int* buf, int N, double* out) {
+  const int inst = blockIdx.y;
+  const Real* src = arena + (size_t)inst * inst_stride + (buf[inst] ? off1 : off0);
+  double* o = out + (size_t)inst * 2 * N;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    o[i] = (double)src[i];
+    o[N + i] = (double)src[comp_stride + i];
+  }
+}
+
+// Energy/steps outputs of the last level solve.
+__global__ void k_collect(const double* e, const int* s, int num, double* e_out, int* s_out, int s_stride,
+                          int s_col) {
+  for (int i = threadIdx.x; i < num; i += blockDim.x) {
+    if (e_out) e_out[i] = e[i];
+    if (s_out) s_out[(size_t)i * s_stride + s_col] = s[i];
+  }
+}
+
+// ScalarArray<QC_2D>::interpolate (scalarArray.h:499-525).
+__device__ __forceinline__ double interp_d(const double* img, int n, double X, double Y) {
+  int xL = (int)X, yL = (int)Y;
+  if (X >= (double)(n - 1)) xL = n - 2;
+  if (Y >= (double)(n - 1)) yL = n - 2;
+  if (X < 0.) xL = 0;
+  if (Y < 0.) yL = 0;
+  X -= xL;
+  Y -= yL;
+  const int xU = xL + 1, yU = yL + 1;
+  const double v0 = img[xL + (size_t)yL * n], v1 = img[xU + (size_t)yL * n];
+  if (Y == 0) return (1 - X) * v0 + X * v1;
+  const double v2 = img[xL + (size_t)yU * n], v3 = img[xU + (size_t)yU * n];
+  return (1 - X) * (1 - Y) * v0 + X * (1 - Y) * v1 + (1 - X) * Y * v2 + X * Y * v3;
+}
+
+// Warped-frame average: DeformImage with Inf extension per frame
+// (deformations.h:62-101), mean over finite samples (matchSeries.h:410-425).
+__global__ void k_warp_mean(const double* __restrict__ frames, const double* __restrict__ phis, int F, int level,
+                            const double* last_mean, double* mean, double* count) {
+  const int n = lvl_n(level);
+  const int N = n * n;
+  const double h = 1.0 / (double)(n - 1);
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < N; j += gridDim.x * blockDim.x) {
+    const int x = j % n, y = j / n;
+    double acc = 0;
+    int k = 0;
+    for (int f = 0; f < F; ++f) {
+      const double* ph = phis + (size_t)f * 2 * N;
+      const double d0 = x + ph[j] / h, d1 = y + ph[N + j] / h;
+      bool in = true;
+      if (d0 < 0. || d0 > (double)(n - 1) || isnan(d0)) in = false;
+      if (d1 < 0. || d1 > (double)(n - 1) || isnan(d1)) in = false;
+      const double v = in ? interp_d(frames + (size_t)f * N, n, d0, d1) : INFINITY;
+      if (v != INFINITY) {
+        acc += v;
+        ++k;
+      }
+    }
+    mean[j] = (k > 0) ? acc / k : *last_mean;
+    count[j] = k;
+  }
+}
+
+__global__ void k_mean(const double* a, int N, double* out) {
+  __shared__ double sm[32];
+  double s = 0;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) s += a[i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sm[w];
+    *out = t / N;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Arena layout of one registration instance (elements of Real), sized for
+// the precision level M.
+struct Layout {
+  size_t off_T[kMaxLevel + 1];
+  size_t off_phi[2], off_d[2], off_s, off_de;
+  size_t off_x2[kMaxLevel + 1], off_x5[kMaxLevel + 1], off_b[kMaxLevel + 1];
+  size_t stride;
+};
+
+Layout make_layout(int M) {
+  Layout L;
+  size_t off = 0;
+  const size_t a = 64;
+  for (int l = 0; l <= M; ++l) { L.off_T[l] = off; off = align_up(off + lvl_N(l), a); }
+  for (int l = M + 1; l <= kMaxLevel; ++l) L.off_T[l] = 0;
+  const size_t two = 2 * lvl_N(M);
+  for (int b = 0; b < 2; ++b) { L.off_phi[b] = off; off = align_up(off + two, a); }
+  for (int b = 0; b < 2; ++b) { L.off_d[b] = off; off = align_up(off + two, a); }
+  L.off_s = off; off = align_up(off + two, a);
+  L.off_de = off; off = align_up(off + two, a);
+  for (int k = 0; k <= kMaxLevel; ++k) {
+    if (k <= M) {
+      L.off_x2[k] = off; off = align_up(off + 2 * lvl_N(k), a);
+      L.off_x5[k] = off; off = align_up(off + 2 * lvl_N(k), a);
+      L.off_b[k] = off; off = align_up(off + 2 * lvl_N(k), a);
+    } else {
+      L.off_x2[k] = L.off_x5[k] = L.off_b[k] = 0;
+    }
+  }
+  L.stride = off;
+  return L;
+}
+
+template <typename Real>
+size_t level_smem_bytes(int lc) {
+  size_t s = std::max(sizeof(GradShared<Real>), std::max(sizeof(DownShared<Real>), sizeof(UpShared<Real>)));
+  s = std::max(s, coarse_smem_elems<Real>(lc) * sizeof(Real));
+  return align_up(s, 16);
+}
+
+template <typename Real>
+int pick_lc(int level) {
+  const int cap = (sizeof(Real) == 4) ? 5 : 4;
+  return std::min(level, cap);
+}
+
+// Cluster size: enough CTAs per instance to fill the GPU, at most one CTA per
+// 16k nodes of the level and at most 16 (non-portable cluster size).
+int pick_cluster(int sms, int num_inst, int level) {
+  const size_t N = lvl_N(level);
+  int g_nodes = (int)std::max<size_t>(1, N / 16384);
+  int g_fill = std::max(1, (2 * sms) / std::max(1, num_inst));
+  int g = std::min(16, std::min(g_nodes, g_fill));
+  int p = 1;
+  while (p * 2 <= g) p *= 2;
+  return p;
+}
+
+template <typename Real>
+int launch_level(msgpu_context* ctx, LevelArgs<Real>& a, int G, cudaStream_t st) {
+  const size_t smem = level_smem_bytes<Real>(a.lc);
+  CK(cudaFuncSetAttribute(level_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(cudaFuncSetAttribute(level_kernel<Real>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  for (;;) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = G;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(kThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cfg.gridDim = dim3(G * std::max(1, a.num_inst), 1, 1);
+    int max_clusters = 0;
+    cudaError_t e = cudaOccupancyMaxActiveClusters(&max_clusters, level_kernel<Real>, &cfg);
+    if (e != cudaSuccess || max_clusters < 1) {
+      (void)cudaGetLastError();
+      if (G > 1) { G >>= 1; continue; }
+      return fail(ctx, MSGPU_ERR_CUDA, "level kernel cannot be resident (smem %zu B): %s", smem,
+                  cudaGetErrorString(e));
+    }
+    const int nclusters = std::min(a.num_inst, max_clusters);
+    cfg.gridDim = dim3(G * nclusters, 1, 1);
+    CK(cudaLaunchKernelEx(&cfg, level_kernel<Real>, a));
+    return MSGPU_OK;
+  }
+}
+
+// ---------------------------------------------------------------------------
+struct BatchIO {
+  const double* ref;        // device, input level
+  const double* tmpl;       // device, F images at input level
+  const double* init_phi;   // device, F x 2 x N_M or null
+  double* phis_out;         // device, F x 2 x N_M
+  double* energies_out;     // device or null
+  int* steps_out;           // device or null
+};
+
+template <typename Real>
+int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& io, cudaStream_t st) {
+  const int M = p.precision_level, Lin = p.input_level;
+  const int start = p.start_level, stop = p.stop_level;
+  const int nimg = F + 1;  // image 0 is the reference
+  const size_t Nin = lvl_N(Lin);
+  const Layout L = make_layout(M);
+  int rc;
+  if ((rc = ensure_tables(ctx))) return rc;
+  // --- double scratch: per image a pyramid from Lin down to 0
+  std::vector<size_t> poff(Lin + 1);
+  size_t pstride = 0;
+  for (int l = Lin; l >= 0; --l) { poff[l] = pstride; pstride = align_up(pstride + lvl_N(l), 32); }
+  const int nlev_all = stop - start + 1;
+  const size_t small_bytes = sizeof(double) * (2 * nimg + 2 * F + 64) + sizeof(int) * ((2 * nlev_all + 4) * F + 64);
+  if ((rc = ensure(ctx, ctx->dscratch, sizeof(double) * pstride * nimg))) return rc;
+  if ((rc = ensure(ctx, ctx->arena, sizeof(Real) * L.stride * F))) return rc;
+  if ((rc = ensure(ctx, ctx->shared_real, sizeof(Real) * (L.off_T[M] + lvl_N(M) + 64)))) return rc;
+  if ((rc = ensure(ctx, ctx->small, small_bytes))) return rc;
+  double* pyr = (double*)ctx->dscratch.p;
+  Real* arena = (Real*)ctx->arena.p;
+  Real* Rpyr = (Real*)ctx->shared_real.p;
+  double* mm = (double*)ctx->small.p;                 // 2 * nimg
+  double* e_lvl = mm + 2 * nimg;                      // F
+  int* ibase = (int*)(e_lvl + 2 * F + 64);
+  int* bufA = ibase;                                  // F
+  int* bufB = ibase + F;                              // F
+  int* steps_all = ibase + 2 * F;                     // nlev x F
+  int* evals_all = steps_all + (size_t)nlev_all * F;  // nlev x F
+  int& launches = ctx->stats.kernel_launches;
+  launches = 0;
+  ctx->stats.num_levels = nlev_all;
+  ctx->stats.first_level = start;
+  if (ctx->profiling && !ctx->ev_ready) {
+    for (int i = 0; i < 32; ++i) CK(cudaEventCreate(&ctx->ev[i]));
+    ctx->ev_ready = true;
+  }
+
+  // 1. copy inputs into the pyramid scratch and prepare (normalise) them
+  CK(cudaMemcpy2DAsync(pyr + poff[Lin], pstride * sizeof(double), io.ref, Nin * sizeof(double),
+                       Nin * sizeof(double), 1, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpy2DAsync(pyr + pstride + poff[Lin], pstride * sizeof(double), io.tmpl, Nin * sizeof(double),
+                       Nin * sizeof(double), F, cudaMemcpyDeviceToDevice, st));
+  if (!p.dont_normalize_input) {
+    if (p.saturation_percent >= 0) {
+      const int m1 = (int)Nin - 1;
+      int il = (int)(p.saturation_percent / 200 * m1), ih = (int)((1 - p.saturation_percent / 200) * m1);
+      il = std::min(std::max(il, 0), m1);
+      ih = std::min(std::max(ih, 0), m1);
+      k_select2<<<nimg, kSelThreads, 0, st>>>(pyr + poff[Lin], pstride, (int)Nin, il, ih, mm);
+    } else {
+      k_minmax<<<nimg, 1024, 0, st>>>(pyr + poff[Lin], pstride, (int)Nin, mm);
+    }
+    CK(cudaGetLastError());
+    k_normalize<<<dim3((unsigned)std::min<size_t>(1024, (Nin + 255) / 256), nimg), 256, 0, st>>>(
+        pyr + poff[Lin], pstride, (int)Nin, mm, p.saturation_percent >= 0 ? 1 : 0, p.normalize_min_to_zero);
+    CK(cudaGetLastError());
+    launches += 2;
+  }
+  // 2. pyramid (double), then Real copies of the levels 0..M
+  for (int l = Lin; l >= 1; --l) {
+    const size_t cN = lvl_N(l - 1);
+    k_restrict<double><<<dim3((unsigned)std::min<size_t>(1024, (cN + 255) / 256), nimg), 256, 0, st>>>(
+        pyr + poff[l], pstride, pyr + poff[l - 1], pstride, l);
+    ++launches;
+  }
+  CK(cudaGetLastError());
+  for (int l = 0; l <= M; ++l) {
+    const size_t Nl = lvl_N(l);
+    const unsigned gx = (unsigned)std::min<size_t>(1024, (Nl + 255) / 256);
+    k_convert<double, Real><<<dim3(gx, 1), 256, 0, st>>>(pyr + poff[l], 0, Rpyr + L.off_T[l], 0, Nl);
+    k_convert<double, Real><<<dim3(gx, F), 256, 0, st>>>(pyr + pstride + poff[l], pstride, arena + L.off_T[l],
+                                                          L.stride, Nl);
+    launches += 2;
+  }
+  CK(cudaGetLastError());
+  // 3. initial displacement at the start level (restricted from M), buffer 0
+  k_set_buf<Real><<<1, 256, 0, st>>>(bufA, F, 0);
+  ++launches;
+  {
+    const size_t Ns = lvl_N(start);
+    if (io.init_phi) {
+      // restrict the initial displacement in double inside the template pyramid scratch of level < M
+      // storage: reuse the double scratch rows of the templates (already converted)
+      double* tmp = pyr + pstride;  // F images, 2 components need 2F slots: use pairs of images
+      for (int c = 0; c < 2; ++c) {
+        const size_t NM = lvl_N(M);
+        CK(cudaMemcpy2DAsync(tmp + poff[M], pstride * sizeof(double), io.init_phi + (size_t)c * NM,
+                             2 * NM * sizeof(double), NM * sizeof(double), F, cudaMemcpyDeviceToDevice, st));
+        for (int l = M; l > start; --l) {
+          const size_t cN = lvl_N(l - 1);
+          k_restrict<double><<<dim3((unsigned)std::min<size_t>(1024, (cN + 255) / 256), F), 256, 0, st>>>(
+              tmp + poff[l], pstride, tmp + poff[l - 1], pstride, l);
+        }
+        k_convert<double, Real><<<dim3((unsigned)std::min<size_t>(1024, (Ns + 255) / 256), F), 256, 0, st>>>(
+            tmp + poff[start], pstride, arena + L.off_phi[0] + (size_t)c * Ns, L.stride, Ns);
+      }
+    } else {
+      CK(cudaMemset2DAsync(arena + L.off_phi[0], L.stride * sizeof(Real), 0, 2 * Ns * sizeof(Real), F, st));
+    }
+  }
+  CK(cudaGetLastError());
+  // 4. level loop
+  int* bin = bufA;
+  int* bout = bufB;
+  const int nlev = stop - start + 1;
+  for (int l = start; l <= stop; ++l) {
+    LevelArgs<Real> a;
+    memset(&a, 0, sizeof(a));
+    a.arena = arena;
+    a.inst_stride = L.stride;
+    a.R = Rpyr + L.off_T[l];
+    a.off_T = L.off_T[l];
+    a.off_phi[0] = L.off_phi[0];
+    a.off_phi[1] = L.off_phi[1];
+    a.off_d[0] = L.off_d[0];
+    a.off_d[1] = L.off_d[1];
+    a.off_s = L.off_s;
+    a.off_de = L.off_de;
+    for (int k = 0; k <= kMaxLevel; ++k) { a.off_x2[k] = L.off_x2[k]; a.off_x5[k] = L.off_x5[k]; a.off_b[k] = L.off_b[k]; }
+    a.level = l;
+    a.n = lvl_n(l);
+    a.num_inst = F;
+    a.lc = pick_lc<Real>(l);
+    a.mode = MODE_SOLVE;
+    a.lambda = std::pow(p.lambda_factor, (double)(stop - l)) * p.lambda;
+    a.stop_eps = p.stop_epsilon;
+    a.max_iter = p.max_gd_iterations;
+    a.phi_in_dev = bin;
+    a.out_energy = e_lvl;
+    a.out_steps = steps_all + (size_t)(l - start) * F;
+    a.out_evals = evals_all + (size_t)(l - start) * F;
+    a.out_phi_buf = bin;   // the level kernel updates the buffer index in place
+    const int G = pick_cluster(ctx->sm_count, F, l);
+    if (ctx->profiling && l - start < 16) CK(cudaEventRecord(ctx->ev[2 * (l - start)], st));
+    if ((rc = launch_level<Real>(ctx, a, G, st))) return rc;
+    if (ctx->profiling && l - start < 16) CK(cudaEventRecord(ctx->ev[2 * (l - start) + 1], st));
+    k_collect<<<1, 256, 0, st>>>(e_lvl, a.out_steps, F, (l == stop) ? io.energies_out : nullptr, io.steps_out,
+                                 nlev, l - start);
+    CK(cudaGetLastError());
+    launches += 2;
+    if (l < stop) {
+      const size_t fw = lvl_N(l + 1);
+      k_phi_up<Real><<<dim3((unsigned)std::min<size_t>(1024, (fw + 255) / 256), F), 256, 0, st>>>(
+          arena, L.stride, L.off_phi[0], L.off_phi[1], lvl_N(l), lvl_N(l + 1), l, bin, bout,
+          p.resample_deformation ? 1 : 0);
+      CK(cudaGetLastError());
+      ++launches;
+      std::swap(bin, bout);
+    }
+  }
+  for (int l = stop; l < M; ++l) {
+    const size_t fw = lvl_N(l + 1);
+    k_phi_up<Real><<<dim3((unsigned)std::min<size_t>(1024, (fw + 255) / 256), F), 256, 0, st>>>(
+        arena, L.stride, L.off_phi[0], L.off_phi[1], lvl_N(l), lvl_N(l + 1), l, bin, bout,
+        p.resample_deformation ? 1 : 0);
+    CK(cudaGetLastError());
+    ++launches;
+    std::swap(bin, bout);
+  }
+  const int NM = (int)lvl_N(M);
+  k_phi_out<Real><<<dim3((unsigned)std::min(1024, (NM + 255) / 256), F), 256, 0, st>>>(
+      arena, L.stride, L.off_phi[0], L.off_phi[1], (size_t)NM, bin, NM, io.phis_out);
+  CK(cudaGetLastError());
+  ++launches;
+  if (ctx->profiling) {
+    std::vector<int> hs((size_t)nlev_all * F), he((size_t)nlev_all * F);
+    CK(cudaMemcpyAsync(hs.data(), steps_all, sizeof(int) * hs.size(), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(he.data(), evals_all, sizeof(int) * he.size(), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int k = 0; k < nlev_all && k < 16; ++k) {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, ctx->ev[2 * k], ctx->ev[2 * k + 1]));
+      ctx->stats.level_ms[k] = ms;
+      long long ss = 0, ee = 0;
+      for (int f = 0; f < F; ++f) { ss += hs[(size_t)k * F + f]; ee += he[(size_t)k * F + f]; }
+      ctx->stats.level_steps[k] = ss;
+      ctx->stats.level_evals[k] = ee;
+    }
+  }
+  return MSGPU_OK;
+}
+
+int check_params(msgpu_context* ctx, const msgpu_params* p) {
+  if (!p) return fail(ctx, MSGPU_ERR_INVALID_ARG, "params is NULL");
+  if (p->precision_level < 1 || p->precision_level > kMaxLevel)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "precisionLevel %d outside [1, %d]", p->precision_level, kMaxLevel);
+  if (p->input_level < p->precision_level || p->input_level > kMaxLevel)
+    return fail(ctx, MSGPU_ERR_SIZE,
+                "Input data size too small. Note: Unless \"resizeInput\" is used, \"precisionLevel\" may not be "
+                "bigger than the grid level of the input data.");
+  if (p->start_level < 1 || p->stop_level > p->precision_level || p->start_level > p->stop_level)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "level range startLevel %d .. stopLevel %d invalid for precisionLevel %d",
+                p->start_level, p->stop_level, p->precision_level);
+  if (p->max_gd_iterations < 0) return fail(ctx, MSGPU_ERR_INVALID_ARG, "maxGDIterations < 0");
+  return MSGPU_OK;
+}
+
+int bind_device(msgpu_context* ctx) {
+  CK(cudaSetDevice(ctx->device));
+  return MSGPU_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+void msgpu_params_default(msgpu_params* p) {
+  if (!p) return;
+  memset(p, 0, sizeof(*p));
+  p->precision_level = 9;
+  p->input_level = 9;
+  p->start_level = 5;
+  p->stop_level = 9;
+  p->lambda = 0.1;
+  p->lambda_factor = 1.0;
+  p->max_gd_iterations = 30;
+  p->stop_epsilon = 0.0;
+  p->saturation_percent = 0.15;
+  p->normalize_min_to_zero = 1;
+  p->dont_normalize_input = 0;
+  p->resample_deformation = 0;
+  p->use_fp64 = 0;
+}
+
+int msgpu_abi_version(void) { return kAbiVersion; }
+
+int msgpu_create(int device, msgpu_context** out) {
+  if (!out) return MSGPU_ERR_INVALID_ARG;
+  *out = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) return MSGPU_ERR_CUDA;
+  if (device < 0 || device >= count) return MSGPU_ERR_INVALID_ARG;
+  msgpu_context* ctx = new msgpu_context();
+  ctx->device = device;
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return MSGPU_ERR_CUDA;
+  }
+  *out = ctx;
+  return MSGPU_OK;
+}
+
+int msgpu_destroy(msgpu_context* ctx) {
+  if (!ctx) return MSGPU_OK;
+  cudaSetDevice(ctx->device);
+  msgpu_context::Buf* bufs[] = {&ctx->arena, &ctx->shared_real, &ctx->dscratch, &ctx->small, &ctx->phis_d,
+                                &ctx->io[0], &ctx->io[1], &ctx->io[2], &ctx->io[3], &ctx->io[4], &ctx->io[5]};
+  for (auto* b : bufs)
+    if (b->p) cudaFree(b->p);
+  if (ctx->ev_ready)
+    for (int i = 0; i < 32; ++i) cudaEventDestroy(ctx->ev[i]);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return MSGPU_OK;
+}
+
+const char* msgpu_last_error(const msgpu_context* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+int msgpu_register_batch_device(msgpu_context* ctx, const msgpu_params* p, const double* d_reference,
+                                const double* d_templates, int num_templates, const double* d_initial_phis,
+                                double* d_phis_out, double* d_energies_out, int* d_steps_out, void* stream) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  int rc;
+  if ((rc = check_params(ctx, p))) return rc;
+  if (num_templates < 1) return fail(ctx, MSGPU_ERR_INVALID_ARG, "num_templates must be >= 1");
+  if (!d_reference || !d_templates || !d_phis_out) return fail(ctx, MSGPU_ERR_INVALID_ARG, "null buffer");
+  if ((rc = bind_device(ctx))) return rc;
+  BatchIO io{d_reference, d_templates, d_initial_phis, d_phis_out, d_energies_out, d_steps_out};
+  cudaStream_t st = (cudaStream_t)stream;
+  return p->use_fp64 ? run_batch<double>(ctx, *p, num_templates, io, st)
+                     : run_batch<float>(ctx, *p, num_templates, io, st);
+}
+
+int msgpu_register_batch(msgpu_context* ctx, const msgpu_params* p, const double* reference,
+                         const double* templates, int num_templates, const double* initial_phis,
+                         double* phis_out, double* energies_out, int* steps_out) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  int rc;
+  if ((rc = check_params(ctx, p))) return rc;
+  if (num_templates < 1) return fail(ctx, MSGPU_ERR_INVALID_ARG, "num_templates must be >= 1");
+  if (!reference || !templates || !phis_out) return fail(ctx, MSGPU_ERR_INVALID_ARG, "null buffer");
+  if ((rc = bind_device(ctx))) return rc;
+  const size_t Nin = lvl_N(p->input_level), NM = lvl_N(p->precision_level);
+  const int F = num_templates;
+  const int nlev = p->stop_level - p->start_level + 1;
+  if ((rc = ensure(ctx, ctx->io[0], sizeof(double) * Nin))) return rc;
+  if ((rc = ensure(ctx, ctx->io[1], sizeof(double) * Nin * F))) return rc;
+  if ((rc = ensure(ctx, ctx->io[2], sizeof(double) * 2 * NM * F))) return rc;
+  if ((rc = ensure(ctx, ctx->io[3], sizeof(double) * 2 * NM * F))) return rc;
+  if ((rc = ensure(ctx, ctx->io[4], sizeof(double) * F + sizeof(int) * F * nlev + 64))) return rc;
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(ctx->io[0].p, reference, sizeof(double) * Nin, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctx->io[1].p, templates, sizeof(double) * Nin * F, cudaMemcpyHostToDevice, st));
+  if (initial_phis)
+    CK(cudaMemcpyAsync(ctx->io[2].p, initial_phis, sizeof(double) * 2 * NM * F, cudaMemcpyHostToDevice, st));
+  double* d_e = (double*)ctx->io[4].p;
+  int* d_s = (int*)(d_e + F);
+  BatchIO io{(const double*)ctx->io[0].p, (const double*)ctx->io[1].p,
+             initial_phis ? (const double*)ctx->io[2].p : nullptr, (double*)ctx->io[3].p, d_e, d_s};
+  rc = p->use_fp64 ? run_batch<double>(ctx, *p, F, io, st) : run_batch<float>(ctx, *p, F, io, st);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(phis_out, ctx->io[3].p, sizeof(double) * 2 * NM * F, cudaMemcpyDeviceToHost, st));
+  std::vector<double> e(F);
+  std::vector<int> s((size_t)F * nlev);
+  CK(cudaMemcpyAsync(e.data(), d_e, sizeof(double) * F, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(s.data(), d_s, sizeof(int) * F * nlev, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (energies_out) memcpy(energies_out, e.data(), sizeof(double) * F);
+  if (steps_out) memcpy(steps_out, s.data(), sizeof(int) * F * nlev);
+  return MSGPU_OK;
+}
+
+int msgpu_warp_mean_device(msgpu_context* ctx, int level, const double* d_frames, const double* d_phis,
+                           int num_frames, double* d_mean_out, double* d_count_out, void* stream) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (level < 1 || level > kMaxLevel || num_frames < 1 || !d_frames || !d_phis || !d_mean_out || !d_count_out)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid warp_mean arguments");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  if ((rc = ensure(ctx, ctx->io[5], 64))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int N = (int)lvl_N(level);
+  k_mean<<<1, 1024, 0, st>>>(d_frames + (size_t)(num_frames - 1) * N, N, (double*)ctx->io[5].p);
+  k_warp_mean<<<std::min(2048, (N + 255) / 256), 256, 0, st>>>(d_frames, d_phis, num_frames, level,
+                                                               (const double*)ctx->io[5].p, d_mean_out,
+                                                               d_count_out);
+  CK(cudaGetLastError());
+  ctx->stats.kernel_launches += 2;
+  return MSGPU_OK;
+}
+
+int msgpu_match_series_stage_device(msgpu_context* ctx, const msgpu_params* p, const double* d_reference,
+                                    const double* d_templates, int num_templates, double* d_phis_out,
+                                    double* d_energies_out, int* d_steps_out, double* d_mean_out,
+                                    double* d_count_out, void* stream) {
+  int rc = msgpu_register_batch_device(ctx, p, d_reference, d_templates, num_templates, nullptr, d_phis_out,
+                                       d_energies_out, d_steps_out, stream);
+  if (rc) return rc;
+  if (p->input_level != p->precision_level)
+    return fail(ctx, MSGPU_ERR_UNSUPPORTED, "the stage average needs input_level == precision_level");
+  return msgpu_warp_mean_device(ctx, p->precision_level, d_templates, d_phis_out, num_templates, d_mean_out,
+                                d_count_out, stream);
+}
+
+int msgpu_match_series_stage(msgpu_context* ctx, const msgpu_params* p, const double* reference,
+                             const double* templates, int num_templates, double* phis_out, double* energies_out,
+                             int* steps_out, double* mean_out, double* count_out) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  int rc;
+  if ((rc = check_params(ctx, p))) return rc;
+  if (num_templates < 1) return fail(ctx, MSGPU_ERR_INVALID_ARG, "num_templates must be >= 1");
+  if (!reference || !templates || !phis_out || !mean_out || !count_out)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "null buffer");
+  if (p->input_level != p->precision_level)
+    return fail(ctx, MSGPU_ERR_UNSUPPORTED, "the stage average needs input_level == precision_level");
+  if ((rc = bind_device(ctx))) return rc;
+  const size_t N = lvl_N(p->precision_level);
+  const int F = num_templates;
+  const int nlev = p->stop_level - p->start_level + 1;
+  if ((rc = ensure(ctx, ctx->io[0], sizeof(double) * N))) return rc;
+  if ((rc = ensure(ctx, ctx->io[1], sizeof(double) * N * F))) return rc;
+  if ((rc = ensure(ctx, ctx->io[3], sizeof(double) * (2 * N * F + 2 * N)))) return rc;
+  if ((rc = ensure(ctx, ctx->io[4], sizeof(double) * F + sizeof(int) * F * nlev + 64))) return rc;
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(ctx->io[0].p, reference, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctx->io[1].p, templates, sizeof(double) * N * F, cudaMemcpyHostToDevice, st));
+  double* d_phis = (double*)ctx->io[3].p;
+  double* d_mean = d_phis + 2 * N * F;
+  double* d_e = (double*)ctx->io[4].p;
+  int* d_s = (int*)(d_e + F);
+  if ((rc = msgpu_match_series_stage_device(ctx, p, (const double*)ctx->io[0].p, (const double*)ctx->io[1].p, F,
+                                            d_phis, d_e, d_s, d_mean, d_mean + N, st)))
+    return rc;
+  CK(cudaMemcpyAsync(phis_out, d_phis, sizeof(double) * 2 * N * F, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(mean_out, d_mean, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(count_out, d_mean + N, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+  std::vector<double> e(F);
+  std::vector<int> s((size_t)F * nlev);
+  CK(cudaMemcpyAsync(e.data(), d_e, sizeof(double) * F, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(s.data(), d_s, sizeof(int) * F * nlev, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (energies_out) memcpy(energies_out, e.data(), sizeof(double) * F);
+  if (steps_out) memcpy(steps_out, s.data(), sizeof(int) * F * nlev);
+  return MSGPU_OK;
+}
+
+int msgpu_set_profiling(msgpu_context* ctx, int on) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  ctx->profiling = (on != 0);
+  return MSGPU_OK;
+}
+
+int msgpu_get_stats(const msgpu_context* ctx, msgpu_stats* out) {
+  if (!ctx || !out) return MSGPU_ERR_INVALID_ARG;
+  *out = ctx->stats;
+  return MSGPU_OK;
+}
+
+int msgpu_warp_mean(msgpu_context* ctx, int level, const double* frames, const double* phis, int num_frames,
+                    double* mean_out, double* count_out) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (level < 1 || level > kMaxLevel || num_frames < 1 || !frames || !phis || !mean_out || !count_out)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid warp_mean arguments");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  const size_t N = lvl_N(level);
+  const int F = num_frames;
+  if ((rc = ensure(ctx, ctx->io[0], sizeof(double) * N * F))) return rc;
+  if ((rc = ensure(ctx, ctx->io[1], sizeof(double) * 2 * N * F))) return rc;
+  if ((rc = ensure(ctx, ctx->io[2], sizeof(double) * 2 * N))) return rc;
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(ctx->io[0].p, frames, sizeof(double) * N * F, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctx->io[1].p, phis, sizeof(double) * 2 * N * F, cudaMemcpyHostToDevice, st));
+  double* dm = (double*)ctx->io[2].p;
+  if ((rc = msgpu_warp_mean_device(ctx, level, (const double*)ctx->io[0].p, (const double*)ctx->io[1].p, F, dm,
+                                    dm + N, st)))
+    return rc;
+  CK(cudaMemcpyAsync(mean_out, dm, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(count_out, dm + N, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return MSGPU_OK;
+}
+
+}  // extern "C"
+
+// --- single operators ------------------------------------------------------
+
+namespace {
+// Runs the level kernel for ONE instance at `level` in the given mode with
+// R/T/phi (and for MODE_SMOOTH the vector in the DE slot) uploaded from host.
+template <typename Real>
+int single_level(msgpu_context* ctx, int level, int mode, const double* R, const double* T, const double* phix,
+                 const double* phiy, const double* de_in, double lambda, int max_iter, double stop_eps,
+                 double sigma, double* energy_out, int* steps_out, double* phix_out, double* phiy_out,
+                 double* de_out, double* trace, int max_trace) {
+  int rc;
+  if ((rc = ensure_tables(ctx))) return rc;
+  const Layout L = make_layout(level);
+  const size_t N = lvl_N(level);
+  if ((rc = ensure(ctx, ctx->arena, sizeof(Real) * L.stride))) return rc;
+  if ((rc = ensure(ctx, ctx->shared_real, sizeof(Real) * (N + 64)))) return rc;
+  if ((rc = ensure(ctx, ctx->io[0], sizeof(double) * 6 * N))) return rc;
+  const size_t trace_n = (size_t)std::max(1, max_trace) * 4;
+  if ((rc = ensure(ctx, ctx->small, sizeof(double) * (8 + trace_n) + 64))) return rc;
+  cudaStream_t st = ctx->stream;
+  Real* arena = (Real*)ctx->arena.p;
+  Real* Rd = (Real*)ctx->shared_real.p;
+  double* h = (double*)ctx->io[0].p;
+  double* sm = (double*)ctx->small.p;
+  double* d_e = sm;
+  int* d_i = (int*)(sm + 2);  // steps, buf
+  double* d_trace = sm + 8;
+  CK(cudaMemsetAsync(arena, 0, sizeof(Real) * L.stride, st));
+  const double* srcs[5] = {R, T, phix, phiy, de_in};
+  for (int k = 0; k < 5; ++k)
+    if (srcs[k]) CK(cudaMemcpyAsync(h + k * N, srcs[k], sizeof(double) * N, cudaMemcpyHostToDevice, st));
+  const unsigned gx = (unsigned)std::min<size_t>(1024, (N + 255) / 256);
+  if (R) k_convert<double, Real><<<gx, 256, 0, st>>>(h, 0, Rd, 0, N);
+  if (T) k_convert<double, Real><<<gx, 256, 0, st>>>(h + N, 0, arena + L.off_T[level], 0, N);
+  if (phix) k_convert<double, Real><<<gx, 256, 0, st>>>(h + 2 * N, 0, arena + L.off_phi[0], 0, N);
+  if (phiy) k_convert<double, Real><<<gx, 256, 0, st>>>(h + 3 * N, 0, arena + L.off_phi[0] + N, 0, N);
+  if (de_in) k_convert<double, Real><<<gx, 256, 0, st>>>(h + 4 * N, 0, arena + L.off_de, 0, N);
+  k_set_buf<Real><<<1, 32, 0, st>>>(d_i + 1, 1, 0);
+  CK(cudaGetLastError());
+  LevelArgs<Real> a;
+  memset(&a, 0, sizeof(a));
+  a.arena = arena;
+  a.inst_stride = L.stride;
+  a.R = Rd;
+  a.off_T = L.off_T[level];
+  a.off_phi[0] = L.off_phi[0];
+  a.off_phi[1] = L.off_phi[1];
+  a.off_d[0] = L.off_d[0];
+  a.off_d[1] = L.off_d[1];
+  a.off_s = L.off_s;
+  a.off_de = L.off_de;
+  for (int k = 0; k <= kMaxLevel; ++k) { a.off_x2[k] = L.off_x2[k]; a.off_x5[k] = L.off_x5[k]; a.off_b[k] = L.off_b[k]; }
+  a.level = level;
+  a.n = lvl_n(level);
+  a.num_inst = 1;
+  a.lc = pick_lc<Real>(level);
+  a.mode = mode;
+  a.lambda = lambda;
+  a.stop_eps = stop_eps;
+  a.sigma_fixed = sigma;
+  a.max_iter = max_iter;
+  a.phi_in_dev = d_i + 1;
+  a.out_energy = d_e;
+  a.out_steps = d_i;
+  a.out_phi_buf = d_i + 1;
+  a.trace = trace ? d_trace : nullptr;
+  a.max_trace = max_trace;
+  const int G = pick_cluster(ctx->sm_count, 1, level);
+  if ((rc = launch_level<Real>(ctx, a, G, st))) return rc;
+  CK(cudaGetLastError());
+  // outputs
+  int hi[2] = {0, 0};
+  double he = 0;
+  CK(cudaMemcpyAsync(&he, d_e, sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(hi, d_i, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (energy_out) *energy_out = he;
+  if (steps_out) *steps_out = hi[0];
+  auto fetch = [&](size_t off, double* dst) -> int {
+    k_convert<Real, double><<<gx, 256, 0, st>>>(arena + off, 0, h + 5 * N, 0, N);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(dst, h + 5 * N, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return MSGPU_OK;
+  };
+  if (mode == MODE_SMOOTH) {
+    if ((rc = fetch(L.off_s, de_out))) return rc;
+    return MSGPU_OK;
+  }
+  if (de_out) {
+    if ((rc = fetch(L.off_de, de_out))) return rc;
+    if ((rc = fetch(L.off_de + N, de_out + N))) return rc;
+  }
+  const size_t phioff = hi[1] ? L.off_phi[1] : L.off_phi[0];
+  if (phix_out && (rc = fetch(phioff, phix_out))) return rc;
+  if (phiy_out && (rc = fetch(phioff + N, phiy_out))) return rc;
+  if (trace && max_trace > 0) {
+    const int rows = std::min(hi[0], max_trace);
+    CK(cudaMemcpy(trace, d_trace, sizeof(double) * 4 * rows, cudaMemcpyDeviceToHost));
+  }
+  return MSGPU_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int msgpu_energy(msgpu_context* ctx, int level, const double* R, const double* T, const double* phix,
+                 const double* phiy, double lambda, int use_fp64, double* energy_out, double* de_out) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (level < 1 || level > kMaxLevel || !R || !T || !phix || !phiy)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid energy arguments");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  return use_fp64 ? single_level<double>(ctx, level, MODE_ENERGY, R, T, phix, phiy, nullptr, lambda, 0, 0, 0,
+                                         energy_out, nullptr, nullptr, nullptr, de_out, nullptr, 0)
+                  : single_level<float>(ctx, level, MODE_ENERGY, R, T, phix, phiy, nullptr, lambda, 0, 0, 0,
+                                        energy_out, nullptr, nullptr, nullptr, de_out, nullptr, 0);
+}
+
+int msgpu_smooth(msgpu_context* ctx, int level, double sigma, int use_fp64, const double* in, double* out) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (level < 1 || level > kMaxLevel || !in || !out) return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid smooth arguments");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  // the V-cycle smooths -DE: place -in into the DE slot (exact negation)
+  const size_t N = lvl_N(level);
+  std::vector<double> neg(N);
+  for (size_t i = 0; i < N; ++i) neg[i] = in[i] * -1.0;
+  return use_fp64 ? single_level<double>(ctx, level, MODE_SMOOTH, nullptr, nullptr, nullptr, nullptr, neg.data(),
+                                         1.0, 0, 0, sigma, nullptr, nullptr, nullptr, nullptr, out, nullptr, 0)
+                  : single_level<float>(ctx, level, MODE_SMOOTH, nullptr, nullptr, nullptr, nullptr, neg.data(),
+                                        1.0, 0, 0, sigma, nullptr, nullptr, nullptr, nullptr, out, nullptr, 0);
+}
+
+int msgpu_gd_level(msgpu_context* ctx, int level, const double* R, const double* T, double* phix, double* phiy,
+                   double lambda, int max_iter, double stop_eps, int use_fp64, double* energy_out, int* steps_out,
+                   double* trace, int max_trace) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (level < 1 || level > kMaxLevel || !R || !T || !phix || !phiy || max_iter < 0)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid gd_level arguments");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  return use_fp64 ? single_level<double>(ctx, level, MODE_SOLVE, R, T, phix, phiy, nullptr, lambda, max_iter,
+                                         stop_eps, 0, energy_out, steps_out, phix, phiy, nullptr, trace, max_trace)
+                  : single_level<float>(ctx, level, MODE_SOLVE, R, T, phix, phiy, nullptr, lambda, max_iter,
+                                        stop_eps, 0, energy_out, steps_out, phix, phiy, nullptr, trace, max_trace);
+}
+
+int msgpu_restrict(msgpu_context* ctx, int fine_level, const double* in, double* out) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (fine_level < 1 || fine_level > kMaxLevel || !in || !out)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid restrict arguments");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  const size_t Nf = lvl_N(fine_level), Nc = lvl_N(fine_level - 1);
+  if ((rc = ensure(ctx, ctx->io[0], sizeof(double) * (Nf + Nc)))) return rc;
+  double* d = (double*)ctx->io[0].p;
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(d, in, sizeof(double) * Nf, cudaMemcpyHostToDevice, st));
+  k_restrict<double><<<dim3((unsigned)std::min<size_t>(1024, (Nc + 255) / 256), 1), 256, 0, st>>>(d, 0, d + Nf, 0,
+                                                                                                 fine_level);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, d + Nf, sizeof(double) * Nc, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return MSGPU_OK;
+}
+
+int msgpu_prolong(msgpu_context* ctx, int coarse_level, const double* in, double* out) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (coarse_level < 0 || coarse_level >= kMaxLevel || !in || !out)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid prolong arguments");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  const size_t Nc = lvl_N(coarse_level), Nf = lvl_N(coarse_level + 1);
+  if ((rc = ensure(ctx, ctx->io[0], sizeof(double) * (Nf + Nc)))) return rc;
+  double* d = (double*)ctx->io[0].p;
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(d, in, sizeof(double) * Nc, cudaMemcpyHostToDevice, st));
+  k_prolong<double><<<dim3((unsigned)std::min<size_t>(1024, (Nf + 255) / 256), 1), 256, 0, st>>>(d, 0, d + Nc, 0,
+                                                                                                coarse_level);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, d + Nc, sizeof(double) * Nf, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return MSGPU_OK;
+}
+
+int msgpu_normalize(msgpu_context* ctx, const double* in, int count, double saturation_percent,
+                    int normalize_min_to_zero, double* out) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (!in || !out || count < 1) return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid normalize arguments");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  if ((rc = ensure(ctx, ctx->io[0], sizeof(double) * (count + 8)))) return rc;
+  double* d = (double*)ctx->io[0].p;
+  double* mm = d + count;
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(d, in, sizeof(double) * count, cudaMemcpyHostToDevice, st));
+  if (saturation_percent >= 0) {
+    const int m1 = count - 1;
+    int il = (int)(saturation_percent / 200 * m1), ih = (int)((1 - saturation_percent / 200) * m1);
+    il = std::min(std::max(il, 0), m1);
+    ih = std::min(std::max(ih, 0), m1);
+    k_select2<<<1, kSelThreads, 0, st>>>(d, 0, count, il, ih, mm);
+  } else {
+    k_minmax<<<1, 1024, 0, st>>>(d, 0, count, mm);
+  }
+  k_normalize<<<dim3((unsigned)std::min(1024, (count + 255) / 256), 1), 256, 0, st>>>(
+      d, 0, count, mm, saturation_percent >= 0 ? 1 : 0, normalize_min_to_zero);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, d, sizeof(double) * count, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return MSGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,267 @@
+"""Python binding of the msgpu C ABI (include/msgpu.h).
+
+The CUDA library libmsgpu.so is built in-tree by ``msgpu.build.build()``.  There
+is no CPU fallback: every call goes to the CUDA kernels, and a missing library
+or a missing GPU raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmsgpu.so")
+
+MSGPU_OK = 0
+STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "SIZE", 3: "CUDA", 4: "UNSUPPORTED"}
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+class Params(ctypes.Structure):
+    """msgpu_params: the parameter-file keys of the registration path."""
+    _fields_ = [
+        ("precision_level", ctypes.c_int),
+        ("input_level", ctypes.c_int),
+        ("start_level", ctypes.c_int),
+        ("stop_level", ctypes.c_int),
+        ("lambda_", ctypes.c_double),
+        ("lambda_factor", ctypes.c_double),
+        ("max_gd_iterations", ctypes.c_int),
+        ("stop_epsilon", ctypes.c_double),
+        ("saturation_percent", ctypes.c_double),
+        ("normalize_min_to_zero", ctypes.c_int),
+        ("dont_normalize_input", ctypes.c_int),
+        ("resample_deformation", ctypes.c_int),
+        ("use_fp64", ctypes.c_int),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("kernel_launches", ctypes.c_int), ("num_levels", ctypes.c_int), ("first_level", ctypes.c_int),
+                ("level_ms", ctypes.c_float * 16), ("level_steps", ctypes.c_longlong * 16),
+                ("level_evals", ctypes.c_longlong * 16)]
+
+
+class MsgpuError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"msgpu {STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+_lib = None
+
+EXPORTS = [
+    "msgpu_params_default", "msgpu_abi_version", "msgpu_create", "msgpu_destroy", "msgpu_last_error",
+    "msgpu_register_batch", "msgpu_register_batch_device", "msgpu_warp_mean", "msgpu_warp_mean_device",
+    "msgpu_energy", "msgpu_smooth", "msgpu_restrict", "msgpu_prolong", "msgpu_normalize", "msgpu_gd_level",
+    "msgpu_match_series_stage", "msgpu_match_series_stage_device", "msgpu_set_profiling", "msgpu_get_stats",
+]
+
+
+def lib():
+    """Loads libmsgpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with msgpu.build.build() (no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        L.msgpu_last_error.restype = ctypes.c_char_p
+        L.msgpu_last_error.argtypes = [ctypes.c_void_p]
+        L.msgpu_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+        L.msgpu_destroy.argtypes = [ctypes.c_void_p]
+        L.msgpu_params_default.argtypes = [ctypes.POINTER(Params)]
+        L.msgpu_params_default.restype = None
+        L.msgpu_register_batch.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params), _dp, _dp, ctypes.c_int, _dp,
+                                           _dp, _dp, _ip]
+        L.msgpu_register_batch_device.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params), ctypes.c_void_p,
+                                                  ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.msgpu_warp_mean.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp, _dp]
+        L.msgpu_warp_mean_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.msgpu_energy.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_double,
+                                   ctypes.c_int, _dp, _dp]
+        L.msgpu_smooth.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp, _dp]
+        L.msgpu_restrict.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
+        L.msgpu_prolong.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
+        L.msgpu_normalize.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp]
+        L.msgpu_gd_level.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_double,
+                                     ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp, _ip, _dp, ctypes.c_int]
+        L.msgpu_match_series_stage.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params), _dp, _dp, ctypes.c_int,
+                                               _dp, _dp, _ip, _dp, _dp]
+        L.msgpu_match_series_stage_device.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params), ctypes.c_void_p,
+                                                      ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                      ctypes.c_void_p, ctypes.c_void_p]
+        L.msgpu_set_profiling.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.msgpu_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(Stats)]
+        _lib = L
+    return _lib
+
+
+def default_params(**kw) -> Params:
+    p = Params()
+    lib().msgpu_params_default(ctypes.byref(p))
+    for k, v in kw.items():
+        setattr(p, "lambda_" if k == "lambda" else k, v)
+    return p
+
+
+def n_of(level: int) -> int:
+    return (1 << level) + 1
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+class Context:
+    """A msgpu_context bound to one CUDA device."""
+
+    def __init__(self, device: int = 0):
+        self._h = ctypes.c_void_p()
+        st = lib().msgpu_create(device, ctypes.byref(self._h))
+        if st != MSGPU_OK:
+            raise MsgpuError(st, f"msgpu_create(device={device}) failed (no CUDA device?)")
+
+    def close(self):
+        if self._h:
+            lib().msgpu_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int):
+        if st != MSGPU_OK:
+            msg = lib().msgpu_last_error(self._h)
+            raise MsgpuError(st, msg.decode() if msg else "")
+
+    # --- batch path -----------------------------------------------------
+    def register_batch(self, params: Params, reference, templates, initial_phis=None):
+        """Registers every template to the reference; returns (phis[F,2,N], energies[F], steps[F,levels])."""
+        ref = _f64(reference).reshape(-1)
+        tm = _f64(templates)
+        F = tm.shape[0]
+        tm = tm.reshape(F, -1)
+        N = n_of(params.precision_level) ** 2
+        nlev = params.stop_level - params.start_level + 1
+        phis = np.zeros((F, 2, N))
+        energies = np.zeros(F)
+        steps = np.zeros((F, nlev), dtype=np.int32)
+        ip = None
+        if initial_phis is not None:
+            ip = _f64(initial_phis).reshape(F, 2, N)
+        self._check(lib().msgpu_register_batch(self._h, ctypes.byref(params), _p(ref), _p(tm), F,
+                                               _p(ip) if ip is not None else None, _p(phis), _p(energies),
+                                               steps.ctypes.data_as(_ip)))
+        return phis, energies, steps
+
+    def register_batch_device(self, params: Params, d_ref: int, d_templates: int, num_templates: int,
+                              d_phis_out: int, d_energies: int = 0, d_steps: int = 0, d_init: int = 0,
+                              stream: int = 0):
+        self._check(lib().msgpu_register_batch_device(self._h, ctypes.byref(params), d_ref, d_templates,
+                                                      num_templates, d_init or None, d_phis_out, d_energies or None,
+                                                      d_steps or None, stream or None))
+
+    def warp_mean(self, level: int, frames, phis):
+        fr = _f64(frames)
+        F = fr.shape[0]
+        N = n_of(level) ** 2
+        ph = _f64(phis).reshape(F, 2, N)
+        mean = np.zeros(N)
+        count = np.zeros(N)
+        self._check(lib().msgpu_warp_mean(self._h, level, _p(fr.reshape(F, N)), _p(ph), F, _p(mean), _p(count)))
+        return mean, count
+
+    def warp_mean_device(self, level: int, d_frames: int, d_phis: int, num_frames: int, d_mean: int, d_count: int,
+                         stream: int = 0):
+        self._check(lib().msgpu_warp_mean_device(self._h, level, d_frames, d_phis, num_frames, d_mean, d_count,
+                                                 stream or None))
+
+    def match_series_stage(self, params: Params, reference, templates, out=None):
+        """register_batch + warp_mean in one call; returns (phis, energies, steps, mean, count).
+        ``out`` may hold preallocated (phis, energies, steps, mean, count) arrays."""
+        ref = _f64(reference).reshape(-1)
+        tm = _f64(templates)
+        F = tm.shape[0]
+        tm = tm.reshape(F, -1)
+        N = n_of(params.precision_level) ** 2
+        nlev = params.stop_level - params.start_level + 1
+        if out is None:
+            out = (np.zeros((F, 2, N)), np.zeros(F), np.zeros((F, nlev), dtype=np.int32), np.zeros(N), np.zeros(N))
+        phis, energies, steps, mean, count = out
+        self._check(lib().msgpu_match_series_stage(self._h, ctypes.byref(params), _p(ref), _p(tm), F, _p(phis),
+                                                   _p(energies), steps.ctypes.data_as(_ip), _p(mean), _p(count)))
+        return out
+
+    def match_series_stage_device(self, params: Params, d_ref: int, d_templates: int, num_templates: int,
+                                  d_phis: int, d_energies: int, d_steps: int, d_mean: int, d_count: int,
+                                  stream: int = 0):
+        self._check(lib().msgpu_match_series_stage_device(self._h, ctypes.byref(params), d_ref, d_templates,
+                                                          num_templates, d_phis, d_energies or None, d_steps or None,
+                                                          d_mean, d_count, stream or None))
+
+    def set_profiling(self, on: bool):
+        self._check(lib().msgpu_set_profiling(self._h, int(bool(on))))
+
+    def stats(self) -> dict:
+        s = Stats()
+        self._check(lib().msgpu_get_stats(self._h, ctypes.byref(s)))
+        k = s.num_levels
+        return {"kernel_launches": s.kernel_launches, "first_level": s.first_level,
+                "level_ms": list(s.level_ms[:k]), "level_steps": list(s.level_steps[:k]),
+                "level_evals": list(s.level_evals[:k])}
+
+    # --- single operators ------------------------------------------------
+    def energy(self, level, R, T, phix, phiy, lam, fp64=False):
+        N = n_of(level) ** 2
+        e = ctypes.c_double()
+        de = np.zeros(2 * N)
+        self._check(lib().msgpu_energy(self._h, level, _p(_f64(R)), _p(_f64(T)), _p(_f64(phix)), _p(_f64(phiy)),
+                                       float(lam), int(fp64), ctypes.byref(e), _p(de)))
+        return e.value, de[:N], de[N:]
+
+    def smooth(self, level, sigma, x, fp64=False):
+        out = np.zeros(n_of(level) ** 2)
+        self._check(lib().msgpu_smooth(self._h, level, float(sigma), int(fp64), _p(_f64(x)), _p(out)))
+        return out
+
+    def restrict(self, fine_level, x):
+        out = np.zeros(n_of(fine_level - 1) ** 2)
+        self._check(lib().msgpu_restrict(self._h, fine_level, _p(_f64(x)), _p(out)))
+        return out
+
+    def prolong(self, coarse_level, x):
+        out = np.zeros(n_of(coarse_level + 1) ** 2)
+        self._check(lib().msgpu_prolong(self._h, coarse_level, _p(_f64(x)), _p(out)))
+        return out
+
+    def normalize(self, x, sat=0.15, min_to_zero=1):
+        a = _f64(x).reshape(-1)
+        out = np.zeros_like(a)
+        self._check(lib().msgpu_normalize(self._h, _p(a), a.size, float(sat), int(min_to_zero), _p(out)))
+        return out
+
+    def gd_level(self, level, R, T, phix, phiy, lam, max_iter, stop_eps=0.0, fp64=False, max_trace=256):
+        px = _f64(phix).copy()
+        py = _f64(phiy).copy()
+        e = ctypes.c_double()
+        st = ctypes.c_int()
+        tr = np.zeros((max_trace, 4))
+        self._check(lib().msgpu_gd_level(self._h, level, _p(_f64(R)), _p(_f64(T)), _p(px), _p(py), float(lam),
+                                         int(max_iter), float(stop_eps), int(fp64), ctypes.byref(e),
+                                         ctypes.byref(st), _p(tr), max_trace))
+        steps = st.value
+        return px, py, e.value, steps, tr[:min(steps, max_trace)]

@@ -1,0 +1,124 @@
+"""Generates the golden fixtures of tests/golden/ from the reference itself.
+
+Runs the reference's own templates through oracle/_ref/ms_ref (built from the
+quocmesh sources by oracle/Makefile.ref) on seeded synthetic lattice images
+and stores inputs and outputs as compressed .npz files.  The reference's own
+tests hold no golden vectors for this path, so these fixtures pin both the
+CPU oracle and the CUDA path.  Run from the repository root:
+
+    make -f oracle/Makefile.ref && python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.join(ROOT, "match-series_b200"))
+import msor  # noqa: E402
+from msgpu import synthetic as syn  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def n_of(level):
+    return (1 << level) + 1
+
+
+def ops(ref: msor.RefRunner, level: int, seed: int):
+    n = n_of(level)
+    rng = np.random.default_rng(seed)
+    fr, _, _ = syn.make_series(n, 2, syn.HEX_513, seed=seed)
+    raw_t = fr[1].ravel()
+    R = ref.normalize(level, fr[0].ravel())
+    T = ref.normalize(level, raw_t)
+    px = rng.normal(0, 0.5 / (n - 1), n * n)     # about half a pixel
+    py = rng.normal(0, 0.5 / (n - 1), n * n)
+    bx = px.copy()
+    bx[: n] += 2.0 / (n - 1)                       # push the first row past the boundary (clipping)
+    d = {"level": level, "R": R, "T": T, "px": px, "py": py, "lam": 0.1, "raw_t": raw_t}
+    for tag, qx in (("", px), ("_clip", bx)):
+        r = ref.energy(level, R, T, qx, py, 0.1)
+        d["E" + tag] = np.array([r["essd"], r["ereg"], r["e"]])
+        d["DE" + tag] = np.stack([r["dex"], r["dey"]])
+        d["F" + tag] = np.stack([r["fx"], r["fy"]])
+    d["px_clip"] = bx
+    x = rng.normal(size=n * n)
+    d["smooth_in"] = x
+    d["smooth_sigmas"] = np.array([1.0, 0.25, 0.01])
+    d["smooth_out"] = np.stack([ref.smooth(level, s, x) for s in d["smooth_sigmas"]])
+    d["restrict_out"] = ref.restrict(level, x)
+    xc = rng.normal(size=n_of(level - 1) ** 2)
+    d["prolong_in"] = xc
+    d["prolong_out"] = ref.prolong(level - 1, xc)
+    d["resample_out"] = ref.resample(level - 1, xc, level)
+    big = 3.0 / (n - 1)
+    qx, qy = rng.normal(0, big, n * n), rng.normal(0, big, n * n)
+    d["deform_px"], d["deform_py"] = qx, qy
+    d["deform_out"] = ref.deform(level, raw_t, qx, qy)
+    d["normalize_out"] = T
+    d["normalize_nosat_out"] = ref.normalize(level, raw_t, sat=-1, min_to_zero=1)
+    np.savez_compressed(os.path.join(OUT, f"ops_L{level}.npz"), **d)
+
+
+def gd(ref: msor.RefRunner, level: int, seed: int, lam: float, max_iter: int):
+    n = n_of(level)
+    fr, _, _ = syn.make_series(n, 2, syn.SQUARE_257, seed=seed)
+    R = ref.normalize(level, fr[0].ravel())
+    T = ref.normalize(level, fr[1].ravel())
+    z = np.zeros(n * n)
+    px, py, e, steps, trace = ref.gd_level(level, R, T, z, z, lam, max_iter)
+    np.savez_compressed(os.path.join(OUT, f"gd_L{level}.npz"), level=level, R=R, T=T, lam=lam, max_iter=max_iter,
+                        px=px, py=py, energy=e, steps=steps, trace=np.array(trace, dtype=np.float64))
+
+
+def register(ref: msor.RefRunner, level: int, seed: int):
+    n = n_of(level)
+    fr, _, _ = syn.make_series(n, 2, syn.HEX_513, seed=seed)
+    R = ref.normalize(level, fr[0].ravel())
+    T = ref.normalize(level, fr[1].ravel())
+    cases = [
+        dict(start=4, stop=level, lam=0.1, lam_factor=1.0, max_iter=20, stop_eps=0.0, resample=0),
+        dict(start=3, stop=level - 1, lam=0.2, lam_factor=0.5, max_iter=15, stop_eps=1e-7, resample=0),
+        dict(start=4, stop=level, lam=0.1, lam_factor=1.0, max_iter=10, stop_eps=0.0, resample=1),
+    ]
+    out = {"level": level, "R": R, "T": T}
+    for i, c in enumerate(cases):
+        px, py, e = ref.register(level, c["start"], c["stop"], R, T, lam=c["lam"], lam_factor=c["lam_factor"],
+                                 max_iter=c["max_iter"], stop_eps=c["stop_eps"], resample_phi=bool(c["resample"]))
+        out[f"case{i}"] = np.array([c["start"], c["stop"], c["lam"], c["lam_factor"], c["max_iter"], c["stop_eps"],
+                                    c["resample"]], dtype=np.float64)
+        out[f"phi{i}"] = np.stack([px, py])
+        out[f"E{i}"] = np.array([e])
+    np.savez_compressed(os.path.join(OUT, f"register_L{level}.npz"), **out)
+
+
+def series(ref: msor.RefRunner, level: int, F: int, seed: int):
+    n = n_of(level)
+    fr, clean, _ = syn.make_series(n, F, syn.SQUARE_257, seed=seed)
+    frames = fr.reshape(F, -1)
+    phis, mean, info = ref.series(level, 3, level, frames, 0.1, 1.0, 15)
+    np.savez_compressed(os.path.join(OUT, f"series_L{level}.npz"), level=level, frames=frames, phis=phis,
+                        mean=mean, energies=np.array(info["energies"]), start=3, lam=0.1, max_iter=15)
+
+
+def main():
+    if not msor.have_ref():
+        raise SystemExit("oracle/_ref/ms_ref is missing: make -f oracle/Makefile.ref")
+    ref = msor.RefRunner()
+    ops(ref, 5, 101)
+    ops(ref, 6, 102)
+    gd(ref, 5, 201, 0.1, 20)
+    gd(ref, 6, 202, 0.05, 30)
+    register(ref, 7, 301)
+    series(ref, 6, 4, 401)
+    for f in sorted(os.listdir(OUT)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(OUT, f)))
+
+
+if __name__ == "__main__":
+    main()

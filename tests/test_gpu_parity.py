@@ -1,0 +1,138 @@
+"""CUDA path against the reference (golden fixtures) and the CPU oracle.
+
+Tolerances:
+* FP64 mode (the parity path): energies within 1e-9 relative, displacements
+  within 1e-6 px of the reference; operators to rounding (<= 1e-13).
+* FP32 mode: operators within single-precision rounding (smooth 1e-6, energy
+  1e-6, DE 1e-5 relative).  Whole registrations in FP32 are NOT held to the
+  1e-3 px / 1e-6 energy tolerance: the reference's own iteration amplifies a
+  1e-9 relative input perturbation to ~1e-5 relative energy after 20 steps
+  (tests/test_gpu_solver.py::test_fp32_registration_within_conditioning).
+"""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.abs(np.asarray(a) - np.asarray(b)).max() / max(1e-300, np.abs(b).max()))
+
+
+@pytest.mark.parametrize("level", [5, 6])
+def test_transfer_and_preparation_exact(gpu, level):
+    g = golden(f"ops_L{level}.npz")
+    assert np.array_equal(gpu.restrict(level, g["smooth_in"]), g["restrict_out"])
+    assert np.array_equal(gpu.prolong(level - 1, g["prolong_in"]), g["prolong_out"])
+    assert np.array_equal(gpu.normalize(g["raw_t"]), g["normalize_out"])
+    assert np.array_equal(gpu.normalize(g["raw_t"], sat=-1, min_to_zero=1), g["normalize_nosat_out"])
+
+
+@pytest.mark.parametrize("level", [5, 6])
+@pytest.mark.parametrize("fp64", [1, 0])
+def test_smoother_vcycle(gpu, level, fp64):
+    g = golden(f"ops_L{level}.npz")
+    for s, out in zip(g["smooth_sigmas"], g["smooth_out"]):
+        got = gpu.smooth(level, s, g["smooth_in"], fp64=fp64)
+        assert rel(got, out) <= (1e-15 if fp64 else 1e-6), s
+
+
+@pytest.mark.parametrize("level", [5, 6])
+@pytest.mark.parametrize("fp64", [1, 0])
+def test_energy_and_variation(gpu, level, fp64):
+    g = golden(f"ops_L{level}.npz")
+    for tag, qx in (("", g["px"]), ("_clip", g["px_clip"])):
+        e, gx, gy = gpu.energy(level, g["R"], g["T"], qx, g["py"], float(g["lam"]), fp64=fp64)
+        ref_e = g["E" + tag][2]
+        assert abs(e - ref_e) / ref_e <= (1e-13 if fp64 else 1e-6)
+        if fp64:
+            assert rel(np.stack([gx, gy]), g["DE" + tag]) <= 1e-13
+        elif tag == "":
+            assert rel(np.stack([gx, gy]), g["DE"]) <= 1e-5
+
+
+@pytest.mark.parametrize("level", [3, 7, 8])
+def test_operators_vs_oracle_other_levels(gpu, oracle, level):
+    from msgpu import synthetic as syn
+    n = (1 << level) + 1
+    rng = np.random.default_rng(level)
+    fr, _, _ = syn.make_series(n, 2, syn.HEX_513, seed=50 + level)
+    R, T = oracle.normalize(fr[0].ravel()), oracle.normalize(fr[1].ravel())
+    px, py = rng.normal(0, 1.0 / (n - 1), n * n), rng.normal(0, 1.0 / (n - 1), n * n)
+    e, gx, gy = gpu.energy(level, R, T, px, py, 0.1, fp64=1)
+    e0, _ = oracle.energy(level, R, T, px, py, 0.1)
+    g0 = oracle.denergy(level, R, T, px, py, 0.1)
+    assert abs(e - e0) / e0 <= 1e-13
+    assert rel(np.stack([gx, gy]), np.stack(g0)) <= 1e-13
+    x = rng.normal(size=n * n)
+    assert rel(gpu.smooth(level, 0.3, x, fp64=1), oracle.smooth(level, 0.3, x)) <= 1e-15
+    assert np.array_equal(gpu.restrict(level, x), oracle.restrict(level, x))
+    xc = rng.normal(size=((1 << (level - 1)) + 1) ** 2)
+    assert np.array_equal(gpu.prolong(level - 1, xc), oracle.prolong(level - 1, xc))
+
+
+@pytest.mark.parametrize("level", [5, 6])
+def test_level_gradient_flow_matches_reference_trace(gpu, level):
+    g = golden(f"gd_L{level}.npz")
+    n = (1 << level) + 1
+    z = np.zeros(n * n)
+    px, py, e, steps, trace = gpu.gd_level(level, g["R"], g["T"], z, z, float(g["lam"]), int(g["max_iter"]), fp64=1)
+    ref = g["trace"][1:]
+    assert steps == int(g["steps"])
+    # identical control decisions: accepted tau, filter width, number of energy evaluations
+    assert np.array_equal(trace[:, 1], ref[:, 2])
+    assert np.array_equal(trace[:, 2], ref[:, 3])
+    assert np.array_equal(trace[:, 3], ref[:, 4])
+    assert np.abs(trace[:, 0] - ref[:, 1]).max() / ref[:, 1].max() <= 1e-9
+    assert abs(e - float(g["energy"])) / float(g["energy"]) <= 1e-9
+    assert max(np.abs(px - g["px"]).max(), np.abs(py - g["py"]).max()) * (n - 1) <= 1e-6
+
+
+def _params(level, **kw):
+    import msgpu
+    p = msgpu.default_params(precision_level=level, input_level=level)
+    for k, v in kw.items():
+        setattr(p, "lambda_" if k == "lam" else k, v)
+    return p
+
+
+def test_multilevel_registration_matches_reference(gpu):
+    g = golden("register_L7.npz")
+    n = (1 << 7) + 1
+    for i in range(3):
+        start, stop, lam, lf, mi, se, rs = g[f"case{i}"]
+        p = _params(7, start_level=int(start), stop_level=int(stop), lam=lam, lambda_factor=lf,
+                    max_gd_iterations=int(mi), stop_epsilon=se, resample_deformation=int(rs), use_fp64=1,
+                    dont_normalize_input=1)
+        phis, en, steps = gpu.register_batch(p, g["R"], g["T"][None])
+        assert max(np.abs(phis[0] - g[f"phi{i}"]).max(), 0) * (n - 1) <= 1e-6, i
+        assert abs(en[0] - g[f"E{i}"][0]) / g[f"E{i}"][0] <= 1e-9, i
+
+
+def test_series_stage_and_average_match_reference(gpu):
+    g = golden("series_L6.npz")
+    level, frames = int(g["level"]), g["frames"]
+    n = (1 << level) + 1
+    p = _params(level, start_level=int(g["start"]), stop_level=level, lam=float(g["lam"]),
+                max_gd_iterations=int(g["max_iter"]), use_fp64=1)
+    phis, en, steps = gpu.register_batch(p, frames[0], frames[1:])
+    assert np.abs(phis - g["phis"][1:]).max() * (n - 1) <= 1e-6
+    assert np.abs(en - g["energies"][1:]).max() / g["energies"][1:].max() <= 1e-9
+    mean, count = gpu.warp_mean(level, frames, g["phis"])
+    assert np.abs(mean - g["mean"]).max() <= 1e-12
+
+
+def test_warp_mean_out_of_domain_and_empty_pixels(gpu, oracle):
+    level = 5
+    n = (1 << level) + 1
+    rng = np.random.default_rng(3)
+    frames = rng.uniform(0, 100, size=(3, n * n))
+    phis = rng.normal(0, 6.0 / (n - 1), size=(3, 2, n * n))
+    phis[:, 0, :n] = 10.0  # whole first row out of the domain in every frame -> no samples
+    m, c = gpu.warp_mean(level, frames, phis)
+    m0, c0 = oracle.warp_mean(level, frames, phis)
+    assert np.array_equal(c, c0) and (c0 == 0).sum() >= n
+    assert np.abs(m - m0).max() <= 1e-12 * np.abs(m0).max()
+    assert np.allclose(m[:n], frames[-1].mean(), rtol=1e-14)
