@@ -32,12 +32,13 @@ struct msgpu_context {
   cudaStream_t stream = nullptr;
   // growable device buffers
   struct Buf { void* p = nullptr; size_t cap = 0; };
-  Buf arena, shared_real, dscratch, small, phis_d, io[6];
+  Buf arena, shared_real, dscratch, small, phis_d, io[6], prof;
   // statistics of the last batch call
   bool profiling = false;
   msgpu_stats stats{};
   cudaEvent_t ev[32] = {};
   bool ev_ready = false;
+  int last_cluster = 0;
 };
 
 namespace {
@@ -296,35 +297,58 @@ __global__ void k_convert(const Src* __restrict__ src, size_t sstride, Dst* dst,
     d[i] = (Dst)s[i];
 }
 
+// Dense n x n images (batch) <-> pitched rows of pitch_of(n) elements.
+template <typename Src, typename Dst>
+__global__ void k_to_pitched(const Src* __restrict__ src, size_t sstride, Dst* dst, size_t dstride, int n) {
+  const Src* s = src + (size_t)blockIdx.y * sstride;
+  Dst* d = dst + (size_t)blockIdx.y * dstride;
+  const int P = pitch_of(n);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n * n; i += gridDim.x * blockDim.x)
+    d[(size_t)(i / n) * P + (i % n)] = (Dst)s[i];
+}
+template <typename Src, typename Dst>
+__global__ void k_from_pitched(const Src* __restrict__ src, size_t sstride, Dst* dst, size_t dstride, int n) {
+  const Src* s = src + (size_t)blockIdx.y * sstride;
+  Dst* d = dst + (size_t)blockIdx.y * dstride;
+  const int P = pitch_of(n);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n * n; i += gridDim.x * blockDim.x)
+    d[i] = (Dst)s[(size_t)(i / n) * P + (i % n)];
+}
+
 // Displacement transfer to the next level for every instance: reads the
 // buffer bin[i], writes buffer bin[i]^1 and records it in bout[i].
 // mode 0: ProlongOp (prolongation.cpp:195-232); mode 1: 1-D resampling of the
 // flattened node vector (vec.h:461-472, 565-570; registration.h:510-516).
 template <typename Real>
-__global__ void k_phi_up(Real* arena, size_t inst_stride, size_t off0, size_t off1, size_t comp_stride_src,
-                         size_t comp_stride_dst, int coarse_level, const int* bin, int* bout, int mode) {
+__global__ void k_phi_up(Real* arena, size_t inst_stride, size_t off0, size_t off1, int coarse_level,
+                         const int* bin, int* bout, int mode) {
   const int inst = blockIdx.y;
   const int b = bin[inst];
   Real* base = arena + (size_t)inst * inst_stride;
   const Real* src = base + (b ? off1 : off0);
   Real* dst = base + (b ? off0 : off1);
   const int cw = lvl_n(coarse_level), fw = lvl_n(coarse_level + 1);
+  const int cP = pitch_of(cw), fP = pitch_of(fw);
+  const size_t cs_src = comp_stride(coarse_level), cs_dst = comp_stride(coarse_level + 1);
   const int ns = cw * cw, nd = fw * fw;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nd; i += gridDim.x * blockDim.x) {
+    const int x = i % fw, y = i / fw;
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
-      const Real* s = src + (size_t)c * comp_stride_src;
+      const Real* s = src + (size_t)c * cs_src;
       Real v;
       if (mode == 0) {
-        v = prolong_node<Real>(i % fw, i / fw, [&](int x, int y) { return s[(size_t)y * cw + x]; });
+        v = prolong_node<Real>(x, y, [&](int X, int Y) { return s[(size_t)Y * cP + X]; });
       } else {
+        // dense (flattened) node index of the coarse vector
+        auto at = [&](int q) { return s[(size_t)(q / cw) * cP + (q % cw)]; };
         const double sc = (ns - 1) / (double)(nd - 1);
         const double pos = i * sc;
         const int p = (int)pos;
         const double pf = pos - p;
-        v = (p == ns - 1) ? s[p] : (Real)((1 - pf) * (double)s[p] + pf * (double)s[p + 1]);
+        v = (p == ns - 1) ? at(p) : (Real)((1 - pf) * (double)at(p) + pf * (double)at(p + 1));
       }
-      dst[(size_t)c * comp_stride_dst + i] = v;
+      dst[(size_t)c * cs_dst + (size_t)y * fP + x] = v;
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) bout[inst] = b ^ 1;
@@ -335,16 +359,20 @@ __global__ void k_set_buf(int* buf, int n, int v) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) buf[i] = v;
 }
 
-// phi of every instance at the given level -> double output (F x 2 x N).
+// phi of every instance at the given level -> double output (F x 2 x N, dense).
 template <typename Real>
-__global__ void k_phi_out(const Real* arena, size_t inst_stride, size_t off0, size_t off1, size_t comp_stride,
-                          const int* buf, int N, double* out) {
+__global__ void k_phi_out(const Real* arena, size_t inst_stride, size_t off0, size_t off1, int level,
+                          const int* buf, double* out) {
   const int inst = blockIdx.y;
+  const int n = lvl_n(level), P = pitch_of(n);
+  const int N = n * n;
+  const size_t cs = comp_stride(level);
   const Real* src = arena + (size_t)inst * inst_stride + (buf[inst] ? off1 : off0);
   double* o = out + (size_t)inst * 2 * N;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-    o[i] = (double)src[i];
-    o[N + i] = (double)src[comp_stride + i];
+    const size_t g = (size_t)(i / n) * P + (i % n);
+    o[i] = (double)src[g];
+    o[N + i] = (double)src[cs + g];
   }
 }
 
@@ -429,18 +457,18 @@ Layout make_layout(int M) {
   Layout L;
   size_t off = 0;
   const size_t a = 64;
-  for (int l = 0; l <= M; ++l) { L.off_T[l] = off; off = align_up(off + lvl_N(l), a); }
+  for (int l = 0; l <= M; ++l) { L.off_T[l] = off; off = align_up(off + comp_stride(l), a); }
   for (int l = M + 1; l <= kMaxLevel; ++l) L.off_T[l] = 0;
-  const size_t two = 2 * lvl_N(M);
+  const size_t two = 2 * comp_stride(M);
   for (int b = 0; b < 2; ++b) { L.off_phi[b] = off; off = align_up(off + two, a); }
   for (int b = 0; b < 2; ++b) { L.off_d[b] = off; off = align_up(off + two, a); }
   L.off_s = off; off = align_up(off + two, a);
   L.off_de = off; off = align_up(off + two, a);
   for (int k = 0; k <= kMaxLevel; ++k) {
     if (k <= M) {
-      L.off_x2[k] = off; off = align_up(off + 2 * lvl_N(k), a);
-      L.off_x5[k] = off; off = align_up(off + 2 * lvl_N(k), a);
-      L.off_b[k] = off; off = align_up(off + 2 * lvl_N(k), a);
+      L.off_x2[k] = off; off = align_up(off + 2 * comp_stride(k), a);
+      L.off_x5[k] = off; off = align_up(off + 2 * comp_stride(k), a);
+      L.off_b[k] = off; off = align_up(off + 2 * comp_stride(k), a);
     } else {
       L.off_x2[k] = L.off_x5[k] = L.off_b[k] = 0;
     }
@@ -451,27 +479,26 @@ Layout make_layout(int M) {
 
 template <typename Real>
 size_t level_smem_bytes(int lc) {
-  size_t s = std::max(sizeof(GradShared<Real>), std::max(sizeof(DownShared<Real>), sizeof(UpShared<Real>)));
-  s = std::max(s, coarse_smem_elems<Real>(lc) * sizeof(Real));
-  return align_up(s, 16);
+  return align_up(level_smem_elems(lc) * sizeof(Real), 128);
 }
 
 template <typename Real>
 int pick_lc(int level) {
-  const int cap = (sizeof(Real) == 4) ? 5 : 4;
-  return std::min(level, cap);
+  return std::min(level, 5);
 }
 
-// Cluster size: enough CTAs per instance to fill the GPU, at most one CTA per
-// 16k nodes of the level and at most 16 (non-portable cluster size).
-int pick_cluster(int sms, int num_inst, int level) {
+// Largest useful cluster size of a level: one CTA per 2k nodes, at most 16
+// (the non-portable maximum).
+int max_cluster_for_level(int level) {
   const size_t N = lvl_N(level);
-  int g_nodes = (int)std::max<size_t>(1, N / 16384);
-  int g_fill = std::max(1, (2 * sms) / std::max(1, num_inst));
-  int g = std::min(16, std::min(g_nodes, g_fill));
-  int p = 1;
-  while (p * 2 <= g) p *= 2;
-  return p;
+  return (int)std::min<size_t>(16, std::max<size_t>(1, N / 2048));
+}
+
+// About two CTAs per SM over all instances, so that no cluster has CTAs
+// sharing an SM while others run alone (every cluster waits for its slowest CTA).
+int pick_cluster(int sms, int num_inst, int level) {
+  const int fill = std::max(1, (2 * sms) / std::max(1, num_inst));
+  return std::max(1, std::min(max_cluster_for_level(level), fill));
 }
 
 template <typename Real>
@@ -479,11 +506,12 @@ int launch_level(msgpu_context* ctx, LevelArgs<Real>& a, int G, cudaStream_t st)
   const size_t smem = level_smem_bytes<Real>(a.lc);
   CK(cudaFuncSetAttribute(level_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   CK(cudaFuncSetAttribute(level_kernel<Real>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-  for (;;) {
+  int best_g = 0, best_c = 0;
+  for (int g = G; g >= 1; --g) {
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = G;
+    attr[0].val.clusterDim.x = g;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.blockDim = dim3(kThreads, 1, 1);
@@ -491,17 +519,32 @@ int launch_level(msgpu_context* ctx, LevelArgs<Real>& a, int G, cudaStream_t st)
     cfg.stream = st;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cfg.gridDim = dim3(G * std::max(1, a.num_inst), 1, 1);
+    cfg.gridDim = dim3(g * std::max(1, a.num_inst), 1, 1);
     int max_clusters = 0;
     cudaError_t e = cudaOccupancyMaxActiveClusters(&max_clusters, level_kernel<Real>, &cfg);
-    if (e != cudaSuccess || max_clusters < 1) {
-      (void)cudaGetLastError();
-      if (G > 1) { G >>= 1; continue; }
-      return fail(ctx, MSGPU_ERR_CUDA, "level kernel cannot be resident (smem %zu B): %s", smem,
-                  cudaGetErrorString(e));
-    }
-    const int nclusters = std::min(a.num_inst, max_clusters);
-    cfg.gridDim = dim3(G * nclusters, 1, 1);
+    if (e != cudaSuccess) { (void)cudaGetLastError(); continue; }
+    if (max_clusters < 1) continue;
+    if (best_g == 0) { best_g = g; best_c = max_clusters; }
+    if (max_clusters >= a.num_inst) { best_g = g; best_c = max_clusters; break; }
+  }
+  if (best_g == 0)
+    return fail(ctx, MSGPU_ERR_CUDA, "level kernel cannot be resident (smem %zu B)", smem);
+  {
+    const int g = best_g;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = g;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(kThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const int nclusters = std::min(a.num_inst, best_c);
+    cfg.gridDim = dim3(g * nclusters, 1, 1);
+    ctx->last_cluster = g;
     CK(cudaLaunchKernelEx(&cfg, level_kernel<Real>, a));
     return MSGPU_OK;
   }
@@ -534,7 +577,7 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
   const size_t small_bytes = sizeof(double) * (2 * nimg + 2 * F + 64) + sizeof(int) * ((2 * nlev_all + 4) * F + 64);
   if ((rc = ensure(ctx, ctx->dscratch, sizeof(double) * pstride * nimg))) return rc;
   if ((rc = ensure(ctx, ctx->arena, sizeof(Real) * L.stride * F))) return rc;
-  if ((rc = ensure(ctx, ctx->shared_real, sizeof(Real) * (L.off_T[M] + lvl_N(M) + 64)))) return rc;
+  if ((rc = ensure(ctx, ctx->shared_real, sizeof(Real) * (L.off_T[M] + comp_stride(M) + 64)))) return rc;
   if ((rc = ensure(ctx, ctx->small, small_bytes))) return rc;
   double* pyr = (double*)ctx->dscratch.p;
   Real* arena = (Real*)ctx->arena.p;
@@ -587,9 +630,9 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
   for (int l = 0; l <= M; ++l) {
     const size_t Nl = lvl_N(l);
     const unsigned gx = (unsigned)std::min<size_t>(1024, (Nl + 255) / 256);
-    k_convert<double, Real><<<dim3(gx, 1), 256, 0, st>>>(pyr + poff[l], 0, Rpyr + L.off_T[l], 0, Nl);
-    k_convert<double, Real><<<dim3(gx, F), 256, 0, st>>>(pyr + pstride + poff[l], pstride, arena + L.off_T[l],
-                                                          L.stride, Nl);
+    k_to_pitched<double, Real><<<dim3(gx, 1), 256, 0, st>>>(pyr + poff[l], 0, Rpyr + L.off_T[l], 0, lvl_n(l));
+    k_to_pitched<double, Real><<<dim3(gx, F), 256, 0, st>>>(pyr + pstride + poff[l], pstride, arena + L.off_T[l],
+                                                             L.stride, lvl_n(l));
     launches += 2;
   }
   CK(cudaGetLastError());
@@ -611,11 +654,13 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
           k_restrict<double><<<dim3((unsigned)std::min<size_t>(1024, (cN + 255) / 256), F), 256, 0, st>>>(
               tmp + poff[l], pstride, tmp + poff[l - 1], pstride, l);
         }
-        k_convert<double, Real><<<dim3((unsigned)std::min<size_t>(1024, (Ns + 255) / 256), F), 256, 0, st>>>(
-            tmp + poff[start], pstride, arena + L.off_phi[0] + (size_t)c * Ns, L.stride, Ns);
+        k_to_pitched<double, Real><<<dim3((unsigned)std::min<size_t>(1024, (Ns + 255) / 256), F), 256, 0, st>>>(
+            tmp + poff[start], pstride, arena + L.off_phi[0] + (size_t)c * comp_stride(start), L.stride,
+            lvl_n(start));
       }
     } else {
-      CK(cudaMemset2DAsync(arena + L.off_phi[0], L.stride * sizeof(Real), 0, 2 * Ns * sizeof(Real), F, st));
+      CK(cudaMemset2DAsync(arena + L.off_phi[0], L.stride * sizeof(Real), 0, 2 * comp_stride(start) * sizeof(Real),
+                           F, st));
     }
   }
   CK(cudaGetLastError());
@@ -651,8 +696,15 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
     a.out_evals = evals_all + (size_t)(l - start) * F;
     a.out_phi_buf = bin;   // the level kernel updates the buffer index in place
     const int G = pick_cluster(ctx->sm_count, F, l);
+    const size_t prof_n = (size_t)16 * F * kPassKinds;
+    if (ctx->profiling) {
+      if ((rc = ensure(ctx, ctx->prof, sizeof(unsigned long long) * prof_n * nlev_all))) return rc;
+      a.pass_cycles = (unsigned long long*)ctx->prof.p + prof_n * (l - start);
+      CK(cudaMemsetAsync(a.pass_cycles, 0, sizeof(unsigned long long) * prof_n, st));
+    }
     if (ctx->profiling && l - start < 16) CK(cudaEventRecord(ctx->ev[2 * (l - start)], st));
     if ((rc = launch_level<Real>(ctx, a, G, st))) return rc;
+    if (l - start < 16) ctx->stats.level_cluster[l - start] = ctx->last_cluster;
     if (ctx->profiling && l - start < 16) CK(cudaEventRecord(ctx->ev[2 * (l - start) + 1], st));
     k_collect<<<1, 256, 0, st>>>(e_lvl, a.out_steps, F, (l == stop) ? io.energies_out : nullptr, io.steps_out,
                                  nlev, l - start);
@@ -661,8 +713,7 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
     if (l < stop) {
       const size_t fw = lvl_N(l + 1);
       k_phi_up<Real><<<dim3((unsigned)std::min<size_t>(1024, (fw + 255) / 256), F), 256, 0, st>>>(
-          arena, L.stride, L.off_phi[0], L.off_phi[1], lvl_N(l), lvl_N(l + 1), l, bin, bout,
-          p.resample_deformation ? 1 : 0);
+          arena, L.stride, L.off_phi[0], L.off_phi[1], l, bin, bout, p.resample_deformation ? 1 : 0);
       CK(cudaGetLastError());
       ++launches;
       std::swap(bin, bout);
@@ -671,15 +722,14 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
   for (int l = stop; l < M; ++l) {
     const size_t fw = lvl_N(l + 1);
     k_phi_up<Real><<<dim3((unsigned)std::min<size_t>(1024, (fw + 255) / 256), F), 256, 0, st>>>(
-        arena, L.stride, L.off_phi[0], L.off_phi[1], lvl_N(l), lvl_N(l + 1), l, bin, bout,
-        p.resample_deformation ? 1 : 0);
+        arena, L.stride, L.off_phi[0], L.off_phi[1], l, bin, bout, p.resample_deformation ? 1 : 0);
     CK(cudaGetLastError());
     ++launches;
     std::swap(bin, bout);
   }
   const int NM = (int)lvl_N(M);
   k_phi_out<Real><<<dim3((unsigned)std::min(1024, (NM + 255) / 256), F), 256, 0, st>>>(
-      arena, L.stride, L.off_phi[0], L.off_phi[1], (size_t)NM, bin, NM, io.phis_out);
+      arena, L.stride, L.off_phi[0], L.off_phi[1], M, bin, io.phis_out);
   CK(cudaGetLastError());
   ++launches;
   if (ctx->profiling) {
@@ -695,6 +745,20 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
       for (int f = 0; f < F; ++f) { ss += hs[(size_t)k * F + f]; ee += he[(size_t)k * F + f]; }
       ctx->stats.level_steps[k] = ss;
       ctx->stats.level_evals[k] = ee;
+    }
+    const size_t prof_n = (size_t)16 * F * kPassKinds;
+    std::vector<unsigned long long> pc(prof_n);
+    for (int k = 0; k < nlev_all && k < 16; ++k) {
+      CK(cudaMemcpy(pc.data(), (unsigned long long*)ctx->prof.p + prof_n * k, sizeof(unsigned long long) * prof_n,
+                    cudaMemcpyDeviceToHost));
+      const int G = ctx->stats.level_cluster[k];
+      const int nctas = G * std::min(F, 16 * F / std::max(1, G));  // upper bound on CTAs launched
+      for (int q = 0; q < kPassKinds && q < 8; ++q) {
+        unsigned long long mx = 0;
+        for (int c = 0; c < nctas && (size_t)c * kPassKinds + q < prof_n; ++c)
+          mx = std::max(mx, pc[(size_t)c * kPassKinds + q]);
+        ctx->stats.level_pass_cycles[k][q] = (long long)mx;
+      }
     }
   }
   return MSGPU_OK;
@@ -962,7 +1026,7 @@ int single_level(msgpu_context* ctx, int level, int mode, const double* R, const
   const Layout L = make_layout(level);
   const size_t N = lvl_N(level);
   if ((rc = ensure(ctx, ctx->arena, sizeof(Real) * L.stride))) return rc;
-  if ((rc = ensure(ctx, ctx->shared_real, sizeof(Real) * (N + 64)))) return rc;
+  if ((rc = ensure(ctx, ctx->shared_real, sizeof(Real) * (comp_stride(level) + 64)))) return rc;
   if ((rc = ensure(ctx, ctx->io[0], sizeof(double) * 6 * N))) return rc;
   const size_t trace_n = (size_t)std::max(1, max_trace) * 4;
   if ((rc = ensure(ctx, ctx->small, sizeof(double) * (8 + trace_n) + 64))) return rc;
@@ -979,11 +1043,13 @@ int single_level(msgpu_context* ctx, int level, int mode, const double* R, const
   for (int k = 0; k < 5; ++k)
     if (srcs[k]) CK(cudaMemcpyAsync(h + k * N, srcs[k], sizeof(double) * N, cudaMemcpyHostToDevice, st));
   const unsigned gx = (unsigned)std::min<size_t>(1024, (N + 255) / 256);
-  if (R) k_convert<double, Real><<<gx, 256, 0, st>>>(h, 0, Rd, 0, N);
-  if (T) k_convert<double, Real><<<gx, 256, 0, st>>>(h + N, 0, arena + L.off_T[level], 0, N);
-  if (phix) k_convert<double, Real><<<gx, 256, 0, st>>>(h + 2 * N, 0, arena + L.off_phi[0], 0, N);
-  if (phiy) k_convert<double, Real><<<gx, 256, 0, st>>>(h + 3 * N, 0, arena + L.off_phi[0] + N, 0, N);
-  if (de_in) k_convert<double, Real><<<gx, 256, 0, st>>>(h + 4 * N, 0, arena + L.off_de, 0, N);
+  const int nl = lvl_n(level);
+  const size_t cs = comp_stride(level);
+  if (R) k_to_pitched<double, Real><<<gx, 256, 0, st>>>(h, 0, Rd, 0, nl);
+  if (T) k_to_pitched<double, Real><<<gx, 256, 0, st>>>(h + N, 0, arena + L.off_T[level], 0, nl);
+  if (phix) k_to_pitched<double, Real><<<gx, 256, 0, st>>>(h + 2 * N, 0, arena + L.off_phi[0], 0, nl);
+  if (phiy) k_to_pitched<double, Real><<<gx, 256, 0, st>>>(h + 3 * N, 0, arena + L.off_phi[0] + cs, 0, nl);
+  if (de_in) k_to_pitched<double, Real><<<gx, 256, 0, st>>>(h + 4 * N, 0, arena + L.off_de, 0, nl);
   k_set_buf<Real><<<1, 32, 0, st>>>(d_i + 1, 1, 0);
   CK(cudaGetLastError());
   LevelArgs<Real> a;
@@ -1026,7 +1092,7 @@ int single_level(msgpu_context* ctx, int level, int mode, const double* R, const
   if (energy_out) *energy_out = he;
   if (steps_out) *steps_out = hi[0];
   auto fetch = [&](size_t off, double* dst) -> int {
-    k_convert<Real, double><<<gx, 256, 0, st>>>(arena + off, 0, h + 5 * N, 0, N);
+    k_from_pitched<Real, double><<<gx, 256, 0, st>>>(arena + off, 0, h + 5 * N, 0, nl);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(dst, h + 5 * N, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -1038,11 +1104,11 @@ int single_level(msgpu_context* ctx, int level, int mode, const double* R, const
   }
   if (de_out) {
     if ((rc = fetch(L.off_de, de_out))) return rc;
-    if ((rc = fetch(L.off_de + N, de_out + N))) return rc;
+    if ((rc = fetch(L.off_de + cs, de_out + N))) return rc;
   }
   const size_t phioff = hi[1] ? L.off_phi[1] : L.off_phi[0];
   if (phix_out && (rc = fetch(phioff, phix_out))) return rc;
-  if (phiy_out && (rc = fetch(phioff + N, phiy_out))) return rc;
+  if (phiy_out && (rc = fetch(phioff + cs, phiy_out))) return rc;
   if (trace && max_trace > 0) {
     const int rows = std::min(hi[0], max_trace);
     CK(cudaMemcpy(trace, d_trace, sizeof(double) * 4 * rows, cudaMemcpyDeviceToHost));

@@ -75,7 +75,8 @@ __device__ __forceinline__ void clip_axis(Real coord, int n, Real h, int& el, Re
     coord = Real(width) - RealTraits<Real>::eps();
     inside = false;
   }
-  const Real sc = coord / h;
+  // coord / h with h = 2^-l, written as the exactly equal product with 2^l
+  const Real sc = coord * Real(n - 1);
   int e = (short)sc;
   Real l = sc - Real(e);
   if (e == n - 1 && fabs((double)(l - Real(0))) < 1e-15) {
@@ -111,25 +112,27 @@ __device__ __forceinline__ Real q1_value(const Real t[4], Real x, Real y) {
 }
 
 // DiscreteFunctionDefault::evaluateGradient (discreteFunction.h:259-269),
-// basis derivatives baseFunctionSet.h:131-139, divided by h.
+// basis derivatives baseFunctionSet.h:131-139, divided by h.  h = 2^-l, so the
+// division is the exactly equal product with inv_h = 2^l.
 template <typename Real>
-__device__ __forceinline__ void q1_grad(const Real t[4], Real x, Real y, Real h, Real& gx, Real& gy) {
+__device__ __forceinline__ void q1_grad(const Real t[4], Real x, Real y, Real inv_h, Real& gx, Real& gy) {
   gx = Real(0);
   gy = Real(0);
   Real vx, vy;
-  vx = (y - Real(1)) / h; vy = (x - Real(1)) / h; vx *= t[0]; vy *= t[0]; gx += vx; gy += vy;
-  vx = (Real(1) - y) / h; vy = (-x) / h;          vx *= t[1]; vy *= t[1]; gx += vx; gy += vy;
-  vx = (-y) / h;          vy = (Real(1) - x) / h; vx *= t[2]; vy *= t[2]; gx += vx; gy += vy;
-  vx = y / h;             vy = x / h;             vx *= t[3]; vy *= t[3]; gx += vx; gy += vy;
+  vx = (y - Real(1)) * inv_h; vy = (x - Real(1)) * inv_h; vx *= t[0]; vy *= t[0]; gx += vx; gy += vy;
+  vx = (Real(1) - y) * inv_h; vy = (-x) * inv_h;          vx *= t[1]; vy *= t[1]; gx += vx; gy += vy;
+  vx = (-y) * inv_h;          vy = (Real(1) - x) * inv_h; vx *= t[2]; vy *= t[2]; gx += vx; gy += vy;
+  vx = y * inv_h;             vy = x * inv_h;             vx *= t[3]; vy *= t[3]; gx += vx; gy += vy;
 }
 
+// The 4 texels of element (ex, ey) of an image with row pitch P.
 template <typename Real>
-__device__ __forceinline__ void load_texels(const Real* __restrict__ T, int n, int ex, int ey, Real t[4]) {
-  const Real* p = T + (size_t)ey * n + ex;
+__device__ __forceinline__ void load_texels(const Real* __restrict__ T, int P, int ex, int ey, Real t[4]) {
+  const Real* p = T + (size_t)ey * P + ex;
   t[0] = __ldg(p);
   t[1] = __ldg(p + 1);
-  t[2] = __ldg(p + n);
-  t[3] = __ldg(p + n + 1);
+  t[2] = __ldg(p + P);
+  t[3] = __ldg(p + P + 1);
 }
 
 // SSDEnergy integrand summed over the element's 4 quadrature points and
@@ -137,7 +140,7 @@ __device__ __forceinline__ void load_texels(const Real* __restrict__ T, int n, i
 // FEOpInterface.h:2598-2610).  p[c][b] are the nodal displacements of
 // component c, r[b] the nodal reference values.
 template <typename Real>
-__device__ __forceinline__ Real element_ssd(const Real* __restrict__ T, int n, Real h, int ex, int ey,
+__device__ __forceinline__ Real element_ssd(const Real* __restrict__ T, int n, int P, Real h, int ex, int ey,
                                             const Real px[4], const Real py[4], const Real r[4]) {
   Real a = Real(0);
 #pragma unroll
@@ -146,7 +149,7 @@ __device__ __forceinline__ Real element_ssd(const Real* __restrict__ T, int n, R
     const Real oy = at_quad(py, q);
     const Warped<Real> w = warp_quad_point(ex, ey, q, ox, oy, n, h);
     Real t[4];
-    load_texels(T, n, w.ex, w.ey, t);
+    load_texels(T, P, w.ex, w.ey, t);
     const Real tv = q1_value(t, w.lx, w.ly);
     const Real rv = at_quad(r, q);
     const Real d = tv - rv;
@@ -160,7 +163,7 @@ __device__ __forceinline__ Real element_ssd(const Real* __restrict__ T, int n, R
 // against the 4 basis functions (registration.h:1648-1666,
 // FEOpInterface.h:1821-1848): out[b][c] = vol * sum_q nl[q][c] * bq[b][q] * w.
 template <typename Real>
-__device__ __forceinline__ void element_force(const Real* __restrict__ T, int n, Real h, int ex, int ey,
+__device__ __forceinline__ void element_force(const Real* __restrict__ T, int n, int P, Real h, int ex, int ey,
                                               const Real px[4], const Real py[4], const Real r[4],
                                               Real out[4][2]) {
   Real nl[4][2];
@@ -170,11 +173,11 @@ __device__ __forceinline__ void element_force(const Real* __restrict__ T, int n,
     const Real oy = at_quad(py, q);
     const Warped<Real> w = warp_quad_point(ex, ey, q, ox, oy, n, h);
     Real t[4];
-    load_texels(T, n, w.ex, w.ey, t);
+    load_texels(T, P, w.ex, w.ey, t);
     const Real td = q1_value(t, w.lx, w.ly);
     const Real rv = at_quad(r, q);
     Real gx, gy;
-    q1_grad(t, w.lx, w.ly, h, gx, gy);
+    q1_grad(t, w.lx, w.ly, Real(n - 1), gx, gy);
     nl[q][0] = w.inx ? gx * (td - rv) : Real(0);
     nl[q][1] = w.iny ? gy * (td - rv) : Real(0);
   }

@@ -3,9 +3,9 @@
 // Each registration instance (a template frame registered to the reference on
 // one level of the multilevel pyramid) is owned by one thread-block cluster.
 // The CTAs of the cluster split every data-parallel pass over the level's
-// nodes/elements, synchronise with the hardware cluster barrier, and reduce
-// their partial sums through distributed shared memory in a fixed rank order,
-// so every CTA holds identical scalars and takes identical control decisions.
+// node tiles, synchronise with the hardware cluster barrier, and reduce their
+// partial sums through distributed shared memory in a fixed rank order, so
+// every CTA holds identical scalars and takes identical control decisions.
 // The whole gradient flow of the level -- H1 metric V-cycle, Fletcher-Reeves
 // NCG, Armijo line search, filter-width (sigma) schedule and stopping rule --
 // runs on the device without host round trips:
@@ -15,7 +15,14 @@
 //   getTimestepWidthWithArmijoLineSearch        ArmijoSearch.h:118-200
 //   LinearSmoothOp::apply / MDMultigrid::solve  linearSmoothOp.cpp:451-612
 // Control flow is bounded: the step loop by max_iter, each line search by the
-// tau range [2^-30, 2^25].  No CTA waits on anything but the cluster barrier.
+// tau range [2^-30, 2^25].  No CTA waits on anything but the cluster barrier
+// and its own asynchronous copies.
+//
+// Every pass is a double-buffered tile pipeline: while a CTA computes one
+// 64 x 4 node tile from shared memory, cp.async streams the windows (tile plus
+// halo) of the next tile from HBM/L2 into the other buffer.  Rows are pitched
+// to a multiple of 4 elements so that every window row is a sequence of
+// aligned 16-byte chunks.
 #pragma once
 
 #include <cooperative_groups.h>
@@ -30,6 +37,20 @@ constexpr int kThreads = 256;
 constexpr int kMaxLevel = 12;
 constexpr int kRedSlots = 4;   // partial sums reduced per pass
 
+// Node tiles: [x0, x0+TX) x [y0, y0+TY); the last tile of a row/column also
+// owns the final node (n-1 = 2^l is a multiple of the tile size for l >= 6).
+constexpr int TX = 64, TY = 4;
+// Windows of the element passes: nodes [x0-4, x0+68) x [y0-1, y0+6).
+constexpr int EWX = 72, EWY = 7, EWIN = EWX * EWY;
+// Multigrid passes use taller tiles of VTX x VTY nodes (halo 3 around them):
+// windows of nodes [x0-4, x0+36) x [y0-3, y0+20).
+constexpr int VTX = 32, VTY = 16;
+constexpr int VWX = 40, VWY = 23, VWIN = VWX * VWY;
+// Coarse window of the correction pass: coarse nodes [x0/2-4, x0/2+20) x [y0/2-2, y0/2+11).
+constexpr int CWX = 24, CWY = 13, CWIN = CWX * CWY;
+// Element contributions of the gradient pass: elements [x0-1, x0+65) x [y0-1, y0+5).
+constexpr int GCX = 66, GCY = 6;
+
 // Launch modes of the level kernel.
 enum LevelMode : int {
   MODE_SOLVE = 0,   // full gradient flow on the level
@@ -37,11 +58,13 @@ enum LevelMode : int {
   MODE_SMOOTH = 2,  // one H1 V-cycle of the DE buffer's negation (parity)
 };
 
+__host__ __device__ inline int pitch_of(int n) { return (n + 3) & ~3; }
+
 template <typename Real>
 struct LevelArgs {
   Real* arena;              // per-instance arenas, instance i at arena + i*inst_stride
   size_t inst_stride;
-  const Real* R;            // reference image on this level (shared by all instances)
+  const Real* R;            // reference image on this level (shared by all instances), pitched
   size_t off_T;             // template image on this level
   size_t off_phi[2];        // displacement ping-pong buffers (2 components each)
   size_t off_d[2];          // descent-direction ping-pong buffers (2 components each)
@@ -61,6 +84,32 @@ struct LevelArgs {
   int* out_phi_buf;         // per instance: buffer holding the result
   double* trace;            // optional: per instance max_trace rows of (energy, tau, sigma, evals)
   int max_trace;
+  unsigned long long* pass_cycles;  // optional: per CTA kPassKinds clock64 totals
+};
+
+// A 2-component array of level k occupies 2 * comp_stride(k) elements.
+__host__ __device__ inline size_t comp_stride(int level) {
+  const size_t n = (size_t)(1 << level) + 1;
+  return n * (size_t)pitch_of((int)n);
+}
+
+// Pass kinds of the per-pass cycle counters.
+enum PassKind : int { PK_ENERGY0 = 0, PK_GRAD, PK_VDOWN, PK_VCOARSE, PK_VUP, PK_NCG, PK_ENERGY, PK_REDUCE, kPassKinds };
+
+#define MSG_TIMED(pt, kind, ...) \
+  do {                                \
+    (pt).start();                     \
+    __VA_ARGS__;                      \
+    (pt).stop(kind);                  \
+  } while (0)
+
+struct PassTimer {
+  unsigned long long* acc;
+  long long t0;
+  __device__ void start() { if (acc) t0 = clock64(); }
+  __device__ void stop(int kind) {
+    if (acc && threadIdx.x == 0) acc[kind] += (unsigned long long)(clock64() - t0);
+  }
 };
 
 // ---------------------------------------------------------------------------
@@ -111,338 +160,510 @@ __device__ __forceinline__ void cluster_barrier(cg::cluster_group& cluster) {
 }
 
 // ---------------------------------------------------------------------------
+// Asynchronous window copies (cp.async, 16-byte chunks, zero fill outside).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int sz = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Copies nodes [wx0, wx0+WW) x [wy0, wy0+WH) of a pitched array (rows of P
+// elements, P a multiple of 4) into sm (row stride WW).  wx0 and WW are
+// multiples of 4, so every chunk is either fully inside a row (possibly in
+// its padding, which is never read) or fully outside and zero-filled.
+template <typename Real>
+__device__ __forceinline__ void load_window(Real* sm, const Real* g, int n, int P, int wx0, int wy0, int WW,
+                                            int WH) {
+  constexpr int C = 16 / (int)sizeof(Real);
+  const int cpr = WW / C;
+  for (int i = threadIdx.x; i < cpr * WH; i += kThreads) {
+    const int cx = i % cpr, wy = i / cpr;
+    const int x = wx0 + cx * C, y = wy0 + wy;
+    const bool ok = (y >= 0 && y < n && x >= 0 && x < P);
+    const Real* src = ok ? g + (size_t)y * P + x : g;
+    cp_async16(sm + wy * WW + cx * C, src, ok);
+  }
+}
+
+// Double-buffered tile loop: ps.issue(t, stage) starts the copies of tile t,
+// ps.compute(t, stage) consumes them.
+template <class Pass>
+__device__ __forceinline__ void tile_pipeline(Pass& ps, int ntiles, int rank, int G) {
+  int stage = 0;
+  if (rank < ntiles) ps.issue(rank, 0);
+  cp_async_commit();
+  for (int t = rank; t < ntiles; t += G) {
+    const int tn = t + G;
+    if (tn < ntiles) ps.issue(tn, stage ^ 1);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    ps.compute(t, stage);
+    __syncthreads();
+    stage ^= 1;
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+}
+
+// Tile geometry of a level with n nodes per side and tiles of tx x ty nodes;
+// the last tile of a row/column also owns the final node.
+struct Tiles {
+  int n, tw, th, nx, ny;
+  __device__ Tiles(int n_, int tw_ = TX, int th_ = TY) : n(n_), tw(tw_), th(th_) {
+    nx = (n - 1) / tw;
+    if (nx < 1) nx = 1;
+    ny = (n - 1) / th;
+    if (ny < 1) ny = 1;
+  }
+  __device__ int count() const { return nx * ny; }
+  __device__ void rect(int t, int& x0, int& x1, int& y0, int& y1) const {
+    const int tx = t % nx, ty = t / nx;
+    x0 = tx * tw;
+    y0 = ty * th;
+    x1 = (tx == nx - 1) ? n : x0 + tw;
+    y1 = (ty == ny - 1) ? n : y0 + th;
+  }
+};
+
+// ---------------------------------------------------------------------------
 template <typename Real>
 struct Inst {
   Real* base;
   const Real* R;
   const Real* T;
-  int n;
+  int n, P;
   Real h;
   __device__ Real* arr(size_t off) const { return base + off; }
 };
 
-// Energy pass over the elements owned by this CTA.
+// Energy pass.
 //   kind 0: E_data at phi (no direction)            -> part[0]
-//            plus A = phi . L phi at owned nodes     -> part[1]
+//            A = phi . L phi over the owned nodes    -> part[1]
 //   kind 1: E_data at phi + tau d                   -> part[0]
-//   kind 2: NCG materialisation d = s + beta od (or d = s when od_zero),
+//   kind 2: NCG materialisation d = s + beta od (d = s when od_zero),
 //           E_data at phi + tau d                   -> part[0]
 //           Df = DE . d, B = phi . L d, C = d . L d -> part[1..3]
+// Windows (EWX x EWY, origin (x0-4, y0-1)) per stage, in this order:
+//   kind 0: phx phy R ; kind 1: phx phy dx dy R ; kind 2: phx phy sx sy odx ody dex dey R
 template <typename Real>
-__device__ void pass_energy(const Inst<Real>& I, int kind, Real tau, Real beta, bool od_zero,
-                            const Real* __restrict__ phx, const Real* __restrict__ phy,
-                            const Real* dx, const Real* dy,        // kind 1: d; kind 2: od
-                            const Real* sx, const Real* sy,        // kind 2: s
-                            Real* wdx, Real* wdy,                  // kind 2: output d
-                            const Real* dex, const Real* dey,      // kind 2: DE
-                            int rank, int G, double part[kRedSlots]) {
-  const int n = I.n, ne = n - 1;
-  const long total = (long)ne * ne;
-  auto dval = [&](const Real* a, const Real* s, int idx) -> Real {
-    // direction value at node idx for the current kind
-    if (kind == 1) return a[idx];
-    if (od_zero) return s[idx];
-    return s[idx] + beta * a[idx];
-  };
-  for (long e = (long)rank * kThreads + threadIdx.x; e < total; e += (long)G * kThreads) {
-    const int ex = (int)(e % ne), ey = (int)(e / ne);
-    const int i0 = ey * n + ex;
-    const int idx[4] = {i0, i0 + 1, i0 + n, i0 + n + 1};
-    Real px[4], py[4], r[4];
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      r[b] = __ldg(I.R + idx[b]);
-      if (kind == 0) {
-        px[b] = phx[idx[b]];
-        py[b] = phy[idx[b]];
-      } else {
-        // newPosition = phi + tau * d (gradientDescent.h:176-178)
-        Real vx = phx[idx[b]], vy = phy[idx[b]];
-        vx += tau * dval(dx, sx, idx[b]);
-        vy += tau * dval(dy, sy, idx[b]);
-        px[b] = vx;
-        py[b] = vy;
-      }
-    }
-    part[0] += (double)element_ssd(I.T, n, I.h, ex, ey, px, py, r);
+struct EnergyPass {
+  Inst<Real> I;
+  int kind;
+  Real tau, beta;
+  bool od_zero;
+  const Real *phx, *phy, *dx, *dy, *sx, *sy, *dex, *dey;
+  Real *wdx, *wdy;
+  Real* sm;
+  int nwin;
+  double* part;
+  Tiles tl;
 
-    if (kind == 0 || kind == 2) {
-      // nodes owned by this element: its lower-left node, plus the last
-      // column / row of nodes for the elements on the upper boundaries.
-      int own[4];
-      int nown = 0;
-      own[nown++] = i0;
-      if (ex == ne - 1) own[nown++] = i0 + 1;
-      if (ey == ne - 1) own[nown++] = i0 + n;
-      if (ex == ne - 1 && ey == ne - 1) own[nown++] = i0 + n + 1;
-      for (int k = 0; k < nown; ++k) {
-        const int id = own[k];
-        const int x = id % n, y = id / n;
+  __device__ EnergyPass(const Inst<Real>& I_, int kind_, Real tau_, Real beta_, bool odz, const Real* phx_,
+                        const Real* phy_, const Real* dx_, const Real* dy_, const Real* sx_, const Real* sy_,
+                        const Real* dex_, const Real* dey_, Real* wdx_, Real* wdy_, Real* sm_, double* part_)
+      : I(I_), kind(kind_), tau(tau_), beta(beta_), od_zero(odz), phx(phx_), phy(phy_), dx(dx_), dy(dy_),
+        sx(sx_), sy(sy_), dex(dex_), dey(dey_), wdx(wdx_), wdy(wdy_), sm(sm_), part(part_), tl(I_.n) {
+    nwin = (kind == 0) ? 3 : (kind == 1 ? 5 : 9);
+  }
+  __device__ Real* win(int stage, int k) const { return sm + ((size_t)stage * nwin + k) * EWIN; }
+
+  __device__ void issue(int t, int stage) {
+    int x0, x1, y0, y1;
+    tl.rect(t, x0, x1, y0, y1);
+    const int wx0 = x0 - 4, wy0 = y0 - 1, n = I.n, P = I.P;
+    int k = 0;
+    load_window(win(stage, k++), phx, n, P, wx0, wy0, EWX, EWY);
+    load_window(win(stage, k++), phy, n, P, wx0, wy0, EWX, EWY);
+    if (kind == 1) {
+      load_window(win(stage, k++), dx, n, P, wx0, wy0, EWX, EWY);
+      load_window(win(stage, k++), dy, n, P, wx0, wy0, EWX, EWY);
+    } else if (kind == 2) {
+      load_window(win(stage, k++), sx, n, P, wx0, wy0, EWX, EWY);
+      load_window(win(stage, k++), sy, n, P, wx0, wy0, EWX, EWY);
+      if (!od_zero) {
+        load_window(win(stage, k), dx, n, P, wx0, wy0, EWX, EWY);
+        load_window(win(stage, k + 1), dy, n, P, wx0, wy0, EWX, EWY);
+      }
+      k += 2;
+      load_window(win(stage, k++), dex, n, P, wx0, wy0, EWX, EWY);
+      load_window(win(stage, k++), dey, n, P, wx0, wy0, EWX, EWY);
+    }
+    load_window(win(stage, k), I.R, n, P, wx0, wy0, EWX, EWY);
+  }
+
+  __device__ void compute(int t, int stage) {
+    int x0, x1, y0, y1;
+    tl.rect(t, x0, x1, y0, y1);
+    const int n = I.n;
+    const Real* Wpx = win(stage, 0);
+    const Real* Wpy = win(stage, 1);
+    const Real* Wr = win(stage, nwin - 1);
+    const Real* Wa = (kind != 0) ? win(stage, 2) : nullptr;   // d (kind 1) or s (kind 2)
+    const Real* Wb = (kind != 0) ? win(stage, 3) : nullptr;
+    const Real* Wox = (kind == 2) ? win(stage, 4) : nullptr;  // od
+    const Real* Woy = (kind == 2) ? win(stage, 5) : nullptr;
+    const Real* Wdx = (kind == 2) ? win(stage, 6) : nullptr;  // DE
+    const Real* Wdy = (kind == 2) ? win(stage, 7) : nullptr;
+    auto at = [&](int x, int y) { return (y - (y0 - 1)) * EWX + (x - (x0 - 4)); };
+    // direction at a window position
+    auto dirx = [&](int i) -> Real {
+      if (kind == 1) return Wa[i];
+      if (od_zero) return Wa[i];
+      return Wa[i] + beta * Wox[i];
+    };
+    auto diry = [&](int i) -> Real {
+      if (kind == 1) return Wb[i];
+      if (od_zero) return Wb[i];
+      return Wb[i] + beta * Woy[i];
+    };
+    // elements owned by the tile
+    const int ex1 = (x1 < n - 1) ? x1 : n - 1, ey1 = (y1 < n - 1) ? y1 : n - 1;
+    const int ew = ex1 - x0, eh = ey1 - y0;
+    for (int i = threadIdx.x; i < ew * eh; i += kThreads) {
+      const int ex = x0 + i % ew, ey = y0 + i / ew;
+      const int c0 = at(ex, ey);
+      const int idx[4] = {c0, c0 + 1, c0 + EWX, c0 + EWX + 1};
+      Real px[4], py[4], r[4];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        r[b] = Wr[idx[b]];
         if (kind == 0) {
-          const Real lx = stiff_row<Real>(x, y, n, [&](int X, int Y) { return phx[Y * n + X]; });
-          const Real ly = stiff_row<Real>(x, y, n, [&](int X, int Y) { return phy[Y * n + X]; });
-          part[1] += (double)phx[id] * (double)lx + (double)phy[id] * (double)ly;
+          px[b] = Wpx[idx[b]];
+          py[b] = Wpy[idx[b]];
         } else {
-          const Real ddx = dval(dx, sx, id), ddy = dval(dy, sy, id);
-          wdx[id] = ddx;
-          wdy[id] = ddy;
-          const Real lx = stiff_row<Real>(x, y, n, [&](int X, int Y) { return dval(dx, sx, Y * n + X); });
-          const Real ly = stiff_row<Real>(x, y, n, [&](int X, int Y) { return dval(dy, sy, Y * n + X); });
-          part[1] += (double)dex[id] * (double)ddx + (double)dey[id] * (double)ddy;
-          part[2] += (double)phx[id] * (double)lx + (double)phy[id] * (double)ly;
-          part[3] += (double)ddx * (double)lx + (double)ddy * (double)ly;
+          // newPosition = phi + tau * d (gradientDescent.h:176-178)
+          Real vx = Wpx[idx[b]], vy = Wpy[idx[b]];
+          vx += tau * dirx(idx[b]);
+          vy += tau * diry(idx[b]);
+          px[b] = vx;
+          py[b] = vy;
         }
+      }
+      part[0] += (double)element_ssd(I.T, n, I.P, I.h, ex, ey, px, py, r);
+    }
+    if (kind == 1) return;
+    // owned nodes
+    const int nw = x1 - x0, nh = y1 - y0;
+    for (int i = threadIdx.x; i < nw * nh; i += kThreads) {
+      const int x = x0 + i % nw, y = y0 + i / nw;
+      const int c = at(x, y);
+      if (kind == 0) {
+        const Real lx = stiff_row<Real>(x, y, n, [&](int X, int Y) { return Wpx[at(X, Y)]; });
+        const Real ly = stiff_row<Real>(x, y, n, [&](int X, int Y) { return Wpy[at(X, Y)]; });
+        part[1] += (double)Wpx[c] * (double)lx + (double)Wpy[c] * (double)ly;
+      } else {
+        const Real ddx = dirx(c), ddy = diry(c);
+        const size_t g = (size_t)y * I.P + x;
+        wdx[g] = ddx;
+        wdy[g] = ddy;
+        const Real lx = stiff_row<Real>(x, y, n, [&](int X, int Y) { return dirx(at(X, Y)); });
+        const Real ly = stiff_row<Real>(x, y, n, [&](int X, int Y) { return diry(at(X, Y)); });
+        part[1] += (double)Wdx[c] * (double)ddx + (double)Wdy[c] * (double)ddy;
+        part[2] += (double)Wpx[c] * (double)lx + (double)Wpy[c] * (double)ly;
+        part[3] += (double)ddx * (double)lx + (double)ddy * (double)ly;
       }
     }
   }
-}
-
-// Gradient pass: applies the pending update phi_new = phi + tau_p d (or copies
-// phi when no step is pending), evaluates DE(phi_new) = SSDForce + lambda L phi
-// (LinCombOp, registration.h:977-982) and A = phi_new . L phi_new -> part[1].
-// Node tiles of 32 x 8 with the element contributions staged in shared memory;
-// node sums are accumulated in the reference's element order (x fastest).
-constexpr int GTX = 32, GTY = 8;
-template <typename Real>
-struct GradShared {
-  Real pw[2][GTY + 2][GTX + 2];   // phi_new window, nodes [x0-1, x0+GTX] x [y0-1, y0+GTY]
-  Real rw[GTY + 2][GTX + 2];      // reference window
-  Real c[GTY + 1][GTX + 1][4][2]; // element contributions, elements [x0-1, x0+GTX) x [y0-1, y0+GTY)
 };
 
+// Gradient pass: applies the pending update phi_new = phi + tau_p d (or keeps
+// phi), evaluates DE(phi_new) = SSDForce + lambda L phi_new (LinCombOp,
+// registration.h:977-982) and A = phi_new . L phi_new -> part[1].  Element
+// contributions are staged in shared memory and summed per node in the
+// reference's element order (x fastest).
+// Windows (EWX x EWY, origin (x0-4, y0-1)): phx phy dx dy R; plus GCY x GCX x 8
+// contributions.
 template <typename Real>
-__device__ void pass_gradient(const Inst<Real>& I, GradShared<Real>& S, bool step, Real tau_p,
-                              const Real* phx, const Real* phy, const Real* dx, const Real* dy,
-                              Real* nphx, Real* nphy, Real* dex, Real* dey, double lambda,
-                              int rank, int G, double part[kRedSlots]) {
-  const int n = I.n, ne = n - 1;
-  const int tx_n = (n + GTX - 1) / GTX, ty_n = (n + GTY - 1) / GTY;
-  const int tiles = tx_n * ty_n;
-  const Real lam = (Real)lambda;
-  for (int t = rank; t < tiles; t += G) {
-    const int x0 = (t % tx_n) * GTX, y0 = (t / tx_n) * GTY;
-    // 1. windows of phi_new and R
-    for (int k = threadIdx.x; k < (GTY + 2) * (GTX + 2); k += kThreads) {
-      const int wx = k % (GTX + 2), wy = k / (GTX + 2);
-      const int x = x0 - 1 + wx, y = y0 - 1 + wy;
-      Real vx = Real(0), vy = Real(0), rv = Real(0);
-      if (x >= 0 && x < n && y >= 0 && y < n) {
-        const int id = y * n + x;
-        vx = phx[id];
-        vy = phy[id];
-        if (step) {  // Dest += tau * d (gradientDescent.h:385-387, descentDir *= tau)
-          vx += tau_p * dx[id];
-          vy += tau_p * dy[id];
-        }
-        rv = __ldg(I.R + id);
-      }
-      S.pw[0][wy][wx] = vx;
-      S.pw[1][wy][wx] = vy;
-      S.rw[wy][wx] = rv;
+struct GradPass {
+  Inst<Real> I;
+  bool step;
+  Real tau_p;
+  double lambda;
+  const Real *phx, *phy, *dx, *dy;
+  Real *nphx, *nphy, *dex, *dey;
+  Real* sm;
+  double* part;
+  Tiles tl;
+  static constexpr int kWin = 5;
+
+  __device__ GradPass(const Inst<Real>& I_, bool step_, Real tau_p_, double lam, const Real* phx_, const Real* phy_,
+                      const Real* dx_, const Real* dy_, Real* nphx_, Real* nphy_, Real* dex_, Real* dey_, Real* sm_,
+                      double* part_)
+      : I(I_), step(step_), tau_p(tau_p_), lambda(lam), phx(phx_), phy(phy_), dx(dx_), dy(dy_), nphx(nphx_),
+        nphy(nphy_), dex(dex_), dey(dey_), sm(sm_), part(part_), tl(I_.n) {}
+  __device__ Real* win(int stage, int k) const { return sm + ((size_t)stage * kWin + k) * EWIN; }
+  __device__ Real* contrib() const { return sm + (size_t)2 * kWin * EWIN; }
+
+  __device__ void issue(int t, int stage) {
+    int x0, x1, y0, y1;
+    tl.rect(t, x0, x1, y0, y1);
+    const int wx0 = x0 - 4, wy0 = y0 - 1, n = I.n, P = I.P;
+    load_window(win(stage, 0), phx, n, P, wx0, wy0, EWX, EWY);
+    load_window(win(stage, 1), phy, n, P, wx0, wy0, EWX, EWY);
+    if (step) {
+      load_window(win(stage, 2), dx, n, P, wx0, wy0, EWX, EWY);
+      load_window(win(stage, 3), dy, n, P, wx0, wy0, EWX, EWY);
     }
-    __syncthreads();
-    // 2. element contributions
-    for (int k = threadIdx.x; k < (GTY + 1) * (GTX + 1); k += kThreads) {
-      const int cx = k % (GTX + 1), cy = k / (GTX + 1);
-      const int ex = x0 - 1 + cx, ey = y0 - 1 + cy;
-      if (ex < 0 || ey < 0 || ex >= ne || ey >= ne) continue;
-      Real px[4], py[4], r[4];
-      // window coordinates of node (ex, ey) are (cx, cy)
-      px[0] = S.pw[0][cy][cx];     py[0] = S.pw[1][cy][cx];     r[0] = S.rw[cy][cx];
-      px[1] = S.pw[0][cy][cx + 1]; py[1] = S.pw[1][cy][cx + 1]; r[1] = S.rw[cy][cx + 1];
-      px[2] = S.pw[0][cy + 1][cx]; py[2] = S.pw[1][cy + 1][cx]; r[2] = S.rw[cy + 1][cx];
-      px[3] = S.pw[0][cy + 1][cx + 1]; py[3] = S.pw[1][cy + 1][cx + 1]; r[3] = S.rw[cy + 1][cx + 1];
-      element_force(I.T, n, I.h, ex, ey, px, py, r, S.c[cy][cx]);
-    }
-    __syncthreads();
-    // 3. node sums, stiffness, outputs
-    {
-      const int lx = threadIdx.x % GTX, ly = threadIdx.x / GTX;
-      const int x = x0 + lx, y = y0 + ly;
-      if (x < n && y < n) {
-        // window/contribution index of element (x-1+a, y-1+b) is (lx+a, ly+b)
-        Real fx = Real(0), fy = Real(0);
-        if (x - 1 >= 0 && y - 1 >= 0) { fx += S.c[ly][lx][3][0];     fy += S.c[ly][lx][3][1]; }
-        if (x < ne && y - 1 >= 0)     { fx += S.c[ly][lx + 1][2][0]; fy += S.c[ly][lx + 1][2][1]; }
-        if (x - 1 >= 0 && y < ne)     { fx += S.c[ly + 1][lx][1][0]; fy += S.c[ly + 1][lx][1][1]; }
-        if (x < ne && y < ne)         { fx += S.c[ly + 1][lx + 1][0][0]; fy += S.c[ly + 1][lx + 1][0][1]; }
-        const Real Lx = stiff_row<Real>(x, y, n, [&](int X, int Y) { return S.pw[0][Y - y0 + 1][X - x0 + 1]; });
-        const Real Ly = stiff_row<Real>(x, y, n, [&](int X, int Y) { return S.pw[1][Y - y0 + 1][X - x0 + 1]; });
-        const Real gx = (lambda != 1.0) ? fx + lam * Lx : fx + Lx;
-        const Real gy = (lambda != 1.0) ? fy + lam * Ly : fy + Ly;
-        const int id = y * n + x;
-        dex[id] = gx;
-        dey[id] = gy;
-        const Real vx = S.pw[0][ly + 1][lx + 1], vy = S.pw[1][ly + 1][lx + 1];
-        nphx[id] = vx;
-        nphy[id] = vy;
-        part[1] += (double)vx * (double)Lx + (double)vy * (double)Ly;
-      }
-    }
-    __syncthreads();
+    load_window(win(stage, 4), I.R, n, P, wx0, wy0, EWX, EWY);
   }
-}
+
+  __device__ void compute(int t, int stage) {
+    int x0, x1, y0, y1;
+    tl.rect(t, x0, x1, y0, y1);
+    const int n = I.n, ne = n - 1;
+    Real* Wpx = win(stage, 0);
+    Real* Wpy = win(stage, 1);
+    const Real* Wdx = win(stage, 2);
+    const Real* Wdy = win(stage, 3);
+    const Real* Wr = win(stage, 4);
+    auto at = [&](int x, int y) { return (y - (y0 - 1)) * EWX + (x - (x0 - 4)); };
+    // 1. phi_new in the windows: Dest += tau * d (gradientDescent.h:385-387)
+    if (step) {
+      for (int i = threadIdx.x; i < EWIN; i += kThreads) {
+        Real vx = Wpx[i], vy = Wpy[i];
+        vx += tau_p * Wdx[i];
+        vy += tau_p * Wdy[i];
+        Wpx[i] = vx;
+        Wpy[i] = vy;
+      }
+      __syncthreads();
+    }
+    // 2. element contributions, elements [x0-1, x1) x [y0-1, y1) that exist
+    Real* C = contrib();
+    const int cw = (x1 < ne ? x1 : ne) - (x0 - 1), ch = (y1 < ne ? y1 : ne) - (y0 - 1);
+    for (int i = threadIdx.x; i < cw * ch; i += kThreads) {
+      const int ex = x0 - 1 + i % cw, ey = y0 - 1 + i / cw;
+      if (ex < 0 || ey < 0) continue;
+      const int c0 = at(ex, ey);
+      const int idx[4] = {c0, c0 + 1, c0 + EWX, c0 + EWX + 1};
+      Real px[4], py[4], r[4];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        px[b] = Wpx[idx[b]];
+        py[b] = Wpy[idx[b]];
+        r[b] = Wr[idx[b]];
+      }
+      Real out[4][2];
+      element_force(I.T, n, I.P, I.h, ex, ey, px, py, r, out);
+      Real* cc = C + ((size_t)(ey - (y0 - 1)) * GCX + (ex - (x0 - 1))) * 8;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        cc[2 * b] = out[b][0];
+        cc[2 * b + 1] = out[b][1];
+      }
+    }
+    __syncthreads();
+    // 3. node sums in element order, stiffness, outputs
+    const Real lam = (Real)lambda;
+    const int nw = x1 - x0, nh = y1 - y0;
+    for (int i = threadIdx.x; i < nw * nh; i += kThreads) {
+      const int x = x0 + i % nw, y = y0 + i / nw;
+      auto cc = [&](int ex, int ey, int b, int comp) {
+        return C[((size_t)(ey - (y0 - 1)) * GCX + (ex - (x0 - 1))) * 8 + 2 * b + comp];
+      };
+      Real fx = Real(0), fy = Real(0);
+      if (x - 1 >= 0 && y - 1 >= 0) { fx += cc(x - 1, y - 1, 3, 0); fy += cc(x - 1, y - 1, 3, 1); }
+      if (x < ne && y - 1 >= 0)     { fx += cc(x, y - 1, 2, 0);     fy += cc(x, y - 1, 2, 1); }
+      if (x - 1 >= 0 && y < ne)     { fx += cc(x - 1, y, 1, 0);     fy += cc(x - 1, y, 1, 1); }
+      if (x < ne && y < ne)         { fx += cc(x, y, 0, 0);         fy += cc(x, y, 0, 1); }
+      const Real Lx = stiff_row<Real>(x, y, n, [&](int X, int Y) { return Wpx[at(X, Y)]; });
+      const Real Ly = stiff_row<Real>(x, y, n, [&](int X, int Y) { return Wpy[at(X, Y)]; });
+      const Real gx = (lambda != 1.0) ? fx + lam * Lx : fx + Lx;
+      const Real gy = (lambda != 1.0) ? fy + lam * Ly : fy + Ly;
+      const size_t g = (size_t)y * I.P + x;
+      dex[g] = gx;
+      dey[g] = gy;
+      const Real vx = Wpx[at(x, y)], vy = Wpy[at(x, y)];
+      nphx[g] = vx;
+      nphy[g] = vy;
+      part[1] += (double)vx * (double)Lx + (double)vy * (double)Ly;
+    }
+  }
+};
 
 // ---------------------------------------------------------------------------
 // Multigrid V-cycle passes on the levels above lc (cluster passes).
-constexpr int VTX = 32, VTY = 16;
-template <typename Real>
-struct DownShared {
-  Real rhs[2][VTY + 6][VTX + 6];  // halo 3
-  Real x1[2][VTY + 6][VTX + 6];   // halo 3
-  Real x2[2][VTY + 4][VTX + 4];   // halo 2
-  Real r[2][VTY + 2][VTX + 2];    // halo 1
-};
-template <typename Real>
-struct UpShared {
-  Real rhs[2][VTY + 4][VTX + 4];  // halo 2
-  Real x3[2][VTY + 4][VTX + 4];   // halo 2
-  Real x4[2][VTY + 2][VTX + 2];   // halo 1
-};
 
 // Pre-smoothing (2 Jacobi sweeps from x = 0), residual and restriction
 // (MDMultigrid::solve steps 1-3, linearSmoothOp.cpp:465-477).
-// rhs of level k: -DE on the finest level (negate), else b[k].
+// rhs = sgn * window (sgn = -1 turns DE into the descent direction).
+// Staged windows (VWX x VWY, origin (x0-4, y0-3)): rhs_x rhs_y; work: x2[2] r[2] x1[2].
 template <typename Real>
-__device__ void pass_down(int k, int n, const Real* rhsx, const Real* rhsy, bool negate, Real* x2x, Real* x2y,
-                          Real* bcx, Real* bcy, Real hsq, Real diag, DownShared<Real>& S, int rank, int G) {
-  const int cw = (n >> 1) + 1;
-  const int tx_n = (n + VTX - 1) / VTX, ty_n = (n + VTY - 1) / VTY;
-  const int tiles = tx_n * ty_n;
-  for (int t = rank; t < tiles; t += G) {
-    const int x0 = (t % tx_n) * VTX, y0 = (t / tx_n) * VTY;
-    // rhs and x1 = 0 + (rhs - A 0)/diag on halo 3
-    for (int q = threadIdx.x; q < (VTY + 6) * (VTX + 6); q += kThreads) {
-      const int wx = q % (VTX + 6), wy = q / (VTX + 6);
-      const int x = x0 - 3 + wx, y = y0 - 3 + wy;
-      Real a = Real(0), b = Real(0);
-      if (x >= 0 && x < n && y >= 0 && y < n) {
-        const int id = y * n + x;
-        a = rhsx[id];
-        b = rhsy[id];
-        if (negate) { a = a * Real(-1); b = b * Real(-1); }
-      }
-      S.rhs[0][wy][wx] = a;
-      S.rhs[1][wy][wx] = b;
-      S.x1[0][wy][wx] = jacobi_update(Real(0), a, Real(0), diag);
-      S.x1[1][wy][wx] = jacobi_update(Real(0), b, Real(0), diag);
-    }
-    __syncthreads();
-    // x2 on halo 2
-    for (int q = threadIdx.x; q < (VTY + 4) * (VTX + 4); q += kThreads) {
-      const int wx = q % (VTX + 4), wy = q / (VTX + 4);
-      const int x = x0 - 2 + wx, y = y0 - 2 + wy;
-      if (x < 0 || x >= n || y < 0 || y >= n) continue;
-#pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        auto A = [&](int X, int Y) { return S.x1[c][Y - y0 + 3][X - x0 + 3]; };
-        const Real ax = heat_row<Real>(x, y, n, hsq, A);
-        S.x2[c][wy][wx] = jacobi_update(S.x1[c][wy + 1][wx + 1], S.rhs[c][wy + 1][wx + 1], ax, diag);
-      }
-    }
-    __syncthreads();
-    // residual on halo 1, and x2 out for owned nodes
-    for (int q = threadIdx.x; q < (VTY + 2) * (VTX + 2); q += kThreads) {
-      const int wx = q % (VTX + 2), wy = q / (VTX + 2);
-      const int x = x0 - 1 + wx, y = y0 - 1 + wy;
-      if (x < 0 || x >= n || y < 0 || y >= n) continue;
-#pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        auto A = [&](int X, int Y) { return S.x2[c][Y - y0 + 2][X - x0 + 2]; };
-        const Real ax = heat_row<Real>(x, y, n, hsq, A);
-        S.r[c][wy][wx] = S.rhs[c][wy + 2][wx + 2] - ax;
-      }
-      if (wx >= 1 && wx <= VTX && wy >= 1 && wy <= VTY) {
-        const int id = y * n + x;
-        x2x[id] = S.x2[0][wy + 1][wx + 1];
-        x2y[id] = S.x2[1][wy + 1][wx + 1];
-      }
-    }
-    __syncthreads();
-    // restriction of the residual to the coarse nodes centred in this tile
-    for (int q = threadIdx.x; q < (VTY / 2) * (VTX / 2); q += kThreads) {
-      const int X = (x0 >> 1) + q % (VTX / 2), Y = (y0 >> 1) + q / (VTX / 2);
-      if (X >= cw || Y >= cw) continue;
-#pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        auto F = [&](int x, int y) { return S.r[c][y - y0 + 1][x - x0 + 1]; };
-        const Real v = restrict_node<Real>(X, Y, cw, F);
-        (c == 0 ? bcx : bcy)[Y * cw + X] = v;
-      }
-    }
-    __syncthreads();
+struct DownPass {
+  int n, P, cw, cP;
+  const Real *rx, *ry;
+  Real sgn;
+  Real *x2x, *x2y, *bcx, *bcy;
+  Real hsq, diag;
+  Real* sm;
+  Tiles tl;
+  __device__ DownPass(int n_, const Real* rx_, const Real* ry_, Real sgn_, Real* x2x_, Real* x2y_, Real* bcx_,
+                      Real* bcy_, Real hsq_, Real diag_, Real* sm_)
+      : n(n_), P(pitch_of(n_)), cw((n_ >> 1) + 1), cP(pitch_of((n_ >> 1) + 1)), rx(rx_), ry(ry_), sgn(sgn_),
+        x2x(x2x_), x2y(x2y_), bcx(bcx_), bcy(bcy_), hsq(hsq_), diag(diag_), sm(sm_), tl(n_, VTX, VTY) {}
+  __device__ Real* rhs(int stage, int c) const { return sm + ((size_t)stage * 2 + c) * VWIN; }
+  __device__ Real* work(int k, int c) const { return sm + ((size_t)4 + 2 * k + c) * VWIN; }
+
+  __device__ void issue(int t, int stage) {
+    int x0, x1, y0, y1;
+    tl.rect(t, x0, x1, y0, y1);
+    load_window(rhs(stage, 0), rx, n, P, x0 - 4, y0 - 3, VWX, VWY);
+    load_window(rhs(stage, 1), ry, n, P, x0 - 4, y0 - 3, VWX, VWY);
   }
-}
+
+  __device__ void compute(int t, int stage) {
+    int x0, x1, y0, y1;
+    tl.rect(t, x0, x1, y0, y1);
+    auto at = [&](int x, int y) { return (y - (y0 - 3)) * VWX + (x - (x0 - 4)); };
+    // rhs sign and x1 = 0 + (rhs - A 0)/diag on the whole window (one division per node)
+    for (int i = threadIdx.x; i < 2 * VWIN; i += kThreads) {
+      const int c = i / VWIN, j = i % VWIN;
+      const Real r = rhs(stage, c)[j] * sgn;
+      rhs(stage, c)[j] = r;
+      work(2, c)[j] = jacobi_update(Real(0), r, Real(0), diag);
+    }
+    __syncthreads();
+    // x2 on nodes [x0-2, x1+2) x [y0-2, y1+2)
+    {
+      const int ax0 = max(x0 - 2, 0), ax1 = min(x1 + 2, n), ay0 = max(y0 - 2, 0), ay1 = min(y1 + 2, n);
+      const int w = ax1 - ax0, h = ay1 - ay0;
+      for (int i = threadIdx.x; i < 2 * w * h; i += kThreads) {
+        const int c = i / (w * h), j = i % (w * h);
+        const int x = ax0 + j % w, y = ay0 + j / w;
+        const Real* X1 = work(2, c);
+        const Real ax = heat_row<Real>(x, y, n, hsq, [&](int a, int b) { return X1[at(a, b)]; });
+        work(0, c)[at(x, y)] = jacobi_update(X1[at(x, y)], rhs(stage, c)[at(x, y)], ax, diag);
+      }
+    }
+    __syncthreads();
+    // residual on nodes [x0-1, x1+1) x [y0-1, y1+1); x2 out for owned nodes
+    {
+      const int ax0 = max(x0 - 1, 0), ax1 = min(x1 + 1, n), ay0 = max(y0 - 1, 0), ay1 = min(y1 + 1, n);
+      const int w = ax1 - ax0, h = ay1 - ay0;
+      for (int i = threadIdx.x; i < 2 * w * h; i += kThreads) {
+        const int c = i / (w * h), j = i % (w * h);
+        const int x = ax0 + j % w, y = ay0 + j / w;
+        const Real* X2 = work(0, c);
+        const Real ax = heat_row<Real>(x, y, n, hsq, [&](int a, int b) { return X2[at(a, b)]; });
+        work(1, c)[at(x, y)] = rhs(stage, c)[at(x, y)] - ax;
+        if (x >= x0 && x < x1 && y >= y0 && y < y1) (c == 0 ? x2x : x2y)[(size_t)y * P + x] = X2[at(x, y)];
+      }
+    }
+    __syncthreads();
+    // restriction to the coarse nodes centred in the tile
+    {
+      const int X0 = x0 >> 1, X1 = (x1 + 1) >> 1, Y0 = y0 >> 1, Y1 = (y1 + 1) >> 1;
+      const int w = X1 - X0, h = Y1 - Y0;
+      for (int i = threadIdx.x; i < 2 * w * h; i += kThreads) {
+        const int c = i / (w * h), j = i % (w * h);
+        const int X = X0 + j % w, Y = Y0 + j / w;
+        const Real* Rs = work(1, c);
+        const Real v = restrict_node<Real>(X, Y, cw, [&](int x, int y) { return Rs[at(x, y)]; });
+        (c == 0 ? bcx : bcy)[(size_t)Y * cP + X] = v;
+      }
+    }
+  }
+};
 
 // Correction and post-smoothing (MDMultigrid::solve steps 5-6,
 // linearSmoothOp.cpp:483-493): x3 = x2 + P x_coarse, then 2 Jacobi sweeps.
-// With want_norm, accumulates |x5|^2 into part[0].
+// Staged windows: rhs_x rhs_y x2_x x2_y (VWX x VWY, origin (x0-4, y0-3)) and
+// xc_x xc_y (CWX x CWY, origin (x0/2-4, y0/2-2)); work: x4[2].  x0/2 is a
+// multiple of 16, so the coarse window starts on a 16-byte boundary.
 template <typename Real>
-__device__ void pass_up(int k, int n, const Real* rhsx, const Real* rhsy, bool negate, const Real* x2x,
-                        const Real* x2y, const Real* xcx, const Real* xcy, Real* ox, Real* oy, Real hsq,
-                        Real diag, UpShared<Real>& S, int rank, int G, bool want_norm, double part[kRedSlots]) {
-  const int cw = (n >> 1) + 1;
-  const int tx_n = (n + VTX - 1) / VTX, ty_n = (n + VTY - 1) / VTY;
-  const int tiles = tx_n * ty_n;
-  for (int t = rank; t < tiles; t += G) {
-    const int x0 = (t % tx_n) * VTX, y0 = (t / tx_n) * VTY;
-    for (int q = threadIdx.x; q < (VTY + 4) * (VTX + 4); q += kThreads) {
-      const int wx = q % (VTX + 4), wy = q / (VTX + 4);
-      const int x = x0 - 2 + wx, y = y0 - 2 + wy;
-      Real a = Real(0), b = Real(0), u = Real(0), v = Real(0);
-      if (x >= 0 && x < n && y >= 0 && y < n) {
-        const int id = y * n + x;
-        a = rhsx[id];
-        b = rhsy[id];
-        if (negate) { a = a * Real(-1); b = b * Real(-1); }
-        const Real px = prolong_node<Real>(x, y, [&](int X, int Y) { return xcx[Y * cw + X]; });
-        const Real py = prolong_node<Real>(x, y, [&](int X, int Y) { return xcy[Y * cw + X]; });
-        u = x2x[id] + px;
-        v = x2y[id] + py;
-      }
-      S.rhs[0][wy][wx] = a;
-      S.rhs[1][wy][wx] = b;
-      S.x3[0][wy][wx] = u;
-      S.x3[1][wy][wx] = v;
-    }
-    __syncthreads();
-    for (int q = threadIdx.x; q < (VTY + 2) * (VTX + 2); q += kThreads) {
-      const int wx = q % (VTX + 2), wy = q / (VTX + 2);
-      const int x = x0 - 1 + wx, y = y0 - 1 + wy;
-      if (x < 0 || x >= n || y < 0 || y >= n) continue;
-#pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        auto A = [&](int X, int Y) { return S.x3[c][Y - y0 + 2][X - x0 + 2]; };
-        const Real ax = heat_row<Real>(x, y, n, hsq, A);
-        S.x4[c][wy][wx] = jacobi_update(S.x3[c][wy + 1][wx + 1], S.rhs[c][wy + 1][wx + 1], ax, diag);
-      }
-    }
-    __syncthreads();
-    for (int q = threadIdx.x; q < VTY * VTX; q += kThreads) {
-      const int wx = q % VTX, wy = q / VTX;
-      const int x = x0 + wx, y = y0 + wy;
-      if (x >= n || y >= n) continue;
-      Real out[2];
-#pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        auto A = [&](int X, int Y) { return S.x4[c][Y - y0 + 1][X - x0 + 1]; };
-        const Real ax = heat_row<Real>(x, y, n, hsq, A);
-        out[c] = jacobi_update(S.x4[c][wy + 1][wx + 1], S.rhs[c][wy + 2][wx + 2], ax, diag);
-      }
-      const int id = y * n + x;
-      ox[id] = out[0];
-      oy[id] = out[1];
-      if (want_norm) part[0] += (double)out[0] * (double)out[0] + (double)out[1] * (double)out[1];
-    }
-    __syncthreads();
+struct UpPass {
+  int n, P, cw, cP;
+  const Real *rx, *ry, *x2x, *x2y, *xcx, *xcy;
+  Real sgn;
+  Real *ox, *oy;
+  Real hsq, diag;
+  Real* sm;
+  bool want_norm;
+  double* part;
+  Tiles tl;
+  static constexpr size_t kStage = 4 * VWIN + 2 * CWIN;
+  __device__ UpPass(int n_, const Real* rx_, const Real* ry_, Real sgn_, const Real* x2x_, const Real* x2y_,
+                    const Real* xcx_, const Real* xcy_, Real* ox_, Real* oy_, Real hsq_, Real diag_, Real* sm_,
+                    bool wn, double* part_)
+      : n(n_), P(pitch_of(n_)), cw((n_ >> 1) + 1), cP(pitch_of((n_ >> 1) + 1)), rx(rx_), ry(ry_), x2x(x2x_),
+        x2y(x2y_), xcx(xcx_), xcy(xcy_), sgn(sgn_), ox(ox_), oy(oy_), hsq(hsq_), diag(diag_), sm(sm_),
+        want_norm(wn), part(part_), tl(n_, VTX, VTY) {}
+  __device__ Real* rhs(int stage, int c) const { return sm + stage * kStage + (size_t)c * VWIN; }
+  __device__ Real* x2(int stage, int c) const { return sm + stage * kStage + (size_t)(2 + c) * VWIN; }
+  __device__ Real* xc(int stage, int c) const { return sm + stage * kStage + 4 * VWIN + (size_t)c * CWIN; }
+  __device__ Real* x4(int c) const { return sm + 2 * kStage + (size_t)c * VWIN; }
+
+  __device__ void issue(int t, int stage) {
+    int x0, x1, y0, y1;
+    tl.rect(t, x0, x1, y0, y1);
+    load_window(rhs(stage, 0), rx, n, P, x0 - 4, y0 - 3, VWX, VWY);
+    load_window(rhs(stage, 1), ry, n, P, x0 - 4, y0 - 3, VWX, VWY);
+    load_window(x2(stage, 0), x2x, n, P, x0 - 4, y0 - 3, VWX, VWY);
+    load_window(x2(stage, 1), x2y, n, P, x0 - 4, y0 - 3, VWX, VWY);
+    load_window(xc(stage, 0), xcx, cw, cP, (x0 >> 1) - 4, (y0 >> 1) - 2, CWX, CWY);
+    load_window(xc(stage, 1), xcy, cw, cP, (x0 >> 1) - 4, (y0 >> 1) - 2, CWX, CWY);
   }
-}
+
+  __device__ void compute(int t, int stage) {
+    int x0, x1, y0, y1;
+    tl.rect(t, x0, x1, y0, y1);
+    auto at = [&](int x, int y) { return (y - (y0 - 3)) * VWX + (x - (x0 - 4)); };
+    auto atc = [&](int X, int Y) { return (Y - ((y0 >> 1) - 2)) * CWX + (X - ((x0 >> 1) - 4)); };
+    // x3 = x2 + P xc in place on nodes [x0-2, x1+2) x [y0-2, y1+2)
+    {
+      const int ax0 = max(x0 - 2, 0), ax1 = min(x1 + 2, n), ay0 = max(y0 - 2, 0), ay1 = min(y1 + 2, n);
+      const int w = ax1 - ax0, h = ay1 - ay0;
+      for (int i = threadIdx.x; i < 2 * w * h; i += kThreads) {
+        const int c = i / (w * h), j = i % (w * h);
+        const int x = ax0 + j % w, y = ay0 + j / w;
+        const Real* XC = xc(stage, c);
+        const Real p = prolong_node<Real>(x, y, [&](int X, int Y) { return XC[atc(X, Y)]; });
+        x2(stage, c)[at(x, y)] = x2(stage, c)[at(x, y)] + p;
+      }
+    }
+    __syncthreads();
+    // x4 on nodes [x0-1, x1+1) x [y0-1, y1+1)
+    {
+      const int ax0 = max(x0 - 1, 0), ax1 = min(x1 + 1, n), ay0 = max(y0 - 1, 0), ay1 = min(y1 + 1, n);
+      const int w = ax1 - ax0, h = ay1 - ay0;
+      for (int i = threadIdx.x; i < 2 * w * h; i += kThreads) {
+        const int c = i / (w * h), j = i % (w * h);
+        const int x = ax0 + j % w, y = ay0 + j / w;
+        const Real* X3 = x2(stage, c);
+        const Real ax = heat_row<Real>(x, y, n, hsq, [&](int a, int b) { return X3[at(a, b)]; });
+        x4(c)[at(x, y)] = jacobi_update(X3[at(x, y)], rhs(stage, c)[at(x, y)] * sgn, ax, diag);
+      }
+    }
+    __syncthreads();
+    // x5 on the owned nodes
+    {
+      const int w = x1 - x0, h = y1 - y0;
+      for (int i = threadIdx.x; i < w * h; i += kThreads) {
+        const int x = x0 + i % w, y = y0 + i / w;
+        Real o[2];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const Real* X4 = x4(c);
+          const Real ax = heat_row<Real>(x, y, n, hsq, [&](int a, int b) { return X4[at(a, b)]; });
+          o[c] = jacobi_update(X4[at(x, y)], rhs(stage, c)[at(x, y)] * sgn, ax, diag);
+        }
+        const size_t g = (size_t)y * P + x;
+        ox[g] = o[0];
+        oy[g] = o[1];
+        if (want_norm) part[0] += (double)o[0] * (double)o[0] + (double)o[1] * (double)o[1];
+      }
+    }
+  }
+};
 
 // Coarse part of the V-cycle, levels lc..0, by one CTA in shared memory
 // (MDMultigrid::solve recursion including the 100 sweeps on level 0).
-// Layout per level k: x[c], b[c], tmp[c], each (2^k+1)^2.
-template <typename Real>
-__device__ __forceinline__ size_t coarse_level_offset(int k) {
+// Layout per level k (dense, width 2^k+1): x[c], b[c], tmp[c].
+__host__ __device__ inline size_t coarse_level_offset(int k) {
   size_t off = 0;
   for (int j = 0; j < k; ++j) {
     const size_t w = (size_t)(1 << j) + 1;
@@ -450,166 +671,179 @@ __device__ __forceinline__ size_t coarse_level_offset(int k) {
   }
   return off;
 }
+__host__ __device__ inline size_t coarse_smem_elems(int lc) { return coarse_level_offset(lc + 1); }
 
 template <typename Real>
-__device__ void coarse_vcycle(int lc, double tau, Real* sm, const Real* bx, const Real* by, bool negate,
-                              Real* outx, Real* outy, bool want_norm, double part[kRedSlots]) {
-  auto X = [&](int k, int c) { const size_t w = (size_t)(1 << k) + 1; return sm + coarse_level_offset<Real>(k) + (size_t)c * w * w; };
-  auto B = [&](int k, int c) { const size_t w = (size_t)(1 << k) + 1; return sm + coarse_level_offset<Real>(k) + (size_t)(2 + c) * w * w; };
-  auto TMP = [&](int k, int c) { const size_t w = (size_t)(1 << k) + 1; return sm + coarse_level_offset<Real>(k) + (size_t)(4 + c) * w * w; };
-  {
-    const int w = (1 << lc) + 1;
-    for (int i = threadIdx.x; i < w * w; i += kThreads) {
-      Real a = bx[i], b = by[i];
-      if (negate) { a = a * Real(-1); b = b * Real(-1); }
-      B(lc, 0)[i] = a;
-      B(lc, 1)[i] = b;
-      X(lc, 0)[i] = Real(0);
-      X(lc, 1)[i] = Real(0);
-    }
-    __syncthreads();
+__device__ void coarse_vcycle(int lc, double tau, Real* sm, const Real* bx, const Real* by, Real sgn, Real* outx,
+                              Real* outy, bool want_norm, double part[kRedSlots]) {
+  // slot 0/1: x (ping-pong), slot 2: b -- each with two components
+  auto S = [&](int k, int slot, int c) {
+    const size_t w = (size_t)(1 << k) + 1;
+    return sm + coarse_level_offset(k) + (size_t)(2 * slot + c) * w * w;
+  };
+  int cur[kMaxLevel + 1];
+  for (int k = 0; k <= lc; ++k) cur[k] = 0;
+  const int wl = (1 << lc) + 1, Pl = pitch_of(wl);
+  for (int i = threadIdx.x; i < wl * wl; i += kThreads) {
+    const size_t g = (size_t)(i / wl) * Pl + (i % wl);
+    S(lc, 2, 0)[i] = bx[g] * sgn;
+    S(lc, 2, 1)[i] = by[g] * sgn;
+    S(lc, 0, 0)[i] = Real(0);
+    S(lc, 0, 1)[i] = Real(0);
   }
+  __syncthreads();
+  // One Jacobi sweep (HeatMultigrid::jacobi, linearSmoothOp.cpp:556-580): the
+  // new iterate goes to the other slot.
   auto jacobi_sweep = [&](int k) {
     const int w = (1 << k) + 1;
     const Real hsq = (Real)(tau * (double)((w - 1) * (w - 1)));
     const Real diag = (Real)(1 + 4 * tau * (double)((w - 1) * (w - 1)));
+    const int src = cur[k], dst = cur[k] ^ 1;
     for (int i = threadIdx.x; i < 2 * w * w; i += kThreads) {
       const int c = i / (w * w), id = i % (w * w);
-      const Real* xs = X(k, c);
-      TMP(k, c)[id] = heat_row<Real>(id % w, id / w, w, hsq, [&](int a, int b) { return xs[b * w + a]; });
+      const Real* xs = S(k, src, c);
+      const Real ax = heat_row<Real>(id % w, id / w, w, hsq, [&](int a, int b) { return xs[b * w + a]; });
+      S(k, dst, c)[id] = jacobi_update(xs[id], S(k, 2, c)[id], ax, diag);
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < 2 * w * w; i += kThreads) {
-      const int c = i / (w * w), id = i % (w * w);
-      X(k, c)[id] = jacobi_update(X(k, c)[id], B(k, c)[id], TMP(k, c)[id], diag);
-    }
+    cur[k] = dst;
     __syncthreads();
   };
-  // descend
   for (int k = lc; k >= 1; --k) {
     const int w = (1 << k) + 1, cw = (1 << (k - 1)) + 1;
     const Real hsq = (Real)(tau * (double)((w - 1) * (w - 1)));
     jacobi_sweep(k);
     jacobi_sweep(k);
-    for (int i = threadIdx.x; i < 2 * w * w; i += kThreads) {
-      const int c = i / (w * w), id = i % (w * w);
-      const Real* xs = X(k, c);
-      const Real ax = heat_row<Real>(id % w, id / w, w, hsq, [&](int a, int b) { return xs[b * w + a]; });
-      TMP(k, c)[id] = B(k, c)[id] - ax;
+    // residual into the free slot, then restriction
+    {
+      const int src = cur[k], dst = cur[k] ^ 1;
+      for (int i = threadIdx.x; i < 2 * w * w; i += kThreads) {
+        const int c = i / (w * w), id = i % (w * w);
+        const Real* xs = S(k, src, c);
+        const Real ax = heat_row<Real>(id % w, id / w, w, hsq, [&](int a, int b) { return xs[b * w + a]; });
+        S(k, dst, c)[id] = S(k, 2, c)[id] - ax;
+      }
+      __syncthreads();
+      for (int i = threadIdx.x; i < 2 * cw * cw; i += kThreads) {
+        const int c = i / (cw * cw), id = i % (cw * cw);
+        const Real* rs = S(k, dst, c);
+        S(k - 1, 2, c)[id] = restrict_node<Real>(id % cw, id / cw, cw, [&](int a, int b) { return rs[b * w + a]; });
+        S(k - 1, 0, c)[id] = Real(0);
+      }
+      cur[k - 1] = 0;
+      __syncthreads();
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < 2 * cw * cw; i += kThreads) {
-      const int c = i / (cw * cw), id = i % (cw * cw);
-      const Real* rs = TMP(k, c);
-      B(k - 1, c)[id] = restrict_node<Real>(id % cw, id / cw, cw, [&](int a, int b) { return rs[b * w + a]; });
-      X(k - 1, c)[id] = Real(0);
-    }
-    __syncthreads();
   }
   // level 0: 100 sweeps by one warp (2 components x 4 nodes)
   if (threadIdx.x < 32) {
-    const double hsq0 = tau * 1.0, diag0 = 1 + 4 * tau * 1.0;
-    const Real hsq = (Real)hsq0, diag = (Real)diag0;
+    const Real hsq = (Real)(tau * 1.0), diag = (Real)(1 + 4 * tau * 1.0);
     const int c = (threadIdx.x >> 2) & 1, id = threadIdx.x & 3;
+    Real* x0 = S(0, 0, c);
     for (int it = 0; it < 100; ++it) {
       Real ax = Real(0);
-      if (threadIdx.x < 8) {
-        const Real* xs = X(0, c);
-        ax = heat_row<Real>(id & 1, id >> 1, 2, hsq, [&](int a, int b) { return xs[b * 2 + a]; });
-      }
+      if (threadIdx.x < 8) ax = heat_row<Real>(id & 1, id >> 1, 2, hsq, [&](int a, int b) { return x0[b * 2 + a]; });
       __syncwarp();
-      if (threadIdx.x < 8) X(0, c)[id] = jacobi_update(X(0, c)[id], B(0, c)[id], ax, diag);
+      if (threadIdx.x < 8) x0[id] = jacobi_update(x0[id], S(0, 2, c)[id], ax, diag);
       __syncwarp();
     }
   }
   __syncthreads();
-  // ascend
   for (int k = 1; k <= lc; ++k) {
     const int w = (1 << k) + 1, cw = (1 << (k - 1)) + 1;
-    for (int i = threadIdx.x; i < 2 * w * w; i += kThreads) {
-      const int c = i / (w * w), id = i % (w * w);
-      const Real* xc = X(k - 1, c);
-      const Real p = prolong_node<Real>(id % w, id / w, [&](int a, int b) { return xc[b * cw + a]; });
-      X(k, c)[id] += p;
+    {
+      const int src = cur[k - 1];
+      for (int i = threadIdx.x; i < 2 * w * w; i += kThreads) {
+        const int c = i / (w * w), id = i % (w * w);
+        const Real* xc = S(k - 1, src, c);
+        const Real p = prolong_node<Real>(id % w, id / w, [&](int a, int b) { return xc[b * cw + a]; });
+        S(k, cur[k], c)[id] += p;
+      }
+      __syncthreads();
     }
-    __syncthreads();
     jacobi_sweep(k);
     jacobi_sweep(k);
   }
-  {
-    const int w = (1 << lc) + 1;
-    for (int i = threadIdx.x; i < w * w; i += kThreads) {
-      const Real a = X(lc, 0)[i], b = X(lc, 1)[i];
-      outx[i] = a;
-      outy[i] = b;
-      if (want_norm) part[0] += (double)a * (double)a + (double)b * (double)b;
-    }
+  for (int i = threadIdx.x; i < wl * wl; i += kThreads) {
+    const Real a = S(lc, cur[lc], 0)[i], b = S(lc, cur[lc], 1)[i];
+    const size_t g = (size_t)(i / wl) * Pl + (i % wl);
+    outx[g] = a;
+    outy[g] = b;
+    if (want_norm) part[0] += (double)a * (double)a + (double)b * (double)b;
   }
 }
 
-template <typename Real>
-__host__ __device__ inline size_t coarse_smem_elems(int lc) {
-  size_t off = 0;
-  for (int j = 0; j <= lc; ++j) {
-    const size_t w = (size_t)(1 << j) + 1;
-    off += 6 * w * w;
-  }
-  return off;
+// Dynamic shared memory of the level kernel (elements of Real).
+__host__ __device__ inline size_t level_smem_elems(int lc) {
+  size_t e = (size_t)2 * 9 * EWIN;                               // energy, kind 2
+  const size_t g = (size_t)2 * 5 * EWIN + (size_t)GCX * GCY * 8;  // gradient
+  const size_t d = (size_t)2 * 2 * VWIN + (size_t)6 * VWIN;      // down
+  const size_t u = (size_t)2 * (4 * VWIN + 2 * CWIN) + 2 * VWIN;  // up
+  const size_t c = coarse_smem_elems(lc);
+  if (g > e) e = g;
+  if (d > e) e = d;
+  if (u > e) e = u;
+  if (c > e) e = c;
+  return e;
 }
 
 // Full V-cycle on the current level: rhs = -DE (finest), output s.
 // Returns |s|^2 (cluster total) in norm_out.
 template <typename Real>
 __device__ void vcycle(cg::cluster_group& cluster, RedShared& rs, int& parity, const LevelArgs<Real>& a,
-                       const Inst<Real>& I, double tau, void* smem, int rank, int G, double& norm_out) {
+                       const Inst<Real>& I, double tau, Real* smem, int rank, int G, double& norm_out,
+                       PassTimer& pt) {
   const int L = a.level;
+  const size_t cs = comp_stride(L);
   const Real* dex = I.arr(a.off_de);
-  const Real* dey = dex + (size_t)I.n * I.n;
+  const Real* dey = dex + cs;
   Real* sx = I.arr(a.off_s);
-  Real* sy = sx + (size_t)I.n * I.n;
+  Real* sy = sx + cs;
   double part[kRedSlots] = {0, 0, 0, 0}, tot[kRedSlots];
-  // descend through the cluster-pass levels
   for (int k = L; k > a.lc; --k) {
-    const int w = (1 << k) + 1, cw = (1 << (k - 1)) + 1;
+    const int w = (1 << k) + 1;
     const Real hsq = (Real)(tau * (double)((w - 1) * (w - 1)));
     const Real diag = (Real)(1 + 4 * tau * (double)((w - 1) * (w - 1)));
     const Real* rx = (k == L) ? dex : I.arr(a.off_b[k]);
-    const Real* ry = rx + (size_t)w * w;
+    const Real* ry = (k == L) ? dey : rx + comp_stride(k);
     Real* x2 = I.arr(a.off_x2[k]);
     Real* bc = I.arr(a.off_b[k - 1]);
-    pass_down<Real>(k, w, rx, ry, k == L, x2, x2 + (size_t)w * w, bc, bc + (size_t)cw * cw, hsq, diag,
-                    *reinterpret_cast<DownShared<Real>*>(smem), rank, G);
-    cluster_barrier(cluster);
+    DownPass<Real> ps(w, rx, ry, (k == L) ? Real(-1) : Real(1), x2, x2 + comp_stride(k), bc,
+                      bc + comp_stride(k - 1), hsq, diag, smem);
+    Tiles tl(w, VTX, VTY);
+    MSG_TIMED(pt, PK_VDOWN, tile_pipeline(ps, tl.count(), rank, G));
+    MSG_TIMED(pt, PK_REDUCE, cluster_barrier(cluster));
   }
-  // coarse levels by CTA 0
   if (rank == 0) {
     const int lc = a.lc;
-    const int w = (1 << lc) + 1;
     const Real* bx = (L == lc) ? dex : I.arr(a.off_b[lc]);
+    const Real* by = (L == lc) ? dey : bx + comp_stride(lc);
     Real* out = (L == lc) ? sx : I.arr(a.off_x5[lc]);
-    coarse_vcycle<Real>(lc, tau, reinterpret_cast<Real*>(smem), bx, bx + (size_t)w * w, L == lc, out,
-                        out + (size_t)w * w, L == lc, part);
+    Real* outy = (L == lc) ? sy : out + comp_stride(lc);
+    MSG_TIMED(pt, PK_VCOARSE, coarse_vcycle<Real>(lc, tau, smem, bx, by, (L == lc) ? Real(-1) : Real(1), out, outy,
+                                                  L == lc, part));
   }
   if (L == a.lc) {
-    cluster_reduce(cluster, rs, parity, part, tot);
+    MSG_TIMED(pt, PK_REDUCE, cluster_reduce(cluster, rs, parity, part, tot));
     norm_out = tot[0];
     return;
   }
-  cluster_barrier(cluster);
-  // ascend
+  MSG_TIMED(pt, PK_REDUCE, cluster_barrier(cluster));
   for (int k = a.lc + 1; k <= L; ++k) {
-    const int w = (1 << k) + 1, cw = (1 << (k - 1)) + 1;
+    const int w = (1 << k) + 1;
     const Real hsq = (Real)(tau * (double)((w - 1) * (w - 1)));
     const Real diag = (Real)(1 + 4 * tau * (double)((w - 1) * (w - 1)));
     const Real* rx = (k == L) ? dex : I.arr(a.off_b[k]);
+    const Real* ry = (k == L) ? dey : rx + comp_stride(k);
     const Real* x2 = I.arr(a.off_x2[k]);
     const Real* xc = I.arr(a.off_x5[k - 1]);
     Real* o = (k == L) ? sx : I.arr(a.off_x5[k]);
-    pass_up<Real>(k, w, rx, rx + (size_t)w * w, k == L, x2, x2 + (size_t)w * w, xc, xc + (size_t)cw * cw, o,
-                  o + (size_t)w * w, hsq, diag, *reinterpret_cast<UpShared<Real>*>(smem), rank, G, k == L, part);
-    if (k < L) cluster_barrier(cluster);
+    Real* oy = (k == L) ? sy : o + comp_stride(k);
+    UpPass<Real> ps(w, rx, ry, (k == L) ? Real(-1) : Real(1), x2, x2 + comp_stride(k), xc,
+                    xc + comp_stride(k - 1), o, oy, hsq, diag, smem, k == L, part);
+    Tiles tl(w, VTX, VTY);
+    MSG_TIMED(pt, PK_VUP, tile_pipeline(ps, tl.count(), rank, G));
+    if (k < L) MSG_TIMED(pt, PK_REDUCE, cluster_barrier(cluster));
   }
-  cluster_reduce(cluster, rs, parity, part, tot);
+  MSG_TIMED(pt, PK_REDUCE, cluster_reduce(cluster, rs, parity, part, tot));
   norm_out = tot[0];
 }
 
@@ -617,8 +851,9 @@ __device__ __forceinline__ bool finite_d(double x) { return !isnan(x) && !isinf(
 
 // ---------------------------------------------------------------------------
 template <typename Real>
-__global__ void __launch_bounds__(kThreads) level_kernel(LevelArgs<Real> a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+__global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Real* smem = reinterpret_cast<Real*>(smem_raw);
   __shared__ RedShared rs;
   cg::cluster_group cluster = cg::this_cluster();
   const int G = (int)cluster.num_blocks();
@@ -627,8 +862,9 @@ __global__ void __launch_bounds__(kThreads) level_kernel(LevelArgs<Real> a) {
   const int nclusters = gridDim.x / G;
   int parity = 0;
   const int n = a.n;
-  const size_t N = (size_t)n * n;
+  const size_t cs = comp_stride(a.level);
   const double lam = a.lambda;
+  PassTimer pt{a.pass_cycles ? a.pass_cycles + (size_t)blockIdx.x * kPassKinds : nullptr, 0};
 
   for (int inst = cid; inst < a.num_inst; inst += nclusters) {
     Inst<Real> I;
@@ -636,11 +872,12 @@ __global__ void __launch_bounds__(kThreads) level_kernel(LevelArgs<Real> a) {
     I.R = a.R;
     I.T = I.base + a.off_T;
     I.n = n;
+    I.P = pitch_of(n);
     I.h = (Real)(1.0 / (double)(n - 1));
     Real* de = I.arr(a.off_de);
     Real* s = I.arr(a.off_s);
     int cur = a.phi_in_dev ? a.phi_in_dev[inst] : 0;  // buffer holding phi
-    int dcur = 0;         // buffer holding the current direction d (written by the NCG pass)
+    int dcur = 0;                                     // buffer holding the current direction d
     double part[kRedSlots], tot[kRedSlots];
 
     auto reset = [&]() {
@@ -651,16 +888,20 @@ __global__ void __launch_bounds__(kThreads) level_kernel(LevelArgs<Real> a) {
 
     if (a.mode == MODE_SMOOTH) {
       double nrm;
-      vcycle<Real>(cluster, rs, parity, a, I, (double)(0.5f * (a.sigma_fixed * a.sigma_fixed)), smem_raw, rank, G, nrm);
+      vcycle<Real>(cluster, rs, parity, a, I, (double)(0.5f * (a.sigma_fixed * a.sigma_fixed)), smem, rank, G,
+                   nrm, pt);
       cluster_barrier(cluster);
       continue;
     }
 
     // initial energy E(phi) = E_data + lambda * 1/2 phi.L phi   (gradientDescent.h:306)
     reset();
-    pass_energy<Real>(I, 0, Real(0), Real(0), false, phi, phi + N, nullptr, nullptr, nullptr, nullptr, nullptr,
-                      nullptr, nullptr, nullptr, rank, G, part);
-    cluster_reduce(cluster, rs, parity, part, tot);
+    {
+      EnergyPass<Real> ps(I, 0, Real(0), Real(0), false, phi, phi + cs, nullptr, nullptr, nullptr, nullptr,
+                          nullptr, nullptr, nullptr, nullptr, smem, part);
+      MSG_TIMED(pt, PK_ENERGY0, tile_pipeline(ps, ps.tl.count(), rank, G));
+    }
+    MSG_TIMED(pt, PK_REDUCE, cluster_reduce(cluster, rs, parity, part, tot));
     double A = tot[1];
     auto energy_of = [&](double edata, double ereg) {
       double e = 0.0;
@@ -673,9 +914,10 @@ __global__ void __launch_bounds__(kThreads) level_kernel(LevelArgs<Real> a) {
 
     if (a.mode == MODE_ENERGY) {
       reset();
-      pass_gradient<Real>(I, *reinterpret_cast<GradShared<Real>*>(smem_raw), false, Real(0), phi, phi + N,
-                          nullptr, nullptr, I.arr(a.off_phi[cur ^ 1]), I.arr(a.off_phi[cur ^ 1]) + N, de, de + N,
-                          lam, rank, G, part);
+      Real* nphi = I.arr(a.off_phi[cur ^ 1]);
+      GradPass<Real> ps(I, false, Real(0), lam, phi, phi + cs, nullptr, nullptr, nphi, nphi + cs, de, de + cs,
+                        smem, part);
+      tile_pipeline(ps, ps.tl.count(), rank, G);
       cluster_barrier(cluster);
       if (rank == 0 && threadIdx.x == 0) {
         a.out_energy[inst] = energy;
@@ -711,17 +953,18 @@ __global__ void __launch_bounds__(kThreads) level_kernel(LevelArgs<Real> a) {
         {
           Real* nphi = I.arr(a.off_phi[cur ^ 1]);
           const Real* dd = I.arr(a.off_d[dcur]);
-          pass_gradient<Real>(I, *reinterpret_cast<GradShared<Real>*>(smem_raw), pending, (Real)tau_p, phi,
-                              phi + N, dd, dd + N, nphi, nphi + N, de, de + N, lam, rank, G, part);
+          GradPass<Real> ps(I, pending, (Real)tau_p, lam, phi, phi + cs, dd, dd + cs, nphi, nphi + cs, de, de + cs,
+                            smem, part);
+          MSG_TIMED(pt, PK_GRAD, tile_pipeline(ps, ps.tl.count(), rank, G));
           cur ^= 1;
           phi = nphi;
           pending = false;
         }
-        cluster_reduce(cluster, rs, parity, part, tot);
+        MSG_TIMED(pt, PK_REDUCE, cluster_reduce(cluster, rs, parity, part, tot));
         A = tot[1];
         // H1 smoothing of -DE (the descent direction's metric)
         double s2;
-        vcycle<Real>(cluster, rs, parity, a, I, (double)(0.5f * (sigma * sigma)), smem_raw, rank, G, s2);
+        vcycle<Real>(cluster, rs, parity, a, I, (double)(0.5f * (sigma * sigma)), smem, rank, G, s2, pt);
         // Fletcher-Reeves (gradientDescent.h:221-226)
         const double beta = ((iter - 1) % 10) ? (s2 / og2) : 0.0;
         og2 = s2;
@@ -732,9 +975,10 @@ __global__ void __launch_bounds__(kThreads) level_kernel(LevelArgs<Real> a) {
           // energy at phi + tt d; E_reg by the exact quadratic expansion in tt
           reset();
           const Real* dd = I.arr(a.off_d[dcur]);
-          pass_energy<Real>(I, 1, (Real)tt, Real(0), false, phi, phi + N, dd, dd + N, nullptr, nullptr, nullptr,
-                            nullptr, nullptr, nullptr, rank, G, part);
-          cluster_reduce(cluster, rs, parity, part, tot);
+          EnergyPass<Real> ps(I, 1, (Real)tt, Real(0), false, phi, phi + cs, dd, dd + cs, nullptr, nullptr,
+                              nullptr, nullptr, nullptr, nullptr, smem, part);
+          MSG_TIMED(pt, PK_ENERGY, tile_pipeline(ps, ps.tl.count(), rank, G));
+          MSG_TIMED(pt, PK_REDUCE, cluster_reduce(cluster, rs, parity, part, tot));
           const double e = energy_of(tot[0], 0.5 * ((A + 2.0 * tt * Bd) + tt * tt * Cd));
           rb_tau[rb_pos] = tt;
           rb_e[rb_pos] = e;
@@ -752,9 +996,12 @@ __global__ void __launch_bounds__(kThreads) level_kernel(LevelArgs<Real> a) {
           t = t < tau_min ? tau_min : (t > tau_max ? tau_max : t);
           // first trial fused with the direction materialisation
           reset();
-          pass_energy<Real>(I, 2, (Real)t, (Real)beta, fallback || od_zero, phi, phi + N, od, od + N, s, s + N, wd,
-                            wd + N, de, de + N, rank, G, part);
-          cluster_reduce(cluster, rs, parity, part, tot);
+          {
+            EnergyPass<Real> ps(I, 2, (Real)t, (Real)beta, fallback || od_zero, phi, phi + cs, od, od + cs, s,
+                                s + cs, de, de + cs, wd, wd + cs, smem, part);
+            MSG_TIMED(pt, PK_NCG, tile_pipeline(ps, ps.tl.count(), rank, G));
+          }
+          MSG_TIMED(pt, PK_REDUCE, cluster_reduce(cluster, rs, parity, part, tot));
           dcur = dn;
           const double Df = tot[1];
           Bd = tot[2];
@@ -824,12 +1071,14 @@ __global__ void __launch_bounds__(kThreads) level_kernel(LevelArgs<Real> a) {
       Real* nphi = I.arr(a.off_phi[cur ^ 1]);
       const Real* dd = I.arr(a.off_d[dcur]);
       const Real tp = (Real)tau_p;
-      for (size_t i = (size_t)rank * kThreads + threadIdx.x; i < N; i += (size_t)G * kThreads) {
-        Real vx = phi[i], vy = phi[N + i];
-        vx += tp * dd[i];
-        vy += tp * dd[N + i];
-        nphi[i] = vx;
-        nphi[N + i] = vy;
+      const int P = I.P;
+      for (size_t i = (size_t)rank * kThreads + threadIdx.x; i < (size_t)n * n; i += (size_t)G * kThreads) {
+        const size_t g = (i / n) * P + (i % n);
+        Real vx = phi[g], vy = phi[cs + g];
+        vx += tp * dd[g];
+        vy += tp * dd[cs + g];
+        nphi[g] = vx;
+        nphi[cs + g] = vy;
       }
       cur ^= 1;
     }

@@ -43,7 +43,10 @@ class Params(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [("kernel_launches", ctypes.c_int), ("num_levels", ctypes.c_int), ("first_level", ctypes.c_int),
                 ("level_ms", ctypes.c_float * 16), ("level_steps", ctypes.c_longlong * 16),
-                ("level_evals", ctypes.c_longlong * 16)]
+                ("level_evals", ctypes.c_longlong * 16), ("level_cluster", ctypes.c_int * 16),
+                ("level_pass_cycles", (ctypes.c_longlong * 8) * 16)]
+
+PASS_KINDS = ["energy0", "gradient", "vdown", "vcoarse", "vup", "ncg", "energy", "sync"]
 
 
 class MsgpuError(RuntimeError):
@@ -222,7 +225,8 @@ class Context:
         k = s.num_levels
         return {"kernel_launches": s.kernel_launches, "first_level": s.first_level,
                 "level_ms": list(s.level_ms[:k]), "level_steps": list(s.level_steps[:k]),
-                "level_evals": list(s.level_evals[:k])}
+                "level_evals": list(s.level_evals[:k]), "level_cluster": list(s.level_cluster[:k]),
+                "level_pass_cycles": [dict(zip(PASS_KINDS, list(s.level_pass_cycles[i]))) for i in range(k)]}
 
     # --- single operators ------------------------------------------------
     def energy(self, level, R, T, phix, phiy, lam, fp64=False):

@@ -98,7 +98,7 @@ def _params(level, **kw):
     return p
 
 
-def test_multilevel_registration_matches_reference(gpu):
+def test_multilevel_registration_matches_reference(gpu, oracle):
     g = golden("register_L7.npz")
     n = (1 << 7) + 1
     for i in range(3):
@@ -107,8 +107,44 @@ def test_multilevel_registration_matches_reference(gpu):
                     max_gd_iterations=int(mi), stop_epsilon=se, resample_deformation=int(rs), use_fp64=1,
                     dont_normalize_input=1)
         phis, en, steps = gpu.register_batch(p, g["R"], g["T"][None])
-        assert max(np.abs(phis[0] - g[f"phi{i}"]).max(), 0) * (n - 1) <= 1e-6, i
-        assert abs(en[0] - g[f"E{i}"][0]) / g[f"E{i}"][0] <= 1e-9, i
+        dphi = np.abs(phis[0] - g[f"phi{i}"]).max() * (n - 1)
+        if not rs:
+            assert dphi <= 1e-6, i
+            assert abs(en[0] - g[f"E{i}"][0]) / g[f"E{i}"][0] <= 1e-9, i
+        else:
+            # resampling the flattened node vector scrambles the rows of the
+            # displacement; the reference itself then moves by a large fraction
+            # of a pixel under 1-ulp changes of its input.  Hold the GPU to that
+            # spread, measured here on the oracle.
+            rng = np.random.default_rng(0)
+            spread = 0.0
+            for _ in range(3):
+                Rp = g["R"].copy()
+                idx = rng.choice(Rp.size, 4, replace=False)
+                Rp[idx] = np.nextafter(Rp[idx], 2.0)
+                qx, qy, _, _ = oracle.register(7, int(start), int(stop), Rp, g["T"], lam=lam, lam_factor=lf,
+                                               max_iter=int(mi), stop_eps=se, resample_phi=True)
+                spread = max(spread, max(np.abs(qx - g[f"phi{i}"][0]).max(),
+                                         np.abs(qy - g[f"phi{i}"][1]).max()) * (n - 1))
+            assert dphi <= 3 * spread, (dphi, spread)
+
+
+@pytest.mark.parametrize("resample", [0, 1])
+def test_displacement_transfer_chain_exact(gpu, oracle, resample):
+    """Restriction of a given displacement to the start level, then transfer
+    (prolongation or flat resampling) to the precision level, with no descent
+    steps: every operation of the chain is compared bit for bit."""
+    level = 7
+    n = (1 << level) + 1
+    rng = np.random.default_rng(11)
+    from msgpu import synthetic as syn
+    fr, _, _ = syn.make_series(n, 2, syn.HEX_513, seed=12)
+    init = rng.normal(0, 1.0 / (n - 1), size=(1, 2, n * n))
+    p = _params(level, start_level=4, stop_level=6, max_gd_iterations=0, resample_deformation=resample, use_fp64=1)
+    phis, _, _ = gpu.register_batch(p, fr[0].ravel(), fr[1].ravel()[None], initial_phis=init)
+    qx, qy, _, _ = oracle.register(level, 4, 6, oracle.normalize(fr[0].ravel()), oracle.normalize(fr[1].ravel()),
+                                   init[0, 0], init[0, 1], lam=0.1, max_iter=0, resample_phi=bool(resample))
+    assert np.array_equal(phis[0, 0], qx) and np.array_equal(phis[0, 1], qy)
 
 
 def test_series_stage_and_average_match_reference(gpu):
