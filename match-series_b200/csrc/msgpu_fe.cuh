@@ -43,11 +43,12 @@ template <> struct RealTraits<double> {
 __device__ __forceinline__ int node_class(int x, int n) { return x == 0 ? 0 : (x == n - 1 ? 2 : 1); }
 
 // DiscreteFunctionDefault::evaluateAtQuadPoint (discreteFunction.h:239-246)
-// on the four nodal values v[b] of an element.
+// on the four nodal values v[b] of an element.  The reference starts the sum
+// at 0.; starting at the first product differs only in the sign of an exact
+// zero, which no later operation of the path can observe.
 template <typename Real>
 __device__ __forceinline__ Real at_quad(const Real v[4], int q) {
-  Real w = Real(0);
-  w += v[0] * Real(c_fe.bq[0][q]);
+  Real w = v[0] * Real(c_fe.bq[0][q]);
   w += v[1] * Real(c_fe.bq[1][q]);
   w += v[2] * Real(c_fe.bq[2][q]);
   w += v[3] * Real(c_fe.bq[3][q]);
@@ -65,26 +66,23 @@ struct Warped {
 
 template <typename Real>
 __device__ __forceinline__ void clip_axis(Real coord, int n, Real h, int& el, Real& loc, bool& inside) {
-  // width = (int)((n-1) * h) is 1 on every dyadic level.
-  const int width = (int)((double)(n - 1) * (double)h);
+  // width = (int)((n-1) * h) is exactly 1 on every dyadic level.
+  (void)h;
   inside = true;
   if (coord < Real(0)) {
     coord = Real(0);
     inside = false;
-  } else if (coord >= Real(width)) {
-    coord = Real(width) - RealTraits<Real>::eps();
+  } else if (coord >= Real(1)) {
+    coord = Real(1) - RealTraits<Real>::eps();
     inside = false;
   }
-  // coord / h with h = 2^-l, written as the exactly equal product with 2^l
+  // coord / h with h = 2^-l, written as the exactly equal product with 2^l.
+  // After clipping sc < n-1, so the reference's "exactly on the right
+  // boundary" adjustment (configurators.h:40-44) cannot apply.
   const Real sc = coord * Real(n - 1);
-  int e = (short)sc;
-  Real l = sc - Real(e);
-  if (e == n - 1 && fabs((double)(l - Real(0))) < 1e-15) {
-    e = n - 2;
-    l = Real(1);
-  }
+  const int e = (short)sc;
   el = e;
-  loc = l;
+  loc = sc - Real(e);
 }
 
 template <typename Real>
@@ -103,8 +101,7 @@ __device__ __forceinline__ Warped<Real> warp_quad_point(int ex, int ey, int q, R
 // basis (baseFunctionSet.h:141-144) on the 4 texels t[0..3] of the element.
 template <typename Real>
 __device__ __forceinline__ Real q1_value(const Real t[4], Real x, Real y) {
-  Real w = Real(0);
-  w += t[0] * ((Real(1) - x) * (Real(1) - y));
+  Real w = t[0] * ((Real(1) - x) * (Real(1) - y));
   w += t[1] * (x * (Real(1) - y));
   w += t[2] * ((Real(1) - x) * y);
   w += t[3] * (x * y);
@@ -116,10 +113,8 @@ __device__ __forceinline__ Real q1_value(const Real t[4], Real x, Real y) {
 // division is the exactly equal product with inv_h = 2^l.
 template <typename Real>
 __device__ __forceinline__ void q1_grad(const Real t[4], Real x, Real y, Real inv_h, Real& gx, Real& gy) {
-  gx = Real(0);
-  gy = Real(0);
   Real vx, vy;
-  vx = (y - Real(1)) * inv_h; vy = (x - Real(1)) * inv_h; vx *= t[0]; vy *= t[0]; gx += vx; gy += vy;
+  vx = (y - Real(1)) * inv_h; vy = (x - Real(1)) * inv_h; vx *= t[0]; vy *= t[0]; gx = vx; gy = vy;
   vx = (Real(1) - y) * inv_h; vy = (-x) * inv_h;          vx *= t[1]; vy *= t[1]; gx += vx; gy += vy;
   vx = (-y) * inv_h;          vy = (Real(1) - x) * inv_h; vx *= t[2]; vy *= t[2]; gx += vx; gy += vy;
   vx = y * inv_h;             vy = x * inv_h;             vx *= t[3]; vy *= t[3]; gx += vx; gy += vy;
@@ -142,7 +137,7 @@ __device__ __forceinline__ void load_texels(const Real* __restrict__ T, int P, i
 template <typename Real>
 __device__ __forceinline__ Real element_ssd(const Real* __restrict__ T, int n, int P, Real h, int ex, int ey,
                                             const Real px[4], const Real py[4], const Real r[4]) {
-  Real a = Real(0);
+  Real a;
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const Real ox = at_quad(px, q);
@@ -153,7 +148,8 @@ __device__ __forceinline__ Real element_ssd(const Real* __restrict__ T, int n, i
     const Real tv = q1_value(t, w.lx, w.ly);
     const Real rv = at_quad(r, q);
     const Real d = tv - rv;
-    a += (Real(0.5) * (d * d)) * Real(c_fe.w);
+    const Real v = (Real(0.5) * (d * d)) * Real(c_fe.w);
+    if (q == 0) a = v; else a += v;   // the integrand is >= 0: no signed-zero difference
   }
   a *= h * h;
   return a;

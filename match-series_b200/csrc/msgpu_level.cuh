@@ -229,6 +229,37 @@ struct Tiles {
   }
 };
 
+// Runs f(x, y) over [0, w) x [0, h) with the CTA's threads laid out as LX x
+// (kThreads/LX) lanes (no integer division in the index math).
+template <int LX, class F>
+__device__ __forceinline__ void for_2d(int w, int h, F&& f) {
+  constexpr int LY = kThreads / LX;
+  const int lx = threadIdx.x % LX, ly = threadIdx.x / LX;
+  for (int y = ly; y < h; y += LY)
+    for (int x = lx; x < w; x += LX) f(x, y);
+}
+
+// Runs f(x, y) over [0, w) x [0, h), the w*h points spread evenly over the
+// CTA's threads.  The row index is a multiply-high by m = floor((2^32-1)/w)+1:
+// with m*w = 2^32 + e, 0 <= e < w, the product i*m/2^32 exceeds i/w by less
+// than i/2^32 < 1/w for i*w < 2^32, so it floors to i/w exactly.
+template <class F>
+__device__ __forceinline__ void for_rect(int w, int h, F&& f) {
+  const unsigned m = 0xFFFFFFFFu / (unsigned)w + 1u;
+  for (int i = threadIdx.x; i < w * h; i += kThreads) {
+    const int y = (w == 1) ? i : (int)__umulhi((unsigned)i, m);
+    f(i - y * w, y);
+  }
+}
+// Same over two components stacked in y: f(c, x, y) for c in {0, 1}.
+template <class F>
+__device__ __forceinline__ void for_rect2(int w, int h, F&& f) {
+  for_rect(w, 2 * h, [&](int x, int yy) {
+    const int c = yy >= h;
+    f(c, x, yy - c * h);
+  });
+}
+
 // ---------------------------------------------------------------------------
 template <typename Real>
 struct Inst {
@@ -323,8 +354,8 @@ struct EnergyPass {
     // elements owned by the tile
     const int ex1 = (x1 < n - 1) ? x1 : n - 1, ey1 = (y1 < n - 1) ? y1 : n - 1;
     const int ew = ex1 - x0, eh = ey1 - y0;
-    for (int i = threadIdx.x; i < ew * eh; i += kThreads) {
-      const int ex = x0 + i % ew, ey = y0 + i / ew;
+    for_2d<64>(ew, eh, [&](int ix, int iy) {
+      const int ex = x0 + ix, ey = y0 + iy;
       const int c0 = at(ex, ey);
       const int idx[4] = {c0, c0 + 1, c0 + EWX, c0 + EWX + 1};
       Real px[4], py[4], r[4];
@@ -344,12 +375,12 @@ struct EnergyPass {
         }
       }
       part[0] += (double)element_ssd(I.T, n, I.P, I.h, ex, ey, px, py, r);
-    }
+    });
     if (kind == 1) return;
     // owned nodes
     const int nw = x1 - x0, nh = y1 - y0;
-    for (int i = threadIdx.x; i < nw * nh; i += kThreads) {
-      const int x = x0 + i % nw, y = y0 + i / nw;
+    for_2d<64>(nw, nh, [&](int ix, int iy) {
+      const int x = x0 + ix, y = y0 + iy;
       const int c = at(x, y);
       if (kind == 0) {
         const Real lx = stiff_row<Real>(x, y, n, [&](int X, int Y) { return Wpx[at(X, Y)]; });
@@ -366,7 +397,7 @@ struct EnergyPass {
         part[2] += (double)Wpx[c] * (double)lx + (double)Wpy[c] * (double)ly;
         part[3] += (double)ddx * (double)lx + (double)ddy * (double)ly;
       }
-    }
+    });
   }
 };
 
@@ -435,9 +466,9 @@ struct GradPass {
     // 2. element contributions, elements [x0-1, x1) x [y0-1, y1) that exist
     Real* C = contrib();
     const int cw = (x1 < ne ? x1 : ne) - (x0 - 1), ch = (y1 < ne ? y1 : ne) - (y0 - 1);
-    for (int i = threadIdx.x; i < cw * ch; i += kThreads) {
-      const int ex = x0 - 1 + i % cw, ey = y0 - 1 + i / cw;
-      if (ex < 0 || ey < 0) continue;
+    for_rect(cw, ch, [&](int ix, int iy) {
+      const int ex = x0 - 1 + ix, ey = y0 - 1 + iy;
+      if (ex < 0 || ey < 0) return;
       const int c0 = at(ex, ey);
       const int idx[4] = {c0, c0 + 1, c0 + EWX, c0 + EWX + 1};
       Real px[4], py[4], r[4];
@@ -455,13 +486,13 @@ struct GradPass {
         cc[2 * b] = out[b][0];
         cc[2 * b + 1] = out[b][1];
       }
-    }
+    });
     __syncthreads();
     // 3. node sums in element order, stiffness, outputs
     const Real lam = (Real)lambda;
     const int nw = x1 - x0, nh = y1 - y0;
-    for (int i = threadIdx.x; i < nw * nh; i += kThreads) {
-      const int x = x0 + i % nw, y = y0 + i / nw;
+    for_2d<64>(nw, nh, [&](int ix, int iy) {
+      const int x = x0 + ix, y = y0 + iy;
       auto cc = [&](int ex, int ey, int b, int comp) {
         return C[((size_t)(ey - (y0 - 1)) * GCX + (ex - (x0 - 1))) * 8 + 2 * b + comp];
       };
@@ -481,7 +512,7 @@ struct GradPass {
       nphx[g] = vx;
       nphy[g] = vy;
       part[1] += (double)vx * (double)Lx + (double)vy * (double)Ly;
-    }
+    });
   }
 };
 
@@ -531,40 +562,37 @@ struct DownPass {
     {
       const int ax0 = max(x0 - 2, 0), ax1 = min(x1 + 2, n), ay0 = max(y0 - 2, 0), ay1 = min(y1 + 2, n);
       const int w = ax1 - ax0, h = ay1 - ay0;
-      for (int i = threadIdx.x; i < 2 * w * h; i += kThreads) {
-        const int c = i / (w * h), j = i % (w * h);
-        const int x = ax0 + j % w, y = ay0 + j / w;
+      for_rect2(w, h, [&](int c, int ix, int iy) {
+        const int x = ax0 + ix, y = ay0 + iy;
         const Real* X1 = work(2, c);
         const Real ax = heat_row<Real>(x, y, n, hsq, [&](int a, int b) { return X1[at(a, b)]; });
         work(0, c)[at(x, y)] = jacobi_update(X1[at(x, y)], rhs(stage, c)[at(x, y)], ax, diag);
-      }
+      });
     }
     __syncthreads();
     // residual on nodes [x0-1, x1+1) x [y0-1, y1+1); x2 out for owned nodes
     {
       const int ax0 = max(x0 - 1, 0), ax1 = min(x1 + 1, n), ay0 = max(y0 - 1, 0), ay1 = min(y1 + 1, n);
       const int w = ax1 - ax0, h = ay1 - ay0;
-      for (int i = threadIdx.x; i < 2 * w * h; i += kThreads) {
-        const int c = i / (w * h), j = i % (w * h);
-        const int x = ax0 + j % w, y = ay0 + j / w;
+      for_rect2(w, h, [&](int c, int ix, int iy) {
+        const int x = ax0 + ix, y = ay0 + iy;
         const Real* X2 = work(0, c);
         const Real ax = heat_row<Real>(x, y, n, hsq, [&](int a, int b) { return X2[at(a, b)]; });
         work(1, c)[at(x, y)] = rhs(stage, c)[at(x, y)] - ax;
         if (x >= x0 && x < x1 && y >= y0 && y < y1) (c == 0 ? x2x : x2y)[(size_t)y * P + x] = X2[at(x, y)];
-      }
+      });
     }
     __syncthreads();
     // restriction to the coarse nodes centred in the tile
     {
       const int X0 = x0 >> 1, X1 = (x1 + 1) >> 1, Y0 = y0 >> 1, Y1 = (y1 + 1) >> 1;
       const int w = X1 - X0, h = Y1 - Y0;
-      for (int i = threadIdx.x; i < 2 * w * h; i += kThreads) {
-        const int c = i / (w * h), j = i % (w * h);
-        const int X = X0 + j % w, Y = Y0 + j / w;
+      for_rect2(w, h, [&](int c, int ix, int iy) {
+        const int X = X0 + ix, Y = Y0 + iy;
         const Real* Rs = work(1, c);
         const Real v = restrict_node<Real>(X, Y, cw, [&](int x, int y) { return Rs[at(x, y)]; });
         (c == 0 ? bcx : bcy)[(size_t)Y * cP + X] = v;
-      }
+      });
     }
   }
 };
@@ -617,33 +645,31 @@ struct UpPass {
     {
       const int ax0 = max(x0 - 2, 0), ax1 = min(x1 + 2, n), ay0 = max(y0 - 2, 0), ay1 = min(y1 + 2, n);
       const int w = ax1 - ax0, h = ay1 - ay0;
-      for (int i = threadIdx.x; i < 2 * w * h; i += kThreads) {
-        const int c = i / (w * h), j = i % (w * h);
-        const int x = ax0 + j % w, y = ay0 + j / w;
+      for_rect2(w, h, [&](int c, int ix, int iy) {
+        const int x = ax0 + ix, y = ay0 + iy;
         const Real* XC = xc(stage, c);
         const Real p = prolong_node<Real>(x, y, [&](int X, int Y) { return XC[atc(X, Y)]; });
         x2(stage, c)[at(x, y)] = x2(stage, c)[at(x, y)] + p;
-      }
+      });
     }
     __syncthreads();
     // x4 on nodes [x0-1, x1+1) x [y0-1, y1+1)
     {
       const int ax0 = max(x0 - 1, 0), ax1 = min(x1 + 1, n), ay0 = max(y0 - 1, 0), ay1 = min(y1 + 1, n);
       const int w = ax1 - ax0, h = ay1 - ay0;
-      for (int i = threadIdx.x; i < 2 * w * h; i += kThreads) {
-        const int c = i / (w * h), j = i % (w * h);
-        const int x = ax0 + j % w, y = ay0 + j / w;
+      for_rect2(w, h, [&](int c, int ix, int iy) {
+        const int x = ax0 + ix, y = ay0 + iy;
         const Real* X3 = x2(stage, c);
         const Real ax = heat_row<Real>(x, y, n, hsq, [&](int a, int b) { return X3[at(a, b)]; });
         x4(c)[at(x, y)] = jacobi_update(X3[at(x, y)], rhs(stage, c)[at(x, y)] * sgn, ax, diag);
-      }
+      });
     }
     __syncthreads();
     // x5 on the owned nodes
     {
       const int w = x1 - x0, h = y1 - y0;
-      for (int i = threadIdx.x; i < w * h; i += kThreads) {
-        const int x = x0 + i % w, y = y0 + i / w;
+      for_rect(w, h, [&](int ix, int iy) {
+        const int x = x0 + ix, y = y0 + iy;
         Real o[2];
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
@@ -655,7 +681,7 @@ struct UpPass {
         ox[g] = o[0];
         oy[g] = o[1];
         if (want_norm) part[0] += (double)o[0] * (double)o[0] + (double)o[1] * (double)o[1];
-      }
+      });
     }
   }
 };
