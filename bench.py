@@ -247,6 +247,24 @@ def run_reference_arm(args, world, rank):
     return 0
 
 
+def profile_case(level: int, iters: int, fp64: bool):
+    """One launch of the level kernel on the bench's frames generated at
+    `level` (start = stop = level, `iters` steps): the case ncu captures."""
+    import msgpu
+    from msgpu import build as mbuild
+    from msgpu import synthetic as syn
+    mbuild.build()
+    n = (1 << level) + 1
+    frames, _, _ = syn.make_series(n, FRAMES + 1, syn.HEX_513, seed=2000)
+    ctx = msgpu.Context(0)
+    p = msgpu.default_params(precision_level=level, input_level=level, start_level=level, stop_level=level,
+                             max_gd_iterations=iters, use_fp64=int(fp64))
+    ctx.set_profiling(True)
+    ctx.register_batch(p, frames[FRAMES], frames[:FRAMES])
+    print(json.dumps({"profile_level": level, "frames": FRAMES, "iters": iters, "fp64": fp64,
+                      "stats": ctx.stats()}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -255,8 +273,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--fp32", action="store_true", help="FP32 bulk with FP64 reductions (outside the energy tol)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-level", type=int, default=0,
+                    help="small case for ncu captures: one level solve of FRAMES frames at this level, "
+                         "--profile-iters gradient steps, no timing")
+    ap.add_argument("--profile-iters", type=int, default=5)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.profile_level:
+        return profile_case(args.profile_level, args.profile_iters, not args.fp32)
     world, rank, local = dist_setup()
     if args.impl == "reference":
         return run_reference_arm(args, world, rank)
