@@ -140,6 +140,34 @@ int msgpu_gd_level(msgpu_context* ctx, int level, const double* R, const double*
                    double* phiy, double lambda, int max_iter, double stop_eps, int use_fp64,
                    double* energy_out, int* steps_out, double* trace, int max_trace);
 
+/* --- allocation-free level solve ----------------------------------------
+ * No counterpart in the reference.  The same level solve as msgpu_gd_level,
+ * for callers that cannot allocate device memory: applications whose device
+ * memory belongs to their own pool allocator (cudaMalloc/cudaFree from other
+ * code would synchronise the device and fragment the pool), or hosts that
+ * admit only a fixed, known device footprint.  It needs no context and
+ * allocates nothing: its scratch (pitched image copies, the gradient-flow
+ * arena and the multigrid pyramid) lives in one static device array of
+ * 12 MiB that every GPU loading this library holds until the process exits.
+ *   Limit: levels up to 8 (257^2 nodes) in FP64 or FP32; larger levels
+ *   return MSGPU_ERR_SIZE without touching the device.
+ *   d_R, d_T   : device, (2^level+1)^2 doubles each (prepared images)
+ *   d_phi      : device, 2*(2^level+1)^2 doubles [phi_x, phi_y], updated in place
+ *   d_energy_out / d_steps_out : device, one double / one int (nullable)
+ *   stream     : cudaStream_t (NULL = legacy default stream); the call
+ *                returns after enqueueing.
+ * The first call on a device (with that device current) does a one-time
+ * set-up: it looks up the device address of the scratch array and uploads
+ * the finite-element tables; make that first call before any stream capture.
+ * Every call on a device shares the one scratch array and leaves its
+ * contents behind (each call clears what must start at zero); calls whose
+ * work overlaps on the GPU (other streams, other host threads) race on it,
+ * so serialise them.  Errors are status codes only (no context holds a
+ * message): MSGPU_ERR_INVALID_ARG, MSGPU_ERR_SIZE, MSGPU_ERR_CUDA.          */
+int msgpu_gd_level_noalloc(int level, const double* d_R, const double* d_T, double* d_phi, double lambda,
+                           int max_iter, double stop_eps, int use_fp64, double* d_energy_out, int* d_steps_out,
+                           void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -17,6 +17,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1228,3 +1229,172 @@ int msgpu_normalize(msgpu_context* ctx, const double* in, int count, double satu
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free level solve (msgpu_gd_level_noalloc).
+//
+// Some callers cannot allocate device memory: an application whose device
+// memory is owned by its own pool allocator (which forbids other code from
+// calling cudaMalloc / cudaFree behind its back, because those calls
+// synchronise the device and fragment the pool), or a host that admits only
+// code with a fixed, known device footprint.  For them this entry point runs
+// the same level kernel as msgpu_gd_level with all of its scratch (the
+// pitched copies of the images, the per-level arena of the gradient flow and
+// the multigrid pyramid) carved out of one file-scope device array, so no
+// device memory is allocated per call; the caller passes only inputs and
+// outputs.
+namespace {
+
+// Size of the scratch array: enough for one level-8 solve (257^2 nodes) in
+// FP64 (11.45 MB needed); every GPU that loads this library holds it until
+// the process exits.
+constexpr size_t kNoAllocScratchBytes = (size_t)12 << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+struct NoAllocDevice {
+  bool ready = false;
+  unsigned char* scratch = nullptr;  // device address of g_noalloc_scratch
+  int sms = 0;
+};
+constexpr int kNoAllocMaxDevices = 64;
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+std::mutex g_noalloc_mu;
+
+size_t noalloc_bytes_needed(int level, size_t real_bytes) {
+  const Layout L = make_layout(level);
+  return align_up(real_bytes * L.stride, 256) + align_up(real_bytes * (comp_stride(level) + 64), 256) + 256;
+}
+
+// Per-device set-up, run by the first call on a device with that device
+// current: the device address of the scratch array, the finite-element
+// tables in constant memory, the SM count.
+int noalloc_setup(int dev, NoAllocDevice** out) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  NoAllocDevice& d = g_noalloc_dev[dev];
+  if (!d.ready) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr) return MSGPU_ERR_CUDA;
+    FeTables t;
+    host_fe_tables(t);
+    if (cudaMemcpyToSymbol(c_fe, &t, sizeof(t)) != cudaSuccess) return MSGPU_ERR_CUDA;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+      return MSGPU_ERR_CUDA;
+    d.scratch = (unsigned char*)p;
+    d.sms = sms;
+    d.ready = true;
+  }
+  *out = &d;
+  return MSGPU_OK;
+}
+
+#define NA_CK(call)                                \
+  do {                                             \
+    if ((call) != cudaSuccess) return MSGPU_ERR_CUDA; \
+  } while (0)
+
+template <typename Real>
+int noalloc_level(const NoAllocDevice& dv, int level, const double* d_R, const double* d_T, double* d_phi,
+                  double lambda, int max_iter, double stop_eps, double* d_energy, int* d_steps, cudaStream_t st) {
+  const Layout L = make_layout(level);
+  const size_t cs = comp_stride(level);
+  const size_t arena_b = align_up(sizeof(Real) * L.stride, 256);
+  const size_t ref_b = align_up(sizeof(Real) * (cs + 64), 256);
+  Real* arena = (Real*)dv.scratch;
+  Real* Rd = (Real*)(dv.scratch + arena_b);
+  double* e_slot = (double*)(dv.scratch + arena_b + ref_b);
+  int* i_slot = (int*)(e_slot + 1);  // [0] steps, [1] buffer holding phi
+  // The scratch keeps the previous call's contents: clear everything the
+  // kernel reads before writing (as the allocating entry point does).
+  NA_CK(cudaMemsetAsync(dv.scratch, 0, arena_b + ref_b + 256, st));
+  const int nl = lvl_n(level);
+  const size_t N = lvl_N(level);
+  const unsigned gx = (unsigned)std::min<size_t>(1024, (N + 255) / 256);
+  k_to_pitched<double, Real><<<gx, 256, 0, st>>>(d_R, 0, Rd, 0, nl);
+  k_to_pitched<double, Real><<<gx, 256, 0, st>>>(d_T, 0, arena + L.off_T[level], 0, nl);
+  k_to_pitched<double, Real><<<gx, 256, 0, st>>>(d_phi, 0, arena + L.off_phi[0], 0, nl);
+  k_to_pitched<double, Real><<<gx, 256, 0, st>>>(d_phi + N, 0, arena + L.off_phi[0] + cs, 0, nl);
+  NA_CK(cudaGetLastError());
+  LevelArgs<Real> a;
+  memset(&a, 0, sizeof(a));
+  a.arena = arena;
+  a.inst_stride = L.stride;
+  a.R = Rd;
+  a.off_T = L.off_T[level];
+  a.off_phi[0] = L.off_phi[0];
+  a.off_phi[1] = L.off_phi[1];
+  a.off_d[0] = L.off_d[0];
+  a.off_d[1] = L.off_d[1];
+  a.off_s = L.off_s;
+  a.off_de = L.off_de;
+  for (int k = 0; k <= kMaxLevel; ++k) { a.off_x2[k] = L.off_x2[k]; a.off_x5[k] = L.off_x5[k]; a.off_b[k] = L.off_b[k]; }
+  a.level = level;
+  a.n = nl;
+  a.num_inst = 1;
+  a.lc = pick_lc<Real>(level);
+  a.mode = MODE_SOLVE;
+  a.lambda = lambda;
+  a.stop_eps = stop_eps;
+  a.sigma_fixed = 0;
+  a.max_iter = max_iter;
+  a.phi_in_dev = i_slot + 1;  // zeroed above: phi starts in buffer 0
+  a.out_energy = d_energy ? d_energy : e_slot;
+  a.out_steps = d_steps ? d_steps : i_slot;
+  a.out_phi_buf = i_slot + 1;
+  // Launch: the largest cluster (up to the level's useful size) that the
+  // occupancy query admits.
+  const size_t smem = level_smem_bytes<Real>(a.lc);
+  NA_CK(cudaFuncSetAttribute(level_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  NA_CK(cudaFuncSetAttribute(level_kernel<Real>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  int g = pick_cluster(dv.sms, 1, level);
+  for (; g >= 1; --g) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = g;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(kThreads, 1, 1);
+    cfg.gridDim = dim3(g, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, level_kernel<Real>, &cfg) != cudaSuccess) {
+      (void)cudaGetLastError();
+      continue;
+    }
+    if (clusters < 1) continue;
+    NA_CK(cudaLaunchKernelEx(&cfg, level_kernel<Real>, a));
+    break;
+  }
+  if (g < 1) return MSGPU_ERR_CUDA;
+  // result: [phi_x, phi_y] dense, from whichever buffer the solve ended in
+  k_phi_out<Real><<<dim3(gx, 1), 256, 0, st>>>(arena, L.stride, L.off_phi[0], L.off_phi[1], level, i_slot + 1,
+                                               d_phi);
+  NA_CK(cudaGetLastError());
+  return MSGPU_OK;
+}
+#undef NA_CK
+
+}  // namespace
+
+extern "C" int msgpu_gd_level_noalloc(int level, const double* d_R, const double* d_T, double* d_phi,
+                                      double lambda, int max_iter, double stop_eps, int use_fp64,
+                                      double* d_energy_out, int* d_steps_out, void* stream) {
+  if (level < 1 || level > kMaxLevel || !d_R || !d_T || !d_phi || max_iter < 0) return MSGPU_ERR_INVALID_ARG;
+  if (noalloc_bytes_needed(level, use_fp64 ? sizeof(double) : sizeof(float)) > kNoAllocScratchBytes)
+    return MSGPU_ERR_SIZE;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return MSGPU_ERR_CUDA;
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return MSGPU_ERR_UNSUPPORTED;
+  NoAllocDevice* dv = nullptr;
+  int rc = noalloc_setup(dev, &dv);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  return use_fp64 ? noalloc_level<double>(*dv, level, d_R, d_T, d_phi, lambda, max_iter, stop_eps, d_energy_out,
+                                          d_steps_out, st)
+                  : noalloc_level<float>(*dv, level, d_R, d_T, d_phi, lambda, max_iter, stop_eps, d_energy_out,
+                                         d_steps_out, st);
+}
