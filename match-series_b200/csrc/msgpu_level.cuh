@@ -687,114 +687,138 @@ struct UpPass {
 };
 
 // Coarse part of the V-cycle, levels lc..0, by one CTA in shared memory
-// (MDMultigrid::solve recursion including the 100 sweeps on level 0).
-// Layout per level k (dense, width 2^k+1): x[c], b[c], tmp[c].
+// (MDMultigrid::solve recursion including the 100 sweeps on level 0,
+// linearSmoothOp.cpp:451-494, 556-580).
+// Layout per level k (dense, width w = 2^k+1): slots 0/1 hold the iterate
+// (ping-pong), slot 2 the right-hand side, each with two components.
+// The offset of level k is sum_{j<k} 6 (2^j+1)^2 = 2(4^k-1) + 12(2^k-1) + 6k.
 __host__ __device__ inline size_t coarse_level_offset(int k) {
-  size_t off = 0;
-  for (int j = 0; j < k; ++j) {
-    const size_t w = (size_t)(1 << j) + 1;
-    off += 6 * w * w;
-  }
-  return off;
+  return (size_t)2 * ((1u << (2 * k)) - 1u) + (size_t)12 * ((1u << k) - 1u) + (size_t)6 * k;
 }
 __host__ __device__ inline size_t coarse_smem_elems(int lc) { return coarse_level_offset(lc + 1); }
 
 template <typename Real>
+struct Coarse {
+  Real* sm;
+  double tau;
+  unsigned cur = 0;  // bit k: slot holding the iterate of level k
+  __device__ Real* S(int k, int slot, int c) const {
+    const int w = (1 << k) + 1;
+    return sm + coarse_level_offset(k) + (size_t)(2 * slot + c) * (size_t)(w * w);
+  }
+  __device__ int slot(int k) const { return (int)((cur >> k) & 1u); }
+  __device__ Real hsq(int k) const {
+    const int w = (1 << k) + 1;
+    return (Real)(tau * (double)((w - 1) * (w - 1)));
+  }
+  __device__ Real diag(int k) const {
+    const int w = (1 << k) + 1;
+    return (Real)(1 + 4 * tau * (double)((w - 1) * (w - 1)));
+  }
+
+  // One Jacobi sweep (HeatMultigrid::jacobi) on level k; the items are
+  // (component, node) pairs, components stacked in y.
+  __device__ void sweep(int k) {
+    const int w = (1 << k) + 1, s = slot(k);
+    const Real h2 = hsq(k), dg = diag(k);
+    for_rect(w, 2 * w, [&](int x, int yy) {
+      const int c = yy >= w, y = yy - c * w, id = y * w + x;
+      const Real* xs = S(k, s, c);
+      const Real a = heat_row<Real>(x, y, w, h2, [&](int i, int j) { return xs[j * w + i]; });
+      S(k, s ^ 1, c)[id] = jacobi_update(xs[id], S(k, 2, c)[id], a, dg);
+    });
+    cur ^= 1u << k;
+    __syncthreads();
+  }
+
+  // Second pre-sweep, residual, restriction to level k-1 and (k-1 >= 1) the
+  // first pre-sweep of level k-1 from x = 0, where A 0 is exactly +0.
+  __device__ void down(int k) {
+    sweep(k);
+    const int w = (1 << k) + 1, cw = (1 << (k - 1)) + 1, s = slot(k);
+    const Real h2 = hsq(k);
+    for_rect(w, 2 * w, [&](int x, int yy) {
+      const int c = yy >= w, y = yy - c * w, id = y * w + x;
+      const Real* xs = S(k, s, c);
+      const Real a = heat_row<Real>(x, y, w, h2, [&](int i, int j) { return xs[j * w + i]; });
+      S(k, s ^ 1, c)[id] = S(k, 2, c)[id] - a;
+    });
+    __syncthreads();
+    const Real cdg = diag(k - 1);
+    const bool first_sweep = (k - 1 >= 1);
+    for_rect(cw, 2 * cw, [&](int X, int YY) {
+      const int c = YY >= cw, Y = YY - c * cw, id = Y * cw + X;
+      const Real* rs = S(k, s ^ 1, c);
+      const Real v = restrict_node<Real>(X, Y, cw, [&](int i, int j) { return rs[j * w + i]; });
+      S(k - 1, 2, c)[id] = v;
+      if (first_sweep) S(k - 1, 0, c)[id] = jacobi_update(Real(0), v, Real(0), cdg);
+    });
+    cur &= ~(1u << (k - 1));  // level k-1 iterate in slot 0
+    __syncthreads();
+  }
+
+  // Correction x3 = x2 + P x_coarse, then the two post-sweeps.
+  __device__ void up(int k) {
+    const int w = (1 << k) + 1, cw = (1 << (k - 1)) + 1, s = slot(k), sc = slot(k - 1);
+    for_rect(w, 2 * w, [&](int x, int yy) {
+      const int c = yy >= w, y = yy - c * w, id = y * w + x;
+      const Real* xc = S(k - 1, sc, c);
+      const Real p = prolong_node<Real>(x, y, [&](int X, int Y) { return xc[Y * cw + X]; });
+      S(k, s, c)[id] += p;
+    });
+    __syncthreads();
+    sweep(k);
+    sweep(k);
+  }
+
+  // Level 0 (2 x 2 nodes, all corners): 100 sweeps from x = 0 by the first 8
+  // lanes (component x node), the iterate in registers, neighbours by shuffle.
+  __device__ void bottom() {
+    if (threadIdx.x < 32) {
+      const int lane = threadIdx.x, c = (lane >> 2) & 1, i = lane & 3, x = i & 1, y = i >> 1;
+      const Real h2 = hsq(0), dg = diag(0);
+      const Real bv = (lane < 8) ? S(0, 2, c)[i] : Real(0);
+      Real xv = Real(0);
+      for (int it = 0; it < 100; ++it) {
+        const Real nx = __shfl_xor_sync(0xffffffffu, xv, 1);  // node (x^1, y)
+        const Real ny = __shfl_xor_sync(0xffffffffu, xv, 2);  // node (x, y^1)
+        const Real a = heat_row<Real>(x, y, 2, h2, [&](int p, int q) { return (p != x) ? nx : ((q != y) ? ny : xv); });
+        xv = jacobi_update(xv, bv, a, dg);
+      }
+      if (lane < 8) S(0, slot(0), c)[i] = xv;
+    }
+    __syncthreads();
+  }
+};
+
+template <typename Real>
 __device__ void coarse_vcycle(int lc, double tau, Real* sm, const Real* bx, const Real* by, Real sgn, Real* outx,
                               Real* outy, bool want_norm, double part[kRedSlots]) {
-  // slot 0/1: x (ping-pong), slot 2: b -- each with two components
-  auto S = [&](int k, int slot, int c) {
-    const size_t w = (size_t)(1 << k) + 1;
-    return sm + coarse_level_offset(k) + (size_t)(2 * slot + c) * w * w;
-  };
-  int cur[kMaxLevel + 1];
-  for (int k = 0; k <= lc; ++k) cur[k] = 0;
+  Coarse<Real> C{sm, tau};
   const int wl = (1 << lc) + 1, Pl = pitch_of(wl);
-  for (int i = threadIdx.x; i < wl * wl; i += kThreads) {
-    const size_t g = (size_t)(i / wl) * Pl + (i % wl);
-    S(lc, 2, 0)[i] = bx[g] * sgn;
-    S(lc, 2, 1)[i] = by[g] * sgn;
-    S(lc, 0, 0)[i] = Real(0);
-    S(lc, 0, 1)[i] = Real(0);
-  }
-  __syncthreads();
-  // One Jacobi sweep (HeatMultigrid::jacobi, linearSmoothOp.cpp:556-580): the
-  // new iterate goes to the other slot.
-  auto jacobi_sweep = [&](int k) {
-    const int w = (1 << k) + 1;
-    const Real hsq = (Real)(tau * (double)((w - 1) * (w - 1)));
-    const Real diag = (Real)(1 + 4 * tau * (double)((w - 1) * (w - 1)));
-    const int src = cur[k], dst = cur[k] ^ 1;
-    for (int i = threadIdx.x; i < 2 * w * w; i += kThreads) {
-      const int c = i / (w * w), id = i % (w * w);
-      const Real* xs = S(k, src, c);
-      const Real ax = heat_row<Real>(id % w, id / w, w, hsq, [&](int a, int b) { return xs[b * w + a]; });
-      S(k, dst, c)[id] = jacobi_update(xs[id], S(k, 2, c)[id], ax, diag);
-    }
-    cur[k] = dst;
+  {
+    // right-hand side and the first pre-sweep from x = 0 on level lc
+    const Real dg = C.diag(lc);
+    for_rect(wl, 2 * wl, [&](int x, int yy) {
+      const int c = yy >= wl, y = yy - c * wl, id = y * wl + x;
+      const Real r = (c ? by : bx)[(size_t)y * Pl + x] * sgn;
+      C.S(lc, 2, c)[id] = r;
+      C.S(lc, 0, c)[id] = jacobi_update(Real(0), r, Real(0), dg);
+    });
     __syncthreads();
-  };
-  for (int k = lc; k >= 1; --k) {
-    const int w = (1 << k) + 1, cw = (1 << (k - 1)) + 1;
-    const Real hsq = (Real)(tau * (double)((w - 1) * (w - 1)));
-    jacobi_sweep(k);
-    jacobi_sweep(k);
-    // residual into the free slot, then restriction
-    {
-      const int src = cur[k], dst = cur[k] ^ 1;
-      for (int i = threadIdx.x; i < 2 * w * w; i += kThreads) {
-        const int c = i / (w * w), id = i % (w * w);
-        const Real* xs = S(k, src, c);
-        const Real ax = heat_row<Real>(id % w, id / w, w, hsq, [&](int a, int b) { return xs[b * w + a]; });
-        S(k, dst, c)[id] = S(k, 2, c)[id] - ax;
-      }
-      __syncthreads();
-      for (int i = threadIdx.x; i < 2 * cw * cw; i += kThreads) {
-        const int c = i / (cw * cw), id = i % (cw * cw);
-        const Real* rs = S(k, dst, c);
-        S(k - 1, 2, c)[id] = restrict_node<Real>(id % cw, id / cw, cw, [&](int a, int b) { return rs[b * w + a]; });
-        S(k - 1, 0, c)[id] = Real(0);
-      }
-      cur[k - 1] = 0;
-      __syncthreads();
-    }
   }
-  // level 0: 100 sweeps by one warp (2 components x 4 nodes)
-  if (threadIdx.x < 32) {
-    const Real hsq = (Real)(tau * 1.0), diag = (Real)(1 + 4 * tau * 1.0);
-    const int c = (threadIdx.x >> 2) & 1, id = threadIdx.x & 3;
-    Real* x0 = S(0, 0, c);
-    for (int it = 0; it < 100; ++it) {
-      Real ax = Real(0);
-      if (threadIdx.x < 8) ax = heat_row<Real>(id & 1, id >> 1, 2, hsq, [&](int a, int b) { return x0[b * 2 + a]; });
-      __syncwarp();
-      if (threadIdx.x < 8) x0[id] = jacobi_update(x0[id], S(0, 2, c)[id], ax, diag);
-      __syncwarp();
-    }
-  }
-  __syncthreads();
-  for (int k = 1; k <= lc; ++k) {
-    const int w = (1 << k) + 1, cw = (1 << (k - 1)) + 1;
-    {
-      const int src = cur[k - 1];
-      for (int i = threadIdx.x; i < 2 * w * w; i += kThreads) {
-        const int c = i / (w * w), id = i % (w * w);
-        const Real* xc = S(k - 1, src, c);
-        const Real p = prolong_node<Real>(id % w, id / w, [&](int a, int b) { return xc[b * cw + a]; });
-        S(k, cur[k], c)[id] += p;
-      }
-      __syncthreads();
-    }
-    jacobi_sweep(k);
-    jacobi_sweep(k);
-  }
-  for (int i = threadIdx.x; i < wl * wl; i += kThreads) {
-    const Real a = S(lc, cur[lc], 0)[i], b = S(lc, cur[lc], 1)[i];
-    const size_t g = (size_t)(i / wl) * Pl + (i % wl);
+  for (int k = lc; k >= 1; --k) C.down(k);
+  C.bottom();
+  for (int k = 1; k <= lc; ++k) C.up(k);
+  const Real *s0 = C.S(lc, C.slot(lc), 0), *s1 = C.S(lc, C.slot(lc), 1);
+  for_rect(wl, wl, [&](int x, int y) {
+    const int id = y * wl + x;
+    const Real a = s0[id], b = s1[id];
+    const size_t g = (size_t)y * Pl + x;
     outx[g] = a;
     outy[g] = b;
     if (want_norm) part[0] += (double)a * (double)a + (double)b * (double)b;
-  }
+  });
 }
 
 // Dynamic shared memory of the level kernel (elements of Real).
