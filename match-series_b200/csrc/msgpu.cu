@@ -33,13 +33,14 @@ struct msgpu_context {
   cudaStream_t stream = nullptr;
   // growable device buffers
   struct Buf { void* p = nullptr; size_t cap = 0; };
-  Buf arena, shared_real, dscratch, small, phis_d, io[6], prof;
+  Buf arena, shared_real, dscratch, small, phis_d, io[6], prof, sched, flags;
+  int* sched_error = nullptr;  // device flag of the level scheduler (in flags)
   // statistics of the last batch call
   bool profiling = false;
   msgpu_stats stats{};
   cudaEvent_t ev[32] = {};
   bool ev_ready = false;
-  int last_cluster = 0;
+  int last_grid = 0;        // CTAs of the last level launch
 };
 
 namespace {
@@ -488,68 +489,106 @@ int pick_lc(int level) {
   return std::min(level, 5);
 }
 
-// Largest useful cluster size of a level: one CTA per 2k nodes, at most 16
-// (the non-portable maximum).
-int max_cluster_for_level(int level) {
-  const size_t N = lvl_N(level);
-  return (int)std::min<size_t>(16, std::max<size_t>(1, N / 2048));
+// Largest number of tiles of any pass of a level (the per-tile partial sums
+// of one instance).
+int level_max_tiles(int level) {
+  const int e = lvl_n(level) - 1;
+  const int el = std::max(1, e / TX) * std::max(1, e / TY);
+  const int vt = std::max(1, e / VTX) * std::max(1, e / VTY);
+  return std::max(el, vt);
 }
 
-// About two CTAs per SM over all instances, so that no cluster has CTAs
-// sharing an SM while others run alone (every cluster waits for its slowest CTA).
-int pick_cluster(int sms, int num_inst, int level) {
-  const int fill = std::max(1, (2 * sms) / std::max(1, num_inst));
-  return std::max(1, std::min(max_cluster_for_level(level), fill));
+// Scheduler state of a level launch: dispenser words, the finished counter,
+// per-instance control blocks, per-tile partial sums.
+size_t sched_bytes(int num_inst, int max_tiles) {
+  return align_up(sizeof(unsigned long long) * kWordStride * (size_t)num_inst, 256) + 256 +
+         align_up(sizeof(InstCtl) * (size_t)num_inst, 256) +
+         align_up(sizeof(double) * kRedSlots * (size_t)max_tiles * num_inst, 256);
 }
 
 template <typename Real>
-int launch_level(msgpu_context* ctx, LevelArgs<Real>& a, int G, cudaStream_t st) {
-  const size_t smem = level_smem_bytes<Real>(a.lc);
-  CK(cudaFuncSetAttribute(level_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  CK(cudaFuncSetAttribute(level_kernel<Real>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-  int best_g = 0, best_c = 0;
-  for (int g = G; g >= 1; --g) {
-    cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = g;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.blockDim = dim3(kThreads, 1, 1);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cfg.gridDim = dim3(g * std::max(1, a.num_inst), 1, 1);
-    int max_clusters = 0;
-    cudaError_t e = cudaOccupancyMaxActiveClusters(&max_clusters, level_kernel<Real>, &cfg);
-    if (e != cudaSuccess) { (void)cudaGetLastError(); continue; }
-    if (max_clusters < 1) continue;
-    if (best_g == 0) { best_g = g; best_c = max_clusters; }
-    if (max_clusters >= a.num_inst) { best_g = g; best_c = max_clusters; break; }
-  }
-  if (best_g == 0)
-    return fail(ctx, MSGPU_ERR_CUDA, "level kernel cannot be resident (smem %zu B)", smem);
-  {
-    const int g = best_g;
-    cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = g;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.blockDim = dim3(kThreads, 1, 1);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    const int nclusters = std::min(a.num_inst, best_c);
-    cfg.gridDim = dim3(g * nclusters, 1, 1);
-    ctx->last_cluster = g;
-    CK(cudaLaunchKernelEx(&cfg, level_kernel<Real>, a));
-    return MSGPU_OK;
-  }
+SchedPtrs<Real> carve_sched(void* mem, int num_inst, int max_tiles, size_t* zero_bytes) {
+  unsigned char* p = (unsigned char*)mem;
+  SchedPtrs<Real> sp;
+  sp.words = (unsigned long long*)p;
+  p += align_up(sizeof(unsigned long long) * kWordStride * (size_t)num_inst, 256);
+  sp.finished = (int*)p;
+  sp.error = nullptr;
+  p += 256;
+  *zero_bytes = (size_t)(p - (unsigned char*)mem);
+  sp.ctl = (InstCtl*)p;
+  p += align_up(sizeof(InstCtl) * (size_t)num_inst, 256);
+  sp.partials = (double*)p;
+  sp.max_tiles = max_tiles;
+  return sp;
 }
+
+// Launches the level kernel as a cooperative grid (every CTA resident, two
+// per SM where registers and shared memory allow); sched_mem holds
+// sched_bytes(a.num_inst, level_max_tiles(a.level)) bytes.
+// error_flag: device int, set by a worker that gave up waiting for work; it
+// is cleared by the caller at the start of an API call, not per launch.
+template <typename Real>
+cudaError_t launch_level_core(LevelArgs<Real>& a, void* sched_mem, int* error_flag, int sms, cudaStream_t st,
+                              int* grid_out) {
+  const int max_tiles = level_max_tiles(a.level);
+  size_t zb = 0;
+  SchedPtrs<Real> sp = carve_sched<Real>(sched_mem, a.num_inst, max_tiles, &zb);
+  sp.error = error_flag;
+  cudaError_t e = cudaMemsetAsync(sched_mem, 0, zb, st);
+  if (e != cudaSuccess) return e;
+  const size_t smem = level_smem_bytes<Real>(a.lc);
+  e = cudaFuncSetAttribute(level_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, level_kernel<Real>, kThreads, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  const int grid = per_sm * sms;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.gridDim = dim3(grid, 1, 1);
+  cfg.blockDim = dim3(kThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (grid_out) *grid_out = grid;
+  return cudaLaunchKernelEx(&cfg, level_kernel<Real>, a, sp);
+}
+
+template <typename Real>
+int launch_level(msgpu_context* ctx, LevelArgs<Real>& a, cudaStream_t st) {
+  int rc;
+  if ((rc = ensure(ctx, ctx->sched, sched_bytes(a.num_inst, level_max_tiles(a.level))))) return rc;
+  CK(launch_level_core<Real>(a, ctx->sched.p, ctx->sched_error, ctx->sm_count, st, &ctx->last_grid));
+  return MSGPU_OK;
+}
+
+// Clears the scheduler error flag at the start of an API call.
+int sched_error_reset(msgpu_context* ctx, cudaStream_t st) {
+  int rc;
+  if (!ctx->sched_error) {
+    if ((rc = ensure(ctx, ctx->flags, 256))) return rc;
+    ctx->sched_error = (int*)ctx->flags.p;
+  }
+  CK(cudaMemsetAsync(ctx->sched_error, 0, sizeof(int), st));
+  return MSGPU_OK;
+}
+
+// After the call's work has completed: reports a scheduler that stalled.
+int sched_error_check(msgpu_context* ctx) {
+  int h = 0;
+  if (!ctx->sched_error) return MSGPU_OK;
+  CK(cudaMemcpy(&h, ctx->sched_error, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) return fail(ctx, MSGPU_ERR_CUDA, "level kernel: a worker waited too long for work (scheduler stalled)");
+  return MSGPU_OK;
+}
+
+// Upper bound on the CTAs of a level launch (for the per-CTA pass counters).
+int max_level_grid(int sms) { return 4 * sms; }
 
 // ---------------------------------------------------------------------------
 struct BatchIO {
@@ -570,6 +609,7 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
   const Layout L = make_layout(M);
   int rc;
   if ((rc = ensure_tables(ctx))) return rc;
+  if ((rc = sched_error_reset(ctx, st))) return rc;
   // --- double scratch: per image a pyramid from Lin down to 0
   std::vector<size_t> poff(Lin + 1);
   size_t pstride = 0;
@@ -696,16 +736,15 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
     a.out_steps = steps_all + (size_t)(l - start) * F;
     a.out_evals = evals_all + (size_t)(l - start) * F;
     a.out_phi_buf = bin;   // the level kernel updates the buffer index in place
-    const int G = pick_cluster(ctx->sm_count, F, l);
-    const size_t prof_n = (size_t)16 * F * kPassKinds;
+    const size_t prof_n = (size_t)max_level_grid(ctx->sm_count) * kPassKinds;
     if (ctx->profiling) {
       if ((rc = ensure(ctx, ctx->prof, sizeof(unsigned long long) * prof_n * nlev_all))) return rc;
       a.pass_cycles = (unsigned long long*)ctx->prof.p + prof_n * (l - start);
       CK(cudaMemsetAsync(a.pass_cycles, 0, sizeof(unsigned long long) * prof_n, st));
     }
     if (ctx->profiling && l - start < 16) CK(cudaEventRecord(ctx->ev[2 * (l - start)], st));
-    if ((rc = launch_level<Real>(ctx, a, G, st))) return rc;
-    if (l - start < 16) ctx->stats.level_cluster[l - start] = ctx->last_cluster;
+    if ((rc = launch_level<Real>(ctx, a, st))) return rc;
+    if (l - start < 16) ctx->stats.level_cluster[l - start] = ctx->last_grid;
     if (ctx->profiling && l - start < 16) CK(cudaEventRecord(ctx->ev[2 * (l - start) + 1], st));
     k_collect<<<1, 256, 0, st>>>(e_lvl, a.out_steps, F, (l == stop) ? io.energies_out : nullptr, io.steps_out,
                                  nlev, l - start);
@@ -747,17 +786,16 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
       ctx->stats.level_steps[k] = ss;
       ctx->stats.level_evals[k] = ee;
     }
-    const size_t prof_n = (size_t)16 * F * kPassKinds;
+    const size_t prof_n = (size_t)max_level_grid(ctx->sm_count) * kPassKinds;
     std::vector<unsigned long long> pc(prof_n);
     for (int k = 0; k < nlev_all && k < 16; ++k) {
       CK(cudaMemcpy(pc.data(), (unsigned long long*)ctx->prof.p + prof_n * k, sizeof(unsigned long long) * prof_n,
                     cudaMemcpyDeviceToHost));
-      const int G = ctx->stats.level_cluster[k];
-      const int nctas = G * std::min(F, 16 * F / std::max(1, G));  // upper bound on CTAs launched
+      const int nctas = std::min<int>(ctx->stats.level_cluster[k], max_level_grid(ctx->sm_count));
       for (int q = 0; q < kPassKinds && q < 8; ++q) {
-        unsigned long long mx = 0;
-        for (int c = 0; c < nctas && (size_t)c * kPassKinds + q < prof_n; ++c)
-          mx = std::max(mx, pc[(size_t)c * kPassKinds + q]);
+        unsigned long long sum = 0;
+        for (int c = 0; c < nctas; ++c) sum += pc[(size_t)c * kPassKinds + q];
+        const unsigned long long mx = nctas > 0 ? sum / (unsigned long long)nctas : 0ull;
         ctx->stats.level_pass_cycles[k][q] = (long long)mx;
       }
     }
@@ -894,6 +932,7 @@ int msgpu_register_batch(msgpu_context* ctx, const msgpu_params* p, const double
   CK(cudaMemcpyAsync(e.data(), d_e, sizeof(double) * F, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(s.data(), d_s, sizeof(int) * F * nlev, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  if ((rc = sched_error_check(ctx))) return rc;
   if (energies_out) memcpy(energies_out, e.data(), sizeof(double) * F);
   if (steps_out) memcpy(steps_out, s.data(), sizeof(int) * F * nlev);
   return MSGPU_OK;
@@ -968,6 +1007,7 @@ int msgpu_match_series_stage(msgpu_context* ctx, const msgpu_params* p, const do
   CK(cudaMemcpyAsync(e.data(), d_e, sizeof(double) * F, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(s.data(), d_s, sizeof(int) * F * nlev, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  if ((rc = sched_error_check(ctx))) return rc;
   if (energies_out) memcpy(energies_out, e.data(), sizeof(double) * F);
   if (steps_out) memcpy(steps_out, s.data(), sizeof(int) * F * nlev);
   return MSGPU_OK;
@@ -1081,8 +1121,8 @@ int single_level(msgpu_context* ctx, int level, int mode, const double* R, const
   a.out_phi_buf = d_i + 1;
   a.trace = trace ? d_trace : nullptr;
   a.max_trace = max_trace;
-  const int G = pick_cluster(ctx->sm_count, 1, level);
-  if ((rc = launch_level<Real>(ctx, a, G, st))) return rc;
+  if ((rc = sched_error_reset(ctx, st))) return rc;
+  if ((rc = launch_level<Real>(ctx, a, st))) return rc;
   CK(cudaGetLastError());
   // outputs
   int hi[2] = {0, 0};
@@ -1090,6 +1130,7 @@ int single_level(msgpu_context* ctx, int level, int mode, const double* R, const
   CK(cudaMemcpyAsync(&he, d_e, sizeof(double), cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(hi, d_i, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  if ((rc = sched_error_check(ctx))) return rc;
   if (energy_out) *energy_out = he;
   if (steps_out) *steps_out = hi[0];
   auto fetch = [&](size_t off, double* dst) -> int {
@@ -1262,7 +1303,8 @@ std::mutex g_noalloc_mu;
 
 size_t noalloc_bytes_needed(int level, size_t real_bytes) {
   const Layout L = make_layout(level);
-  return align_up(real_bytes * L.stride, 256) + align_up(real_bytes * (comp_stride(level) + 64), 256) + 256;
+  return align_up(real_bytes * L.stride, 256) + align_up(real_bytes * (comp_stride(level) + 64), 256) + 256 +
+         sched_bytes(1, level_max_tiles(level));
 }
 
 // Per-device set-up, run by the first call on a device with that device
@@ -1303,7 +1345,7 @@ int noalloc_level(const NoAllocDevice& dv, int level, const double* d_R, const d
   Real* arena = (Real*)dv.scratch;
   Real* Rd = (Real*)(dv.scratch + arena_b);
   double* e_slot = (double*)(dv.scratch + arena_b + ref_b);
-  int* i_slot = (int*)(e_slot + 1);  // [0] steps, [1] buffer holding phi
+  int* i_slot = (int*)(e_slot + 1);  // [0] steps, [1] buffer holding phi; e_slot[4]: scheduler error flag
   // The scratch keeps the previous call's contents: clear everything the
   // kernel reads before writing (as the allocating entry point does).
   NA_CK(cudaMemsetAsync(dv.scratch, 0, arena_b + ref_b + 256, st));
@@ -1341,35 +1383,10 @@ int noalloc_level(const NoAllocDevice& dv, int level, const double* d_R, const d
   a.out_energy = d_energy ? d_energy : e_slot;
   a.out_steps = d_steps ? d_steps : i_slot;
   a.out_phi_buf = i_slot + 1;
-  // Launch: the largest cluster (up to the level's useful size) that the
-  // occupancy query admits.
-  const size_t smem = level_smem_bytes<Real>(a.lc);
-  NA_CK(cudaFuncSetAttribute(level_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  NA_CK(cudaFuncSetAttribute(level_kernel<Real>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-  int g = pick_cluster(dv.sms, 1, level);
-  for (; g >= 1; --g) {
-    cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = g;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.blockDim = dim3(kThreads, 1, 1);
-    cfg.gridDim = dim3(g, 1, 1);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    int clusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&clusters, level_kernel<Real>, &cfg) != cudaSuccess) {
-      (void)cudaGetLastError();
-      continue;
-    }
-    if (clusters < 1) continue;
-    NA_CK(cudaLaunchKernelEx(&cfg, level_kernel<Real>, a));
-    break;
-  }
-  if (g < 1) return MSGPU_ERR_CUDA;
+  // the level kernel's scheduler state follows the other scratch
+  unsigned char* sched = dv.scratch + arena_b + ref_b + 256;
+  int* err = (int*)(e_slot + 4);
+  NA_CK(launch_level_core<Real>(a, sched, err, dv.sms, st, nullptr));
   // result: [phi_x, phi_y] dense, from whichever buffer the solve ended in
   k_phi_out<Real><<<dim3(gx, 1), 256, 0, st>>>(arena, L.stride, L.off_phi[0], L.off_phi[1], level, i_slot + 1,
                                                d_phi);

@@ -1,22 +1,23 @@
 // msgpu_level.cuh -- the per-level solve as ONE persistent launch.
 //
 // Each registration instance (a template frame registered to the reference on
-// one level of the multilevel pyramid) is owned by one thread-block cluster.
-// The CTAs of the cluster split every data-parallel pass over the level's
-// node tiles, synchronise with the hardware cluster barrier, and reduce their
-// partial sums through distributed shared memory in a fixed rank order, so
-// every CTA holds identical scalars and takes identical control decisions.
-// The whole gradient flow of the level -- H1 metric V-cycle, Fletcher-Reeves
-// NCG, Armijo line search, filter-width (sigma) schedule and stopping rule --
-// runs on the device without host round trips:
+// one level of the multilevel pyramid) runs the whole gradient flow of the
+// level -- H1 metric V-cycle, Fletcher-Reeves NCG, Armijo line search,
+// filter-width (sigma) schedule and stopping rule -- on the device without
+// host round trips:
 //   GradientDescentBase::applySingle            gradientDescent.h:295-464
 //   calcTaudAndDescentDir                       gradientDescent.h:200-236
 //   GradientDescentWithAutomaticFilterWidth     gradientDescent.h:675-691
 //   getTimestepWidthWithArmijoLineSearch        ArmijoSearch.h:118-200
 //   LinearSmoothOp::apply / MDMultigrid::solve  linearSmoothOp.cpp:451-612
-// Control flow is bounded: the step loop by max_iter, each line search by the
-// tau range [2^-30, 2^25].  No CTA waits on anything but the cluster barrier
-// and its own asynchronous copies.
+// Every data-parallel pass of an instance is cut into node tiles, and one
+// persistent grid of CTAs (two per SM) executes the tiles of all instances
+// through a task scheduler (end of this file): tiles are handed out in
+// chunks, and whoever completes the last chunk of a pass reduces the
+// per-chunk partial sums in chunk order and takes the instance's next control
+// decision.  Control flow is bounded: the step
+// loop by max_iter, each line search by the tau range [2^-30, 2^25], every
+// wait for work by an iteration limit.
 //
 // Every pass is a double-buffered tile pipeline: while a CTA computes one
 // 64 x 4 node tile from shared memory, cp.async streams the windows (tile plus
@@ -25,13 +26,9 @@
 // aligned 16-byte chunks.
 #pragma once
 
-#include <cooperative_groups.h>
-
 #include "msgpu_fe.cuh"
 
 namespace msg {
-
-namespace cg = cooperative_groups;
 
 constexpr int kThreads = 256;
 constexpr int kMaxLevel = 12;
@@ -113,50 +110,10 @@ struct PassTimer {
 };
 
 // ---------------------------------------------------------------------------
-// Cluster-wide deterministic reduction of kRedSlots doubles.
-struct RedShared {
-  double warp[kThreads / 32][kRedSlots];
-  double slot[2][kRedSlots];  // double-buffered per-CTA partials read through DSMEM
-};
-
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
-}
-
-// Returns the cluster totals in out[] (identical in every thread of every CTA).
-__device__ __forceinline__ void cluster_reduce(cg::cluster_group& cluster, RedShared& rs, int& parity,
-                                               const double part[kRedSlots], double out[kRedSlots]) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int k = 0; k < kRedSlots; ++k) {
-    const double v = warp_sum(part[k]);
-    if (lane == 0) rs.warp[wid][k] = v;
-  }
-  __syncthreads();
-  if (threadIdx.x < kRedSlots) {
-    double s = 0.0;
-#pragma unroll
-    for (int w = 0; w < kThreads / 32; ++w) s += rs.warp[w][threadIdx.x];
-    rs.slot[parity][threadIdx.x] = s;
-  }
-  __threadfence();
-  cluster.sync();
-  const unsigned G = cluster.num_blocks();
-#pragma unroll
-  for (int k = 0; k < kRedSlots; ++k) out[k] = 0.0;
-  for (unsigned r = 0; r < G; ++r) {
-    const double* remote = cluster.map_shared_rank(&rs.slot[parity][0], r);
-#pragma unroll
-    for (int k = 0; k < kRedSlots; ++k) out[k] += remote[k];
-  }
-  parity ^= 1;
-}
-
-__device__ __forceinline__ void cluster_barrier(cg::cluster_group& cluster) {
-  __threadfence();
-  cluster.sync();
 }
 
 // ---------------------------------------------------------------------------
@@ -186,27 +143,6 @@ __device__ __forceinline__ void load_window(Real* sm, const Real* g, int n, int 
     const Real* src = ok ? g + (size_t)y * P + x : g;
     cp_async16(sm + wy * WW + cx * C, src, ok);
   }
-}
-
-// Double-buffered tile loop: ps.issue(t, stage) starts the copies of tile t,
-// ps.compute(t, stage) consumes them.
-template <class Pass>
-__device__ __forceinline__ void tile_pipeline(Pass& ps, int ntiles, int rank, int G) {
-  int stage = 0;
-  if (rank < ntiles) ps.issue(rank, 0);
-  cp_async_commit();
-  for (int t = rank; t < ntiles; t += G) {
-    const int tn = t + G;
-    if (tn < ntiles) ps.issue(tn, stage ^ 1);
-    cp_async_commit();
-    cp_async_wait<1>();
-    __syncthreads();
-    ps.compute(t, stage);
-    __syncthreads();
-    stage ^= 1;
-  }
-  cp_async_wait<0>();
-  __syncthreads();
 }
 
 // Tile geometry of a level with n nodes per side and tiles of tx x ty nodes;
@@ -517,7 +453,7 @@ struct GradPass {
 };
 
 // ---------------------------------------------------------------------------
-// Multigrid V-cycle passes on the levels above lc (cluster passes).
+// Multigrid V-cycle passes on the levels above lc (tiled passes).
 
 // Pre-smoothing (2 Jacobi sweeps from x = 0), residual and restriction
 // (MDMultigrid::solve steps 1-3, linearSmoothOp.cpp:465-477).
@@ -835,311 +771,737 @@ __host__ __device__ inline size_t level_smem_elems(int lc) {
   return e;
 }
 
-// Full V-cycle on the current level: rhs = -DE (finest), output s.
-// Returns |s|^2 (cluster total) in norm_out.
-template <typename Real>
-__device__ void vcycle(cg::cluster_group& cluster, RedShared& rs, int& parity, const LevelArgs<Real>& a,
-                       const Inst<Real>& I, double tau, Real* smem, int rank, int G, double& norm_out,
-                       PassTimer& pt) {
-  const int L = a.level;
-  const size_t cs = comp_stride(L);
-  const Real* dex = I.arr(a.off_de);
-  const Real* dey = dex + cs;
-  Real* sx = I.arr(a.off_s);
-  Real* sy = sx + cs;
-  double part[kRedSlots] = {0, 0, 0, 0}, tot[kRedSlots];
-  for (int k = L; k > a.lc; --k) {
-    const int w = (1 << k) + 1;
-    const Real hsq = (Real)(tau * (double)((w - 1) * (w - 1)));
-    const Real diag = (Real)(1 + 4 * tau * (double)((w - 1) * (w - 1)));
-    const Real* rx = (k == L) ? dex : I.arr(a.off_b[k]);
-    const Real* ry = (k == L) ? dey : rx + comp_stride(k);
-    Real* x2 = I.arr(a.off_x2[k]);
-    Real* bc = I.arr(a.off_b[k - 1]);
-    DownPass<Real> ps(w, rx, ry, (k == L) ? Real(-1) : Real(1), x2, x2 + comp_stride(k), bc,
-                      bc + comp_stride(k - 1), hsq, diag, smem);
-    Tiles tl(w, VTX, VTY);
-    MSG_TIMED(pt, PK_VDOWN, tile_pipeline(ps, tl.count(), rank, G));
-    MSG_TIMED(pt, PK_REDUCE, cluster_barrier(cluster));
-  }
-  if (rank == 0) {
-    const int lc = a.lc;
-    const Real* bx = (L == lc) ? dex : I.arr(a.off_b[lc]);
-    const Real* by = (L == lc) ? dey : bx + comp_stride(lc);
-    Real* out = (L == lc) ? sx : I.arr(a.off_x5[lc]);
-    Real* outy = (L == lc) ? sy : out + comp_stride(lc);
-    MSG_TIMED(pt, PK_VCOARSE, coarse_vcycle<Real>(lc, tau, smem, bx, by, (L == lc) ? Real(-1) : Real(1), out, outy,
-                                                  L == lc, part));
-  }
-  if (L == a.lc) {
-    MSG_TIMED(pt, PK_REDUCE, cluster_reduce(cluster, rs, parity, part, tot));
-    norm_out = tot[0];
-    return;
-  }
-  MSG_TIMED(pt, PK_REDUCE, cluster_barrier(cluster));
-  for (int k = a.lc + 1; k <= L; ++k) {
-    const int w = (1 << k) + 1;
-    const Real hsq = (Real)(tau * (double)((w - 1) * (w - 1)));
-    const Real diag = (Real)(1 + 4 * tau * (double)((w - 1) * (w - 1)));
-    const Real* rx = (k == L) ? dex : I.arr(a.off_b[k]);
-    const Real* ry = (k == L) ? dey : rx + comp_stride(k);
-    const Real* x2 = I.arr(a.off_x2[k]);
-    const Real* xc = I.arr(a.off_x5[k - 1]);
-    Real* o = (k == L) ? sx : I.arr(a.off_x5[k]);
-    Real* oy = (k == L) ? sy : o + comp_stride(k);
-    UpPass<Real> ps(w, rx, ry, (k == L) ? Real(-1) : Real(1), x2, x2 + comp_stride(k), xc,
-                    xc + comp_stride(k - 1), o, oy, hsq, diag, smem, k == L, part);
-    Tiles tl(w, VTX, VTY);
-    MSG_TIMED(pt, PK_VUP, tile_pipeline(ps, tl.count(), rank, G));
-    if (k < L) MSG_TIMED(pt, PK_REDUCE, cluster_barrier(cluster));
-  }
-  MSG_TIMED(pt, PK_REDUCE, cluster_reduce(cluster, rs, parity, part, tot));
-  norm_out = tot[0];
-}
-
 __device__ __forceinline__ bool finite_d(double x) { return !isnan(x) && !isinf(x); }
 
 // ---------------------------------------------------------------------------
+// Persistent task scheduler of the level kernel.
+//
+// A level solve of one instance is a chain of passes (initial energy,
+// gradient, V-cycle down per level, coarse V-cycle, V-cycle up per level,
+// NCG + first Armijo trial, further trials, final flush).  Every pass is cut
+// into tiles.  All CTAs of the launch pull chunks of tiles from whichever
+// instance has a published pass with chunks left; the CTA that completes the
+// last chunk of a pass reduces the per-chunk partial sums in chunk order (so every total is
+// independent of which CTA did what), runs the instance's descent control
+// (gradientDescent.h / ArmijoSearch.h) and publishes the next pass.  No CTA
+// ever waits for a particular other CTA, so uneven SM sharing, slow tiles and
+// the single-CTA coarse V-cycle of one instance are hidden by the work of the
+// others.
+//
+// Tiles are handed out in chunks of consecutive tiles.  Dispenser word per
+// instance: [63:40] pass sequence number, [39:20] chunks of the pass, [19:0]
+// next chunk.  A worker reads the word and only when chunks are left takes
+// one with an atomic increment; an increment that arrives after the next pass
+// was published takes a valid chunk of that pass, whose descriptor was written
+// (and fenced) before the word.  Every wait for work is
+// bounded; a worker that gives up sets the error flag and all workers return.
+enum TaskKind : int { TK_E0 = 0, TK_GRAD, TK_VDOWN, TK_COARSE, TK_VUP, TK_NCG, TK_TRIAL, TK_FLUSH, TK_DONE };
+__device__ __forceinline__ int task_pass_kind(int kind) {
+  switch (kind) {
+    case TK_E0: return PK_ENERGY0;
+    case TK_GRAD: return PK_GRAD;
+    case TK_VDOWN: return PK_VDOWN;
+    case TK_COARSE: return PK_VCOARSE;
+    case TK_VUP: return PK_VUP;
+    case TK_NCG: return PK_NCG;
+    default: return PK_ENERGY;
+  }
+}
+constexpr int PF_STEP = 1;     // GRAD / FLUSH: add tau_p * d[dcur] to phi[cur]
+constexpr int PF_ODZERO = 2;   // NCG: the old direction is zero (d = s)
+
+struct PassDesc {
+  int kind, k, cur, dcur, dn, flags;
+  int ntiles, chunk;   // tiles of the pass, tiles per dispensed chunk
+  double t;      // trial step (NCG, TRIAL) or pending step (GRAD, FLUSH)
+  double beta;   // Fletcher-Reeves factor (NCG)
+  double vtau;   // tau of the V-cycle passes
+};
+
+// Descent state of one instance; written only by the CTA completing a pass.
+struct InstCtl {
+  PassDesc desc;
+  int done;            // tiles of the current pass completed
+  int ls;              // TRIAL role: 0 doubling, 1 halving, 2 energy at the accepted step
+  int iter, evals, total_evals, attempt, rb_pos, pending, od_zero, cur, dcur;
+  double energy, energy_new, f, sigma, sigma_used, tau, og2, A, Bd, Cd, Df, t, beta, tau_p;
+  double rb_tau[2], rb_e[2];
+};
+constexpr int kCtlWords = (int)((sizeof(InstCtl) + 7) / 8);
+constexpr int kWordStride = 16;  // dispenser words 128 bytes apart
+
+__host__ __device__ inline unsigned long long pack_word(unsigned long long seq, int ntiles, int next) {
+  return ((seq & 0xFFFFFFull) << 40) | ((unsigned long long)(ntiles & 0xFFFFF) << 20) | (unsigned long long)(next & 0xFFFFF);
+}
+
 template <typename Real>
-__global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  Real* smem = reinterpret_cast<Real*>(smem_raw);
-  __shared__ RedShared rs;
-  cg::cluster_group cluster = cg::this_cluster();
-  const int G = (int)cluster.num_blocks();
-  const int rank = (int)cluster.block_rank();
-  const int cid = blockIdx.x / G;
-  const int nclusters = gridDim.x / G;
-  int parity = 0;
-  const int n = a.n;
-  const size_t cs = comp_stride(a.level);
-  const double lam = a.lambda;
-  PassTimer pt{a.pass_cycles ? a.pass_cycles + (size_t)blockIdx.x * kPassKinds : nullptr, 0};
+struct SchedPtrs {
+  InstCtl* ctl;                 // num_inst
+  unsigned long long* words;    // num_inst * kWordStride
+  double* partials;             // num_inst * max_tiles * kRedSlots
+  int* finished;                // instances finished
+  int* error;                   // non-zero: a worker gave up waiting
+  int max_tiles;
+};
 
-  for (int inst = cid; inst < a.num_inst; inst += nclusters) {
-    Inst<Real> I;
-    I.base = a.arena + (size_t)inst * a.inst_stride;
-    I.R = a.R;
-    I.T = I.base + a.off_T;
-    I.n = n;
-    I.P = pitch_of(n);
-    I.h = (Real)(1.0 / (double)(n - 1));
-    Real* de = I.arr(a.off_de);
-    Real* s = I.arr(a.off_s);
-    int cur = a.phi_in_dev ? a.phi_in_dev[inst] : 0;  // buffer holding phi
-    int dcur = 0;                                     // buffer holding the current direction d
-    double part[kRedSlots], tot[kRedSlots];
+template <typename Real>
+__device__ __forceinline__ Inst<Real> make_inst(const LevelArgs<Real>& a, int inst) {
+  Inst<Real> I;
+  I.base = a.arena + (size_t)inst * a.inst_stride;
+  I.R = a.R;
+  I.T = I.base + a.off_T;
+  I.n = a.n;
+  I.P = pitch_of(a.n);
+  I.h = (Real)(1.0 / (double)(a.n - 1));
+  return I;
+}
 
-    auto reset = [&]() {
-#pragma unroll
-      for (int k = 0; k < kRedSlots; ++k) part[k] = 0.0;
-    };
-    Real* phi = I.arr(a.off_phi[cur]);
-
-    if (a.mode == MODE_SMOOTH) {
-      double nrm;
-      vcycle<Real>(cluster, rs, parity, a, I, (double)(0.5f * (a.sigma_fixed * a.sigma_fixed)), smem, rank, G,
-                   nrm, pt);
-      cluster_barrier(cluster);
-      continue;
+__device__ __forceinline__ int pass_tiles(int kind, int k, int level, int n) {
+  switch (kind) {
+    case TK_VDOWN:
+    case TK_VUP: {
+      const int w = (1 << k) + 1;
+      int nx = (w - 1) / VTX, ny = (w - 1) / VTY;
+      return (nx < 1 ? 1 : nx) * (ny < 1 ? 1 : ny);
     }
-
-    // initial energy E(phi) = E_data + lambda * 1/2 phi.L phi   (gradientDescent.h:306)
-    reset();
-    {
-      EnergyPass<Real> ps(I, 0, Real(0), Real(0), false, phi, phi + cs, nullptr, nullptr, nullptr, nullptr,
-                          nullptr, nullptr, nullptr, nullptr, smem, part);
-      MSG_TIMED(pt, PK_ENERGY0, tile_pipeline(ps, ps.tl.count(), rank, G));
-    }
-    MSG_TIMED(pt, PK_REDUCE, cluster_reduce(cluster, rs, parity, part, tot));
-    double A = tot[1];
-    auto energy_of = [&](double edata, double ereg) {
-      double e = 0.0;
-      e += edata;
-      if (lam != 1.0) e += lam * ereg; else e += ereg;
-      return e;
-    };
-    double energy = energy_of(tot[0], 0.5 * A);
-    double energy_new = energy;
-
-    if (a.mode == MODE_ENERGY) {
-      reset();
-      Real* nphi = I.arr(a.off_phi[cur ^ 1]);
-      GradPass<Real> ps(I, false, Real(0), lam, phi, phi + cs, nullptr, nullptr, nphi, nphi + cs, de, de + cs,
-                        smem, part);
-      tile_pipeline(ps, ps.tl.count(), rank, G);
-      cluster_barrier(cluster);
-      if (rank == 0 && threadIdx.x == 0) {
-        a.out_energy[inst] = energy;
-        a.out_steps[inst] = 0;
-        a.out_phi_buf[inst] = cur;
-      }
-      continue;
-    }
-
-    double tau = 1.0, sigma = 1.0;
-    const double tau_min = 9.313225746154785e-10;  // 2^-30 (ArmijoSearch.h:77)
-    const double tau_max = 33554432.0;             // 2^25  (ArmijoSearch.h:67)
-    const double stop_sigma = 0.0001, sigma_tol = 0.00001;
-    double og2 = 0.0;           // |OldGradient|^2
-    bool od_zero = true;        // OldDirection is zero (start, or after the NCG fallback)
-    double rb_tau[2] = {nan(""), nan("")}, rb_e[2] = {0, 0};
-    int rb_pos = 0;
-    bool pending = false;       // a step tau_p * d[dcur] still has to be added to phi
-    double tau_p = 0.0;
-    int iter = 0;
-    int total_evals = 0;
-
-    if (a.max_iter > 0) {
-      bool go;
-      do {
-        iter++;
-        energy = energy_new;
-        const double f = energy;
-        const double sigma_used = sigma;
-        int evals = 0;
-        // DE at the current position; applies the pending update (ping-pong phi)
-        reset();
-        {
-          Real* nphi = I.arr(a.off_phi[cur ^ 1]);
-          const Real* dd = I.arr(a.off_d[dcur]);
-          GradPass<Real> ps(I, pending, (Real)tau_p, lam, phi, phi + cs, dd, dd + cs, nphi, nphi + cs, de, de + cs,
-                            smem, part);
-          MSG_TIMED(pt, PK_GRAD, tile_pipeline(ps, ps.tl.count(), rank, G));
-          cur ^= 1;
-          phi = nphi;
-          pending = false;
-        }
-        MSG_TIMED(pt, PK_REDUCE, cluster_reduce(cluster, rs, parity, part, tot));
-        A = tot[1];
-        // H1 smoothing of -DE (the descent direction's metric)
-        double s2;
-        vcycle<Real>(cluster, rs, parity, a, I, (double)(0.5f * (sigma * sigma)), smem, rank, G, s2, pt);
-        // Fletcher-Reeves (gradientDescent.h:221-226)
-        const double beta = ((iter - 1) % 10) ? (s2 / og2) : 0.0;
-        og2 = s2;
-
-        // Armijo line search with the NCG direction, then the NCG fallback
-        double Bd = 0.0, Cd = 0.0;
-        auto eval_at = [&](double tt) {
-          // energy at phi + tt d; E_reg by the exact quadratic expansion in tt
-          reset();
-          const Real* dd = I.arr(a.off_d[dcur]);
-          EnergyPass<Real> ps(I, 1, (Real)tt, Real(0), false, phi, phi + cs, dd, dd + cs, nullptr, nullptr,
-                              nullptr, nullptr, nullptr, nullptr, smem, part);
-          MSG_TIMED(pt, PK_ENERGY, tile_pipeline(ps, ps.tl.count(), rank, G));
-          MSG_TIMED(pt, PK_REDUCE, cluster_reduce(cluster, rs, parity, part, tot));
-          const double e = energy_of(tot[0], 0.5 * ((A + 2.0 * tt * Bd) + tt * tt * Cd));
-          rb_tau[rb_pos] = tt;
-          rb_e[rb_pos] = e;
-          rb_pos ^= 1;
-          evals++;
-          return e;
-        };
-        double acc_tau = 0.0;
-        for (int attempt = 0; attempt < 2; ++attempt) {
-          const bool fallback = (attempt == 1);
-          const int dn = dcur ^ 1;   // buffer receiving the new direction
-          Real* wd = I.arr(a.off_d[dn]);
-          const Real* od = I.arr(a.off_d[dcur]);
-          double t = (attempt == 0) ? tau : 0.0;
-          t = t < tau_min ? tau_min : (t > tau_max ? tau_max : t);
-          // first trial fused with the direction materialisation
-          reset();
-          {
-            EnergyPass<Real> ps(I, 2, (Real)t, (Real)beta, fallback || od_zero, phi, phi + cs, od, od + cs, s,
-                                s + cs, de, de + cs, wd, wd + cs, smem, part);
-            MSG_TIMED(pt, PK_NCG, tile_pipeline(ps, ps.tl.count(), rank, G));
-          }
-          MSG_TIMED(pt, PK_REDUCE, cluster_reduce(cluster, rs, parity, part, tot));
-          dcur = dn;
-          const double Df = tot[1];
-          Bd = tot[2];
-          Cd = tot[3];
-          double fnew = energy_of(tot[0], 0.5 * ((A + 2.0 * t * Bd) + t * t * Cd));
-          rb_tau[rb_pos] = t;
-          rb_e[rb_pos] = fnew;
-          rb_pos ^= 1;
-          evals++;
-          double G_ = (fnew - f) / (Df * t);
-          double res;
-          if (Df >= 0) {
-            res = 0.0;
-          } else if (!finite_d(f)) {
-            res = 0.0;
-          } else {
-            if (G_ >= 0.5 && f >= fnew) {
-              do {
-                t *= 2.;
-                fnew = eval_at(t);
-                G_ = (fnew - f) / (Df * t);
-              } while (G_ >= 0.5 && f >= fnew && t <= tau_max);
-              t *= 0.5;
-            } else {
-              do {
-                if (t > tau_min) t *= 0.5;
-                fnew = eval_at(t);
-                G_ = (fnew - f) / (Df * t);
-              } while ((!finite_d(fnew) || (G_ < 0.5 || f < fnew)) && (t > tau_min));
-            }
-            res = (t > tau_min) ? t : 0.0;
-          }
-          acc_tau = res;
-          od_zero = fallback;
-          if (res != 0.0) break;
-        }
-        tau = acc_tau;
-        // energy at the new position (gradientDescent.h:365-395)
-        double en = nan("");
-        if (rb_tau[0] == tau) en = rb_e[0];
-        else if (rb_tau[1] == tau) en = rb_e[1];
-        else if (tau == 0) en = energy;
-        if (isnan(en) && tau != 0) en = eval_at(tau);
-        if (tau != 0) {
-          pending = true;
-          tau_p = tau;
-        }
-        energy_new = en;
-        total_evals += evals;
-        if (a.trace && rank == 0 && threadIdx.x == 0 && iter <= a.max_trace) {
-          double* tr = a.trace + ((size_t)inst * a.max_trace + (iter - 1)) * 4;
-          tr[0] = energy_new;
-          tr[1] = tau;
-          tr[2] = sigma_used;
-          tr[3] = evals;
-        }
-        go = ((energy - energy_new) > a.stop_eps) && (iter < a.max_iter);
-        if ((0.5 * sigma > stop_sigma) && ((energy - energy_new) < sigma_tol)) {
-          sigma *= 0.5;
-          tau = 1.;
-          go = (sigma > stop_sigma) && (iter < a.max_iter);
-        }
-      } while (go);
-    }
-    // flush the last accepted step into phi
-    if (pending) {
-      Real* nphi = I.arr(a.off_phi[cur ^ 1]);
-      const Real* dd = I.arr(a.off_d[dcur]);
-      const Real tp = (Real)tau_p;
-      const int P = I.P;
-      for (size_t i = (size_t)rank * kThreads + threadIdx.x; i < (size_t)n * n; i += (size_t)G * kThreads) {
-        const size_t g = (i / n) * P + (i % n);
-        Real vx = phi[g], vy = phi[cs + g];
-        vx += tp * dd[g];
-        vy += tp * dd[cs + g];
-        nphi[g] = vx;
-        nphi[cs + g] = vy;
-      }
-      cur ^= 1;
-    }
-    cluster_barrier(cluster);
-    if (rank == 0 && threadIdx.x == 0) {
-      a.out_energy[inst] = energy_new;
-      a.out_steps[inst] = iter;
-      a.out_phi_buf[inst] = cur;
-      if (a.out_evals) a.out_evals[inst] = total_evals;
+    case TK_COARSE: return 1;
+    default: {
+      int nx = (n - 1) / TX, ny = (n - 1) / TY;
+      return (nx < 1 ? 1 : nx) * (ny < 1 ? 1 : ny);
     }
   }
+}
+
+// Tiles per dispensed chunk: large enough that taking a chunk (a few L2
+// round trips) is small against its work, small enough that a pass still
+// spreads over many CTAs.  A function of the pass alone, so the chunk
+// partition -- and with it every reduction order -- does not depend on the
+// schedule.
+__device__ __forceinline__ int chunk_tiles(int ntiles) {
+  const int c = ntiles / 24;
+  return c < 1 ? 1 : (c > 16 ? 16 : c);
+}
+
+// Tiles of one pass: issue(t, stage) starts the window copies, compute(t,
+// stage) does the work and accumulates part[].
+template <typename Real>
+struct TaskRunner {
+  const LevelArgs<Real>& a;
+  Real* smem;
+  __device__ TaskRunner(const LevelArgs<Real>& a_, Real* sm) : a(a_), smem(sm) {}
+
+  template <class F>
+  __device__ void with_pass(int inst, const PassDesc& d, double* part, F&& f) const {
+    const Inst<Real> I = make_inst(a, inst);
+    const int L = a.level;
+    const size_t cs = comp_stride(L);
+    Real* phi = I.arr(a.off_phi[d.cur]);
+    Real* de = I.arr(a.off_de);
+    Real* s = I.arr(a.off_s);
+    switch (d.kind) {
+      case TK_E0: {
+        EnergyPass<Real> ps(I, 0, Real(0), Real(0), false, phi, phi + cs, nullptr, nullptr, nullptr, nullptr, nullptr,
+                            nullptr, nullptr, nullptr, smem, part);
+        f(ps);
+        break;
+      }
+      case TK_TRIAL: {
+        const Real* dd = I.arr(a.off_d[d.dcur]);
+        EnergyPass<Real> ps(I, 1, (Real)d.t, Real(0), false, phi, phi + cs, dd, dd + cs, nullptr, nullptr, nullptr,
+                            nullptr, nullptr, nullptr, smem, part);
+        f(ps);
+        break;
+      }
+      case TK_NCG: {
+        const Real* od = I.arr(a.off_d[d.dcur]);
+        Real* wd = I.arr(a.off_d[d.dn]);
+        EnergyPass<Real> ps(I, 2, (Real)d.t, (Real)d.beta, (d.flags & PF_ODZERO) != 0, phi, phi + cs, od, od + cs, s,
+                            s + cs, de, de + cs, wd, wd + cs, smem, part);
+        f(ps);
+        break;
+      }
+      case TK_GRAD: {
+        Real* nphi = I.arr(a.off_phi[d.cur ^ 1]);
+        const Real* dd = I.arr(a.off_d[d.dcur]);
+        GradPass<Real> ps(I, (d.flags & PF_STEP) != 0, (Real)d.t, a.lambda, phi, phi + cs, dd, dd + cs, nphi,
+                          nphi + cs, de, de + cs, smem, part);
+        f(ps);
+        break;
+      }
+      case TK_VDOWN: {
+        const int k = d.k, w = (1 << k) + 1;
+        const Real hsq = (Real)(d.vtau * (double)((w - 1) * (w - 1)));
+        const Real diag = (Real)(1 + 4 * d.vtau * (double)((w - 1) * (w - 1)));
+        const Real* rx = (k == L) ? de : I.arr(a.off_b[k]);
+        const Real* ry = (k == L) ? de + cs : rx + comp_stride(k);
+        Real* x2 = I.arr(a.off_x2[k]);
+        Real* bc = I.arr(a.off_b[k - 1]);
+        DownPass<Real> ps(w, rx, ry, (k == L) ? Real(-1) : Real(1), x2, x2 + comp_stride(k), bc,
+                          bc + comp_stride(k - 1), hsq, diag, smem);
+        f(ps);
+        break;
+      }
+      case TK_VUP: {
+        const int k = d.k, w = (1 << k) + 1;
+        const Real hsq = (Real)(d.vtau * (double)((w - 1) * (w - 1)));
+        const Real diag = (Real)(1 + 4 * d.vtau * (double)((w - 1) * (w - 1)));
+        const Real* rx = (k == L) ? de : I.arr(a.off_b[k]);
+        const Real* ry = (k == L) ? de + cs : rx + comp_stride(k);
+        const Real* x2 = I.arr(a.off_x2[k]);
+        const Real* xc = I.arr(a.off_x5[k - 1]);
+        Real* o = (k == L) ? s : I.arr(a.off_x5[k]);
+        Real* oy = (k == L) ? s + cs : o + comp_stride(k);
+        UpPass<Real> ps(w, rx, ry, (k == L) ? Real(-1) : Real(1), x2, x2 + comp_stride(k), xc,
+                        xc + comp_stride(k - 1), o, oy, hsq, diag, smem, k == L, part);
+        f(ps);
+        break;
+      }
+      default: break;
+    }
+  }
+
+  __device__ void issue(int inst, const PassDesc& d, int tile, int stage) const {
+    if (d.kind == TK_COARSE || d.kind == TK_FLUSH) return;  // these read global memory directly
+    double dummy[kRedSlots];
+    with_pass(inst, d, dummy, [&](auto& ps) { ps.issue(tile, stage); });
+  }
+
+  __device__ void compute(int inst, const PassDesc& d, int tile, int stage, double* part) const {
+    if (d.kind == TK_COARSE) {
+      const Inst<Real> I = make_inst(a, inst);
+      const int L = a.level, lc = a.lc;
+      const size_t cs = comp_stride(L);
+      Real* de = I.arr(a.off_de);
+      Real* s = I.arr(a.off_s);
+      const Real* bx = (L == lc) ? de : I.arr(a.off_b[lc]);
+      const Real* by = (L == lc) ? de + cs : bx + comp_stride(lc);
+      Real* out = (L == lc) ? s : I.arr(a.off_x5[lc]);
+      Real* outy = (L == lc) ? s + cs : out + comp_stride(lc);
+      coarse_vcycle<Real>(lc, d.vtau, smem, bx, by, (L == lc) ? Real(-1) : Real(1), out, outy, L == lc, part);
+      return;
+    }
+    if (d.kind == TK_FLUSH) {
+      // phi[cur^1] = phi[cur] + tau_p d[dcur] on the tile's nodes (gradientDescent.h:385-387)
+      const Inst<Real> I = make_inst(a, inst);
+      const size_t cs = comp_stride(a.level);
+      const Real* phi = I.arr(a.off_phi[d.cur]);
+      Real* nphi = I.arr(a.off_phi[d.cur ^ 1]);
+      const Real* dd = I.arr(a.off_d[d.dcur]);
+      const Real tp = (Real)d.t;
+      Tiles tl(a.n);
+      int x0, x1, y0, y1;
+      tl.rect(tile, x0, x1, y0, y1);
+      for_rect(x1 - x0, y1 - y0, [&](int ix, int iy) {
+        const size_t g = (size_t)(y0 + iy) * I.P + (x0 + ix);
+        Real vx = __ldcg(phi + g), vy = __ldcg(phi + cs + g);
+        vx += tp * __ldcg(dd + g);
+        vy += tp * __ldcg(dd + cs + g);
+        nphi[g] = vx;
+        nphi[cs + g] = vy;
+      });
+      return;
+    }
+    with_pass(inst, d, part, [&](auto& ps) { ps.compute(tile, stage); });
+  }
+};
+
+// Deterministic CTA sum of kRedSlots per-thread values (warp butterflies,
+// then the warps in order); the result is in out[] for every thread.
+__device__ __forceinline__ void block_sum(const double part[kRedSlots], double (*wbuf)[kRedSlots],
+                                          double* out) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < kRedSlots; ++k) {
+    const double v = warp_sum(part[k]);
+    if (lane == 0) wbuf[wid][k] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < kRedSlots) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) s += wbuf[w][threadIdx.x];
+    out[threadIdx.x] = s;
+  }
+  __syncthreads();
+}
+
+// Descent control of one instance after a completed pass (run by one thread
+// on a private copy of the state).  tot[] are the pass's totals.  Fills c.desc
+// with the next pass; kind TK_DONE when the level solve is finished.
+// Follows GradientDescentBase::applySingle with the automatic filter width
+// (gradientDescent.h:295-464, 675-691), Fletcher-Reeves NCG
+// (gradientDescent.h:200-236) and ArmijoLineSearchUsingOp
+// (ArmijoSearch.h:118-200).
+template <typename Real>
+__device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const double tot[kRedSlots]) {
+  const double lam = a.lambda;
+  const double tau_min = 9.313225746154785e-10;  // 2^-30 (ArmijoSearch.h:77)
+  const double tau_max = 33554432.0;             // 2^25  (ArmijoSearch.h:67)
+  const double stop_sigma = 0.0001, sigma_tol = 0.00001;
+  const int L = a.level, lc = a.lc;
+  PassDesc& d = c.desc;
+  auto energy_of = [&](double edata, double ereg) {
+    double e = 0.0;
+    e += edata;
+    if (lam != 1.0) e += lam * ereg; else e += ereg;
+    return e;
+  };
+  auto quad = [&](double tt) { return 0.5 * ((c.A + 2.0 * tt * c.Bd) + tt * tt * c.Cd); };
+  auto start_vcycle = [&](double vtau) {
+    d.vtau = vtau;
+    if (L > lc) { d.kind = TK_VDOWN; d.k = L; } else { d.kind = TK_COARSE; d.k = lc; }
+  };
+  auto start_iteration = [&]() {
+    c.iter++;
+    c.energy = c.energy_new;
+    c.f = c.energy;
+    c.sigma_used = c.sigma;
+    c.evals = 0;
+    d.kind = TK_GRAD;
+    d.cur = c.cur;
+    d.dcur = c.dcur;
+    d.flags = c.pending ? PF_STEP : 0;
+    d.t = c.tau_p;
+  };
+  auto finish = [&]() {
+    if (c.pending) {
+      d.kind = TK_FLUSH;
+      d.cur = c.cur;
+      d.dcur = c.dcur;
+      d.t = c.tau_p;
+      d.flags = PF_STEP;
+    } else {
+      d.kind = TK_DONE;
+    }
+  };
+  auto start_attempt = [&]() {
+    const bool fallback = (c.attempt == 1);
+    double t = (c.attempt == 0) ? c.tau : 0.0;
+    t = t < tau_min ? tau_min : (t > tau_max ? tau_max : t);
+    c.t = t;
+    d.kind = TK_NCG;
+    d.cur = c.cur;
+    d.dcur = c.dcur;
+    d.dn = c.dcur ^ 1;
+    d.t = t;
+    d.beta = c.beta;
+    d.flags = (fallback || c.od_zero) ? PF_ODZERO : 0;
+  };
+  auto trial = [&](double t, int role) {
+    c.t = t;
+    c.ls = role;
+    d.kind = TK_TRIAL;
+    d.cur = c.cur;
+    d.dcur = c.dcur;
+    d.t = t;
+  };
+  auto push_ring = [&](double t, double e) {
+    c.rb_tau[c.rb_pos] = t;
+    c.rb_e[c.rb_pos] = e;
+    c.rb_pos ^= 1;
+    c.evals++;
+  };
+  auto end_iteration = [&](double en) {
+    if (c.tau != 0) {
+      c.pending = 1;
+      c.tau_p = c.tau;
+    }
+    c.energy_new = en;
+    c.total_evals += c.evals;
+    if (a.trace && c.iter <= a.max_trace) {
+      double* tr = a.trace + ((size_t)inst * a.max_trace + (c.iter - 1)) * 4;
+      tr[0] = c.energy_new;
+      tr[1] = c.tau;
+      tr[2] = c.sigma_used;
+      tr[3] = c.evals;
+    }
+    bool go = ((c.energy - c.energy_new) > a.stop_eps) && (c.iter < a.max_iter);
+    if ((0.5 * c.sigma > stop_sigma) && ((c.energy - c.energy_new) < sigma_tol)) {
+      c.sigma *= 0.5;
+      c.tau = 1.;
+      go = (c.sigma > stop_sigma) && (c.iter < a.max_iter);
+    }
+    if (go) start_iteration(); else finish();
+  };
+  auto step_done = [&](double acc_tau) {
+    c.tau = acc_tau;
+    // energy at the new position (gradientDescent.h:365-395)
+    double en = nan("");
+    if (c.rb_tau[0] == c.tau) en = c.rb_e[0];
+    else if (c.rb_tau[1] == c.tau) en = c.rb_e[1];
+    else if (c.tau == 0) en = c.energy;
+    if (isnan(en) && c.tau != 0) {
+      trial(c.tau, 2);
+      return;
+    }
+    end_iteration(en);
+  };
+  auto attempt_done = [&](double res) {
+    const bool fallback = (c.attempt == 1);
+    c.od_zero = fallback ? 1 : 0;
+    if (res != 0.0 || fallback) {
+      step_done(res);
+    } else {
+      c.attempt = 1;
+      start_attempt();
+    }
+  };
+
+  switch (d.kind) {
+    case TK_E0: {
+      c.A = tot[1];
+      c.energy = energy_of(tot[0], 0.5 * c.A);
+      c.energy_new = c.energy;
+      if (a.mode == MODE_ENERGY) {
+        d.kind = TK_GRAD;
+        d.cur = c.cur;
+        d.dcur = c.dcur;
+        d.flags = 0;
+        d.t = 0;
+      } else if (a.max_iter > 0) {
+        start_iteration();
+      } else {
+        d.kind = TK_DONE;
+      }
+      break;
+    }
+    case TK_GRAD: {
+      if (a.mode == MODE_ENERGY) {
+        d.kind = TK_DONE;
+        break;
+      }
+      c.A = tot[1];
+      c.cur ^= 1;
+      c.pending = 0;
+      start_vcycle((double)(0.5f * (c.sigma * c.sigma)));
+      break;
+    }
+    case TK_VDOWN: {
+      if (d.k - 1 > lc) d.k -= 1; else { d.kind = TK_COARSE; d.k = lc; }
+      break;
+    }
+    case TK_COARSE:
+    case TK_VUP: {
+      const bool top = (d.kind == TK_COARSE) ? (L == lc) : (d.k == L);
+      if (!top) {
+        d.k = (d.kind == TK_COARSE) ? lc + 1 : d.k + 1;
+        d.kind = TK_VUP;
+        break;
+      }
+      if (a.mode == MODE_SMOOTH) {
+        d.kind = TK_DONE;
+        break;
+      }
+      const double s2 = tot[0];
+      c.beta = ((c.iter - 1) % 10) ? (s2 / c.og2) : 0.0;
+      c.og2 = s2;
+      c.attempt = 0;
+      start_attempt();
+      break;
+    }
+    case TK_NCG: {
+      c.dcur = d.dn;
+      c.Df = tot[1];
+      c.Bd = tot[2];
+      c.Cd = tot[3];
+      const double t = c.t, f = c.f;
+      const double fnew = energy_of(tot[0], quad(t));
+      push_ring(t, fnew);
+      const double G = (fnew - f) / (c.Df * t);
+      if (c.Df >= 0 || !finite_d(f)) {
+        attempt_done(0.0);
+      } else if (G >= 0.5 && f >= fnew) {
+        trial(t * 2., 0);
+      } else {
+        trial((t > tau_min) ? t * 0.5 : t, 1);
+      }
+      break;
+    }
+    case TK_TRIAL: {
+      const double t = c.t, f = c.f;
+      const double fnew = energy_of(tot[0], quad(t));
+      push_ring(t, fnew);
+      if (c.ls == 2) {
+        end_iteration(fnew);
+        break;
+      }
+      const double G = (fnew - f) / (c.Df * t);
+      if (c.ls == 0) {
+        if (G >= 0.5 && f >= fnew && t <= tau_max) {
+          trial(t * 2., 0);
+        } else {
+          const double tt = t * 0.5;
+          attempt_done((tt > tau_min) ? tt : 0.0);
+        }
+      } else {
+        if ((!finite_d(fnew) || (G < 0.5 || f < fnew)) && (t > tau_min)) {
+          trial((t > tau_min) ? t * 0.5 : t, 1);
+        } else {
+          attempt_done((t > tau_min) ? t : 0.0);
+        }
+      }
+      break;
+    }
+    case TK_FLUSH: {
+      c.cur ^= 1;
+      c.pending = 0;
+      d.kind = TK_DONE;
+      break;
+    }
+    default: d.kind = TK_DONE; break;
+  }
+}
+
+__device__ __forceinline__ void init_ctl_state(InstCtl& c, int cur) {
+  memset(&c, 0, sizeof(c));
+  c.cur = cur;
+  c.dcur = 0;
+  c.tau = 1.0;
+  c.sigma = 1.0;
+  c.og2 = 0.0;
+  c.od_zero = 1;
+  c.rb_tau[0] = c.rb_tau[1] = nan("");
+}
+
+__device__ __forceinline__ void ctl_load(InstCtl& dst, const InstCtl* src) {
+  const unsigned long long* s = reinterpret_cast<const unsigned long long*>(src);
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(&dst);
+  for (int i = 0; i < kCtlWords; ++i) d[i] = __ldcg(s + i);
+}
+__device__ __forceinline__ void ctl_store(InstCtl* dst, const InstCtl& src) {
+  const unsigned long long* s = reinterpret_cast<const unsigned long long*>(&src);
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(dst);
+  for (int i = 0; i < kCtlWords; ++i) __stcg(d + i, s[i]);
+}
+
+// Publishes the instance's next pass (thread 0 of the completing CTA), or
+// writes its results and counts it finished.
+template <typename Real>
+__device__ void publish(const LevelArgs<Real>& a, const SchedPtrs<Real>& sp, int inst, InstCtl& c) {
+  unsigned long long* word = sp.words + (size_t)inst * kWordStride;
+  const unsigned long long seq = (atomicAdd(word, 0ull) >> 40) + 1;
+  if (c.desc.kind == TK_DONE) {
+    if (a.mode != MODE_SMOOTH) {
+      a.out_energy[inst] = c.energy_new;
+      a.out_steps[inst] = c.iter;
+      a.out_phi_buf[inst] = c.cur;
+      if (a.out_evals) a.out_evals[inst] = c.total_evals;
+    }
+    c.done = 0;
+    ctl_store(sp.ctl + inst, c);
+    __threadfence();
+    atomicExch(word, pack_word(seq, 0, 0));
+    atomicAdd(sp.finished, 1);
+    return;
+  }
+  c.desc.ntiles = pass_tiles(c.desc.kind, c.desc.k, a.level, a.n);
+  c.desc.chunk = chunk_tiles(c.desc.ntiles);
+  const int nchunks = (c.desc.ntiles + c.desc.chunk - 1) / c.desc.chunk;
+  c.done = 0;
+  ctl_store(sp.ctl + inst, c);
+  __threadfence();
+  atomicExch(word, pack_word(seq, nchunks, 0));
+}
+
+struct TaskSlot {
+  int inst, chunk, nchunks;   // chunk index of the pass, chunks of the pass
+  PassDesc desc;
+};
+
+// One scan over the instances by the first warp (every lane of it calls this):
+// each lane reads the dispenser words of its instances, and the lanes that
+// see chunks left try to take one, in order from `start`.  Returns the same
+// value in every lane; on success the task is in t (written by one lane).
+template <typename Real>
+__device__ bool try_take(const LevelArgs<Real>& a, const SchedPtrs<Real>& sp, int start, TaskSlot& t) {
+  const int lane = threadIdx.x & 31;
+  for (int base = 0; base < a.num_inst; base += 32) {
+    const bool valid = base + lane < a.num_inst;
+    const int inst = valid ? (start + base + lane) % a.num_inst : 0;
+    unsigned long long* word = sp.words + (size_t)inst * kWordStride;
+    bool avail = false;
+    if (valid) {
+      const unsigned long long w = __ldcg(word);
+      avail = (int)(w & 0xFFFFF) < (int)((w >> 20) & 0xFFFFF);
+    }
+    unsigned mask = __ballot_sync(0xffffffffu, avail);
+    while (mask) {
+      const int src = __ffs(mask) - 1;
+      mask &= mask - 1;
+      int got = 0;
+      if (lane == src) {
+        const unsigned long long old = atomicAdd(word, 1ull);
+        const int chunk = (int)(old & 0xFFFFF), nchunks = (int)((old >> 20) & 0xFFFFF);
+        if (chunk < nchunks) {
+          __threadfence();
+          t.inst = inst;
+          t.chunk = chunk;
+          t.nchunks = nchunks;
+          const unsigned long long* src_d = reinterpret_cast<const unsigned long long*>(&sp.ctl[inst].desc);
+          unsigned long long* dst = reinterpret_cast<unsigned long long*>(&t.desc);
+#pragma unroll
+          for (int i = 0; i < (int)(sizeof(PassDesc) / 8); ++i) dst[i] = __ldcg(src_d + i);
+          got = 1;
+        }
+      }
+      if (__shfl_sync(0xffffffffu, got, src)) return true;
+    }
+  }
+  return false;
+}
+
+// Upper bound on one wait for work (nanoseconds of the global timer); beyond
+// it the worker sets the error flag and every worker returns.
+constexpr unsigned long long kMaxIdleNs = 4000000000ull;
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, SchedPtrs<Real> sp) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Real* smem = reinterpret_cast<Real*>(smem_raw);
+  __shared__ double wbuf[kThreads / 32][kRedSlots];
+  __shared__ double tot[kRedSlots];
+  __shared__ TaskSlot slot[2];
+  __shared__ int flag_wait, flag_next, flag_last;
+  __shared__ InstCtl cs;
+  PassTimer pt{a.pass_cycles ? a.pass_cycles + (size_t)blockIdx.x * kPassKinds : nullptr, 0};
+  const TaskRunner<Real> run(a, smem);
+
+  // publish the first pass of the instances this CTA owns
+  if (threadIdx.x == 0) {
+    for (int inst = blockIdx.x; inst < a.num_inst; inst += gridDim.x) {
+      init_ctl_state(cs, a.phi_in_dev ? a.phi_in_dev[inst] : 0);
+      if (a.mode == MODE_SMOOTH) {
+        cs.desc.vtau = (double)(0.5f * (a.sigma_fixed * a.sigma_fixed));
+        if (a.level > a.lc) { cs.desc.kind = TK_VDOWN; cs.desc.k = a.level; }
+        else { cs.desc.kind = TK_COARSE; cs.desc.k = a.lc; }
+      } else {
+        cs.desc.kind = TK_E0;
+      }
+      cs.desc.cur = cs.cur;
+      publish(a, sp, inst, cs);
+    }
+  }
+
+  int cur_slot = 0, stage = 0;
+  bool have = false;
+  int last_inst = (a.num_inst > 0) ? (int)(blockIdx.x % (unsigned)a.num_inst) : 0;
+  for (;;) {
+    if (!have) {
+      // wait for work (bounded)
+      pt.start();
+      if (threadIdx.x < 32) {
+        int code = 0;
+        const unsigned long long t_begin = global_ns();
+        for (;;) {
+          if (try_take(a, sp, last_inst, slot[cur_slot])) { code = 1; break; }
+          int stop = 0;
+          if (threadIdx.x == 0) {
+            if (*(volatile int*)sp.error || *(volatile int*)sp.finished >= a.num_inst) stop = 2;
+            else if (global_ns() - t_begin > kMaxIdleNs) {
+              atomicExch(sp.error, 1);
+              stop = 2;
+            }
+          }
+          stop = __shfl_sync(0xffffffffu, stop, 0);
+          if (stop) { code = stop; break; }
+          __nanosleep(64);
+        }
+        if (threadIdx.x == 0) flag_wait = code;
+      }
+      __syncthreads();
+      pt.stop(PK_REDUCE);
+      if (flag_wait != 1) break;
+      {
+        const TaskSlot& f = slot[cur_slot];
+        run.issue(f.inst, f.desc, f.chunk * f.desc.chunk, stage);
+      }
+      cp_async_commit();
+      have = true;
+    }
+    const TaskSlot t = slot[cur_slot];
+    const int tb = t.chunk * t.desc.chunk;
+    const int te = min(tb + t.desc.chunk, t.desc.ntiles);
+    TaskSlot nt;
+    bool nh = false, pre = false;
+    double part[kRedSlots] = {0.0, 0.0, 0.0, 0.0};
+    pt.start();
+    for (int tile = tb; tile < te; ++tile) {
+      if (tile + 1 < te) {
+        run.issue(t.inst, t.desc, tile + 1, stage ^ 1);
+      } else {
+        // last tile of the chunk: take the next chunk now (without waiting)
+        // and prefetch its first tile when it uses the same layout
+        if (threadIdx.x < 32) {
+          const bool got = try_take(a, sp, t.inst, slot[cur_slot ^ 1]);
+          if (threadIdx.x == 0) flag_next = got ? 1 : 0;
+        }
+        __syncthreads();
+        nh = (flag_next == 1);
+        if (nh) nt = slot[cur_slot ^ 1];
+        pre = nh && nt.desc.kind == t.desc.kind && t.desc.kind != TK_COARSE && t.desc.kind != TK_FLUSH;
+        if (pre) run.issue(nt.inst, nt.desc, nt.chunk * nt.desc.chunk, stage ^ 1);
+      }
+      cp_async_commit();
+      cp_async_wait<1>();
+      __syncthreads();
+      run.compute(t.inst, t.desc, tile, stage, part);
+      __syncthreads();
+      stage ^= 1;
+    }
+    block_sum(part, wbuf, tot);
+    pt.stop(task_pass_kind(t.desc.kind));
+    pt.start();
+    if (threadIdx.x == 0) {
+      double* pp = sp.partials + ((size_t)t.inst * sp.max_tiles + t.chunk) * kRedSlots;
+#pragma unroll
+      for (int k = 0; k < kRedSlots; ++k) __stcg(pp + k, tot[k]);
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int dn = atomicAdd(&sp.ctl[t.inst].done, 1);
+      flag_last = (dn == t.nchunks - 1) ? 1 : 0;
+      __threadfence();
+    }
+    __syncthreads();
+    if (flag_last) {
+      // this CTA completed the pass: totals in chunk order, then the control step
+      double acc[kRedSlots] = {0.0, 0.0, 0.0, 0.0};
+      const double* pp = sp.partials + (size_t)t.inst * sp.max_tiles * kRedSlots;
+      for (int i = threadIdx.x; i < t.nchunks; i += kThreads) {
+#pragma unroll
+        for (int k = 0; k < kRedSlots; ++k) acc[k] += __ldcg(pp + (size_t)i * kRedSlots + k);
+      }
+      block_sum(acc, wbuf, tot);
+      if (threadIdx.x == 0) {
+        ctl_load(cs, sp.ctl + t.inst);
+        advance(a, t.inst, cs, tot);
+        publish(a, sp, t.inst, cs);
+      }
+      __syncthreads();
+    }
+    pt.stop(PK_REDUCE);
+    last_inst = t.inst;
+    if (nh) {
+      cur_slot ^= 1;
+      if (!pre) {
+        cp_async_wait<0>();
+        __syncthreads();
+        run.issue(nt.inst, nt.desc, nt.chunk * nt.desc.chunk, stage);
+        cp_async_commit();
+      }
+    } else {
+      have = false;
+      cp_async_wait<0>();
+      __syncthreads();
+    }
+  }
+  cp_async_wait<0>();
 }
 
 }  // namespace msg
