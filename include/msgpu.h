@@ -110,10 +110,11 @@ typedef struct {
   float level_ms[16];           /* device time of each level launch         */
   long long level_steps[16];    /* gradient steps summed over the frames    */
   long long level_evals[16];    /* energy evaluations summed over the frames */
-  int level_cluster[16];        /* CTAs per instance (cluster size) per level */
-  /* clock cycles per CTA spent in each pass kind of the level kernel:
-   * initial energy, gradient, V-cycle down, coarse V-cycle, V-cycle up,
-   * NCG + first trial, further line-search trials, barriers/reductions     */
+  int level_cluster[16];        /* CTAs of the level launch (persistent grid) */
+  /* clock cycles per CTA (average over the grid) spent in each pass kind of
+   * the level kernel: initial energy, gradient, V-cycle down, coarse
+   * V-cycle, V-cycle up, NCG + first trial, further line-search trials,
+   * waiting for work and completing passes                                 */
   long long level_pass_cycles[16][8];
 } msgpu_stats;
 int msgpu_set_profiling(msgpu_context* ctx, int on);
