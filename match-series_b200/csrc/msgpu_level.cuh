@@ -36,9 +36,9 @@ constexpr int kRedSlots = 4;   // partial sums reduced per pass
 
 // Node tiles: [x0, x0+TX) x [y0, y0+TY); the last tile of a row/column also
 // owns the final node (n-1 = 2^l is a multiple of the tile size for l >= 6).
-constexpr int TX = 64, TY = 4;
+constexpr int TX = 64, TY = 8;
 // Windows of the element passes: nodes [x0-4, x0+68) x [y0-1, y0+6).
-constexpr int EWX = 72, EWY = 7, EWIN = EWX * EWY;
+constexpr int EWX = 72, EWY = TY + 3, EWIN = EWX * EWY;
 // Multigrid passes use taller tiles of VTX x VTY nodes (halo 3 around them):
 // windows of nodes [x0-4, x0+36) x [y0-3, y0+20).
 constexpr int VTX = 32, VTY = 16;
@@ -46,7 +46,7 @@ constexpr int VWX = 40, VWY = 23, VWIN = VWX * VWY;
 // Coarse window of the correction pass: coarse nodes [x0/2-4, x0/2+20) x [y0/2-2, y0/2+11).
 constexpr int CWX = 24, CWY = 13, CWIN = CWX * CWY;
 // Element contributions of the gradient pass: elements [x0-1, x0+65) x [y0-1, y0+5).
-constexpr int GCX = 66, GCY = 6;
+constexpr int GCX = 66, GCY = TY + 2;
 
 // Launch modes of the level kernel.
 enum LevelMode : int {
@@ -215,7 +215,8 @@ struct Inst {
 //           E_data at phi + tau d                   -> part[0]
 //           Df = DE . d, B = phi . L d, C = d . L d -> part[1..3]
 // Windows (EWX x EWY, origin (x0-4, y0-1)) per stage, in this order:
-//   kind 0: phx phy R ; kind 1: phx phy dx dy R ; kind 2: phx phy sx sy odx ody dex dey R
+//   kind 0: phx phy R ; kind 1: phx phy dx dy R ; kind 2: phx phy sx sy odx ody R
+// (kind 2 reads DE, needed at the owned nodes only, straight from L2).
 template <typename Real>
 struct EnergyPass {
   Inst<Real> I;
@@ -234,7 +235,7 @@ struct EnergyPass {
                         const Real* dex_, const Real* dey_, Real* wdx_, Real* wdy_, Real* sm_, double* part_)
       : I(I_), kind(kind_), tau(tau_), beta(beta_), od_zero(odz), phx(phx_), phy(phy_), dx(dx_), dy(dy_),
         sx(sx_), sy(sy_), dex(dex_), dey(dey_), wdx(wdx_), wdy(wdy_), sm(sm_), part(part_), tl(I_.n) {
-    nwin = (kind == 0) ? 3 : (kind == 1 ? 5 : 9);
+    nwin = (kind == 0) ? 3 : (kind == 1 ? 5 : 7);
   }
   __device__ Real* win(int stage, int k) const { return sm + ((size_t)stage * nwin + k) * EWIN; }
 
@@ -256,8 +257,6 @@ struct EnergyPass {
         load_window(win(stage, k + 1), dy, n, P, wx0, wy0, EWX, EWY);
       }
       k += 2;
-      load_window(win(stage, k++), dex, n, P, wx0, wy0, EWX, EWY);
-      load_window(win(stage, k++), dey, n, P, wx0, wy0, EWX, EWY);
     }
     load_window(win(stage, k), I.R, n, P, wx0, wy0, EWX, EWY);
   }
@@ -273,8 +272,6 @@ struct EnergyPass {
     const Real* Wb = (kind != 0) ? win(stage, 3) : nullptr;
     const Real* Wox = (kind == 2) ? win(stage, 4) : nullptr;  // od
     const Real* Woy = (kind == 2) ? win(stage, 5) : nullptr;
-    const Real* Wdx = (kind == 2) ? win(stage, 6) : nullptr;  // DE
-    const Real* Wdy = (kind == 2) ? win(stage, 7) : nullptr;
     auto at = [&](int x, int y) { return (y - (y0 - 1)) * EWX + (x - (x0 - 4)); };
     // direction at a window position
     auto dirx = [&](int i) -> Real {
@@ -329,7 +326,7 @@ struct EnergyPass {
         wdy[g] = ddy;
         const Real lx = stiff_row<Real>(x, y, n, [&](int X, int Y) { return dirx(at(X, Y)); });
         const Real ly = stiff_row<Real>(x, y, n, [&](int X, int Y) { return diry(at(X, Y)); });
-        part[1] += (double)Wdx[c] * (double)ddx + (double)Wdy[c] * (double)ddy;
+        part[1] += (double)__ldcg(dex + g) * (double)ddx + (double)__ldcg(dey + g) * (double)ddy;
         part[2] += (double)Wpx[c] * (double)lx + (double)Wpy[c] * (double)ly;
         part[3] += (double)ddx * (double)lx + (double)ddy * (double)ly;
       }
@@ -759,7 +756,7 @@ __device__ void coarse_vcycle(int lc, double tau, Real* sm, const Real* bx, cons
 
 // Dynamic shared memory of the level kernel (elements of Real).
 __host__ __device__ inline size_t level_smem_elems(int lc) {
-  size_t e = (size_t)2 * 9 * EWIN;                               // energy, kind 2
+  size_t e = (size_t)2 * 7 * EWIN;                               // energy, kind 2
   const size_t g = (size_t)2 * 5 * EWIN + (size_t)GCX * GCY * 8;  // gradient
   const size_t d = (size_t)2 * 2 * VWIN + (size_t)6 * VWIN;      // down
   const size_t u = (size_t)2 * (4 * VWIN + 2 * CWIN) + 2 * VWIN;  // up
