@@ -252,6 +252,20 @@ static double dot(const double* a, const double* b, int N) {
   return r;
 }
 
+/* data term of a level solve: SSD, or NCC with its precomputed parts */
+typedef struct dterm_s {
+  int ncc;           /* 0: SSD, 1: NCC                                   */
+  double* M;         /* mass matrix (NCC)                                */
+  double* normR;     /* normalised reference (NCC)                       */
+} dterm_t;
+static double ncc_energy_with(const dterm_t* D, int level, const double* T, const double* phix,
+                              const double* phiy, double* var_out, double* normT_out);
+static void ncc_variation_with(const dterm_t* D, int level, const double* T, const double* phix,
+                               const double* phiy, double* gx, double* gy);
+static double interp(const double* img, int n, double X, double Y);
+static void dterm_init(dterm_t* D, int ncc, int level, const double* R);
+static void dterm_free(dterm_t* D);
+
 /* DisplacementLengthEnergy::apply (hyperelastic.h:178-183) */
 static double reg_energy_with(const double* st, int level, const double* phix, const double* phiy) {
   const int n = lvl_n(level), N = n * n;
@@ -265,10 +279,11 @@ static double reg_energy_with(const double* st, int level, const double* phix, c
   return 0.5 * d;
 }
 
-static double energy_with(const double* st, int level, const double* R, const double* T,
+static double energy_with(const double* st, const dterm_t* D, int level, const double* R, const double* T,
                           const double* phix, const double* phiy, double lambda, double* ereg) {
   double e = 0.;
-  e += msor_ssd_energy(level, R, T, phix, phiy);
+  if (D && D->ncc) e += ncc_energy_with(D, level, T, phix, phiy, NULL, NULL);
+  else e += msor_ssd_energy(level, R, T, phix, phiy);
   const double r = reg_energy_with(st, level, phix, phiy);
   if (ereg) *ereg = r;
   if (lambda != 1.0) e += lambda * r; else e += r;
@@ -278,16 +293,28 @@ static double energy_with(const double* st, int level, const double* R, const do
 double msor_energy(int level, const double* R, const double* T, const double* phix,
                    const double* phiy, double lambda, double* ereg) {
   double* st = stiff_build(level);
-  const double e = energy_with(st, level, R, T, phix, phiy, lambda, ereg);
+  const double e = energy_with(st, NULL, level, R, T, phix, phiy, lambda, ereg);
   free(st);
   return e;
 }
 
-static void denergy_with(const double* st, int level, const double* R, const double* T,
+double msor_energy_dt(int data_term, int level, const double* R, const double* T, const double* phix,
+                      const double* phiy, double lambda, double* ereg) {
+  double* st = stiff_build(level);
+  dterm_t D;
+  dterm_init(&D, data_term, level, R);
+  const double e = energy_with(st, &D, level, R, T, phix, phiy, lambda, ereg);
+  dterm_free(&D);
+  free(st);
+  return e;
+}
+
+static void denergy_with(const double* st, const dterm_t* D, int level, const double* R, const double* T,
                          const double* phix, const double* phiy, double lambda,
                          double* gx, double* gy) {
   const int n = lvl_n(level), N = n * n;
-  msor_ssd_force(level, R, T, phix, phiy, gx, gy);
+  if (D && D->ncc) ncc_variation_with(D, level, T, phix, phiy, gx, gy);
+  else msor_ssd_force(level, R, T, phix, phiy, gx, gy);
   double* tmp = (double*)malloc(sizeof(double) * N);
   stiff_apply_with(st, level, phix, tmp);
   for (int i = 0; i < N; ++i) gx[i] += (lambda != 1.0) ? lambda * tmp[i] : tmp[i];
@@ -299,8 +326,220 @@ static void denergy_with(const double* st, int level, const double* R, const dou
 void msor_denergy(int level, const double* R, const double* T, const double* phix,
                   const double* phiy, double lambda, double* gx, double* gy) {
   double* st = stiff_build(level);
-  denergy_with(st, level, R, T, phix, phiy, lambda, gx, gy);
+  denergy_with(st, NULL, level, R, T, phix, phiy, lambda, gx, gy);
   free(st);
+}
+
+void msor_denergy_dt(int data_term, int level, const double* R, const double* T, const double* phix,
+                     const double* phiy, double lambda, double* gx, double* gy) {
+  double* st = stiff_build(level);
+  dterm_t D;
+  dterm_init(&D, data_term, level, R);
+  denergy_with(st, &D, level, R, T, phix, phiy, lambda, gx, gy);
+  dterm_free(&D);
+  free(st);
+}
+
+/* --- normalized cross-correlation data term (registration.h:1828-2018) ---- */
+
+/* Assembled Q1 mass matrix (MassOp ASSEMBLED, FEOpInterface.h:2382-2394):
+ * local matrix by quadrature (FELinScalarWeightedMassInterface::
+ * prepareLocalMatrix, FEOpInterface.h:1445-1475) in the layout and
+ * assembly order of the stiffness matrix above.                             */
+static double* mass_build(int level) {
+  const int n = lvl_n(level);
+  const double h = lvl_h(level);
+  const double vol = sqr(h);
+  quad_t Q;
+  quad_init(&Q, h);
+  double L[4][4];
+  for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) L[i][j] = 0.;
+  for (int q = 0; q < 4; ++q) {
+    const double coeff = 1.;
+    for (int i = 0; i < 4; ++i) {
+      const double basisi = Q.bq[i][q];
+      for (int j = i; j < 4; ++j) L[i][j] += basisi * Q.bq[j][q] * coeff * Q.w;
+    }
+  }
+  for (int i = 0; i < 4; ++i)
+    for (int j = i; j < 4; ++j) L[j][i] = L[i][j] = L[i][j] * vol;
+  double* st = (double*)calloc((size_t)n * n * 9, sizeof(double));
+  for (int ey = 0; ey < n - 1; ++ey)
+    for (int ex = 0; ex < n - 1; ++ex)
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) {
+          const int gi = dof(n, ex, ey, i), gj = dof(n, ex, ey, j);
+          const int dx = (gj % n) - (gi % n), dy = (gj / n) - (gi / n);
+          double* e = &st[(size_t)gi * 9 + (dy + 1) * 3 + (dx + 1)];
+          *e += 1.0 * L[i][j];
+        }
+  return st;
+}
+
+void msor_mass_apply(int level, const double* u, double* Mu) {
+  double* m = mass_build(level);
+  stiff_apply_with(m, level, u, Mu);
+  free(m);
+}
+
+/* NormalizedCrossCorrelationEnergy::normalizeImageForNCC (registration.h:
+ * 1932-1944): subtract the mass-weighted mean, divide by the mass-weighted
+ * norm; returns that norm.                                                 */
+static double ncc_normalize(const double* M, int level, const double* img, double* out) {
+  const int n = lvl_n(level), N = n * n;
+  double* temp = (double*)malloc(sizeof(double) * N);
+  stiff_apply_with(M, level, img, temp);
+  double mean = 0.;                          /* Vector::sum (vec.cpp:847-860) */
+  for (int i = 0; i < N; ++i) mean += temp[i];
+  for (int i = 0; i < N; ++i) { out[i] = img[i]; out[i] += -mean; }   /* addToAll */
+  stiff_apply_with(M, level, out, temp);
+  const double var = sqrt(dot(out, temp, N));
+  if (!(fabs(var - 0.) < 1e-15))             /* aol::appeqAbsolute, aol.h:791-794 */
+    for (int i = 0; i < N; ++i) out[i] /= var;
+  free(temp);
+  return var;
+}
+
+/* FastDeformImage, 2-D (deformations.h:138-159): nodal positions clamped to
+ * the grid, bilinear ScalarArray::interpolate.                             */
+static void fast_deform(int level, const double* img, const double* phix, const double* phiy, double* out) {
+  const int n = lvl_n(level);
+  const double h = lvl_h(level);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) {
+      const int index = i + j * n;
+      double ds0 = i + phix[index] / h, ds1 = j + phiy[index] / h;
+      const double hi = (double)(n - 1);
+      ds0 = ds0 < 0. ? 0. : (ds0 > hi ? hi : ds0);            /* aol::Clamp */
+      ds1 = ds1 < 0. ? 0. : (ds1 > hi ? hi : ds1);
+      out[index] = interp(img, n, ds0, ds1);
+    }
+}
+
+
+static void dterm_init(dterm_t* D, int ncc, int level, const double* R) {
+  D->ncc = ncc;
+  D->M = NULL;
+  D->normR = NULL;
+  if (ncc) {
+    const int n = lvl_n(level);
+    D->M = mass_build(level);
+    D->normR = (double*)malloc(sizeof(double) * n * n);
+    ncc_normalize(D->M, level, R, D->normR);
+  }
+}
+
+static void dterm_free(dterm_t* D) {
+  free(D->M);
+  free(D->normR);
+}
+
+/* NormalizedCrossCorrelationEnergy::computeEnergy (registration.h:1950-1962);
+ * var_out / normT_out (nullable) receive the norm and the normalised
+ * deformed template.                                                       */
+static double ncc_energy_with(const dterm_t* D, int level, const double* T, const double* phix,
+                              const double* phiy, double* var_out, double* normT_out) {
+  const int n = lvl_n(level), N = n * n;
+  double* deformedT = (double*)malloc(sizeof(double) * N);
+  double* normT = (double*)malloc(sizeof(double) * N);
+  fast_deform(level, T, phix, phiy, deformedT);
+  const double var = ncc_normalize(D->M, level, deformedT, normT);
+  stiff_apply_with(D->M, level, normT, deformedT);
+  const double e = -(dot(deformedT, D->normR, N));
+  if (var_out) *var_out = var;
+  if (normT_out) memcpy(normT_out, normT, sizeof(double) * N);
+  free(deformedT);
+  free(normT);
+  return e;
+}
+
+double msor_ncc_energy(int level, const double* R, const double* T, const double* phix, const double* phiy) {
+  dterm_t D;
+  dterm_init(&D, 1, level, R);
+  const double e = ncc_energy_with(&D, level, T, phix, phiy, NULL, NULL);
+  dterm_free(&D);
+  return e;
+}
+
+/* transformCoord<ConfiguratorType, false> (deformations.h:622-668): grid
+ * coordinates El + RefCoord + Offset / H, no clipping; 0 when the point
+ * leaves the grid.                                                         */
+static int transform_noclip(const quad_t* Q, int n, double h, int ex, int ey, int q, double off_x,
+                            double off_y, tcoord_t* t) {
+  const double coord[2] = {(double)ex + Q->rc[q][0], (double)ey + Q->rc[q][1]};
+  const double off[2] = {off_x, off_y};
+  for (int c = 0; c < 2; ++c) {
+    const double tc = coord[c] + off[c] / h;
+    int e = (short)tc;
+    double l = tc - e;
+    if (e == n - 1 && l == 0) { e = n - 2; l = 1; }
+    if (tc < 0. || e < 0 || e >= n - 1) return 0;
+    t->el[c] = e;
+    t->loc[c] = l;
+    t->within[c] = 1;
+  }
+  return 1;
+}
+
+/* NormalizedCrossCorrelationEnergy::applyDerivative (registration.h:1972-1983)
+ * with CrossCorrelationForce (registration.h:1828-1862) integrated like
+ * FENonlinVectorOpInterface::applyAdd (FEOpInterface.h:1803-1852).          */
+static void ncc_variation_with(const dterm_t* D, int level, const double* T, const double* phix,
+                               const double* phiy, double* gx, double* gy) {
+  const int n = lvl_n(level), N = n * n;
+  const double h = lvl_h(level);
+  const double vol = sqr(h);
+  double var;
+  double* normT = (double*)malloc(sizeof(double) * N);
+  double* temp = (double*)malloc(sizeof(double) * N);
+  const double energy = ncc_energy_with(D, level, T, phix, phiy, &var, normT);
+  for (int i = 0; i < N; ++i) temp[i] = D->normR[i];
+  for (int i = 0; i < N; ++i) temp[i] += normT[i] * energy;          /* addMultiple */
+  if (!(fabs(var - 0.) < 1e-15))
+    for (int i = 0; i < N; ++i) temp[i] /= var;
+  quad_t Q;
+  quad_init(&Q, h);
+  memset(gx, 0, sizeof(double) * N);
+  memset(gy, 0, sizeof(double) * N);
+  for (int ey = 0; ey < n - 1; ++ey)
+    for (int ex = 0; ex < n - 1; ++ex) {
+      double nl[4][2];
+      for (int q = 0; q < 4; ++q) {
+        const double ox = eval_at_quad(&Q, phix, n, ex, ey, q);
+        const double oy = eval_at_quad(&Q, phiy, n, ex, ey, q);
+        tcoord_t t;
+        if (!transform_noclip(&Q, n, h, ex, ey, q, ox, oy, &t)) {
+          nl[q][0] = 0.;
+          nl[q][1] = 0.;
+          continue;
+        }
+        eval_grad_local(T, n, t.el[0], t.el[1], t.loc[0], t.loc[1], h, nl[q]);
+        const double f = -eval_at_quad(&Q, temp, n, ex, ey, q);
+        nl[q][0] *= f;
+        nl[q][1] *= f;
+      }
+      for (int b = 0; b < 4; ++b) {
+        double a0 = 0., a1 = 0.;
+        for (int q = 0; q < 4; ++q) {
+          const double f = Q.bq[b][q] * Q.w;
+          a0 += nl[q][0] * f;
+          a1 += nl[q][1] * f;
+        }
+        const int g = dof(n, ex, ey, b);
+        gx[g] += vol * a0;
+        gy[g] += vol * a1;
+      }
+    }
+  free(normT);
+  free(temp);
+}
+
+void msor_ncc_variation(int level, const double* R, const double* T, const double* phix, const double* phiy,
+                        double* gx, double* gy) {
+  dterm_t D;
+  dterm_init(&D, 1, level, R);
+  ncc_variation_with(&D, level, T, phix, phiy, gx, gy);
+  dterm_free(&D);
 }
 
 /* --- multigrid heat smoother (linearSmoothOp.cpp) --------------------- */
@@ -553,6 +792,7 @@ typedef struct {
   const double *R, *T;
   const double* st;
   double lambda;
+  const dterm_t* D;
   /* ring buffer of the last two Armijo evaluations (gradientDescent.h:56-59) */
   double rb_tau[2], rb_e[2];
   int rb_pos;
@@ -567,7 +807,7 @@ static double armijo_eval(gd_ctx* C, const double* px, const double* py, const d
   if (tw == 0) return C->e_at_pos;
   for (int i = 0; i < C->N; ++i) { C->tx[i] = px[i]; C->tx[i] += tw * dx[i]; }
   for (int i = 0; i < C->N; ++i) { C->ty[i] = py[i]; C->ty[i] += tw * dy[i]; }
-  const double e = energy_with(C->st, C->level, C->R, C->T, C->tx, C->ty, C->lambda, NULL);
+  const double e = energy_with(C->st, C->D, C->level, C->R, C->T, C->tx, C->ty, C->lambda, NULL);
   C->rb_tau[C->rb_pos] = tw;
   C->rb_e[C->rb_pos] = e;
   C->rb_pos ^= 1;
@@ -610,11 +850,19 @@ static double armijo(gd_ctx* C, const double* px, const double* py, const double
 int msor_gd_level(int level, const double* R, const double* T, double* phix, double* phiy,
                   double lambda, int max_iter, double stop_eps, double* energy_out,
                   msor_step* trace, int trace_cap) {
+  return msor_gd_level_dt(0, level, R, T, phix, phiy, lambda, max_iter, stop_eps, energy_out, trace, trace_cap);
+}
+
+int msor_gd_level_dt(int data_term, int level, const double* R, const double* T, double* phix, double* phiy,
+                     double lambda, int max_iter, double stop_eps, double* energy_out,
+                     msor_step* trace, int trace_cap) {
   const int n = lvl_n(level), N = n * n;
   double* st = stiff_build(level);
+  dterm_t D;
+  dterm_init(&D, data_term, level, R);
   gd_ctx C;
   memset(&C, 0, sizeof(C));
-  C.level = level; C.N = N; C.R = R; C.T = T; C.st = st; C.lambda = lambda;
+  C.level = level; C.N = N; C.R = R; C.T = T; C.st = st; C.lambda = lambda; C.D = &D;
   C.rb_tau[0] = C.rb_tau[1] = NAN;
   double* buf = (double*)calloc((size_t)N * 12, sizeof(double));
   double *dx = buf, *dy = buf + N;            /* descent direction           */
@@ -627,12 +875,12 @@ int msor_gd_level(int level, const double* R, const double* T, double* phix, dou
   double tau = 1.0;              /* startTau (registration.h:52) */
   double sigma = 1.0;            /* GradientDescentWithAutomaticFilterWidth (gradientDescent.h:688) */
   const double stop_sigma = 0.0001, sigma_tol = 0.00001;
-  double energy = energy_with(st, level, R, T, phix, phiy, lambda, NULL);
+  double energy = energy_with(st, &D, level, R, T, phix, phiy, lambda, NULL);
   double energy_new = energy;
   int iter = 0, n_trace = 0;
   if (max_iter <= 0) {
     if (energy_out) *energy_out = energy_new;
-    free(buf); free(st);
+    free(buf); free(st); dterm_free(&D);
     return 0;
   }
   int go;
@@ -643,7 +891,7 @@ int msor_gd_level(int level, const double* R, const double* T, double* phix, dou
     C.evals = 0;
     const double sigma_used = sigma;
     /* calcTaudAndDescentDir (gradientDescent.h:200-236) */
-    denergy_with(st, level, R, T, phix, phiy, lambda, DEx, DEy);
+    denergy_with(st, &D, level, R, T, phix, phiy, lambda, DEx, DEy);
     for (int i = 0; i < N; ++i) { dx[i] = DEx[i] * -1.; dy[i] = DEy[i] * -1.; }
     msor_smooth(level, sigma, dx, sx); memcpy(dx, sx, sizeof(double) * N);
     msor_smooth(level, sigma, dy, sy); memcpy(dy, sy, sizeof(double) * N);
@@ -673,7 +921,7 @@ int msor_gd_level(int level, const double* R, const double* T, double* phix, dou
     if (tau != 0) {
       for (int i = 0; i < N; ++i) { phix[i] += dx[i]; phiy[i] += dy[i]; }
     }
-    if (isnan(enew)) enew = energy_with(st, level, R, T, phix, phiy, lambda, NULL);
+    if (isnan(enew)) enew = energy_with(st, &D, level, R, T, phix, phiy, lambda, NULL);
     energy_new = enew;
     if (trace && n_trace < trace_cap) {
       trace[n_trace].iter = iter; trace[n_trace].energy = energy_new; trace[n_trace].tau = tau;
@@ -690,6 +938,7 @@ int msor_gd_level(int level, const double* R, const double* T, double* phix, dou
   if (energy_out) *energy_out = energy_new;
   free(buf);
   free(st);
+  dterm_free(&D);
   return iter;
 }
 
@@ -725,6 +974,14 @@ double msor_register(int max_level, int start_level, int stop_level, const doubl
                      const double* T, double* phix, double* phiy, double lambda,
                      double lambda_factor, int max_iter, double stop_eps, int resample_phi,
                      int* steps_per_level) {
+  return msor_register_dt(0, max_level, start_level, stop_level, R, T, phix, phiy, lambda, lambda_factor,
+                          max_iter, stop_eps, resample_phi, steps_per_level);
+}
+
+double msor_register_dt(int data_term, int max_level, int start_level, int stop_level, const double* R,
+                        const double* T, double* phix, double* phiy, double lambda,
+                        double lambda_factor, int max_iter, double stop_eps, int resample_phi,
+                        int* steps_per_level) {
   double *Rl[16] = {0}, *Tl[16] = {0}, *Px[16] = {0}, *Py[16] = {0};
   for (int l = 0; l <= max_level; ++l) {
     const int n = lvl_n(l);
@@ -751,8 +1008,8 @@ double msor_register(int max_level, int start_level, int stop_level, const doubl
     for (int level = start_level; level <= stop_level; ++level) {
       /* getRegularizationWeight (registration.h:523-526) */
       const double lam = (double)pow(lambda_factor, stop_level - level) * lambda;
-      const int steps = msor_gd_level(level, Rl[level], Tl[level], Px[level], Py[level], lam,
-                                      max_iter, stop_eps, &energy, NULL, 0);
+      const int steps = msor_gd_level_dt(data_term, level, Rl[level], Tl[level], Px[level], Py[level], lam,
+                                         max_iter, stop_eps, &energy, NULL, 0);
       if (steps_per_level) steps_per_level[level - start_level] = steps;
       if (level < stop_level) {
         phi_up(level, resample_phi, Px, Py);

@@ -102,6 +102,31 @@ double msor_register(int max_level, int start_level, int stop_level,
 void   msor_warp_mean(int level, int num_frames, const double* frames,
                       const double* phis, double* mean, double* count);
 
+/* --- normalized cross-correlation data term ------------------------------
+ * data_term 0 = SSD (the functions above), 1 = NCC:
+ * NormalizedCrossCorrelationEnergy / VariationOfNormalizedCrossCorrelationEnergy
+ * (registration.h:1909-2018) with the same Dirichlet regulariser.          */
+/* MassOp ASSEMBLED apply (FEOpInterface.h:2382-2394, 1445-1475)             */
+void   msor_mass_apply(int level, const double* u, double* Mu);
+/* the NCC energy alone (computeEnergy, registration.h:1950-1962)           */
+double msor_ncc_energy(int level, const double* R, const double* T,
+                       const double* phix, const double* phiy);
+/* its variation alone (applyDerivative, registration.h:1972-1983)          */
+void   msor_ncc_variation(int level, const double* R, const double* T,
+                          const double* phix, const double* phiy, double* gx, double* gy);
+double msor_energy_dt(int data_term, int level, const double* R, const double* T,
+                      const double* phix, const double* phiy, double lambda, double* ereg);
+void   msor_denergy_dt(int data_term, int level, const double* R, const double* T,
+                       const double* phix, const double* phiy, double lambda,
+                       double* gx, double* gy);
+int    msor_gd_level_dt(int data_term, int level, const double* R, const double* T,
+                        double* phix, double* phiy, double lambda, int max_iter,
+                        double stop_eps, double* energy_out, msor_step* trace, int trace_cap);
+double msor_register_dt(int data_term, int max_level, int start_level, int stop_level,
+                        const double* R, const double* T, double* phix, double* phiy,
+                        double lambda, double lambda_factor, int max_iter, double stop_eps,
+                        int resample_phi, int* steps_per_level);
+
 #ifdef __cplusplus
 }
 #endif

@@ -42,6 +42,10 @@ def lib():
         L.msor_energy.restype = ctypes.c_double
         L.msor_register.restype = ctypes.c_double
         L.msor_gd_level.restype = ctypes.c_int
+        L.msor_ncc_energy.restype = ctypes.c_double
+        L.msor_energy_dt.restype = ctypes.c_double
+        L.msor_register_dt.restype = ctypes.c_double
+        L.msor_gd_level_dt.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -63,20 +67,30 @@ def ssd_energy(level, R, T, px, py):
     return lib().msor_ssd_energy(level, _p(_c(R)), _p(_c(T)), _p(_c(px)), _p(_c(py)))
 
 
-def energy(level, R, T, px, py, lam):
+def energy(level, R, T, px, py, lam, ncc=False):
     ereg = ctypes.c_double()
-    e = lib().msor_energy(level, _p(_c(R)), _p(_c(T)), _p(_c(px)), _p(_c(py)),
-                          ctypes.c_double(lam), ctypes.byref(ereg))
+    e = lib().msor_energy_dt(int(bool(ncc)), level, _p(_c(R)), _p(_c(T)), _p(_c(px)), _p(_c(py)),
+                             ctypes.c_double(lam), ctypes.byref(ereg))
     return e, ereg.value
 
 
-def denergy(level, R, T, px, py, lam):
+def denergy(level, R, T, px, py, lam, ncc=False):
     n = n_of(level)
     gx = np.zeros(n * n)
     gy = np.zeros(n * n)
-    lib().msor_denergy(level, _p(_c(R)), _p(_c(T)), _p(_c(px)), _p(_c(py)), ctypes.c_double(lam),
-                       _p(gx), _p(gy))
+    lib().msor_denergy_dt(int(bool(ncc)), level, _p(_c(R)), _p(_c(T)), _p(_c(px)), _p(_c(py)),
+                          ctypes.c_double(lam), _p(gx), _p(gy))
     return gx, gy
+
+
+def ncc_energy(level, R, T, px, py):
+    return lib().msor_ncc_energy(level, _p(_c(R)), _p(_c(T)), _p(_c(px)), _p(_c(py)))
+
+
+def mass_apply(level, u):
+    out = np.zeros(n_of(level) ** 2)
+    lib().msor_mass_apply(level, _p(_c(u)), _p(out))
+    return out
 
 
 def ssd_force(level, R, T, px, py):
@@ -129,26 +143,27 @@ def normalize(img, sat=0.15, min_to_zero=1):
     return a
 
 
-def gd_level(level, R, T, px, py, lam, max_iter, stop_eps=0.0, trace_cap=4096):
+def gd_level(level, R, T, px, py, lam, max_iter, stop_eps=0.0, trace_cap=4096, ncc=False):
     px = _c(px).copy()
     py = _c(py).copy()
     tr = (Step * trace_cap)()
     e = ctypes.c_double()
-    steps = lib().msor_gd_level(level, _p(_c(R)), _p(_c(T)), _p(px), _p(py), ctypes.c_double(lam),
-                                max_iter, ctypes.c_double(stop_eps), ctypes.byref(e), tr, trace_cap)
+    steps = lib().msor_gd_level_dt(int(bool(ncc)), level, _p(_c(R)), _p(_c(T)), _p(px), _p(py),
+                                   ctypes.c_double(lam), max_iter, ctypes.c_double(stop_eps), ctypes.byref(e),
+                                   tr, trace_cap)
     trace = [(tr[i].iter, tr[i].energy, tr[i].tau, tr[i].sigma, tr[i].evals) for i in range(min(steps, trace_cap))]
     return px, py, e.value, steps, trace
 
 
 def register(max_level, start, stop, R, T, px=None, py=None, lam=0.1, lam_factor=1.0,
-             max_iter=20, stop_eps=0.0, resample_phi=False):
+             max_iter=20, stop_eps=0.0, resample_phi=False, ncc=False):
     N = n_of(max_level) ** 2
     px = np.zeros(N) if px is None else _c(px).copy()
     py = np.zeros(N) if py is None else _c(py).copy()
     steps = (ctypes.c_int * max(1, stop - start + 1))()
-    e = lib().msor_register(max_level, start, stop, _p(_c(R)), _p(_c(T)), _p(px), _p(py),
-                            ctypes.c_double(lam), ctypes.c_double(lam_factor), max_iter,
-                            ctypes.c_double(stop_eps), int(bool(resample_phi)), steps)
+    e = lib().msor_register_dt(int(bool(ncc)), max_level, start, stop, _p(_c(R)), _p(_c(T)), _p(px), _p(py),
+                               ctypes.c_double(lam), ctypes.c_double(lam_factor), max_iter,
+                               ctypes.c_double(stop_eps), int(bool(resample_phi)), steps)
     return px, py, e, list(steps)
 
 
@@ -186,9 +201,9 @@ class RefRunner:
         subprocess.run([REF_BIN, *map(str, args)], check=True, stdout=subprocess.DEVNULL,
                        stderr=subprocess.DEVNULL)
 
-    def energy(self, level, R, T, px, py, lam):
+    def energy(self, level, R, T, px, py, lam, ncc=False):
         N = n_of(level) ** 2
-        self.run("energy", level, self._w("R", R), self._w("T", T), self._w("px", px), self._w("py", py),
+        self.run("energy_ncc" if ncc else "energy", level, self._w("R", R), self._w("T", T), self._w("px", px), self._w("py", py),
                  repr(float(lam)), os.path.join(self.dir, "e"))
         essd, ereg, etot = map(float, open(os.path.join(self.dir, "e.txt")).read().split())
         de = self._r("e_de.bin")
@@ -220,9 +235,9 @@ class RefRunner:
                  os.path.join(self.dir, "out"))
         return self._r("out")
 
-    def gd_level(self, level, R, T, px, py, lam, max_iter, stop_eps=0.0):
+    def gd_level(self, level, R, T, px, py, lam, max_iter, stop_eps=0.0, ncc=False):
         N = n_of(level) ** 2
-        self.run("gdlevel", level, self._w("R", R), self._w("T", T), self._w("px", px), self._w("py", py),
+        self.run("gdlevel_ncc" if ncc else "gdlevel", level, self._w("R", R), self._w("T", T), self._w("px", px), self._w("py", py),
                  repr(float(lam)), max_iter, repr(float(stop_eps)), os.path.join(self.dir, "phi"),
                  os.path.join(self.dir, "trace.txt"))
         phi = self._r("phi")
@@ -235,11 +250,11 @@ class RefRunner:
         return phi[:N], phi[N:], final_e, steps, trace
 
     def register(self, max_level, start, stop, R, T, px=None, py=None, lam=0.1, lam_factor=1.0,
-                 max_iter=20, stop_eps=0.0, resample_phi=False):
+                 max_iter=20, stop_eps=0.0, resample_phi=False, ncc=False):
         N = n_of(max_level) ** 2
         px = np.zeros(N) if px is None else px
         py = np.zeros(N) if py is None else py
-        self.run("register", max_level, start, stop, self._w("R", R), self._w("T", T), self._w("px", px),
+        self.run("register_ncc" if ncc else "register", max_level, start, stop, self._w("R", R), self._w("T", T), self._w("px", px),
                  self._w("py", py), repr(float(lam)), repr(float(lam_factor)), max_iter, repr(float(stop_eps)),
                  int(bool(resample_phi)), os.path.join(self.dir, "phi"), os.path.join(self.dir, "e.txt"))
         phi = self._r("phi")

@@ -9,7 +9,9 @@
 // Arrays are raw little-endian float64 files, x fastest (quoc ILex order).
 // The configurator is the dyadic 2^l+1 grid with Q1 elements and 2x2 Gauss
 // quadrature (QuocConfiguratorTraitMultiLin, configurators.h:218-330), with the
-// SSD data term (registration.h:1257-1273), the Dirichlet regulariser
+// SSD data term (registration.h:1257-1273) or, for the commands ending in
+// _ncc, the normalized cross-correlation data term (NCCRegistrationConfigurator,
+// registration.h:1766-1780, 1909-2018), the Dirichlet regulariser
 // (registration.h:677-710) and the H1 gradient flow with automatic filter
 // width (gradientDescent.h:632-709).
 #include <registration.h>
@@ -27,6 +29,7 @@ typedef double RealType;
 typedef qc::QuocConfiguratorTraitMultiLin<RealType, qc::QC_2D, aol::GaussQuadrature<RealType, qc::QC_2D, 3> > ConfType;
 typedef qc::ScalarArray<RealType, qc::QC_2D> ArrayType;
 typedef qc::StandardRegistrationMultilevelDescent<ConfType, qc::SSDRegistrationConfigurator<ConfType> > RegisType;
+typedef qc::StandardRegistrationMultilevelDescent<ConfType, qc::NCCRegistrationConfigurator<ConfType> > RegisTypeNCC;
 typedef aol::H1GradientDescent<ConfType, aol::MultiVector<RealType>, qc::LinearSmoothOp<RealType> > H1Type;
 typedef aol::GradientDescentWithAutomaticFilterWidth<ConfType, aol::MultiVector<RealType>, H1Type> GDType;
 
@@ -97,14 +100,97 @@ static aol::ParameterParser* makeParser ( int maxLevel, int start, int stop, dou
   return p;
 }
 
+// E = Edata + lambda Ereg and DE = DEdata + lambda DEreg (LinCombOp, as
+// StandardRegistration::findTransformation builds them, registration.h:971-982);
+// writes Edata, Ereg, E and [DE, DEdata].
+template <typename EnergyType, typename VariationType>
+static void energyCommand ( const qc::GridDefinition &grid, const EnergyType &Edata, const VariationType &DEdata,
+                            const aol::MultiVector<RealType> &phi, RealType lambda, const char *prefix ) {
+  const int N = grid.getNumberOfNodes ( );
+  qc::DirichletRegularizationConfigurator<ConfType> regul ( grid );
+  aol::LinCombOp<aol::MultiVector<RealType>, aol::Scalar<RealType> > E;
+  E.appendReference ( Edata ); E.appendReference ( regul.getRegERef ( ), lambda );
+  aol::LinCombOp<aol::MultiVector<RealType> > DE;
+  DE.appendReference ( DEdata ); DE.appendReference ( regul.getRegDERef ( ), lambda );
+  aol::Scalar<RealType> edata, ereg, etot;
+  Edata.apply ( phi, edata ); regul.getRegERef ( ).apply ( phi, ereg ); E.apply ( phi, etot );
+  aol::MultiVector<RealType> de ( 2, N ), fo ( 2, N );
+  DE.apply ( phi, de );
+  DEdata.apply ( phi, fo );
+  std::vector<RealType> out ( 4 * N );
+  memcpy ( &out[0], de[0].getData ( ), N * sizeof ( RealType ) );
+  memcpy ( &out[N], de[1].getData ( ), N * sizeof ( RealType ) );
+  memcpy ( &out[2 * N], fo[0].getData ( ), N * sizeof ( RealType ) );
+  memcpy ( &out[3 * N], fo[1].getData ( ), N * sizeof ( RealType ) );
+  writeBin ( ( std::string ( prefix ) + "_de.bin" ).c_str ( ), &out[0], 4 * N );
+  FILE *f = fopen ( ( std::string ( prefix ) + ".txt" ).c_str ( ), "w" );
+  fprintf ( f, "%.17g %.17g %.17g\n", edata[0], ereg[0], etot[0] );
+  fclose ( f );
+}
+
+// StandardRegistration::findTransformation + updateTransformationWithGD
+// (registration.h:967-1021) with the tracing solver.
+template <typename EnergyType, typename VariationType>
+static void gdLevelCommand ( const qc::GridDefinition &grid, const EnergyType &Edata, const VariationType &DEdata,
+                             aol::MultiVector<RealType> &phi, RealType lambda, int maxIter, RealType stopEps,
+                             const char *outPhi, const char *outTrace ) {
+  const int N = grid.getNumberOfNodes ( );
+  qc::DirichletRegularizationConfigurator<ConfType> regul ( grid );
+  aol::LinCombOp<aol::MultiVector<RealType>, aol::Scalar<RealType> > E;
+  E.appendReference ( Edata ); E.appendReference ( regul.getRegERef ( ), lambda );
+  aol::LinCombOp<aol::MultiVector<RealType> > DE;
+  DE.appendReference ( DEdata ); DE.appendReference ( regul.getRegDERef ( ), lambda );
+  TracingGD gd ( grid, E, DE, maxIter, stopEps );
+  gd.setConfigurationFlags ( GDType::USE_NONLINEAR_CG | GDType::DO_NOT_WRITE_CONSOLE_OUTPUT );
+  gd.applySingle ( phi );
+  std::vector<RealType> out ( 2 * N );
+  memcpy ( &out[0], phi[0].getData ( ), N * sizeof ( RealType ) );
+  memcpy ( &out[N], phi[1].getData ( ), N * sizeof ( RealType ) );
+  writeBin ( outPhi, &out[0], 2 * N );
+  FILE *f = fopen ( outTrace, "w" );
+  fprintf ( f, "# iter energy tau sigma evals ; final %.17g steps %d\n", gd.getEnergyAtLastPosition ( ), gd.getIterations ( ) );
+  for ( size_t i = 0; i < gd.energies.size ( ); ++i )
+    fprintf ( f, "%d %.17g %.17g %.17g %d\n", ( int ) i, gd.energies[i], gd.taus[i], gd.sigmas[i], gd.evals[i] );
+  fclose ( f );
+}
+
+// solveAndProlongToMaxDepth of the registration class Regis from a given
+// displacement (registration.h:462-467).
+template <typename Regis>
+static void registerCommand ( char **argv ) {
+  const int maxL = atoi ( argv[2] ), start = atoi ( argv[3] ), stop = atoi ( argv[4] );
+  const int n = lvlN ( maxL ), N = n * n;
+  aol::ParameterParser *parser = makeParser ( maxL, start, stop, atof ( argv[9] ), atof ( argv[10] ), atoi ( argv[11] ),
+                                              atof ( argv[12] ), atoi ( argv[13] ), -1, 0 );
+  Regis regis ( *parser );
+  qc::GridDefinition grid ( maxL, qc::QC_2D );
+  ArrayType R ( grid ), T ( grid );
+  readBin ( argv[5], R.getData ( ), N ); readBin ( argv[6], T.getData ( ), N );
+  regis.initRefOrTemplate ( R, qc::REFERENCE, true );
+  regis.initRefOrTemplate ( T, qc::TEMPLATE, true );
+  qc::MultiArray<RealType, qc::QC_2D> phi ( grid );
+  readBin ( argv[7], phi[0].getData ( ), N ); readBin ( argv[8], phi[1].getData ( ), N );
+  regis.setTransformation ( phi );
+  regis.solveAndProlongToMaxDepth ( );
+  regis.getTransformation ( phi );
+  std::vector<RealType> out ( 2 * N );
+  memcpy ( &out[0], phi[0].getData ( ), N * sizeof ( RealType ) );
+  memcpy ( &out[N], phi[1].getData ( ), N * sizeof ( RealType ) );
+  writeBin ( argv[14], &out[0], 2 * N );
+  FILE *f = fopen ( argv[15], "w" );
+  fprintf ( f, "%.17g\n", regis.getEnergyOfLastSolution ( ) );
+  fclose ( f );
+  delete parser;
+}
+
 static int usage ( ) {
   fprintf ( stderr,
-    "ms_ref energy L R T px py lambda outPrefix\n"
+    "ms_ref energy[_ncc] L R T px py lambda outPrefix\n"
     "ms_ref smooth L sigma in out\n"
     "ms_ref restrict Lfine in out | prolong Lcoarse in out | resample Lsrc in Ldst out\n"
     "ms_ref deform L img px py out\n"
-    "ms_ref gdlevel L R T px py lambda maxIter stopEps outPhi outTrace\n"
-    "ms_ref register maxL start stop R T px py lambda lambdaFactor maxIter stopEps resample outPhi outTxt\n"
+    "ms_ref gdlevel[_ncc] L R T px py lambda maxIter stopEps outPhi outTrace\n"
+    "ms_ref register[_ncc] maxL start stop R T px py lambda lambdaFactor maxIter stopEps resample outPhi outTxt\n"
     "ms_ref normalize L in sat minToZero out\n"
     "ms_ref series maxL start stop lambda lambdaFactor maxIter stopEps sat minToZero F framesBin outPhis outMean outTxt\n" );
   return 1;
@@ -114,35 +200,23 @@ int main ( int argc, char **argv ) {
   if ( argc < 2 ) return usage ( );
   const std::string cmd = argv[1];
   try {
-    if ( cmd == "energy" && argc == 9 ) {
+    if ( ( cmd == "energy" || cmd == "energy_ncc" ) && argc == 9 ) {
       const int L = atoi ( argv[2] ), n = lvlN ( L ), N = n * n;
       qc::GridDefinition grid ( L, qc::QC_2D );
       ArrayType R ( grid ), T ( grid );
-      aol::MultiVector<RealType> phi ( 2, N ), de ( 2, N );
+      aol::MultiVector<RealType> phi ( 2, N );
       readBin ( argv[3], R.getData ( ), N ); readBin ( argv[4], T.getData ( ), N );
       readBin ( argv[5], phi[0].getData ( ), N ); readBin ( argv[6], phi[1].getData ( ), N );
       const RealType lambda = atof ( argv[7] );
-      qc::SSDEnergy<ConfType> ssd ( grid, R, T );
-      qc::SSDForce<ConfType> force ( grid, R, T );
-      qc::DirichletRegularizationConfigurator<ConfType> regul ( grid );
-      aol::LinCombOp<aol::MultiVector<RealType>, aol::Scalar<RealType> > E;
-      E.appendReference ( ssd ); E.appendReference ( regul.getRegERef ( ), lambda );
-      aol::LinCombOp<aol::MultiVector<RealType> > DE;
-      DE.appendReference ( force ); DE.appendReference ( regul.getRegDERef ( ), lambda );
-      aol::Scalar<RealType> essd, ereg, etot;
-      ssd.apply ( phi, essd ); regul.getRegERef ( ).apply ( phi, ereg ); E.apply ( phi, etot );
-      DE.apply ( phi, de );
-      aol::MultiVector<RealType> fo ( 2, N );
-      force.apply ( phi, fo );
-      std::vector<RealType> out ( 4 * N );
-      memcpy ( &out[0], de[0].getData ( ), N * sizeof ( RealType ) );
-      memcpy ( &out[N], de[1].getData ( ), N * sizeof ( RealType ) );
-      memcpy ( &out[2 * N], fo[0].getData ( ), N * sizeof ( RealType ) );
-      memcpy ( &out[3 * N], fo[1].getData ( ), N * sizeof ( RealType ) );
-      writeBin ( ( std::string ( argv[8] ) + "_de.bin" ).c_str ( ), &out[0], 4 * N );
-      FILE *f = fopen ( ( std::string ( argv[8] ) + ".txt" ).c_str ( ), "w" );
-      fprintf ( f, "%.17g %.17g %.17g\n", essd[0], ereg[0], etot[0] );
-      fclose ( f );
+      if ( cmd == "energy" ) {
+        qc::SSDEnergy<ConfType> ssd ( grid, R, T );
+        qc::SSDForce<ConfType> force ( grid, R, T );
+        energyCommand ( grid, ssd, force, phi, lambda, argv[8] );
+      } else {
+        qc::NormalizedCrossCorrelationEnergy<ConfType> ncc ( grid, R, T );
+        qc::VariationOfNormalizedCrossCorrelationEnergy<ConfType> var ( grid, R, T );
+        energyCommand ( grid, ncc, var, phi, lambda, argv[8] );
+      }
       return 0;
     }
     if ( cmd == "smooth" && argc == 6 ) {
@@ -196,7 +270,7 @@ int main ( int argc, char **argv ) {
       writeBin ( argv[6], out.getData ( ), N );
       return 0;
     }
-    if ( cmd == "gdlevel" && argc == 12 ) {
+    if ( ( cmd == "gdlevel" || cmd == "gdlevel_ncc" ) && argc == 12 ) {
       const int L = atoi ( argv[2] ), n = lvlN ( L ), N = n * n;
       qc::GridDefinition grid ( L, qc::QC_2D );
       ArrayType R ( grid ), T ( grid );
@@ -206,52 +280,20 @@ int main ( int argc, char **argv ) {
       const RealType lambda = atof ( argv[7] );
       const int maxIter = atoi ( argv[8] );
       const RealType stopEps = atof ( argv[9] );
-      // StandardRegistration::findTransformation + updateTransformationWithGD (registration.h:967-1021)
-      qc::SSDEnergy<ConfType> ssd ( grid, R, T );
-      qc::SSDForce<ConfType> force ( grid, R, T );
-      qc::DirichletRegularizationConfigurator<ConfType> regul ( grid );
-      aol::LinCombOp<aol::MultiVector<RealType>, aol::Scalar<RealType> > E;
-      E.appendReference ( ssd ); E.appendReference ( regul.getRegERef ( ), lambda );
-      aol::LinCombOp<aol::MultiVector<RealType> > DE;
-      DE.appendReference ( force ); DE.appendReference ( regul.getRegDERef ( ), lambda );
-      TracingGD gd ( grid, E, DE, maxIter, stopEps );
-      gd.setConfigurationFlags ( GDType::USE_NONLINEAR_CG | GDType::DO_NOT_WRITE_CONSOLE_OUTPUT );
-      gd.applySingle ( phi );
-      std::vector<RealType> out ( 2 * N );
-      memcpy ( &out[0], phi[0].getData ( ), N * sizeof ( RealType ) );
-      memcpy ( &out[N], phi[1].getData ( ), N * sizeof ( RealType ) );
-      writeBin ( argv[10], &out[0], 2 * N );
-      FILE *f = fopen ( argv[11], "w" );
-      fprintf ( f, "# iter energy tau sigma evals ; final %.17g steps %d\n", gd.getEnergyAtLastPosition ( ), gd.getIterations ( ) );
-      for ( size_t i = 0; i < gd.energies.size ( ); ++i )
-        fprintf ( f, "%d %.17g %.17g %.17g %d\n", ( int ) i, gd.energies[i], gd.taus[i], gd.sigmas[i], gd.evals[i] );
-      fclose ( f );
+      if ( cmd == "gdlevel" ) {
+        qc::SSDEnergy<ConfType> ssd ( grid, R, T );
+        qc::SSDForce<ConfType> force ( grid, R, T );
+        gdLevelCommand ( grid, ssd, force, phi, lambda, maxIter, stopEps, argv[10], argv[11] );
+      } else {
+        qc::NormalizedCrossCorrelationEnergy<ConfType> ncc ( grid, R, T );
+        qc::VariationOfNormalizedCrossCorrelationEnergy<ConfType> var ( grid, R, T );
+        gdLevelCommand ( grid, ncc, var, phi, lambda, maxIter, stopEps, argv[10], argv[11] );
+      }
       return 0;
     }
-    if ( cmd == "register" && argc == 16 ) {
-      const int maxL = atoi ( argv[2] ), start = atoi ( argv[3] ), stop = atoi ( argv[4] );
-      const int n = lvlN ( maxL ), N = n * n;
-      aol::ParameterParser *parser = makeParser ( maxL, start, stop, atof ( argv[9] ), atof ( argv[10] ), atoi ( argv[11] ),
-                                                  atof ( argv[12] ), atoi ( argv[13] ), -1, 0 );
-      RegisType regis ( *parser );
-      qc::GridDefinition grid ( maxL, qc::QC_2D );
-      ArrayType R ( grid ), T ( grid );
-      readBin ( argv[5], R.getData ( ), N ); readBin ( argv[6], T.getData ( ), N );
-      regis.initRefOrTemplate ( R, qc::REFERENCE, true );
-      regis.initRefOrTemplate ( T, qc::TEMPLATE, true );
-      qc::MultiArray<RealType, qc::QC_2D> phi ( grid );
-      readBin ( argv[7], phi[0].getData ( ), N ); readBin ( argv[8], phi[1].getData ( ), N );
-      regis.setTransformation ( phi );
-      regis.solveAndProlongToMaxDepth ( );
-      regis.getTransformation ( phi );
-      std::vector<RealType> out ( 2 * N );
-      memcpy ( &out[0], phi[0].getData ( ), N * sizeof ( RealType ) );
-      memcpy ( &out[N], phi[1].getData ( ), N * sizeof ( RealType ) );
-      writeBin ( argv[14], &out[0], 2 * N );
-      FILE *f = fopen ( argv[15], "w" );
-      fprintf ( f, "%.17g\n", regis.getEnergyOfLastSolution ( ) );
-      fclose ( f );
-      delete parser;
+    if ( ( cmd == "register" || cmd == "register_ncc" ) && argc == 16 ) {
+      if ( cmd == "register" ) registerCommand<RegisType> ( argv );
+      else registerCommand<RegisTypeNCC> ( argv );
       return 0;
     }
     if ( cmd == "normalize" && argc == 7 ) {

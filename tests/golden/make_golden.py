@@ -7,6 +7,8 @@ tests hold no golden vectors for this path, so these fixtures pin both the
 CPU oracle and the CUDA path.  Run from the repository root:
 
     make -f oracle/Makefile.ref && python tests/golden/make_golden.py
+
+(--ncc-only regenerates only the fixtures of the cross-correlation data term.)
 """
 from __future__ import annotations
 
@@ -105,16 +107,59 @@ def series(ref: msor.RefRunner, level: int, F: int, seed: int):
                         mean=mean, energies=np.array(info["energies"]), start=3, lam=0.1, max_iter=15)
 
 
+def ncc(ref: msor.RefRunner, level: int, seed: int, max_iter: int):
+    """Normalized cross-correlation data term: energy and variation at a small
+    displacement and at one that pushes points out of the domain, and a traced
+    level solve from zero."""
+    n = n_of(level)
+    rng = np.random.default_rng(seed)
+    fr, _, _ = syn.make_series(n, 2, syn.HEX_513, seed=seed)
+    R = ref.normalize(level, fr[0].ravel())
+    T = ref.normalize(level, fr[1].ravel())
+    px = rng.normal(0, 0.5 / (n - 1), n * n)
+    py = rng.normal(0, 0.5 / (n - 1), n * n)
+    bx = px.copy()
+    bx[: n] += 2.0 / (n - 1)
+    d = {"level": level, "R": R, "T": T, "px": px, "py": py, "px_out": bx, "lam": 0.1, "max_iter": max_iter}
+    for tag, qx in (("", px), ("_out", bx)):
+        r = ref.energy(level, R, T, qx, py, 0.1, ncc=True)
+        d["E" + tag] = np.array([r["essd"], r["ereg"], r["e"]])
+        d["DE" + tag] = np.stack([r["dex"], r["dey"]])
+        d["F" + tag] = np.stack([r["fx"], r["fy"]])
+    z = np.zeros(n * n)
+    gx, gy, e, steps, trace = ref.gd_level(level, R, T, z, z, 0.1, max_iter, ncc=True)
+    d.update(gd_px=gx, gd_py=gy, gd_energy=e, gd_steps=steps, gd_trace=np.array(trace, dtype=np.float64))
+    np.savez_compressed(os.path.join(OUT, f"ncc_L{level}.npz"), **d)
+
+
+def ncc_register(ref: msor.RefRunner, level: int, seed: int):
+    n = n_of(level)
+    fr, _, _ = syn.make_series(n, 2, syn.HEX_513, seed=seed)
+    R = ref.normalize(level, fr[0].ravel())
+    T = ref.normalize(level, fr[1].ravel())
+    px, py, e = ref.register(level, 4, level, R, T, lam=0.1, max_iter=15, ncc=True)
+    np.savez_compressed(os.path.join(OUT, f"ncc_register_L{level}.npz"), level=level, R=R, T=T, start=4,
+                        lam=0.1, max_iter=15, phi=np.stack([px, py]), E=np.array([e]))
+
+
 def main():
     if not msor.have_ref():
         raise SystemExit("oracle/_ref/ms_ref is missing: make -f oracle/Makefile.ref")
     ref = msor.RefRunner()
+    if "--ncc-only" in sys.argv:
+        ncc(ref, 5, 501, 20)
+        ncc(ref, 6, 502, 15)
+        ncc_register(ref, 7, 503)
+        return
     ops(ref, 5, 101)
     ops(ref, 6, 102)
     gd(ref, 5, 201, 0.1, 20)
     gd(ref, 6, 202, 0.05, 30)
     register(ref, 7, 301)
     series(ref, 6, 4, 401)
+    ncc(ref, 5, 501, 20)
+    ncc(ref, 6, 502, 15)
+    ncc_register(ref, 7, 503)
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(OUT, f)))
