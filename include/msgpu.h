@@ -45,12 +45,20 @@ typedef struct {
   int dont_normalize_input;    /* dontNormalizeInputImages                   */
   int resample_deformation;    /* resampleInsteadOfProlongateDeformation     */
   int use_fp64;                /* 0: FP32 bulk + FP64 reductions; 1: FP64   */
+  int data_term;               /* deformationModel's data term: 0 SSD
+                                  (SSDRegistrationConfigurator), 1 normalized
+                                  cross-correlation (NCCRegistrationConfigurator,
+                                  registration.h:1766-1780, 1909-2018)        */
 } msgpu_params;
 
 void msgpu_params_default(msgpu_params* p);
 int  msgpu_abi_version(void);
 
 int  msgpu_create(int device, msgpu_context** out);
+/* Data term (0 SSD, 1 NCC) of the single-operator entry points msgpu_energy
+ * and msgpu_gd_level of this context; the batch entry points take it from
+ * msgpu_params.data_term.                                                  */
+int  msgpu_set_data_term(msgpu_context* ctx, int data_term);
 int  msgpu_destroy(msgpu_context* ctx);
 const char* msgpu_last_error(const msgpu_context* ctx);
 
@@ -122,7 +130,9 @@ int msgpu_get_stats(const msgpu_context* ctx, msgpu_stats* out);
 
 /* --- single operators of the path (parity entry points) ----------------- */
 /* E = SSDEnergy + lambda * DisplacementLengthEnergy and DE = SSDForce +
- * lambda * L phi (registration.h:971-982, 1584-1667).  de_out: 2*N doubles. */
+ * lambda * L phi (registration.h:971-982, 1584-1667); with the NCC data term
+ * (msgpu_set_data_term) NormalizedCrossCorrelationEnergy and its variation
+ * (registration.h:1909-1983) instead of the SSD parts.  de_out: 2*N doubles. */
 int msgpu_energy(msgpu_context* ctx, int level, const double* R, const double* T, const double* phix,
                  const double* phiy, double lambda, int use_fp64, double* energy_out, double* de_out);
 /* LinearSmoothOp::apply with sigma (linearSmoothOp.cpp:591-612).          */

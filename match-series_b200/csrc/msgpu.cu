@@ -33,7 +33,8 @@ struct msgpu_context {
   cudaStream_t stream = nullptr;
   // growable device buffers
   struct Buf { void* p = nullptr; size_t cap = 0; };
-  Buf arena, shared_real, dscratch, small, phis_d, io[6], prof, sched, flags;
+  Buf arena, shared_real, dscratch, small, phis_d, io[6], prof, sched, flags, nccbuf;
+  int data_term = 0;           // data term of the single-operator entry points
   int* sched_error = nullptr;  // device flag of the level scheduler (in flags)
   // statistics of the last batch call
   bool profiling = false;
@@ -45,7 +46,7 @@ struct msgpu_context {
 
 namespace {
 
-constexpr int kAbiVersion = 1;
+constexpr int kAbiVersion = 2;
 
 int fail(msgpu_context* ctx, int code, const char* fmt, ...) {
   char buf[512];
@@ -144,6 +145,33 @@ void host_fe_tables(FeTables& t) {
       const int node = rep[cx] + rep[cy] * n;
       for (int j = 0; j < 3; ++j)
         for (int i = 0; i < 3; ++i) t.st[cx + 3 * cy][j][i] = st[(size_t)node * 9 + j * 3 + i];
+    }
+  // mass matrix (FELinScalarWeightedMassInterface::prepareLocalMatrix,
+  // FEOpInterface.h:1445-1475) with element volume 1, same assembly
+  double M[4][4];
+  for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) M[i][j] = 0.;
+  for (int q = 0; q < 4; ++q)
+    for (int i = 0; i < 4; ++i) {
+      const double basisi = t.bq[i][q];
+      for (int j = i; j < 4; ++j) M[i][j] += basisi * t.bq[j][q] * 1. * t.w;
+    }
+  for (int i = 0; i < 4; ++i)
+    for (int j = i; j < 4; ++j) M[j][i] = M[i][j] = M[i][j] * 1.0;
+  std::vector<double> ms((size_t)n * n * 9, 0.0);
+  for (int ey = 0; ey < n - 1; ++ey)
+    for (int ex = 0; ex < n - 1; ++ex)
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) {
+          const int gi = ex + ey * n + ((i & 1) ? 1 : 0) + ((i & 2) ? n : 0);
+          const int gj = ex + ey * n + ((j & 1) ? 1 : 0) + ((j & 2) ? n : 0);
+          const int dx = (gj % n) - (gi % n), dy = (gj / n) - (gi / n);
+          ms[(size_t)gi * 9 + (dy + 1) * 3 + (dx + 1)] += 1.0 * M[i][j];
+        }
+  for (int cy = 0; cy < 3; ++cy)
+    for (int cx = 0; cx < 3; ++cx) {
+      const int node = rep[cx] + rep[cy] * n;
+      for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) t.ms[cx + 3 * cy][j][i] = ms[(size_t)node * 9 + j * 3 + i];
     }
 }
 
@@ -361,6 +389,57 @@ __global__ void k_set_buf(int* buf, int n, int v) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) buf[i] = v;
 }
 
+// normalizeImageForNCC of the reference image of a level by one CTA
+// (registration.h:1932-1944): u = R - sum_i (M R)_i, var = sqrt(u . M u),
+// out = u / var (u when var is within 1e-15 of 0).  Sums are deterministic
+// (fixed thread assignment, warps reduced in order).
+template <typename Real>
+__global__ void k_ncc_normalize(const Real* __restrict__ R, int level, Real* out) {
+  const int n = lvl_n(level), P = pitch_of(n), N = n * n;
+  const Real h = (Real)(1.0 / (double)(n - 1)), hh = h * h;
+  __shared__ double red[32];
+  __shared__ double val;
+  auto block_sum = [&](double v) -> double {
+    v = warp_sum(v);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+      val = t;
+    }
+    __syncthreads();
+    return val;
+  };
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    const int x = i % n, y = i / n;
+    acc += (double)mass_row<Real>(x, y, n, hh, [&](int X, int Y) { return R[(size_t)Y * P + X]; });
+  }
+  const Real m = (Real)(-block_sum(acc));
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    const size_t g = (size_t)(i / n) * P + (i % n);
+    Real u = R[g];
+    u += m;
+    out[g] = u;
+  }
+  __syncthreads();
+  acc = 0.0;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    const int x = i % n, y = i / n;
+    const Real mu = mass_row<Real>(x, y, n, hh, [&](int X, int Y) { return out[(size_t)Y * P + X]; });
+    acc += (double)(out[(size_t)y * P + x] * mu);
+  }
+  const double var = sqrt(block_sum(acc));
+  if (!(fabs(var - 0.0) < 1e-15)) {
+    const Real v = (Real)var;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+      const size_t g = (size_t)(i / n) * P + (i % n);
+      out[g] /= v;
+    }
+  }
+}
+
 // phi of every instance at the given level -> double output (F x 2 x N, dense).
 template <typename Real>
 __global__ void k_phi_out(const Real* arena, size_t inst_stride, size_t off0, size_t off1, int level,
@@ -451,11 +530,12 @@ __global__ void k_mean(const double* a, int N, double* out) {
 struct Layout {
   size_t off_T[kMaxLevel + 1];
   size_t off_phi[2], off_d[2], off_s, off_de;
+  size_t off_td;   // NCC only: deformed template at the nodes
   size_t off_x2[kMaxLevel + 1], off_x5[kMaxLevel + 1], off_b[kMaxLevel + 1];
   size_t stride;
 };
 
-Layout make_layout(int M) {
+Layout make_layout(int M, bool ncc = false) {
   Layout L;
   size_t off = 0;
   const size_t a = 64;
@@ -466,6 +546,8 @@ Layout make_layout(int M) {
   for (int b = 0; b < 2; ++b) { L.off_d[b] = off; off = align_up(off + two, a); }
   L.off_s = off; off = align_up(off + two, a);
   L.off_de = off; off = align_up(off + two, a);
+  L.off_td = 0;
+  if (ncc) { L.off_td = off; off = align_up(off + comp_stride(M), a); }
   for (int k = 0; k <= kMaxLevel; ++k) {
     if (k <= M) {
       L.off_x2[k] = off; off = align_up(off + 2 * comp_stride(k), a);
@@ -606,10 +688,12 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
   const int start = p.start_level, stop = p.stop_level;
   const int nimg = F + 1;  // image 0 is the reference
   const size_t Nin = lvl_N(Lin);
-  const Layout L = make_layout(M);
+  const bool ncc = p.data_term == 1;
+  const Layout L = make_layout(M, ncc);
   int rc;
   if ((rc = ensure_tables(ctx))) return rc;
   if ((rc = sched_error_reset(ctx, st))) return rc;
+  if (ncc && (rc = ensure(ctx, ctx->nccbuf, sizeof(Real) * (comp_stride(M) + 64)))) return rc;
   // --- double scratch: per image a pyramid from Lin down to 0
   std::vector<size_t> poff(Lin + 1);
   size_t pstride = 0;
@@ -715,6 +799,13 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
     a.arena = arena;
     a.inst_stride = L.stride;
     a.R = Rpyr + L.off_T[l];
+    if (ncc) {
+      a.ncc = 1;
+      a.normR = (const Real*)ctx->nccbuf.p;
+      a.off_td = L.off_td;
+      k_ncc_normalize<Real><<<1, 1024, 0, st>>>(a.R, l, (Real*)ctx->nccbuf.p);
+      ++launches;
+    }
     a.off_T = L.off_T[l];
     a.off_phi[0] = L.off_phi[0];
     a.off_phi[1] = L.off_phi[1];
@@ -815,6 +906,8 @@ int check_params(msgpu_context* ctx, const msgpu_params* p) {
     return fail(ctx, MSGPU_ERR_INVALID_ARG, "level range startLevel %d .. stopLevel %d invalid for precisionLevel %d",
                 p->start_level, p->stop_level, p->precision_level);
   if (p->max_gd_iterations < 0) return fail(ctx, MSGPU_ERR_INVALID_ARG, "maxGDIterations < 0");
+  if (p->data_term != 0 && p->data_term != 1)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "data_term %d: 0 (SSD) or 1 (NCC)", p->data_term);
   return MSGPU_OK;
 }
 
@@ -847,6 +940,14 @@ void msgpu_params_default(msgpu_params* p) {
 }
 
 int msgpu_abi_version(void) { return kAbiVersion; }
+
+int msgpu_set_data_term(msgpu_context* ctx, int data_term) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (data_term != 0 && data_term != 1)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "data_term %d: 0 (SSD) or 1 (NCC)", data_term);
+  ctx->data_term = data_term;
+  return MSGPU_OK;
+}
 
 int msgpu_create(int device, msgpu_context** out) {
   if (!out) return MSGPU_ERR_INVALID_ARG;
@@ -1064,7 +1165,9 @@ int single_level(msgpu_context* ctx, int level, int mode, const double* R, const
                  double* de_out, double* trace, int max_trace) {
   int rc;
   if ((rc = ensure_tables(ctx))) return rc;
-  const Layout L = make_layout(level);
+  const bool ncc = ctx->data_term == 1 && mode != MODE_SMOOTH;
+  const Layout L = make_layout(level, ncc);
+  if (ncc && (rc = ensure(ctx, ctx->nccbuf, sizeof(Real) * (comp_stride(level) + 64)))) return rc;
   const size_t N = lvl_N(level);
   if ((rc = ensure(ctx, ctx->arena, sizeof(Real) * L.stride))) return rc;
   if ((rc = ensure(ctx, ctx->shared_real, sizeof(Real) * (comp_stride(level) + 64)))) return rc;
@@ -1098,6 +1201,12 @@ int single_level(msgpu_context* ctx, int level, int mode, const double* R, const
   a.arena = arena;
   a.inst_stride = L.stride;
   a.R = Rd;
+  if (ncc) {
+    a.ncc = 1;
+    a.normR = (const Real*)ctx->nccbuf.p;
+    a.off_td = L.off_td;
+    k_ncc_normalize<Real><<<1, 1024, 0, st>>>(Rd, level, (Real*)ctx->nccbuf.p);
+  }
   a.off_T = L.off_T[level];
   a.off_phi[0] = L.off_phi[0];
   a.off_phi[1] = L.off_phi[1];

@@ -28,6 +28,10 @@ struct FeTables {
   // c = 0 (first node), 1 (interior), 2 (last node) along each axis;
   // entry [class][j+1][i+1] couples node (x,y) with (x+i, y+j).
   double st[9][3][3];
+  // Assembled Q1 mass stencil (MassOp ASSEMBLED, FEOpInterface.h:2382-2394,
+  // local matrix 1445-1475) for element volume 1; the stencil of a level is
+  // this times h^2, an exact power-of-two scaling.
+  double ms[9][3][3];
 };
 
 __constant__ FeTables c_fe;
@@ -206,6 +210,108 @@ __device__ __forceinline__ Real stiff_row(int x, int y, int n, Get get) {
       if (X >= 0 && X < n && Y >= 0 && Y < n) d += Real(c_fe.st[cls][j + 1][i + 1]) * get(X, Y);
     }
   return d;
+}
+
+// Assembled mass row at node (x,y) applied to u, same order as stiff_row;
+// hh = h^2.
+template <typename Real, typename Get>
+__device__ __forceinline__ Real mass_row(int x, int y, int n, Real hh, Get get) {
+  const int cls = node_class(x, n) + 3 * node_class(y, n);
+  Real d = Real(0);
+#pragma unroll
+  for (int j = -1; j <= 1; ++j)
+#pragma unroll
+    for (int i = -1; i <= 1; ++i) {
+      const int X = x + i, Y = y + j;
+      if (X >= 0 && X < n && Y >= 0 && Y < n) d += (Real(c_fe.ms[cls][j + 1][i + 1]) * hh) * get(X, Y);
+    }
+  return d;
+}
+
+// FastDeformImage at node (x,y) (deformations.h:138-159): position
+// x + phi/h clamped to the grid, then ScalarArray::interpolate
+// (scalarArray.h:499-525) of the pitched image T.  inv_h = 2^l makes the
+// division by h an exact product.
+template <typename Real>
+__device__ __forceinline__ Real fast_deform_node(const Real* __restrict__ T, int n, int P, int x, int y, Real px,
+                                                 Real py, Real inv_h) {
+  const Real hi = Real(n - 1);
+  Real X = Real(x) + px * inv_h, Y = Real(y) + py * inv_h;
+  X = X < Real(0) ? Real(0) : (X > hi ? hi : X);
+  Y = Y < Real(0) ? Real(0) : (Y > hi ? hi : Y);
+  int xL = (int)X, yL = (int)Y;
+  if (X >= hi) xL = n - 2;
+  if (Y >= hi) yL = n - 2;
+  X -= Real(xL);
+  Y -= Real(yL);
+  const Real* p = T + (size_t)yL * P + xL;
+  const Real v0 = __ldg(p), v1 = __ldg(p + 1);
+  if (Y == Real(0)) return (Real(1) - X) * v0 + X * v1;
+  const Real v2 = __ldg(p + P), v3 = __ldg(p + P + 1);
+  return (Real(1) - X) * (Real(1) - Y) * v0 + X * (Real(1) - Y) * v1 + (Real(1) - X) * Y * v2 + X * Y * v3;
+}
+
+// transformCoord<ConfiguratorType, false> (deformations.h:622-668) of
+// quadrature point q of element (ex,ey): grid coordinates El + RefCoord +
+// offset / h without clipping; false when the point leaves the grid.
+template <typename Real>
+__device__ __forceinline__ bool transform_noclip_axis(Real coord, Real off, int n, Real inv_h, int& el, Real& loc) {
+  const Real tc = coord + off * inv_h;
+  int e = (short)tc;
+  Real l = tc - Real(e);
+  if (e == n - 1 && l == Real(0)) {
+    e = n - 2;
+    l = Real(1);
+  }
+  el = e;
+  loc = l;
+  return !(tc < Real(0) || e < 0 || e >= n - 1);
+}
+
+// CrossCorrelationForce nonlinearity at the 4 quadrature points and its
+// integration against the 4 basis functions (registration.h:1849-1861,
+// FEOpInterface.h:1821-1848): out[b][c] = vol * sum_q nl[q][c] * bq[b][q] * w
+// with nl = -temp(x_q) * grad T(transformed x_q), 0 outside the grid.
+template <typename Real>
+__device__ __forceinline__ void element_ncc_force(const Real* __restrict__ T, int n, int P, Real h, int ex, int ey,
+                                                  const Real px[4], const Real py[4], const Real tmp[4],
+                                                  Real out[4][2]) {
+  Real nl[4][2];
+  const Real inv_h = Real(n - 1);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const Real ox = at_quad(px, q);
+    const Real oy = at_quad(py, q);
+    int elx, ely;
+    Real lx, ly;
+    const bool inx = transform_noclip_axis(Real(ex) + Real(c_fe.rc[q][0]), ox, n, inv_h, elx, lx);
+    const bool iny = inx && transform_noclip_axis(Real(ey) + Real(c_fe.rc[q][1]), oy, n, inv_h, ely, ly);
+    if (!iny) {
+      nl[q][0] = Real(0);
+      nl[q][1] = Real(0);
+      continue;
+    }
+    Real t[4];
+    load_texels(T, P, elx, ely, t);
+    Real gx, gy;
+    q1_grad(t, lx, ly, inv_h, gx, gy);
+    const Real f = -at_quad(tmp, q);
+    nl[q][0] = gx * f;
+    nl[q][1] = gy * f;
+  }
+  const Real vol = h * h;
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    Real a0 = Real(0), a1 = Real(0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const Real f = Real(c_fe.bq[b][q]) * Real(c_fe.w);
+      a0 += nl[q][0] * f;
+      a1 += nl[q][1] * f;
+    }
+    out[b][0] = vol * a0;
+    out[b][1] = vol * a1;
+  }
 }
 
 // HeatEquation2DFD::apply at one node (linearSmoothOp.cpp:61-146):

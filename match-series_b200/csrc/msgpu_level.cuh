@@ -82,6 +82,10 @@ struct LevelArgs {
   double* trace;            // optional: per instance max_trace rows of (energy, tau, sigma, evals)
   int max_trace;
   unsigned long long* pass_cycles;  // optional: per CTA kPassKinds clock64 totals
+  // normalized cross-correlation data term (ncc != 0)
+  int ncc;
+  const Real* normR;        // normalised reference on this level, pitched (shared)
+  size_t off_td;            // per instance: deformed template at the nodes (1 component)
 };
 
 // A 2-component array of level k occupies 2 * comp_stride(k) elements.
@@ -450,6 +454,279 @@ struct GradPass {
 };
 
 // ---------------------------------------------------------------------------
+// Normalized cross-correlation data term (NormalizedCrossCorrelationEnergy,
+// registration.h:1909-1983).  One energy evaluation is three passes, each
+// followed by a global sum:
+//   sub 1: Td = FastDeformImage(T, p) at the nodes, sum_i (M Td)_i   (mean)
+//   sub 2: u = Td - mean,                     sum_i u_i (M u)_i      (var^2)
+//   sub 3: normT = u / var,                   sum_i (M normT)_i normR_i
+// and E_ncc = -(last sum) (normalizeImageForNCC, computeEnergy,
+// registration.h:1932-1962).  The position p of sub 1 depends on the purpose:
+//   E0:   p = phi; also A = phi . L phi                     -> part[1]
+//   GRAD: p = phi + tau_p d (pending step), written to nphi
+//   TRIAL: p = phi + tau d
+//   NCG:  d = s + beta od materialised (written), p = phi + tau d,
+//         Df = DE . d, B = phi . L d, C = d . L d           -> part[1..3]
+// Windows (EWX x EWY, origin (x0-4, y0-1)) per stage: sub 1 as the energy
+// passes (phx phy [dx dy | sx sy odx ody]); sub 2: Td; sub 3: Td normR.
+// Work window: Td (sub 1) or u / normT (subs 2, 3).
+enum NccMode : int { NM_E0 = 0, NM_GRAD, NM_TRIAL, NM_NCG };
+
+template <typename Real>
+struct NccPass {
+  Inst<Real> I;
+  int sub, mode;
+  Real tau, beta;
+  double mean, var;
+  bool od_zero, step;
+  const Real *phx, *phy, *dx, *dy, *sx, *sy, *dex, *dey, *normR;
+  Real *wdx, *wdy, *nphx, *nphy, *td;
+  Real* sm;
+  int nwin;
+  double* part;
+  Tiles tl;
+
+  __device__ NccPass(const Inst<Real>& I_, int sub_, int mode_, Real tau_, Real beta_, double mean_, double var_,
+                     bool odz, bool step_, const Real* phx_, const Real* phy_, const Real* dx_, const Real* dy_,
+                     const Real* sx_, const Real* sy_, const Real* dex_, const Real* dey_, const Real* normR_,
+                     Real* wdx_, Real* wdy_, Real* nphx_, Real* nphy_, Real* td_, Real* sm_, double* part_)
+      : I(I_), sub(sub_), mode(mode_), tau(tau_), beta(beta_), mean(mean_), var(var_), od_zero(odz), step(step_),
+        phx(phx_), phy(phy_), dx(dx_), dy(dy_), sx(sx_), sy(sy_), dex(dex_), dey(dey_), normR(normR_), wdx(wdx_),
+        wdy(wdy_), nphx(nphx_), nphy(nphy_), td(td_), sm(sm_), part(part_), tl(I_.n) {
+    if (sub == 1) nwin = (mode == NM_NCG) ? 6 : ((mode == NM_TRIAL || (mode == NM_GRAD && step)) ? 4 : 2);
+    else nwin = (sub == 2) ? 1 : 2;
+  }
+  __device__ Real* win(int stage, int k) const { return sm + ((size_t)stage * nwin + k) * EWIN; }
+  __device__ Real* work() const { return sm + (size_t)2 * nwin * EWIN; }
+
+  __device__ void issue(int t, int stage) {
+    int x0, x1, y0, y1;
+    tl.rect(t, x0, x1, y0, y1);
+    const int wx0 = x0 - 4, wy0 = y0 - 1, n = I.n, P = I.P;
+    if (sub == 1) {
+      load_window(win(stage, 0), phx, n, P, wx0, wy0, EWX, EWY);
+      load_window(win(stage, 1), phy, n, P, wx0, wy0, EWX, EWY);
+      if (mode == NM_TRIAL || (mode == NM_GRAD && step)) {
+        load_window(win(stage, 2), dx, n, P, wx0, wy0, EWX, EWY);
+        load_window(win(stage, 3), dy, n, P, wx0, wy0, EWX, EWY);
+      } else if (mode == NM_NCG) {
+        load_window(win(stage, 2), sx, n, P, wx0, wy0, EWX, EWY);
+        load_window(win(stage, 3), sy, n, P, wx0, wy0, EWX, EWY);
+        if (!od_zero) {
+          load_window(win(stage, 4), dx, n, P, wx0, wy0, EWX, EWY);
+          load_window(win(stage, 5), dy, n, P, wx0, wy0, EWX, EWY);
+        }
+      }
+    } else {
+      load_window(win(stage, 0), td, n, P, wx0, wy0, EWX, EWY);
+      if (sub == 3) load_window(win(stage, 1), normR, n, P, wx0, wy0, EWX, EWY);
+    }
+  }
+
+  __device__ void compute(int t, int stage) {
+    int x0, x1, y0, y1;
+    tl.rect(t, x0, x1, y0, y1);
+    const int n = I.n, P = I.P;
+    const Real hh = I.h * I.h, inv_h = Real(n - 1);
+    auto at = [&](int x, int y) { return (y - (y0 - 1)) * EWX + (x - (x0 - 4)); };
+    Real* W = work();
+    // nodes of the tile and a one-node halo (the mass stencil's support)
+    const int hx0 = max(x0 - 1, 0), hx1 = min(x1 + 1, n), hy0 = max(y0 - 1, 0), hy1 = min(y1 + 1, n);
+    if (sub == 1) {
+      const Real* Wpx = win(stage, 0);
+      const Real* Wpy = win(stage, 1);
+      const Real* Wa = (nwin >= 4) ? win(stage, 2) : nullptr;
+      const Real* Wb = (nwin >= 4) ? win(stage, 3) : nullptr;
+      const Real* Wox = (mode == NM_NCG) ? win(stage, 4) : nullptr;
+      const Real* Woy = (mode == NM_NCG) ? win(stage, 5) : nullptr;
+      const bool moves = (mode == NM_TRIAL || mode == NM_NCG || (mode == NM_GRAD && step));
+      auto dirx = [&](int i) -> Real {
+        if (mode != NM_NCG || od_zero) return Wa[i];
+        return Wa[i] + beta * Wox[i];
+      };
+      auto diry = [&](int i) -> Real {
+        if (mode != NM_NCG || od_zero) return Wb[i];
+        return Wb[i] + beta * Woy[i];
+      };
+      for_rect(hx1 - hx0, hy1 - hy0, [&](int ix, int iy) {
+        const int x = hx0 + ix, y = hy0 + iy;
+        const int c = at(x, y);
+        Real vx = Wpx[c], vy = Wpy[c];
+        if (moves) {
+          // newPosition = phi + tau * d (gradientDescent.h:176-178, 385-387)
+          vx += tau * dirx(c);
+          vy += tau * diry(c);
+        }
+        W[c] = fast_deform_node(I.T, n, P, x, y, vx, vy, inv_h);
+        if (x >= x0 && x < x1 && y >= y0 && y < y1) {
+          const size_t g = (size_t)y * P + x;
+          td[g] = W[c];
+          if (mode == NM_GRAD) {
+            nphx[g] = vx;
+            nphy[g] = vy;
+          }
+        }
+      });
+      __syncthreads();
+      for_2d<64>(x1 - x0, y1 - y0, [&](int ix, int iy) {
+        const int x = x0 + ix, y = y0 + iy;
+        const int c = at(x, y);
+        part[0] += (double)mass_row<Real>(x, y, n, hh, [&](int X, int Y) { return W[at(X, Y)]; });
+        if (mode == NM_E0) {
+          const Real lx = stiff_row<Real>(x, y, n, [&](int X, int Y) { return Wpx[at(X, Y)]; });
+          const Real ly = stiff_row<Real>(x, y, n, [&](int X, int Y) { return Wpy[at(X, Y)]; });
+          part[1] += (double)Wpx[c] * (double)lx + (double)Wpy[c] * (double)ly;
+        } else if (mode == NM_NCG) {
+          const Real ddx = dirx(c), ddy = diry(c);
+          const size_t g = (size_t)y * P + x;
+          wdx[g] = ddx;
+          wdy[g] = ddy;
+          const Real lx = stiff_row<Real>(x, y, n, [&](int X, int Y) { return dirx(at(X, Y)); });
+          const Real ly = stiff_row<Real>(x, y, n, [&](int X, int Y) { return diry(at(X, Y)); });
+          part[1] += (double)__ldcg(dex + g) * (double)ddx + (double)__ldcg(dey + g) * (double)ddy;
+          part[2] += (double)Wpx[c] * (double)lx + (double)Wpy[c] * (double)ly;
+          part[3] += (double)ddx * (double)lx + (double)ddy * (double)ly;
+        }
+      });
+      return;
+    }
+    // subs 2 and 3: u = Td + (-mean) (addToAll), normT = u / var
+    const Real* Wt = win(stage, 0);
+    const Real m = (Real)(-mean), vr = (Real)var;
+    const bool divide = !(fabs(var - 0.0) < 1e-15);  // aol::appeqAbsolute (aol.h:791-794)
+    for_rect(hx1 - hx0, hy1 - hy0, [&](int ix, int iy) {
+      const int c = at(hx0 + ix, hy0 + iy);
+      Real u = Wt[c];
+      u += m;
+      if (sub == 3 && divide) u /= vr;
+      W[c] = u;
+    });
+    __syncthreads();
+    const Real* Wr = (sub == 3) ? win(stage, 1) : nullptr;
+    for_2d<64>(x1 - x0, y1 - y0, [&](int ix, int iy) {
+      const int x = x0 + ix, y = y0 + iy;
+      const int c = at(x, y);
+      const Real mu = mass_row<Real>(x, y, n, hh, [&](int X, int Y) { return W[at(X, Y)]; });
+      if (sub == 2) part[0] += (double)(W[c] * mu);
+      else part[0] += (double)(mu * Wr[c]);
+    });
+  }
+};
+
+// Variation of the NCC energy at phi (applyDerivative, registration.h:
+// 1972-1983): temp = (normR + E normT) / var, CrossCorrelationForce with
+// temp as the weight (registration.h:1828-1862), plus lambda L phi; the
+// force contributions are staged per element and summed per node in the
+// reference's element order (as the SSD gradient pass).  A = phi . L phi ->
+// part[1].  Windows per stage: phx phy Td normR; work: temp window and
+// GCY x GCX x 8 contributions.
+template <typename Real>
+struct NccForcePass {
+  Inst<Real> I;
+  double lambda, mean, var, energy;
+  const Real *phx, *phy, *td, *normR;
+  Real *dex, *dey;
+  Real* sm;
+  double* part;
+  Tiles tl;
+  static constexpr int kWin = 4;
+
+  __device__ NccForcePass(const Inst<Real>& I_, double lam, double mean_, double var_, double e_, const Real* phx_,
+                          const Real* phy_, const Real* td_, const Real* normR_, Real* dex_, Real* dey_, Real* sm_,
+                          double* part_)
+      : I(I_), lambda(lam), mean(mean_), var(var_), energy(e_), phx(phx_), phy(phy_), td(td_), normR(normR_),
+        dex(dex_), dey(dey_), sm(sm_), part(part_), tl(I_.n) {}
+  __device__ Real* win(int stage, int k) const { return sm + ((size_t)stage * kWin + k) * EWIN; }
+  __device__ Real* tmpw() const { return sm + (size_t)2 * kWin * EWIN; }
+  __device__ Real* contrib() const { return sm + (size_t)(2 * kWin + 1) * EWIN; }
+
+  __device__ void issue(int t, int stage) {
+    int x0, x1, y0, y1;
+    tl.rect(t, x0, x1, y0, y1);
+    const int wx0 = x0 - 4, wy0 = y0 - 1, n = I.n, P = I.P;
+    load_window(win(stage, 0), phx, n, P, wx0, wy0, EWX, EWY);
+    load_window(win(stage, 1), phy, n, P, wx0, wy0, EWX, EWY);
+    load_window(win(stage, 2), td, n, P, wx0, wy0, EWX, EWY);
+    load_window(win(stage, 3), normR, n, P, wx0, wy0, EWX, EWY);
+  }
+
+  __device__ void compute(int t, int stage) {
+    int x0, x1, y0, y1;
+    tl.rect(t, x0, x1, y0, y1);
+    const int n = I.n, ne = n - 1;
+    const Real* Wpx = win(stage, 0);
+    const Real* Wpy = win(stage, 1);
+    const Real* Wt = win(stage, 2);
+    const Real* Wr = win(stage, 3);
+    Real* Wm = tmpw();
+    auto at = [&](int x, int y) { return (y - (y0 - 1)) * EWX + (x - (x0 - 4)); };
+    // 1. temp on the nodes of the elements [x0-1, x1) x [y0-1, y1)
+    {
+      const Real m = (Real)(-mean), vr = (Real)var, e = (Real)energy;
+      const bool divide = !(fabs(var - 0.0) < 1e-15);
+      const int hx0 = max(x0 - 1, 0), hx1 = min(x1 + 1, n), hy0 = max(y0 - 1, 0), hy1 = min(y1 + 1, n);
+      for_rect(hx1 - hx0, hy1 - hy0, [&](int ix, int iy) {
+        const int c = at(hx0 + ix, hy0 + iy);
+        Real nt = Wt[c];
+        nt += m;
+        if (divide) nt /= vr;
+        Real v = Wr[c];
+        v += nt * e;                 // addMultiple (vec.cpp:768-777)
+        if (divide) v /= vr;
+        Wm[c] = v;
+      });
+    }
+    __syncthreads();
+    // 2. element contributions
+    Real* C = contrib();
+    const int cw = (x1 < ne ? x1 : ne) - (x0 - 1), ch = (y1 < ne ? y1 : ne) - (y0 - 1);
+    for_rect(cw, ch, [&](int ix, int iy) {
+      const int ex = x0 - 1 + ix, ey = y0 - 1 + iy;
+      if (ex < 0 || ey < 0) return;
+      const int c0 = at(ex, ey);
+      const int idx[4] = {c0, c0 + 1, c0 + EWX, c0 + EWX + 1};
+      Real px[4], py[4], tm[4];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        px[b] = Wpx[idx[b]];
+        py[b] = Wpy[idx[b]];
+        tm[b] = Wm[idx[b]];
+      }
+      Real out[4][2];
+      element_ncc_force(I.T, n, I.P, I.h, ex, ey, px, py, tm, out);
+      Real* cc = C + ((size_t)(ey - (y0 - 1)) * GCX + (ex - (x0 - 1))) * 8;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        cc[2 * b] = out[b][0];
+        cc[2 * b + 1] = out[b][1];
+      }
+    });
+    __syncthreads();
+    // 3. node sums in element order, stiffness, outputs
+    const Real lam = (Real)lambda;
+    for_2d<64>(x1 - x0, y1 - y0, [&](int ix, int iy) {
+      const int x = x0 + ix, y = y0 + iy;
+      auto cc = [&](int ex, int ey, int b, int comp) {
+        return C[((size_t)(ey - (y0 - 1)) * GCX + (ex - (x0 - 1))) * 8 + 2 * b + comp];
+      };
+      Real fx = Real(0), fy = Real(0);
+      if (x - 1 >= 0 && y - 1 >= 0) { fx += cc(x - 1, y - 1, 3, 0); fy += cc(x - 1, y - 1, 3, 1); }
+      if (x < ne && y - 1 >= 0)     { fx += cc(x, y - 1, 2, 0);     fy += cc(x, y - 1, 2, 1); }
+      if (x - 1 >= 0 && y < ne)     { fx += cc(x - 1, y, 1, 0);     fy += cc(x - 1, y, 1, 1); }
+      if (x < ne && y < ne)         { fx += cc(x, y, 0, 0);         fy += cc(x, y, 0, 1); }
+      const Real Lx = stiff_row<Real>(x, y, n, [&](int X, int Y) { return Wpx[at(X, Y)]; });
+      const Real Ly = stiff_row<Real>(x, y, n, [&](int X, int Y) { return Wpy[at(X, Y)]; });
+      const Real gx = (lambda != 1.0) ? fx + lam * Lx : fx + Lx;
+      const Real gy = (lambda != 1.0) ? fy + lam * Ly : fy + Ly;
+      const size_t g = (size_t)y * I.P + x;
+      dex[g] = gx;
+      dey[g] = gy;
+      part[1] += (double)Wpx[at(x, y)] * (double)Lx + (double)Wpy[at(x, y)] * (double)Ly;
+    });
+  }
+};
+
+// ---------------------------------------------------------------------------
 // Multigrid V-cycle passes on the levels above lc (tiled passes).
 
 // Pre-smoothing (2 Jacobi sweeps from x = 0), residual and restriction
@@ -761,6 +1038,10 @@ __host__ __device__ inline size_t level_smem_elems(int lc) {
   const size_t d = (size_t)2 * 2 * VWIN + (size_t)6 * VWIN;      // down
   const size_t u = (size_t)2 * (4 * VWIN + 2 * CWIN) + 2 * VWIN;  // up
   const size_t c = coarse_smem_elems(lc);
+  const size_t n1 = (size_t)(2 * 6 + 1) * EWIN;                       // NCC energy, NCG purpose
+  const size_t nf = (size_t)(2 * 4 + 1) * EWIN + (size_t)GCX * GCY * 8; // NCC variation
+  if (n1 > e) e = n1;
+  if (nf > e) e = nf;
   if (g > e) e = g;
   if (d > e) e = d;
   if (u > e) e = u;
@@ -792,7 +1073,11 @@ __device__ __forceinline__ bool finite_d(double x) { return !isnan(x) && !isinf(
 // was published takes a valid chunk of that pass, whose descriptor was written
 // (and fenced) before the word.  Every wait for work is
 // bounded; a worker that gives up sets the error flag and all workers return.
-enum TaskKind : int { TK_E0 = 0, TK_GRAD, TK_VDOWN, TK_COARSE, TK_VUP, TK_NCG, TK_TRIAL, TK_FLUSH, TK_DONE };
+enum TaskKind : int {
+  TK_E0 = 0, TK_GRAD, TK_VDOWN, TK_COARSE, TK_VUP, TK_NCG, TK_TRIAL, TK_FLUSH,
+  TK_N1, TK_N2, TK_N3, TK_NF,   // NCC data term: energy subs 1-3, variation
+  TK_DONE
+};
 __device__ __forceinline__ int task_pass_kind(int kind) {
   switch (kind) {
     case TK_E0: return PK_ENERGY0;
@@ -801,6 +1086,7 @@ __device__ __forceinline__ int task_pass_kind(int kind) {
     case TK_COARSE: return PK_VCOARSE;
     case TK_VUP: return PK_VUP;
     case TK_NCG: return PK_NCG;
+    case TK_NF: return PK_GRAD;
     default: return PK_ENERGY;
   }
 }
@@ -810,9 +1096,11 @@ constexpr int PF_ODZERO = 2;   // NCG: the old direction is zero (d = s)
 struct PassDesc {
   int kind, k, cur, dcur, dn, flags;
   int ntiles, chunk;   // tiles of the pass, tiles per dispensed chunk
+  int purpose;   // NCC energy subs: the pass they stand for (TK_E0, TK_GRAD, TK_TRIAL, TK_NCG)
   double t;      // trial step (NCG, TRIAL) or pending step (GRAD, FLUSH)
   double beta;   // Fletcher-Reeves factor (NCG)
   double vtau;   // tau of the V-cycle passes
+  double mean, var, e;   // NCC: mass mean and norm of the deformed template, NCC energy
 };
 
 // Descent state of one instance; written only by the CTA completing a pass.
@@ -823,6 +1111,7 @@ struct InstCtl {
   int iter, evals, total_evals, attempt, rb_pos, pending, od_zero, cur, dcur;
   double energy, energy_new, f, sigma, sigma_used, tau, og2, A, Bd, Cd, Df, t, beta, tau_p;
   double rb_tau[2], rb_e[2];
+  double n1[kRedSlots];      // NCC: totals of energy sub 1 (mean, then A or Df B C)
 };
 constexpr int kCtlWords = (int)((sizeof(InstCtl) + 7) / 8);
 constexpr int kWordStride = 16;  // dispenser words 128 bytes apart
@@ -922,6 +1211,29 @@ struct TaskRunner {
         const Real* dd = I.arr(a.off_d[d.dcur]);
         GradPass<Real> ps(I, (d.flags & PF_STEP) != 0, (Real)d.t, a.lambda, phi, phi + cs, dd, dd + cs, nphi,
                           nphi + cs, de, de + cs, smem, part);
+        f(ps);
+        break;
+      }
+      case TK_N1:
+      case TK_N2:
+      case TK_N3: {
+        const int sub = (d.kind == TK_N1) ? 1 : (d.kind == TK_N2 ? 2 : 3);
+        const int mode = (d.purpose == TK_GRAD) ? NM_GRAD
+                         : (d.purpose == TK_TRIAL ? NM_TRIAL : (d.purpose == TK_NCG ? NM_NCG : NM_E0));
+        const Real* dd = I.arr(a.off_d[d.dcur]);
+        Real* wd = I.arr(a.off_d[d.dn]);
+        Real* nphi = I.arr(a.off_phi[d.cur ^ 1]);
+        Real* td = I.arr(a.off_td);
+        const bool step = (d.flags & PF_STEP) != 0, odz = (d.flags & PF_ODZERO) != 0;
+        NccPass<Real> ps(I, sub, mode, (Real)d.t, (Real)d.beta, d.mean, d.var, odz, step, phi, phi + cs, dd, dd + cs,
+                         s, s + cs, de, de + cs, a.normR, wd, wd + cs, nphi, nphi + cs, td, smem, part);
+        f(ps);
+        break;
+      }
+      case TK_NF: {
+        Real* nphi = I.arr(a.off_phi[d.cur ^ 1]);
+        NccForcePass<Real> ps(I, a.lambda, d.mean, d.var, d.e, nphi, nphi + cs, I.arr(a.off_td), a.normR, de, de + cs,
+                              smem, part);
         f(ps);
         break;
       }
@@ -1030,7 +1342,7 @@ __device__ __forceinline__ void block_sum(const double part[kRedSlots], double (
 // (gradientDescent.h:200-236) and ArmijoLineSearchUsingOp
 // (ArmijoSearch.h:118-200).
 template <typename Real>
-__device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const double tot[kRedSlots]) {
+__device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const double* tot) {
   const double lam = a.lambda;
   const double tau_min = 9.313225746154785e-10;  // 2^-30 (ArmijoSearch.h:77)
   const double tau_max = 33554432.0;             // 2^25  (ArmijoSearch.h:67)
@@ -1044,6 +1356,16 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
     return e;
   };
   auto quad = [&](double tt) { return 0.5 * ((c.A + 2.0 * tt * c.Bd) + tt * tt * c.Cd); };
+  // the next pass is an energy-type pass: with the NCC data term it starts
+  // with energy sub 1 and remembers what it stands for
+  auto to = [&](int kind) {
+    if (a.ncc) {
+      d.purpose = kind;
+      d.kind = TK_N1;
+    } else {
+      d.kind = kind;
+    }
+  };
   auto start_vcycle = [&](double vtau) {
     d.vtau = vtau;
     if (L > lc) { d.kind = TK_VDOWN; d.k = L; } else { d.kind = TK_COARSE; d.k = lc; }
@@ -1054,7 +1376,7 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
     c.f = c.energy;
     c.sigma_used = c.sigma;
     c.evals = 0;
-    d.kind = TK_GRAD;
+    to(TK_GRAD);
     d.cur = c.cur;
     d.dcur = c.dcur;
     d.flags = c.pending ? PF_STEP : 0;
@@ -1076,7 +1398,7 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
     double t = (c.attempt == 0) ? c.tau : 0.0;
     t = t < tau_min ? tau_min : (t > tau_max ? tau_max : t);
     c.t = t;
-    d.kind = TK_NCG;
+    to(TK_NCG);
     d.cur = c.cur;
     d.dcur = c.dcur;
     d.dn = c.dcur ^ 1;
@@ -1087,7 +1409,7 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
   auto trial = [&](double t, int role) {
     c.t = t;
     c.ls = role;
-    d.kind = TK_TRIAL;
+    to(TK_TRIAL);
     d.cur = c.cur;
     d.dcur = c.dcur;
     d.t = t;
@@ -1144,13 +1466,44 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
     }
   };
 
+  // NCC energy subs: chain them, then continue as the pass they stand for
+  double nt[kRedSlots];
+  switch (d.kind) {
+    case TK_N1:
+#pragma unroll
+      for (int k = 0; k < kRedSlots; ++k) c.n1[k] = tot[k];
+      d.mean = tot[0];
+      d.kind = TK_N2;
+      return;
+    case TK_N2:
+      d.var = sqrt(tot[0]);
+      d.kind = TK_N3;
+      return;
+    case TK_N3:
+      d.e = -(tot[0]);
+      if (d.purpose == TK_GRAD) {
+        d.kind = TK_NF;
+        return;
+      }
+      nt[0] = d.e;
+#pragma unroll
+      for (int k = 1; k < kRedSlots; ++k) nt[k] = c.n1[k];
+      tot = nt;
+      d.kind = d.purpose;
+      break;
+    case TK_NF:
+      d.kind = TK_GRAD;
+      break;
+    default: break;
+  }
+
   switch (d.kind) {
     case TK_E0: {
       c.A = tot[1];
       c.energy = energy_of(tot[0], 0.5 * c.A);
       c.energy_new = c.energy;
       if (a.mode == MODE_ENERGY) {
-        d.kind = TK_GRAD;
+        to(TK_GRAD);
         d.cur = c.cur;
         d.dcur = c.dcur;
         d.flags = 0;
@@ -1300,6 +1653,14 @@ __device__ void publish(const LevelArgs<Real>& a, const SchedPtrs<Real>& sp, int
   atomicExch(word, pack_word(seq, nchunks, 0));
 }
 
+// Two passes whose tiles use the same shared-memory layout (so the first
+// tile of one can be prefetched while the other computes).
+__device__ __forceinline__ bool same_layout(const PassDesc& a, const PassDesc& b) {
+  if (a.kind != b.kind || a.kind == TK_COARSE || a.kind == TK_FLUSH) return false;
+  if (a.kind == TK_N1) return a.purpose == b.purpose && a.flags == b.flags;
+  return true;
+}
+
 struct TaskSlot {
   int inst, chunk, nchunks;   // chunk index of the pass, chunks of the pass
   PassDesc desc;
@@ -1376,6 +1737,9 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
         cs.desc.vtau = (double)(0.5f * (a.sigma_fixed * a.sigma_fixed));
         if (a.level > a.lc) { cs.desc.kind = TK_VDOWN; cs.desc.k = a.level; }
         else { cs.desc.kind = TK_COARSE; cs.desc.k = a.lc; }
+      } else if (a.ncc) {
+        cs.desc.kind = TK_N1;
+        cs.desc.purpose = TK_E0;
       } else {
         cs.desc.kind = TK_E0;
       }
@@ -1440,7 +1804,7 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
         __syncthreads();
         nh = (flag_next == 1);
         if (nh) nt = slot[cur_slot ^ 1];
-        pre = nh && nt.desc.kind == t.desc.kind && t.desc.kind != TK_COARSE && t.desc.kind != TK_FLUSH;
+        pre = nh && same_layout(nt.desc, t.desc);
         if (pre) run.issue(nt.inst, nt.desc, nt.chunk * nt.desc.chunk, stage ^ 1);
       }
       cp_async_commit();

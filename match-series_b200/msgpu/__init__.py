@@ -37,6 +37,7 @@ class Params(ctypes.Structure):
         ("dont_normalize_input", ctypes.c_int),
         ("resample_deformation", ctypes.c_int),
         ("use_fp64", ctypes.c_int),
+        ("data_term", ctypes.c_int),
     ]
 
 
@@ -62,6 +63,7 @@ EXPORTS = [
     "msgpu_register_batch", "msgpu_register_batch_device", "msgpu_warp_mean", "msgpu_warp_mean_device",
     "msgpu_energy", "msgpu_smooth", "msgpu_restrict", "msgpu_prolong", "msgpu_normalize", "msgpu_gd_level",
     "msgpu_match_series_stage", "msgpu_match_series_stage_device", "msgpu_set_profiling", "msgpu_get_stats",
+    "msgpu_set_data_term",
 ]
 
 
@@ -101,6 +103,7 @@ def lib():
                                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                       ctypes.c_void_p, ctypes.c_void_p]
         L.msgpu_set_profiling.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.msgpu_set_data_term.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.msgpu_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(Stats)]
         _lib = L
     return _lib
@@ -257,6 +260,10 @@ class Context:
         out = np.zeros_like(a)
         self._check(lib().msgpu_normalize(self._h, _p(a), a.size, float(sat), int(min_to_zero), _p(out)))
         return out
+
+    def set_data_term(self, data_term: int):
+        """0: SSD, 1: normalized cross-correlation, for energy() and gd_level()."""
+        self._check(lib().msgpu_set_data_term(self._h, int(data_term)))
 
     def gd_level(self, level, R, T, phix, phiy, lam, max_iter, stop_eps=0.0, fp64=False, max_trace=256):
         px = _f64(phix).copy()
