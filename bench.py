@@ -35,6 +35,7 @@ sys.path.insert(0, os.path.join(ROOT, "match-series_b200"))
 METRIC = "registered frames/s at 513² to stated energy tol: warm-start+batched vs plain GPU"
 UNIT = "frames/s"
 LEVEL, START, FRAMES, MAX_ITER, LAMBDA = 9, 5, 20, 30, 0.1
+DATA_TERM = 0   # 0: SSD (deformationModel 22); 1: normalized cross-correlation (--ncc)
 
 
 def workload(rank: int):
@@ -49,7 +50,7 @@ def workload(rank: int):
 def params(fp64: bool):
     import msgpu
     return msgpu.default_params(precision_level=LEVEL, input_level=LEVEL, start_level=START, stop_level=LEVEL,
-                                max_gd_iterations=MAX_ITER, use_fp64=int(fp64))
+                                max_gd_iterations=MAX_ITER, use_fp64=int(fp64), data_term=DATA_TERM)
 
 
 class ClockSampler:
@@ -113,16 +114,22 @@ def level_traffic(fp64: bool):
     """DRAM bytes per launch of the finest-level kernel from the committed ncu summary (or None)."""
     try:
         d = json.load(open(os.path.join(ROOT, "profiles", "level_kernel_traffic.json")))
-        return d.get("f64" if fp64 else "f32", {}).get("bytes_per_launch_513x20")
+        key = ("f64" if fp64 else "f32") + ("_ncc" if DATA_TERM else "")
+        return d.get(key, {}).get("bytes_per_launch_513x20")
     except Exception:
         return None
 
 
 def algorithmic_bytes(steps: int, evals: int, real_bytes: int) -> float:
-    """Per-level algorithmic bytes: per node and frame 24 B per energy trial,
-    24 B gradient + 20 B NCG/update per step, 96 B per V-cycle component with
-    2 components per step (FP32 figures, scaled by the word size)."""
+    """Per-level algorithmic bytes, per node and frame in FP32 units (scaled by
+    real_bytes/4).  SSD: 24 B per energy trial (phi, d, R, gathered T), 24 B
+    gradient, 20 B NCG/update, 2 x 96 B V-cycle per step.  NCC: an energy
+    evaluation is three passes (phi, d, gathered T, Td write; Td; Td and the
+    normalised R) = 40 B, the gradient adds them to its force pass (phi, Td,
+    normalised R, gathered T, DE write = 28 B) = 68 B."""
     n = (1 << LEVEL) + 1
+    if DATA_TERM:
+        return n * n * (40.0 * evals + (68.0 + 20.0 + 2 * 96.0) * steps) * (real_bytes / 4.0)
     return n * n * (24.0 * evals + (24.0 + 20.0 + 2 * 96.0) * steps) * (real_bytes / 4.0)
 
 
@@ -143,7 +150,7 @@ def run_reference_sample(ref, tmpl, procs: int, workdir: str):
             os.makedirs(d, exist_ok=True)
             fr = np.stack([ref, tmpl[i]])
             fr.tofile(os.path.join(d, "frames.bin"))
-            cmd = [msor.REF_BIN, "series", str(LEVEL), str(START), str(LEVEL), repr(LAMBDA), "1.0", str(MAX_ITER),
+            cmd = [msor.REF_BIN, "series_ncc" if DATA_TERM else "series", str(LEVEL), str(START), str(LEVEL), repr(LAMBDA), "1.0", str(MAX_ITER),
                    "0.0", "0.15", "1", "2", os.path.join(d, "frames.bin"), os.path.join(d, "phis.bin"),
                    os.path.join(d, "mean.bin"), os.path.join(d, "info.txt")]
             jobs.append(subprocess.Popen(cmd, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL))
@@ -181,7 +188,7 @@ def _oracle_one(ref, tpl):
     import msor
     R = msor.normalize(ref)
     T = msor.normalize(tpl)
-    px, py, e, _ = msor.register(LEVEL, START, LEVEL, R, T, lam=LAMBDA, max_iter=MAX_ITER)
+    px, py, e, _ = msor.register(LEVEL, START, LEVEL, R, T, lam=LAMBDA, max_iter=MAX_ITER, ncc=bool(DATA_TERM))
     return px, py, e
 
 
@@ -239,7 +246,8 @@ def run_reference_arm(args, world, rank):
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "config": {"workload": f"stage registration of {procs} of the 20 hex-lattice frames 513x513 (level 9) "
                                   f"to a reference frame, levels {START}-{LEVEL}, maxGDIterations {MAX_ITER}, "
-                                  f"lambda {LAMBDA}; one process per host core", "frames_per_step": procs},
+                                  f"lambda {LAMBDA}, {'NCC' if DATA_TERM else 'SSD'} data term; one process per "
+                                  f"host core", "frames_per_step": procs, "data_term": "ncc" if DATA_TERM else "ssd"},
            "cpu_baseline": {"value": v, "unit": UNIT, "cores": procs, "kind": kind,
                             "sample": f"{procs} frames 513x513 per step, one per process"},
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -258,7 +266,7 @@ def profile_case(level: int, iters: int, fp64: bool):
     frames, _, _ = syn.make_series(n, FRAMES + 1, syn.HEX_513, seed=2000)
     ctx = msgpu.Context(0)
     p = msgpu.default_params(precision_level=level, input_level=level, start_level=level, stop_level=level,
-                             max_gd_iterations=iters, use_fp64=int(fp64))
+                             max_gd_iterations=iters, use_fp64=int(fp64), data_term=DATA_TERM)
     ctx.set_profiling(True)
     ctx.register_batch(p, frames[FRAMES], frames[:FRAMES])
     print(json.dumps({"profile_level": level, "frames": FRAMES, "iters": iters, "fp64": fp64,
@@ -273,12 +281,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--fp32", action="store_true", help="FP32 bulk with FP64 reductions (outside the energy tol)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ncc", action="store_true",
+                    help="normalized cross-correlation data term (matchSeries' default model) instead of SSD")
     ap.add_argument("--profile-level", type=int, default=0,
                     help="small case for ncu captures: one level solve of FRAMES frames at this level, "
                          "--profile-iters gradient steps, no timing")
     ap.add_argument("--profile-iters", type=int, default=5)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    global DATA_TERM
+    DATA_TERM = 1 if args.ncc else 0
     if args.profile_level:
         return profile_case(args.profile_level, args.profile_iters, not args.fp32)
     world, rank, local = dist_setup()
@@ -405,7 +417,9 @@ def main():
             "vs_baseline": None, "dtype": "f64" if fp64 else "f32+f64-reductions", "data": "synthetic",
             "config": {"workload": f"stage registration: {FRAMES} hex-lattice frames 513x513 (level {LEVEL}) to a "
                                    f"reference frame, levels {START}-{LEVEL}, maxGDIterations {MAX_ITER}, "
-                                   f"lambda {LAMBDA}, saturation 0.15%, plus warped-frame average",
+                                   f"lambda {LAMBDA}, saturation 0.15%, {'NCC' if DATA_TERM else 'SSD'} data term, "
+                                   f"plus warped-frame average",
+                       "data_term": "ncc" if DATA_TERM else "ssd",
                        "frames_per_gpu": FRAMES, "level": LEVEL, "start_level": START,
                        "max_gd_iterations": MAX_ITER, "lambda": LAMBDA,
                        "l2": "no flush: per-step working set (~0.6 GB) exceeds the 126 MB L2",

@@ -183,6 +183,70 @@ static void registerCommand ( char **argv ) {
   delete parser;
 }
 
+// One stage of series matching with a fixed reference: every frame is
+// prepared (normalised), registered to the reference from a zero
+// displacement, and the raw frames are averaged after warping
+// (matchSeries.h:141-155, 385-425).  Frame 0 of framesBin is the reference.
+template <typename Regis>
+static void seriesCommand ( char **argv ) {
+  const int maxL = atoi ( argv[2] ), start = atoi ( argv[3] ), stop = atoi ( argv[4] );
+  const int n = lvlN ( maxL ), N = n * n;
+  const int F = atoi ( argv[11] );
+  aol::ParameterParser *parser = makeParser ( maxL, start, stop, atof ( argv[5] ), atof ( argv[6] ), atoi ( argv[7] ),
+                                              atof ( argv[8] ), 0, atof ( argv[9] ), atoi ( argv[10] ) );
+  Regis regis ( *parser );
+  qc::GridDefinition grid ( maxL, qc::QC_2D );
+  std::vector<RealType> frames ( ( size_t ) N * F );
+  readBin ( argv[12], &frames[0], ( size_t ) N * F );
+  ArrayType ref ( grid );
+  memcpy ( ref.getData ( ), &frames[0], N * sizeof ( RealType ) );
+  const double t0 = wallSeconds ( );
+  regis.initRefOrTemplate ( ref, qc::REFERENCE, false );
+  std::vector<RealType> phis ( ( size_t ) 2 * N * F, 0. );
+  std::vector<double> energies ( F, 0. );
+  qc::MultiArray<RealType, qc::QC_2D> phi ( grid );
+  for ( int f = 1; f < F; ++f ) {
+    ArrayType tpl ( grid );
+    memcpy ( tpl.getData ( ), &frames[( size_t ) f * N], N * sizeof ( RealType ) );
+    regis.initRefOrTemplate ( tpl, qc::TEMPLATE, false );
+    regis.setTransformationToZero ( );
+    regis.solveAndProlongToMaxDepth ( );
+    regis.getTransformation ( phi );
+    energies[f] = regis.getEnergyOfLastSolution ( );
+    memcpy ( &phis[( size_t ) 2 * f * N], phi[0].getData ( ), N * sizeof ( RealType ) );
+    memcpy ( &phis[( size_t ) ( 2 * f + 1 ) * N], phi[1].getData ( ), N * sizeof ( RealType ) );
+  }
+  const double t1 = wallSeconds ( );
+  // averageSeries: DeformImage with Inf extension, mean over finite samples.
+  std::vector<RealType> mean ( N, 0. );
+  {
+    aol::MultiVector<RealType> deformed ( F, N );
+    for ( int f = 0; f < F; ++f ) {
+      aol::Vector<RealType> img ( &frames[( size_t ) f * N], N, aol::FLAT_COPY );
+      aol::MultiVector<RealType> p ( 2, N );
+      memcpy ( p[0].getData ( ), &phis[( size_t ) 2 * f * N], N * sizeof ( RealType ) );
+      memcpy ( p[1].getData ( ), &phis[( size_t ) ( 2 * f + 1 ) * N], N * sizeof ( RealType ) );
+      qc::DeformImage<ConfType> ( img, grid, deformed[f], p, true, aol::NumberTrait<RealType>::Inf, false );
+    }
+    aol::Vector<RealType> last ( &frames[( size_t ) ( F - 1 ) * N], N, aol::FLAT_COPY );
+    const RealType lastMean = last.getMeanValue ( );
+    for ( int j = 0; j < N; ++j ) {
+      RealType a = 0; int k = 0;
+      for ( int f = 0; f < F; ++f )
+        if ( deformed[f][j] != aol::NumberTrait<RealType>::Inf ) { a += deformed[f][j]; ++k; }
+      mean[j] = ( k > 0 ) ? a / k : lastMean;
+    }
+  }
+  const double t2 = wallSeconds ( );
+  writeBin ( argv[13], &phis[0], ( size_t ) 2 * N * F );
+  writeBin ( argv[14], &mean[0], N );
+  FILE *f = fopen ( argv[15], "w" );
+  fprintf ( f, "registration_seconds %.6f\naverage_seconds %.6f\n", t1 - t0, t2 - t1 );
+  for ( int i = 0; i < F; ++i ) fprintf ( f, "energy %d %.17g\n", i, energies[i] );
+  fclose ( f );
+  delete parser;
+}
+
 static int usage ( ) {
   fprintf ( stderr,
     "ms_ref energy[_ncc] L R T px py lambda outPrefix\n"
@@ -192,7 +256,7 @@ static int usage ( ) {
     "ms_ref gdlevel[_ncc] L R T px py lambda maxIter stopEps outPhi outTrace\n"
     "ms_ref register[_ncc] maxL start stop R T px py lambda lambdaFactor maxIter stopEps resample outPhi outTxt\n"
     "ms_ref normalize L in sat minToZero out\n"
-    "ms_ref series maxL start stop lambda lambdaFactor maxIter stopEps sat minToZero F framesBin outPhis outMean outTxt\n" );
+    "ms_ref series[_ncc] maxL start stop lambda lambdaFactor maxIter stopEps sat minToZero F framesBin outPhis outMean outTxt\n" );
   return 1;
 }
 
@@ -308,67 +372,9 @@ int main ( int argc, char **argv ) {
       delete parser;
       return 0;
     }
-    if ( cmd == "series" && argc == 16 ) {
-      // One stage of series matching with a fixed reference: every frame is
-      // prepared (normalised), registered to the reference from a zero
-      // displacement, and the raw frames are averaged after warping
-      // (matchSeries.h:141-155, 385-425).  Frame 0 of framesBin is the reference.
-      const int maxL = atoi ( argv[2] ), start = atoi ( argv[3] ), stop = atoi ( argv[4] );
-      const int n = lvlN ( maxL ), N = n * n;
-      const int F = atoi ( argv[11] );
-      aol::ParameterParser *parser = makeParser ( maxL, start, stop, atof ( argv[5] ), atof ( argv[6] ), atoi ( argv[7] ),
-                                                  atof ( argv[8] ), 0, atof ( argv[9] ), atoi ( argv[10] ) );
-      RegisType regis ( *parser );
-      qc::GridDefinition grid ( maxL, qc::QC_2D );
-      std::vector<RealType> frames ( ( size_t ) N * F );
-      readBin ( argv[12], &frames[0], ( size_t ) N * F );
-      ArrayType ref ( grid );
-      memcpy ( ref.getData ( ), &frames[0], N * sizeof ( RealType ) );
-      const double t0 = wallSeconds ( );
-      regis.initRefOrTemplate ( ref, qc::REFERENCE, false );
-      std::vector<RealType> phis ( ( size_t ) 2 * N * F, 0. );
-      std::vector<double> energies ( F, 0. );
-      qc::MultiArray<RealType, qc::QC_2D> phi ( grid );
-      for ( int f = 1; f < F; ++f ) {
-        ArrayType tpl ( grid );
-        memcpy ( tpl.getData ( ), &frames[( size_t ) f * N], N * sizeof ( RealType ) );
-        regis.initRefOrTemplate ( tpl, qc::TEMPLATE, false );
-        regis.setTransformationToZero ( );
-        regis.solveAndProlongToMaxDepth ( );
-        regis.getTransformation ( phi );
-        energies[f] = regis.getEnergyOfLastSolution ( );
-        memcpy ( &phis[( size_t ) 2 * f * N], phi[0].getData ( ), N * sizeof ( RealType ) );
-        memcpy ( &phis[( size_t ) ( 2 * f + 1 ) * N], phi[1].getData ( ), N * sizeof ( RealType ) );
-      }
-      const double t1 = wallSeconds ( );
-      // averageSeries: DeformImage with Inf extension, mean over finite samples.
-      std::vector<RealType> mean ( N, 0. );
-      {
-        aol::MultiVector<RealType> deformed ( F, N );
-        for ( int f = 0; f < F; ++f ) {
-          aol::Vector<RealType> img ( &frames[( size_t ) f * N], N, aol::FLAT_COPY );
-          aol::MultiVector<RealType> p ( 2, N );
-          memcpy ( p[0].getData ( ), &phis[( size_t ) 2 * f * N], N * sizeof ( RealType ) );
-          memcpy ( p[1].getData ( ), &phis[( size_t ) ( 2 * f + 1 ) * N], N * sizeof ( RealType ) );
-          qc::DeformImage<ConfType> ( img, grid, deformed[f], p, true, aol::NumberTrait<RealType>::Inf, false );
-        }
-        aol::Vector<RealType> last ( &frames[( size_t ) ( F - 1 ) * N], N, aol::FLAT_COPY );
-        const RealType lastMean = last.getMeanValue ( );
-        for ( int j = 0; j < N; ++j ) {
-          RealType a = 0; int k = 0;
-          for ( int f = 0; f < F; ++f )
-            if ( deformed[f][j] != aol::NumberTrait<RealType>::Inf ) { a += deformed[f][j]; ++k; }
-          mean[j] = ( k > 0 ) ? a / k : lastMean;
-        }
-      }
-      const double t2 = wallSeconds ( );
-      writeBin ( argv[13], &phis[0], ( size_t ) 2 * N * F );
-      writeBin ( argv[14], &mean[0], N );
-      FILE *f = fopen ( argv[15], "w" );
-      fprintf ( f, "registration_seconds %.6f\naverage_seconds %.6f\n", t1 - t0, t2 - t1 );
-      for ( int i = 0; i < F; ++i ) fprintf ( f, "energy %d %.17g\n", i, energies[i] );
-      fclose ( f );
-      delete parser;
+    if ( ( cmd == "series" || cmd == "series_ncc" ) && argc == 16 ) {
+      if ( cmd == "series" ) seriesCommand<RegisType> ( argv );
+      else seriesCommand<RegisTypeNCC> ( argv );
       return 0;
     }
   } catch ( aol::Exception &e ) {
