@@ -11,6 +11,7 @@
 
 #include <float.h>
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -978,10 +979,26 @@ double msor_register(int max_level, int start_level, int stop_level, const doubl
                           max_iter, stop_eps, resample_phi, steps_per_level);
 }
 
+static double register_core(int data_term, int max_level, int start_level, int stop_level, int lambda_stop,
+                            const double* R, const double* T, double* phix, double* phiy, double lambda,
+                            double lambda_factor, int max_iter, double stop_eps, int resample_phi,
+                            int* steps_per_level);
+
 double msor_register_dt(int data_term, int max_level, int start_level, int stop_level, const double* R,
                         const double* T, double* phix, double* phiy, double lambda,
                         double lambda_factor, int max_iter, double stop_eps, int resample_phi,
                         int* steps_per_level) {
+  return register_core(data_term, max_level, start_level, stop_level, stop_level, R, T, phix, phiy, lambda,
+                       lambda_factor, max_iter, stop_eps, resample_phi, steps_per_level);
+}
+
+/* lambda_stop: the parameter file's stopLevel, which the level weights
+ * lambda * lambdaFactor^(stopLevel - level) refer to also when a solve runs
+ * on other levels (the refinement of series matching).                     */
+static double register_core(int data_term, int max_level, int start_level, int stop_level, int lambda_stop,
+                            const double* R, const double* T, double* phix, double* phiy, double lambda,
+                            double lambda_factor, int max_iter, double stop_eps, int resample_phi,
+                            int* steps_per_level) {
   double *Rl[16] = {0}, *Tl[16] = {0}, *Px[16] = {0}, *Py[16] = {0};
   for (int l = 0; l <= max_level; ++l) {
     const int n = lvl_n(l);
@@ -1007,7 +1024,7 @@ double msor_register_dt(int data_term, int max_level, int start_level, int stop_
   if (start_level <= stop_level) {
     for (int level = start_level; level <= stop_level; ++level) {
       /* getRegularizationWeight (registration.h:523-526) */
-      const double lam = (double)pow(lambda_factor, stop_level - level) * lambda;
+      const double lam = (double)pow(lambda_factor, lambda_stop - level) * lambda;
       const int steps = msor_gd_level_dt(data_term, level, Rl[level], Tl[level], Px[level], Py[level], lam,
                                          max_iter, stop_eps, &energy, NULL, 0);
       if (steps_per_level) steps_per_level[level - start_level] = steps;
@@ -1022,6 +1039,169 @@ double msor_register_dt(int data_term, int max_level, int start_level, int stop_
   memcpy(phiy, Py[max_level], sizeof(double) * nm * nm);
   for (int l = 0; l <= max_level; ++l) { free(Rl[l]); free(Tl[l]); free(Px[l]); free(Py[l]); }
   return energy;
+}
+
+/* --- composition of displacements (series matching) ---------------------- */
+
+/* StiffOp ONTHEFLY apply: Dest = 0, then per element (x fastest) and local
+ * row i, column j: Dest[g_i] += L[i][j] * Arg[g_j]
+ * (LocalAssemblyHelper::doMultiplyOnTheFly, FEOpInterface.h:136-157).      */
+static void stiff_apply_onthefly(int level, const double* u, double* out) {
+  const int n = lvl_n(level);
+  const double h = lvl_h(level);
+  const double vol = sqr(h);
+  quad_t Q;
+  quad_init(&Q, h);
+  double L[4][4];
+  for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) L[i][j] = 0.;
+  for (int q = 0; q < 4; ++q)
+    for (int i = 0; i < 4; ++i)
+      for (int j = i; j < 4; ++j) {
+        double d = 0;
+        d += Q.gq[i][q][0] * Q.gq[j][q][0];
+        d += Q.gq[i][q][1] * Q.gq[j][q][1];
+        L[i][j] += d * 1. * Q.w;
+      }
+  for (int i = 0; i < 4; ++i)
+    for (int j = i; j < 4; ++j) L[j][i] = L[i][j] = L[i][j] * vol;
+  memset(out, 0, sizeof(double) * n * n);
+  for (int ey = 0; ey < n - 1; ++ey)
+    for (int ex = 0; ex < n - 1; ++ex)
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) out[dof(n, ex, ey, i)] += L[i][j] * u[dof(n, ex, ey, j)];
+}
+
+/* Masked system matrix of SmoothlyExtendImage (deformations.h:364-410):
+ * the assembled stiffness without the rows and columns of defined nodes,
+ * whose diagonal is 1 (LocalAssemblyHelper::doLocalAssemblyDirichlet,
+ * FEOpInterface.h:92-128).                                                  */
+static double* masked_stiff_build(int level, const unsigned char* defined) {
+  const int n = lvl_n(level);
+  double* full = stiff_build(level);
+  double* m = (double*)calloc((size_t)n * n * 9, sizeof(double));
+  /* the same element-order sums as the unmasked assembly, restricted to
+   * undefined rows and columns: an entry is either its full value or 0     */
+  for (int r = 0; r < n * n; ++r) {
+    if (defined[r]) { m[(size_t)r * 9 + 4] = 0. + 1.; continue; }
+    const int x = r % n, y = r / n;
+    for (int j = -1; j <= 1; ++j)
+      for (int i = -1; i <= 1; ++i) {
+        const int X = x + i, Y = y + j;
+        if (X < 0 || X >= n || Y < 0 || Y >= n) continue;
+        if (!defined[X + Y * n]) m[(size_t)r * 9 + (j + 1) * 3 + (i + 1)] = full[(size_t)r * 9 + (j + 1) * 3 + (i + 1)];
+      }
+  }
+  free(full);
+  return m;
+}
+
+/* PCGInverse::apply with the diagonal preconditioner |1/diag|
+ * (solver.h:264-358, matrix.h:1256-1269, 1199-1210), absolute stopping
+ * g.g < eps (solverInfo.h:162-192), at most max_iter steps.              */
+static int pcg(const double* A, int level, const double* b, double* x, double eps, int max_iter) {
+  const int n = lvl_n(level), N = n * n;
+  double* g = (double*)calloc(N, sizeof(double));
+  double* d = (double*)calloc(N, sizeof(double));
+  double* h = (double*)calloc(N, sizeof(double));
+  double* dinv = (double*)malloc(sizeof(double) * N);
+  for (int i = 0; i < N; ++i) {
+    const double a = A[(size_t)i * 9 + 4];
+    dinv[i] = (a != 0.) ? fabs(1. / a) : 1.;
+  }
+  stiff_apply_with(A, level, x, h);
+  for (int i = 0; i < N; ++i) { g[i] = h[i]; g[i] -= b[i]; }
+  for (int i = 0; i < N; ++i) h[i] = g[i] * dinv[i];
+  double spn = dot(g, g, N);
+  for (int i = 0; i < N; ++i) d[i] -= h[i];
+  int it = 0;
+  while (!(spn < eps) && it < max_iter && !isnan(spn)) {
+    ++it;
+    const double alpha_numer = dot(g, h, N), beta_denom = alpha_numer;
+    stiff_apply_with(A, level, d, h);
+    const double alpha_denom = dot(d, h, N);
+    for (int i = 0; i < N; ++i) x[i] += d[i] * (alpha_numer / alpha_denom);
+    for (int i = 0; i < N; ++i) g[i] += h[i] * (alpha_numer / alpha_denom);
+    for (int i = 0; i < N; ++i) h[i] = g[i] * dinv[i];
+    const double beta_numer = dot(g, h, N);
+    for (int i = 0; i < N; ++i) d[i] *= (beta_numer / beta_denom);
+    for (int i = 0; i < N; ++i) d[i] -= h[i];
+    spn = dot(g, g, N);
+  }
+  free(g); free(d); free(h); free(dinv);
+  return it;
+}
+
+/* ConcatAndSmoothlyExtendDeformations (deformations.h:498-520):
+ * identity + out = (identity + D1) o (identity + D2), extended where
+ * x + D2(x) leaves the domain by the discrete harmonic extension of
+ * SmoothlyExtendImage.  outx/outy hold the solver's initial guess on entry
+ * (the previous content of the destination in the reference).              */
+int msor_compose(int level, const double* d1x, const double* d1y, const double* d2x, const double* d2y,
+                 double* outx, double* outy) {
+  const int n = lvl_n(level), N = n * n;
+  const double h = lvl_h(level);
+  double* res[2];
+  res[0] = (double*)malloc(sizeof(double) * N);
+  res[1] = (double*)malloc(sizeof(double) * N);
+  const double* d1[2] = {d1x, d1y};
+  const double* d2[2] = {d2x, d2y};
+  /* DeformImage with an extension image of NaN (deformations.h:225-253) */
+  for (int c = 0; c < 2; ++c)
+    for (int y = 0; y < n; ++y)
+      for (int x = 0; x < n; ++x) {
+        const int i = x + y * n;
+        const double ds0 = x + d2x[i] / h, ds1 = y + d2y[i] / h;
+        const int in = !(ds0 < 0. || ds0 > (double)(n - 1) || ds1 < 0. || ds1 > (double)(n - 1));
+        res[c][i] = in ? interp(d1[c], n, ds0, ds1) : NAN;
+      }
+  for (int c = 0; c < 2; ++c)
+    for (int i = 0; i < N; ++i) res[c][i] += d2[c][i];
+  unsigned char* defined = (unsigned char*)malloc(N);
+  for (int i = 0; i < N; ++i) defined[i] = !isnan(res[0][i]);
+  /* SmoothlyExtendImage (deformations.h:364-410) */
+  double* A = masked_stiff_build(level, defined);
+  double* bc = (double*)malloc(sizeof(double) * N);
+  double* rhs = (double*)malloc(sizeof(double) * N);
+  double* out[2] = {outx, outy};
+  int iters = 0;
+  for (int c = 0; c < 2; ++c) {
+    for (int i = 0; i < N; ++i) bc[i] = defined[i] ? res[c][i] : 0.;
+    stiff_apply_onthefly(level, bc, rhs);
+    for (int i = 0; i < N; ++i) rhs[i] *= -1.;
+    for (int i = 0; i < N; ++i) if (defined[i]) rhs[i] = bc[i];
+    iters += pcg(A, level, rhs, out[c], 1e-16, 1000);
+  }
+  free(A); free(bc); free(rhs); free(defined); free(res[0]); free(res[1]);
+  return iters;
+}
+
+/* MultiVector::getMedianVecOverComponents (multiVector.cpp:99-117) of the
+ * warped frames (DeformImage with Inf extension), Vector::getMedianValue
+ * (vec.cpp:933-949); pixels without samples take fill.                     */
+static int cmp_d(const void* a, const void* b) {
+  const double x = *(const double*)a, y = *(const double*)b;
+  return (x < y) ? -1 : (x > y) ? 1 : 0;
+}
+
+void msor_warp_median(int level, int F, const double* frames, const double* phis, double fill, double* median) {
+  const int n = lvl_n(level), N = n * n;
+  double* def = (double*)malloc(sizeof(double) * (size_t)N * F);
+  for (int f = 0; f < F; ++f)
+    msor_deform_image(level, frames + (size_t)f * N, phis + (size_t)2 * f * N,
+                      phis + (size_t)(2 * f + 1) * N, INFINITY, def + (size_t)f * N);
+  double* tmp = (double*)malloc(sizeof(double) * F);
+  for (int j = 0; j < N; ++j) {
+    int k = 0;
+    for (int f = 0; f < F; ++f) {
+      const double v = def[(size_t)f * N + j];
+      if (v != INFINITY) tmp[k++] = v;
+    }
+    if (k == 0) { median[j] = fill; continue; }
+    qsort(tmp, k, sizeof(double), cmp_d);
+    median[j] = (k % 2 == 1) ? tmp[k / 2] : (tmp[k / 2 - 1] + tmp[k / 2]) / 2;
+  }
+  free(tmp);
+  free(def);
 }
 
 void msor_warp_mean(int level, int F, const double* frames, const double* phis, double* mean,
@@ -1045,4 +1225,74 @@ void msor_warp_mean(int level, int F, const double* frames, const double* phis, 
     count[j] = k;
   }
   free(def);
+}
+
+/* --- the series pipeline --------------------------------------------------- */
+
+/* The stage loop of matchSeries<>() (matchSeries.h:1250-1320) with its
+ * default options, each stage SeriesMatching::matchSeries with accumulated
+ * deformations (matchSeries.h:87-265) followed by averageSeries
+ * (matchSeries.h:353-445):
+ *   stage 1: reference frame 0, templates 1..F-1; stage s > 1: reference the
+ *   average (median with use_median) of stage s-1, templates 0..F-1, lambda
+ *   the "%f" print of lambda * extra_lambda_factor (matchSeries.h:1300).
+ *   Per template i: registration to the previous template (to the reference
+ *   for i = 0) from zero; acc = compose(current, acc); for i > 0 refinement
+ *   of acc against the stage reference on refine_start..refine_stop.
+ * The images are prepared by msor_normalize(sat, min_to_zero) like the
+ * reference's loadRefOrTemplate; the average and median warp the raw frames.
+ * Outputs of the last stage: phis (m x 2 x N, m = F-1 without extra stages,
+ * else F), avg, median, count (N each); energies (nullable) receives, per
+ * stage, m energies (the pairwise one for i = 0, the refined one after).    */
+void msor_match_series(int data_term, int level, int start, int stop, double lambda, double lambda_factor,
+                       int max_iter, double stop_eps, double sat, int min_to_zero, int refine_start,
+                       int refine_stop, int extra_stages, double extra_lambda_factor, int use_median, int F,
+                       const double* frames, double* phis, double* avg, double* median, double* count,
+                       double* energies) {
+  const int n = lvl_n(level), N = n * n;
+  double* target = (double*)malloc(sizeof(double) * N);
+  double* R = (double*)malloc(sizeof(double) * N);
+  double* Rprev = (double*)malloc(sizeof(double) * N);
+  double* T = (double*)malloc(sizeof(double) * N);
+  double* cur = (double*)malloc(sizeof(double) * 2 * N);
+  double* acc = (double*)malloc(sizeof(double) * 2 * N);
+  double* tmp = (double*)malloc(sizeof(double) * 2 * N);
+  memcpy(target, frames, sizeof(double) * N);
+  int eoff = 0;
+  for (int stage = 1; stage <= 1 + extra_stages; ++stage) {
+    double lam = lambda;
+    if (stage > 1) {
+      char buf[64];
+      snprintf(buf, sizeof buf, "%f", lambda * extra_lambda_factor);
+      lam = atof(buf);
+    }
+    const int first = (stage == 1) ? 1 : 0, m = F - first;
+    memcpy(R, target, sizeof(double) * N);
+    msor_normalize(R, N, sat, min_to_zero);
+    memcpy(Rprev, R, sizeof(double) * N);
+    memset(acc, 0, sizeof(double) * 2 * N);
+    for (int i = 0; i < m; ++i) {
+      memcpy(T, frames + (size_t)(first + i) * N, sizeof(double) * N);
+      msor_normalize(T, N, sat, min_to_zero);
+      memset(cur, 0, sizeof(double) * 2 * N);
+      double e = register_core(data_term, level, start, stop, stop, Rprev, T, cur, cur + N, lam, lambda_factor,
+                               max_iter, stop_eps, 0, NULL);
+      memcpy(tmp, acc, sizeof(double) * 2 * N);
+      msor_compose(level, cur, cur + N, tmp, tmp + N, acc, acc + N);
+      if (i > 0)
+        e = register_core(data_term, level, refine_start, refine_stop, stop, R, T, acc, acc + N, lam,
+                          lambda_factor, max_iter, stop_eps, 0, NULL);
+      memcpy(phis + (size_t)2 * i * N, (i == 0) ? cur : acc, sizeof(double) * 2 * N);
+      if (energies) energies[eoff + i] = e;
+      memcpy(Rprev, T, sizeof(double) * N);
+    }
+    eoff += m;
+    msor_warp_mean(level, m, frames + (size_t)first * N, phis, avg, count);
+    double last_mean = 0;
+    for (int j = 0; j < N; ++j) last_mean += frames[(size_t)(F - 1) * N + j];
+    last_mean /= N;
+    msor_warp_median(level, m, frames + (size_t)first * N, phis, last_mean, median);
+    memcpy(target, use_median ? median : avg, sizeof(double) * N);
+  }
+  free(target); free(R); free(Rprev); free(T); free(cur); free(acc); free(tmp);
 }

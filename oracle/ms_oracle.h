@@ -127,6 +127,26 @@ double msor_register_dt(int data_term, int max_level, int start_level, int stop_
                         double lambda, double lambda_factor, int max_iter, double stop_eps,
                         int resample_phi, int* steps_per_level);
 
+/* --- series matching helpers -------------------------------------------- */
+/* ConcatAndSmoothlyExtendDeformations (deformations.h:498-520): out = the
+ * displacement of (id + d1) o (id + d2), harmonically extended where
+ * x + d2(x) leaves the domain; outx/outy carry the PCG's initial guess in.
+ * Returns the PCG iterations of both components.                          */
+int    msor_compose(int level, const double* d1x, const double* d1y, const double* d2x,
+                    const double* d2y, double* outx, double* outy);
+/* median of the warped frames over the finite samples (averageSeries,
+ * matchSeries.h:442; multiVector.cpp:99-117), fill where none            */
+void   msor_warp_median(int level, int F, const double* frames, const double* phis, double fill,
+                        double* median);
+/* matchSeries<>() with accumulated deformations, refinement and extra stages
+ * (matchSeries.h:87-265, 353-445, 1250-1320); see ms_oracle.c.             */
+void   msor_match_series(int data_term, int level, int start, int stop, double lambda,
+                         double lambda_factor, int max_iter, double stop_eps, double sat,
+                         int min_to_zero, int refine_start, int refine_stop, int extra_stages,
+                         double extra_lambda_factor, int use_median, int F, const double* frames,
+                         double* phis, double* avg, double* median, double* count,
+                         double* energies);
+
 #ifdef __cplusplus
 }
 #endif

@@ -167,6 +167,49 @@ def register(max_level, start, stop, R, T, px=None, py=None, lam=0.1, lam_factor
     return px, py, e, list(steps)
 
 
+def compose(level, d1, d2, init=None):
+    """ConcatAndSmoothlyExtendDeformations of displacements d1, d2 (2 x N each);
+    init: the solver's initial guess (default d2, as in series matching)."""
+    N = n_of(level) ** 2
+    out = (_c(d2) if init is None else _c(init)).reshape(2, N).copy()
+    d1 = _c(d1).reshape(2, N)
+    d2 = _c(d2).reshape(2, N)
+    ox, oy = out[0].copy(), out[1].copy()
+    lib().msor_compose(level, _p(d1[0].copy()), _p(d1[1].copy()), _p(d2[0].copy()), _p(d2[1].copy()), _p(ox), _p(oy))
+    return np.stack([ox, oy])
+
+
+def warp_median(level, frames, phis, fill):
+    N = n_of(level) ** 2
+    out = np.zeros(N)
+    lib().msor_warp_median(level, frames.shape[0], _p(_c(frames).reshape(-1)), _p(_c(phis).reshape(-1)),
+                           ctypes.c_double(fill), _p(out))
+    return out
+
+
+def match_series(level, start, stop, frames, lam=0.1, lam_factor=1.0, max_iter=15, stop_eps=0.0, sat=0.15,
+                 min_to_zero=1, refine_start=None, refine_stop=None, extra_stages=0, extra_lam_factor=1.0,
+                 use_median=False, ncc=False):
+    """matchSeries<>() with accumulated deformations, refinement and extra
+    stages; returns the last stage's (phis m x 2 x N, avg, median, count) and
+    the energies of every stage (one array per stage)."""
+    F = frames.shape[0]
+    N = n_of(level) ** 2
+    rs = start if refine_start is None else refine_start
+    rp = level if refine_stop is None else refine_stop
+    m = F - 1 if extra_stages == 0 else F
+    phis = np.zeros((m, 2, N))
+    avg, med, cnt = np.zeros(N), np.zeros(N), np.zeros(N)
+    ne = (F - 1) + extra_stages * F
+    en = np.zeros(ne)
+    lib().msor_match_series(1 if ncc else 0, level, start, stop, ctypes.c_double(lam), ctypes.c_double(lam_factor),
+                            max_iter, ctypes.c_double(stop_eps), ctypes.c_double(sat), min_to_zero, rs, rp,
+                            extra_stages, ctypes.c_double(extra_lam_factor), 1 if use_median else 0, F,
+                            _p(_c(frames).reshape(-1)), _p(phis), _p(avg), _p(med), _p(cnt), _p(en))
+    stages = [en[: F - 1]] + [en[F - 1 + k * F: F - 1 + (k + 1) * F] for k in range(extra_stages)]
+    return phis, avg, med, cnt, stages
+
+
 def warp_mean(level, frames, phis):
     n = n_of(level)
     F = frames.shape[0]
@@ -230,6 +273,18 @@ class RefRunner:
                  os.path.join(self.dir, "out"))
         return self._r("out")
 
+    def compose(self, level, d1, d2, init=None):
+        N = n_of(level) ** 2
+        init = d2 if init is None else init
+        self.run("compose", level, self._w("d1", _c(d1).reshape(-1)), self._w("d2", _c(d2).reshape(-1)),
+                 self._w("io", _c(init).reshape(-1)), os.path.join(self.dir, "out"))
+        return self._r("out").reshape(2, N)
+
+    def median(self, level, frames, phis, fill):
+        self.run("median", level, frames.shape[0], self._w("fr", frames), self._w("ph", phis), repr(float(fill)),
+                 os.path.join(self.dir, "out"))
+        return self._r("out")
+
     def normalize(self, level, img, sat=0.15, min_to_zero=1):
         self.run("normalize", level, self._w("img", img), repr(float(sat)), min_to_zero,
                  os.path.join(self.dir, "out"))
@@ -259,6 +314,36 @@ class RefRunner:
                  int(bool(resample_phi)), os.path.join(self.dir, "phi"), os.path.join(self.dir, "e.txt"))
         phi = self._r("phi")
         return phi[:N], phi[N:], float(open(os.path.join(self.dir, "e.txt")).read())
+
+    def match_series(self, level, start, stop, frames, lam=0.1, lam_factor=1.0, max_iter=15, stop_eps=0.0,
+                     sat=0.15, min_to_zero=1, refine_start=None, refine_stop=None, extra_stages=0,
+                     extra_lam_factor=1.0, use_median=False, ncc=False):
+        """The reference's stage loop (see match_series); returns the same
+        tuple plus per-stage timings."""
+        F = frames.shape[0]
+        N = n_of(level) ** 2
+        rs = start if refine_start is None else refine_start
+        rp = level if refine_stop is None else refine_stop
+        out = os.path.join(self.dir, "ms")
+        self.run("matchseries_ncc" if ncc else "matchseries", level, start, stop, repr(float(lam)),
+                 repr(float(lam_factor)), max_iter, repr(float(stop_eps)), repr(float(sat)), min_to_zero, rs, rp,
+                 extra_stages, repr(float(extra_lam_factor)), 1 if use_median else 0, F,
+                 self._w("frames", frames), out)
+        last = extra_stages + 1
+        m = F - 1 if extra_stages == 0 else F
+        phis = self._r(f"ms_phis{last}.bin").reshape(m, 2, N)
+        avg, med, cnt = (self._r(f"ms_{k}{last}.bin") for k in ("avg", "median", "count"))
+        stages = [dict() for _ in range(last)]
+        timing = {}
+        for line in open(out + ".txt"):
+            t = line.split()
+            if t[0] == "energy":
+                stages[int(t[1]) - 1][int(t[2])] = float(t[3])
+            elif t[0] == "stage":
+                timing[int(t[1])] = dict(lam=float(t[3]), registration_seconds=float(t[5]),
+                                         average_seconds=float(t[7]))
+        energies = [np.array([d[i] for i in sorted(d)]) for d in stages]
+        return phis, avg, med, cnt, energies, timing
 
     def series(self, max_level, start, stop, frames, lam, lam_factor, max_iter, stop_eps=0.0, sat=0.15,
                min_to_zero=1):

@@ -247,6 +247,108 @@ static void seriesCommand ( char **argv ) {
   delete parser;
 }
 
+// The stage loop of matchSeries<>() (matchSeries.h:1250-1320) with the
+// default options: stage 1 registers frames 1..F-1 with frame 0 as the
+// reference, every further stage registers frames 0..F-1 with the average
+// (or median) of the previous stage as the reference and lambda replaced by
+// the "%f" print of lambda * extraStagesLambdaFactor (matchSeries.h:1300).
+// Inside a stage, SeriesMatching::matchSeries (matchSeries.h:87-265) with
+// accumulated deformations: each template is registered to the previous one
+// from zero, its displacement is composed with the accumulated one
+// (composeDeformations, registration.h:584-586) and, from the second template
+// on, refined against the stage's reference on refineStartLevel..
+// refineStopLevel.  The average and median of the warped raw templates follow
+// averageSeries (matchSeries.h:353-445).  Writes per stage s (1-based)
+// <out>_phis<s>.bin, <out>_avg<s>.bin, <out>_median<s>.bin, <out>_count<s>.bin
+// and <out>.txt (energies and timings).
+template <typename Regis>
+static void matchSeriesCommand ( char **argv ) {
+  const int maxL = atoi ( argv[2] ), start = atoi ( argv[3] ), stop = atoi ( argv[4] );
+  const double lambda = atof ( argv[5] ), lamFac = atof ( argv[6] );
+  const int maxIter = atoi ( argv[7] );
+  const double stopEps = atof ( argv[8] ), sat = atof ( argv[9] );
+  const int minToZero = atoi ( argv[10] ), refineStart = atoi ( argv[11] ), refineStop = atoi ( argv[12] );
+  const int extraStages = atoi ( argv[13] );
+  const double extraLamFac = atof ( argv[14] );
+  const int useMedian = atoi ( argv[15] ), F = atoi ( argv[16] );
+  const std::string out = argv[18];
+  const int n = lvlN ( maxL ), N = n * n;
+  qc::GridDefinition grid ( maxL, qc::QC_2D );
+  std::vector<RealType> frames ( ( size_t ) N * F );
+  readBin ( argv[17], &frames[0], ( size_t ) N * F );
+  FILE *info = fopen ( ( out + ".txt" ).c_str ( ), "w" );
+  ArrayType target ( grid );
+  memcpy ( target.getData ( ), &frames[0], N * sizeof ( RealType ) );
+  for ( int stage = 1; stage <= 1 + extraStages; ++stage ) {
+    const double lam = ( stage == 1 ) ? lambda : atof ( aol::strprintf ( "%f", lambda * extraLamFac ).c_str ( ) );
+    const int first = ( stage == 1 ) ? 1 : 0, m = F - first;
+    aol::ParameterParser *parser = makeParser ( maxL, start, stop, lam, lamFac, maxIter, stopEps, 0, sat, minToZero );
+    Regis regis ( *parser );
+    const double t0 = wallSeconds ( );
+    regis.initRefOrTemplate ( target, qc::REFERENCE, false );
+    const ArrayType reference ( regis.getRefImageReference ( ), aol::DEEP_COPY );
+    regis.setTransformationToZero ( );
+    qc::MultiArray<RealType, qc::QC_2D> acc ( grid ), cur ( grid );
+    regis.getTransformation ( acc );
+    std::vector<RealType> phis ( ( size_t ) 2 * N * m );
+    for ( int i = 0; i < m; ++i ) {
+      regis.setTransformationToZero ( );
+      ArrayType tpl ( grid );
+      memcpy ( tpl.getData ( ), &frames[( size_t ) ( first + i ) * N], N * sizeof ( RealType ) );
+      regis.initRefOrTemplate ( tpl, qc::TEMPLATE, false );
+      regis.solveAndProlongToMaxDepth ( );
+      double energy = regis.getEnergyOfLastSolution ( );
+      regis.getTransformation ( cur );
+      qc::MultiArray<RealType, qc::QC_2D> tmp ( acc, aol::DEEP_COPY );
+      regis.composeDeformations ( cur, tmp, acc );
+      if ( i > 0 ) {
+        regis.setTransformation ( acc );
+        regis.setReference ( reference );
+        regis.solveAndProlongToMaxDepth ( refineStart, refineStop );
+        energy = regis.getEnergyOfLastSolution ( );
+        regis.getTransformation ( acc );
+      }
+      const qc::MultiArray<RealType, qc::QC_2D> &res = ( i == 0 ) ? cur : acc;
+      memcpy ( &phis[( size_t ) 2 * i * N], res[0].getData ( ), N * sizeof ( RealType ) );
+      memcpy ( &phis[( size_t ) ( 2 * i + 1 ) * N], res[1].getData ( ), N * sizeof ( RealType ) );
+      fprintf ( info, "energy %d %d %.17g\n", stage, i, energy );
+      regis.setReference ( regis.getTemplImageReference ( ) );
+    }
+    const double t1 = wallSeconds ( );
+    aol::MultiVector<RealType> deformed ( m, N );
+    for ( int i = 0; i < m; ++i ) {
+      aol::Vector<RealType> img ( &frames[( size_t ) ( first + i ) * N], N, aol::FLAT_COPY );
+      aol::MultiVector<RealType> p ( 2, N );
+      memcpy ( p[0].getData ( ), &phis[( size_t ) 2 * i * N], N * sizeof ( RealType ) );
+      memcpy ( p[1].getData ( ), &phis[( size_t ) ( 2 * i + 1 ) * N], N * sizeof ( RealType ) );
+      qc::DeformImage<ConfType> ( img, grid, deformed[i], p, true, aol::NumberTrait<RealType>::Inf, false );
+    }
+    aol::Vector<RealType> last ( &frames[( size_t ) ( F - 1 ) * N], N, aol::FLAT_COPY );
+    const RealType lastMean = last.getMeanValue ( );
+    ArrayType avg ( grid ), cnt ( grid );
+    for ( int j = 0; j < N; ++j ) {
+      RealType a = 0; int k = 0;
+      for ( int i = 0; i < m; ++i )
+        if ( deformed[i][j] != aol::NumberTrait<RealType>::Inf ) { a += deformed[i][j]; ++k; }
+      avg[j] = ( k > 0 ) ? a / k : lastMean;
+      cnt[j] = k;
+    }
+    aol::Vector<RealType> median ( N );
+    deformed.getMedianVecOverComponents ( median, lastMean );
+    const double t2 = wallSeconds ( );
+    fprintf ( info, "stage %d lambda %.17g registration_seconds %.6f average_seconds %.6f\n", stage, lam, t1 - t0, t2 - t1 );
+    const std::string sfx = aol::strprintf ( "%d.bin", stage );
+    writeBin ( ( out + "_phis" + sfx ).c_str ( ), &phis[0], ( size_t ) 2 * N * m );
+    writeBin ( ( out + "_avg" + sfx ).c_str ( ), avg.getData ( ), N );
+    writeBin ( ( out + "_median" + sfx ).c_str ( ), median.getData ( ), N );
+    writeBin ( ( out + "_count" + sfx ).c_str ( ), cnt.getData ( ), N );
+    if ( useMedian ) memcpy ( target.getData ( ), median.getData ( ), N * sizeof ( RealType ) );
+    else memcpy ( target.getData ( ), avg.getData ( ), N * sizeof ( RealType ) );
+    delete parser;
+  }
+  fclose ( info );
+}
+
 static int usage ( ) {
   fprintf ( stderr,
     "ms_ref energy[_ncc] L R T px py lambda outPrefix\n"
@@ -256,7 +358,10 @@ static int usage ( ) {
     "ms_ref gdlevel[_ncc] L R T px py lambda maxIter stopEps outPhi outTrace\n"
     "ms_ref register[_ncc] maxL start stop R T px py lambda lambdaFactor maxIter stopEps resample outPhi outTxt\n"
     "ms_ref normalize L in sat minToZero out\n"
-    "ms_ref series[_ncc] maxL start stop lambda lambdaFactor maxIter stopEps sat minToZero F framesBin outPhis outMean outTxt\n" );
+    "ms_ref compose L d1 d2 inout | median L F frames phis fill out\n"
+    "ms_ref series[_ncc] maxL start stop lambda lambdaFactor maxIter stopEps sat minToZero F framesBin outPhis outMean outTxt\n"
+    "ms_ref matchseries[_ncc] maxL start stop lambda lambdaFactor maxIter stopEps sat minToZero refineStart refineStop\n"
+    "       extraStages extraLambdaFactor useMedian F framesBin outPrefix\n" );
   return 1;
 }
 
@@ -358,6 +463,48 @@ int main ( int argc, char **argv ) {
     if ( ( cmd == "register" || cmd == "register_ncc" ) && argc == 16 ) {
       if ( cmd == "register" ) registerCommand<RegisType> ( argv );
       else registerCommand<RegisTypeNCC> ( argv );
+      return 0;
+    }
+    if ( ( cmd == "matchseries" || cmd == "matchseries_ncc" ) && argc == 19 ) {
+      if ( cmd == "matchseries" ) matchSeriesCommand<RegisType> ( argv );
+      else matchSeriesCommand<RegisTypeNCC> ( argv );
+      return 0;
+    }
+    if ( cmd == "compose" && argc == 7 ) {
+      // ms_ref compose L d1 d2 inout (2 components each; inout: initial guess in, result out)
+      const int L = atoi ( argv[2] ), n = lvlN ( L ), N = n * n;
+      qc::GridDefinition grid ( L, qc::QC_2D );
+      aol::MultiVector<RealType> d1 ( 2, N ), d2 ( 2, N ), out ( 2, N );
+      std::vector<RealType> buf ( 2 * N );
+      readBin ( argv[3], &buf[0], 2 * N );
+      memcpy ( d1[0].getData ( ), &buf[0], N * sizeof ( RealType ) ); memcpy ( d1[1].getData ( ), &buf[N], N * sizeof ( RealType ) );
+      readBin ( argv[4], &buf[0], 2 * N );
+      memcpy ( d2[0].getData ( ), &buf[0], N * sizeof ( RealType ) ); memcpy ( d2[1].getData ( ), &buf[N], N * sizeof ( RealType ) );
+      readBin ( argv[5], &buf[0], 2 * N );
+      memcpy ( out[0].getData ( ), &buf[0], N * sizeof ( RealType ) ); memcpy ( out[1].getData ( ), &buf[N], N * sizeof ( RealType ) );
+      qc::ConcatAndSmoothlyExtendDeformations<ConfType> ( d1, d2, grid, out );
+      memcpy ( &buf[0], out[0].getData ( ), N * sizeof ( RealType ) ); memcpy ( &buf[N], out[1].getData ( ), N * sizeof ( RealType ) );
+      writeBin ( argv[6], &buf[0], 2 * N );
+      return 0;
+    }
+    if ( cmd == "median" && argc == 8 ) {
+      // ms_ref median L F frames phis fill out: median of the warped frames (Inf extension)
+      const int L = atoi ( argv[2] ), n = lvlN ( L ), N = n * n, F = atoi ( argv[3] );
+      qc::GridDefinition grid ( L, qc::QC_2D );
+      std::vector<RealType> frames ( ( size_t ) F * N ), phis ( ( size_t ) 2 * F * N );
+      readBin ( argv[4], &frames[0], ( size_t ) F * N );
+      readBin ( argv[5], &phis[0], ( size_t ) 2 * F * N );
+      aol::MultiVector<RealType> deformed ( F, N );
+      for ( int f = 0; f < F; ++f ) {
+        aol::Vector<RealType> img ( &frames[( size_t ) f * N], N, aol::FLAT_COPY );
+        aol::MultiVector<RealType> p ( 2, N );
+        memcpy ( p[0].getData ( ), &phis[( size_t ) 2 * f * N], N * sizeof ( RealType ) );
+        memcpy ( p[1].getData ( ), &phis[( size_t ) ( 2 * f + 1 ) * N], N * sizeof ( RealType ) );
+        qc::DeformImage<ConfType> ( img, grid, deformed[f], p, true, aol::NumberTrait<RealType>::Inf, false );
+      }
+      aol::Vector<RealType> median ( N );
+      deformed.getMedianVecOverComponents ( median, atof ( argv[6] ) );
+      writeBin ( argv[7], median.getData ( ), N );
       return 0;
     }
     if ( cmd == "normalize" && argc == 7 ) {

@@ -8,7 +8,8 @@ CPU oracle and the CUDA path.  Run from the repository root:
 
     make -f oracle/Makefile.ref && python tests/golden/make_golden.py
 
-(--ncc-only regenerates only the fixtures of the cross-correlation data term.)
+(--ncc-only regenerates only the fixtures of the cross-correlation data term,
+--series-only those of the series pipeline: composition, median, stages.)
 """
 from __future__ import annotations
 
@@ -142,10 +143,63 @@ def ncc_register(ref: msor.RefRunner, level: int, seed: int):
                         lam=0.1, max_iter=15, phi=np.stack([px, py]), E=np.array([e]))
 
 
+def smooth_field(n, rng, amp_px, shift_px=(0.0, 0.0)):
+    """A smooth displacement (domain units): a constant shift plus two
+    sinusoids per component, amplitudes in pixels."""
+    y, x = np.mgrid[0:n, 0:n] / (n - 1)
+    out = np.zeros((2, n * n))
+    for c in range(2):
+        f = shift_px[c] + sum(amp_px * rng.uniform(0.3, 1.0) *
+                              np.sin(2 * np.pi * (rng.uniform(0.5, 2) * x + rng.uniform(0.5, 2) * y) + rng.uniform(0, 6))
+                              for _ in range(2))
+        out[c] = (f / (n - 1)).ravel()
+    return out
+
+
+def compose(ref: msor.RefRunner, level: int, seed: int):
+    """ConcatAndSmoothlyExtendDeformations with a shifted d2 (a band of
+    nodes leaves the domain and is extended) and with a small d2 (no node
+    leaves), the initial guess being d2 as in series matching; and the
+    median of warped frames for an odd and an even frame count."""
+    n = n_of(level)
+    rng = np.random.default_rng(seed)
+    d1 = smooth_field(n, rng, 1.5)
+    d2 = smooth_field(n, rng, 1.0, shift_px=(2.5, -1.5))
+    d2s = smooth_field(n, rng, 0.3)
+    out = ref.compose(level, d1, d2)
+    out_in = ref.compose(level, d1, d2s)
+    F = 5
+    fr, _, _ = syn.make_series(n, F, syn.HEX_513, seed=seed)
+    frames = fr.reshape(F, -1)
+    phis = np.stack([smooth_field(n, rng, 2.0, shift_px=(rng.uniform(-3, 3), rng.uniform(-3, 3))) for _ in range(F)])
+    med5 = ref.median(level, frames, phis, 0.5)
+    med4 = ref.median(level, frames[:4], phis[:4], 0.25)
+    np.savez_compressed(os.path.join(OUT, f"compose_L{level}.npz"), level=level, d1=d1, d2=d2, out=out, d2_in=d2s,
+                        out_in=out_in, frames=frames, phis=phis, med5=med5, med4=med4)
+
+
+def match_series(ref: msor.RefRunner, level: int, F: int, seed: int):
+    """matchSeries<>() with accumulated deformations: stage 1 plus one extra
+    stage against the median, refinement from level 5."""
+    n = n_of(level)
+    fr, _, _ = syn.make_series(n, F, syn.HEX_513, seed=seed)
+    frames = fr.reshape(F, -1)
+    kw = dict(start=3, stop=level, max_iter=12, refine_start=5, extra_stages=1, extra_lam_factor=0.3,
+              use_median=True)
+    phis, avg, med, cnt, energies, _ = ref.match_series(level, frames=frames, **kw)
+    np.savez_compressed(os.path.join(OUT, f"match_series_L{level}.npz"), level=level, frames=frames, phis=phis,
+                        avg=avg, median=med, count=cnt, energies1=energies[0], energies2=energies[1],
+                        **{k: np.array(v) for k, v in kw.items()})
+
+
 def main():
     if not msor.have_ref():
         raise SystemExit("oracle/_ref/ms_ref is missing: make -f oracle/Makefile.ref")
     ref = msor.RefRunner()
+    if "--series-only" in sys.argv:
+        compose(ref, 6, 601)
+        match_series(ref, 6, 4, 602)
+        return
     if "--ncc-only" in sys.argv:
         ncc(ref, 5, 501, 20)
         ncc(ref, 6, 502, 15)
@@ -160,6 +214,8 @@ def main():
     ncc(ref, 5, 501, 20)
     ncc(ref, 6, 502, 15)
     ncc_register(ref, 7, 503)
+    compose(ref, 6, 601)
+    match_series(ref, 6, 4, 602)
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(OUT, f)))
