@@ -108,6 +108,68 @@ int msgpu_match_series_stage_device(msgpu_context* ctx, const msgpu_params* p, c
                                     double* d_energies_out, int* d_steps_out, double* d_mean_out,
                                     double* d_count_out, void* stream);
 
+/* --- series pipeline ------------------------------------------------------ */
+/* Options of matchSeries<>() beyond the registration keys (parameter-file
+ * names of the reference).                                                  */
+typedef struct {
+  int refine_start_level;            /* refineStartLevel (required by the reference) */
+  int refine_stop_level;             /* refineStopLevel (default precisionLevel)     */
+  int num_extra_stages;              /* numExtraStages                               */
+  double extra_stages_lambda_factor; /* extraStagesLambdaFactor                      */
+  int use_median_as_new_target;      /* useMedianAsNewTarget                         */
+  int dont_accumulate_deformation;   /* dontAccumulateDeformation                    */
+} msgpu_series_params;
+/* refine levels = the registration's start_level .. precision_level, no extra
+ * stages, factor 1, average as the new target, accumulation on.             */
+void msgpu_series_params_default(const msgpu_params* p, msgpu_series_params* s);
+
+/* matchSeries<>() (matchSeries.h:1250-1320) with SeriesMatching::matchSeries
+ * (matchSeries.h:87-265) and averageSeries (matchSeries.h:353-445) per stage:
+ *   stage 1: frame 0 is the reference, frames 1..F-1 the templates; every
+ *   extra stage registers frames 0..F-1 to the previous stage's average (or
+ *   median) with lambda = the "%f" print of lambda * extra_stages_lambda_factor.
+ *   With accumulation each template is registered to the previous template
+ *   (all of a stage in one batch), composed with the accumulated displacement
+ *   (ConcatAndSmoothlyExtendDeformations) and, from the second template on,
+ *   refined against the stage's reference on refine_start..refine_stop, one
+ *   template after the other; without accumulation every template is
+ *   registered to the stage's reference.
+ *   frames      : num_frames images of (2^precision_level+1)^2 doubles
+ *                 (input_level must equal precision_level; stop_level too)
+ *   phis_out    : the last stage's displacements, m x 2 x N doubles, m =
+ *                 num_frames-1 without extra stages, num_frames with them
+ *   energies_out (nullable): per stage and template the energy of its last
+ *                 solve (energies.txt): (num_frames-1) + extra*num_frames
+ *   average_out + count_out, median_out (nullable): the last stage's average
+ *                 with its sample count, and median, of the warped raw frames */
+int msgpu_match_series(msgpu_context* ctx, const msgpu_params* p, const msgpu_series_params* s,
+                       const double* frames, int num_frames, double* phis_out, double* energies_out,
+                       double* average_out, double* median_out, double* count_out);
+int msgpu_match_series_device(msgpu_context* ctx, const msgpu_params* p, const msgpu_series_params* s,
+                              const double* d_frames, int num_frames, double* d_phis_out, double* d_energies_out,
+                              double* d_average_out, double* d_median_out, double* d_count_out, void* stream);
+
+/* ConcatAndSmoothlyExtendDeformations (deformations.h:498-520) as called by
+ * composeDeformations(d1, d2, inout) (registration.h:584-586): the
+ * displacement of (id + d1) o (id + d2); where x + d2(x) leaves the domain the
+ * result is the discrete harmonic extension of SmoothlyExtendImage
+ * (deformations.h:364-410, PCG to g.g < 1e-16, at most 1000 steps).
+ *   d1, d2, inout: 2*N doubles [x | y]; inout holds the solver's initial
+ *   guess on entry (the destination's previous content in the reference).
+ *   iterations_out (nullable): PCG steps of the two components.            */
+int msgpu_compose(msgpu_context* ctx, int level, const double* d1, const double* d2, double* inout,
+                  int* iterations_out);
+int msgpu_compose_device(msgpu_context* ctx, int level, const double* d_d1, const double* d_d2, double* d_inout,
+                         void* stream);
+
+/* Median of the warped frames over the finite samples (averageSeries,
+ * matchSeries.h:442, MultiVector::getMedianVecOverComponents,
+ * multiVector.cpp:99-117); pixels without samples take the last frame's mean. */
+int msgpu_warp_median(msgpu_context* ctx, int level, const double* frames, const double* phis, int num_frames,
+                      double* median_out);
+int msgpu_warp_median_device(msgpu_context* ctx, int level, const double* d_frames, const double* d_phis,
+                             int num_frames, double* d_median_out, void* stream);
+
 /* Per-call statistics (no counterpart in the reference; used for the roofline).
  * With profiling on, every batch call records CUDA events around each level
  * launch on its stream and waits for them at the end of the call.          */

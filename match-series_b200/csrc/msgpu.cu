@@ -23,6 +23,7 @@
 
 #include "../../include/msgpu.h"
 #include "msgpu_level.cuh"
+#include "msgpu_series.cuh"
 
 using namespace msg;
 
@@ -33,7 +34,7 @@ struct msgpu_context {
   cudaStream_t stream = nullptr;
   // growable device buffers
   struct Buf { void* p = nullptr; size_t cap = 0; };
-  Buf arena, shared_real, dscratch, small, phis_d, io[6], prof, sched, flags, nccbuf;
+  Buf arena, shared_real, dscratch, small, phis_d, io[6], prof, sched, flags, nccbuf, ext, series, vals;
   int data_term = 0;           // data term of the single-operator entry points
   int* sched_error = nullptr;  // device flag of the level scheduler (in flags)
   // statistics of the last batch call
@@ -46,7 +47,7 @@ struct msgpu_context {
 
 namespace {
 
-constexpr int kAbiVersion = 2;
+constexpr int kAbiVersion = 3;
 
 int fail(msgpu_context* ctx, int code, const char* fmt, ...) {
   char buf[512];
@@ -127,6 +128,8 @@ void host_fe_tables(FeTables& t) {
       }
   for (int i = 0; i < 4; ++i)
     for (int j = i; j < 4; ++j) L[j][i] = L[i][j] = L[i][j] * vol;
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) t.lst[i][j] = L[i][j];
   // assemble on a 5x5 node grid in element order and read the 9 node classes
   const int n = 5;
   std::vector<double> st((size_t)n * n * 9, 0.0);
@@ -393,8 +396,14 @@ __global__ void k_set_buf(int* buf, int n, int v) {
 // (registration.h:1932-1944): u = R - sum_i (M R)_i, var = sqrt(u . M u),
 // out = u / var (u when var is within 1e-15 of 0).  Sums are deterministic
 // (fixed thread assignment, warps reduced in order).
+// One block per reference: block 0 normalises R0 into out0; with pairwise
+// references block b > 0 normalises the template of instance b - 1 (at
+// arena + (b-1)*inst_stride + off_T) into out0 + b*out_stride.
 template <typename Real>
-__global__ void k_ncc_normalize(const Real* __restrict__ R, int level, Real* out) {
+__global__ void k_ncc_normalize(const Real* __restrict__ R0, const Real* __restrict__ arena, size_t inst_stride,
+                                size_t off_T, int level, Real* out0, size_t out_stride) {
+  const Real* __restrict__ R = blockIdx.x == 0 ? R0 : arena + (size_t)(blockIdx.x - 1) * inst_stride + off_T;
+  Real* out = out0 + (size_t)blockIdx.x * out_stride;
   const int n = lvl_n(level), P = pitch_of(n), N = n * n;
   const Real h = (Real)(1.0 / (double)(n - 1)), hh = h * h;
   __shared__ double red[32];
@@ -466,22 +475,6 @@ __global__ void k_collect(const double* e, const int* s, int num, double* e_out,
   }
 }
 
-// ScalarArray<QC_2D>::interpolate (scalarArray.h:499-525).
-__device__ __forceinline__ double interp_d(const double* img, int n, double X, double Y) {
-  int xL = (int)X, yL = (int)Y;
-  if (X >= (double)(n - 1)) xL = n - 2;
-  if (Y >= (double)(n - 1)) yL = n - 2;
-  if (X < 0.) xL = 0;
-  if (Y < 0.) yL = 0;
-  X -= xL;
-  Y -= yL;
-  const int xU = xL + 1, yU = yL + 1;
-  const double v0 = img[xL + (size_t)yL * n], v1 = img[xU + (size_t)yL * n];
-  if (Y == 0) return (1 - X) * v0 + X * v1;
-  const double v2 = img[xL + (size_t)yU * n], v3 = img[xU + (size_t)yU * n];
-  return (1 - X) * (1 - Y) * v0 + X * (1 - Y) * v1 + (1 - X) * Y * v2 + X * Y * v3;
-}
-
 // Warped-frame average: DeformImage with Inf extension per frame
 // (deformations.h:62-101), mean over finite samples (matchSeries.h:410-425).
 __global__ void k_warp_mean(const double* __restrict__ frames, const double* __restrict__ phis, int F, int level,
@@ -531,11 +524,12 @@ struct Layout {
   size_t off_T[kMaxLevel + 1];
   size_t off_phi[2], off_d[2], off_s, off_de;
   size_t off_td;   // NCC only: deformed template at the nodes
+  size_t off_nr;   // NCC with pairwise references only: the instance's normalised reference
   size_t off_x2[kMaxLevel + 1], off_x5[kMaxLevel + 1], off_b[kMaxLevel + 1];
   size_t stride;
 };
 
-Layout make_layout(int M, bool ncc = false) {
+Layout make_layout(int M, bool ncc = false, bool pairwise = false) {
   Layout L;
   size_t off = 0;
   const size_t a = 64;
@@ -548,6 +542,8 @@ Layout make_layout(int M, bool ncc = false) {
   L.off_de = off; off = align_up(off + two, a);
   L.off_td = 0;
   if (ncc) { L.off_td = off; off = align_up(off + comp_stride(M), a); }
+  L.off_nr = 0;
+  if (ncc && pairwise) { L.off_nr = off; off = align_up(off + comp_stride(M), a); }
   for (int k = 0; k <= kMaxLevel; ++k) {
     if (k <= M) {
       L.off_x2[k] = off; off = align_up(off + 2 * comp_stride(k), a);
@@ -649,23 +645,26 @@ int launch_level(msgpu_context* ctx, LevelArgs<Real>& a, cudaStream_t st) {
   return MSGPU_OK;
 }
 
-// Clears the scheduler error flag at the start of an API call.
+// Clears the error flags at the start of an API call: word 0 is set by a
+// level-kernel worker that gave up waiting for work, word 1 by the
+// composition kernel when a grid-barrier wait gave up.
 int sched_error_reset(msgpu_context* ctx, cudaStream_t st) {
   int rc;
   if (!ctx->sched_error) {
     if ((rc = ensure(ctx, ctx->flags, 256))) return rc;
     ctx->sched_error = (int*)ctx->flags.p;
   }
-  CK(cudaMemsetAsync(ctx->sched_error, 0, sizeof(int), st));
+  CK(cudaMemsetAsync(ctx->sched_error, 0, 2 * sizeof(int), st));
   return MSGPU_OK;
 }
 
-// After the call's work has completed: reports a scheduler that stalled.
+// After the call's work has completed: reports a kernel that gave up waiting.
 int sched_error_check(msgpu_context* ctx) {
-  int h = 0;
+  int h[2] = {0, 0};
   if (!ctx->sched_error) return MSGPU_OK;
-  CK(cudaMemcpy(&h, ctx->sched_error, sizeof(int), cudaMemcpyDeviceToHost));
-  if (h) return fail(ctx, MSGPU_ERR_CUDA, "level kernel: a worker waited too long for work (scheduler stalled)");
+  CK(cudaMemcpy(h, ctx->sched_error, sizeof(h), cudaMemcpyDeviceToHost));
+  if (h[0]) return fail(ctx, MSGPU_ERR_CUDA, "level kernel: a worker waited too long for work (scheduler stalled)");
+  if (h[1]) return fail(ctx, MSGPU_ERR_CUDA, "composition: a grid-barrier wait timed out");
   return MSGPU_OK;
 }
 
@@ -682,17 +681,27 @@ struct BatchIO {
   int* steps_out;           // device or null
 };
 
+// Options of a batch beyond the parameter file.
+struct BatchOpts {
+  int pairwise = 0;      // template i > 0 is registered to template i - 1 (series matching, matchSeries.h:141-155)
+  int lambda_stop = -1;  // level that lambdaFactor's exponent counts from (default: stop_level)
+  int reset_error = 1;   // clear the error flags (0: a caller running several batches clears them once)
+};
+
 template <typename Real>
-int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& io, cudaStream_t st) {
+int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& io, cudaStream_t st,
+              const BatchOpts& opt = BatchOpts()) {
   const int M = p.precision_level, Lin = p.input_level;
   const int start = p.start_level, stop = p.stop_level;
+  const int lambda_stop = opt.lambda_stop >= 0 ? opt.lambda_stop : stop;
   const int nimg = F + 1;  // image 0 is the reference
   const size_t Nin = lvl_N(Lin);
   const bool ncc = p.data_term == 1;
-  const Layout L = make_layout(M, ncc);
+  const bool pairwise = opt.pairwise != 0 && F > 1;
+  const Layout L = make_layout(M, ncc, pairwise);
   int rc;
   if ((rc = ensure_tables(ctx))) return rc;
-  if ((rc = sched_error_reset(ctx, st))) return rc;
+  if (opt.reset_error && (rc = sched_error_reset(ctx, st))) return rc;
   if (ncc && (rc = ensure(ctx, ctx->nccbuf, sizeof(Real) * (comp_stride(M) + 64)))) return rc;
   // --- double scratch: per image a pyramid from Lin down to 0
   std::vector<size_t> poff(Lin + 1);
@@ -799,11 +808,16 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
     a.arena = arena;
     a.inst_stride = L.stride;
     a.R = Rpyr + L.off_T[l];
+    a.r_prev = pairwise ? 1 : 0;
     if (ncc) {
       a.ncc = 1;
       a.normR = (const Real*)ctx->nccbuf.p;
       a.off_td = L.off_td;
-      k_ncc_normalize<Real><<<1, 1024, 0, st>>>(a.R, l, (Real*)ctx->nccbuf.p);
+      a.off_nr = L.off_nr;
+      if (pairwise)
+        k_ncc_normalize<Real><<<F, 1024, 0, st>>>(a.R, arena, L.stride, L.off_T[l], l, arena + L.off_nr, L.stride);
+      else
+        k_ncc_normalize<Real><<<1, 1024, 0, st>>>(a.R, arena, L.stride, L.off_T[l], l, (Real*)ctx->nccbuf.p, 0);
       ++launches;
     }
     a.off_T = L.off_T[l];
@@ -819,7 +833,7 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
     a.num_inst = F;
     a.lc = pick_lc<Real>(l);
     a.mode = MODE_SOLVE;
-    a.lambda = std::pow(p.lambda_factor, (double)(stop - l)) * p.lambda;
+    a.lambda = std::pow(p.lambda_factor, (double)(lambda_stop - l)) * p.lambda;
     a.stop_eps = p.stop_epsilon;
     a.max_iter = p.max_gd_iterations;
     a.phi_in_dev = bin;
@@ -916,6 +930,214 @@ int bind_device(msgpu_context* ctx) {
   return MSGPU_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Series pipeline: composition, median, the stage loop.
+
+// Grid of the composition kernel (cooperative: every CTA resident).
+int compose_grid(msgpu_context* ctx, int* grid) {
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_extend_pcg, kExtThreads, 0));
+  if (per_sm < 1) return fail(ctx, MSGPU_ERR_CUDA, "composition kernel does not fit on an SM");
+  *grid = std::min(per_sm, 2) * ctx->sm_count;
+  return MSGPU_OK;
+}
+
+// Doubles of the composition scratch before its counters: bc, g, hA, hB (2N
+// each), two directions (4N), the per-CTA partials.
+size_t compose_doubles(size_t N, int grid) { return 12 * N + (size_t)grid * 4; }
+
+// ConcatAndSmoothlyExtendDeformations on device arrays (2N each); inout
+// carries the solver's initial guess in.  The error flags must have been
+// cleared by the API call (sched_error_reset).
+int compose_device(msgpu_context* ctx, int level, const double* d1, const double* d2, double* inout,
+                   cudaStream_t st) {
+  const size_t N = lvl_N(level);
+  int rc, grid = 0;
+  if ((rc = ensure_tables(ctx))) return rc;
+  if ((rc = compose_grid(ctx, &grid))) return rc;
+  const size_t nd = compose_doubles(N, grid);
+  const size_t bytes = sizeof(double) * nd + 64 + align_up(N, 256);
+  if ((rc = ensure(ctx, ctx->ext, bytes))) return rc;
+  double* base = (double*)ctx->ext.p;
+  ExtArgs a;
+  a.d1 = d1;
+  a.d2 = d2;
+  a.x = inout;
+  a.bc = base;
+  a.g = base + 2 * N;
+  a.hA = base + 4 * N;
+  a.hB = base + 6 * N;
+  a.dbuf = base + 8 * N;
+  a.partials = base + 12 * N;
+  a.bar = (unsigned*)(base + nd);
+  a.iters_out = (int*)(a.bar + 2);
+  a.defined = (unsigned char*)(base + nd) + 64;
+  a.error = ctx->sched_error + 1;
+  a.level = level;
+  CK(cudaMemsetAsync(a.bar, 0, 2 * sizeof(unsigned), st));
+  k_compose_prep<<<(unsigned)std::min<size_t>(2048, (N + 255) / 256), 256, 0, st>>>(a);
+  CK(cudaGetLastError());
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.gridDim = dim3(grid, 1, 1);
+  cfg.blockDim = dim3(kExtThreads, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  CK(cudaLaunchKernelEx(&cfg, k_extend_pcg, a));
+  ctx->stats.kernel_launches += 2;
+  return MSGPU_OK;
+}
+
+// PCG steps per component of the last composition (after synchronising).
+int compose_iterations(msgpu_context* ctx, int level, int it[2]) {
+  int rc, grid = 0;
+  if ((rc = compose_grid(ctx, &grid))) return rc;
+  const size_t nd = compose_doubles(lvl_N(level), grid);
+  CK(cudaMemcpy(it, (const unsigned char*)ctx->ext.p + sizeof(double) * nd + 2 * sizeof(unsigned), 2 * sizeof(int),
+                cudaMemcpyDeviceToHost));
+  return MSGPU_OK;
+}
+
+// Average and median of the warped frames (averageSeries, matchSeries.h:
+// 385-445); the fill of pixels without samples is the mean of the last frame.
+int average_median_device(msgpu_context* ctx, int level, const double* frames, const double* phis, int F,
+                          double* avg, double* median, double* count, cudaStream_t st) {
+  const size_t N = lvl_N(level);
+  int rc;
+  if ((rc = ensure(ctx, ctx->io[5], 64))) return rc;
+  double* fill = (double*)ctx->io[5].p;
+  k_mean<<<1, 1024, 0, st>>>(frames + (size_t)(F - 1) * N, (int)N, fill);
+  ctx->stats.kernel_launches += 1;
+  if (avg) {
+    k_warp_mean<<<(unsigned)std::min<size_t>(2048, (N + 255) / 256), 256, 0, st>>>(frames, phis, F, level, fill,
+                                                                                  avg, count);
+    ctx->stats.kernel_launches += 1;
+  }
+  if (median) {
+    if ((rc = ensure(ctx, ctx->vals, sizeof(double) * N * F))) return rc;
+    double* vals = (double*)ctx->vals.p;
+    k_warp_values<<<dim3((unsigned)std::min<size_t>(1024, (N + 255) / 256), F), 256, 0, st>>>(frames, phis, F,
+                                                                                              level, vals);
+    k_median<<<(unsigned)std::min<size_t>(2048, (N + 255) / 256), 256, 0, st>>>(vals, F, (int)N, fill, median);
+    ctx->stats.kernel_launches += 2;
+  }
+  CK(cudaGetLastError());
+  return MSGPU_OK;
+}
+
+// lambda of the extra stages: the parameter file value is replaced by the
+// "%f" print of lambda * extraStagesLambdaFactor (matchSeries.h:1300).
+double extra_stage_lambda(double lambda, double factor) {
+  char buf[64];
+  snprintf(buf, sizeof buf, "%f", lambda * factor);
+  return strtod(buf, nullptr);
+}
+
+int check_series_params(msgpu_context* ctx, const msgpu_params* p, const msgpu_series_params* sp, int F) {
+  int rc;
+  if ((rc = check_params(ctx, p))) return rc;
+  if (!sp) return fail(ctx, MSGPU_ERR_INVALID_ARG, "series params is NULL");
+  if (F < 2) return fail(ctx, MSGPU_ERR_INVALID_ARG, "series matching needs at least 2 frames");
+  if (p->input_level != p->precision_level)
+    return fail(ctx, MSGPU_ERR_UNSUPPORTED, "series matching needs input_level == precision_level");
+  if (p->stop_level != p->precision_level)
+    return fail(ctx, MSGPU_ERR_UNSUPPORTED, "series matching needs stopLevel == precisionLevel");
+  if (sp->num_extra_stages < 0) return fail(ctx, MSGPU_ERR_INVALID_ARG, "numExtraStages < 0");
+  if (!sp->dont_accumulate_deformation &&
+      (sp->refine_start_level < 1 || sp->refine_stop_level > p->precision_level ||
+       sp->refine_start_level > sp->refine_stop_level))
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "refineStartLevel %d .. refineStopLevel %d invalid for precisionLevel %d",
+                sp->refine_start_level, sp->refine_stop_level, p->precision_level);
+  return MSGPU_OK;
+}
+
+int series_num_energies(int F, int extra) { return (F - 1) + extra * F; }
+
+// The stage loop of matchSeries<>() on device arrays (see msgpu.h).
+template <typename Real>
+int run_series(msgpu_context* ctx, const msgpu_params& p, const msgpu_series_params& sp, const double* frames,
+               int F, double* phis_out, double* energies_out, double* avg_out, double* median_out,
+               double* count_out, cudaStream_t st) {
+  const int M = p.precision_level;
+  const size_t N = lvl_N(M);
+  const int stages = 1 + sp.num_extra_stages;
+  int rc;
+  // scratch: target N | acc 2N | tmp 2N | stage phis F*2N | energies | stage avg, median, count 3N
+  const size_t ne = (size_t)series_num_energies(F, sp.num_extra_stages);
+  const size_t need = sizeof(double) * (N + 4 * N + 2 * N * F + ne + 3 * N + 64);
+  if ((rc = ensure(ctx, ctx->series, need))) return rc;
+  double* target = (double*)ctx->series.p;
+  double* acc = target + N;
+  double* tmp = acc + 2 * N;
+  double* sphis = tmp + 2 * N;
+  double* en_scratch = sphis + 2 * N * F;
+  double* savg = en_scratch + ne;
+  double* smed = savg + N;
+  double* scnt = smed + N;
+  double* energies = energies_out ? energies_out : en_scratch;
+  if ((rc = sched_error_reset(ctx, st))) return rc;
+  int launches = 0;
+  BatchOpts keep;
+  keep.reset_error = 0;
+  size_t eoff = 0;
+  for (int s = 1; s <= stages; ++s) {
+    msgpu_params ps = p;
+    if (s > 1) ps.lambda = extra_stage_lambda(p.lambda, sp.extra_stages_lambda_factor);
+    const int first = (s == 1) ? 1 : 0, m = F - first;
+    const double* ref = (s == 1) ? frames : target;
+    const double* tmpl = frames + (size_t)first * N;
+    const bool last = (s == stages);
+    double* phis = last ? phis_out : sphis;
+    double* en = energies + eoff;
+    if (sp.dont_accumulate_deformation) {
+      BatchIO io{ref, tmpl, nullptr, phis, en, nullptr};
+      if ((rc = run_batch<Real>(ctx, ps, m, io, st, keep))) return rc;
+      launches += ctx->stats.kernel_launches;
+    } else {
+      BatchOpts pw = keep;
+      pw.pairwise = 1;
+      BatchIO io{ref, tmpl, nullptr, phis, en, nullptr};
+      if ((rc = run_batch<Real>(ctx, ps, m, io, st, pw))) return rc;
+      launches += ctx->stats.kernel_launches;
+      CK(cudaMemsetAsync(acc, 0, sizeof(double) * 2 * N, st));
+      msgpu_params pr = ps;
+      pr.start_level = sp.refine_start_level;
+      pr.stop_level = sp.refine_stop_level;
+      BatchOpts rf = keep;
+      rf.lambda_stop = ps.stop_level;
+      for (int i = 0; i < m; ++i) {
+        double* phi_i = phis + (size_t)2 * i * N;
+        CK(cudaMemcpyAsync(tmp, acc, sizeof(double) * 2 * N, cudaMemcpyDeviceToDevice, st));
+        ctx->stats.kernel_launches = 0;
+        if ((rc = compose_device(ctx, M, phi_i, tmp, acc, st))) return rc;
+        launches += ctx->stats.kernel_launches;
+        if (i > 0) {
+          BatchIO ri{ref, tmpl + (size_t)i * N, acc, acc, en + i, nullptr};
+          if ((rc = run_batch<Real>(ctx, pr, 1, ri, st, rf))) return rc;
+          launches += ctx->stats.kernel_launches;
+          CK(cudaMemcpyAsync(phi_i, acc, sizeof(double) * 2 * N, cudaMemcpyDeviceToDevice, st));
+        }
+      }
+    }
+    ctx->stats.kernel_launches = 0;
+    double* a_out = last ? avg_out : (sp.use_median_as_new_target ? nullptr : savg);
+    double* m_out = last ? median_out : (sp.use_median_as_new_target ? smed : nullptr);
+    if ((rc = average_median_device(ctx, M, tmpl, phis, m, a_out, m_out, last ? count_out : scnt, st)))
+      return rc;
+    launches += ctx->stats.kernel_launches;
+    if (!last)
+      CK(cudaMemcpyAsync(target, sp.use_median_as_new_target ? smed : savg, sizeof(double) * N,
+                         cudaMemcpyDeviceToDevice, st));
+    eoff += (size_t)m;
+  }
+  ctx->stats.kernel_launches = launches;
+  return MSGPU_OK;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -972,7 +1194,9 @@ int msgpu_destroy(msgpu_context* ctx) {
   if (!ctx) return MSGPU_OK;
   cudaSetDevice(ctx->device);
   msgpu_context::Buf* bufs[] = {&ctx->arena, &ctx->shared_real, &ctx->dscratch, &ctx->small, &ctx->phis_d,
-                                &ctx->io[0], &ctx->io[1], &ctx->io[2], &ctx->io[3], &ctx->io[4], &ctx->io[5]};
+                                &ctx->io[0], &ctx->io[1],   &ctx->io[2],    &ctx->io[3], &ctx->io[4],
+                                &ctx->io[5], &ctx->prof,    &ctx->sched,    &ctx->flags, &ctx->nccbuf,
+                                &ctx->ext,   &ctx->series,  &ctx->vals};
   for (auto* b : bufs)
     if (b->p) cudaFree(b->p);
   if (ctx->ev_ready)
@@ -1114,6 +1338,143 @@ int msgpu_match_series_stage(msgpu_context* ctx, const msgpu_params* p, const do
   return MSGPU_OK;
 }
 
+void msgpu_series_params_default(const msgpu_params* p, msgpu_series_params* s) {
+  if (!s) return;
+  s->refine_start_level = p ? p->start_level : 1;
+  s->refine_stop_level = p ? p->precision_level : 1;
+  s->num_extra_stages = 0;
+  s->extra_stages_lambda_factor = 1.0;
+  s->use_median_as_new_target = 0;
+  s->dont_accumulate_deformation = 0;
+}
+
+int msgpu_match_series_device(msgpu_context* ctx, const msgpu_params* p, const msgpu_series_params* s,
+                              const double* d_frames, int num_frames, double* d_phis_out, double* d_energies_out,
+                              double* d_average_out, double* d_median_out, double* d_count_out, void* stream) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  int rc;
+  if ((rc = check_series_params(ctx, p, s, num_frames))) return rc;
+  if (!d_frames || !d_phis_out || (d_average_out && !d_count_out))
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "null buffer");
+  if ((rc = bind_device(ctx))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  return p->use_fp64 ? run_series<double>(ctx, *p, *s, d_frames, num_frames, d_phis_out, d_energies_out,
+                                          d_average_out, d_median_out, d_count_out, st)
+                     : run_series<float>(ctx, *p, *s, d_frames, num_frames, d_phis_out, d_energies_out,
+                                         d_average_out, d_median_out, d_count_out, st);
+}
+
+int msgpu_match_series(msgpu_context* ctx, const msgpu_params* p, const msgpu_series_params* s,
+                       const double* frames, int num_frames, double* phis_out, double* energies_out,
+                       double* average_out, double* median_out, double* count_out) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  int rc;
+  if ((rc = check_series_params(ctx, p, s, num_frames))) return rc;
+  if (!frames || !phis_out || (average_out && !count_out)) return fail(ctx, MSGPU_ERR_INVALID_ARG, "null buffer");
+  if ((rc = bind_device(ctx))) return rc;
+  const size_t N = lvl_N(p->precision_level);
+  const int F = num_frames;
+  const int m = s->num_extra_stages > 0 ? F : F - 1;
+  const size_t ne = (size_t)series_num_energies(F, s->num_extra_stages);
+  if ((rc = ensure(ctx, ctx->io[1], sizeof(double) * N * F))) return rc;
+  if ((rc = ensure(ctx, ctx->io[3], sizeof(double) * (2 * N * m + 3 * N + ne)))) return rc;
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(ctx->io[1].p, frames, sizeof(double) * N * F, cudaMemcpyHostToDevice, st));
+  double* d_phis = (double*)ctx->io[3].p;
+  double* d_avg = d_phis + 2 * N * m;
+  double* d_med = d_avg + N;
+  double* d_cnt = d_med + N;
+  double* d_e = d_cnt + N;
+  rc = p->use_fp64 ? run_series<double>(ctx, *p, *s, (const double*)ctx->io[1].p, F, d_phis, d_e,
+                                        average_out ? d_avg : nullptr, median_out ? d_med : nullptr, d_cnt, st)
+                   : run_series<float>(ctx, *p, *s, (const double*)ctx->io[1].p, F, d_phis, d_e,
+                                       average_out ? d_avg : nullptr, median_out ? d_med : nullptr, d_cnt, st);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(phis_out, d_phis, sizeof(double) * 2 * N * m, cudaMemcpyDeviceToHost, st));
+  if (average_out) {
+    CK(cudaMemcpyAsync(average_out, d_avg, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(count_out, d_cnt, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+  }
+  if (median_out) CK(cudaMemcpyAsync(median_out, d_med, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+  if (energies_out) CK(cudaMemcpyAsync(energies_out, d_e, sizeof(double) * ne, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return sched_error_check(ctx);
+}
+
+int msgpu_compose_device(msgpu_context* ctx, int level, const double* d_d1, const double* d_d2, double* d_inout,
+                         void* stream) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (level < 1 || level > kMaxLevel || !d_d1 || !d_d2 || !d_inout)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid compose arguments");
+  if (d_inout == d_d1 || d_inout == d_d2)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "compose: inout must not alias d1 or d2");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((rc = sched_error_reset(ctx, st))) return rc;
+  ctx->stats.kernel_launches = 0;
+  return compose_device(ctx, level, d_d1, d_d2, d_inout, st);
+}
+
+int msgpu_compose(msgpu_context* ctx, int level, const double* d1, const double* d2, double* inout,
+                  int* iterations_out) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (level < 1 || level > kMaxLevel || !d1 || !d2 || !inout)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid compose arguments");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  const size_t N = lvl_N(level);
+  if ((rc = ensure(ctx, ctx->io[0], sizeof(double) * 6 * N))) return rc;
+  double* dd = (double*)ctx->io[0].p;
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(dd, d1, sizeof(double) * 2 * N, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dd + 2 * N, d2, sizeof(double) * 2 * N, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dd + 4 * N, inout, sizeof(double) * 2 * N, cudaMemcpyHostToDevice, st));
+  if ((rc = sched_error_reset(ctx, st))) return rc;
+  ctx->stats.kernel_launches = 0;
+  if ((rc = compose_device(ctx, level, dd, dd + 2 * N, dd + 4 * N, st))) return rc;
+  CK(cudaMemcpyAsync(inout, dd + 4 * N, sizeof(double) * 2 * N, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if ((rc = sched_error_check(ctx))) return rc;
+  if (iterations_out && (rc = compose_iterations(ctx, level, iterations_out))) return rc;
+  return MSGPU_OK;
+}
+
+int msgpu_warp_median_device(msgpu_context* ctx, int level, const double* d_frames, const double* d_phis,
+                             int num_frames, double* d_median_out, void* stream) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (level < 1 || level > kMaxLevel || num_frames < 1 || !d_frames || !d_phis || !d_median_out)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid warp_median arguments");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  ctx->stats.kernel_launches = 0;
+  return average_median_device(ctx, level, d_frames, d_phis, num_frames, nullptr, d_median_out, nullptr,
+                               (cudaStream_t)stream);
+}
+
+int msgpu_warp_median(msgpu_context* ctx, int level, const double* frames, const double* phis, int num_frames,
+                      double* median_out) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (level < 1 || level > kMaxLevel || num_frames < 1 || !frames || !phis || !median_out)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid warp_median arguments");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  const size_t N = lvl_N(level);
+  const int F = num_frames;
+  if ((rc = ensure(ctx, ctx->io[0], sizeof(double) * N * F))) return rc;
+  if ((rc = ensure(ctx, ctx->io[1], sizeof(double) * 2 * N * F))) return rc;
+  if ((rc = ensure(ctx, ctx->io[2], sizeof(double) * N))) return rc;
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(ctx->io[0].p, frames, sizeof(double) * N * F, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctx->io[1].p, phis, sizeof(double) * 2 * N * F, cudaMemcpyHostToDevice, st));
+  if ((rc = msgpu_warp_median_device(ctx, level, (const double*)ctx->io[0].p, (const double*)ctx->io[1].p, F,
+                                     (double*)ctx->io[2].p, st)))
+    return rc;
+  CK(cudaMemcpyAsync(median_out, ctx->io[2].p, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return MSGPU_OK;
+}
+
 int msgpu_set_profiling(msgpu_context* ctx, int on) {
   if (!ctx) return MSGPU_ERR_INVALID_ARG;
   ctx->profiling = (on != 0);
@@ -1205,7 +1566,7 @@ int single_level(msgpu_context* ctx, int level, int mode, const double* R, const
     a.ncc = 1;
     a.normR = (const Real*)ctx->nccbuf.p;
     a.off_td = L.off_td;
-    k_ncc_normalize<Real><<<1, 1024, 0, st>>>(Rd, level, (Real*)ctx->nccbuf.p);
+    k_ncc_normalize<Real><<<1, 1024, 0, st>>>(Rd, nullptr, 0, 0, level, (Real*)ctx->nccbuf.p, 0);
   }
   a.off_T = L.off_T[level];
   a.off_phi[0] = L.off_phi[0];

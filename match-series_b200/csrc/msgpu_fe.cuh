@@ -32,6 +32,9 @@ struct FeTables {
   // local matrix 1445-1475) for element volume 1; the stencil of a level is
   // this times h^2, an exact power-of-two scaling.
   double ms[9][3][3];
+  // Local Q1 stiffness matrix of one element (FELinScalarWeightedStiffInterface::
+  // prepareLocalMatrix, FEOpInterface.h:1362-1395), local node i = x + 2y.
+  double lst[4][4];
 };
 
 __constant__ FeTables c_fe;
@@ -391,6 +394,22 @@ __device__ __forceinline__ Real prolong_node(int x, int y, Get C) {
   };
   if ((y & 1) == 0) return even_row(Y);
   return (even_row(Y) + even_row(Y + 1)) / Real(2);
+}
+
+// ScalarArray<QC_2D>::interpolate (scalarArray.h:499-525).
+__device__ __forceinline__ double interp_d(const double* img, int n, double X, double Y) {
+  int xL = (int)X, yL = (int)Y;
+  if (X >= (double)(n - 1)) xL = n - 2;
+  if (Y >= (double)(n - 1)) yL = n - 2;
+  if (X < 0.) xL = 0;
+  if (Y < 0.) yL = 0;
+  X -= xL;
+  Y -= yL;
+  const int xU = xL + 1, yU = yL + 1;
+  const double v0 = img[xL + (size_t)yL * n], v1 = img[xU + (size_t)yL * n];
+  if (Y == 0) return (1 - X) * v0 + X * v1;
+  const double v2 = img[xL + (size_t)yU * n], v3 = img[xU + (size_t)yU * n];
+  return (1 - X) * (1 - Y) * v0 + X * (1 - Y) * v1 + (1 - X) * Y * v2 + X * Y * v3;
 }
 
 }  // namespace msg

@@ -86,6 +86,11 @@ struct LevelArgs {
   int ncc;
   const Real* normR;        // normalised reference on this level, pitched (shared)
   size_t off_td;            // per instance: deformed template at the nodes (1 component)
+  // r_prev != 0: instance i > 0 is registered to the template of instance
+  // i - 1 (the pairwise step of series matching) instead of R; with NCC each
+  // instance then reads its own normalised reference at off_nr.
+  int r_prev;
+  size_t off_nr;
 };
 
 // A 2-component array of level k occupies 2 * comp_stride(k) elements.
@@ -206,6 +211,7 @@ struct Inst {
   Real* base;
   const Real* R;
   const Real* T;
+  const Real* normR;
   int n, P;
   Real h;
   __device__ Real* arr(size_t off) const { return base + off; }
@@ -1134,8 +1140,9 @@ template <typename Real>
 __device__ __forceinline__ Inst<Real> make_inst(const LevelArgs<Real>& a, int inst) {
   Inst<Real> I;
   I.base = a.arena + (size_t)inst * a.inst_stride;
-  I.R = a.R;
+  I.R = (a.r_prev && inst > 0) ? a.arena + (size_t)(inst - 1) * a.inst_stride + a.off_T : a.R;
   I.T = I.base + a.off_T;
+  I.normR = a.r_prev ? I.base + a.off_nr : a.normR;
   I.n = a.n;
   I.P = pitch_of(a.n);
   I.h = (Real)(1.0 / (double)(a.n - 1));
@@ -1226,13 +1233,13 @@ struct TaskRunner {
         Real* td = I.arr(a.off_td);
         const bool step = (d.flags & PF_STEP) != 0, odz = (d.flags & PF_ODZERO) != 0;
         NccPass<Real> ps(I, sub, mode, (Real)d.t, (Real)d.beta, d.mean, d.var, odz, step, phi, phi + cs, dd, dd + cs,
-                         s, s + cs, de, de + cs, a.normR, wd, wd + cs, nphi, nphi + cs, td, smem, part);
+                         s, s + cs, de, de + cs, I.normR, wd, wd + cs, nphi, nphi + cs, td, smem, part);
         f(ps);
         break;
       }
       case TK_NF: {
         Real* nphi = I.arr(a.off_phi[d.cur ^ 1]);
-        NccForcePass<Real> ps(I, a.lambda, d.mean, d.var, d.e, nphi, nphi + cs, I.arr(a.off_td), a.normR, de, de + cs,
+        NccForcePass<Real> ps(I, a.lambda, d.mean, d.var, d.e, nphi, nphi + cs, I.arr(a.off_td), I.normR, de, de + cs,
                               smem, part);
         f(ps);
         break;

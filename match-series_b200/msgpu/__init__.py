@@ -41,6 +41,18 @@ class Params(ctypes.Structure):
     ]
 
 
+class SeriesParams(ctypes.Structure):
+    """msgpu_series_params: the keys of matchSeries<>() beyond the registration."""
+    _fields_ = [
+        ("refine_start_level", ctypes.c_int),
+        ("refine_stop_level", ctypes.c_int),
+        ("num_extra_stages", ctypes.c_int),
+        ("extra_stages_lambda_factor", ctypes.c_double),
+        ("use_median_as_new_target", ctypes.c_int),
+        ("dont_accumulate_deformation", ctypes.c_int),
+    ]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("kernel_launches", ctypes.c_int), ("num_levels", ctypes.c_int), ("first_level", ctypes.c_int),
                 ("level_ms", ctypes.c_float * 16), ("level_steps", ctypes.c_longlong * 16),
@@ -63,7 +75,8 @@ EXPORTS = [
     "msgpu_register_batch", "msgpu_register_batch_device", "msgpu_warp_mean", "msgpu_warp_mean_device",
     "msgpu_energy", "msgpu_smooth", "msgpu_restrict", "msgpu_prolong", "msgpu_normalize", "msgpu_gd_level",
     "msgpu_match_series_stage", "msgpu_match_series_stage_device", "msgpu_set_profiling", "msgpu_get_stats",
-    "msgpu_set_data_term",
+    "msgpu_set_data_term", "msgpu_series_params_default", "msgpu_match_series", "msgpu_match_series_device",
+    "msgpu_compose", "msgpu_compose_device", "msgpu_warp_median", "msgpu_warp_median_device",
 ]
 
 
@@ -105,6 +118,20 @@ def lib():
         L.msgpu_set_profiling.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.msgpu_set_data_term.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.msgpu_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(Stats)]
+        L.msgpu_series_params_default.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(SeriesParams)]
+        L.msgpu_series_params_default.restype = None
+        L.msgpu_match_series.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params), ctypes.POINTER(SeriesParams), _dp,
+                                         ctypes.c_int, _dp, _dp, _dp, _dp, _dp]
+        L.msgpu_match_series_device.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params),
+                                                ctypes.POINTER(SeriesParams), ctypes.c_void_p, ctypes.c_int,
+                                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                ctypes.c_void_p, ctypes.c_void_p]
+        L.msgpu_compose.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp, _ip]
+        L.msgpu_compose_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_void_p]
+        L.msgpu_warp_median.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp]
+        L.msgpu_warp_median_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                               ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -115,6 +142,14 @@ def default_params(**kw) -> Params:
     for k, v in kw.items():
         setattr(p, "lambda_" if k == "lambda" else k, v)
     return p
+
+
+def default_series_params(params: Params, **kw) -> SeriesParams:
+    s = SeriesParams()
+    lib().msgpu_series_params_default(ctypes.byref(params), ctypes.byref(s))
+    for k, v in kw.items():
+        setattr(s, k, v)
+    return s
 
 
 def n_of(level: int) -> int:
@@ -218,6 +253,52 @@ class Context:
         self._check(lib().msgpu_match_series_stage_device(self._h, ctypes.byref(params), d_ref, d_templates,
                                                           num_templates, d_phis, d_energies or None, d_steps or None,
                                                           d_mean, d_count, stream or None))
+
+    # --- series pipeline ----------------------------------------------------
+    def match_series(self, params: Params, series: SeriesParams, frames):
+        """matchSeries<>(): returns (phis[m,2,N], energies, average, median, count) of the last stage;
+        energies holds every stage's per-template energies in order."""
+        fr = _f64(frames)
+        F = fr.shape[0]
+        fr = fr.reshape(F, -1)
+        N = n_of(params.precision_level) ** 2
+        m = F if series.num_extra_stages > 0 else F - 1
+        phis = np.zeros((m, 2, N))
+        energies = np.zeros((F - 1) + series.num_extra_stages * F)
+        avg, med, cnt = np.zeros(N), np.zeros(N), np.zeros(N)
+        self._check(lib().msgpu_match_series(self._h, ctypes.byref(params), ctypes.byref(series), _p(fr), F,
+                                             _p(phis), _p(energies), _p(avg), _p(med), _p(cnt)))
+        return phis, energies, avg, med, cnt
+
+    def match_series_device(self, params: Params, series: SeriesParams, d_frames: int, num_frames: int,
+                            d_phis: int, d_energies: int = 0, d_avg: int = 0, d_median: int = 0, d_count: int = 0,
+                            stream: int = 0):
+        self._check(lib().msgpu_match_series_device(self._h, ctypes.byref(params), ctypes.byref(series), d_frames,
+                                                    num_frames, d_phis, d_energies or None, d_avg or None,
+                                                    d_median or None, d_count or None, stream or None))
+
+    def compose(self, level: int, d1, d2, init=None):
+        """ConcatAndSmoothlyExtendDeformations; init (default d2) is the solver's initial guess.
+        Returns (composition[2,N], pcg_iterations[2])."""
+        N = n_of(level) ** 2
+        a = _f64(d1).reshape(2, N)
+        b = _f64(d2).reshape(2, N)
+        out = (b if init is None else _f64(init).reshape(2, N)).copy()
+        it = np.zeros(2, dtype=np.int32)
+        self._check(lib().msgpu_compose(self._h, level, _p(a), _p(b), _p(out), it.ctypes.data_as(_ip)))
+        return out, it
+
+    def compose_device(self, level: int, d_d1: int, d_d2: int, d_inout: int, stream: int = 0):
+        self._check(lib().msgpu_compose_device(self._h, level, d_d1, d_d2, d_inout, stream or None))
+
+    def warp_median(self, level: int, frames, phis):
+        fr = _f64(frames)
+        F = fr.shape[0]
+        N = n_of(level) ** 2
+        ph = _f64(phis).reshape(F, 2, N)
+        med = np.zeros(N)
+        self._check(lib().msgpu_warp_median(self._h, level, _p(fr.reshape(F, N)), _p(ph), F, _p(med)))
+        return med
 
     def set_profiling(self, on: bool):
         self._check(lib().msgpu_set_profiling(self._h, int(bool(on))))

@@ -119,6 +119,19 @@ def make_series(n: int, num_frames: int, spec: LatticeSpec = HEX_513, seed: int 
     return frames, clean, disp
 
 
+def smooth_field(n: int, rng: np.random.Generator, amp_px: float, shift_px=(0.0, 0.0)) -> np.ndarray:
+    """A smooth displacement [x | y] in domain units (2 x n*n): a constant
+    shift plus two plane sinusoids per component, amplitudes in pixels."""
+    y, x = np.mgrid[0:n, 0:n] / (n - 1)
+    out = np.zeros((2, n * n))
+    for c in range(2):
+        f = shift_px[c] + sum(amp_px * rng.uniform(0.3, 1.0) *
+                              np.sin(2 * np.pi * (rng.uniform(0.5, 2) * x + rng.uniform(0.5, 2) * y) + rng.uniform(0, 6))
+                              for _ in range(2))
+        out[c] = (f / (n - 1)).ravel()
+    return out
+
+
 def psnr(a: np.ndarray, b: np.ndarray) -> float:
     """Peak signal-to-noise ratio of a against b, peak = range of b."""
     mse = float(np.mean((a - b) ** 2))

@@ -167,16 +167,19 @@ def register(max_level, start, stop, R, T, px=None, py=None, lam=0.1, lam_factor
     return px, py, e, list(steps)
 
 
-def compose(level, d1, d2, init=None):
+def compose(level, d1, d2, init=None, with_iterations=False):
     """ConcatAndSmoothlyExtendDeformations of displacements d1, d2 (2 x N each);
-    init: the solver's initial guess (default d2, as in series matching)."""
+    init: the solver's initial guess (default d2, as in series matching).
+    with_iterations: also return the PCG steps of both components together."""
     N = n_of(level) ** 2
     out = (_c(d2) if init is None else _c(init)).reshape(2, N).copy()
     d1 = _c(d1).reshape(2, N)
     d2 = _c(d2).reshape(2, N)
     ox, oy = out[0].copy(), out[1].copy()
-    lib().msor_compose(level, _p(d1[0].copy()), _p(d1[1].copy()), _p(d2[0].copy()), _p(d2[1].copy()), _p(ox), _p(oy))
-    return np.stack([ox, oy])
+    its = lib().msor_compose(level, _p(d1[0].copy()), _p(d1[1].copy()), _p(d2[0].copy()), _p(d2[1].copy()),
+                             _p(ox), _p(oy))
+    res = np.stack([ox, oy])
+    return (res, int(its)) if with_iterations else res
 
 
 def warp_median(level, frames, phis, fill):

@@ -143,19 +143,6 @@ def ncc_register(ref: msor.RefRunner, level: int, seed: int):
                         lam=0.1, max_iter=15, phi=np.stack([px, py]), E=np.array([e]))
 
 
-def smooth_field(n, rng, amp_px, shift_px=(0.0, 0.0)):
-    """A smooth displacement (domain units): a constant shift plus two
-    sinusoids per component, amplitudes in pixels."""
-    y, x = np.mgrid[0:n, 0:n] / (n - 1)
-    out = np.zeros((2, n * n))
-    for c in range(2):
-        f = shift_px[c] + sum(amp_px * rng.uniform(0.3, 1.0) *
-                              np.sin(2 * np.pi * (rng.uniform(0.5, 2) * x + rng.uniform(0.5, 2) * y) + rng.uniform(0, 6))
-                              for _ in range(2))
-        out[c] = (f / (n - 1)).ravel()
-    return out
-
-
 def compose(ref: msor.RefRunner, level: int, seed: int):
     """ConcatAndSmoothlyExtendDeformations with a shifted d2 (a band of
     nodes leaves the domain and is extended) and with a small d2 (no node
@@ -163,15 +150,15 @@ def compose(ref: msor.RefRunner, level: int, seed: int):
     median of warped frames for an odd and an even frame count."""
     n = n_of(level)
     rng = np.random.default_rng(seed)
-    d1 = smooth_field(n, rng, 1.5)
-    d2 = smooth_field(n, rng, 1.0, shift_px=(2.5, -1.5))
-    d2s = smooth_field(n, rng, 0.3)
+    d1 = syn.smooth_field(n, rng, 1.5)
+    d2 = syn.smooth_field(n, rng, 1.0, shift_px=(2.5, -1.5))
+    d2s = syn.smooth_field(n, rng, 0.3)
     out = ref.compose(level, d1, d2)
     out_in = ref.compose(level, d1, d2s)
     F = 5
     fr, _, _ = syn.make_series(n, F, syn.HEX_513, seed=seed)
     frames = fr.reshape(F, -1)
-    phis = np.stack([smooth_field(n, rng, 2.0, shift_px=(rng.uniform(-3, 3), rng.uniform(-3, 3))) for _ in range(F)])
+    phis = np.stack([syn.smooth_field(n, rng, 2.0, shift_px=(rng.uniform(-3, 3), rng.uniform(-3, 3))) for _ in range(F)])
     med5 = ref.median(level, frames, phis, 0.5)
     med4 = ref.median(level, frames[:4], phis[:4], 0.25)
     np.savez_compressed(os.path.join(OUT, f"compose_L{level}.npz"), level=level, d1=d1, d2=d2, out=out, d2_in=d2s,
@@ -192,6 +179,26 @@ def match_series(ref: msor.RefRunner, level: int, F: int, seed: int):
                         **{k: np.array(v) for k, v in kw.items()})
 
 
+def match_series_conditioned(ref: msor.RefRunner, level: int, F: int, seed: int):
+    """A configuration of the same loop on which the reference is well
+    conditioned: when every input pixel moves by one ulp, the displacements
+    move by spread_px at most (stored), so that an implementation whose sums
+    are reordered can be held to a tight tolerance."""
+    n = n_of(level)
+    fr, _, _ = syn.make_series(n, F, syn.SQUARE_257, seed=seed)
+    frames = fr.reshape(F, -1)
+    kw = dict(start=5, stop=level, max_iter=6, refine_start=6, extra_stages=1, extra_lam_factor=1.0, use_median=True)
+    phis, avg, med, cnt, energies, _ = ref.match_series(level, frames=frames, **kw)
+    spread = 0.0
+    for k in range(2):
+        sign = np.random.default_rng(k).choice([-1.0, 1.0], size=frames.shape)
+        q = ref.match_series(level, frames=np.nextafter(frames, frames + sign * np.inf), **kw)[0]
+        spread = max(spread, float(np.abs(q - phis).max() * (n - 1)))
+    np.savez_compressed(os.path.join(OUT, f"match_series_wc_L{level}.npz"), level=level, frames=frames, phis=phis,
+                        avg=avg, median=med, count=cnt, energies1=energies[0], energies2=energies[1],
+                        spread_px=spread, **{k: np.array(v) for k, v in kw.items()})
+
+
 def main():
     if not msor.have_ref():
         raise SystemExit("oracle/_ref/ms_ref is missing: make -f oracle/Makefile.ref")
@@ -199,6 +206,7 @@ def main():
     if "--series-only" in sys.argv:
         compose(ref, 6, 601)
         match_series(ref, 6, 4, 602)
+        match_series_conditioned(ref, 6, 4, 623)
         return
     if "--ncc-only" in sys.argv:
         ncc(ref, 5, 501, 20)
@@ -216,6 +224,7 @@ def main():
     ncc_register(ref, 7, 503)
     compose(ref, 6, 601)
     match_series(ref, 6, 4, 602)
+    match_series_conditioned(ref, 6, 4, 623)
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(OUT, f)))

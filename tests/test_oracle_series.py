@@ -51,3 +51,14 @@ def test_match_series_stages_bit_exact(oracle):
     assert np.array_equal(phis, g["phis"])
     assert np.array_equal(avg, g["avg"]) and np.array_equal(med, g["median"]) and np.array_equal(cnt, g["count"])
     assert np.array_equal(energies[0], g["energies1"]) and np.array_equal(energies[1], g["energies2"])
+
+
+def test_match_series_conditioned_fixture_bit_exact(oracle):
+    g = golden("match_series_wc_L6.npz")
+    kw = dict(start=int(g["start"]), stop=int(g["stop"]), max_iter=int(g["max_iter"]),
+              refine_start=int(g["refine_start"]), extra_stages=int(g["extra_stages"]),
+              extra_lam_factor=float(g["extra_lam_factor"]), use_median=bool(g["use_median"]))
+    phis, avg, med, cnt, energies = oracle.match_series(6, frames=g["frames"], **kw)
+    assert np.array_equal(phis, g["phis"]) and np.array_equal(med, g["median"])
+    assert np.array_equal(energies[1], g["energies2"])
+    assert float(g["spread_px"]) < 1e-7
