@@ -1166,13 +1166,17 @@ __device__ __forceinline__ int pass_tiles(int kind, int k, int level, int n) {
 }
 
 // Tiles per dispensed chunk: large enough that taking a chunk (a few L2
-// round trips) is small against its work, small enough that a pass still
-// spreads over many CTAs.  A function of the pass alone, so the chunk
-// partition -- and with it every reduction order -- does not depend on the
-// schedule.
-__device__ __forceinline__ int chunk_tiles(int ntiles) {
-  const int c = ntiles / 24;
-  return c < 1 ? 1 : (c > 16 ? 16 : c);
+// round trips) is small against its work -- about a 24th of the pass, at
+// most 16 tiles -- but no larger than the pass's tiles times the instances
+// still running spread over the grid, so that the pass of a lone instance
+// still spreads over every CTA.  Every tile stores its own partial sums and
+// a pass adds them in tile order, so the chunking never changes a result.
+__device__ __forceinline__ int chunk_tiles(int ntiles, int active) {
+  int c = ntiles / 24;
+  c = c < 1 ? 1 : (c > 16 ? 16 : c);
+  const long long work = (long long)ntiles * (active < 1 ? 1 : active);
+  const int spread = (int)((work + gridDim.x - 1) / gridDim.x);
+  return spread < c ? (spread < 1 ? 1 : spread) : c;
 }
 
 // Tiles of one pass: issue(t, stage) starts the window copies, compute(t,
@@ -1652,7 +1656,7 @@ __device__ void publish(const LevelArgs<Real>& a, const SchedPtrs<Real>& sp, int
     return;
   }
   c.desc.ntiles = pass_tiles(c.desc.kind, c.desc.k, a.level, a.n);
-  c.desc.chunk = chunk_tiles(c.desc.ntiles);
+  c.desc.chunk = chunk_tiles(c.desc.ntiles, a.num_inst - *(volatile int*)sp.finished);
   const int nchunks = (c.desc.ntiles + c.desc.chunk - 1) / c.desc.chunk;
   c.done = 0;
   ctl_store(sp.ctl + inst, c);
@@ -1818,17 +1822,19 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
       cp_async_wait<1>();
       __syncthreads();
       run.compute(t.inst, t.desc, tile, stage, part);
-      __syncthreads();
+      // the tile's partial sums, reduced in a fixed order and stored per tile
+      block_sum(part, wbuf, tot);
+      if (threadIdx.x == 0) {
+        double* pp = sp.partials + ((size_t)t.inst * sp.max_tiles + tile) * kRedSlots;
+#pragma unroll
+        for (int k = 0; k < kRedSlots; ++k) __stcg(pp + k, tot[k]);
+      }
+#pragma unroll
+      for (int k = 0; k < kRedSlots; ++k) part[k] = 0.0;
       stage ^= 1;
     }
-    block_sum(part, wbuf, tot);
     pt.stop(task_pass_kind(t.desc.kind));
     pt.start();
-    if (threadIdx.x == 0) {
-      double* pp = sp.partials + ((size_t)t.inst * sp.max_tiles + t.chunk) * kRedSlots;
-#pragma unroll
-      for (int k = 0; k < kRedSlots; ++k) __stcg(pp + k, tot[k]);
-    }
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1838,10 +1844,10 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
     }
     __syncthreads();
     if (flag_last) {
-      // this CTA completed the pass: totals in chunk order, then the control step
+      // this CTA completed the pass: totals in tile order, then the control step
       double acc[kRedSlots] = {0.0, 0.0, 0.0, 0.0};
       const double* pp = sp.partials + (size_t)t.inst * sp.max_tiles * kRedSlots;
-      for (int i = threadIdx.x; i < t.nchunks; i += kThreads) {
+      for (int i = threadIdx.x; i < t.desc.ntiles; i += kThreads) {
 #pragma unroll
         for (int k = 0; k < kRedSlots; ++k) acc[k] += __ldcg(pp + (size_t)i * kRedSlots + k);
       }
