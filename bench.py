@@ -16,6 +16,13 @@ stage (all 20 registrations + the average).  Seeded synthetic data.
 quocmesh templates built from the reference sources) on a bounded sample of
 the same workload, one process per host core.
 
+--series times the whole of matchSeries' first stage instead
+(msgpu_match_series, accumulated deformations): the 20 templates are
+registered to their predecessors in one batch, then composed and refined
+against frame 0 one after the other, then averaged.  Its CPU baseline is the
+reference's own stage loop on the first 3 templates (a sequential chain, one
+core).
+
 Multi-GPU (torchrun): weak scaling; every rank registers its own series.
 """
 from __future__ import annotations
@@ -273,6 +280,150 @@ def profile_case(level: int, iters: int, fp64: bool):
                       "stats": ctx.stats()}))
 
 
+SERIES_SAMPLE = 3   # templates of the chain the CPU reference runs in --series
+
+
+def reference_series_sample(frames, workdir: str):
+    """The reference's stage loop on frames[0..SERIES_SAMPLE] (one process);
+    returns (seconds of the registration phase, phis, energies)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import msor
+    r = msor.RefRunner()
+    phis, _, _, _, energies, timing = r.match_series(LEVEL, START, LEVEL, frames[:SERIES_SAMPLE + 1], lam=LAMBDA,
+                                                     max_iter=MAX_ITER, refine_start=START, ncc=bool(DATA_TERM))
+    return timing[1]["registration_seconds"], phis, energies[0]
+
+
+def main_series(args, world, rank, local):
+    """--series: msgpu_match_series (stage 1 with accumulated deformations)."""
+    import numpy as np
+    import torch
+    import msgpu
+    from msgpu import build as mbuild
+
+    torch.cuda.set_device(local)
+    mbuild.build()
+    fp64 = not args.fp32
+    p = params(fp64)
+    sp = msgpu.default_series_params(p)
+    ref, tmpl, _ = workload(rank)
+    frames = np.concatenate([ref[None], tmpl])            # frame 0 is the stage's reference
+    F = frames.shape[0]
+    m = F - 1
+    n = (1 << LEVEL) + 1
+    N = n * n
+    ctx = msgpu.Context(local)
+    dev = torch.device("cuda", local)
+    d_frames = torch.from_numpy(frames).to(dev)
+    d_phis = torch.empty((m, 2, N), dtype=torch.float64, device=dev)
+    d_e = torch.empty(m, dtype=torch.float64, device=dev)
+    d_avg = torch.empty(N, dtype=torch.float64, device=dev)
+    d_med = torch.empty(N, dtype=torch.float64, device=dev)
+    d_cnt = torch.empty(N, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        ctx.match_series_device(p, sp, d_frames.data_ptr(), F, d_phis.data_ptr(), d_e.data_ptr(), d_avg.data_ptr(),
+                                d_med.data_ptr(), d_cnt.data_ptr(), stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    start_ev = torch.cuda.Event(enable_timing=True)
+    stop_ev = torch.cuda.Event(enable_timing=True)
+    launches = 0
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clocks:
+        start_ev.record(stream)
+        for _ in range(args.steps):
+            step()
+            launches += ctx.stats()["kernel_launches"]
+        stop_ev.record(stream)
+        torch.cuda.synchronize(dev)
+    barrier(world)
+    elapsed_ms = allreduce_max(start_ev.elapsed_time(stop_ev), world)
+    value = world * m * args.steps / (elapsed_ms / 1000.0)
+    phis = d_phis.cpu().numpy()
+    energies = d_e.cpu().numpy()
+    # one profiled call: per-level launch times of its last solve (a single-frame refinement)
+    ctx.set_profiling(True)
+    step()
+    torch.cuda.synchronize(dev)
+    st = ctx.stats()
+    ctx.set_profiling(False)
+    # end to end through the host entry point, pinned host buffers
+    h_frames = torch.from_numpy(frames).pin_memory().numpy()
+    ctx.match_series(p, sp, h_frames)
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ctx.match_series(p, sp, h_frames)
+    e2e_s = allreduce_max(time.perf_counter() - t0, world)
+    e2e_value = world * m * args.steps / e2e_s
+    h2d = F * N * 8
+    d2h = (2 * m * N + 3 * N + m) * 8
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        real_bytes = 8 if fp64 else 4
+        lv = LEVEL - st["first_level"]
+        lvl_ms = st["level_ms"][lv]
+        alg = algorithmic_bytes(st["level_steps"][lv], st["level_evals"][lv], real_bytes)
+        achieved = alg / (lvl_ms / 1000.0) / 1e9
+        clk = clocks.summary()
+        cpu = accuracy = None
+        if world == 1 and not args.no_cpu_baseline:
+            with tempfile.TemporaryDirectory() as wd:
+                secs, rphis, ren = reference_series_sample(frames, wd)
+            cpu = {"value": SERIES_SAMPLE / secs, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"the reference's stage loop on frames 0..{SERIES_SAMPLE} (the first {SERIES_SAMPLE} "
+                             f"templates of the chain, 513x513, levels {START}-{LEVEL}), registration phase "
+                             f"{secs:.1f} s; the chain is sequential, one core"}
+            fp = frames.copy()
+            up = np.random.default_rng(7).random(fp.shape) < 0.5
+            fp = np.where(up, np.nextafter(fp, np.inf), np.nextafter(fp, -np.inf))
+            with tempfile.TemporaryDirectory() as wd:
+                _, pphis, pen = reference_series_sample(fp, wd)
+            k = SERIES_SAMPLE
+            accuracy = {"templates_checked": k,
+                        "max_dphi_px": float(np.abs(phis[:k] - rphis).max()) * (n - 1),
+                        "max_rel_energy": float(np.max(np.abs(energies[:k] - ren) / np.abs(ren))),
+                        "tolerance": {"dphi_px": 1e-3, "rel_energy": 1e-6},
+                        "reference_1ulp_spread": {"max_dphi_px": float(np.abs(pphis - rphis).max()) * (n - 1),
+                                                  "max_rel_energy": float(np.max(np.abs(pen - ren) / np.abs(ren))),
+                                                  "perturbation": "every pixel of every frame +-1 ulp"}}
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if fp64 else "f32+f64-reductions",
+            "data": "synthetic",
+            "config": {"workload": f"matchSeries stage 1 with accumulated deformations: {m} hex-lattice templates "
+                                   f"513x513 (level {LEVEL}) and frame 0, pairwise batch, composition and "
+                                   f"refinement (levels {START}-{LEVEL}) per template, average and median; "
+                                   f"maxGDIterations {MAX_ITER}, lambda {LAMBDA}, "
+                                   f"{'NCC' if DATA_TERM else 'SSD'} data term",
+                       "data_term": "ncc" if DATA_TERM else "ssd", "templates_per_gpu": m, "level": LEVEL,
+                       "l2": "no flush: per-step working set exceeds the 126 MB L2",
+                       "parallelism": f"weak, {world} independent series"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": f"level_kernel<{'double' if fp64 else 'float'}> level {LEVEL}, "
+                                                   f"single-frame refinement",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_launch": alg,
+                         "avg_launch_ms": lvl_ms},
+            "cpu_baseline": cpu,
+            "accuracy": accuracy,
+            "clocks": {k2: clk[k2] for k2 in ("sm_mhz", "sm_max_mhz", "reasons")},
+        }
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -287,6 +438,8 @@ def main():
                     help="small case for ncu captures: one level solve of FRAMES frames at this level, "
                          "--profile-iters gradient steps, no timing")
     ap.add_argument("--profile-iters", type=int, default=5)
+    ap.add_argument("--series", action="store_true",
+                    help="time matchSeries' whole first stage with accumulated deformations (msgpu_match_series)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     global DATA_TERM
@@ -296,6 +449,8 @@ def main():
     world, rank, local = dist_setup()
     if args.impl == "reference":
         return run_reference_arm(args, world, rank)
+    if args.series:
+        return main_series(args, world, rank, local)
 
     import numpy as np
     import torch
