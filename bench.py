@@ -283,6 +283,33 @@ def profile_case(level: int, iters: int, fp64: bool):
 SERIES_SAMPLE = 3   # templates of the chain the CPU reference runs in --series
 
 
+def profile_series(compose_level: int, fp64: bool):
+    """Small cases for ncu: with compose_level > 0 one composition at that
+    level (smooth displacements of 3 px and 2 px, the second shifted so that a
+    band of nodes leaves the domain); otherwise one msgpu_match_series call on
+    the bench's frames (no timing)."""
+    import numpy as np
+    import msgpu
+    from msgpu import build as mbuild
+    from msgpu import synthetic as syn
+    mbuild.build()
+    ctx = msgpu.Context(0)
+    if compose_level:
+        n = (1 << compose_level) + 1
+        rng = np.random.default_rng(compose_level)
+        d1 = syn.smooth_field(n, rng, 3.0)
+        d2 = syn.smooth_field(n, rng, 2.0, shift_px=(-3.0, 2.0))
+        _, it = ctx.compose(compose_level, d1, d2)
+        print(json.dumps({"profile_compose_level": compose_level, "pcg_iterations": it.tolist()}))
+        return 0
+    p = params(fp64)
+    ref, tmpl, _ = workload(0)
+    frames = np.concatenate([ref[None], tmpl])
+    ctx.match_series(p, msgpu.default_series_params(p), frames)
+    print(json.dumps({"profile_series_frames": int(frames.shape[0]), "launches": ctx.stats()["kernel_launches"]}))
+    return 0
+
+
 def reference_series_sample(frames, workdir: str):
     """The reference's stage loop on frames[0..SERIES_SAMPLE] (one process);
     returns (seconds of the registration phase, phis, energies)."""
@@ -438,6 +465,10 @@ def main():
                     help="small case for ncu captures: one level solve of FRAMES frames at this level, "
                          "--profile-iters gradient steps, no timing")
     ap.add_argument("--profile-iters", type=int, default=5)
+    ap.add_argument("--profile-compose", type=int, default=0,
+                    help="small case for ncu: one displacement composition at this level, no timing")
+    ap.add_argument("--profile-series", action="store_true",
+                    help="small case for ncu: one msgpu_match_series call on the bench's frames, no timing")
     ap.add_argument("--series", action="store_true",
                     help="time matchSeries' whole first stage with accumulated deformations (msgpu_match_series)")
     args = ap.parse_args()
@@ -446,6 +477,8 @@ def main():
     DATA_TERM = 1 if args.ncc else 0
     if args.profile_level:
         return profile_case(args.profile_level, args.profile_iters, not args.fp32)
+    if args.profile_compose or args.profile_series:
+        return profile_series(args.profile_compose, not args.fp32)
     world, rank, local = dist_setup()
     if args.impl == "reference":
         return run_reference_arm(args, world, rank)
