@@ -170,6 +170,37 @@ int msgpu_warp_median(msgpu_context* ctx, int level, const double* frames, const
 int msgpu_warp_median_device(msgpu_context* ctx, int level, const double* d_frames, const double* d_phis,
                              int num_frames, double* d_median_out, void* stream);
 
+/* --- on-disk arrays (host only, no context) --------------------------------
+ * The reference's 2-D array files (qc::ScalarArray<QC_2D>::save / load,
+ * scalarArray.cpp:330-420, 481-569; header auxiliary.h:10-45): magic P2, P5,
+ * P7, P8, P9, Pa, Pb, '#' comments, "numX numY", "max", raw values x fastest;
+ * compressed by file-name suffix like aol::Bzipifstream (.bz2, .q2bz, .q3bz
+ * bzip2; .gz, .svgz, .zz zlib/gzip).  Values are returned as doubles.
+ * Errors: status code plus msgpu_io_last_error() (per host thread).          */
+const char* msgpu_io_last_error(void);
+/* out == NULL: only *nx, *ny are returned.  capacity: doubles at out.       */
+int msgpu_read_array(const char* path, double* out, long long capacity, int* nx, int* ny);
+/* type 9 (double binary, the reference's PGM_DOUBLE_BINARY) or 8 (float).  */
+int msgpu_write_array(const char* path, const double* data, int nx, int ny, int type);
+/* count files of nx x ny values each into out (count*nx*ny doubles), decoded
+ * by `threads` host threads (< 1: one per hardware thread); every file must
+ * have the given size (the frames of a series).                            */
+int msgpu_read_arrays(const char* const* paths, int count, int nx, int ny, double* out, int threads);
+/* The same in the background: returns at once with a task (NULL on invalid
+ * arguments), whose msgpu_io_wait returns the status and frees it; out must
+ * stay valid until then.  Lets the decoding of the next series overlap the
+ * GPU work on the current one (no counterpart in the reference, which loads
+ * each frame when its registration starts, matchSeries.h:141).            */
+typedef struct msgpu_io_task msgpu_io_task;
+msgpu_io_task* msgpu_read_arrays_start(const char* const* paths, int count, int nx, int ny, double* out,
+                                       int threads);
+int msgpu_io_wait(msgpu_io_task* task);
+/* A displacement as one file per component, named by a printf mask with one
+ * %d (qc::MultiArray::load / save, multiArray.h:272-306, e.g. the
+ * reference's "deformation_09_%d.dat.bz2"); phi: [x | y], 2*nx*ny doubles. */
+int msgpu_read_displacement(const char* mask, int nx, int ny, double* phi);
+int msgpu_write_displacement(const char* mask, const double* phi, int nx, int ny);
+
 /* Per-call statistics (no counterpart in the reference; used for the roofline).
  * With profiling on, every batch call records CUDA events around each level
  * launch on its stream and waits for them at the end of the call.          */

@@ -77,6 +77,8 @@ EXPORTS = [
     "msgpu_match_series_stage", "msgpu_match_series_stage_device", "msgpu_set_profiling", "msgpu_get_stats",
     "msgpu_set_data_term", "msgpu_series_params_default", "msgpu_match_series", "msgpu_match_series_device",
     "msgpu_compose", "msgpu_compose_device", "msgpu_warp_median", "msgpu_warp_median_device",
+    "msgpu_io_last_error", "msgpu_read_array", "msgpu_write_array", "msgpu_read_arrays", "msgpu_read_displacement",
+    "msgpu_write_displacement", "msgpu_read_arrays_start", "msgpu_io_wait",
 ]
 
 
@@ -132,6 +134,18 @@ def lib():
         L.msgpu_warp_median.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_int, _dp]
         L.msgpu_warp_median_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                                ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        L.msgpu_io_last_error.restype = ctypes.c_char_p
+        L.msgpu_io_last_error.argtypes = []
+        L.msgpu_read_array.argtypes = [ctypes.c_char_p, _dp, ctypes.c_longlong, _ip, _ip]
+        L.msgpu_write_array.argtypes = [ctypes.c_char_p, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.msgpu_read_arrays.argtypes = [ctypes.POINTER(ctypes.c_char_p), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        _dp, ctypes.c_int]
+        L.msgpu_read_displacement.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _dp]
+        L.msgpu_write_displacement.argtypes = [ctypes.c_char_p, _dp, ctypes.c_int, ctypes.c_int]
+        L.msgpu_read_arrays_start.argtypes = [ctypes.POINTER(ctypes.c_char_p), ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, _dp, ctypes.c_int]
+        L.msgpu_read_arrays_start.restype = ctypes.c_void_p
+        L.msgpu_io_wait.argtypes = [ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -142,6 +156,63 @@ def default_params(**kw) -> Params:
     for k, v in kw.items():
         setattr(p, "lambda_" if k == "lambda" else k, v)
     return p
+
+
+# --- on-disk arrays (host only) ------------------------------------------------
+def _io_check(st: int):
+    if st != MSGPU_OK:
+        raise MsgpuError(st, lib().msgpu_io_last_error().decode())
+
+
+def read_array(path: str) -> np.ndarray:
+    """A 2-D array file of the reference's formats as a (numY, numX) float64 array."""
+    nx, ny = ctypes.c_int(), ctypes.c_int()
+    _io_check(lib().msgpu_read_array(path.encode(), None, 0, ctypes.byref(nx), ctypes.byref(ny)))
+    out = np.zeros(nx.value * ny.value)
+    _io_check(lib().msgpu_read_array(path.encode(), _p(out), out.size, ctypes.byref(nx), ctypes.byref(ny)))
+    return out.reshape(ny.value, nx.value)
+
+
+def write_array(path: str, a, type_: int = 9):
+    a = _f64(a)
+    ny, nx = a.shape
+    _io_check(lib().msgpu_write_array(path.encode(), _p(a), nx, ny, type_))
+
+
+def read_arrays(paths, nx: int, ny: int, threads: int = 0) -> np.ndarray:
+    """Frames of one size from many files, decoded by host threads; (count, ny, nx)."""
+    out = np.zeros((len(paths), ny, nx))
+    arr = (ctypes.c_char_p * len(paths))(*[p.encode() for p in paths])
+    _io_check(lib().msgpu_read_arrays(arr, len(paths), nx, ny, _p(out), threads))
+    return out
+
+
+class ReadTask:
+    """Background decoding of frames into `out` (see msgpu_read_arrays_start)."""
+
+    def __init__(self, paths, nx: int, ny: int, out: np.ndarray, threads: int = 0):
+        assert out.dtype == np.float64 and out.flags.c_contiguous and out.size >= len(paths) * nx * ny
+        self._out = out
+        arr = (ctypes.c_char_p * len(paths))(*[p.encode() for p in paths])
+        self._h = lib().msgpu_read_arrays_start(arr, len(paths), nx, ny, _p(out), threads)
+        if not self._h:
+            _io_check(MSGPU_ERR_INVALID_ARG)
+
+    def wait(self) -> np.ndarray:
+        h, self._h = self._h, None
+        if h:
+            _io_check(lib().msgpu_io_wait(h))
+        return self._out
+
+
+def read_displacement(mask: str, n: int) -> np.ndarray:
+    out = np.zeros((2, n * n))
+    _io_check(lib().msgpu_read_displacement(mask.encode(), n, n, _p(out)))
+    return out
+
+
+def write_displacement(mask: str, phi, n: int):
+    _io_check(lib().msgpu_write_displacement(mask.encode(), _p(_f64(phi).reshape(2, n * n)), n, n))
 
 
 def default_series_params(params: Params, **kw) -> SeriesParams:

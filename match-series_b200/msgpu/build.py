@@ -8,7 +8,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 CSRC = os.path.join(PKG, "csrc")
 OUT = os.path.join(HERE, "libmsgpu.so")
-SOURCES = [os.path.join(CSRC, "msgpu.cu")]
+SOURCES = [os.path.join(CSRC, "msgpu.cu"), os.path.join(CSRC, "msgpu_io.cpp")]
 DEPS = SOURCES + [os.path.join(CSRC, f) for f in ("msgpu_level.cuh", "msgpu_fe.cuh", "msgpu_series.cuh")] + [
     os.path.join(os.path.dirname(PKG), "include", "msgpu.h")]
 
@@ -16,6 +16,9 @@ DEPS = SOURCES + [os.path.join(CSRC, f) for f in ("msgpu_level.cuh", "msgpu_fe.c
 # rounds like the reference build (which has no FMA contraction).
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
               "-Xcompiler", "-fPIC", "-shared"]
+# bzip2 (the image has the shared library without its development symlink)
+# and zlib for the compressed array files of msgpu_io.cpp
+LIBS = ["-l:libbz2.so.1.0", "-lz"]
 
 
 def nvcc() -> str:
@@ -33,7 +36,7 @@ def up_to_date() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return OUT
-    cmd = [nvcc(), *NVCC_FLAGS, "-o", OUT, *SOURCES]
+    cmd = [nvcc(), *NVCC_FLAGS, "-o", OUT, *SOURCES, *LIBS]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -288,6 +288,23 @@ class RefRunner:
                  os.path.join(self.dir, "out"))
         return self._r("out")
 
+    def save_array(self, a, path, type_):
+        """qc::ScalarArray<QC_2D>::save of a (numY, numX) array to path."""
+        ny, nx = a.shape
+        self.run("save", nx, ny, self._w("arr", a), path, type_)
+
+    def load_array(self, path):
+        self.run("load", path, os.path.join(self.dir, "arr_out"), os.path.join(self.dir, "dims"))
+        nx, ny = map(int, open(os.path.join(self.dir, "dims")).read().split())
+        return self._r("arr_out").reshape(ny, nx)
+
+    def save_displacement(self, level, phi, mask):
+        self.run("savedef", level, self._w("def", phi), mask)
+
+    def load_displacement(self, level, mask):
+        self.run("loaddef", level, mask, os.path.join(self.dir, "def_out"))
+        return self._r("def_out").reshape(2, -1)
+
     def normalize(self, level, img, sat=0.15, min_to_zero=1):
         self.run("normalize", level, self._w("img", img), repr(float(sat)), min_to_zero,
                  os.path.join(self.dir, "out"))

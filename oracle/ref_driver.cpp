@@ -359,6 +359,7 @@ static int usage ( ) {
     "ms_ref register[_ncc] maxL start stop R T px py lambda lambdaFactor maxIter stopEps resample outPhi outTxt\n"
     "ms_ref normalize L in sat minToZero out\n"
     "ms_ref compose L d1 d2 inout | median L F frames phis fill out\n"
+    "ms_ref save nx ny in out type | load file out dims | savedef L in mask | loaddef L mask out\n"
     "ms_ref series[_ncc] maxL start stop lambda lambdaFactor maxIter stopEps sat minToZero F framesBin outPhis outMean outTxt\n"
     "ms_ref matchseries[_ncc] maxL start stop lambda lambdaFactor maxIter stopEps sat minToZero refineStart refineStop\n"
     "       extraStages extraLambdaFactor useMedian F framesBin outPrefix\n" );
@@ -468,6 +469,40 @@ int main ( int argc, char **argv ) {
     if ( ( cmd == "matchseries" || cmd == "matchseries_ncc" ) && argc == 19 ) {
       if ( cmd == "matchseries" ) matchSeriesCommand<RegisType> ( argv );
       else matchSeriesCommand<RegisTypeNCC> ( argv );
+      return 0;
+    }
+    if ( cmd == "save" && argc == 7 ) {
+      // ms_ref save nx ny in out type: qc::ScalarArray<QC_2D>::save (file format and compression by suffix)
+      const int nx = atoi ( argv[2] ), ny = atoi ( argv[3] );
+      ArrayType a ( nx, ny );
+      readBin ( argv[4], a.getData ( ), ( size_t ) nx * ny );
+      a.save ( argv[5], static_cast<qc::SaveType> ( atoi ( argv[6] ) ) );
+      return 0;
+    }
+    if ( cmd == "load" && argc == 5 ) {
+      // ms_ref load file out dims: qc::ScalarArray<QC_2D> load, values as doubles, "numX numY" in dims
+      ArrayType a ( argv[2] );
+      writeBin ( argv[3], a.getData ( ), a.size ( ) );
+      FILE *f = fopen ( argv[4], "w" );
+      fprintf ( f, "%d %d\n", a.getNumX ( ), a.getNumY ( ) );
+      fclose ( f );
+      return 0;
+    }
+    if ( ( cmd == "savedef" || cmd == "loaddef" ) && argc == 5 ) {
+      // ms_ref savedef L in mask | loaddef L mask out: qc::MultiArray save / load, one file per component
+      const int L = atoi ( argv[2] ), N = lvlN ( L ) * lvlN ( L );
+      qc::GridDefinition grid ( L, qc::QC_2D );
+      qc::MultiArray<RealType, qc::QC_2D> phi ( grid );
+      std::vector<RealType> buf ( 2 * N );
+      if ( cmd == "savedef" ) {
+        readBin ( argv[3], &buf[0], 2 * N );
+        memcpy ( phi[0].getData ( ), &buf[0], N * sizeof ( RealType ) ); memcpy ( phi[1].getData ( ), &buf[N], N * sizeof ( RealType ) );
+        phi.save ( argv[4], qc::PGM_DOUBLE_BINARY );
+      } else {
+        phi.load ( argv[3] );
+        memcpy ( &buf[0], phi[0].getData ( ), N * sizeof ( RealType ) ); memcpy ( &buf[N], phi[1].getData ( ), N * sizeof ( RealType ) );
+        writeBin ( argv[4], &buf[0], 2 * N );
+      }
       return 0;
     }
     if ( cmd == "compose" && argc == 7 ) {

@@ -9,7 +9,8 @@ CPU oracle and the CUDA path.  Run from the repository root:
     make -f oracle/Makefile.ref && python tests/golden/make_golden.py
 
 (--ncc-only regenerates only the fixtures of the cross-correlation data term,
---series-only those of the series pipeline: composition, median, stages.)
+--series-only those of the series pipeline: composition, median, stages;
+--io-only the array files written by the reference's savers.)
 """
 from __future__ import annotations
 
@@ -199,10 +200,37 @@ def match_series_conditioned(ref: msor.RefRunner, level: int, F: int, seed: int)
                         spread_px=spread, **{k: np.array(v) for k, v in kw.items()})
 
 
+IO_FILES = (("ref_p9.q2bz", 9), ("ref_p8.dat.bz2", 8), ("ref_p5.pgm", 5), ("ref_pa.pgm", 10), ("ref_p2.pgm", 2),
+            ("ref_p7.txt", 7), ("ref_p9.pgm", 9))
+
+
+def io_files(ref: msor.RefRunner, seed: int):
+    """Array files written by the reference's own savers (one per format and
+    compression) and what the reference's loader reads back from each; and a
+    displacement saved as the reference's per-component files."""
+    d = os.path.join(OUT, "io")
+    os.makedirs(d, exist_ok=True)
+    rng = np.random.default_rng(seed)
+    a = rng.normal(0, 50, (17, 33)) + 100
+    expected = {"source": a}
+    for name, t in IO_FILES:
+        path = os.path.join(d, name)
+        ref.save_array(a, path, t)
+        expected[name] = ref.load_array(path)
+    n = n_of(4)
+    phi = rng.normal(0, 0.01, (2, n * n))
+    ref.save_displacement(4, phi, os.path.join(d, "ref_deformation_04_%d.dat.bz2"))
+    expected["deformation"] = phi
+    np.savez_compressed(os.path.join(OUT, "io_expected.npz"), **expected)
+
+
 def main():
     if not msor.have_ref():
         raise SystemExit("oracle/_ref/ms_ref is missing: make -f oracle/Makefile.ref")
     ref = msor.RefRunner()
+    if "--io-only" in sys.argv:
+        io_files(ref, 701)
+        return
     if "--series-only" in sys.argv:
         compose(ref, 6, 601)
         match_series(ref, 6, 4, 602)
@@ -225,6 +253,7 @@ def main():
     compose(ref, 6, 601)
     match_series(ref, 6, 4, 602)
     match_series_conditioned(ref, 6, 4, 623)
+    io_files(ref, 701)
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(OUT, f)))
