@@ -23,6 +23,12 @@ against frame 0 one after the other, then averaged.  Its CPU baseline is the
 reference's own stage loop on the first 3 templates (a sequential chain, one
 core).
 
+--files times series read from disk: FILE_SERIES series of 21 frames each,
+stored as the reference's bzip2-compressed double arrays (.q2bz), are decoded
+by host threads and registered stage by stage through the host entry point,
+the decoding of the next series overlapping the GPU work on the current one.
+Its CPU baseline is the reference's own loader on the same files.
+
 Multi-GPU (torchrun): weak scaling; every rank registers its own series.
 """
 from __future__ import annotations
@@ -451,6 +457,127 @@ def main_series(args, world, rank, local):
     return 0
 
 
+FILE_SERIES = 4
+
+
+def main_files(args, world, rank, local):
+    """--files: series decoded from .q2bz files, overlapped with the GPU stages."""
+    import numpy as np
+    import torch
+    import msgpu
+    from concurrent.futures import ThreadPoolExecutor
+    from msgpu import build as mbuild
+    from msgpu import synthetic as syn
+
+    torch.cuda.set_device(local)
+    mbuild.build()
+    fp64 = not args.fp32
+    p = params(fp64)
+    n = (1 << LEVEL) + 1
+    N = n * n
+    nlev = LEVEL - START + 1
+    threads = cpu_procs()
+    ctx = msgpu.Context(local)
+    with tempfile.TemporaryDirectory() as wd:
+        # --- the files (untimed): FILE_SERIES series, reference frame first
+        series = []
+        with ThreadPoolExecutor(threads) as pool:
+            for k in range(FILE_SERIES):
+                fr, _, _ = syn.make_series(n, FRAMES + 1, syn.HEX_513, seed=2000 + 1000 * rank + 17 * k)
+                paths = [os.path.join(wd, f"s{k}_f{i:02d}.q2bz") for i in range(FRAMES + 1)]
+                order = [FRAMES] + list(range(FRAMES))
+                list(pool.map(lambda a: msgpu.write_array(a[0], fr[a[1]]), zip(paths, order)))
+                series.append(paths)
+        file_bytes = sum(os.path.getsize(q) for q in series[0])
+        bufs = [torch.zeros((FRAMES + 1, N), dtype=torch.float64).pin_memory().numpy() for _ in range(2)]
+        outs = (torch.zeros((FRAMES, 2, N), dtype=torch.float64).pin_memory().numpy(),
+                torch.zeros(FRAMES, dtype=torch.float64).pin_memory().numpy(),
+                torch.zeros((FRAMES, nlev), dtype=torch.int32).pin_memory().numpy(),
+                torch.zeros(N, dtype=torch.float64).pin_memory().numpy(),
+                torch.zeros(N, dtype=torch.float64).pin_memory().numpy())
+
+        def stage(buf):
+            ctx.match_series_stage(p, buf[0], buf[1:], out=outs)
+            return ctx.stats()["kernel_launches"]
+
+        # warm-up: decoding and one stage
+        for _ in range(args.warmup):
+            msgpu.read_arrays(series[0], n, n, threads)
+        bufs[0][:] = msgpu.read_arrays(series[0], n, n, threads).reshape(FRAMES + 1, N)
+        stage(bufs[0])
+        # decoding alone
+        t0 = time.perf_counter()
+        for k in range(FILE_SERIES):
+            msgpu.ReadTask(series[k], n, n, bufs[k % 2], threads).wait()
+        t_dec = time.perf_counter() - t0
+        # decode then register, series after series
+        barrier(world)
+        t0 = time.perf_counter()
+        for k in range(FILE_SERIES):
+            msgpu.ReadTask(series[k], n, n, bufs[0], threads).wait()
+            stage(bufs[0])
+        t_seq = allreduce_max(time.perf_counter() - t0, world)
+        # decoding of series k+1 overlapping the stage of series k (the timed value)
+        launches = 0
+        barrier(world)
+        with ClockSampler(local) as clocks:
+            t0 = time.perf_counter()
+            task = msgpu.ReadTask(series[0], n, n, bufs[0], threads)
+            for k in range(FILE_SERIES):
+                task.wait()
+                task = msgpu.ReadTask(series[k + 1], n, n, bufs[(k + 1) % 2], threads) if k + 1 < FILE_SERIES else None
+                launches += stage(bufs[k % 2])
+            t_ovl = allreduce_max(time.perf_counter() - t0, world)
+        # the reference's own loader on 3 of the files, one after the other (one core)
+        cpu = None
+        if rank == 0 and not args.no_cpu_baseline:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import msor
+            if msor.have_ref():
+                r = msor.RefRunner()
+                t0 = time.perf_counter()
+                for q in series[0][:3]:
+                    r.load_array(q)
+                t_ref = (time.perf_counter() - t0) / 3
+                cpu = {"value": 1.0 / t_ref, "unit": "frames/s", "cores": 1, "kind": "reference",
+                       "sample": "the reference's loader (qc::ScalarArray<QC_2D>::load via aol::Bzipifstream) on 3 "
+                                 "of the .q2bz frames, one process each, process start included; decoding only"}
+    if rank == 0:
+        frames_total = world * FRAMES * FILE_SERIES
+        clk = clocks.summary()
+        out = {
+            "metric": METRIC, "value": frames_total / t_ovl, "unit": UNIT, "n_gpus": world, "steps": FILE_SERIES,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * t_ovl / FILE_SERIES, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if fp64 else "f32+f64-reductions",
+            "data": "synthetic, stored as .q2bz files",
+            "config": {"workload": f"{FILE_SERIES} series of {FRAMES} hex-lattice templates 513x513 and a reference "
+                                   f"frame, each frame a bzip2-compressed double array file (.q2bz, "
+                                   f"{file_bytes / (FRAMES + 1) / 1e6:.2f} MB); per series: decode on {threads} "
+                                   f"host threads, then msgpu_match_series_stage (levels {START}-{LEVEL}, "
+                                   f"maxGDIterations {MAX_ITER}); a step is one series",
+                       "decode_threads": threads,
+                       "parallelism": f"weak, {world} ranks"},
+            "e2e": {"value": frames_total / t_ovl, "unit": UNIT,
+                    "h2d_bytes_per_step": (FRAMES + 1) * N * 8,
+                    "d2h_bytes_per_step": (2 * FRAMES * N + 2 * N + FRAMES) * 8 + FRAMES * nlev * 4},
+            "gpu_launches": launches,
+            "files": {"overlapped_frames_per_s": frames_total / t_ovl,
+                      "sequential_frames_per_s": frames_total / t_seq,
+                      "decode_only_frames_per_s": FRAMES * FILE_SERIES / t_dec,
+                      "decode_MB_per_s": (FILE_SERIES * (FRAMES + 1) * N * 8 / 1e6) / t_dec,
+                      "compressed_MB_per_series": file_bytes / 1e6},
+            "roofline": None,
+            "cpu_baseline": cpu,
+            "clocks": {k2: clk[k2] for k2 in ("sm_mhz", "sm_max_mhz", "reasons")},
+        }
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -469,6 +596,8 @@ def main():
                     help="small case for ncu: one displacement composition at this level, no timing")
     ap.add_argument("--profile-series", action="store_true",
                     help="small case for ncu: one msgpu_match_series call on the bench's frames, no timing")
+    ap.add_argument("--files", action="store_true",
+                    help="series read from .q2bz files, decoding overlapped with the GPU stages")
     ap.add_argument("--series", action="store_true",
                     help="time matchSeries' whole first stage with accumulated deformations (msgpu_match_series)")
     args = ap.parse_args()
@@ -484,6 +613,8 @@ def main():
         return run_reference_arm(args, world, rank)
     if args.series:
         return main_series(args, world, rank, local)
+    if args.files:
+        return main_files(args, world, rank, local)
 
     import numpy as np
     import torch
