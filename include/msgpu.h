@@ -175,7 +175,9 @@ int msgpu_warp_median_device(msgpu_context* ctx, int level, const double* d_fram
  * scalarArray.cpp:330-420, 481-569; header auxiliary.h:10-45): magic P2, P5,
  * P7, P8, P9, Pa, Pb, '#' comments, "numX numY", "max", raw values x fastest;
  * compressed by file-name suffix like aol::Bzipifstream (.bz2, .q2bz, .q3bz
- * bzip2; .gz, .svgz, .zz zlib/gzip).  Values are returned as doubles.
+ * bzip2; .gz, .svgz, .zz zlib/gzip); and ".dm3" / ".dm4" Gatan
+ * DigitalMicrograph images (qc::DM3Reader, dm3Import.h: the last image of the
+ * ImageList).  Values are returned as doubles.
  * Errors: status code plus msgpu_io_last_error() (per host thread).          */
 const char* msgpu_io_last_error(void);
 /* out == NULL: only *nx, *ny are returned.  capacity: doubles at out.       */

@@ -15,6 +15,8 @@
 //   ".q2bz", ".q3bz" are one bzip2 stream, ".gz", ".svgz", ".zz" zlib or gzip.
 //   A displacement is one such file per component, the name made from a
 //   printf mask with one %d (qc::MultiArray::save / load, multiArray.h:272-306).
+//   ".dm3" / ".dm4": Gatan DigitalMicrograph images (loadDM3,
+//   scalarArray.cpp:727-730, qc::DM3Reader).
 // Decoding runs on a pool of host threads, one file per thread at a time.
 #include <zlib.h>
 
@@ -280,12 +282,234 @@ int decode(const std::vector<char>& b, const Header& h, double* out, const std::
   }
 }
 
+// --- Gatan DigitalMicrograph 3 and 4 -------------------------------------
+// The tag tree of DM3Reader (dm3Import.h:16-438): big-endian header
+// (version 3 or 4, length, byte order 1 = little-endian values), then tag
+// directories (identifier 20) and tags (21): a big-endian name length and
+// name (version 4: a 64-bit size follows), tags "%%%%", an info count and the
+// info words (32-bit in version 3, 64-bit in version 4, big-endian), then the
+// value(s).  The image is the last ImageList.<i>.ImageData: its Data array
+// (offset, element type, count) and Dimensions.0/1 (numX, numY).
+struct DmImage {
+  int num = -1;
+  long long offset = -1, count = -1;
+  int type = -1, nx = -1, ny = -1, nz = -1;
+};
+
+struct DmParser {
+  const std::vector<char>& b;
+  size_t pos = 0;
+  int version = 3;
+  std::vector<std::string> tag;
+  std::vector<DmImage> images;
+  std::string err;
+  explicit DmParser(const std::vector<char>& bytes) : b(bytes) {}
+
+  bool need(size_t n) {
+    if (pos + n > b.size()) {
+      if (err.empty()) err = "truncated DM file";
+      return false;
+    }
+    return true;
+  }
+  long long be(int bytes) {
+    if (!need(bytes)) return 0;
+    unsigned long long v = 0;
+    for (int i = 0; i < bytes; ++i) v = (v << 8) | (unsigned char)b[pos + i];
+    pos += bytes;
+    if (bytes == 2) return (int16_t)v;
+    if (bytes == 4) return (int32_t)v;
+    return (long long)v;
+  }
+  long long word() { return be(version == 3 ? 4 : 8); }
+  static int type_size(int t) {
+    switch (t) {
+      case 2: case 4: return 2;
+      case 3: case 5: case 6: return 4;
+      case 7: case 11: case 12: return 8;
+      case 8: case 10: return 1;
+      default: return 0;
+    }
+  }
+  bool skip_values(int t, long long n) {
+    const int sz = type_size(t);
+    if (!sz) {
+      err = "DM value type " + std::to_string(t) + " not implemented";
+      return false;
+    }
+    if (n < 0 || !need((size_t)(sz * n))) return false;
+    pos += (size_t)(sz * n);
+    return true;
+  }
+  uint32_t le32() {
+    if (!need(4)) return 0;
+    uint32_t v;
+    memcpy(&v, &b[pos], 4);
+    pos += 4;
+    return v;
+  }
+  bool in_image(size_t depth, const char* leaf) const {
+    return !images.empty() && tag.size() == depth && tag[0] == "ImageList" &&
+           images.back().num == atoi(tag[1].c_str()) && tag[2] == "ImageData" && tag[3] == leaf;
+  }
+  bool read_tag() {
+    for (int i = 0; i < 4; ++i) {
+      if (!need(1)) return false;
+      if (b[pos++] != '%') {
+        err = "unexpected character in a DM tag";
+        return false;
+      }
+    }
+    const long long n = word();
+    if (n < 1 || n > (1 << 20)) {
+      err = "DM info size must be positive";
+      return false;
+    }
+    std::vector<long long> info((size_t)n);
+    for (long long i = 0; i < n; ++i) info[(size_t)i] = word();
+    if (!err.empty()) return false;
+    if (n == 1) {
+      if (in_image(5, "Dimensions") && info[0] == 5) {
+        const int dir = atoi(tag[4].c_str());
+        const int v = (int)le32();
+        if (dir == 0) images.back().nx = v;
+        else if (dir == 1) images.back().ny = v;
+        else if (dir == 2) images.back().nz = v;
+      } else if (!skip_values((int)info[0], 1)) {
+        return false;
+      }
+    } else if (info[0] == 15) {  // group
+      if (info[1] != 0 || (long long)info.size() - 3 != 2 * info[2]) {
+        err = "inconsistent DM group";
+        return false;
+      }
+      for (long long i = 0; i < info[2]; ++i)
+        if (info[(size_t)(3 + 2 * i)] != 0 || !skip_values((int)info[(size_t)(4 + 2 * i)], 1)) {
+          if (err.empty()) err = "length of fieldname has to be zero";
+          return false;
+        }
+    } else if (info[0] == 20) {  // array
+      if (info[1] == 15) {
+        if (info.size() < 5 || info[2] != 0 || (long long)info.size() - 5 != 2 * info[3]) {
+          err = "inconsistent DM array of groups";
+          return false;
+        }
+        const long long ng = info[3], cnt = info[(size_t)(4 + 2 * ng)];
+        for (long long j = 0; j < cnt; ++j)
+          for (long long i = 0; i < ng; ++i)
+            if (!skip_values((int)info[(size_t)(5 + 2 * i)], 1)) return false;
+      } else {
+        if (info.size() < 3) {
+          err = "inconsistent DM array";
+          return false;
+        }
+        if (in_image(4, "Data")) {
+          images.back().offset = (long long)pos;
+          images.back().type = (int)info[1];
+          images.back().count = info[2];
+        }
+        if (!skip_values((int)info[1], info[2])) return false;
+      }
+    } else {
+      err = "DM numberType " + std::to_string(info[0]) + " not implemented";
+      return false;
+    }
+    tag.pop_back();
+    return true;
+  }
+  // Returns the identifier read (0 at the end of a directory), -1 on error.
+  int read_entry(int dirnum) {
+    if (!need(1)) return -1;
+    const int id = (unsigned char)b[pos++];
+    if (id == 0) return 0;
+    const long long len = be(2);
+    if (len < 0 || !need((size_t)len)) {
+      if (err.empty()) err = "negative DM tag name length";
+      return -1;
+    }
+    const std::string name(&b[pos], (size_t)len);
+    pos += (size_t)len;
+    tag.push_back(len > 0 ? name : (dirnum > -1 ? std::to_string(dirnum) : std::string("nameless")));
+    if (tag.size() == 3 && tag[0] == "ImageList" && tag[2] == "ImageData") {
+      images.emplace_back();
+      images.back().num = atoi(tag[1].c_str());
+    }
+    if (version == 4) be(8);
+    if (id == 21) return read_tag() ? id : -1;
+    if (id == 20) {
+      if (!need(2)) return -1;
+      pos += 2;  // sorted, closed
+      const long long nt = word();
+      for (long long i = 0; i < nt; ++i)
+        if (read_entry((int)i) < 0) return -1;
+      tag.pop_back();
+      return id;
+    }
+    err = "invalid DM tag identifier " + std::to_string(id);
+    return -1;
+  }
+  bool parse() {
+    version = (int)be(4);
+    if (version != 3 && version != 4) {
+      err = "unexpected DM version " + std::to_string(version) + ", expected 3 or 4";
+      return false;
+    }
+    word();  // file length
+    if (be(4) != 1) {
+      err = "DM byte order not implemented";
+      return false;
+    }
+    if (!need(2)) return false;
+    pos += 2;
+    word();  // number of tags of the root directory
+    while (pos < b.size()) {
+      const int id = read_entry(-1);
+      if (id < 0) return false;
+      if (id == 0) break;
+      tag.clear();
+    }
+    return err.empty();
+  }
+};
+
+int read_dm(const std::string& path, const std::vector<char>& b, double* out, long long capacity, int* nx, int* ny,
+            int expect_nx, int expect_ny) {
+  DmParser d(b);
+  if (!d.parse()) return io_fail(MSGPU_ERR_SIZE, "\"" + path + "\": " + d.err);
+  if (d.images.empty()) return io_fail(MSGPU_ERR_SIZE, "\"" + path + "\": No data entry found.");
+  const DmImage& im = d.images.back();
+  if (im.offset < 0 || im.nx <= 0 || im.ny <= 0)
+    return io_fail(MSGPU_ERR_SIZE, "\"" + path + "\": incomplete image entry");
+  if (nx) *nx = im.nx;
+  if (ny) *ny = im.ny;
+  if (expect_nx > 0 && (im.nx != expect_nx || im.ny != expect_ny))
+    return io_fail(MSGPU_ERR_SIZE, "\"" + path + "\": size " + std::to_string(im.nx) + "x" + std::to_string(im.ny) +
+                                       " differs from " + std::to_string(expect_nx) + "x" + std::to_string(expect_ny));
+  if (!out) return MSGPU_OK;
+  const size_t count = (size_t)im.nx * im.ny;
+  if ((long long)count > capacity)
+    return io_fail(MSGPU_ERR_SIZE, "\"" + path + "\": image does not fit the buffer");
+  switch (im.type) {  // DM3ImageData::getSaveType (dm3Import.h:37-51)
+    case 3: return convert_binary<int32_t>(b, (size_t)im.offset, count, out, false, path);
+    case 2: return convert_binary<int16_t>(b, (size_t)im.offset, count, out, false, path);
+    case 4: return convert_binary<uint16_t>(b, (size_t)im.offset, count, out, false, path);
+    case 5: return convert_binary<uint32_t>(b, (size_t)im.offset, count, out, false, path);
+    case 6: return convert_binary<float>(b, (size_t)im.offset, count, out, false, path);
+    case 10: return convert_binary<unsigned char>(b, (size_t)im.offset, count, out, false, path);
+    default:
+      return io_fail(MSGPU_ERR_UNSUPPORTED, "\"" + path + "\": Data type " + std::to_string(im.type) +
+                                                " not implemented");
+  }
+}
+
 // expect_nx/expect_ny > 0: the file must have exactly that size.
 int read_one(const std::string& path, double* out, long long capacity, int* nx, int* ny, int expect_nx = 0,
              int expect_ny = 0) {
   std::vector<char> b;
   int rc = load_bytes(path, b);
   if (rc) return rc;
+  if (ends_with(path, ".dm3") || ends_with(path, ".dm4"))
+    return read_dm(path, b, out, capacity, nx, ny, expect_nx, expect_ny);
   Header h;
   if ((rc = parse_header(b, h, path))) return rc;
   if (nx) *nx = (int)h.nx;

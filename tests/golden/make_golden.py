@@ -217,6 +217,16 @@ def io_files(ref: msor.RefRunner, seed: int):
         path = os.path.join(d, name)
         ref.save_array(a, path, t)
         expected[name] = ref.load_array(path)
+    # DigitalMicrograph files (this repository's writer, the reference's reader)
+    from msgpu.dmfile import dm_bytes
+    for v, t in ((3, 6), (4, 4), (3, 2), (4, 10)):
+        img = rng.normal(0, 100, (13, 21)) + (200 if t in (4, 10) else 0)
+        if t in (4, 10):
+            img = np.clip(img, 0, 255)
+        name = f"dm_t{t}.dm{v}"
+        with open(os.path.join(d, name), "wb") as f:
+            f.write(dm_bytes([(rng.normal(size=(5, 7)), 6), (img, t)], v))
+        expected[name] = ref.load_array(os.path.join(d, name))
     n = n_of(4)
     phi = rng.normal(0, 0.01, (2, n * n))
     ref.save_displacement(4, phi, os.path.join(d, "ref_deformation_04_%d.dat.bz2"))

@@ -12,7 +12,8 @@ import pytest
 from conftest import GOLDEN, golden
 
 IO = os.path.join(GOLDEN, "io")
-FILES = ("ref_p9.q2bz", "ref_p8.dat.bz2", "ref_p5.pgm", "ref_pa.pgm", "ref_p2.pgm", "ref_p7.txt", "ref_p9.pgm")
+FILES = ("ref_p9.q2bz", "ref_p8.dat.bz2", "ref_p5.pgm", "ref_pa.pgm", "ref_p2.pgm", "ref_p7.txt", "ref_p9.pgm",
+         "dm_t6.dm3", "dm_t4.dm4", "dm_t2.dm3", "dm_t10.dm4")
 
 
 @pytest.fixture(scope="module")
@@ -27,8 +28,30 @@ def io():
 def test_reads_reference_files_bit_exact(io, name):
     g = golden("io_expected.npz")
     a = io.read_array(os.path.join(IO, name))
-    assert a.shape == (17, 33)
+    assert a.shape == g[name].shape == ((13, 21) if name.startswith("dm_") else (17, 33))
     assert np.array_equal(a, g[name])
+
+
+@pytest.mark.parametrize("version", [3, 4])
+@pytest.mark.parametrize("t", [2, 3, 4, 5, 6, 10])
+def test_digital_micrograph_like_the_reference(io, tmp_path, version, t):
+    """Every image type DM3Reader exports, in DM3 and DM4: the last image of
+    the ImageList is read, other tags (groups, arrays of groups, strings) are
+    skipped; decoded values as the reference's importer decodes them."""
+    import msor
+    from msgpu.dmfile import dm_bytes
+    rng = np.random.default_rng(10 * version + t)
+    a = rng.normal(0, 100, (11, 19)) + (200 if t in (4, 5, 10) else 0)
+    if t in (4, 5, 10):
+        a = np.clip(a, 0, 255)
+    p = tmp_path / f"x.dm{version}"
+    p.write_bytes(dm_bytes([(rng.normal(size=(4, 6)), 6), (a, t)], version))
+    ours = io.read_array(str(p))
+    assert ours.shape == (11, 19)
+    assert np.array_equal(ours, np.asarray(a.astype({2: "<i2", 3: "<i4", 4: "<u2", 5: "<u4", 6: "<f4",
+                                                      10: "<u1"}[t]), dtype=np.float64))
+    if msor.have_ref():
+        assert np.array_equal(msor.RefRunner().load_array(str(p)), ours)
 
 
 def test_reads_reference_displacement(io):
