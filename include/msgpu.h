@@ -108,6 +108,32 @@ int msgpu_match_series_stage_device(msgpu_context* ctx, const msgpu_params* p, c
                                     double* d_energies_out, int* d_steps_out, double* d_mean_out,
                                     double* d_count_out, void* stream);
 
+/* --- ragged batches -------------------------------------------------------
+ * Many series of different sizes in one batch (no counterpart in the
+ * reference, which registers one frame at a time): every template is
+ * registered to the reference of its series as msgpu_register_batch does,
+ * and one level-kernel launch per level serves every series that has that
+ * level (the largest series run alone on their finest levels).  Each series
+ * brings its own level (precision = input = stop level); of msgpu_params the
+ * batch uses start_level (common to all series), lambda, lambda_factor
+ * (weights count from each series' own stop level), max_gd_iterations,
+ * stop_epsilon, the normalisation keys, resample_deformation, use_fp64 and
+ * data_term.  A frame's result does not depend on the batch it is in.    */
+typedef struct {
+  int level;                 /* (2^level+1)^2 images                          */
+  int num_templates;
+  const double* reference;   /* one image                                     */
+  const double* templates;   /* num_templates images                          */
+  double* phis_out;          /* num_templates * 2 * (2^level+1)^2 doubles     */
+  double* energies_out;      /* nullable: num_templates doubles               */
+} msgpu_series_desc;
+/* host buffers; synchronous */
+int msgpu_register_ragged(msgpu_context* ctx, const msgpu_params* p, const msgpu_series_desc* series,
+                          int num_series);
+/* device buffers, enqueued on `stream` */
+int msgpu_register_ragged_device(msgpu_context* ctx, const msgpu_params* p, const msgpu_series_desc* series,
+                                 int num_series, void* stream);
+
 /* --- series pipeline ------------------------------------------------------ */
 /* Options of matchSeries<>() beyond the registration keys (parameter-file
  * names of the reference).                                                  */

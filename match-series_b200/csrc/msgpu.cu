@@ -398,11 +398,14 @@ __global__ void k_set_buf(int* buf, int n, int v) {
 // (fixed thread assignment, warps reduced in order).
 // One block per reference: block 0 normalises R0 into out0; with pairwise
 // references block b > 0 normalises the template of instance b - 1 (at
-// arena + (b-1)*inst_stride + off_T) into out0 + b*out_stride.
+// arena + (b-1)*inst_stride + off_T) into out0 + b*out_stride; with inst_ref
+// (ragged batches) block b normalises R0 + inst_ref[b]*ref_stride.
 template <typename Real>
 __global__ void k_ncc_normalize(const Real* __restrict__ R0, const Real* __restrict__ arena, size_t inst_stride,
-                                size_t off_T, int level, Real* out0, size_t out_stride) {
-  const Real* __restrict__ R = blockIdx.x == 0 ? R0 : arena + (size_t)(blockIdx.x - 1) * inst_stride + off_T;
+                                size_t off_T, int level, Real* out0, size_t out_stride,
+                                const int* inst_ref = nullptr, size_t ref_stride = 0) {
+  const Real* __restrict__ R = inst_ref ? R0 + (size_t)inst_ref[blockIdx.x] * ref_stride
+                               : (blockIdx.x == 0 ? R0 : arena + (size_t)(blockIdx.x - 1) * inst_stride + off_T);
   Real* out = out0 + (size_t)blockIdx.x * out_stride;
   const int n = lvl_n(level), P = pitch_of(n), N = n * n;
   const Real h = (Real)(1.0 / (double)(n - 1)), hh = h * h;
@@ -908,6 +911,204 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
   return MSGPU_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Ragged batches: series of different sizes, each registered to its own
+// reference, one level-kernel launch per level for all of them.
+
+struct RaggedSeries {
+  int level, F;            // precision = input = stop level of the series, templates
+  const double* ref;       // device, (2^level+1)^2
+  const double* tmpl;      // device, F images
+  double* phis;            // device, F x 2 x N_level
+  double* energies;        // device or null, F
+};
+
+// Normalisation and image pyramid of one series (reference + templates), as
+// steps 1-2 of run_batch, into the arena slots starting at instance i0 and the
+// reference slot at Rslot (layout L of the batch's largest level).
+template <typename Real>
+int prepare_series(msgpu_context* ctx, const msgpu_params& p, const RaggedSeries& S, const Layout& L, Real* arena,
+                   size_t i0, Real* Rslot, double* pyr, size_t pstride, const std::vector<size_t>& poff,
+                   double* mm, cudaStream_t st, int& launches) {
+  const int Lin = S.level, F = S.F, nimg = F + 1;
+  const size_t Nin = lvl_N(Lin);
+  CK(cudaMemcpy2DAsync(pyr + poff[Lin], pstride * sizeof(double), S.ref, Nin * sizeof(double), Nin * sizeof(double),
+                       1, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpy2DAsync(pyr + pstride + poff[Lin], pstride * sizeof(double), S.tmpl, Nin * sizeof(double),
+                       Nin * sizeof(double), F, cudaMemcpyDeviceToDevice, st));
+  if (!p.dont_normalize_input) {
+    if (p.saturation_percent >= 0) {
+      const int m1 = (int)Nin - 1;
+      int il = (int)(p.saturation_percent / 200 * m1), ih = (int)((1 - p.saturation_percent / 200) * m1);
+      il = std::min(std::max(il, 0), m1);
+      ih = std::min(std::max(ih, 0), m1);
+      k_select2<<<nimg, kSelThreads, 0, st>>>(pyr + poff[Lin], pstride, (int)Nin, il, ih, mm);
+    } else {
+      k_minmax<<<nimg, 1024, 0, st>>>(pyr + poff[Lin], pstride, (int)Nin, mm);
+    }
+    k_normalize<<<dim3((unsigned)std::min<size_t>(1024, (Nin + 255) / 256), nimg), 256, 0, st>>>(
+        pyr + poff[Lin], pstride, (int)Nin, mm, p.saturation_percent >= 0 ? 1 : 0, p.normalize_min_to_zero);
+    launches += 2;
+  }
+  for (int l = Lin; l >= 1; --l) {
+    const size_t cN = lvl_N(l - 1);
+    k_restrict<double><<<dim3((unsigned)std::min<size_t>(1024, (cN + 255) / 256), nimg), 256, 0, st>>>(
+        pyr + poff[l], pstride, pyr + poff[l - 1], pstride, l);
+    ++launches;
+  }
+  for (int l = 0; l <= Lin; ++l) {
+    const size_t Nl = lvl_N(l);
+    const unsigned gx = (unsigned)std::min<size_t>(1024, (Nl + 255) / 256);
+    k_to_pitched<double, Real><<<dim3(gx, 1), 256, 0, st>>>(pyr + poff[l], 0, Rslot + L.off_T[l], 0, lvl_n(l));
+    k_to_pitched<double, Real><<<dim3(gx, F), 256, 0, st>>>(pyr + pstride + poff[l], pstride,
+                                                             arena + i0 * L.stride + L.off_T[l], L.stride, lvl_n(l));
+    launches += 2;
+  }
+  CK(cudaGetLastError());
+  return MSGPU_OK;
+}
+
+template <typename Real>
+int run_ragged(msgpu_context* ctx, const msgpu_params& p, std::vector<RaggedSeries> S, cudaStream_t st) {
+  // largest series first: the instances still running at a level are a prefix
+  std::stable_sort(S.begin(), S.end(), [](const RaggedSeries& a, const RaggedSeries& b) { return a.level > b.level; });
+  const int ns = (int)S.size();
+  const int Lmax = S[0].level, start = p.start_level;
+  const bool ncc = p.data_term == 1;
+  const Layout L = make_layout(Lmax, ncc, ncc);
+  int Ftot = 0;
+  std::vector<int> first(ns);
+  for (int s = 0; s < ns; ++s) { first[s] = Ftot; Ftot += S[s].F; }
+  int rc;
+  if ((rc = ensure_tables(ctx))) return rc;
+  if ((rc = sched_error_reset(ctx, st))) return rc;
+  const size_t rstride = align_up(L.off_T[Lmax] + comp_stride(Lmax), 64);
+  size_t pmax = 0;
+  std::vector<std::vector<size_t>> poffs(ns);
+  std::vector<size_t> pstrides(ns);
+  for (int s = 0; s < ns; ++s) {
+    poffs[s].assign(S[s].level + 1, 0);
+    size_t ps = 0;
+    for (int l = S[s].level; l >= 0; --l) { poffs[s][l] = ps; ps = align_up(ps + lvl_N(l), 32); }
+    pstrides[s] = ps;
+    pmax = std::max(pmax, ps * (size_t)(S[s].F + 1));
+  }
+  const int nlev = Lmax - start + 1;
+  const size_t small_bytes = sizeof(double) * (2 * (size_t)(Ftot + ns + 1) + (size_t)Ftot * (nlev + 1) + 64) +
+                             sizeof(int) * ((size_t)Ftot * 5 + 64);
+  if ((rc = ensure(ctx, ctx->dscratch, sizeof(double) * pmax))) return rc;
+  if ((rc = ensure(ctx, ctx->arena, sizeof(Real) * L.stride * Ftot))) return rc;
+  if ((rc = ensure(ctx, ctx->shared_real, sizeof(Real) * rstride * ns))) return rc;
+  if ((rc = ensure(ctx, ctx->small, small_bytes))) return rc;
+  double* pyr = (double*)ctx->dscratch.p;
+  Real* arena = (Real*)ctx->arena.p;
+  Real* refs = (Real*)ctx->shared_real.p;
+  double* mm = (double*)ctx->small.p;                       // 2 * (Fmax + 1)
+  double* e_lvl = mm + 2 * (size_t)(Ftot + ns + 1);        // Ftot
+  double* lam_all = e_lvl + Ftot;                           // nlev x Ftot
+  int* ibase = (int*)(lam_all + (size_t)Ftot * nlev + 64);
+  int* bufA = ibase;
+  int* bufB = ibase + Ftot;
+  int* steps = ibase + 2 * (size_t)Ftot;
+  int* evals = ibase + 3 * (size_t)Ftot;
+  int* inst_ref = ibase + 4 * (size_t)Ftot;
+  int& launches = ctx->stats.kernel_launches;
+  launches = 0;
+  ctx->stats.num_levels = nlev;
+  ctx->stats.first_level = start;
+  // per-instance reference index and level weights
+  std::vector<int> h_ref(Ftot);
+  std::vector<double> h_lam((size_t)Ftot * nlev);
+  for (int s = 0; s < ns; ++s)
+    for (int f = 0; f < S[s].F; ++f) {
+      h_ref[first[s] + f] = s;
+      for (int l = start; l <= Lmax; ++l)
+        h_lam[(size_t)(l - start) * Ftot + first[s] + f] =
+            std::pow(p.lambda_factor, (double)(S[s].level - l)) * p.lambda;
+    }
+  CK(cudaMemcpyAsync(inst_ref, h_ref.data(), sizeof(int) * Ftot, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(lam_all, h_lam.data(), sizeof(double) * h_lam.size(), cudaMemcpyHostToDevice, st));
+  // 1. every series' images
+  for (int s = 0; s < ns; ++s)
+    if ((rc = prepare_series<Real>(ctx, p, S[s], L, arena, (size_t)first[s], refs + (size_t)s * rstride, pyr,
+                                   pstrides[s], poffs[s], mm, st, launches)))
+      return rc;
+  // 2. zero displacement at the start level
+  k_set_buf<Real><<<1, 256, 0, st>>>(bufA, Ftot, 0);
+  CK(cudaMemset2DAsync(arena + L.off_phi[0], L.stride * sizeof(Real), 0, 2 * comp_stride(start) * sizeof(Real), Ftot,
+                       st));
+  ++launches;
+  // 3. level loop over the running prefix of instances
+  int* bin = bufA;
+  int* bout = bufB;
+  for (int l = start; l <= Lmax; ++l) {
+    int A = 0, Anext = 0;
+    for (int s = 0; s < ns; ++s) {
+      if (S[s].level >= l) A += S[s].F;
+      if (S[s].level > l) Anext += S[s].F;
+    }
+    LevelArgs<Real> a;
+    memset(&a, 0, sizeof(a));
+    a.arena = arena;
+    a.inst_stride = L.stride;
+    a.R = refs + L.off_T[l];
+    a.inst_ref = inst_ref;
+    a.ref_stride = rstride;
+    a.lambda = p.lambda;
+    a.lambda_inst = lam_all + (size_t)(l - start) * Ftot;
+    if (ncc) {
+      a.ncc = 1;
+      a.off_td = L.off_td;
+      a.off_nr = L.off_nr;
+      k_ncc_normalize<Real><<<A, 1024, 0, st>>>(refs + L.off_T[l], arena, L.stride, L.off_T[l], l, arena + L.off_nr,
+                                               L.stride, inst_ref, rstride);
+      ++launches;
+    }
+    a.off_T = L.off_T[l];
+    a.off_phi[0] = L.off_phi[0];
+    a.off_phi[1] = L.off_phi[1];
+    a.off_d[0] = L.off_d[0];
+    a.off_d[1] = L.off_d[1];
+    a.off_s = L.off_s;
+    a.off_de = L.off_de;
+    for (int k = 0; k <= kMaxLevel; ++k) { a.off_x2[k] = L.off_x2[k]; a.off_x5[k] = L.off_x5[k]; a.off_b[k] = L.off_b[k]; }
+    a.level = l;
+    a.n = lvl_n(l);
+    a.num_inst = A;
+    a.lc = pick_lc<Real>(l);
+    a.mode = MODE_SOLVE;
+    a.stop_eps = p.stop_epsilon;
+    a.max_iter = p.max_gd_iterations;
+    a.phi_in_dev = bin;
+    a.out_energy = e_lvl;
+    a.out_steps = steps;
+    a.out_evals = evals;
+    a.out_phi_buf = bin;
+    if ((rc = launch_level<Real>(ctx, a, st))) return rc;
+    ++launches;
+    // series finishing at this level: displacements and energies out
+    for (int s = 0; s < ns; ++s) {
+      if (S[s].level != l) continue;
+      const int NM = (int)lvl_N(l);
+      k_phi_out<Real><<<dim3((unsigned)std::min(1024, (NM + 255) / 256), S[s].F), 256, 0, st>>>(
+          arena + (size_t)first[s] * L.stride, L.stride, L.off_phi[0], L.off_phi[1], l, bin + first[s], S[s].phis);
+      ++launches;
+      if (S[s].energies)
+        CK(cudaMemcpyAsync(S[s].energies, e_lvl + first[s], sizeof(double) * S[s].F, cudaMemcpyDeviceToDevice, st));
+    }
+    CK(cudaGetLastError());
+    if (Anext > 0) {
+      const size_t fw = lvl_N(l + 1);
+      k_phi_up<Real><<<dim3((unsigned)std::min<size_t>(1024, (fw + 255) / 256), Anext), 256, 0, st>>>(
+          arena, L.stride, L.off_phi[0], L.off_phi[1], l, bin, bout, p.resample_deformation ? 1 : 0);
+      CK(cudaGetLastError());
+      ++launches;
+      std::swap(bin, bout);
+    }
+  }
+  return MSGPU_OK;
+}
+
 int check_params(msgpu_context* ctx, const msgpu_params* p) {
   if (!p) return fail(ctx, MSGPU_ERR_INVALID_ARG, "params is NULL");
   if (p->precision_level < 1 || p->precision_level > kMaxLevel)
@@ -1336,6 +1537,83 @@ int msgpu_match_series_stage(msgpu_context* ctx, const msgpu_params* p, const do
   if (energies_out) memcpy(energies_out, e.data(), sizeof(double) * F);
   if (steps_out) memcpy(steps_out, s.data(), sizeof(int) * F * nlev);
   return MSGPU_OK;
+}
+
+namespace {
+int check_ragged(msgpu_context* ctx, const msgpu_params* p, const msgpu_series_desc* series, int num_series) {
+  if (!p) return fail(ctx, MSGPU_ERR_INVALID_ARG, "params is NULL");
+  if (!series || num_series < 1) return fail(ctx, MSGPU_ERR_INVALID_ARG, "no series");
+  if (p->max_gd_iterations < 0) return fail(ctx, MSGPU_ERR_INVALID_ARG, "maxGDIterations < 0");
+  if (p->data_term != 0 && p->data_term != 1)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "data_term %d: 0 (SSD) or 1 (NCC)", p->data_term);
+  for (int s = 0; s < num_series; ++s) {
+    const msgpu_series_desc& d = series[s];
+    if (d.level < 1 || d.level > kMaxLevel || d.level < p->start_level || p->start_level < 1)
+      return fail(ctx, MSGPU_ERR_INVALID_ARG, "series %d: level %d outside [startLevel %d, %d]", s, d.level,
+                  p->start_level, kMaxLevel);
+    if (d.num_templates < 1 || !d.reference || !d.templates || !d.phis_out)
+      return fail(ctx, MSGPU_ERR_INVALID_ARG, "series %d: no templates or a null buffer", s);
+  }
+  return MSGPU_OK;
+}
+}  // namespace
+
+int msgpu_register_ragged_device(msgpu_context* ctx, const msgpu_params* p, const msgpu_series_desc* series,
+                                 int num_series, void* stream) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  int rc;
+  if ((rc = check_ragged(ctx, p, series, num_series))) return rc;
+  if ((rc = bind_device(ctx))) return rc;
+  std::vector<RaggedSeries> S(num_series);
+  for (int s = 0; s < num_series; ++s)
+    S[s] = RaggedSeries{series[s].level, series[s].num_templates, series[s].reference, series[s].templates,
+                        series[s].phis_out, series[s].energies_out};
+  cudaStream_t st = (cudaStream_t)stream;
+  return p->use_fp64 ? run_ragged<double>(ctx, *p, S, st) : run_ragged<float>(ctx, *p, S, st);
+}
+
+int msgpu_register_ragged(msgpu_context* ctx, const msgpu_params* p, const msgpu_series_desc* series,
+                          int num_series) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  int rc;
+  if ((rc = check_ragged(ctx, p, series, num_series))) return rc;
+  if ((rc = bind_device(ctx))) return rc;
+  size_t in = 0, out = 0;
+  std::vector<size_t> ioff(num_series), ooff(num_series);
+  for (int s = 0; s < num_series; ++s) {
+    const size_t N = lvl_N(series[s].level);
+    ioff[s] = in;
+    ooff[s] = out;
+    in += N * (1 + (size_t)series[s].num_templates);
+    out += 2 * N * series[s].num_templates + series[s].num_templates;
+  }
+  if ((rc = ensure(ctx, ctx->io[1], sizeof(double) * in))) return rc;
+  if ((rc = ensure(ctx, ctx->io[3], sizeof(double) * out))) return rc;
+  cudaStream_t st = ctx->stream;
+  double* din = (double*)ctx->io[1].p;
+  double* dout = (double*)ctx->io[3].p;
+  std::vector<RaggedSeries> S(num_series);
+  for (int s = 0; s < num_series; ++s) {
+    const msgpu_series_desc& d = series[s];
+    const size_t N = lvl_N(d.level);
+    CK(cudaMemcpyAsync(din + ioff[s], d.reference, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(din + ioff[s] + N, d.templates, sizeof(double) * N * d.num_templates, cudaMemcpyHostToDevice,
+                       st));
+    S[s] = RaggedSeries{d.level, d.num_templates, din + ioff[s], din + ioff[s] + N, dout + ooff[s],
+                        dout + ooff[s] + 2 * N * d.num_templates};
+  }
+  if ((rc = p->use_fp64 ? run_ragged<double>(ctx, *p, S, st) : run_ragged<float>(ctx, *p, S, st))) return rc;
+  for (int s = 0; s < num_series; ++s) {
+    const msgpu_series_desc& d = series[s];
+    const size_t N = lvl_N(d.level);
+    CK(cudaMemcpyAsync(d.phis_out, dout + ooff[s], sizeof(double) * 2 * N * d.num_templates, cudaMemcpyDeviceToHost,
+                       st));
+    if (d.energies_out)
+      CK(cudaMemcpyAsync(d.energies_out, dout + ooff[s] + 2 * N * d.num_templates, sizeof(double) * d.num_templates,
+                         cudaMemcpyDeviceToHost, st));
+  }
+  CK(cudaStreamSynchronize(st));
+  return sched_error_check(ctx);
 }
 
 void msgpu_series_params_default(const msgpu_params* p, msgpu_series_params* s) {

@@ -91,6 +91,13 @@ struct LevelArgs {
   // instance then reads its own normalised reference at off_nr.
   int r_prev;
   size_t off_nr;
+  // ragged batches (series of different sizes in one launch): inst_ref != 0
+  // gives each instance the reference of its series, R + inst_ref[i] *
+  // ref_stride, and (with NCC) its own normalised reference at off_nr;
+  // lambda_inst != 0 its own regularisation weight.
+  const int* inst_ref;
+  size_t ref_stride;
+  const double* lambda_inst;
 };
 
 // A 2-component array of level k occupies 2 * comp_stride(k) elements.
@@ -212,6 +219,7 @@ struct Inst {
   const Real* R;
   const Real* T;
   const Real* normR;
+  double lambda;
   int n, P;
   Real h;
   __device__ Real* arr(size_t off) const { return base + off; }
@@ -1140,9 +1148,11 @@ template <typename Real>
 __device__ __forceinline__ Inst<Real> make_inst(const LevelArgs<Real>& a, int inst) {
   Inst<Real> I;
   I.base = a.arena + (size_t)inst * a.inst_stride;
-  I.R = (a.r_prev && inst > 0) ? a.arena + (size_t)(inst - 1) * a.inst_stride + a.off_T : a.R;
+  if (a.inst_ref) I.R = a.R + (size_t)a.inst_ref[inst] * a.ref_stride;
+  else I.R = (a.r_prev && inst > 0) ? a.arena + (size_t)(inst - 1) * a.inst_stride + a.off_T : a.R;
   I.T = I.base + a.off_T;
-  I.normR = a.r_prev ? I.base + a.off_nr : a.normR;
+  I.normR = (a.r_prev || a.inst_ref) ? I.base + a.off_nr : a.normR;
+  I.lambda = a.lambda_inst ? a.lambda_inst[inst] : a.lambda;
   I.n = a.n;
   I.P = pitch_of(a.n);
   I.h = (Real)(1.0 / (double)(a.n - 1));
@@ -1220,7 +1230,7 @@ struct TaskRunner {
       case TK_GRAD: {
         Real* nphi = I.arr(a.off_phi[d.cur ^ 1]);
         const Real* dd = I.arr(a.off_d[d.dcur]);
-        GradPass<Real> ps(I, (d.flags & PF_STEP) != 0, (Real)d.t, a.lambda, phi, phi + cs, dd, dd + cs, nphi,
+        GradPass<Real> ps(I, (d.flags & PF_STEP) != 0, (Real)d.t, I.lambda, phi, phi + cs, dd, dd + cs, nphi,
                           nphi + cs, de, de + cs, smem, part);
         f(ps);
         break;
@@ -1243,7 +1253,7 @@ struct TaskRunner {
       }
       case TK_NF: {
         Real* nphi = I.arr(a.off_phi[d.cur ^ 1]);
-        NccForcePass<Real> ps(I, a.lambda, d.mean, d.var, d.e, nphi, nphi + cs, I.arr(a.off_td), I.normR, de, de + cs,
+        NccForcePass<Real> ps(I, I.lambda, d.mean, d.var, d.e, nphi, nphi + cs, I.arr(a.off_td), I.normR, de, de + cs,
                               smem, part);
         f(ps);
         break;
@@ -1354,7 +1364,7 @@ __device__ __forceinline__ void block_sum(const double part[kRedSlots], double (
 // (ArmijoSearch.h:118-200).
 template <typename Real>
 __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const double* tot) {
-  const double lam = a.lambda;
+  const double lam = a.lambda_inst ? a.lambda_inst[inst] : a.lambda;
   const double tau_min = 9.313225746154785e-10;  // 2^-30 (ArmijoSearch.h:77)
   const double tau_max = 33554432.0;             // 2^25  (ArmijoSearch.h:67)
   const double stop_sigma = 0.0001, sigma_tol = 0.00001;

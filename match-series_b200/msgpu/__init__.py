@@ -53,6 +53,18 @@ class SeriesParams(ctypes.Structure):
     ]
 
 
+class SeriesDesc(ctypes.Structure):
+    """msgpu_series_desc: one series of a ragged batch."""
+    _fields_ = [
+        ("level", ctypes.c_int),
+        ("num_templates", ctypes.c_int),
+        ("reference", ctypes.c_void_p),
+        ("templates", ctypes.c_void_p),
+        ("phis_out", ctypes.c_void_p),
+        ("energies_out", ctypes.c_void_p),
+    ]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("kernel_launches", ctypes.c_int), ("num_levels", ctypes.c_int), ("first_level", ctypes.c_int),
                 ("level_ms", ctypes.c_float * 16), ("level_steps", ctypes.c_longlong * 16),
@@ -78,7 +90,8 @@ EXPORTS = [
     "msgpu_set_data_term", "msgpu_series_params_default", "msgpu_match_series", "msgpu_match_series_device",
     "msgpu_compose", "msgpu_compose_device", "msgpu_warp_median", "msgpu_warp_median_device",
     "msgpu_io_last_error", "msgpu_read_array", "msgpu_write_array", "msgpu_read_arrays", "msgpu_read_displacement",
-    "msgpu_write_displacement", "msgpu_read_arrays_start", "msgpu_io_wait",
+    "msgpu_write_displacement", "msgpu_read_arrays_start", "msgpu_io_wait", "msgpu_register_ragged",
+    "msgpu_register_ragged_device",
 ]
 
 
@@ -146,6 +159,10 @@ def lib():
                                               ctypes.c_int, _dp, ctypes.c_int]
         L.msgpu_read_arrays_start.restype = ctypes.c_void_p
         L.msgpu_io_wait.argtypes = [ctypes.c_void_p]
+        L.msgpu_register_ragged.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params), ctypes.POINTER(SeriesDesc),
+                                            ctypes.c_int]
+        L.msgpu_register_ragged_device.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params),
+                                                   ctypes.POINTER(SeriesDesc), ctypes.c_int, ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -324,6 +341,35 @@ class Context:
         self._check(lib().msgpu_match_series_stage_device(self._h, ctypes.byref(params), d_ref, d_templates,
                                                           num_templates, d_phis, d_energies or None, d_steps or None,
                                                           d_mean, d_count, stream or None))
+
+    # --- ragged batches -----------------------------------------------------
+    def register_ragged(self, params: Params, series):
+        """series: list of (reference, templates) of any sizes 2^l+1 (square);
+        returns a list of (phis[F,2,N], energies[F]) in the same order."""
+        keep, descs, outs = [], [], []
+        for ref, tm in series:
+            ref = _f64(ref).reshape(-1)
+            tm = _f64(tm)
+            F = tm.shape[0]
+            tm = tm.reshape(F, -1)
+            n = int(round(ref.size ** 0.5))
+            level = (n - 1).bit_length() - 1
+            if (1 << level) + 1 != n or n * n != ref.size:
+                raise ValueError("images must be (2^l+1)^2")
+            phis = np.zeros((F, 2, n * n))
+            en = np.zeros(F)
+            keep += [ref, tm]
+            outs.append((phis, en))
+            descs.append(SeriesDesc(level, F, ref.ctypes.data, tm.ctypes.data, phis.ctypes.data, en.ctypes.data))
+        arr = (SeriesDesc * len(descs))(*descs)
+        self._check(lib().msgpu_register_ragged(self._h, ctypes.byref(params), arr, len(descs)))
+        return outs
+
+    def register_ragged_device(self, params: Params, descs, stream: int = 0):
+        """descs: SeriesDesc entries holding device pointers."""
+        arr = (SeriesDesc * len(descs))(*descs)
+        self._check(lib().msgpu_register_ragged_device(self._h, ctypes.byref(params), arr, len(descs),
+                                                       stream or None))
 
     # --- series pipeline ----------------------------------------------------
     def match_series(self, params: Params, series: SeriesParams, frames):
