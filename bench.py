@@ -29,6 +29,11 @@ by host threads and registered stage by stage through the host entry point,
 the decoding of the next series overlapping the GPU work on the current one.
 Its CPU baseline is the reference's own loader on the same files.
 
+--ragged times uneven series in one batch (msgpu_register_ragged): 16
+series of 8 templates each, sizes drawn from 129², 257², 513², 1025², levels
+4 to each series' own finest level, one launch per level for all series;
+beside it the same series registered one batch after the other.
+
 Multi-GPU (torchrun): weak scaling; every rank registers its own series.
 """
 from __future__ import annotations
@@ -578,6 +583,112 @@ def main_files(args, world, rank, local):
     return 0
 
 
+def main_ragged(args, world, rank, local):
+    """--ragged: uneven series in one ragged batch (msgpu_register_ragged)."""
+    import numpy as np
+    import torch
+    import msgpu
+    from msgpu import build as mbuild
+    from msgpu import synthetic as syn
+
+    torch.cuda.set_device(local)
+    mbuild.build()
+    fp64 = not args.fp32
+    series = syn.ragged_workload(seed=3000 + 1000 * rank)
+    levels = [int(round(np.sqrt(r.size))) - 1 for r, _ in series]
+    levels = [l.bit_length() - 1 for l in levels]
+    F = [t.shape[0] for _, t in series]
+    total = sum(F)
+    p = msgpu.default_params(start_level=4, max_gd_iterations=MAX_ITER, use_fp64=int(fp64), lambda_=LAMBDA)
+    ctx = msgpu.Context(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    keep, descs = [], []
+    for (ref, tm), l in zip(series, levels):
+        N = ((1 << l) + 1) ** 2
+        d_ref = torch.from_numpy(ref).to(dev)
+        d_tm = torch.from_numpy(tm).to(dev)
+        d_ph = torch.empty((tm.shape[0], 2, N), dtype=torch.float64, device=dev)
+        d_e = torch.empty(tm.shape[0], dtype=torch.float64, device=dev)
+        keep += [d_ref, d_tm, d_ph, d_e]
+        descs.append(msgpu.SeriesDesc(l, tm.shape[0], d_ref.data_ptr(), d_tm.data_ptr(), d_ph.data_ptr(),
+                                      d_e.data_ptr()))
+
+    def step():
+        ctx.register_ragged_device(p, descs, stream.cuda_stream)
+
+    def separate():
+        for d in descs:
+            q = msgpu.default_params(precision_level=d.level, input_level=d.level, start_level=4, stop_level=d.level,
+                                     max_gd_iterations=MAX_ITER, use_fp64=int(fp64), lambda_=LAMBDA)
+            ctx.register_batch_device(q, d.reference, d.templates, d.num_templates, d.phis_out, d.energies_out,
+                                      0, 0, stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    start_ev = torch.cuda.Event(enable_timing=True)
+    stop_ev = torch.cuda.Event(enable_timing=True)
+    launches = 0
+    barrier(world)
+    with ClockSampler(local) as clocks:
+        start_ev.record(stream)
+        for _ in range(args.steps):
+            step()
+            launches += ctx.stats()["kernel_launches"]
+        stop_ev.record(stream)
+        torch.cuda.synchronize(dev)
+    elapsed_ms = allreduce_max(start_ev.elapsed_time(stop_ev), world)
+    value = world * total * args.steps / (elapsed_ms / 1000.0)
+    # the same series one batch after the other
+    separate()
+    torch.cuda.synchronize(dev)
+    start_ev.record(stream)
+    separate()
+    stop_ev.record(stream)
+    torch.cuda.synchronize(dev)
+    sep_ms = start_ev.elapsed_time(stop_ev)
+    # end to end through the host entry point
+    host = [(r, t) for r, t in series]
+    ctx.register_ragged(p, host)
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ctx.register_ragged(p, host)
+    e2e_s = allreduce_max(time.perf_counter() - t0, world)
+    h2d = sum((1 + f) * ((1 << l) + 1) ** 2 * 8 for f, l in zip(F, levels))
+    d2h = sum((2 * f * ((1 << l) + 1) ** 2 + f) * 8 for f, l in zip(F, levels))
+    if rank == 0:
+        clk = clocks.summary()
+        sizes = {}
+        for f, l in zip(F, levels):
+            sizes[(1 << l) + 1] = sizes.get((1 << l) + 1, 0) + f
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if fp64 else "f32+f64-reductions",
+            "data": "synthetic",
+            "config": {"workload": f"ragged batch: {len(series)} series, {total} templates, frames per size "
+                                   f"{dict(sorted(sizes.items()))}, square/hex lattices with spacing 8-16 px and "
+                                   f"Poisson peak 20-100, levels 4 to each series' finest, maxGDIterations "
+                                   f"{MAX_ITER}, lambda {LAMBDA}, one level-kernel launch per level",
+                       "parallelism": f"weak, {world} ranks"},
+            "e2e": {"value": world * total * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "separate_batches_frames_per_s": total / (sep_ms / 1000.0),
+            "roofline": None,
+            "cpu_baseline": None,
+            "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        }
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -596,6 +707,8 @@ def main():
                     help="small case for ncu: one displacement composition at this level, no timing")
     ap.add_argument("--profile-series", action="store_true",
                     help="small case for ncu: one msgpu_match_series call on the bench's frames, no timing")
+    ap.add_argument("--ragged", action="store_true",
+                    help="uneven series of 129^2..1025^2 in one ragged batch (msgpu_register_ragged)")
     ap.add_argument("--files", action="store_true",
                     help="series read from .q2bz files, decoding overlapped with the GPU stages")
     ap.add_argument("--series", action="store_true",
@@ -615,6 +728,8 @@ def main():
         return main_series(args, world, rank, local)
     if args.files:
         return main_files(args, world, rank, local)
+    if args.ragged:
+        return main_ragged(args, world, rank, local)
 
     import numpy as np
     import torch

@@ -132,6 +132,22 @@ def smooth_field(n: int, rng: np.random.Generator, amp_px: float, shift_px=(0.0,
     return out
 
 
+def ragged_workload(num_series: int = 16, frames_per_series: int = 8, sizes=(129, 257, 513, 1025),
+                    seed: int = 3000):
+    """Uneven series: each of a size drawn from `sizes`, a square or hexagonal
+    lattice with spacing U(8, 16) px, Poisson peak U(20, 100), displacements
+    up to 3 px; returns a list of (reference[n*n], templates[F, n*n])."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for s in range(num_series):
+        n = int(rng.choice(sizes))
+        spec = LatticeSpec("hex" if rng.random() < 0.5 else "square", float(rng.uniform(8, 16)), 1.8, 0.6, 1.0,
+                           float(rng.uniform(20, 100)), 3.0, 0.5)
+        fr, _, _ = make_series(n, frames_per_series + 1, spec, seed=seed + 100 * s)
+        out.append((fr[0].reshape(-1).copy(), fr[1:].reshape(frames_per_series, -1).copy()))
+    return out
+
+
 def psnr(a: np.ndarray, b: np.ndarray) -> float:
     """Peak signal-to-noise ratio of a against b, peak = range of b."""
     mse = float(np.mean((a - b) ** 2))
