@@ -13,9 +13,9 @@
 // Every data-parallel pass of an instance is cut into node tiles, and one
 // persistent grid of CTAs (two per SM) executes the tiles of all instances
 // through a task scheduler (end of this file): tiles are handed out in
-// chunks, and whoever completes the last chunk of a pass reduces the
-// per-chunk partial sums in chunk order and takes the instance's next control
-// decision.  Control flow is bounded: the step
+// chunks, every tile stores its partial sums, and whoever completes the last
+// chunk of a pass adds them in tile order and takes the instance's next
+// control decision.  Control flow is bounded: the step
 // loop by max_iter, each line search by the tau range [2^-30, 2^25], every
 // wait for work by an iteration limit.
 //
@@ -1072,9 +1072,10 @@ __device__ __forceinline__ bool finite_d(double x) { return !isnan(x) && !isinf(
 // gradient, V-cycle down per level, coarse V-cycle, V-cycle up per level,
 // NCG + first Armijo trial, further trials, final flush).  Every pass is cut
 // into tiles.  All CTAs of the launch pull chunks of tiles from whichever
-// instance has a published pass with chunks left; the CTA that completes the
-// last chunk of a pass reduces the per-chunk partial sums in chunk order (so every total is
-// independent of which CTA did what), runs the instance's descent control
+// instance has a published pass with chunks left; every tile stores its own
+// partial sums, and the CTA that completes the last chunk of a pass adds them
+// in tile order (so every total is independent of which CTA did what and of
+// the chunking), runs the instance's descent control
 // (gradientDescent.h / ArmijoSearch.h) and publishes the next pass.  No CTA
 // ever waits for a particular other CTA, so uneven SM sharing, slow tiles and
 // the single-CTA coarse V-cycle of one instance are hidden by the work of the
