@@ -1296,3 +1296,203 @@ void msor_match_series(int data_term, int level, int start, int stop, double lam
   }
   free(target); free(R); free(Rprev); free(T); free(cur); free(acc); free(tmp);
 }
+
+/* --- the seismic line-shift data term --------------------------------------- */
+/* FELineShiftRegisEnergy (registration.h:2137-2193): per line y of an nx x ny
+ * image, the 1-D NormalizedCrossCorrelationEnergy (registration.h:1909-1983)
+ * of the reference line and the template line under the line's displacement,
+ * on RectangularGridConfigurator<double, QC_1D, Gauss 3> (configurators.h:
+ * 746-820): nodes 0..nx-1, h = 1/(nx-1), two Gauss points, assembled 1-D
+ * mass matrix (DiagBandMatrix<.,1,1>, diagBandMatrix.cpp:123-160).  Lines
+ * whose first reference or template value is NaN are skipped; the energy is
+ * the sum over lines divided by ny, the derivative of each line too.      */
+typedef struct {
+  int n;
+  double h, vol;
+  double bq[2][2];   /* basis b at Gauss point q */
+  double band[0];
+} line1d_t;
+
+static line1d_t* line1d_new(int n) {
+  line1d_t* L = (line1d_t*)calloc(1, sizeof(line1d_t) + sizeof(double) * 3 * (size_t)n);
+  L->n = n;
+  L->h = 1. / (double)(n - 1);
+  L->vol = L->h;
+  const double g[2] = {GP0, GP1};
+  for (int q = 0; q < 2; ++q) { L->bq[0][q] = 1. - g[q]; L->bq[1][q] = g[q]; }
+  double M[2][2] = {{0., 0.}, {0., 0.}};
+  for (int q = 0; q < 2; ++q)
+    for (int i = 0; i < 2; ++i) {
+      const double bi = L->bq[i][q];
+      for (int j = i; j < 2; ++j) M[i][j] += bi * L->bq[j][q] * 1. * 0.5;
+    }
+  for (int i = 0; i < 2; ++i)
+    for (int j = i; j < 2; ++j) M[j][i] = M[i][j] = M[i][j] * L->vol;
+  for (int e = 0; e < n - 1; ++e)
+    for (int i = 0; i < 2; ++i)
+      for (int j = 0; j < 2; ++j) L->band[(size_t)(e + i) * 3 + (j - i + 1)] += 1.0 * M[i][j];
+  return L;
+}
+
+static void line1d_mass(const line1d_t* L, const double* u, double* out) {
+  const int n = L->n;
+  for (int i = 0; i < n; ++i) {
+    double r = 0.;
+    for (int j = (i > 0 ? i - 1 : 0); j <= (i < n - 1 ? i + 1 : n - 1); ++j) r += L->band[(size_t)i * 3 + (j - i + 1)] * u[j];
+    out[i] = r;
+  }
+}
+
+static double line1d_normalize(const line1d_t* L, const double* img, double* out, double* tmp) {
+  const int n = L->n;
+  line1d_mass(L, img, tmp);
+  double mean = 0.;
+  for (int i = 0; i < n; ++i) mean += tmp[i];
+  for (int i = 0; i < n; ++i) { out[i] = img[i]; out[i] += -mean; }
+  line1d_mass(L, out, tmp);
+  const double var = sqrt(dot(out, tmp, n));
+  if (!(fabs(var - 0.) < 1e-15))
+    for (int i = 0; i < n; ++i) out[i] /= var;
+  return var;
+}
+
+/* doFastDeformImage<., QC_1D> (deformations.h:111-137) with
+ * Vector::interpolate (vec.h:461-472) */
+static void line1d_deform(const line1d_t* L, const double* img, const double* phi, double* out) {
+  const int n = L->n;
+  for (int i = 0; i < n; ++i) {
+    double ds = i + phi[i] / L->h;
+    ds = ds < 0. ? 0. : (ds > (double)(n - 1) ? (double)(n - 1) : ds);
+    const int p = (int)ds;
+    const double pf = ds - p;
+    out[i] = (p == n - 1) ? img[p] : (1 - pf) * img[p] + pf * img[p + 1];
+  }
+}
+
+static double line1d_energy(const line1d_t* L, const double* normR, const double* T, const double* phi, double* var,
+                            double* normT, double* w1, double* w2) {
+  const int n = L->n;
+  line1d_deform(L, T, phi, w1);
+  *var = line1d_normalize(L, w1, normT, w2);
+  line1d_mass(L, normT, w1);
+  return -dot(w1, normR, n);
+}
+
+/* VariationOfNormalizedCrossCorrelationEnergy::apply on one line: the energy,
+ * then CrossCorrelationForce (registration.h:1828-1862) integrated like
+ * FENonlinVectorOpInterface::applyAdd (FEOpInterface.h:1803-1852). */
+static void line1d_variation(const line1d_t* L, const double* normR, const double* T, const double* phi, double* dy,
+                             double* w1, double* w2, double* normT, double* temp) {
+  const int n = L->n;
+  double var;
+  const double energy = line1d_energy(L, normR, T, phi, &var, normT, w1, w2);
+  for (int i = 0; i < n; ++i) temp[i] = normR[i];
+  for (int i = 0; i < n; ++i) temp[i] += normT[i] * energy;
+  if (!(fabs(var - 0.) < 1e-15))
+    for (int i = 0; i < n; ++i) temp[i] /= var;
+  const double g[2] = {GP0, GP1};
+  for (int i = 0; i < n; ++i) dy[i] = 0.;
+  for (int e = 0; e < n - 1; ++e) {
+    double nl[2];
+    for (int q = 0; q < 2; ++q) {
+      double off = 0.;
+      off += phi[e] * L->bq[0][q];
+      off += phi[e + 1] * L->bq[1][q];
+      const double tc = ((double)e + g[q]) + off / L->h;
+      int el = (short)tc;
+      double loc = tc - el;
+      if (el == n - 1 && loc == 0) { el = n - 2; loc = 1; }
+      if (tc < 0. || el < 0 || el >= n - 1) { nl[q] = 0.; continue; }
+      double gr = 0.;
+      double v = -1. / L->h;
+      v *= T[el];
+      gr += v;
+      v = 1. / L->h;
+      v *= T[el + 1];
+      gr += v;
+      double tq = 0.;
+      tq += temp[e] * L->bq[0][q];
+      tq += temp[e + 1] * L->bq[1][q];
+      nl[q] = gr * -tq;
+    }
+    for (int b = 0; b < 2; ++b) {
+      double a = 0.;
+      for (int q = 0; q < 2; ++q) a += nl[q] * (L->bq[b][q] * 0.5);
+      dy[e + b] += L->vol * a;
+    }
+  }
+}
+
+double msor_lineshift(int nx, int ny, const double* R, const double* T, const double* phix, double* de) {
+  line1d_t* L = line1d_new(nx);
+  double* normR = (double*)malloc(sizeof(double) * nx);
+  double* w1 = (double*)malloc(sizeof(double) * nx);
+  double* w2 = (double*)malloc(sizeof(double) * nx);
+  double* w3 = (double*)malloc(sizeof(double) * nx);
+  double* w4 = (double*)malloc(sizeof(double) * nx);
+  double e = 0.;
+  if (de) memset(de, 0, sizeof(double) * (size_t)nx * ny);
+  for (int y = 0; y < ny; ++y) {
+    const double* r = R + (size_t)y * nx;
+    const double* t = T + (size_t)y * nx;
+    const double* p = phix + (size_t)y * nx;
+    if (isnan(r[0]) || isnan(t[0])) continue;
+    line1d_normalize(L, r, normR, w1);
+    double var;
+    e += line1d_energy(L, normR, t, p, &var, w3, w1, w2);
+    if (de) {
+      double* dy = de + (size_t)y * nx;
+      line1d_variation(L, normR, t, p, dy, w1, w2, w3, w4);
+      for (int i = 0; i < nx; ++i) dy[i] /= ny;
+    }
+  }
+  e /= ny;
+  free(L); free(normR); free(w1); free(w2); free(w3); free(w4);
+  return e;
+}
+
+/* The regulariser of findXShift for laplaceWeight <= 0 (matchSeries.h:
+ * 819-845): K = stiffX + yRegFactor * stiffY, FEOpMixedDerivative
+ * (FEOpInterface.h:1075-1135) with local matrices
+ * L[i][j] += 1 * g_i[s] * g_j[t] * w, times vol = h^2, assembled element by
+ * element into the nine-point band matrix (stiffX first, then stiffY with the
+ * factor), on the nx x ny rectangular grid with h = 1/(max(nx,ny)-1);
+ * E = 1/2 phi.(K phi) (QuadraticFormOp, op.h:1410-1429).  Returns E, Kphi out. */
+double msor_xshift_reg(int nx, int ny, double yreg, const double* phi, double* kphi) {
+  const double h = 1. / (double)((nx > ny ? nx : ny) - 1);
+  const double vol = sqr(h);
+  quad_t Q;
+  quad_init(&Q, h);
+  double* st = (double*)calloc((size_t)nx * ny * 9, sizeof(double));
+  for (int pass = 0; pass < 2; ++pass) {
+    const int s = pass;  /* stiffX: s = t = 0; stiffY: s = t = 1 */
+    const double factor = pass == 0 ? 1.0 : yreg;
+    double L[4][4];
+    for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) L[i][j] = 0.;
+    for (int q = 0; q < 4; ++q)
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) L[i][j] += 1. * Q.gq[i][q][s] * Q.gq[j][q][s] * Q.w;
+    for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) L[i][j] *= vol;
+    for (int ey = 0; ey < ny - 1; ++ey)
+      for (int ex = 0; ex < nx - 1; ++ex)
+        for (int i = 0; i < 4; ++i)
+          for (int j = 0; j < 4; ++j) {
+            const int gi = ex + ey * nx + ((i & 1) ? 1 : 0) + ((i & 2) ? nx : 0);
+            const int gj = ex + ey * nx + ((j & 1) ? 1 : 0) + ((j & 2) ? nx : 0);
+            const int dx = (gj % nx) - (gi % nx), dy = (gj / nx) - (gi / nx);
+            st[(size_t)gi * 9 + (dy + 1) * 3 + (dx + 1)] += factor * L[i][j];
+          }
+  }
+  for (int r = 0; r < nx * ny; ++r) {
+    const int x = r % nx, y = r / nx;
+    double d = 0.;
+    for (int j = -1; j <= 1; ++j)
+      for (int i = -1; i <= 1; ++i) {
+        const int X = x + i, Y = y + j;
+        if (X >= 0 && X < nx && Y >= 0 && Y < ny) d += st[(size_t)r * 9 + (j + 1) * 3 + (i + 1)] * phi[X + Y * nx];
+      }
+    kphi[r] = d;
+  }
+  free(st);
+  return 0.5 * dot(kphi, phi, nx * ny);
+}

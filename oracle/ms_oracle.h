@@ -138,6 +138,14 @@ int    msor_compose(int level, const double* d1x, const double* d1y, const doubl
  * matchSeries.h:442; multiVector.cpp:99-117), fill where none            */
 void   msor_warp_median(int level, int F, const double* frames, const double* phis, double fill,
                         double* median);
+/* The seismic model's line-shift data term (FELineShiftRegisEnergy,
+ * registration.h:2137-2193): the mean over the ny lines of the 1-D NCC energy
+ * of each reference line against its template line shifted by phix along x
+ * (units of the line grid, h = 1/(nx-1)); de (nullable) its derivative.    */
+double msor_lineshift(int nx, int ny, const double* R, const double* T, const double* phix, double* de);
+/* findXShift's regulariser (laplaceWeight <= 0): K = stiffX + yreg * stiffY
+ * on the nx x ny grid; returns 1/2 phi.K phi, K phi into kphi.             */
+double msor_xshift_reg(int nx, int ny, double yreg, const double* phi, double* kphi);
 /* matchSeries<>() with accumulated deformations, refinement and extra stages
  * (matchSeries.h:87-265, 353-445, 1250-1320); see ms_oracle.c.             */
 void   msor_match_series(int data_term, int level, int start, int stop, double lambda,

@@ -43,6 +43,8 @@ def lib():
         L.msor_register.restype = ctypes.c_double
         L.msor_gd_level.restype = ctypes.c_int
         L.msor_ncc_energy.restype = ctypes.c_double
+        L.msor_lineshift.restype = ctypes.c_double
+        L.msor_xshift_reg.restype = ctypes.c_double
         L.msor_energy_dt.restype = ctypes.c_double
         L.msor_register_dt.restype = ctypes.c_double
         L.msor_gd_level_dt.restype = ctypes.c_int
@@ -182,6 +184,23 @@ def compose(level, d1, d2, init=None, with_iterations=False):
     return (res, int(its)) if with_iterations else res
 
 
+def lineshift(R, T, phix):
+    """The seismic line-shift data term and its derivative; R, T, phix (ny, nx)."""
+    R = _c(R)
+    ny, nx = R.shape
+    de = np.zeros((ny, nx))
+    e = lib().msor_lineshift(nx, ny, _p(R.reshape(-1)), _p(_c(T).reshape(-1)), _p(_c(phix).reshape(-1)), _p(de))
+    return float(e), de
+
+
+def xshift_reg(phix, yreg):
+    """findXShift's regulariser: (1/2 phi.K phi, K phi) for phix (ny, nx)."""
+    ny, nx = phix.shape
+    k = np.zeros((ny, nx))
+    e = lib().msor_xshift_reg(nx, ny, ctypes.c_double(yreg), _p(_c(phix).reshape(-1)), _p(k))
+    return float(e), k
+
+
 def warp_median(level, frames, phis, fill):
     N = n_of(level) ** 2
     out = np.zeros(N)
@@ -287,6 +306,18 @@ class RefRunner:
         self.run("median", level, frames.shape[0], self._w("fr", frames), self._w("ph", phis), repr(float(fill)),
                  os.path.join(self.dir, "out"))
         return self._r("out")
+
+    def lineshift(self, R, T, phix):
+        ny, nx = R.shape
+        self.run("lineshift", nx, ny, self._w("R", R), self._w("T", T), self._w("px", phix),
+                 os.path.join(self.dir, "e"), os.path.join(self.dir, "de"))
+        return float(self._r("e")[0]), self._r("de").reshape(ny, nx)
+
+    def xshift_reg(self, phix, yreg):
+        ny, nx = phix.shape
+        self.run("xshiftreg", nx, ny, repr(float(yreg)), self._w("px", phix), os.path.join(self.dir, "e"),
+                 os.path.join(self.dir, "k"))
+        return float(self._r("e")[0]), self._r("k").reshape(ny, nx)
 
     def save_array(self, a, path, type_):
         """qc::ScalarArray<QC_2D>::save of a (numY, numX) array to path."""

@@ -360,6 +360,7 @@ static int usage ( ) {
     "ms_ref normalize L in sat minToZero out\n"
     "ms_ref compose L d1 d2 inout | median L F frames phis fill out\n"
     "ms_ref save nx ny in out type | load file out dims | savedef L in mask | loaddef L mask out\n"
+    "ms_ref lineshift nx ny R T phix outE outDE | xshiftreg nx ny yRegFactor phix outE outKphi\n"
     "ms_ref series[_ncc] maxL start stop lambda lambdaFactor maxIter stopEps sat minToZero F framesBin outPhis outMean outTxt\n"
     "ms_ref matchseries[_ncc] maxL start stop lambda lambdaFactor maxIter stopEps sat minToZero refineStart refineStop\n"
     "       extraStages extraLambdaFactor useMedian F framesBin outPrefix\n" );
@@ -503,6 +504,49 @@ int main ( int argc, char **argv ) {
         memcpy ( &buf[0], phi[0].getData ( ), N * sizeof ( RealType ) ); memcpy ( &buf[N], phi[1].getData ( ), N * sizeof ( RealType ) );
         writeBin ( argv[4], &buf[0], 2 * N );
       }
+      return 0;
+    }
+    if ( cmd == "lineshift" && argc == 9 ) {
+      // ms_ref lineshift nx ny R T phix outE outDE: FELineShiftRegisEnergy (registration.h:2137-2193), the data
+      // term of the seismic model (matchSeismicSeries.cpp), with its derivative, on the rectangular grid
+      typedef qc::RectangularGridConfigurator<RealType, qc::QC_2D, aol::GaussQuadrature<RealType, qc::QC_2D, 3> > RectConf;
+      typedef qc::RectangularGridConfigurator<RealType, qc::QC_1D, aol::GaussQuadrature<RealType, qc::QC_1D, 3> > RectConf1D;
+      typedef qc::FELineShiftRegisEnergy<RectConf, RectConf1D, qc::NCCRegistrationConfigurator<RectConf1D> > LineEnergy;
+      const int nx = atoi ( argv[2] ), ny = atoi ( argv[3] ), N = nx * ny;
+      ArrayType R ( nx, ny ), T ( nx, ny );
+      readBin ( argv[4], R.getData ( ), N ); readBin ( argv[5], T.getData ( ), N );
+      const RectConf::InitType grid ( qc::GridSize<qc::QC_2D>::createFrom ( R ) );
+      aol::Vector<RealType> phi ( N ), de ( N );
+      readBin ( argv[6], phi.getData ( ), N );
+      LineEnergy E ( grid, R, T );
+      aol::Scalar<RealType> e;
+      E.apply ( phi, e );
+      const aol::DerivativeWrapper<RealType, LineEnergy, aol::Vector<RealType> > DE ( E );
+      DE.apply ( phi, de );
+      writeBin ( argv[7], &e[0], 1 );
+      writeBin ( argv[8], de.getData ( ), N );
+      return 0;
+    }
+    if ( cmd == "xshiftreg" && argc == 8 ) {
+      // ms_ref xshiftreg nx ny yRegFactor phix outE outKphi: the regulariser of findXShift with laplaceWeight <= 0
+      // (matchSeries.h:819-845): K = stiffX + yRegFactor * stiffY assembled, E = 1/2 phi.K phi, and K phi
+      typedef qc::RectangularGridConfigurator<RealType, qc::QC_2D, aol::GaussQuadrature<RealType, qc::QC_2D, 3> > RectConf;
+      const int nx = atoi ( argv[2] ), ny = atoi ( argv[3] ), N = nx * ny;
+      ArrayType dummy ( nx, ny );
+      const RectConf::InitType grid ( qc::GridSize<qc::QC_2D>::createFrom ( dummy ) );
+      const aol::FEOpMixedDerivative<RectConf> stiffX ( grid, 0, 0, aol::ONTHEFLY );
+      const aol::FEOpMixedDerivative<RectConf> stiffY ( grid, 1, 1, aol::ONTHEFLY );
+      RectConf::MatrixType K ( grid );
+      stiffX.assembleAddMatrix ( K );
+      stiffY.assembleAddMatrix ( K, atof ( argv[4] ) );
+      const aol::QuadraticFormOp<aol::Vector<RealType> > EReg ( K );
+      aol::Vector<RealType> phi ( N ), kphi ( N );
+      readBin ( argv[5], phi.getData ( ), N );
+      aol::Scalar<RealType> e;
+      EReg.apply ( phi, e );
+      K.apply ( phi, kphi );
+      writeBin ( argv[6], &e[0], 1 );
+      writeBin ( argv[7], kphi.getData ( ), N );
       return 0;
     }
     if ( cmd == "compose" && argc == 7 ) {

@@ -234,10 +234,35 @@ def io_files(ref: msor.RefRunner, seed: int):
     np.savez_compressed(os.path.join(OUT, "io_expected.npz"), **expected)
 
 
+def seismic(ref: msor.RefRunner, seed: int):
+    """The seismic model's energy pieces (matchSeismicSeries): the line-shift
+    NCC data term with its derivative on a non-square grid (one NaN line that
+    is skipped, displacements that push points off their line), and the
+    anisotropic regulariser of findXShift."""
+    rng = np.random.default_rng(seed)
+    d = {}
+    for tag, (nx, ny) in (("a", (65, 9)), ("b", (40, 6))):
+        x = np.arange(nx)
+        R = np.stack([np.sin(x / 3.0 + k) + 0.1 * rng.normal(size=nx) for k in range(ny)])
+        T = np.stack([np.sin((x - 1.3) / 3.0 + k) + 0.1 * rng.normal(size=nx) for k in range(ny)])
+        phi = rng.normal(0, 1.5 / (nx - 1), (ny, nx))
+        phi[0, :3] = -5.0 / (nx - 1)
+        if tag == "a":
+            R[4, :] = np.nan
+        e, de = ref.lineshift(R, T, phi)
+        ereg, kphi = ref.xshift_reg(phi, 0.3 if tag == "a" else 2.0)
+        d.update({f"R_{tag}": R, f"T_{tag}": T, f"phi_{tag}": phi, f"E_{tag}": e, f"DE_{tag}": de,
+                  f"yreg_{tag}": 0.3 if tag == "a" else 2.0, f"Ereg_{tag}": ereg, f"Kphi_{tag}": kphi})
+    np.savez_compressed(os.path.join(OUT, "seismic.npz"), **d)
+
+
 def main():
     if not msor.have_ref():
         raise SystemExit("oracle/_ref/ms_ref is missing: make -f oracle/Makefile.ref")
     ref = msor.RefRunner()
+    if "--seismic-only" in sys.argv:
+        seismic(ref, 801)
+        return
     if "--io-only" in sys.argv:
         io_files(ref, 701)
         return
@@ -264,6 +289,7 @@ def main():
     match_series(ref, 6, 4, 602)
     match_series_conditioned(ref, 6, 4, 623)
     io_files(ref, 701)
+    seismic(ref, 801)
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(OUT, f)))
