@@ -134,6 +134,28 @@ int msgpu_register_ragged(msgpu_context* ctx, const msgpu_params* p, const msgpu
 int msgpu_register_ragged_device(msgpu_context* ctx, const msgpu_params* p, const msgpu_series_desc* series,
                                  int num_series, void* stream);
 
+/* --- the seismic line-shift model (matchSeismicSeries): its energy --------
+ * Images are nx x ny doubles, x fastest; displacements shift along x in the
+ * units of a line (h = 1/(nx-1)), as findXShift passes them
+ * (matchSeries.h:860-864).                                                   */
+/* FELineShiftRegisEnergy (registration.h:2137-2193): the mean over the lines
+ * of the 1-D normalized cross-correlation of each reference line and its
+ * template line shifted by phix (lines whose first reference or template
+ * value is NaN are skipped); de_out (nullable): its derivative.            */
+int msgpu_lineshift_energy(msgpu_context* ctx, int nx, int ny, const double* R, const double* T, const double* phix,
+                           double* energy_out, double* de_out);
+/* num_images images back to back, one energy each; device pointers.      */
+int msgpu_lineshift_energy_device(msgpu_context* ctx, int nx, int ny, int num_images, const double* d_R,
+                                  const double* d_T, const double* d_phix, double* d_energy_out, double* d_de_out,
+                                  void* stream);
+/* findXShift's regulariser with laplaceWeight <= 0 (matchSeries.h:819-845):
+ * K = stiffX + yreg * stiffY on the nx x ny grid (h = 1/(max(nx,ny)-1)),
+ * energy 1/2 phix.K phix and K phix.                                       */
+int msgpu_xshift_reg(msgpu_context* ctx, int nx, int ny, double yreg, const double* phix, double* energy_out,
+                     double* kphi_out);
+int msgpu_xshift_reg_device(msgpu_context* ctx, int nx, int ny, int num_images, double yreg, const double* d_phix,
+                            double* d_energy_out, double* d_kphi_out, void* stream);
+
 /* --- series pipeline ------------------------------------------------------ */
 /* Options of matchSeries<>() beyond the registration keys (parameter-file
  * names of the reference).                                                  */

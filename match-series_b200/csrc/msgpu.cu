@@ -24,6 +24,7 @@
 #include "../../include/msgpu.h"
 #include "msgpu_level.cuh"
 #include "msgpu_series.cuh"
+#include "msgpu_seismic.cuh"
 
 using namespace msg;
 
@@ -1614,6 +1615,170 @@ int msgpu_register_ragged(msgpu_context* ctx, const msgpu_params* p, const msgpu
   }
   CK(cudaStreamSynchronize(st));
   return sched_error_check(ctx);
+}
+
+namespace {
+// The 1-D mass band of a line of n nodes, assembled in element order as
+// MassOp<RectangularGridConfigurator<., QC_1D, Gauss 3>> does (h = 1/(n-1)).
+LineTables host_line_tables(int n) {
+  LineTables t;
+  t.h = 1. / (double)(n - 1);
+  t.g[0] = 0.2113248654051871;
+  t.g[1] = 0.7886751345948129;
+  for (int q = 0; q < 2; ++q) { t.bq[0][q] = 1. - t.g[q]; t.bq[1][q] = t.g[q]; }
+  double M[2][2] = {{0., 0.}, {0., 0.}};
+  for (int q = 0; q < 2; ++q)
+    for (int i = 0; i < 2; ++i) {
+      const double bi = t.bq[i][q];
+      for (int j = i; j < 2; ++j) M[i][j] += bi * t.bq[j][q] * 1. * 0.5;
+    }
+  for (int i = 0; i < 2; ++i)
+    for (int j = i; j < 2; ++j) M[j][i] = M[i][j] = M[i][j] * t.h;
+  double band[4][3] = {};
+  for (int e = 0; e < 3; ++e)
+    for (int i = 0; i < 2; ++i)
+      for (int j = 0; j < 2; ++j) band[e + i][j - i + 1] += 1.0 * M[i][j];
+  t.d0 = band[0][1];
+  t.u0 = band[0][2];
+  t.l = band[1][0];
+  t.d = band[1][1];
+  t.u = band[1][2];
+  t.ln = band[3][0];
+  t.dn = band[3][1];
+  return t;
+}
+
+// Nine-point rows of K = stiffX + yreg * stiffY (FEOpMixedDerivative) for
+// h = 1/(max(nx,ny)-1), assembled on a 5 x 5 node patch in element order.
+XRegTables host_xreg_tables(int nx, int ny, double yreg) {
+  const double h = 1. / (double)((nx > ny ? nx : ny) - 1), vol = h * h;
+  const double g[2] = {0.2113248654051871, 0.7886751345948129};
+  double rc[4][2];
+  for (int i = 0, k = 0; i < 2; ++i)
+    for (int j = 0; j < 2; ++j, ++k) { rc[k][0] = g[i]; rc[k][1] = g[j]; }
+  double gq[4][4][2];
+  for (int b = 0; b < 4; ++b)
+    for (int q = 0; q < 4; ++q) host_basis_grad(b, rc[q][0], rc[q][1], h, gq[b][q]);
+  const int n = 5;
+  std::vector<double> st((size_t)n * n * 9, 0.0);
+  for (int pass = 0; pass < 2; ++pass) {
+    const int sd = pass;
+    const double factor = pass == 0 ? 1.0 : yreg;
+    double L[4][4] = {};
+    for (int q = 0; q < 4; ++q)
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) L[i][j] += 1. * gq[i][q][sd] * gq[j][q][sd] * 0.25;
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j) L[i][j] *= vol;
+    for (int ey = 0; ey < n - 1; ++ey)
+      for (int ex = 0; ex < n - 1; ++ex)
+        for (int i = 0; i < 4; ++i)
+          for (int j = 0; j < 4; ++j) {
+            const int gi = ex + ey * n + ((i & 1) ? 1 : 0) + ((i & 2) ? n : 0);
+            const int gj = ex + ey * n + ((j & 1) ? 1 : 0) + ((j & 2) ? n : 0);
+            const int dx = (gj % n) - (gi % n), dy = (gj / n) - (gi / n);
+            st[(size_t)gi * 9 + (dy + 1) * 3 + (dx + 1)] += factor * L[i][j];
+          }
+  }
+  XRegTables tb;
+  const int rep[3] = {0, 2, 4};
+  for (int cy = 0; cy < 3; ++cy)
+    for (int cx = 0; cx < 3; ++cx)
+      for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) tb.st[cx + 3 * cy][j][i] = st[(size_t)(rep[cx] + rep[cy] * n) * 9 + j * 3 + i];
+  return tb;
+}
+}  // namespace
+
+int msgpu_lineshift_energy_device(msgpu_context* ctx, int nx, int ny, int num_images, const double* d_R,
+                                  const double* d_T, const double* d_phix, double* d_energy_out, double* d_de_out,
+                                  void* stream) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (nx < 2 || ny < 1 || num_images < 1 || !d_R || !d_T || !d_phix || !d_energy_out)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid lineshift arguments");
+  const size_t smem = sizeof(double) * 3 * (size_t)nx;
+  if (smem > 200 * 1024) return fail(ctx, MSGPU_ERR_SIZE, "lines of %d samples do not fit shared memory", nx);
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  if ((rc = ensure(ctx, ctx->nccbuf, sizeof(double) * (size_t)ny * num_images + 64))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  LineArgs a;
+  a.nx = nx;
+  a.ny = ny;
+  a.img_stride = (size_t)nx * ny;
+  a.R = d_R;
+  a.T = d_T;
+  a.phi = d_phix;
+  a.e_line = (double*)ctx->nccbuf.p;
+  a.de = d_de_out;
+  a.t = host_line_tables(nx);
+  CK(cudaFuncSetAttribute(k_lineshift, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_lineshift<<<dim3(ny, num_images), kLineThreads, smem, st>>>(a);
+  k_lineshift_total<<<(num_images + 127) / 128, 128, 0, st>>>(a.e_line, ny, num_images, d_energy_out);
+  CK(cudaGetLastError());
+  ctx->stats.kernel_launches = 2;
+  return MSGPU_OK;
+}
+
+int msgpu_lineshift_energy(msgpu_context* ctx, int nx, int ny, const double* R, const double* T, const double* phix,
+                           double* energy_out, double* de_out) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (nx < 2 || ny < 1 || !R || !T || !phix || !energy_out)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid lineshift arguments");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  const size_t N = (size_t)nx * ny;
+  if ((rc = ensure(ctx, ctx->io[0], sizeof(double) * (4 * N + 8)))) return rc;
+  double* d = (double*)ctx->io[0].p;
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(d, R, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d + N, T, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d + 2 * N, phix, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+  if ((rc = msgpu_lineshift_energy_device(ctx, nx, ny, 1, d, d + N, d + 2 * N, d + 4 * N, de_out ? d + 3 * N : nullptr,
+                                          st)))
+    return rc;
+  CK(cudaMemcpyAsync(energy_out, d + 4 * N, sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (de_out) CK(cudaMemcpyAsync(de_out, d + 3 * N, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return MSGPU_OK;
+}
+
+int msgpu_xshift_reg_device(msgpu_context* ctx, int nx, int ny, int num_images, double yreg, const double* d_phix,
+                            double* d_energy_out, double* d_kphi_out, void* stream) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (nx < 3 || ny < 3 || num_images < 1 || !d_phix || !d_energy_out || !d_kphi_out)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid xshift_reg arguments (grids of at least 3 x 3 nodes)");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  const int N = nx * ny;
+  const int nb = std::min(1024, (N + 255) / 256);
+  if ((rc = ensure(ctx, ctx->vals, sizeof(double) * (size_t)nb * num_images + 64))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  k_xshift_reg<<<dim3(nb, num_images), 256, 0, st>>>(host_xreg_tables(nx, ny, yreg), nx, ny, (size_t)N, d_phix,
+                                                     d_kphi_out, (double*)ctx->vals.p);
+  k_xshift_reg_total<<<(num_images + 127) / 128, 128, 0, st>>>((const double*)ctx->vals.p, nb, num_images,
+                                                               d_energy_out);
+  CK(cudaGetLastError());
+  ctx->stats.kernel_launches = 2;
+  return MSGPU_OK;
+}
+
+int msgpu_xshift_reg(msgpu_context* ctx, int nx, int ny, double yreg, const double* phix, double* energy_out,
+                     double* kphi_out) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (!phix || !energy_out || !kphi_out) return fail(ctx, MSGPU_ERR_INVALID_ARG, "null buffer");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  const size_t N = (size_t)nx * ny;
+  if ((rc = ensure(ctx, ctx->io[0], sizeof(double) * (2 * N + 8)))) return rc;
+  double* d = (double*)ctx->io[0].p;
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(d, phix, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+  if ((rc = msgpu_xshift_reg_device(ctx, nx, ny, 1, yreg, d, d + 2 * N, d + N, st))) return rc;
+  CK(cudaMemcpyAsync(energy_out, d + 2 * N, sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(kphi_out, d + N, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return MSGPU_OK;
 }
 
 void msgpu_series_params_default(const msgpu_params* p, msgpu_series_params* s) {

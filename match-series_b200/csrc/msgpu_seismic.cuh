@@ -1,0 +1,228 @@
+// msgpu_seismic.cuh -- the energy of the seismic line-shift model
+// (matchSeismicSeries): the data term FELineShiftRegisEnergy
+// (registration.h:2137-2193), a 1-D normalized cross-correlation per image
+// line under a shift of the line along x, and the anisotropic regulariser of
+// findXShift (matchSeries.h:819-845), K = stiffX + yRegFactor * stiffY.
+//
+// k_lineshift: one CTA per line (blockIdx.x) and image (blockIdx.y); the
+// line's reference, deformed template and work vectors live in shared memory.
+// The three global sums of a line (mass-weighted mean, norm, correlation) are
+// fixed-order block reductions; everything else follows the reference's
+// arithmetic step by step (the 1-D mass band assembled on the host in element
+// order, FastDeformImage with Vector::interpolate, CrossCorrelationForce at the
+// two Gauss points of each element, node sums in element order).
+#pragma once
+
+#include "msgpu_level.cuh"
+
+namespace msg {
+
+constexpr int kLineThreads = 256;
+
+// Assembled 1-D mass band (DiagBandMatrix<.,1,1>) of a line of n nodes:
+// row 0 (d0, u0), interior rows (l, d, u), row n-1 (ln, dn); Gauss points
+// and basis values; h = 1/(n-1).
+struct LineTables {
+  double d0, u0, l, d, u, ln, dn;
+  double h;
+  double g[2];
+  double bq[2][2];
+};
+
+struct LineArgs {
+  int nx, ny;
+  size_t img_stride;           // elements between images
+  const double* R;
+  const double* T;
+  const double* phi;
+  double* e_line;              // ny per image
+  double* de;                  // nullable: nx*ny per image
+  LineTables t;
+};
+
+__device__ __forceinline__ double line_block_sum(double v, double* red) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int w = 0; w < kLineThreads / 32; ++w) s += red[w];
+  return s;
+}
+
+__device__ __forceinline__ double line_mass_row(const LineTables& t, const double* u, int i, int n) {
+  double r = 0.;
+  if (i == 0) {
+    r += t.d0 * u[0];
+    r += t.u0 * u[1];
+  } else if (i == n - 1) {
+    r += t.ln * u[n - 2];
+    r += t.dn * u[n - 1];
+  } else {
+    r += t.l * u[i - 1];
+    r += t.d * u[i];
+    r += t.u * u[i + 1];
+  }
+  return r;
+}
+
+// normalizeImageForNCC on a line in shared memory: v <- (v - mean)/norm,
+// returns the norm (tmp: scratch of n).
+__device__ double line_normalize(const LineTables& t, double* v, double* tmp, int n, double* red) {
+  double part = 0.0;
+  for (int i = threadIdx.x; i < n; i += kLineThreads) part += line_mass_row(t, v, i, n);
+  const double mean = line_block_sum(part, red);
+  for (int i = threadIdx.x; i < n; i += kLineThreads) v[i] += -mean;
+  __syncthreads();
+  part = 0.0;
+  for (int i = threadIdx.x; i < n; i += kLineThreads) part += v[i] * line_mass_row(t, v, i, n);
+  const double var = sqrt(line_block_sum(part, red));
+  if (!(fabs(var - 0.) < 1e-15))
+    for (int i = threadIdx.x; i < n; i += kLineThreads) v[i] /= var;
+  __syncthreads();
+  (void)tmp;
+  return var;
+}
+
+__global__ void __launch_bounds__(kLineThreads) k_lineshift(LineArgs a) {
+  extern __shared__ double lsm[];
+  __shared__ double red[kLineThreads / 32];
+  const int n = a.nx, y = blockIdx.x;
+  const size_t base = (size_t)blockIdx.y * a.img_stride + (size_t)y * n;
+  const double* R = a.R + base;
+  const double* T = a.T + base;
+  const double* phi = a.phi + base;
+  double* nr = lsm;            // normalised reference line
+  double* nt = lsm + n;        // deformed, then normalised template line
+  double* tmp = lsm + 2 * n;   // (M nt), then the force weights
+  const LineTables& t = a.t;
+  if (isnan(R[0]) || isnan(T[0])) {
+    if (threadIdx.x == 0) a.e_line[(size_t)blockIdx.y * a.ny + y] = 0.0;
+    if (a.de)
+      for (int i = threadIdx.x; i < n; i += kLineThreads) a.de[base + i] = 0.0;
+    return;
+  }
+  for (int i = threadIdx.x; i < n; i += kLineThreads) {
+    nr[i] = R[i];
+    // doFastDeformImage<., QC_1D> (deformations.h:111-137), Vector::interpolate (vec.h:461-472)
+    double ds = i + phi[i] / t.h;
+    ds = ds < 0. ? 0. : (ds > (double)(n - 1) ? (double)(n - 1) : ds);
+    const int p = (int)ds;
+    const double pf = ds - p;
+    nt[i] = (p == n - 1) ? T[p] : (1 - pf) * T[p] + pf * T[p + 1];
+  }
+  __syncthreads();
+  line_normalize(t, nr, tmp, n, red);
+  const double var = line_normalize(t, nt, tmp, n, red);
+  double part = 0.0;
+  for (int i = threadIdx.x; i < n; i += kLineThreads) part += line_mass_row(t, nt, i, n) * nr[i];
+  const double energy = -line_block_sum(part, red);
+  if (threadIdx.x == 0) a.e_line[(size_t)blockIdx.y * a.ny + y] = energy;
+  if (!a.de) return;
+  // VariationOfNormalizedCrossCorrelationEnergy: temp = (normR + normT * E) / var
+  for (int i = threadIdx.x; i < n; i += kLineThreads) {
+    double v = nr[i];
+    v += nt[i] * energy;
+    if (!(fabs(var - 0.) < 1e-15)) v /= var;
+    tmp[i] = v;
+  }
+  __syncthreads();
+  // CrossCorrelationForce per element at its two Gauss points; node i takes
+  // element i-1 (as its right node) first, then element i (as its left node)
+  auto elem = [&](int e, int b) -> double {
+    double nl[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      double off = 0.;
+      off += phi[e] * t.bq[0][q];
+      off += phi[e + 1] * t.bq[1][q];
+      const double tc = ((double)e + t.g[q]) + off / t.h;
+      int el = (short)tc;
+      double loc = tc - el;
+      if (el == n - 1 && loc == 0) { el = n - 2; loc = 1; }
+      if (tc < 0. || el < 0 || el >= n - 1) { nl[q] = 0.; continue; }
+      double gr = 0.;
+      double v = -1. / t.h;
+      v *= T[el];
+      gr += v;
+      v = 1. / t.h;
+      v *= T[el + 1];
+      gr += v;
+      double tq = 0.;
+      tq += tmp[e] * t.bq[0][q];
+      tq += tmp[e + 1] * t.bq[1][q];
+      nl[q] = gr * -tq;
+    }
+    double acc = 0.;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) acc += nl[q] * (t.bq[b][q] * 0.5);
+    return t.h * acc;
+  };
+  for (int i = threadIdx.x; i < n; i += kLineThreads) {
+    double d = 0.;
+    if (i > 0) d += elem(i - 1, 1);
+    if (i < n - 1) d += elem(i, 0);
+    d /= a.ny;
+    a.de[base + i] = d;
+  }
+}
+
+// Sum of the line energies in line order, divided by the line count.
+__global__ void k_lineshift_total(const double* e_line, int ny, int num_images, double* out) {
+  const int img = blockIdx.x * blockDim.x + threadIdx.x;
+  if (img >= num_images) return;
+  double s = 0.;
+  for (int y = 0; y < ny; ++y) s += e_line[(size_t)img * ny + y];
+  out[img] = s / ny;
+}
+
+// findXShift's regulariser: K phi with the assembled nine-point rows of the
+// nine node classes (first / interior / last along x and y), and the partial
+// sums of phi . K phi per block for E = 1/2 phi.K phi.
+struct XRegTables {
+  double st[9][3][3];
+};
+
+__global__ void __launch_bounds__(256) k_xshift_reg(XRegTables tb, int nx, int ny, size_t img_stride,
+                                                    const double* phi, double* kphi, double* part) {
+  __shared__ double red[8];
+  const double* p = phi + (size_t)blockIdx.y * img_stride;
+  double* k = kphi + (size_t)blockIdx.y * img_stride;
+  const int N = nx * ny;
+  double acc = 0.0;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < N; r += gridDim.x * blockDim.x) {
+    const int x = r % nx, y = r / nx;
+    const int cls = (x == 0 ? 0 : (x == nx - 1 ? 2 : 1)) + 3 * (y == 0 ? 0 : (y == ny - 1 ? 2 : 1));
+    double d = 0.;
+#pragma unroll
+    for (int j = -1; j <= 1; ++j)
+#pragma unroll
+      for (int i = -1; i <= 1; ++i) {
+        const int X = x + i, Y = y + j;
+        if (X >= 0 && X < nx && Y >= 0 && Y < ny) d += tb.st[cls][j + 1][i + 1] * p[X + (size_t)Y * nx];
+      }
+    k[r] = d;
+    acc += d * p[r];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < 8; ++w) s += red[w];
+    part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+__global__ void k_xshift_reg_total(const double* part, int nblocks, int num_images, double* out) {
+  const int img = blockIdx.x * blockDim.x + threadIdx.x;
+  if (img >= num_images) return;
+  double s = 0.0;
+  for (int b = 0; b < nblocks; ++b) s += part[(size_t)img * nblocks + b];
+  out[img] = 0.5 * s;
+}
+
+}  // namespace msg

@@ -91,7 +91,8 @@ EXPORTS = [
     "msgpu_compose", "msgpu_compose_device", "msgpu_warp_median", "msgpu_warp_median_device",
     "msgpu_io_last_error", "msgpu_read_array", "msgpu_write_array", "msgpu_read_arrays", "msgpu_read_displacement",
     "msgpu_write_displacement", "msgpu_read_arrays_start", "msgpu_io_wait", "msgpu_register_ragged",
-    "msgpu_register_ragged_device",
+    "msgpu_register_ragged_device", "msgpu_lineshift_energy", "msgpu_lineshift_energy_device", "msgpu_xshift_reg",
+    "msgpu_xshift_reg_device",
 ]
 
 
@@ -159,6 +160,14 @@ def lib():
                                               ctypes.c_int, _dp, ctypes.c_int]
         L.msgpu_read_arrays_start.restype = ctypes.c_void_p
         L.msgpu_io_wait.argtypes = [ctypes.c_void_p]
+        L.msgpu_lineshift_energy.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp, _dp]
+        L.msgpu_lineshift_energy_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.msgpu_xshift_reg.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp]
+        L.msgpu_xshift_reg_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.c_void_p]
         L.msgpu_register_ragged.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params), ctypes.POINTER(SeriesDesc),
                                             ctypes.c_int]
         L.msgpu_register_ragged_device.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params),
@@ -341,6 +350,26 @@ class Context:
         self._check(lib().msgpu_match_series_stage_device(self._h, ctypes.byref(params), d_ref, d_templates,
                                                           num_templates, d_phis, d_energies or None, d_steps or None,
                                                           d_mean, d_count, stream or None))
+
+    # --- seismic line-shift model ---------------------------------------------
+    def lineshift_energy(self, R, T, phix, with_derivative=True):
+        """FELineShiftRegisEnergy of (ny, nx) images; returns (E, DE or None)."""
+        R = _f64(R)
+        ny, nx = R.shape
+        e = ctypes.c_double()
+        de = np.zeros((ny, nx)) if with_derivative else None
+        self._check(lib().msgpu_lineshift_energy(self._h, nx, ny, _p(R), _p(_f64(T)), _p(_f64(phix)),
+                                                 ctypes.byref(e), _p(de) if de is not None else None))
+        return e.value, de
+
+    def xshift_reg(self, phix, yreg):
+        """findXShift's regulariser: (1/2 phi.K phi, K phi)."""
+        phix = _f64(phix)
+        ny, nx = phix.shape
+        e = ctypes.c_double()
+        k = np.zeros((ny, nx))
+        self._check(lib().msgpu_xshift_reg(self._h, nx, ny, float(yreg), _p(phix), ctypes.byref(e), _p(k)))
+        return e.value, k
 
     # --- ragged batches -----------------------------------------------------
     def register_ragged(self, params: Params, series):
