@@ -1496,3 +1496,253 @@ double msor_xshift_reg(int nx, int ny, double yreg, const double* phi, double* k
   free(st);
   return 0.5 * dot(kphi, phi, nx * ny);
 }
+
+/* --- the seismic solve: findXShift (matchSeries.h:805-865) -------------------- */
+/* Nine-point rows of an assembled Q1 operator on the nx x ny rectangular grid
+ * (h = 1/(max(nx,ny)-1)): mass (FELinScalarWeightedMassInterface) with factor
+ * fm, then stiffness (FELinScalarWeightedStiffInterface) with factor fs, each
+ * assembled element by element (InverseH1MetricBase::assembleSystemMatrix,
+ * linearSmoothOp.h:295-299).                                                */
+static double* rect_system(int nx, int ny, double fm, double fs) {
+  const double h = 1. / (double)((nx > ny ? nx : ny) - 1), vol = sqr(h);
+  quad_t Q;
+  quad_init(&Q, h);
+  double Mm[4][4], Ls[4][4];
+  for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) { Mm[i][j] = 0.; Ls[i][j] = 0.; }
+  for (int q = 0; q < 4; ++q)
+    for (int i = 0; i < 4; ++i) {
+      const double bi = Q.bq[i][q];
+      for (int j = i; j < 4; ++j) {
+        Mm[i][j] += bi * Q.bq[j][q] * 1. * Q.w;
+        double d = 0;
+        d += Q.gq[i][q][0] * Q.gq[j][q][0];
+        d += Q.gq[i][q][1] * Q.gq[j][q][1];
+        Ls[i][j] += d * 1. * Q.w;
+      }
+    }
+  for (int i = 0; i < 4; ++i)
+    for (int j = i; j < 4; ++j) { Mm[j][i] = Mm[i][j] = Mm[i][j] * vol; Ls[j][i] = Ls[i][j] = Ls[i][j] * vol; }
+  double* st = (double*)calloc((size_t)nx * ny * 9, sizeof(double));
+  for (int pass = 0; pass < 2; ++pass) {
+    if (pass == 1 && fs == 0.) break;
+    for (int ey = 0; ey < ny - 1; ++ey)
+      for (int ex = 0; ex < nx - 1; ++ex)
+        for (int i = 0; i < 4; ++i)
+          for (int j = 0; j < 4; ++j) {
+            const int gi = ex + ey * nx + ((i & 1) ? 1 : 0) + ((i & 2) ? nx : 0);
+            const int gj = ex + ey * nx + ((j & 1) ? 1 : 0) + ((j & 2) ? nx : 0);
+            const int dx = (gj % nx) - (gi % nx), dy = (gj / nx) - (gi / nx);
+            st[(size_t)gi * 9 + (dy + 1) * 3 + (dx + 1)] += pass == 0 ? fm * Mm[i][j] : fs * Ls[i][j];
+          }
+  }
+  return st;
+}
+
+static void rect_apply(const double* st, int nx, int ny, const double* u, double* out) {
+  for (int r = 0; r < nx * ny; ++r) {
+    const int x = r % nx, y = r / nx;
+    double d = 0.;
+    for (int j = -1; j <= 1; ++j)
+      for (int i = -1; i <= 1; ++i) {
+        const int X = x + i, Y = y + j;
+        if (X >= 0 && X < nx && Y >= 0 && Y < ny) d += st[(size_t)r * 9 + (j + 1) * 3 + (i + 1)] * u[X + Y * nx];
+      }
+    out[r] = d;
+  }
+}
+
+/* M + tau L with tau = 0.5 sigma^2 (InverseH1MetricBase::setSigma) applied to x */
+void msor_h1sys_apply(int nx, int ny, double sigma, const double* x, double* y) {
+  double* st = rect_system(nx, ny, 1.0, (double)(0.5f * sqr(sigma)));
+  rect_apply(st, nx, ny, x, y);
+  free(st);
+}
+
+/* Band Cholesky of a nine-point SPD matrix (half-bandwidth nx + 1): the
+ * exact solve that CholeskyBasedInverseH1Metric (linearSmoothOp.h:345-378)
+ * obtains from SuiteSparse's CHOLMOD, which the reference does not vendor. */
+typedef struct { int N, b; double* L; } band_chol_t;
+
+static band_chol_t band_chol(const double* st, int nx, int ny) {
+  band_chol_t C;
+  C.N = nx * ny;
+  C.b = nx + 1;
+  const int b = C.b;
+  C.L = (double*)calloc((size_t)C.N * (b + 1), sizeof(double));  /* L[i*(b+1) + k] = A(i, i-k) */
+  for (int r = 0; r < C.N; ++r) {
+    const int x = r % nx, y = r / nx;
+    for (int j = -1; j <= 1; ++j)
+      for (int i = -1; i <= 1; ++i) {
+        const int X = x + i, Y = y + j;
+        if (X < 0 || X >= nx || Y < 0 || Y >= ny) continue;
+        const int c = X + Y * nx;
+        if (c <= r) C.L[(size_t)r * (b + 1) + (r - c)] = st[(size_t)r * 9 + (j + 1) * 3 + (i + 1)];
+      }
+  }
+  for (int i = 0; i < C.N; ++i) {
+    for (int k = (i - b > 0 ? i - b : 0); k < i; ++k) {
+      double s = C.L[(size_t)i * (b + 1) + (i - k)];
+      for (int m = (i - b > k - b ? i - b : k - b); m < k; ++m)
+        if (m >= 0) s -= C.L[(size_t)i * (b + 1) + (i - m)] * C.L[(size_t)k * (b + 1) + (k - m)];
+      C.L[(size_t)i * (b + 1) + (i - k)] = s / C.L[(size_t)k * (b + 1)];
+    }
+    double s = C.L[(size_t)i * (b + 1)];
+    for (int m = (i - b > 0 ? i - b : 0); m < i; ++m) s -= sqr(C.L[(size_t)i * (b + 1) + (i - m)]);
+    C.L[(size_t)i * (b + 1)] = sqrt(s);
+  }
+  return C;
+}
+
+static void band_chol_solve(const band_chol_t* C, double* x) {
+  const int N = C->N, b = C->b;
+  for (int i = 0; i < N; ++i) {
+    double s = x[i];
+    for (int m = (i - b > 0 ? i - b : 0); m < i; ++m) s -= C->L[(size_t)i * (b + 1) + (i - m)] * x[m];
+    x[i] = s / C->L[(size_t)i * (b + 1)];
+  }
+  for (int i = N - 1; i >= 0; --i) {
+    double s = x[i];
+    for (int m = i + 1; m <= (i + b < N - 1 ? i + b : N - 1); ++m) s -= C->L[(size_t)m * (b + 1) + (m - i)] * x[m];
+    x[i] = s / C->L[(size_t)i * (b + 1)];
+  }
+}
+
+/* (M + 0.5 sigma^2 L)^{-1} x in place */
+void msor_h1_metric(int nx, int ny, double sigma, double* x) {
+  double* st = rect_system(nx, ny, 1.0, (double)(0.5f * sqr(sigma)));
+  band_chol_t C = band_chol(st, nx, ny);
+  band_chol_solve(&C, x);
+  free(C.L);
+  free(st);
+}
+
+typedef struct {
+  int nx, ny, N;
+  const double *R, *T;
+  double lambda, yreg;
+  double rb_tau[2], rb_e[2];
+  int rb_pos, evals;
+  double e_at_pos;
+  double *tx, *w;
+} xs_ctx;
+
+/* E = EData + lambda * ERegStiff (LinCombOp, matchSeries.h:847-850) */
+static double xs_energy(xs_ctx* C, const double* phi) {
+  double e = 0.;
+  e += msor_lineshift(C->nx, C->ny, C->R, C->T, phi, NULL);
+  e += C->lambda * msor_xshift_reg(C->nx, C->ny, C->yreg, phi, C->w);
+  return e;
+}
+
+/* DE = DEData + lambda * K phi */
+static void xs_gradient(xs_ctx* C, const double* phi, double* de) {
+  msor_lineshift(C->nx, C->ny, C->R, C->T, phi, de);
+  msor_xshift_reg(C->nx, C->ny, C->yreg, phi, C->w);
+  for (int i = 0; i < C->N; ++i) de[i] += C->lambda * C->w[i];
+}
+
+static double xs_eval(xs_ctx* C, const double* p, const double* d, double tw) {
+  if (tw == 0) return C->e_at_pos;
+  for (int i = 0; i < C->N; ++i) { C->tx[i] = p[i]; C->tx[i] += tw * d[i]; }
+  const double e = xs_energy(C, C->tx);
+  C->rb_tau[C->rb_pos] = tw;
+  C->rb_e[C->rb_pos] = e;
+  C->rb_pos ^= 1;
+  C->evals++;
+  return e;
+}
+
+static double xs_armijo(xs_ctx* C, const double* p, const double* d, const double* DE, double old_tau) {
+  const double sigma = 0.5, tau_min = pow(2., -30.), tau_max = pow(2., 25.);
+  double tau = old_tau < tau_min ? tau_min : (old_tau > tau_max ? tau_max : old_tau);
+  const double f = xs_eval(C, p, d, 0.);
+  double fnew = xs_eval(C, p, d, tau);
+  const double Df = dot(DE, d, C->N);
+  double G = (fnew - f) / (Df * tau);
+  if (Df >= 0) return 0;
+  if (!finite(f)) return 0;
+  if (G >= sigma && f >= fnew) {
+    do {
+      tau *= 2.;
+      fnew = xs_eval(C, p, d, tau);
+      G = (fnew - f) / (Df * tau);
+    } while (G >= sigma && f >= fnew && tau <= tau_max);
+    tau *= 0.5;
+  } else {
+    do {
+      if (tau > tau_min) tau *= 0.5;
+      fnew = xs_eval(C, p, d, tau);
+      G = (fnew - f) / (Df * tau);
+    } while ((!finite(fnew) || (G < sigma || f < fnew)) && (tau > tau_min));
+  }
+  return (tau > tau_min) ? tau : 0.;
+}
+
+/* findXShift with laplaceWeight <= 0: GradientDescentWithAutomaticFilterWidth
+ * over H1GradientDescent with the exact inverse H1 metric, Fletcher-Reeves
+ * NCG, Armijo (the control of gradientDescent.h:295-464, 675-691 and
+ * ArmijoSearch.h:118-200, as in msor_gd_level_dt, on one component); phix is
+ * scaled by nx/max(nx,ny) around the descent (matchSeries.h:860-864).
+ * Returns the steps; *energy_out the energy at the end.                    */
+int msor_xshift(int nx, int ny, const double* R, const double* T, double lambda, double yreg, int max_iter,
+                double* phix, double* energy_out, msor_step* trace, int trace_cap) {
+  const int N = nx * ny;
+  xs_ctx C;
+  memset(&C, 0, sizeof(C));
+  C.nx = nx; C.ny = ny; C.N = N; C.R = R; C.T = T; C.lambda = lambda; C.yreg = yreg;
+  C.rb_tau[0] = C.rb_tau[1] = NAN;
+  double* buf = (double*)calloc((size_t)N * 6, sizeof(double));
+  double *d = buf, *og = buf + N, *od = buf + 2 * N, *DE = buf + 3 * N;
+  C.tx = buf + 4 * N; C.w = buf + 5 * N;
+  const double scale = (double)nx / (double)(nx > ny ? nx : ny);
+  for (int i = 0; i < N; ++i) phix[i] /= scale;
+  double tau = 1.0, sigma = 1.0;
+  const double stop_sigma = 0.0001, sigma_tol = 0.00001, stop_eps = 0.;
+  double energy = xs_energy(&C, phix), energy_new = energy;
+  int iter = 0, n_trace = 0, go = max_iter > 0;
+  while (go) {
+    iter++;
+    energy = energy_new;
+    C.e_at_pos = energy;
+    C.evals = 0;
+    const double sigma_used = sigma;
+    xs_gradient(&C, phix, DE);
+    for (int i = 0; i < N; ++i) d[i] = DE[i] * -1.;
+    msor_h1_metric(nx, ny, sigma, d);
+    double beta = 0.;
+    if ((iter - 1) % 10) beta = dot(d, d, N) / dot(og, og, N);
+    memcpy(og, d, sizeof(double) * N);
+    for (int i = 0; i < N; ++i) d[i] += beta * od[i];
+    memcpy(od, d, sizeof(double) * N);
+    tau = xs_armijo(&C, phix, d, DE, tau);
+    for (int i = 0; i < N; ++i) d[i] *= tau;
+    if (tau == 0) {
+      memcpy(d, og, sizeof(double) * N);
+      memset(od, 0, sizeof(double) * N);
+      tau = xs_armijo(&C, phix, d, DE, tau);
+      for (int i = 0; i < N; ++i) d[i] *= tau;
+    }
+    double enew = NAN;
+    if (C.rb_tau[0] == tau) enew = C.rb_e[0];
+    else if (C.rb_tau[1] == tau) enew = C.rb_e[1];
+    else if (tau == 0) enew = energy;
+    if (tau != 0)
+      for (int i = 0; i < N; ++i) phix[i] += d[i];
+    if (isnan(enew)) enew = xs_energy(&C, phix);
+    energy_new = enew;
+    if (trace && n_trace < trace_cap) {
+      trace[n_trace].iter = iter; trace[n_trace].energy = energy_new; trace[n_trace].tau = tau;
+      trace[n_trace].sigma = sigma_used; trace[n_trace].evals = C.evals; n_trace++;
+    }
+    go = ((energy - energy_new) > stop_eps) && (iter < max_iter);
+    if ((0.5 * sigma > stop_sigma) && ((energy - energy_new) < sigma_tol)) {
+      sigma *= 0.5;
+      tau = 1.;
+      go = (sigma > stop_sigma) && (iter < max_iter);
+    }
+  }
+  for (int i = 0; i < N; ++i) phix[i] *= scale;
+  if (energy_out) *energy_out = energy_new;
+  free(buf);
+  return iter;
+}

@@ -201,6 +201,35 @@ def xshift_reg(phix, yreg):
     return float(e), k
 
 
+def h1sys_apply(x, sigma):
+    """(M + 0.5 sigma^2 L) x on the grid of x (ny, nx)."""
+    ny, nx = x.shape
+    y = np.zeros((ny, nx))
+    lib().msor_h1sys_apply(nx, ny, ctypes.c_double(sigma), _p(_c(x).reshape(-1)), _p(y))
+    return y
+
+
+def h1_metric(x, sigma):
+    """(M + 0.5 sigma^2 L)^{-1} x, exact (band Cholesky)."""
+    y = _c(x).copy()
+    ny, nx = y.shape
+    lib().msor_h1_metric(nx, ny, ctypes.c_double(sigma), _p(y.reshape(-1)))
+    return y
+
+
+def xshift(R, T, lam, yreg, max_iter, phix=None, trace_cap=4096):
+    """findXShift: returns (phix, energy, steps, trace rows (iter, energy, tau, sigma, evals))."""
+    R = _c(R)
+    ny, nx = R.shape
+    ph = np.zeros((ny, nx)) if phix is None else _c(phix).copy()
+    e = ctypes.c_double()
+    tr = (Step * trace_cap)()
+    steps = lib().msor_xshift(nx, ny, _p(R.reshape(-1)), _p(_c(T).reshape(-1)), ctypes.c_double(lam),
+                              ctypes.c_double(yreg), max_iter, _p(ph.reshape(-1)), ctypes.byref(e), tr, trace_cap)
+    rows = [(tr[i].iter, tr[i].energy, tr[i].tau, tr[i].sigma, tr[i].evals) for i in range(min(steps, trace_cap))]
+    return ph, e.value, steps, rows
+
+
 def warp_median(level, frames, phis, fill):
     N = n_of(level) ** 2
     out = np.zeros(N)
@@ -318,6 +347,11 @@ class RefRunner:
         self.run("xshiftreg", nx, ny, repr(float(yreg)), self._w("px", phix), os.path.join(self.dir, "e"),
                  os.path.join(self.dir, "k"))
         return float(self._r("e")[0]), self._r("k").reshape(ny, nx)
+
+    def h1sys(self, x, sigma):
+        ny, nx = x.shape
+        self.run("h1sys", nx, ny, repr(float(sigma)), self._w("x", x), os.path.join(self.dir, "y"))
+        return self._r("y").reshape(ny, nx)
 
     def save_array(self, a, path, type_):
         """qc::ScalarArray<QC_2D>::save of a (numY, numX) array to path."""

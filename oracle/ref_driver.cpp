@@ -361,6 +361,7 @@ static int usage ( ) {
     "ms_ref compose L d1 d2 inout | median L F frames phis fill out\n"
     "ms_ref save nx ny in out type | load file out dims | savedef L in mask | loaddef L mask out\n"
     "ms_ref lineshift nx ny R T phix outE outDE | xshiftreg nx ny yRegFactor phix outE outKphi\n"
+    "ms_ref h1sys nx ny sigma x out\n"
     "ms_ref series[_ncc] maxL start stop lambda lambdaFactor maxIter stopEps sat minToZero F framesBin outPhis outMean outTxt\n"
     "ms_ref matchseries[_ncc] maxL start stop lambda lambdaFactor maxIter stopEps sat minToZero refineStart refineStop\n"
     "       extraStages extraLambdaFactor useMedian F framesBin outPrefix\n" );
@@ -547,6 +548,28 @@ int main ( int argc, char **argv ) {
       K.apply ( phi, kphi );
       writeBin ( argv[6], &e[0], 1 );
       writeBin ( argv[7], kphi.getData ( ), N );
+      return 0;
+    }
+    if ( cmd == "h1sys" && argc == 7 ) {
+      // ms_ref h1sys nx ny sigma x out: the system matrix of InverseH1MetricBase (linearSmoothOp.h:262-301),
+      // M + tau L with tau = 0.5f * sigma^2, assembled on the rectangular grid, applied to x.  (Its Cholesky
+      // inverse, CholeskyBasedInverseH1Metric, needs SuiteSparse, which the reference does not vendor.)
+      typedef qc::RectangularGridConfigurator<RealType, qc::QC_2D, aol::GaussQuadrature<RealType, qc::QC_2D, 3> > RectConf;
+      const int nx = atoi ( argv[2] ), ny = atoi ( argv[3] ), N = nx * ny;
+      ArrayType dummy ( nx, ny );
+      const RectConf::InitType grid ( qc::GridSize<qc::QC_2D>::createFrom ( dummy ) );
+      const aol::MassOp<RectConf> massOp ( grid );
+      const aol::StiffOp<RectConf> stiffOp ( grid );
+      RectConf::MatrixType sys ( grid );
+      const RealType sigma = atof ( argv[4] );
+      const RealType tau = 0.5f * aol::Sqr ( sigma );
+      sys.setZero ( );
+      massOp.assembleAddMatrix ( sys );
+      stiffOp.assembleAddMatrix ( sys, tau );
+      aol::Vector<RealType> x ( N ), y ( N );
+      readBin ( argv[5], x.getData ( ), N );
+      sys.apply ( x, y );
+      writeBin ( argv[6], y.getData ( ), N );
       return 0;
     }
     if ( cmd == "compose" && argc == 7 ) {

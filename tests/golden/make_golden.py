@@ -253,6 +253,13 @@ def seismic(ref: msor.RefRunner, seed: int):
         ereg, kphi = ref.xshift_reg(phi, 0.3 if tag == "a" else 2.0)
         d.update({f"R_{tag}": R, f"T_{tag}": T, f"phi_{tag}": phi, f"E_{tag}": e, f"DE_{tag}": de,
                   f"yreg_{tag}": 0.3 if tag == "a" else 2.0, f"Ereg_{tag}": ereg, f"Kphi_{tag}": kphi})
+    # the H1 metric's system matrix M + 0.5 sigma^2 L (its Cholesky inverse needs
+    # SuiteSparse, which the reference does not vendor: only the matrix is pinned)
+    for tag, (nx, ny, sg) in (("a", (33, 17, 1.0)), ("b", (40, 23, 0.03))):
+        x = rng.normal(size=(ny, nx))
+        d[f"h1x_{tag}"] = x
+        d[f"h1sigma_{tag}"] = sg
+        d[f"h1y_{tag}"] = ref.h1sys(x, sg)
     np.savez_compressed(os.path.join(OUT, "seismic.npz"), **d)
 
 

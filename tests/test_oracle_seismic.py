@@ -28,3 +28,32 @@ def test_xshift_regulariser_bit_exact(oracle, tag):
     e, k = oracle.xshift_reg(g[f"phi_{tag}"], float(g[f"yreg_{tag}"]))
     assert e == float(g[f"Ereg_{tag}"])
     assert np.array_equal(k, g[f"Kphi_{tag}"])
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_h1_metric_system_matrix_bit_exact_and_inverse(oracle, tag):
+    """InverseH1MetricBase's system matrix M + 0.5 sigma^2 L is the
+    reference's bit for bit; the oracle's band Cholesky inverts it to
+    rounding (the reference inverts it with SuiteSparse's CHOLMOD, which it
+    does not vendor)."""
+    g = golden("seismic.npz")
+    x, sg = g[f"h1x_{tag}"], float(g[f"h1sigma_{tag}"])
+    assert np.array_equal(oracle.h1sys_apply(x, sg), g[f"h1y_{tag}"])
+    z = oracle.h1_metric(x, sg)
+    assert np.abs(oracle.h1sys_apply(z, sg) - x).max() <= 1e-13 * np.abs(x).max()
+
+
+def test_xshift_recovers_a_line_shift(oracle):
+    """findXShift on lines shifted by 1.5 px: the energy decreases step by
+    step, the filter width halves on the way, and the mean shift found is
+    the planted one."""
+    rng = np.random.default_rng(6)
+    nx, ny = 65, 17
+    x = np.arange(nx)
+    R = np.stack([np.sin(x / 4.0 + 0.3 * k) + 0.05 * rng.normal(size=nx) for k in range(ny)])
+    T = np.stack([np.sin((x - 1.5) / 4.0 + 0.3 * k) + 0.05 * rng.normal(size=nx) for k in range(ny)])
+    ph, e, steps, rows = oracle.xshift(R, T, 0.01, 1.0, 60)
+    energies = [r[1] for r in rows]
+    assert all(b <= a for a, b in zip(energies, energies[1:]))
+    assert rows[-1][3] < rows[0][3]
+    assert abs(ph[:, 8:-8].mean() * (nx - 1) - 1.5) < 0.05
