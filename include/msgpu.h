@@ -156,6 +156,21 @@ int msgpu_xshift_reg(msgpu_context* ctx, int nx, int ny, double yreg, const doub
 int msgpu_xshift_reg_device(msgpu_context* ctx, int nx, int ny, int num_images, double yreg, const double* d_phix,
                             double* d_energy_out, double* d_kphi_out, void* stream);
 
+/* findXShift (matchSeries.h:805-865) with laplaceWeight <= 0: the gradient
+ * flow with automatic filter width, Fletcher-Reeves NCG and Armijo steps on
+ * E = line-shift data term + lambda * 1/2 phix.K phix, in the metric of
+ * (M + sigma^2/2 L)^{-1} (CholeskyBasedInverseH1Metric, linearSmoothOp.h:
+ * 345-378, here applied exactly through the spectral basis of the grid).
+ *   phix: nx*ny doubles, the x-displacement in/out in the units of the 2-D
+ *   grid (h = 1/(max(nx,ny)-1); scaled to line units inside, as findXShift
+ *   does).  max_iter: maxGDIterations (the reference's default is 500).
+ *   energy_out, steps_out (nullable): host values.                         */
+int msgpu_find_xshift(msgpu_context* ctx, int nx, int ny, const double* R, const double* T, double lambda,
+                      double yreg, int max_iter, double* phix, double* energy_out, int* steps_out);
+int msgpu_find_xshift_device(msgpu_context* ctx, int nx, int ny, const double* d_R, const double* d_T, double lambda,
+                             double yreg, int max_iter, double* d_phix, double* energy_out, int* steps_out,
+                             void* stream);
+
 /* --- series pipeline ------------------------------------------------------ */
 /* Options of matchSeries<>() beyond the registration keys (parameter-file
  * names of the reference).                                                  */

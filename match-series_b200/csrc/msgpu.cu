@@ -10,6 +10,7 @@
 //      (quocDescent.h:83-105, registration.h:510-521)
 //   4. prolongation to the precision level (registration.h:462-467)
 // and msgpu_warp_mean the warped-frame average (matchSeries.h:385-425).
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -44,6 +45,10 @@ struct msgpu_context {
   cudaEvent_t ev[32] = {};
   bool ev_ready = false;
   int last_grid = 0;        // CTAs of the last level launch
+  // seismic line-shift solve: cuBLAS for the H1 metric, its spectral basis
+  cublasHandle_t blas = nullptr;
+  int xs_nx = 0, xs_ny = 0;
+  Buf xs_basis, xs_work;
 };
 
 namespace {
@@ -1398,11 +1403,12 @@ int msgpu_destroy(msgpu_context* ctx) {
   msgpu_context::Buf* bufs[] = {&ctx->arena, &ctx->shared_real, &ctx->dscratch, &ctx->small, &ctx->phis_d,
                                 &ctx->io[0], &ctx->io[1],   &ctx->io[2],    &ctx->io[3], &ctx->io[4],
                                 &ctx->io[5], &ctx->prof,    &ctx->sched,    &ctx->flags, &ctx->nccbuf,
-                                &ctx->ext,   &ctx->series,  &ctx->vals};
+                                &ctx->ext,   &ctx->series,  &ctx->vals,  &ctx->xs_basis, &ctx->xs_work};
   for (auto* b : bufs)
     if (b->p) cudaFree(b->p);
   if (ctx->ev_ready)
     for (int i = 0; i < 32; ++i) cudaEventDestroy(ctx->ev[i]);
+  if (ctx->blas) cublasDestroy(ctx->blas);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return MSGPU_OK;
@@ -1689,6 +1695,299 @@ XRegTables host_xreg_tables(int nx, int ny, double yreg) {
   return tb;
 }
 }  // namespace
+
+namespace {
+// --- findXShift on the device ---------------------------------------------
+// The inverse H1 metric (M + tau L)^{-1} on the nx x ny grid: M and L are
+// Kronecker sums of the line operators (M = My (x) Mx, L = My (x) Kx + Ky (x)
+// Mx for Q1 elements with tensor Gauss quadrature), so with the generalised
+// eigenvectors of (K1, M1) -- the cosine modes v_k(i) = cos(k pi i/(n-1)),
+// normalised to v^T M1 v = 1, eigenvalues 6/h^2 (1 - cos t_k)/(2 + cos t_k) --
+// (M + tau L)^{-1} = V (1 + tau (lx_i + ly_j))^{-1} V^T, four dense products
+// per application (cuBLAS DGEMM) and a spectral scaling.  It is the exact
+// inverse that the reference's CholeskyBasedInverseH1Metric computes by a
+// sparse Cholesky factorisation, up to rounding.
+void host_spectral_basis(int n, double h, double* V, double* lam) {
+  const double pi = 3.14159265358979323846;
+  const double m0 = h / 3.0, md = 2.0 * h / 3.0, mo = h / 6.0;   // line mass: ends, interior, off-diagonal
+  std::vector<double> v(n);
+  for (int k = 0; k < n; ++k) {
+    const int per = 2 * (n - 1);
+    for (int i = 0; i < n; ++i) v[i] = cos(pi * (double)(((long long)k * i) % per) / (double)(n - 1));
+    double c = 0.0;
+    for (int i = 0; i < n; ++i) {
+      double mv = (i == 0 || i == n - 1) ? m0 * v[i] : md * v[i];
+      if (i > 0) mv += mo * v[i - 1];
+      if (i < n - 1) mv += mo * v[i + 1];
+      c += v[i] * mv;
+    }
+    const double s = 1.0 / sqrt(c);
+    for (int i = 0; i < n; ++i) V[i + (size_t)k * n] = v[i] * s;   // column k
+    const double ct = cos(pi * (double)k / (double)(n - 1));
+    lam[k] = 6.0 / (h * h) * (1.0 - ct) / (2.0 + ct);
+  }
+}
+
+struct XsBufs {
+  double *Vx, *Vy, *lx, *ly;           // spectral basis
+  double *d, *og, *od, *de, *tx, *kphi, *t1, *t2, *part, *scal;
+};
+
+int xs_setup(msgpu_context* ctx, int nx, int ny, XsBufs& B, cudaStream_t st) {
+  int rc;
+  if (!ctx->blas) {
+    if (cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS) return fail(ctx, MSGPU_ERR_CUDA, "cublasCreate failed");
+  }
+  if (cublasSetStream(ctx->blas, st) != CUBLAS_STATUS_SUCCESS) return fail(ctx, MSGPU_ERR_CUDA, "cublasSetStream failed");
+  const size_t nb = (size_t)nx * nx + (size_t)ny * ny + nx + ny;
+  if ((rc = ensure(ctx, ctx->xs_basis, sizeof(double) * nb))) return rc;
+  B.Vx = (double*)ctx->xs_basis.p;
+  B.Vy = B.Vx + (size_t)nx * nx;
+  B.lx = B.Vy + (size_t)ny * ny;
+  B.ly = B.lx + nx;
+  if (ctx->xs_nx != nx || ctx->xs_ny != ny) {
+    const double h = 1. / (double)((nx > ny ? nx : ny) - 1);
+    std::vector<double> hb(nb);
+    host_spectral_basis(nx, h, hb.data(), hb.data() + (size_t)nx * nx + (size_t)ny * ny);
+    host_spectral_basis(ny, h, hb.data() + (size_t)nx * nx, hb.data() + (size_t)nx * nx + (size_t)ny * ny + nx);
+    CK(cudaMemcpy(B.Vx, hb.data(), sizeof(double) * nb, cudaMemcpyHostToDevice));
+    ctx->xs_nx = nx;
+    ctx->xs_ny = ny;
+  }
+  const size_t N = (size_t)nx * ny;
+  if ((rc = ensure(ctx, ctx->xs_work, sizeof(double) * (9 * N + 4096)))) return rc;
+  double* w = (double*)ctx->xs_work.p;
+  B.d = w; B.og = w + N; B.od = w + 2 * N; B.de = w + 3 * N; B.tx = w + 4 * N; B.kphi = w + 5 * N;
+  B.t1 = w + 6 * N; B.t2 = w + 7 * N; B.part = w + 8 * N; B.scal = B.part + 2048;
+  return MSGPU_OK;
+}
+
+int xs_metric(msgpu_context* ctx, const XsBufs& B, int nx, int ny, double sigma, double* g, cudaStream_t st) {
+  const double one = 1.0, zero = 0.0;
+  const double tau = 0.5 * (sigma * sigma);
+  // column-major view: G is nx x ny (x fastest)
+  if (cublasDgemm(ctx->blas, CUBLAS_OP_T, CUBLAS_OP_N, nx, ny, nx, &one, B.Vx, nx, g, nx, &zero, B.t1, nx) ||
+      cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, nx, ny, ny, &one, B.t1, nx, B.Vy, ny, &zero, B.t2, nx))
+    return fail(ctx, MSGPU_ERR_CUDA, "cublasDgemm failed");
+  const int N = nx * ny;
+  k_spectral_scale<<<std::min(2048, (N + 255) / 256), 256, 0, st>>>(B.t2, B.lx, B.ly, tau, nx, ny);
+  if (cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, nx, ny, nx, &one, B.Vx, nx, B.t2, nx, &zero, B.t1, nx) ||
+      cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_T, nx, ny, ny, &one, B.t1, nx, B.Vy, ny, &zero, g, nx))
+    return fail(ctx, MSGPU_ERR_CUDA, "cublasDgemm failed");
+  ctx->stats.kernel_launches += 5;
+  return MSGPU_OK;
+}
+
+struct XsSolver {
+  msgpu_context* ctx;
+  XsBufs B;
+  int nx, ny, N;
+  const double *R, *T;
+  double lambda, yreg;
+  LineTables lt;
+  XRegTables rt;
+  cudaStream_t st;
+  double rb_tau[2], rb_e[2];
+  int rb_pos = 0, evals = 0;
+  double e_at_pos = 0;
+  int grid1() const { return std::min(2048, (N + 255) / 256); }
+
+  int dot(const double* a, const double* b, double* out) {
+    const int nb = std::min(1024, (N + 255) / 256);
+    k_dot_part<<<nb, 256, 0, st>>>(a, b, N, B.part);
+    k_sum_serial<<<1, 1, 0, st>>>(B.part, nb, B.scal);
+    CK(cudaMemcpyAsync(out, B.scal, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    ctx->stats.kernel_launches += 2;
+    return MSGPU_OK;
+  }
+  // data term and regulariser at p: energies into B.scal[1..2], derivative (if de) into de
+  int parts(const double* p, double* de) {
+    LineArgs a;
+    a.nx = nx; a.ny = ny; a.img_stride = (size_t)N; a.R = R; a.T = T; a.phi = p;
+    a.e_line = (double*)ctx->nccbuf.p; a.de = de; a.t = lt;
+    const size_t smem = sizeof(double) * 3 * (size_t)nx;
+    k_lineshift<<<dim3(ny, 1), kLineThreads, smem, st>>>(a);
+    k_lineshift_total<<<1, 32, 0, st>>>(a.e_line, ny, 1, B.scal + 1);
+    const int nb = std::min(1024, (N + 255) / 256);
+    k_xshift_reg<<<dim3(nb, 1), 256, 0, st>>>(rt, nx, ny, (size_t)N, p, B.kphi, B.part);
+    k_xshift_reg_total<<<1, 32, 0, st>>>(B.part, nb, 1, B.scal + 2);
+    ctx->stats.kernel_launches += 4;
+    CK(cudaGetLastError());
+    return MSGPU_OK;
+  }
+  int energy(const double* p, double* e) {
+    int rc;
+    if ((rc = parts(p, nullptr))) return rc;
+    double h[2];
+    CK(cudaMemcpyAsync(h, B.scal + 1, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    double v = 0.;
+    v += h[0];
+    v += lambda * h[1];
+    *e = v;
+    return MSGPU_OK;
+  }
+  int gradient(const double* p) {
+    int rc;
+    if ((rc = parts(p, B.de))) return rc;
+    k_axpy<<<grid1(), 256, 0, st>>>(B.de, lambda, B.kphi, B.de, N);
+    ctx->stats.kernel_launches += 1;
+    return MSGPU_OK;
+  }
+  int eval(const double* p, const double* d, double tw, double* e) {
+    if (tw == 0) { *e = e_at_pos; return MSGPU_OK; }
+    k_axpy<<<grid1(), 256, 0, st>>>(p, tw, d, B.tx, N);
+    ctx->stats.kernel_launches += 1;
+    int rc;
+    if ((rc = energy(B.tx, e))) return rc;
+    rb_tau[rb_pos] = tw;
+    rb_e[rb_pos] = *e;
+    rb_pos ^= 1;
+    evals++;
+    return MSGPU_OK;
+  }
+  // getTimestepWidthWithArmijoLineSearch (ArmijoSearch.h:118-200)
+  int armijo(const double* p, const double* d, double old_tau, double* out) {
+    const double sg = 0.5, tau_min = std::pow(2., -30.), tau_max = std::pow(2., 25.);
+    double tau = old_tau < tau_min ? tau_min : (old_tau > tau_max ? tau_max : old_tau);
+    double f, fnew, Df;
+    int rc;
+    if ((rc = eval(p, d, 0., &f)) || (rc = eval(p, d, tau, &fnew)) || (rc = dot(B.de, d, &Df))) return rc;
+    double G = (fnew - f) / (Df * tau);
+    if (Df >= 0 || !std::isfinite(f)) { *out = 0; return MSGPU_OK; }
+    if (G >= sg && f >= fnew) {
+      do {
+        tau *= 2.;
+        if ((rc = eval(p, d, tau, &fnew))) return rc;
+        G = (fnew - f) / (Df * tau);
+      } while (G >= sg && f >= fnew && tau <= tau_max);
+      tau *= 0.5;
+    } else {
+      do {
+        if (tau > tau_min) tau *= 0.5;
+        if ((rc = eval(p, d, tau, &fnew))) return rc;
+        G = (fnew - f) / (Df * tau);
+      } while ((!std::isfinite(fnew) || (G < sg || f < fnew)) && (tau > tau_min));
+    }
+    *out = (tau > tau_min) ? tau : 0.;
+    return MSGPU_OK;
+  }
+};
+
+// findXShift (matchSeries.h:805-865) with laplaceWeight <= 0: the descent
+// control of GradientDescentWithAutomaticFilterWidth over H1GradientDescent
+// (gradientDescent.h:295-464, 675-691) on the host, every vector operation on
+// the device; phi (device, nx*ny) in/out.
+int run_xshift(msgpu_context* ctx, int nx, int ny, const double* R, const double* T, double lambda, double yreg,
+               int max_iter, double* phi, double* energy_out, int* steps_out, cudaStream_t st) {
+  XsSolver S;
+  S.ctx = ctx; S.nx = nx; S.ny = ny; S.N = nx * ny; S.R = R; S.T = T; S.lambda = lambda; S.yreg = yreg; S.st = st;
+  S.rb_tau[0] = S.rb_tau[1] = NAN;
+  S.rb_e[0] = S.rb_e[1] = NAN;
+  int rc;
+  if ((rc = xs_setup(ctx, nx, ny, S.B, st))) return rc;
+  if ((rc = ensure(ctx, ctx->nccbuf, sizeof(double) * (size_t)ny + 64))) return rc;
+  S.lt = host_line_tables(nx);
+  S.rt = host_xreg_tables(nx, ny, yreg);
+  CK(cudaFuncSetAttribute(k_lineshift, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)(sizeof(double) * 3 * (size_t)nx)));
+  const int N = S.N, g1 = S.grid1();
+  const XsBufs& B = S.B;
+  CK(cudaMemsetAsync(B.og, 0, sizeof(double) * N, st));
+  CK(cudaMemsetAsync(B.od, 0, sizeof(double) * N, st));
+  const double scale = (double)nx / (double)(nx > ny ? nx : ny);
+  k_divide<<<g1, 256, 0, st>>>(phi, scale, N);
+  double tau = 1.0, sigma = 1.0;
+  const double stop_sigma = 0.0001, sigma_tol = 0.00001, stop_eps = 0.;
+  double energy, energy_new;
+  if ((rc = S.energy(phi, &energy))) return rc;
+  energy_new = energy;
+  int iter = 0;
+  bool go = max_iter > 0;
+  while (go) {
+    iter++;
+    energy = energy_new;
+    S.e_at_pos = energy;
+    S.evals = 0;
+    if ((rc = S.gradient(phi))) return rc;
+    k_mul<<<g1, 256, 0, st>>>(B.de, -1., B.d, N);
+    if ((rc = xs_metric(ctx, B, nx, ny, sigma, B.d, st))) return rc;
+    double beta = 0.;
+    if ((iter - 1) % 10) {
+      double a, b;
+      if ((rc = S.dot(B.d, B.d, &a)) || (rc = S.dot(B.og, B.og, &b))) return rc;
+      beta = a / b;
+    }
+    CK(cudaMemcpyAsync(B.og, B.d, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+    k_axpy<<<g1, 256, 0, st>>>(B.d, beta, B.od, B.d, N);
+    CK(cudaMemcpyAsync(B.od, B.d, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+    if ((rc = S.armijo(phi, B.d, tau, &tau))) return rc;
+    k_scale<<<g1, 256, 0, st>>>(B.d, tau, N);
+    if (tau == 0) {
+      CK(cudaMemcpyAsync(B.d, B.og, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+      CK(cudaMemsetAsync(B.od, 0, sizeof(double) * N, st));
+      if ((rc = S.armijo(phi, B.d, tau, &tau))) return rc;
+      k_scale<<<g1, 256, 0, st>>>(B.d, tau, N);
+    }
+    double enew = NAN;
+    if (S.rb_tau[0] == tau) enew = S.rb_e[0];
+    else if (S.rb_tau[1] == tau) enew = S.rb_e[1];
+    else if (tau == 0) enew = energy;
+    if (tau != 0) k_axpy<<<g1, 256, 0, st>>>(phi, 1.0, B.d, phi, N);
+    ctx->stats.kernel_launches += 4;
+    if (std::isnan(enew) && (rc = S.energy(phi, &enew))) return rc;
+    energy_new = enew;
+    go = ((energy - energy_new) > stop_eps) && (iter < max_iter);
+    if ((0.5 * sigma > stop_sigma) && ((energy - energy_new) < sigma_tol)) {
+      sigma *= 0.5;
+      tau = 1.;
+      go = (sigma > stop_sigma) && (iter < max_iter);
+    }
+  }
+  k_scale<<<g1, 256, 0, st>>>(phi, scale, N);
+  CK(cudaGetLastError());
+  if (energy_out) *energy_out = energy_new;
+  if (steps_out) *steps_out = iter;
+  return MSGPU_OK;
+}
+}  // namespace
+
+int msgpu_find_xshift_device(msgpu_context* ctx, int nx, int ny, const double* d_R, const double* d_T, double lambda,
+                             double yreg, int max_iter, double* d_phix, double* energy_out, int* steps_out,
+                             void* stream) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (nx < 3 || ny < 3 || max_iter < 0 || !d_R || !d_T || !d_phix)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid find_xshift arguments (grids of at least 3 x 3 nodes)");
+  if (sizeof(double) * 3 * (size_t)nx > 200 * 1024)
+    return fail(ctx, MSGPU_ERR_SIZE, "lines of %d samples do not fit shared memory", nx);
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  ctx->stats.kernel_launches = 0;
+  return run_xshift(ctx, nx, ny, d_R, d_T, lambda, yreg, max_iter, d_phix, energy_out, steps_out,
+                    (cudaStream_t)stream);
+}
+
+int msgpu_find_xshift(msgpu_context* ctx, int nx, int ny, const double* R, const double* T, double lambda,
+                      double yreg, int max_iter, double* phix, double* energy_out, int* steps_out) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (!R || !T || !phix) return fail(ctx, MSGPU_ERR_INVALID_ARG, "null buffer");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  const size_t N = (size_t)nx * ny;
+  if ((rc = ensure(ctx, ctx->io[0], sizeof(double) * 3 * N))) return rc;
+  double* d = (double*)ctx->io[0].p;
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(d, R, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d + N, T, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d + 2 * N, phix, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+  if ((rc = msgpu_find_xshift_device(ctx, nx, ny, d, d + N, lambda, yreg, max_iter, d + 2 * N, energy_out, steps_out,
+                                     st)))
+    return rc;
+  CK(cudaMemcpyAsync(phix, d + 2 * N, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return MSGPU_OK;
+}
 
 int msgpu_lineshift_energy_device(msgpu_context* ctx, int nx, int ny, int num_images, const double* d_R,
                                   const double* d_T, const double* d_phix, double* d_energy_out, double* d_de_out,

@@ -225,4 +225,51 @@ __global__ void k_xshift_reg_total(const double* part, int nblocks, int num_imag
   out[img] = 0.5 * s;
 }
 
+// --- vector kernels of the seismic descent ----------------------------------
+// out[i] = a[i] + s * b[i]  (also the in-place updates, with out == a)
+__global__ void k_axpy(const double* a, double s, const double* b, double* out, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double v = a[i];
+    v += s * b[i];
+    out[i] = v;
+  }
+}
+__global__ void k_scale(double* a, double s, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] *= s;
+}
+__global__ void k_divide(double* a, double s, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] /= s;
+}
+__global__ void k_mul(const double* a, double s, double* out, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = a[i] * s;
+}
+// a[i] * b[i] summed per block in a fixed order (partials, then one serial sum)
+__global__ void __launch_bounds__(256) k_dot_part(const double* a, const double* b, int n, double* part) {
+  __shared__ double red[8];
+  double acc = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc += a[i] * b[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < 8; ++w) s += red[w];
+    part[blockIdx.x] = s;
+  }
+}
+__global__ void k_sum_serial(const double* part, int n, double* out) {
+  double s = 0.0;
+  for (int i = 0; i < n; ++i) s += part[i];
+  *out = s;
+}
+// Spectral scaling of the H1 metric: z[y][x] /= 1 + tau (lx[x] + ly[y])
+__global__ void k_spectral_scale(double* z, const double* lx, const double* ly, double tau, int nx, int ny) {
+  const int N = nx * ny;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    const int x = i % nx, y = i / nx;
+    z[i] /= 1.0 + tau * (lx[x] + ly[y]);
+  }
+}
+
 }  // namespace msg

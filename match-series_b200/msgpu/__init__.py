@@ -92,7 +92,7 @@ EXPORTS = [
     "msgpu_io_last_error", "msgpu_read_array", "msgpu_write_array", "msgpu_read_arrays", "msgpu_read_displacement",
     "msgpu_write_displacement", "msgpu_read_arrays_start", "msgpu_io_wait", "msgpu_register_ragged",
     "msgpu_register_ragged_device", "msgpu_lineshift_energy", "msgpu_lineshift_energy_device", "msgpu_xshift_reg",
-    "msgpu_xshift_reg_device",
+    "msgpu_xshift_reg_device", "msgpu_find_xshift", "msgpu_find_xshift_device",
 ]
 
 
@@ -168,6 +168,11 @@ def lib():
         L.msgpu_xshift_reg_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                               ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                               ctypes.c_void_p]
+        L.msgpu_find_xshift.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_int, _dp, _dp, _ip]
+        L.msgpu_find_xshift_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                               ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                               ctypes.c_void_p, _dp, _ip, ctypes.c_void_p]
         L.msgpu_register_ragged.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params), ctypes.POINTER(SeriesDesc),
                                             ctypes.c_int]
         L.msgpu_register_ragged_device.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params),
@@ -370,6 +375,17 @@ class Context:
         k = np.zeros((ny, nx))
         self._check(lib().msgpu_xshift_reg(self._h, nx, ny, float(yreg), _p(phix), ctypes.byref(e), _p(k)))
         return e.value, k
+
+    def find_xshift(self, R, T, lam, yreg, max_iter=500, phix=None):
+        """findXShift: returns (phix (ny, nx), energy, steps)."""
+        R = _f64(R)
+        ny, nx = R.shape
+        ph = np.zeros((ny, nx)) if phix is None else _f64(phix).copy()
+        e = ctypes.c_double()
+        steps = ctypes.c_int()
+        self._check(lib().msgpu_find_xshift(self._h, nx, ny, _p(R), _p(_f64(T)), float(lam), float(yreg),
+                                            int(max_iter), _p(ph), ctypes.byref(e), ctypes.byref(steps)))
+        return ph, e.value, steps.value
 
     # --- ragged batches -----------------------------------------------------
     def register_ragged(self, params: Params, series):
