@@ -34,6 +34,13 @@ series of 8 templates each, sizes drawn from 129², 257², 513², 1025², levels
 4 to each series' own finest level, one launch per level for all series;
 beside it the same series registered one batch after the other.
 
+--seismic times the seismic line-shift model (matchSeismicSeries'
+findXShift): 32 synthetic gathers of 257 traces x 2049 samples, each
+registered to the mean gather by shifts along the time axis (line-wise NCC,
+anisotropic regulariser, exact H1 metric), maxGDIterations 500; its CPU
+baseline is the oracle port on a 257-sample x 33-trace crop (the reference's
+own solver needs SuiteSparse, which it does not vendor).
+
 Multi-GPU (torchrun): weak scaling; every rank registers its own series.
 """
 from __future__ import annotations
@@ -689,6 +696,90 @@ def main_ragged(args, world, rank, local):
     return 0
 
 
+SEIS_GATHERS, SEIS_LAMBDA, SEIS_YREG, SEIS_ITER, SEIS_WORKERS = 32, 0.1, 1.0, 500, 8
+
+
+def main_seismic(args, world, rank, local):
+    """--seismic: findXShift for 32 gathers (msgpu_find_xshift_batch)."""
+    import numpy as np
+    import torch
+    import msgpu
+    from msgpu import build as mbuild
+    from msgpu import synthetic as syn
+
+    torch.cuda.set_device(local)
+    mbuild.build()
+    gathers = syn.seismic_gathers(SEIS_GATHERS, seed=4000 + 1000 * rank)
+    R = gathers.mean(axis=0)
+    G, ny, nx = gathers.shape
+    ctx = msgpu.Context(local)
+
+    def step():
+        return ctx.find_xshift_batch(R, gathers, SEIS_LAMBDA, SEIS_YREG, SEIS_ITER, workers=SEIS_WORKERS)
+
+    for _ in range(max(1, args.warmup - 2)):
+        step()
+    launches = 0
+    barrier(world)
+    with ClockSampler(local) as clocks:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            ph, en, st = step()
+            launches += ctx.stats()["kernel_launches"]
+        elapsed = allreduce_max(time.perf_counter() - t0, world)
+    value = world * G * args.steps / elapsed
+    if rank == 0:
+        clk = clocks.summary()
+        cpu = accuracy = None
+        if not args.no_cpu_baseline:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import msor
+            crop = (slice(0, 33), slice(0, 257))
+            t0 = time.perf_counter()
+            rph, re, rsteps, _ = msor.xshift(R[crop], gathers[0][crop], SEIS_LAMBDA, SEIS_YREG, SEIS_ITER)
+            t_cpu = time.perf_counter() - t0
+            gph, ge, gsteps = ctx.find_xshift(R[crop], gathers[0][crop], SEIS_LAMBDA, SEIS_YREG, SEIS_ITER)
+            # the oracle's own sensitivity: every template pixel of the crop moved by one ulp
+            tc = gathers[0][crop]
+            up = np.random.default_rng(7).random(tc.shape) < 0.5
+            tp = np.where(up, np.nextafter(tc, np.inf), np.nextafter(tc, -np.inf))
+            pph, pe, psteps, _ = msor.xshift(R[crop], tp, SEIS_LAMBDA, SEIS_YREG, SEIS_ITER)
+            cpu = {"value": 1.0 / t_cpu, "unit": "crops/s", "cores": 1, "kind": "port",
+                   "sample": f"the oracle (band Cholesky for the H1 metric) on a 257-sample x 33-trace crop of one "
+                             f"gather, {rsteps} steps in {t_cpu:.1f} s; the reference's own CholeskyBasedInverseH1Metric "
+                             f"needs SuiteSparse, which it does not vendor"}
+            accuracy = {"crop": "257 x 33", "steps_gpu": int(gsteps), "steps_oracle": int(rsteps),
+                        "max_dphi_px": float(np.abs(gph - rph).max() * 256),
+                        "rel_energy": float(abs(ge - re) / abs(re)),
+                        "oracle_1ulp_spread": {"steps": int(psteps),
+                                               "max_dphi_px": float(np.abs(pph - rph).max() * 256),
+                                               "rel_energy": float(abs(pe - re) / abs(re)),
+                                               "perturbation": "every template pixel of the crop +-1 ulp"}}
+        out = {
+            "metric": METRIC, "value": value, "unit": "gathers/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * elapsed / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic seismic gathers",
+            "config": {"workload": f"findXShift of {G} gathers ({ny} traces x {nx} samples, 0.25 ms, 50 Hz Ricker, "
+                                   f"hyperbolic moveout, +-2 ms statics, 10 dB SNR) to their mean gather, lambda "
+                                   f"{SEIS_LAMBDA}, yRegFactor {SEIS_YREG}, maxGDIterations {SEIS_ITER}, "
+                                   f"{SEIS_WORKERS} concurrent descents",
+                       "mean_steps": float(np.mean(st)), "parallelism": f"weak, {world} ranks"},
+            "e2e": {"value": value, "unit": "gathers/s", "h2d_bytes_per_step": 2 * G * nx * ny * 8 + nx * ny * 8,
+                    "d2h_bytes_per_step": G * nx * ny * 8},
+            "gpu_launches": launches,
+            "roofline": None,
+            "cpu_baseline": cpu,
+            "accuracy": accuracy,
+            "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        }
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -707,6 +798,8 @@ def main():
                     help="small case for ncu: one displacement composition at this level, no timing")
     ap.add_argument("--profile-series", action="store_true",
                     help="small case for ncu: one msgpu_match_series call on the bench's frames, no timing")
+    ap.add_argument("--seismic", action="store_true",
+                    help="the seismic line-shift model: findXShift of 32 gathers 257 x 2049")
     ap.add_argument("--ragged", action="store_true",
                     help="uneven series of 129^2..1025^2 in one ragged batch (msgpu_register_ragged)")
     ap.add_argument("--files", action="store_true",
@@ -730,6 +823,8 @@ def main():
         return main_files(args, world, rank, local)
     if args.ragged:
         return main_ragged(args, world, rank, local)
+    if args.seismic:
+        return main_seismic(args, world, rank, local)
 
     import numpy as np
     import torch

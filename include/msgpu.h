@@ -171,6 +171,17 @@ int msgpu_find_xshift_device(msgpu_context* ctx, int nx, int ny, const double* d
                              double yreg, int max_iter, double* d_phix, double* energy_out, int* steps_out,
                              void* stream);
 
+/* findXShift for num_images images (host buffers, back to back): R is one
+ * reference for all (r_per_image = 0, e.g. the mean stack) or one per image;
+ * phix in/out; energies_out, steps_out (nullable) per image.  The images are
+ * spread over `workers` host threads (< 1: 4), each with its own stream and
+ * buffers, so that their descents overlap on the GPU (no counterpart in the
+ * reference, which registers one image at a time).  Kernel-launch counts of
+ * all workers are summed in msgpu_get_stats.                               */
+int msgpu_find_xshift_batch(msgpu_context* ctx, int nx, int ny, int num_images, const double* R, int r_per_image,
+                            const double* T, double lambda, double yreg, int max_iter, double* phix,
+                            double* energies_out, int* steps_out, int workers);
+
 /* --- series pipeline ------------------------------------------------------ */
 /* Options of matchSeries<>() beyond the registration keys (parameter-file
  * names of the reference).                                                  */

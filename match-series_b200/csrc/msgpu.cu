@@ -19,7 +19,9 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <atomic>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/msgpu.h"
@@ -49,6 +51,7 @@ struct msgpu_context {
   cublasHandle_t blas = nullptr;
   int xs_nx = 0, xs_ny = 0;
   Buf xs_basis, xs_work;
+  std::vector<msgpu_context*> workers;   // contexts of the batch workers (own streams and buffers)
 };
 
 namespace {
@@ -1408,6 +1411,8 @@ int msgpu_destroy(msgpu_context* ctx) {
     if (b->p) cudaFree(b->p);
   if (ctx->ev_ready)
     for (int i = 0; i < 32; ++i) cudaEventDestroy(ctx->ev[i]);
+  for (msgpu_context* w : ctx->workers) msgpu_destroy(w);
+  ctx->workers.clear();
   if (ctx->blas) cublasDestroy(ctx->blas);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -1986,6 +1991,54 @@ int msgpu_find_xshift(msgpu_context* ctx, int nx, int ny, const double* R, const
     return rc;
   CK(cudaMemcpyAsync(phix, d + 2 * N, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  return MSGPU_OK;
+}
+
+int msgpu_find_xshift_batch(msgpu_context* ctx, int nx, int ny, int num_images, const double* R, int r_per_image,
+                            const double* T, double lambda, double yreg, int max_iter, double* phix,
+                            double* energies_out, int* steps_out, int workers) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (num_images < 1 || !R || !T || !phix) return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid find_xshift_batch arguments");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  const int nw = std::max(1, std::min(workers < 1 ? 4 : workers, num_images));
+  while ((int)ctx->workers.size() < nw) {
+    msgpu_context* w = nullptr;
+    if ((rc = msgpu_create(ctx->device, &w))) return fail(ctx, rc, "cannot create a worker context");
+    ctx->workers.push_back(w);
+  }
+  const size_t N = (size_t)nx * ny;
+  std::atomic<int> next(0);
+  std::vector<int> codes(nw, MSGPU_OK);
+  std::vector<std::string> msgs(nw);
+  auto work = [&](int wi) {
+    msgpu_context* w = ctx->workers[wi];
+    for (;;) {
+      const int i = next.fetch_add(1);
+      if (i >= num_images) break;
+      double e = 0;
+      int st = 0;
+      const int c = msgpu_find_xshift(w, nx, ny, R + (r_per_image ? (size_t)i * N : 0), T + (size_t)i * N, lambda,
+                                      yreg, max_iter, phix + (size_t)i * N, &e, &st);
+      if (c) {
+        codes[wi] = c;
+        msgs[wi] = w->err;
+        next.store(num_images);
+        break;
+      }
+      if (energies_out) energies_out[i] = e;
+      if (steps_out) steps_out[i] = st;
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nw; ++t) pool.emplace_back(work, t);
+  work(0);
+  for (auto& t : pool) t.join();
+  int launches = 0;
+  for (int t = 0; t < nw; ++t) launches += ctx->workers[t]->stats.kernel_launches;
+  ctx->stats.kernel_launches = launches;
+  for (int t = 0; t < nw; ++t)
+    if (codes[t]) return fail(ctx, codes[t], "%s", msgs[t].c_str());
   return MSGPU_OK;
 }
 

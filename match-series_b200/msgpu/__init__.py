@@ -92,7 +92,7 @@ EXPORTS = [
     "msgpu_io_last_error", "msgpu_read_array", "msgpu_write_array", "msgpu_read_arrays", "msgpu_read_displacement",
     "msgpu_write_displacement", "msgpu_read_arrays_start", "msgpu_io_wait", "msgpu_register_ragged",
     "msgpu_register_ragged_device", "msgpu_lineshift_energy", "msgpu_lineshift_energy_device", "msgpu_xshift_reg",
-    "msgpu_xshift_reg_device", "msgpu_find_xshift", "msgpu_find_xshift_device",
+    "msgpu_xshift_reg_device", "msgpu_find_xshift", "msgpu_find_xshift_device", "msgpu_find_xshift_batch",
 ]
 
 
@@ -173,6 +173,9 @@ def lib():
         L.msgpu_find_xshift_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                                ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                                ctypes.c_void_p, _dp, _ip, ctypes.c_void_p]
+        L.msgpu_find_xshift_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp,
+                                              ctypes.c_int, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp,
+                                              _dp, _ip, ctypes.c_int]
         L.msgpu_register_ragged.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params), ctypes.POINTER(SeriesDesc),
                                             ctypes.c_int]
         L.msgpu_register_ragged_device.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params),
@@ -386,6 +389,21 @@ class Context:
         self._check(lib().msgpu_find_xshift(self._h, nx, ny, _p(R), _p(_f64(T)), float(lam), float(yreg),
                                             int(max_iter), _p(ph), ctypes.byref(e), ctypes.byref(steps)))
         return ph, e.value, steps.value
+
+    def find_xshift_batch(self, R, T, lam, yreg, max_iter=500, phix=None, workers=4):
+        """findXShift for images T (G, ny, nx) against R (ny, nx) or (G, ny, nx);
+        returns (phix (G, ny, nx), energies[G], steps[G])."""
+        T = _f64(T)
+        G, ny, nx = T.shape
+        R = _f64(R)
+        per = 1 if R.ndim == 3 else 0
+        ph = np.zeros((G, ny, nx)) if phix is None else _f64(phix).copy()
+        en = np.zeros(G)
+        st = np.zeros(G, dtype=np.int32)
+        self._check(lib().msgpu_find_xshift_batch(self._h, nx, ny, G, _p(R), per, _p(T), float(lam), float(yreg),
+                                                  int(max_iter), _p(ph), _p(en), st.ctypes.data_as(_ip),
+                                                  int(workers)))
+        return ph, en, st
 
     # --- ragged batches -----------------------------------------------------
     def register_ragged(self, params: Params, series):

@@ -148,6 +148,38 @@ def ragged_workload(num_series: int = 16, frames_per_series: int = 8, sizes=(129
     return out
 
 
+def seismic_gathers(num_gathers: int = 32, nt: int = 2049, ntr: int = 257, seed: int = 4000, dt: float = 0.25e-3,
+                    f0: float = 50.0, snr_db: float = 10.0):
+    """Synthetic seismic gathers (num_gathers, ntr, nt): per trace, sparse
+    reflectivity (Bernoulli 0.02 x N(0, 1)) at hyperbolic moveout times
+    t(x) = sqrt(t0^2 + (x/v)^2) (offsets 0-200 m, v 1500-1800 m/s), plus a
+    static shift per trace (uniform +-2 ms), convolved with a Ricker wavelet
+    of f0 Hz at dt sampling, and Gaussian noise at snr_db.  Time runs along
+    x (the line of a trace), traces along y."""
+    rng = np.random.default_rng(seed)
+    t = np.arange(nt) * dt
+    tw = np.arange(-64, 65) * dt
+    a = (np.pi * f0 * tw) ** 2
+    ricker = (1 - 2 * a) * np.exp(-a)
+    out = np.zeros((num_gathers, ntr, nt))
+    for g in range(num_gathers):
+        refl_t0 = t[rng.random(nt) < 0.02]
+        amps = rng.normal(size=refl_t0.size)
+        v = rng.uniform(1500, 1800)
+        offsets = np.linspace(0, 200, ntr)
+        statics = rng.uniform(-2e-3, 2e-3, ntr)
+        for k in range(ntr):
+            tt = np.sqrt(refl_t0 ** 2 + (offsets[k] / v) ** 2) + statics[k]
+            spikes = np.zeros(nt)
+            idx = np.round(tt / dt).astype(np.int64)
+            ok = (idx >= 0) & (idx < nt)
+            np.add.at(spikes, idx[ok], amps[ok])
+            out[g, k] = np.convolve(spikes, ricker, mode="same")
+        p_sig = np.mean(out[g] ** 2)
+        out[g] += rng.normal(0, np.sqrt(p_sig / 10 ** (snr_db / 10)), out[g].shape)
+    return out
+
+
 def psnr(a: np.ndarray, b: np.ndarray) -> float:
     """Peak signal-to-noise ratio of a against b, peak = range of b."""
     mse = float(np.mean((a - b) ** 2))

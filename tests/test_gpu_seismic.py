@@ -75,3 +75,20 @@ def test_find_xshift_non_square_larger_grid(gpu, oracle):
     assert steps == rsteps
     assert abs(e - re) <= 1e-8 * abs(re)
     assert np.abs(ph - rph).max() * (nx - 1) <= 1e-4
+
+
+def test_find_xshift_batch_equals_single_calls(gpu):
+    """Images spread over worker threads with their own streams: every image's
+    result equals, bit for bit, its own single call."""
+    nx, ny = 65, 17
+    Rs, Ts = zip(*[_shifted_lines(nx, ny, s, 20 + i) for i, s in enumerate((1.0, -0.5, 2.0, 0.0, 1.5))])
+    R = np.stack(Rs)
+    T = np.stack(Ts)
+    ph, en, st = gpu.find_xshift_batch(R, T, 0.01, 1.0, 30, workers=3)
+    for i in range(len(T)):
+        p1, e1, s1 = gpu.find_xshift(R[i], T[i], 0.01, 1.0, 30)
+        assert np.array_equal(ph[i], p1) and en[i] == e1 and st[i] == s1
+    # one reference for all images
+    ph2, en2, _ = gpu.find_xshift_batch(R[0], T, 0.01, 1.0, 30, workers=2)
+    p1, e1, _ = gpu.find_xshift(R[0], T[3], 0.01, 1.0, 30)
+    assert np.array_equal(ph2[3], p1) and en2[3] == e1
