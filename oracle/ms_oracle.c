@@ -1698,6 +1698,8 @@ int msor_xshift(int nx, int ny, const double* R, const double* T, double lambda,
   for (int i = 0; i < N; ++i) phix[i] /= scale;
   double tau = 1.0, sigma = 1.0;
   const double stop_sigma = 0.0001, sigma_tol = 0.00001, stop_eps = 0.;
+  band_chol_t chol = {0, 0, NULL};
+  double chol_sigma = 0.;
   double energy = xs_energy(&C, phix), energy_new = energy;
   int iter = 0, n_trace = 0, go = max_iter > 0;
   while (go) {
@@ -1708,7 +1710,16 @@ int msor_xshift(int nx, int ny, const double* R, const double* T, double lambda,
     const double sigma_used = sigma;
     xs_gradient(&C, phix, DE);
     for (int i = 0; i < N; ++i) d[i] = DE[i] * -1.;
-    msor_h1_metric(nx, ny, sigma, d);
+    /* the factorisation is redone only when the filter width changes
+     * (InverseH1MetricBase::setTau, linearSmoothOp.h:283-288) */
+    if (!chol.L || chol_sigma != sigma) {
+      free(chol.L);
+      double* sys = rect_system(nx, ny, 1.0, (double)(0.5f * sqr(sigma)));
+      chol = band_chol(sys, nx, ny);
+      free(sys);
+      chol_sigma = sigma;
+    }
+    band_chol_solve(&chol, d);
     double beta = 0.;
     if ((iter - 1) % 10) beta = dot(d, d, N) / dot(og, og, N);
     memcpy(og, d, sizeof(double) * N);
@@ -1743,6 +1754,7 @@ int msor_xshift(int nx, int ny, const double* R, const double* T, double lambda,
   }
   for (int i = 0; i < N; ++i) phix[i] *= scale;
   if (energy_out) *energy_out = energy_new;
+  free(chol.L);
   free(buf);
   return iter;
 }
