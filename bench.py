@@ -728,6 +728,34 @@ def main_seismic(args, world, rank, local):
             launches += ctx.stats()["kernel_launches"]
         elapsed = allreduce_max(time.perf_counter() - t0, world)
     value = world * G * args.steps / elapsed
+    # the data term's kernel (k_lineshift with its derivative) over all gathers in
+    # one launch: R, T, phi read and DE written once per gather (inputs > L2)
+    dev = torch.device("cuda", local)
+    N = nx * ny
+    d_R = torch.from_numpy(np.ascontiguousarray(np.broadcast_to(R, gathers.shape))).to(dev)
+    d_T = torch.from_numpy(gathers).to(dev)
+    d_phi = torch.from_numpy(ph).to(dev)
+    d_de = torch.empty_like(d_T)
+    d_e = torch.empty(G, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def data_term():
+        ctx.lineshift_energy_device(nx, ny, G, d_R.data_ptr(), d_T.data_ptr(), d_phi.data_ptr(), d_e.data_ptr(),
+                                    d_de.data_ptr(), stream.cuda_stream)
+
+    for _ in range(3):
+        data_term()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 20
+    torch.cuda.synchronize(dev)
+    ev0.record(stream)
+    for _ in range(reps):
+        data_term()
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    ls_ms = ev0.elapsed_time(ev1) / reps
+    ls_bytes = G * N * 8 * 4 + G * ny * 8
+    peak, peak_kind = measured_peak()
     if rank == 0:
         clk = clocks.summary()
         cpu = accuracy = None
@@ -767,7 +795,11 @@ def main_seismic(args, world, rank, local):
             "e2e": {"value": value, "unit": "gathers/s", "h2d_bytes_per_step": 2 * G * nx * ny * 8 + nx * ny * 8,
                     "d2h_bytes_per_step": G * nx * ny * 8},
             "gpu_launches": launches,
-            "roofline": None,
+            "roofline": {"bound": "hbm", "kernel": f"k_lineshift with its derivative, all {G} gathers in one launch "
+                                                   f"(timed after the descents, {reps} launches)",
+                         "achieved": ls_bytes / (ls_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": ls_bytes / (ls_ms * 1e-3) / 1e9 / peak, "peak_kind": peak_kind, "traffic": None,
+                         "algorithmic_bytes_per_launch": ls_bytes, "avg_launch_ms": ls_ms},
             "cpu_baseline": cpu,
             "accuracy": accuracy,
             "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
@@ -798,6 +830,8 @@ def main():
                     help="small case for ncu: one displacement composition at this level, no timing")
     ap.add_argument("--profile-series", action="store_true",
                     help="small case for ncu: one msgpu_match_series call on the bench's frames, no timing")
+    ap.add_argument("--profile-seismic", type=int, default=0,
+                    help="small case for ncu: findXShift of one gather 257 x 2049 with this many steps, no timing")
     ap.add_argument("--seismic", action="store_true",
                     help="the seismic line-shift model: findXShift of 32 gathers 257 x 2049")
     ap.add_argument("--ragged", action="store_true",
@@ -814,6 +848,16 @@ def main():
         return profile_case(args.profile_level, args.profile_iters, not args.fp32)
     if args.profile_compose or args.profile_series:
         return profile_series(args.profile_compose, not args.fp32)
+    if args.profile_seismic:
+        import msgpu
+        from msgpu import build as mbuild
+        from msgpu import synthetic as syn
+        mbuild.build()
+        g = syn.seismic_gathers(2, seed=4000)
+        ctx = msgpu.Context(0)
+        _, e, st = ctx.find_xshift(g.mean(axis=0), g[0], SEIS_LAMBDA, SEIS_YREG, args.profile_seismic)
+        print(json.dumps({"profile_seismic_steps": st, "energy": e, "launches": ctx.stats()["kernel_launches"]}))
+        return 0
     world, rank, local = dist_setup()
     if args.impl == "reference":
         return run_reference_arm(args, world, rank)

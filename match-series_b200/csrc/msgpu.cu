@@ -1800,7 +1800,7 @@ struct XsSolver {
   int dot(const double* a, const double* b, double* out) {
     const int nb = std::min(1024, (N + 255) / 256);
     k_dot_part<<<nb, 256, 0, st>>>(a, b, N, B.part);
-    k_sum_serial<<<1, 1, 0, st>>>(B.part, nb, B.scal);
+    k_sum_part<<<1, 256, 0, st>>>(B.part, nb, B.scal);
     CK(cudaMemcpyAsync(out, B.scal, sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     ctx->stats.kernel_launches += 2;
@@ -1813,10 +1813,10 @@ struct XsSolver {
     a.e_line = (double*)ctx->nccbuf.p; a.de = de; a.t = lt;
     const size_t smem = sizeof(double) * 3 * (size_t)nx;
     k_lineshift<<<dim3(ny, 1), kLineThreads, smem, st>>>(a);
-    k_lineshift_total<<<1, 32, 0, st>>>(a.e_line, ny, 1, B.scal + 1);
+    k_lineshift_total<<<1, 256, 0, st>>>(a.e_line, ny, B.scal + 1);
     const int nb = std::min(1024, (N + 255) / 256);
     k_xshift_reg<<<dim3(nb, 1), 256, 0, st>>>(rt, nx, ny, (size_t)N, p, B.kphi, B.part);
-    k_xshift_reg_total<<<1, 32, 0, st>>>(B.part, nb, 1, B.scal + 2);
+    k_xshift_reg_total<<<1, 256, 0, st>>>(B.part, nb, B.scal + 2);
     ctx->stats.kernel_launches += 4;
     CK(cudaGetLastError());
     return MSGPU_OK;
@@ -2066,7 +2066,7 @@ int msgpu_lineshift_energy_device(msgpu_context* ctx, int nx, int ny, int num_im
   a.t = host_line_tables(nx);
   CK(cudaFuncSetAttribute(k_lineshift, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_lineshift<<<dim3(ny, num_images), kLineThreads, smem, st>>>(a);
-  k_lineshift_total<<<(num_images + 127) / 128, 128, 0, st>>>(a.e_line, ny, num_images, d_energy_out);
+  k_lineshift_total<<<num_images, 256, 0, st>>>(a.e_line, ny, d_energy_out);
   CK(cudaGetLastError());
   ctx->stats.kernel_launches = 2;
   return MSGPU_OK;
@@ -2108,8 +2108,7 @@ int msgpu_xshift_reg_device(msgpu_context* ctx, int nx, int ny, int num_images, 
   cudaStream_t st = (cudaStream_t)stream;
   k_xshift_reg<<<dim3(nb, num_images), 256, 0, st>>>(host_xreg_tables(nx, ny, yreg), nx, ny, (size_t)N, d_phix,
                                                      d_kphi_out, (double*)ctx->vals.p);
-  k_xshift_reg_total<<<(num_images + 127) / 128, 128, 0, st>>>((const double*)ctx->vals.p, nb, num_images,
-                                                               d_energy_out);
+  k_xshift_reg_total<<<num_images, 256, 0, st>>>((const double*)ctx->vals.p, nb, d_energy_out);
   CK(cudaGetLastError());
   ctx->stats.kernel_launches = 2;
   return MSGPU_OK;

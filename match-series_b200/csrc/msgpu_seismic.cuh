@@ -169,13 +169,38 @@ __global__ void __launch_bounds__(kLineThreads) k_lineshift(LineArgs a) {
   }
 }
 
-// Sum of the line energies in line order, divided by the line count.
-__global__ void k_lineshift_total(const double* e_line, int ny, int num_images, double* out) {
-  const int img = blockIdx.x * blockDim.x + threadIdx.x;
-  if (img >= num_images) return;
+// Sum of the line energies in line order, divided by the line count: one
+// block per image stages the lines in shared memory (coalesced), one thread
+// adds them in order.
+__global__ void __launch_bounds__(256) k_lineshift_total(const double* e_line, int ny, double* out) {
+  __shared__ double buf[1024];
+  const double* e = e_line + (size_t)blockIdx.x * ny;
   double s = 0.;
-  for (int y = 0; y < ny; ++y) s += e_line[(size_t)img * ny + y];
-  out[img] = s / ny;
+  for (int y0 = 0; y0 < ny; y0 += 1024) {
+    const int m = min(1024, ny - y0);
+    for (int i = threadIdx.x; i < m; i += blockDim.x) buf[i] = e[y0 + i];
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int i = 0; i < m; ++i) s += buf[i];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = s / ny;
+}
+
+// Sum of n values in a fixed order for a block of 256 threads: strided
+// per-thread sums, a shuffle tree per warp, the eight warps in order
+// (thread 0 holds the result).
+__device__ __forceinline__ double block_fixed_sum(const double* v, int n, double* red) {
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += 256) s += v[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < 8; ++w) t += red[w];
+  return t;
 }
 
 // findXShift's regulariser: K phi with the assembled nine-point rows of the
@@ -217,12 +242,11 @@ __global__ void __launch_bounds__(256) k_xshift_reg(XRegTables tb, int nx, int n
   }
 }
 
-__global__ void k_xshift_reg_total(const double* part, int nblocks, int num_images, double* out) {
-  const int img = blockIdx.x * blockDim.x + threadIdx.x;
-  if (img >= num_images) return;
-  double s = 0.0;
-  for (int b = 0; b < nblocks; ++b) s += part[(size_t)img * nblocks + b];
-  out[img] = 0.5 * s;
+// E = 1/2 phi.K phi from the block partials, one block (256 threads) per image
+__global__ void __launch_bounds__(256) k_xshift_reg_total(const double* part, int nblocks, double* out) {
+  __shared__ double red[8];
+  const double s = block_fixed_sum(part + (size_t)blockIdx.x * nblocks, nblocks, red);
+  if (threadIdx.x == 0) out[blockIdx.x] = 0.5 * s;
 }
 
 // --- vector kernels of the seismic descent ----------------------------------
@@ -243,7 +267,7 @@ __global__ void k_divide(double* a, double s, int n) {
 __global__ void k_mul(const double* a, double s, double* out, int n) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = a[i] * s;
 }
-// a[i] * b[i] summed per block in a fixed order (partials, then one serial sum)
+// a[i] * b[i] summed per block in a fixed order (partials, then k_sum_part)
 __global__ void __launch_bounds__(256) k_dot_part(const double* a, const double* b, int n, double* part) {
   __shared__ double red[8];
   double acc = 0.0;
@@ -258,10 +282,10 @@ __global__ void __launch_bounds__(256) k_dot_part(const double* a, const double*
     part[blockIdx.x] = s;
   }
 }
-__global__ void k_sum_serial(const double* part, int n, double* out) {
-  double s = 0.0;
-  for (int i = 0; i < n; ++i) s += part[i];
-  *out = s;
+__global__ void __launch_bounds__(256) k_sum_part(const double* part, int n, double* out) {
+  __shared__ double red[8];
+  const double s = block_fixed_sum(part, n, red);
+  if (threadIdx.x == 0) *out = s;
 }
 // Spectral scaling of the H1 metric: z[y][x] /= 1 + tau (lx[x] + ly[y])
 __global__ void k_spectral_scale(double* z, const double* lx, const double* ly, double tau, int nx, int ny) {

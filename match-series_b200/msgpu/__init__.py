@@ -370,6 +370,11 @@ class Context:
                                                  ctypes.byref(e), _p(de) if de is not None else None))
         return e.value, de
 
+    def lineshift_energy_device(self, nx, ny, num_images, d_R, d_T, d_phix, d_energy, d_de, stream):
+        """msgpu_lineshift_energy_device on device pointers (d_de may be 0)."""
+        self._check(lib().msgpu_lineshift_energy_device(self._h, nx, ny, num_images, d_R, d_T, d_phix, d_energy,
+                                                        d_de or None, stream))
+
     def xshift_reg(self, phix, yreg):
         """findXShift's regulariser: (1/2 phi.K phi, K phi)."""
         phix = _f64(phix)
