@@ -348,6 +348,65 @@ int msgpu_gd_level_noalloc(int level, const double* d_R, const double* d_T, doub
                            int max_iter, double stop_eps, int use_fp64, double* d_energy_out, int* d_steps_out,
                            void* stream);
 
+/* --- learned warm start (no counterpart in the reference) -----------------
+ * A U-Net on 2^l+1 node grids maps the prepared reference and template of a
+ * frame pair at the network's input level l0 to a displacement at level
+ * l0-1, which starts the gradient flow there instead of the coarse levels
+ * startLevel..l0-1 of the plain method.  Encoder 16-32-64-128 channels
+ * (3x3 convolutions, stride-2 convolutions between the node grids), decoder
+ * by bilinear prolongation and [skip | upsampled] concatenation down to
+ * level l0-1, ReLU, a 2-channel head; bf16 weights and activations, fp32
+ * accumulation (tensor pipe), fp32 master parameters trained with Adam on
+ * the mean squared difference to the plain method's displacements.
+ * Parameter layout (msgpu_net_get_params): layer after layer (e0a e0b e1a
+ * e1b e2a e2b e3a e3b d2a d2b d1a d1b head), W[cout][3][3][cin] then b[cout]. */
+typedef struct msgpu_net msgpu_net;
+long long msgpu_net_num_params(void);
+/* input_level l0 in 4..11; parameters He-initialised from seed.            */
+int msgpu_net_create(msgpu_context* ctx, int input_level, unsigned long long seed, msgpu_net** out);
+int msgpu_net_destroy(msgpu_net* net);
+int msgpu_net_input_level(const msgpu_net* net);
+int msgpu_net_get_params(msgpu_net* net, float* out);
+int msgpu_net_set_params(msgpu_net* net, const float* in);   /* resets Adam */
+int msgpu_net_save(msgpu_net* net, const char* path);
+int msgpu_net_load(msgpu_net* net, const char* path);
+/* Prediction for `batch` pairs of prepared images at level l0 (device):
+ * reference image i at d_R + i * r_stride (r_stride 0: one shared
+ * reference), template i at d_T + i * N0; d_phi_out: batch x 2 x N1
+ * doubles ([x | y] per frame, domain units, level l0-1).                    */
+int msgpu_net_predict_device(msgpu_net* net, const double* d_R, long long r_stride, const double* d_T, int batch,
+                             double* d_phi_out, void* stream);
+/* One Adam step on a batch against target displacements (batch x 2 x N1,
+ * domain units); loss_out (host, nullable): the batch's mean squared
+ * difference in pixels of level l0-1, before the step.                      */
+int msgpu_net_train_step_device(msgpu_net* net, const double* d_R, long long r_stride, const double* d_T,
+                                const double* d_phi_target, int batch, float lr, float* loss_out, void* stream);
+/* Loss, prediction and the flat parameter gradient without an update (host
+ * arrays; R and T: batch images each).                                      */
+int msgpu_net_loss_grad(msgpu_net* net, const double* R, const double* T, const double* phi_target, int batch,
+                        float* loss_out, double* phi_out, float* grad_out);
+/* The images of the registration path prepared (prepareMultilevelArray,
+ * registration.h:331-367) and restricted to `level`: count images of
+ * input_level in, count images of `level` out (device).                     */
+int msgpu_prepare_images_device(msgpu_context* ctx, const msgpu_params* p, const double* d_images, int count,
+                                int level, double* d_out, void* stream);
+/* msgpu_register_batch started from the network's prediction at level
+ * l0-1 (which must lie in startLevel..stopLevel; inputLevel >= l0).  With
+ * plain_energies (the plain method's final energies, nullable), a frame
+ * whose warm-started energy exceeds its plain energy by more than
+ * rel_tol * |plain energy| is registered again from the plain start;
+ * warm_used_out[f] (host, nullable) = 1 where the warm start was kept.
+ * steps_out has the plain layout (stop-start+1 levels per frame; levels
+ * below l0-1 count 0 for warm-started frames).                             */
+int msgpu_register_batch_warm(msgpu_context* ctx, const msgpu_params* p, msgpu_net* net, const double* reference,
+                              const double* templates, int num_templates, const double* plain_energies,
+                              double rel_tol, double* phis_out, double* energies_out, int* steps_out,
+                              int* warm_used_out);
+int msgpu_register_batch_warm_device(msgpu_context* ctx, const msgpu_params* p, msgpu_net* net,
+                                     const double* d_reference, const double* d_templates, int num_templates,
+                                     const double* d_plain_energies, double rel_tol, double* d_phis_out,
+                                     double* d_energies_out, int* d_steps_out, int* warm_used_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -28,6 +28,7 @@
 #include "msgpu_level.cuh"
 #include "msgpu_series.cuh"
 #include "msgpu_seismic.cuh"
+#include "msgpu_unet.cuh"
 
 using namespace msg;
 
@@ -683,6 +684,51 @@ int sched_error_check(msgpu_context* ctx) {
 // Upper bound on the CTAs of a level launch (for the per-CTA pass counters).
 int max_level_grid(int sms) { return 4 * sms; }
 
+// Image preparation of prepareMultilevelArray (registration.h:331-367) on
+// nimg images already copied to their pyramid rows at the input level:
+// exact saturated min/max by radix selection, clamp, scale to [0,1]
+// (vec.h:864-871, 1084-1089), then RestrictOp<STD_QUOC_RESTRICT> down to
+// level 0 (multilevelArray.h:94-110).  mm: 2 * nimg doubles of scratch.
+int prepare_pyramid(msgpu_context* ctx, const msgpu_params& p, double* pyr, const std::vector<size_t>& poff,
+                    size_t pstride, int nimg, double* mm, cudaStream_t st) {
+  const int Lin = p.input_level;
+  const size_t Nin = lvl_N(Lin);
+  int& launches = ctx->stats.kernel_launches;
+  if (!p.dont_normalize_input) {
+    if (p.saturation_percent >= 0) {
+      const int m1 = (int)Nin - 1;
+      int il = (int)(p.saturation_percent / 200 * m1), ih = (int)((1 - p.saturation_percent / 200) * m1);
+      il = std::min(std::max(il, 0), m1);
+      ih = std::min(std::max(ih, 0), m1);
+      k_select2<<<nimg, kSelThreads, 0, st>>>(pyr + poff[Lin], pstride, (int)Nin, il, ih, mm);
+    } else {
+      k_minmax<<<nimg, 1024, 0, st>>>(pyr + poff[Lin], pstride, (int)Nin, mm);
+    }
+    CK(cudaGetLastError());
+    k_normalize<<<dim3((unsigned)std::min<size_t>(1024, (Nin + 255) / 256), nimg), 256, 0, st>>>(
+        pyr + poff[Lin], pstride, (int)Nin, mm, p.saturation_percent >= 0 ? 1 : 0, p.normalize_min_to_zero);
+    CK(cudaGetLastError());
+    launches += 2;
+  }
+  for (int l = Lin; l >= 1; --l) {
+    const size_t cN = lvl_N(l - 1);
+    k_restrict<double><<<dim3((unsigned)std::min<size_t>(1024, (cN + 255) / 256), nimg), 256, 0, st>>>(
+        pyr + poff[l], pstride, pyr + poff[l - 1], pstride, l);
+    ++launches;
+  }
+  CK(cudaGetLastError());
+  return MSGPU_OK;
+}
+
+// Pyramid rows of images at input level Lin: offsets of the levels (finest
+// first) and the row stride, in doubles.
+size_t pyramid_layout(int Lin, std::vector<size_t>& poff) {
+  poff.assign(Lin + 1, 0);
+  size_t pstride = 0;
+  for (int l = Lin; l >= 0; --l) { poff[l] = pstride; pstride = align_up(pstride + lvl_N(l), 32); }
+  return pstride;
+}
+
 // ---------------------------------------------------------------------------
 struct BatchIO {
   const double* ref;        // device, input level
@@ -698,7 +744,11 @@ struct BatchOpts {
   int pairwise = 0;      // template i > 0 is registered to template i - 1 (series matching, matchSeries.h:141-155)
   int lambda_stop = -1;  // level that lambdaFactor's exponent counts from (default: stop_level)
   int reset_error = 1;   // clear the error flags (0: a caller running several batches clears them once)
+  msgpu_net* warm = nullptr;   // learned warm start: the network's prediction is the start-level displacement
 };
+
+int warm_start_phi(msgpu_net* net, const double* pyr, const std::vector<size_t>& poff, size_t pstride, int F,
+                   cudaStream_t st, double** phi);
 
 template <typename Real>
 int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& io, cudaStream_t st,
@@ -716,9 +766,8 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
   if (opt.reset_error && (rc = sched_error_reset(ctx, st))) return rc;
   if (ncc && (rc = ensure(ctx, ctx->nccbuf, sizeof(Real) * (comp_stride(M) + 64)))) return rc;
   // --- double scratch: per image a pyramid from Lin down to 0
-  std::vector<size_t> poff(Lin + 1);
-  size_t pstride = 0;
-  for (int l = Lin; l >= 0; --l) { poff[l] = pstride; pstride = align_up(pstride + lvl_N(l), 32); }
+  std::vector<size_t> poff;
+  const size_t pstride = pyramid_layout(Lin, poff);
   const int nlev_all = stop - start + 1;
   const size_t small_bytes = sizeof(double) * (2 * nimg + 2 * F + 64) + sizeof(int) * ((2 * nlev_all + 4) * F + 64);
   if ((rc = ensure(ctx, ctx->dscratch, sizeof(double) * pstride * nimg))) return rc;
@@ -749,29 +798,8 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
                        Nin * sizeof(double), 1, cudaMemcpyDeviceToDevice, st));
   CK(cudaMemcpy2DAsync(pyr + pstride + poff[Lin], pstride * sizeof(double), io.tmpl, Nin * sizeof(double),
                        Nin * sizeof(double), F, cudaMemcpyDeviceToDevice, st));
-  if (!p.dont_normalize_input) {
-    if (p.saturation_percent >= 0) {
-      const int m1 = (int)Nin - 1;
-      int il = (int)(p.saturation_percent / 200 * m1), ih = (int)((1 - p.saturation_percent / 200) * m1);
-      il = std::min(std::max(il, 0), m1);
-      ih = std::min(std::max(ih, 0), m1);
-      k_select2<<<nimg, kSelThreads, 0, st>>>(pyr + poff[Lin], pstride, (int)Nin, il, ih, mm);
-    } else {
-      k_minmax<<<nimg, 1024, 0, st>>>(pyr + poff[Lin], pstride, (int)Nin, mm);
-    }
-    CK(cudaGetLastError());
-    k_normalize<<<dim3((unsigned)std::min<size_t>(1024, (Nin + 255) / 256), nimg), 256, 0, st>>>(
-        pyr + poff[Lin], pstride, (int)Nin, mm, p.saturation_percent >= 0 ? 1 : 0, p.normalize_min_to_zero);
-    CK(cudaGetLastError());
-    launches += 2;
-  }
-  // 2. pyramid (double), then Real copies of the levels 0..M
-  for (int l = Lin; l >= 1; --l) {
-    const size_t cN = lvl_N(l - 1);
-    k_restrict<double><<<dim3((unsigned)std::min<size_t>(1024, (cN + 255) / 256), nimg), 256, 0, st>>>(
-        pyr + poff[l], pstride, pyr + poff[l - 1], pstride, l);
-    ++launches;
-  }
+  if ((rc = prepare_pyramid(ctx, p, pyr, poff, pstride, nimg, mm, st))) return rc;
+  // 2. Real copies of the levels 0..M
   CK(cudaGetLastError());
   for (int l = 0; l <= M; ++l) {
     const size_t Nl = lvl_N(l);
@@ -787,7 +815,15 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
   ++launches;
   {
     const size_t Ns = lvl_N(start);
-    if (io.init_phi) {
+    if (opt.warm) {
+      double* wphi;
+      if ((rc = warm_start_phi(opt.warm, pyr, poff, pstride, F, st, &wphi))) return rc;
+      for (int c = 0; c < 2; ++c)
+        k_to_pitched<double, Real><<<dim3((unsigned)std::min<size_t>(1024, (Ns + 255) / 256), F), 256, 0, st>>>(
+            wphi + (size_t)c * Ns, 2 * Ns, arena + L.off_phi[0] + (size_t)c * comp_stride(start), L.stride,
+            lvl_n(start));
+      launches += 2;
+    } else if (io.init_phi) {
       // restrict the initial displacement in double inside the template pyramid scratch of level < M
       // storage: reuse the double scratch rows of the templates (already converted)
       double* tmp = pyr + pstride;  // F images, 2 components need 2F slots: use pairs of images
@@ -2679,3 +2715,692 @@ extern "C" int msgpu_gd_level_noalloc(int level, const double* d_R, const double
                   : noalloc_level<float>(*dv, level, d_R, d_T, d_phi, lambda, max_iter, stop_eps, d_energy_out,
                                          d_steps_out, st);
 }
+
+// ---------------------------------------------------------------------------
+// Learned warm start: the U-Net of msgpu_unet.cuh, its training step and its
+// use as the start of the gradient flow.
+
+namespace {
+using msg::unet::bf16;
+
+struct NetLayer {
+  int cin, cout, stride, relu;
+  int cin_pad, cout_pad;
+  size_t w_off, b_off;     // in theta / grad (floats)
+  size_t wf_off, wt_off;   // in the packed bf16 weights
+};
+
+// (cin, cout, stride, relu) of e0a e0b e1a e1b e2a e2b e3a e3b d2a d2b d1a d1b head
+constexpr int kNetLayers = 13;
+constexpr int kNetSpec[kNetLayers][4] = {{2, 16, 1, 1},   {16, 16, 1, 1},  {16, 32, 2, 1},   {32, 32, 1, 1},
+                                         {32, 64, 2, 1},  {64, 64, 1, 1},  {64, 128, 2, 1},  {128, 128, 1, 1},
+                                         {192, 64, 1, 1}, {64, 64, 1, 1},  {96, 32, 1, 1},   {32, 32, 1, 1},
+                                         {32, 2, 1, 0}};
+enum { E0A, E0B, E1A, E1B, E2A, E2B, E3A, E3B, D2A, D2B, D1A, D1B, HEAD };
+
+inline int pad16(int c) { return (c + 15) / 16 * 16; }
+// widest tile of 64, 32 or 16 channels that divides a padded channel count
+inline int tile_of(int rows) { return rows % 64 == 0 ? 64 : (rows % 32 == 0 ? 32 : 16); }
+
+// An NHWC bf16 tensor view: base (channel offset applied), image stride,
+// nodes per side, elements per node.
+struct View {
+  bf16* p;
+  size_t img;
+  int n, cs;
+  View ch(int c0) const { return View{p + c0, img, n, cs}; }
+};
+}  // namespace
+
+struct msgpu_net {
+  msgpu_context* ctx = nullptr;
+  int level = 0;          // input grid 2^level + 1; output grid one level coarser
+  int n[4] = {};          // nodes per side of the four grids
+  NetLayer L[kNetLayers];
+  size_t nparams = 0, npacked = 0;
+  float *theta = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr;
+  bf16 *wf = nullptr, *wt = nullptr;
+  long long step = 0;
+  int batch = 0;                         // images the activation buffers hold
+  msgpu_context::Buf act, part, small, phi, gather;
+  // activations and their gradients (views into act)
+  View x0, a0, a1, b0, cat1, c0, cat2, d0, d1, g0, g1, h0, h1;
+  View dout, dh1, dh0, dcat1, dg1, dg0, dcat2, dd1, dd0, dc0, db0, da1, da0;
+  float* out = nullptr;                  // head output, 2 floats per node of grid 1
+};
+
+namespace {
+
+#define NCK(call)                                                                                 \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess)                                                                        \
+      return fail(net->ctx, MSGPU_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                  __FILE__, __LINE__);                                                            \
+  } while (0)
+
+size_t net_param_count() {
+  size_t n = 0;
+  for (int i = 0; i < kNetLayers; ++i) n += (size_t)kNetSpec[i][1] * 9 * kNetSpec[i][0] + kNetSpec[i][1];
+  return n;
+}
+
+int net_pack(msgpu_net* net, cudaStream_t st) {
+  for (int i = 0; i < kNetLayers; ++i) {
+    const NetLayer& l = net->L[i];
+    const int n = l.cout_pad * 9 * l.cin_pad;
+    msg::unet::k_pack_weights<<<std::min(1024, (n + 255) / 256), 256, 0, st>>>(
+        net->theta + l.w_off, l.cout, l.cin, l.cout_pad, l.cin_pad, net->wf + l.wf_off, net->wt + l.wt_off);
+  }
+  NCK(cudaGetLastError());
+  net->ctx->stats.kernel_launches += kNetLayers;
+  return MSGPU_OK;
+}
+
+// Activation buffers for `batch` images.
+int net_buffers(msgpu_net* net, int batch) {
+  if (batch <= net->batch) return MSGPU_OK;
+  const size_t N[4] = {(size_t)net->n[0] * net->n[0], (size_t)net->n[1] * net->n[1], (size_t)net->n[2] * net->n[2],
+                       (size_t)net->n[3] * net->n[3]};
+  struct Spec { View* v; int g, c; };
+  Spec specs[] = {{&net->x0, 0, 16},   {&net->a0, 0, 16},   {&net->a1, 0, 16},   {&net->b0, 1, 32},
+                  {&net->cat1, 1, 96}, {&net->c0, 2, 64},   {&net->cat2, 2, 192}, {&net->d0, 3, 128},
+                  {&net->d1, 3, 128},  {&net->g0, 2, 64},   {&net->g1, 2, 64},   {&net->h0, 1, 32},
+                  {&net->h1, 1, 32},   {&net->dout, 1, 16}, {&net->dh1, 1, 32},  {&net->dh0, 1, 32},
+                  {&net->dcat1, 1, 96}, {&net->dg1, 2, 64}, {&net->dg0, 2, 64},  {&net->dcat2, 2, 192},
+                  {&net->dd1, 3, 128}, {&net->dd0, 3, 128}, {&net->dc0, 2, 64},  {&net->db0, 1, 32},
+                  {&net->da1, 0, 16},  {&net->da0, 0, 16}};
+  size_t total = 0;
+  for (const Spec& s : specs) total += align_up(N[s.g] * s.c * batch, 128);
+  const size_t out_floats = align_up(N[1] * 2 * batch, 64);
+  int rc;
+  if ((rc = ensure(net->ctx, net->act, total * sizeof(bf16) + out_floats * sizeof(float)))) return rc;
+  bf16* p = (bf16*)net->act.p;
+  for (const Spec& s : specs) {
+    *s.v = View{p, N[s.g] * s.c, net->n[s.g], s.c};
+    p += align_up(N[s.g] * s.c * batch, 128);
+  }
+  net->out = (float*)p;
+  // zero once: padding channels of the input and of the loss gradient stay zero
+  NCK(cudaMemset(net->act.p, 0, total * sizeof(bf16) + out_floats * sizeof(float)));
+  net->batch = batch;
+  return MSGPU_OK;
+}
+
+int net_conv_launch(msgpu_net* net, const msg::unet::ConvArgs& a, int rows, cudaStream_t st) {
+  const int bn = tile_of(rows);
+  const dim3 grid((unsigned)((a.total + msg::unet::kBM - 1) / msg::unet::kBM), (unsigned)(rows / bn));
+  if (bn == 64) msg::unet::k_conv<64><<<grid, msg::unet::kThreads, 0, st>>>(a);
+  else if (bn == 32) msg::unet::k_conv<32><<<grid, msg::unet::kThreads, 0, st>>>(a);
+  else msg::unet::k_conv<16><<<grid, msg::unet::kThreads, 0, st>>>(a);
+  NCK(cudaGetLastError());
+  ++net->ctx->stats.kernel_launches;
+  return MSGPU_OK;
+}
+
+// forward convolution of layer i: in -> out (bf16 view, or the float head output)
+int net_fwd(msgpu_net* net, int i, const View& in, const View* out, int B, cudaStream_t st) {
+  const NetLayer& l = net->L[i];
+  msg::unet::ConvArgs a;
+  memset(&a, 0, sizeof(a));
+  a.in = in.p; a.in_img = in.img; a.in_n = in.n; a.in_cs = in.cs; a.cin = l.cin_pad;
+  a.w = net->wf + l.wf_off;
+  a.bias = net->theta + l.b_off;
+  const int on = (in.n - 1) / l.stride + 1;
+  if (out) {
+    a.out = out->p; a.out_img = out->img; a.out_n = out->n; a.out_cs = out->cs;
+  } else {
+    a.out = net->out; a.out_img = (size_t)on * on * 2; a.out_n = on; a.out_cs = 2; a.out_f32 = 1;
+  }
+  a.cout = l.cout;
+  a.mode = 0; a.stride = l.stride; a.relu = l.relu;
+  a.total = B * on * on;
+  return net_conv_launch(net, a, l.cout_pad, st);
+}
+
+// data gradient of layer i: dy (at its output) -> dx (at its input), times the
+// ReLU mask of the input activation; accumulate adds dx's current value first
+int net_bwd_data(msgpu_net* net, int i, const View& dy, const View& dx, const View& mask, int accumulate, int B,
+                 cudaStream_t st) {
+  const NetLayer& l = net->L[i];
+  msg::unet::ConvArgs a;
+  memset(&a, 0, sizeof(a));
+  a.in = dy.p; a.in_img = dy.img; a.in_n = dy.n; a.in_cs = dy.cs; a.cin = l.cout_pad;
+  a.w = net->wt + l.wt_off;
+  a.out = dx.p; a.out_img = dx.img; a.out_n = dx.n; a.out_cs = dx.cs; a.cout = l.cin;
+  a.mode = 1; a.stride = l.stride; a.accumulate = accumulate;
+  a.mask = mask.p; a.mask_img = mask.img; a.mask_cs = mask.cs;
+  a.total = B * dx.n * dx.n;
+  return net_conv_launch(net, a, l.cin_pad, st);
+}
+
+// weight and bias gradients of layer i from its input activation and the gradient at its output
+int net_bwd_weights(msgpu_net* net, int i, const View& in, const View& dy, int B, cudaStream_t st) {
+  const NetLayer& l = net->L[i];
+  const int K = 9 * l.cin_pad;
+  const int bm = tile_of(l.cout_pad);
+  const int xt = (K + 63) / 64, yt = l.cout_pad / bm;
+  const int total = B * dy.n * dy.n;
+  int chunks = std::max(1, (4 * net->ctx->sm_count + xt * yt - 1) / (xt * yt));
+  chunks = std::min(chunks, std::max(1, total / 256));
+  const int chunk = ((total + chunks - 1) / chunks + msg::unet::kBK - 1) / msg::unet::kBK * msg::unet::kBK;
+  chunks = (total + chunk - 1) / chunk;
+  const int bchunks = std::min(256, std::max(1, total / 512));
+  const int bchunk = (total + bchunks - 1) / bchunks;
+  const size_t need = (size_t)chunks * l.cout_pad * K + (size_t)bchunks * l.cout;
+  int rc;
+  if ((rc = ensure(net->ctx, net->part, need * sizeof(float)))) return rc;
+  float* part = (float*)net->part.p;
+  msg::unet::WgradArgs a;
+  a.in = in.p; a.in_img = in.img; a.in_n = in.n; a.in_cs = in.cs; a.cin = l.cin_pad;
+  a.dy = dy.p; a.dy_img = dy.img; a.dy_n = dy.n; a.dy_cs = dy.cs; a.cout_pad = l.cout_pad;
+  a.stride = l.stride; a.part = part; a.total = total; a.chunk = chunk;
+  const dim3 grid((unsigned)xt, (unsigned)yt, (unsigned)chunks);
+  if (bm == 64) msg::unet::k_wgrad<64><<<grid, msg::unet::kThreads, 0, st>>>(a);
+  else if (bm == 32) msg::unet::k_wgrad<32><<<grid, msg::unet::kThreads, 0, st>>>(a);
+  else msg::unet::k_wgrad<16><<<grid, msg::unet::kThreads, 0, st>>>(a);
+  const int nw = l.cout * 9 * l.cin;
+  msg::unet::k_wgrad_reduce<<<std::min(1024, (nw + 255) / 256), 256, 0, st>>>(part, chunks, l.cout, l.cout_pad, l.cin,
+                                                                              l.cin_pad, net->grad + l.w_off);
+  float* bpart = part + (size_t)chunks * l.cout_pad * K;
+  msg::unet::k_bgrad_part<<<bchunks, 128, 0, st>>>(dy.p, dy.img, dy.n * dy.n, dy.cs, l.cout, total, bchunk, bpart);
+  msg::unet::k_bgrad_reduce<<<1, 128, 0, st>>>(bpart, bchunks, l.cout, net->grad + l.b_off);
+  NCK(cudaGetLastError());
+  net->ctx->stats.kernel_launches += 4;
+  return MSGPU_OK;
+}
+
+int net_up(msgpu_net* net, const View& src, const View& dst, int C, int B, cudaStream_t st) {
+  const size_t total = (size_t)B * dst.n * dst.n * C;
+  msg::unet::k_up<<<(unsigned)std::min<size_t>(4096, (total + 255) / 256), 256, 0, st>>>(
+      src.p, src.img, src.n, src.cs, dst.p, dst.img, dst.cs, C, B);
+  NCK(cudaGetLastError());
+  ++net->ctx->stats.kernel_launches;
+  return MSGPU_OK;
+}
+
+int net_up_back(msgpu_net* net, const View& df, const View& dc, const View& mask, int C, int B, cudaStream_t st) {
+  const size_t total = (size_t)B * dc.n * dc.n * C;
+  msg::unet::k_up_back<<<(unsigned)std::min<size_t>(4096, (total + 255) / 256), 256, 0, st>>>(
+      df.p, df.img, df.n, df.cs, dc.p, dc.img, dc.cs, mask.p, mask.img, mask.cs, C, B);
+  NCK(cudaGetLastError());
+  ++net->ctx->stats.kernel_launches;
+  return MSGPU_OK;
+}
+
+// Forward pass on the packed input x0 of B images; output in net->out.
+int net_forward(msgpu_net* net, int B, cudaStream_t st) {
+  int rc;
+  msgpu_net& n = *net;
+  if ((rc = net_fwd(net, E0A, n.x0, &n.a0, B, st)) || (rc = net_fwd(net, E0B, n.a0, &n.a1, B, st)) ||
+      (rc = net_fwd(net, E1A, n.a1, &n.b0, B, st))) return rc;
+  const View s1 = n.cat1.ch(0), up1 = n.cat1.ch(32), s2 = n.cat2.ch(0), up2 = n.cat2.ch(64);
+  if ((rc = net_fwd(net, E1B, n.b0, &s1, B, st)) || (rc = net_fwd(net, E2A, s1, &n.c0, B, st)) ||
+      (rc = net_fwd(net, E2B, n.c0, &s2, B, st)) || (rc = net_fwd(net, E3A, s2, &n.d0, B, st)) ||
+      (rc = net_fwd(net, E3B, n.d0, &n.d1, B, st)) || (rc = net_up(net, n.d1, up2, 128, B, st)) ||
+      (rc = net_fwd(net, D2A, n.cat2, &n.g0, B, st)) || (rc = net_fwd(net, D2B, n.g0, &n.g1, B, st)) ||
+      (rc = net_up(net, n.g1, up1, 64, B, st)) || (rc = net_fwd(net, D1A, n.cat1, &n.h0, B, st)) ||
+      (rc = net_fwd(net, D1B, n.h0, &n.h1, B, st)) || (rc = net_fwd(net, HEAD, n.h1, nullptr, B, st)))
+    return rc;
+  return MSGPU_OK;
+}
+
+// Backward pass from net->dout: every parameter gradient into net->grad.
+int net_backward(msgpu_net* net, int B, cudaStream_t st) {
+  int rc;
+  msgpu_net& n = *net;
+  const View none{nullptr, 0, 0, 0};
+  const View s1 = n.cat1.ch(0), s2 = n.cat2.ch(0);
+  const View ds1 = n.dcat1.ch(0), dup1 = n.dcat1.ch(32), ds2 = n.dcat2.ch(0), dup2 = n.dcat2.ch(64);
+  if ((rc = net_bwd_weights(net, HEAD, n.h1, n.dout, B, st)) ||
+      (rc = net_bwd_data(net, HEAD, n.dout, n.dh1, n.h1, 0, B, st)) ||
+      (rc = net_bwd_weights(net, D1B, n.h0, n.dh1, B, st)) ||
+      (rc = net_bwd_data(net, D1B, n.dh1, n.dh0, n.h0, 0, B, st)) ||
+      (rc = net_bwd_weights(net, D1A, n.cat1, n.dh0, B, st)) ||
+      (rc = net_bwd_data(net, D1A, n.dh0, n.dcat1, none, 0, B, st)) ||
+      (rc = net_up_back(net, dup1, n.dg1, n.g1, 64, B, st)) ||
+      (rc = net_bwd_weights(net, D2B, n.g0, n.dg1, B, st)) ||
+      (rc = net_bwd_data(net, D2B, n.dg1, n.dg0, n.g0, 0, B, st)) ||
+      (rc = net_bwd_weights(net, D2A, n.cat2, n.dg0, B, st)) ||
+      (rc = net_bwd_data(net, D2A, n.dg0, n.dcat2, none, 0, B, st)) ||
+      (rc = net_up_back(net, dup2, n.dd1, n.d1, 128, B, st)) ||
+      (rc = net_bwd_weights(net, E3B, n.d0, n.dd1, B, st)) ||
+      (rc = net_bwd_data(net, E3B, n.dd1, n.dd0, n.d0, 0, B, st)) ||
+      (rc = net_bwd_weights(net, E3A, s2, n.dd0, B, st)) ||
+      (rc = net_bwd_data(net, E3A, n.dd0, ds2, s2, 1, B, st)) ||
+      (rc = net_bwd_weights(net, E2B, n.c0, ds2, B, st)) ||
+      (rc = net_bwd_data(net, E2B, ds2, n.dc0, n.c0, 0, B, st)) ||
+      (rc = net_bwd_weights(net, E2A, s1, n.dc0, B, st)) ||
+      (rc = net_bwd_data(net, E2A, n.dc0, ds1, s1, 1, B, st)) ||
+      (rc = net_bwd_weights(net, E1B, n.b0, ds1, B, st)) ||
+      (rc = net_bwd_data(net, E1B, ds1, n.db0, n.b0, 0, B, st)) ||
+      (rc = net_bwd_weights(net, E1A, n.a1, n.db0, B, st)) ||
+      (rc = net_bwd_data(net, E1A, n.db0, n.da1, n.a1, 0, B, st)) ||
+      (rc = net_bwd_weights(net, E0B, n.a0, n.da1, B, st)) ||
+      (rc = net_bwd_data(net, E0B, n.da1, n.da0, n.a0, 0, B, st)) ||
+      (rc = net_bwd_weights(net, E0A, n.x0, n.da0, B, st)))
+    return rc;
+  return MSGPU_OK;
+}
+
+int net_input(msgpu_net* net, const double* R, size_t r_stride, const double* T, size_t t_stride, int B,
+              cudaStream_t st) {
+  int rc;
+  if ((rc = net_buffers(net, B))) return rc;
+  const size_t total = (size_t)B * net->n[0] * net->n[0];
+  msg::unet::k_pack_input<<<(unsigned)std::min<size_t>(4096, (total + 255) / 256), 256, 0, st>>>(
+      R, r_stride, T, t_stride, net->n[0] * net->n[0], B, net->x0.p);
+  NCK(cudaGetLastError());
+  ++net->ctx->stats.kernel_launches;
+  return MSGPU_OK;
+}
+
+// Loss of the head output against target displacements (B x 2 x N1, domain
+// units) into net->small (float at offset 0), its gradient into dout.
+int net_loss(msgpu_net* net, const double* target, int B, cudaStream_t st) {
+  int rc;
+  if ((rc = ensure(net->ctx, net->small, sizeof(float) * 1024))) return rc;
+  float* s = (float*)net->small.p;
+  const int N1 = net->n[1] * net->n[1];
+  const int blocks = std::min(512, (B * N1 + 255) / 256);
+  msg::unet::k_mse<<<blocks, 256, 0, st>>>(net->out, target, (double)(net->n[1] - 1), N1, B, net->dout.p, s + 8);
+  msg::unet::k_loss_total<<<1, 32, 0, st>>>(s + 8, blocks, s);
+  NCK(cudaGetLastError());
+  net->ctx->stats.kernel_launches += 2;
+  return MSGPU_OK;
+}
+
+int net_adam(msgpu_net* net, float lr, cudaStream_t st) {
+  net->step++;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.f - powf(b1, (float)net->step), c2 = 1.f - powf(b2, (float)net->step);
+  const int n = (int)net->nparams;
+  msg::unet::k_adam<<<std::min(2048, (n + 255) / 256), 256, 0, st>>>(net->theta, net->grad, net->m, net->v, n, lr, b1,
+                                                                    b2, 1e-8f, c1, c2);
+  NCK(cudaGetLastError());
+  ++net->ctx->stats.kernel_launches;
+  return net_pack(net, st);
+}
+
+// Prediction into the net's phi buffer (B x 2 x N1 doubles, domain units).
+int net_predict(msgpu_net* net, const double* R, size_t r_stride, const double* T, size_t t_stride, int B,
+                cudaStream_t st, double** phi_out) {
+  int rc;
+  if ((rc = net_input(net, R, r_stride, T, t_stride, B, st)) || (rc = net_forward(net, B, st))) return rc;
+  const int N1 = net->n[1] * net->n[1];
+  if ((rc = ensure(net->ctx, net->phi, sizeof(double) * 2 * (size_t)N1 * B))) return rc;
+  double* phi = (double*)net->phi.p;
+  msg::unet::k_out_to_phi<<<(unsigned)std::min(4096, (B * N1 + 255) / 256), 256, 0, st>>>(
+      net->out, 1.0 / (double)(net->n[1] - 1), N1, B, phi);
+  NCK(cudaGetLastError());
+  ++net->ctx->stats.kernel_launches;
+  *phi_out = phi;
+  return MSGPU_OK;
+}
+
+// He-normal initialisation (deterministic for a seed), biases zero, the head scaled by 0.1.
+void net_init_host(const msgpu_net* net, unsigned long long seed, std::vector<float>& th) {
+  th.assign(net->nparams, 0.f);
+  unsigned long long s = seed * 0x9E3779B97F4A7C15ull + 1;
+  auto next = [&]() {   // splitmix64
+    unsigned long long z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  };
+  auto unif = [&]() { return ((next() >> 11) + 0.5) * (1.0 / 9007199254740992.0); };
+  for (int i = 0; i < kNetLayers; ++i) {
+    const NetLayer& l = net->L[i];
+    const double sd = std::sqrt(2.0 / (9.0 * l.cin)) * (i == HEAD ? 0.1 : 1.0);
+    const size_t nw = (size_t)l.cout * 9 * l.cin;
+    for (size_t k = 0; k < nw; ++k) {   // Box-Muller
+      const double u1 = unif(), u2 = unif();
+      th[l.w_off + k] = (float)(sd * std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2));
+    }
+  }
+}
+
+int net_set_params_dev(msgpu_net* net, const float* host) {
+  NCK(cudaMemcpy(net->theta, host, sizeof(float) * net->nparams, cudaMemcpyHostToDevice));
+  NCK(cudaMemset(net->m, 0, sizeof(float) * net->nparams));
+  NCK(cudaMemset(net->v, 0, sizeof(float) * net->nparams));
+  net->step = 0;
+  int rc;
+  if ((rc = net_pack(net, net->ctx->stream))) return rc;
+  NCK(cudaStreamSynchronize(net->ctx->stream));
+  return MSGPU_OK;
+}
+
+// The network's start displacement for F templates from their prepared
+// pyramids (reference row 0, templates rows 1..F): F x 2 x N doubles at the
+// network's output level, in the net's phi buffer.
+int warm_start_phi(msgpu_net* net, const double* pyr, const std::vector<size_t>& poff, size_t pstride, int F,
+                   cudaStream_t st, double** phi) {
+  const int l0 = net->level;
+  return net_predict(net, pyr + poff[l0], 0, pyr + pstride + poff[l0], pstride, F, st, phi);
+}
+
+// msgpu_register_batch_warm_device; warm_used (host, nullable).
+template <typename Real>
+int warm_batch(msgpu_context* ctx, const msgpu_params& p, msgpu_net* net, const double* d_ref, const double* d_tmpl,
+               int F, const double* d_plain_e, double rel_tol, double* d_phis, double* d_e_out, int* d_s_out,
+               int* warm_used, cudaStream_t st) {
+  const int ws = net->level - 1;
+  msgpu_params pw = p;
+  pw.start_level = ws;
+  const int nlev = p.stop_level - p.start_level + 1, nw = p.stop_level - ws + 1;
+  const size_t NM = lvl_N(p.precision_level), Nin = lvl_N(p.input_level);
+  int rc;
+  if ((rc = ensure(ctx, ctx->io[5], sizeof(double) * F + sizeof(int) * (size_t)F * nw + 64))) return rc;
+  double* e = (double*)ctx->io[5].p;
+  int* s = (int*)(e + F);
+  BatchIO io{d_ref, d_tmpl, nullptr, d_phis, e, s};
+  BatchOpts opt;
+  opt.warm = net;
+  if ((rc = run_batch<Real>(ctx, pw, F, io, st, opt))) return rc;
+  if (d_e_out) CK(cudaMemcpyAsync(d_e_out, e, sizeof(double) * F, cudaMemcpyDeviceToDevice, st));
+  if (d_s_out) {
+    CK(cudaMemsetAsync(d_s_out, 0, sizeof(int) * (size_t)F * nlev, st));
+    CK(cudaMemcpy2DAsync(d_s_out + (ws - p.start_level), sizeof(int) * nlev, s, sizeof(int) * nw, sizeof(int) * nw, F,
+                         cudaMemcpyDeviceToDevice, st));
+  }
+  std::vector<int> used(F, 1);
+  if (d_plain_e) {
+    // the plain method's energies judge the warm start: worse by more than
+    // rel_tol -> the frame is registered again from the plain start
+    std::vector<double> he(F), hp(F);
+    CK(cudaMemcpyAsync(he.data(), e, sizeof(double) * F, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hp.data(), d_plain_e, sizeof(double) * F, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::vector<int> bad;
+    for (int f = 0; f < F; ++f)
+      if (!(he[f] <= hp[f] + rel_tol * std::fabs(hp[f]))) {
+        bad.push_back(f);
+        used[f] = 0;
+      }
+    const int G = (int)bad.size();
+    if (G) {
+      const size_t need = sizeof(double) * ((size_t)G * (Nin + 2 * NM) + G) + sizeof(int) * (size_t)G * nlev + 64;
+      if ((rc = ensure(ctx, net->gather, need))) return rc;
+      double* tm = (double*)net->gather.p;
+      double* ph = tm + (size_t)G * Nin;
+      double* e2 = ph + 2 * NM * G;
+      int* s2 = (int*)(e2 + G);
+      for (int g = 0; g < G; ++g)
+        CK(cudaMemcpyAsync(tm + g * Nin, d_tmpl + (size_t)bad[g] * Nin, sizeof(double) * Nin,
+                           cudaMemcpyDeviceToDevice, st));
+      BatchIO io2{d_ref, tm, nullptr, ph, e2, s2};
+      if ((rc = run_batch<Real>(ctx, p, G, io2, st))) return rc;
+      for (int g = 0; g < G; ++g) {
+        const int f = bad[g];
+        CK(cudaMemcpyAsync(d_phis + 2 * NM * f, ph + 2 * NM * g, sizeof(double) * 2 * NM, cudaMemcpyDeviceToDevice,
+                           st));
+        if (d_e_out) CK(cudaMemcpyAsync(d_e_out + f, e2 + g, sizeof(double), cudaMemcpyDeviceToDevice, st));
+        if (d_s_out)
+          CK(cudaMemcpyAsync(d_s_out + (size_t)f * nlev, s2 + (size_t)g * nlev, sizeof(int) * nlev,
+                             cudaMemcpyDeviceToDevice, st));
+      }
+    }
+  }
+  if (warm_used) std::copy(used.begin(), used.end(), warm_used);
+  return MSGPU_OK;
+}
+
+int check_warm(msgpu_context* ctx, const msgpu_params* p, msgpu_net* net) {
+  int rc;
+  if ((rc = check_params(ctx, p))) return rc;
+  if (!net || net->ctx != ctx) return fail(ctx, MSGPU_ERR_INVALID_ARG, "the network belongs to another context");
+  const int ws = net->level - 1;
+  if (net->level > p->input_level || ws < p->start_level || ws > p->stop_level)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG,
+                "network input level %d: needs inputLevel >= %d and startLevel <= %d <= stopLevel", net->level,
+                net->level, ws);
+  return MSGPU_OK;
+}
+}  // namespace
+
+extern "C" {
+
+long long msgpu_net_num_params(void) { return (long long)net_param_count(); }
+
+int msgpu_net_create(msgpu_context* ctx, int input_level, unsigned long long seed, msgpu_net** out) {
+  if (!ctx || !out) return MSGPU_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (input_level < 4 || input_level > 11)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "network input level %d: 4..11 (three stride-2 levels below it)",
+                input_level);
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  msgpu_net* net = new msgpu_net();
+  net->ctx = ctx;
+  net->level = input_level;
+  for (int g = 0; g < 4; ++g) net->n[g] = (1 << (input_level - g)) + 1;
+  size_t off = 0, pk = 0;
+  for (int i = 0; i < kNetLayers; ++i) {
+    NetLayer& l = net->L[i];
+    l.cin = kNetSpec[i][0]; l.cout = kNetSpec[i][1]; l.stride = kNetSpec[i][2]; l.relu = kNetSpec[i][3];
+    l.cin_pad = pad16(l.cin); l.cout_pad = pad16(l.cout);
+    l.w_off = off; off += (size_t)l.cout * 9 * l.cin;
+    l.b_off = off; off += l.cout;
+    l.wf_off = pk; l.wt_off = pk; pk += align_up((size_t)l.cout_pad * 9 * l.cin_pad, 64);
+  }
+  net->nparams = off;
+  net->npacked = pk;
+  cudaError_t e = cudaMalloc(&net->theta, sizeof(float) * 4 * off);
+  if (e == cudaSuccess) e = cudaMalloc(&net->wf, sizeof(bf16) * 2 * pk);
+  if (e != cudaSuccess) {
+    cudaFree(net->theta);
+    delete net;
+    return fail(ctx, MSGPU_ERR_CUDA, "network allocation failed: %s", cudaGetErrorString(e));
+  }
+  net->grad = net->theta + off; net->m = net->grad + off; net->v = net->m + off;
+  net->wt = net->wf + pk;
+  std::vector<float> th;
+  net_init_host(net, seed, th);
+  if ((rc = net_set_params_dev(net, th.data()))) {
+    cudaFree(net->theta); cudaFree(net->wf);
+    delete net;
+    return rc;
+  }
+  *out = net;
+  return MSGPU_OK;
+}
+
+int msgpu_net_destroy(msgpu_net* net) {
+  if (!net) return MSGPU_OK;
+  cudaSetDevice(net->ctx->device);
+  cudaFree(net->theta);
+  cudaFree(net->wf);
+  for (msgpu_context::Buf* b : {&net->act, &net->part, &net->small, &net->phi, &net->gather})
+    if (b->p) cudaFree(b->p);
+  delete net;
+  return MSGPU_OK;
+}
+
+int msgpu_net_input_level(const msgpu_net* net) { return net ? net->level : -1; }
+
+int msgpu_net_get_params(msgpu_net* net, float* out) {
+  if (!net || !out) return MSGPU_ERR_INVALID_ARG;
+  int rc;
+  if ((rc = bind_device(net->ctx))) return rc;
+  NCK(cudaStreamSynchronize(net->ctx->stream));
+  NCK(cudaMemcpy(out, net->theta, sizeof(float) * net->nparams, cudaMemcpyDeviceToHost));
+  return MSGPU_OK;
+}
+
+int msgpu_net_set_params(msgpu_net* net, const float* in) {
+  if (!net || !in) return MSGPU_ERR_INVALID_ARG;
+  int rc;
+  if ((rc = bind_device(net->ctx))) return rc;
+  return net_set_params_dev(net, in);
+}
+
+int msgpu_net_save(msgpu_net* net, const char* path) {
+  if (!net || !path) return MSGPU_ERR_INVALID_ARG;
+  std::vector<float> th(net->nparams);
+  int rc;
+  if ((rc = msgpu_net_get_params(net, th.data()))) return rc;
+  FILE* f = fopen(path, "wb");
+  if (!f) return fail(net->ctx, MSGPU_ERR_INVALID_ARG, "Could not open %s for writing", path);
+  const char magic[8] = {'M', 'S', 'G', 'P', 'U', 'N', 'E', 'T'};
+  const int hdr[2] = {1, (int)net->nparams};
+  bool ok = fwrite(magic, 1, 8, f) == 8 && fwrite(hdr, sizeof(int), 2, f) == 2 &&
+            fwrite(th.data(), sizeof(float), th.size(), f) == th.size();
+  ok = (fclose(f) == 0) && ok;
+  return ok ? MSGPU_OK : fail(net->ctx, MSGPU_ERR_INVALID_ARG, "writing %s failed", path);
+}
+
+int msgpu_net_load(msgpu_net* net, const char* path) {
+  if (!net || !path) return MSGPU_ERR_INVALID_ARG;
+  FILE* f = fopen(path, "rb");
+  if (!f) return fail(net->ctx, MSGPU_ERR_INVALID_ARG, "Could not open %s", path);
+  char magic[8];
+  int hdr[2] = {0, 0};
+  std::vector<float> th(net->nparams);
+  const bool ok = fread(magic, 1, 8, f) == 8 && !memcmp(magic, "MSGPUNET", 8) && fread(hdr, sizeof(int), 2, f) == 2 &&
+                  hdr[0] == 1 && hdr[1] == (int)net->nparams &&
+                  fread(th.data(), sizeof(float), th.size(), f) == th.size();
+  fclose(f);
+  if (!ok) return fail(net->ctx, MSGPU_ERR_SIZE, "%s is not a network file of %zu parameters", path, net->nparams);
+  return msgpu_net_set_params(net, th.data());
+}
+
+int msgpu_net_predict_device(msgpu_net* net, const double* d_R, long long r_stride, const double* d_T, int batch,
+                             double* d_phi_out, void* stream) {
+  if (!net || !d_R || !d_T || !d_phi_out || batch < 1 || r_stride < 0) return MSGPU_ERR_INVALID_ARG;
+  int rc;
+  if ((rc = bind_device(net->ctx))) return rc;
+  net->ctx->stats.kernel_launches = 0;
+  const cudaStream_t st = (cudaStream_t)stream;
+  const size_t N0 = (size_t)net->n[0] * net->n[0], N1 = (size_t)net->n[1] * net->n[1];
+  double* phi;
+  if ((rc = net_predict(net, d_R, (size_t)r_stride, d_T, N0, batch, st, &phi))) return rc;
+  NCK(cudaMemcpyAsync(d_phi_out, phi, sizeof(double) * 2 * N1 * batch, cudaMemcpyDeviceToDevice, st));
+  return MSGPU_OK;
+}
+
+int msgpu_net_train_step_device(msgpu_net* net, const double* d_R, long long r_stride, const double* d_T,
+                                const double* d_phi_target, int batch, float lr, float* loss_out, void* stream) {
+  if (!net || !d_R || !d_T || !d_phi_target || batch < 1 || r_stride < 0 || !(lr >= 0))
+    return MSGPU_ERR_INVALID_ARG;
+  int rc;
+  if ((rc = bind_device(net->ctx))) return rc;
+  net->ctx->stats.kernel_launches = 0;
+  const cudaStream_t st = (cudaStream_t)stream;
+  const size_t N0 = (size_t)net->n[0] * net->n[0];
+  if ((rc = net_input(net, d_R, (size_t)r_stride, d_T, N0, batch, st)) || (rc = net_forward(net, batch, st)) ||
+      (rc = net_loss(net, d_phi_target, batch, st)) || (rc = net_backward(net, batch, st)) ||
+      (rc = net_adam(net, lr, st)))
+    return rc;
+  if (loss_out) {
+    NCK(cudaMemcpyAsync(loss_out, net->small.p, sizeof(float), cudaMemcpyDeviceToHost, st));
+    NCK(cudaStreamSynchronize(st));
+  }
+  return MSGPU_OK;
+}
+
+int msgpu_net_loss_grad(msgpu_net* net, const double* R, const double* T, const double* phi_target, int batch,
+                        float* loss_out, double* phi_out, float* grad_out) {
+  if (!net || !R || !T || !phi_target || batch < 1) return MSGPU_ERR_INVALID_ARG;
+  int rc;
+  if ((rc = bind_device(net->ctx))) return rc;
+  msgpu_context* ctx = net->ctx;
+  const cudaStream_t st = ctx->stream;
+  const size_t N0 = (size_t)net->n[0] * net->n[0], N1 = (size_t)net->n[1] * net->n[1];
+  if ((rc = ensure(ctx, ctx->io[0], sizeof(double) * (2 * N0 + 2 * N1) * batch))) return rc;
+  double* d = (double*)ctx->io[0].p;
+  CK(cudaMemcpyAsync(d, R, sizeof(double) * N0 * batch, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d + N0 * batch, T, sizeof(double) * N0 * batch, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d + 2 * N0 * batch, phi_target, sizeof(double) * 2 * N1 * batch, cudaMemcpyHostToDevice, st));
+  double* phi;
+  if ((rc = net_predict(net, d, N0, d + N0 * batch, N0, batch, st, &phi)) ||
+      (rc = net_loss(net, d + 2 * N0 * batch, batch, st)) || (rc = net_backward(net, batch, st)))
+    return rc;
+  if (loss_out) CK(cudaMemcpyAsync(loss_out, net->small.p, sizeof(float), cudaMemcpyDeviceToHost, st));
+  if (phi_out) CK(cudaMemcpyAsync(phi_out, phi, sizeof(double) * 2 * N1 * batch, cudaMemcpyDeviceToHost, st));
+  if (grad_out) CK(cudaMemcpyAsync(grad_out, net->grad, sizeof(float) * net->nparams, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return MSGPU_OK;
+}
+
+int msgpu_prepare_images_device(msgpu_context* ctx, const msgpu_params* p, const double* d_images, int count,
+                                int level, double* d_out, void* stream) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (!p || !d_images || !d_out || count < 1) return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid prepare arguments");
+  if (p->input_level < 1 || p->input_level > 12 || level < 0 || level > p->input_level)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "level %d outside 0..input_level %d", level, p->input_level);
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  ctx->stats.kernel_launches = 0;
+  const cudaStream_t st = (cudaStream_t)stream;
+  std::vector<size_t> poff;
+  const size_t pstride = pyramid_layout(p->input_level, poff);
+  const size_t Nin = lvl_N(p->input_level), Nl = lvl_N(level);
+  if ((rc = ensure(ctx, ctx->dscratch, sizeof(double) * pstride * count)) ||
+      (rc = ensure(ctx, ctx->small, sizeof(double) * (2 * (size_t)count + 64))))
+    return rc;
+  double* pyr = (double*)ctx->dscratch.p;
+  CK(cudaMemcpy2DAsync(pyr + poff[p->input_level], pstride * sizeof(double), d_images, Nin * sizeof(double),
+                       Nin * sizeof(double), count, cudaMemcpyDeviceToDevice, st));
+  if ((rc = prepare_pyramid(ctx, *p, pyr, poff, pstride, count, (double*)ctx->small.p, st))) return rc;
+  CK(cudaMemcpy2DAsync(d_out, Nl * sizeof(double), pyr + poff[level], pstride * sizeof(double), Nl * sizeof(double),
+                       count, cudaMemcpyDeviceToDevice, st));
+  return MSGPU_OK;
+}
+
+int msgpu_register_batch_warm_device(msgpu_context* ctx, const msgpu_params* p, msgpu_net* net,
+                                     const double* d_reference, const double* d_templates, int num_templates,
+                                     const double* d_plain_energies, double rel_tol, double* d_phis_out,
+                                     double* d_energies_out, int* d_steps_out, int* warm_used_out, void* stream) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  int rc;
+  if ((rc = check_warm(ctx, p, net))) return rc;
+  if (num_templates < 1) return fail(ctx, MSGPU_ERR_INVALID_ARG, "num_templates must be >= 1");
+  if (!d_reference || !d_templates || !d_phis_out) return fail(ctx, MSGPU_ERR_INVALID_ARG, "null buffer");
+  if ((rc = bind_device(ctx))) return rc;
+  const cudaStream_t st = (cudaStream_t)stream;
+  return p->use_fp64 ? warm_batch<double>(ctx, *p, net, d_reference, d_templates, num_templates, d_plain_energies,
+                                          rel_tol, d_phis_out, d_energies_out, d_steps_out, warm_used_out, st)
+                     : warm_batch<float>(ctx, *p, net, d_reference, d_templates, num_templates, d_plain_energies,
+                                         rel_tol, d_phis_out, d_energies_out, d_steps_out, warm_used_out, st);
+}
+
+int msgpu_register_batch_warm(msgpu_context* ctx, const msgpu_params* p, msgpu_net* net, const double* reference,
+                              const double* templates, int num_templates, const double* plain_energies,
+                              double rel_tol, double* phis_out, double* energies_out, int* steps_out,
+                              int* warm_used_out) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  int rc;
+  if ((rc = check_warm(ctx, p, net))) return rc;
+  if (num_templates < 1) return fail(ctx, MSGPU_ERR_INVALID_ARG, "num_templates must be >= 1");
+  if (!reference || !templates || !phis_out) return fail(ctx, MSGPU_ERR_INVALID_ARG, "null buffer");
+  if ((rc = bind_device(ctx))) return rc;
+  const size_t Nin = lvl_N(p->input_level), NM = lvl_N(p->precision_level);
+  const int F = num_templates;
+  const int nlev = p->stop_level - p->start_level + 1;
+  if ((rc = ensure(ctx, ctx->io[0], sizeof(double) * Nin)) || (rc = ensure(ctx, ctx->io[1], sizeof(double) * Nin * F)) ||
+      (rc = ensure(ctx, ctx->io[3], sizeof(double) * 2 * NM * F)) ||
+      (rc = ensure(ctx, ctx->io[4], sizeof(double) * 2 * F + sizeof(int) * F * nlev + 64)))
+    return rc;
+  const cudaStream_t st = ctx->stream;
+  double* d_e = (double*)ctx->io[4].p;
+  double* d_pe = d_e + F;
+  int* d_s = (int*)(d_pe + F);
+  CK(cudaMemcpyAsync(ctx->io[0].p, reference, sizeof(double) * Nin, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctx->io[1].p, templates, sizeof(double) * Nin * F, cudaMemcpyHostToDevice, st));
+  if (plain_energies) CK(cudaMemcpyAsync(d_pe, plain_energies, sizeof(double) * F, cudaMemcpyHostToDevice, st));
+  rc = p->use_fp64 ? warm_batch<double>(ctx, *p, net, (const double*)ctx->io[0].p, (const double*)ctx->io[1].p, F,
+                                        plain_energies ? d_pe : nullptr, rel_tol, (double*)ctx->io[3].p, d_e, d_s,
+                                        warm_used_out, st)
+                   : warm_batch<float>(ctx, *p, net, (const double*)ctx->io[0].p, (const double*)ctx->io[1].p, F,
+                                       plain_energies ? d_pe : nullptr, rel_tol, (double*)ctx->io[3].p, d_e, d_s,
+                                       warm_used_out, st);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(phis_out, ctx->io[3].p, sizeof(double) * 2 * NM * F, cudaMemcpyDeviceToHost, st));
+  if (energies_out) CK(cudaMemcpyAsync(energies_out, d_e, sizeof(double) * F, cudaMemcpyDeviceToHost, st));
+  if (steps_out) CK(cudaMemcpyAsync(steps_out, d_s, sizeof(int) * F * nlev, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return sched_error_check(ctx);
+}
+
+}  // extern "C"

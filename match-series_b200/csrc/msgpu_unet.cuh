@@ -1,0 +1,500 @@
+// msgpu_unet.cuh -- kernels of the learned warm start: a U-Net on 2^l+1
+// node grids that maps the normalised reference/template pair of a frame to
+// a coarse displacement, trained and run on the GPU.
+//
+// Tensors are NHWC bf16 "views": image stride, nodes per side, elements per
+// node (channel stride) and a channel offset in the base pointer, so the
+// decoder's concatenations [skip | upsampled] are channel slices of one
+// buffer and no copy is made.  Channel counts are padded to multiples of 16.
+//
+// k_conv: one 3x3 convolution as an implicit GEMM on the tensor pipe
+// (mma.sync m16n8k16, bf16 operands, fp32 accumulation).  A block computes
+// 64 output nodes x BN output channels; the reduction runs over
+// (tap, input channel) in stages of 32, staged in shared memory by
+// cp.async with zero fill for taps outside the grid.  mode 0 reads input
+// node stride*q + d (forward), mode 1 reads (q - d)/stride when that is a
+// node (the data gradient of a forward convolution, with the weights
+// transposed).  The epilogue adds the bias, accumulates into the output,
+// applies ReLU and a ReLU mask as asked.
+//
+// k_wgrad: weight gradient dW[co][(tap, ci)] = sum over nodes of
+// dY[node][co] * X[src(node, tap)][ci], the node sum split into chunks; each
+// block writes its chunk's partial, k_wgrad_reduce adds the partials in
+// chunk order (deterministic training).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+namespace msg {
+namespace unet {
+
+typedef __nv_bfloat16 bf16;
+
+constexpr int kThreads = 128;
+constexpr int kBM = 64;        // output nodes per conv block
+constexpr int kBK = 32;        // reduction elements per stage
+constexpr int kSA = kBK + 8;   // shared-memory row stride (bf16): conflict-free fragment loads
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void mma_bf16(float* c, const uint32_t* a, uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// source node of output node (qy, qx) under tap (dy, dx); false when there is none
+__device__ __forceinline__ bool conv_src(int mode, int stride, int n_in, int qy, int qx, int dy, int dx, int& sy,
+                                         int& sx) {
+  if (mode == 0) {
+    sy = stride * qy + dy;
+    sx = stride * qx + dx;
+  } else {
+    const int ty = qy - dy, tx = qx - dx;
+    if (stride == 2) {
+      if ((ty | tx) & 1) return false;
+      sy = ty >> 1;
+      sx = tx >> 1;
+    } else {
+      sy = ty;
+      sx = tx;
+    }
+  }
+  return sy >= 0 && sy < n_in && sx >= 0 && sx < n_in;
+}
+
+struct ConvArgs {
+  const bf16* in;        // input view: image 0, first channel read
+  size_t in_img;         // elements between images
+  int in_n, in_cs, cin;  // nodes per side, elements per node, channels read (multiple of 16)
+  const bf16* w;         // [rows][9 * cin], (tap, channel) contiguous
+  const float* bias;     // nullable, [cout]
+  void* out;             // output view (bf16, or float with out_f32)
+  size_t out_img;
+  int out_n, out_cs, cout;   // channels stored
+  int out_f32;
+  int mode, stride, relu, accumulate;
+  const bf16* mask;      // nullable: output zeroed where mask <= 0
+  size_t mask_img;
+  int mask_cs;
+  int total;             // images * out_n^2
+};
+
+template <int BN>
+__global__ void __launch_bounds__(kThreads) k_conv(ConvArgs a) {
+  __shared__ __align__(16) bf16 As[2][kBM][kSA];
+  __shared__ __align__(16) bf16 Bs[2][BN][kSA];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int p0 = blockIdx.x * kBM;
+  const int n0 = blockIdx.y * BN;
+  const int K = 9 * a.cin;
+  const int nk = (K + kBK - 1) / kBK;
+  const int outN2 = a.out_n * a.out_n;
+  int r_img[2], r_qy[2], r_qx[2];
+  bool r_ok[2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const int row = (tid + i * kThreads) >> 2;
+    const int p = p0 + row;
+    r_ok[i] = p < a.total;
+    const int img = r_ok[i] ? p / outN2 : 0;
+    const int q = r_ok[i] ? p - img * outN2 : 0;
+    r_img[i] = img;
+    r_qy[i] = q / a.out_n;
+    r_qx[i] = q - r_qy[i] * a.out_n;
+  }
+  auto load_stage = [&](int s, int kt) {
+    const int k0 = kt * kBK;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int idx = tid + i * kThreads;
+      const int row = idx >> 2, g = idx & 3;
+      const int k = k0 + g * 8;
+      const bf16* src = a.in;
+      bool ok = r_ok[i] && k < K;
+      if (ok) {
+        const int tap = k / a.cin, ci = k - tap * a.cin;
+        int sy, sx;
+        ok = conv_src(a.mode, a.stride, a.in_n, r_qy[i], r_qx[i], tap / 3 - 1, tap % 3 - 1, sy, sx);
+        if (ok) src = a.in + (size_t)r_img[i] * a.in_img + ((size_t)sy * a.in_n + sx) * a.in_cs + ci;
+      }
+      cp_async16(&As[s][row][g * 8], src, ok ? 16 : 0);
+    }
+    for (int idx = tid; idx < BN * 4; idx += kThreads) {
+      const int row = idx >> 2, g = idx & 3;
+      const int k = k0 + g * 8;
+      const bool ok = k < K;
+      cp_async16(&Bs[s][row][g * 8], ok ? a.w + (size_t)(n0 + row) * K + k : a.w, ok ? 16 : 0);
+    }
+    cp_async_commit();
+  };
+  float acc[BN / 8][4];
+#pragma unroll
+  for (int j = 0; j < BN / 8; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) acc[j][e] = 0.f;
+  load_stage(0, 0);
+  for (int kt = 0; kt < nk; ++kt) {
+    if (kt + 1 < nk) {
+      load_stage((kt + 1) & 1, kt + 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const int s = kt & 1;
+#pragma unroll
+    for (int kk = 0; kk < kBK; kk += 16) {
+      const int r = warp * 16 + (lane >> 2), c = kk + 2 * (lane & 3);
+      uint32_t af[4];
+      af[0] = *reinterpret_cast<const uint32_t*>(&As[s][r][c]);
+      af[1] = *reinterpret_cast<const uint32_t*>(&As[s][r + 8][c]);
+      af[2] = *reinterpret_cast<const uint32_t*>(&As[s][r][c + 8]);
+      af[3] = *reinterpret_cast<const uint32_t*>(&As[s][r + 8][c + 8]);
+#pragma unroll
+      for (int j = 0; j < BN / 8; ++j) {
+        const int nr = j * 8 + (lane >> 2);
+        mma_bf16(acc[j], af, *reinterpret_cast<const uint32_t*>(&Bs[s][nr][c]),
+                 *reinterpret_cast<const uint32_t*>(&Bs[s][nr][c + 8]));
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int p = p0 + warp * 16 + (lane >> 2) + 8 * h;
+    if (p >= a.total) continue;
+    const int img = p / outN2, q = p - img * outN2;
+#pragma unroll
+    for (int j = 0; j < BN / 8; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int co = n0 + j * 8 + 2 * (lane & 3) + e;
+        if (co >= a.cout) continue;
+        float v = acc[j][2 * h + e];
+        if (a.bias) v += a.bias[co];
+        const size_t o = (size_t)img * a.out_img + (size_t)q * a.out_cs + co;
+        if (a.accumulate) v += __bfloat162float(static_cast<const bf16*>(a.out)[o]);
+        if (a.relu) v = fmaxf(v, 0.f);
+        if (a.mask && !(__bfloat162float(a.mask[(size_t)img * a.mask_img + (size_t)q * a.mask_cs + co]) > 0.f))
+          v = 0.f;
+        if (a.out_f32)
+          static_cast<float*>(a.out)[o] = v;
+        else
+          static_cast<bf16*>(a.out)[o] = __float2bfloat16(v);
+      }
+  }
+}
+
+struct WgradArgs {
+  const bf16* in;        // forward input view
+  size_t in_img;
+  int in_n, in_cs, cin;  // channels read (multiple of 16)
+  const bf16* dy;        // gradient at the forward output (pre-activation)
+  size_t dy_img;
+  int dy_n, dy_cs, cout_pad;
+  int stride;
+  float* part;           // [chunks][cout_pad][9 * cin]
+  int total;             // images * dy_n^2
+  int chunk;             // nodes per block (multiple of kBK)
+};
+
+// GEMM dW^T[co][k] over node chunks: rows = output channels (BM per block),
+// columns = 64 reduction indices (tap, ci), inner dimension = nodes.
+template <int BM>
+__global__ void __launch_bounds__(kThreads) k_wgrad(WgradArgs a) {
+  constexpr int WM = BM / 16, WN = 4 / WM, NT = 64 / WN / 8;
+  constexpr int NA = BM * kBK / 8;   // dY vectors per stage
+  constexpr int RA = (NA + kThreads - 1) / kThreads;
+  __shared__ __align__(16) bf16 As[BM][kSA];   // [co][node]
+  __shared__ __align__(16) bf16 Bs[64][kSA];   // [k][node]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp % WM, wn = warp / WM;
+  const int K = 9 * a.cin;
+  const int kb = blockIdx.x * 64, cb = blockIdx.y * BM;
+  const int pbeg = blockIdx.z * a.chunk;
+  const int pend = min(a.total, pbeg + a.chunk);
+  const int dyN2 = a.dy_n * a.dy_n;
+  float acc[NT][4];
+#pragma unroll
+  for (int j = 0; j < NT; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) acc[j][e] = 0.f;
+  uint4 ra[RA], rb[2];
+  auto gload = [&](int pb) {
+#pragma unroll
+    for (int i = 0; i < RA; ++i) {
+      const int idx = tid + i * kThreads;
+      ra[i] = make_uint4(0, 0, 0, 0);
+      if (idx < NA) {
+        const int pi = idx / (BM / 8), v = idx - pi * (BM / 8);
+        const int p = pb + pi;
+        if (p < pend) {
+          const int img = p / dyN2, q = p - img * dyN2;
+          ra[i] = *reinterpret_cast<const uint4*>(a.dy + (size_t)img * a.dy_img + (size_t)q * a.dy_cs + cb + 8 * v);
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int idx = tid + i * kThreads;   // 32 nodes x 8 groups
+      const int pi = idx >> 3, g = idx & 7;
+      const int p = pb + pi, k = kb + 8 * g;
+      rb[i] = make_uint4(0, 0, 0, 0);
+      if (p < pend && k < K) {
+        const int img = p / dyN2, q = p - img * dyN2;
+        const int qy = q / a.dy_n, qx = q - qy * a.dy_n;
+        const int tap = k / a.cin, ci = k - tap * a.cin;
+        int sy, sx;
+        if (conv_src(0, a.stride, a.in_n, qy, qx, tap / 3 - 1, tap % 3 - 1, sy, sx))
+          rb[i] = *reinterpret_cast<const uint4*>(a.in + (size_t)img * a.in_img +
+                                                  ((size_t)sy * a.in_n + sx) * a.in_cs + ci);
+      }
+    }
+  };
+  auto sstore = [&]() {
+#pragma unroll
+    for (int i = 0; i < RA; ++i) {
+      const int idx = tid + i * kThreads;
+      if (idx < NA) {
+        const int pi = idx / (BM / 8), v = idx - pi * (BM / 8);
+        const bf16* e = reinterpret_cast<const bf16*>(&ra[i]);
+#pragma unroll
+        for (int t = 0; t < 8; ++t) As[8 * v + t][pi] = e[t];
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int idx = tid + i * kThreads;
+      const int pi = idx >> 3, g = idx & 7;
+      const bf16* e = reinterpret_cast<const bf16*>(&rb[i]);
+#pragma unroll
+      for (int t = 0; t < 8; ++t) Bs[8 * g + t][pi] = e[t];
+    }
+  };
+  if (pbeg < pend) gload(pbeg);
+  for (int pb = pbeg; pb < pend; pb += kBK) {
+    sstore();
+    __syncthreads();
+    if (pb + kBK < pend) gload(pb + kBK);
+#pragma unroll
+    for (int kk = 0; kk < kBK; kk += 16) {
+      const int r = wm * 16 + (lane >> 2), c = kk + 2 * (lane & 3);
+      uint32_t af[4];
+      af[0] = *reinterpret_cast<const uint32_t*>(&As[r][c]);
+      af[1] = *reinterpret_cast<const uint32_t*>(&As[r + 8][c]);
+      af[2] = *reinterpret_cast<const uint32_t*>(&As[r][c + 8]);
+      af[3] = *reinterpret_cast<const uint32_t*>(&As[r + 8][c + 8]);
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        const int nr = wn * (64 / WN) + j * 8 + (lane >> 2);
+        mma_bf16(acc[j], af, *reinterpret_cast<const uint32_t*>(&Bs[nr][c]),
+                 *reinterpret_cast<const uint32_t*>(&Bs[nr][c + 8]));
+      }
+    }
+    __syncthreads();
+  }
+  float* part = a.part + (size_t)blockIdx.z * a.cout_pad * K;
+#pragma unroll
+  for (int j = 0; j < NT; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int co = cb + wm * 16 + (lane >> 2) + 8 * (e >> 1);
+      const int k = kb + wn * (64 / WN) + j * 8 + 2 * (lane & 3) + (e & 1);
+      if (k < K) part[(size_t)co * K + k] = acc[j][e];
+    }
+}
+
+// dW of one layer from the chunk partials, added in chunk order, into the
+// flat gradient (W[cout][3][3][cin_real]); padding channels are dropped.
+__global__ void k_wgrad_reduce(const float* part, int chunks, int cout, int cout_pad, int cin_real, int cin_pad,
+                               float* grad) {
+  const int n = cout * 9 * cin_real;
+  const int K = 9 * cin_pad;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int co = i / (9 * cin_real), r = i - co * 9 * cin_real;
+    const int tap = r / cin_real, ci = r - tap * cin_real;
+    const size_t o = (size_t)co * K + tap * cin_pad + ci;
+    float s = 0.f;
+    for (int c = 0; c < chunks; ++c) s += part[(size_t)c * cout_pad * K + o];
+    grad[i] = s;
+  }
+}
+
+// bias gradient: per chunk (block) and channel (thread) the node sum, then in chunk order
+__global__ void k_bgrad_part(const bf16* dy, size_t dy_img, int dy_n2, int dy_cs, int cout, int total, int chunk,
+                             float* part) {
+  const int co = threadIdx.x;
+  if (co >= cout) return;
+  const int pbeg = blockIdx.x * chunk, pend = min(total, pbeg + chunk);
+  float s = 0.f;
+  for (int p = pbeg; p < pend; ++p) {
+    const int img = p / dy_n2, q = p - img * dy_n2;
+    s += __bfloat162float(dy[(size_t)img * dy_img + (size_t)q * dy_cs + co]);
+  }
+  part[(size_t)blockIdx.x * cout + co] = s;
+}
+__global__ void k_bgrad_reduce(const float* part, int chunks, int cout, float* grad) {
+  const int co = blockIdx.x * blockDim.x + threadIdx.x;
+  if (co >= cout) return;
+  float s = 0.f;
+  for (int c = 0; c < chunks; ++c) s += part[(size_t)c * cout + co];
+  grad[co] = s;
+}
+
+// bilinear prolongation of node grids m -> 2m-1, C channels (one thread per node and channel)
+__global__ void k_up(const bf16* src, size_t src_img, int m, int src_cs, bf16* dst, size_t dst_img, int dst_cs,
+                     int C, int images) {
+  const int n = 2 * m - 1;
+  const size_t total = (size_t)images * n * n * C;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(i % C);
+    const size_t node = i / C;
+    const int img = (int)(node / ((size_t)n * n));
+    const int q = (int)(node - (size_t)img * n * n);
+    const int y = q / n, x = q - y * n;
+    const bf16* s = src + (size_t)img * src_img + c;
+    const int y0 = y >> 1, x0 = x >> 1, y1 = y0 + (y & 1), x1 = x0 + (x & 1);
+    float v = __bfloat162float(s[((size_t)y0 * m + x0) * src_cs]);
+    v += __bfloat162float(s[((size_t)y0 * m + x1) * src_cs]);
+    v += __bfloat162float(s[((size_t)y1 * m + x0) * src_cs]);
+    v += __bfloat162float(s[((size_t)y1 * m + x1) * src_cs]);
+    dst[(size_t)img * dst_img + (size_t)q * dst_cs + c] = __float2bfloat16(0.25f * v);
+  }
+}
+
+// adjoint of k_up, times the ReLU mask of the coarse activation
+__global__ void k_up_back(const bf16* df, size_t df_img, int n, int df_cs, bf16* dc, size_t dc_img, int dc_cs,
+                          const bf16* mask, size_t mask_img, int mask_cs, int C, int images) {
+  const int m = (n + 1) / 2;
+  const size_t total = (size_t)images * m * m * C;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(i % C);
+    const size_t node = i / C;
+    const int img = (int)(node / ((size_t)m * m));
+    const int q = (int)(node - (size_t)img * m * m);
+    const int cy = q / m, cx = q - cy * m;
+    const bf16* f = df + (size_t)img * df_img + c;
+    float v = 0.f;
+#pragma unroll
+    for (int a = -1; a <= 1; ++a)
+#pragma unroll
+      for (int b = -1; b <= 1; ++b) {
+        const int y = 2 * cy + a, x = 2 * cx + b;
+        if (y < 0 || y >= n || x < 0 || x >= n) continue;
+        const float w = (a == 0 ? 1.f : 0.5f) * (b == 0 ? 1.f : 0.5f);
+        v += w * __bfloat162float(f[((size_t)y * n + x) * df_cs]);
+      }
+    const size_t mi = (size_t)img * mask_img + (size_t)q * mask_cs + c;
+    if (!(__bfloat162float(mask[mi]) > 0.f)) v = 0.f;
+    dc[(size_t)img * dc_img + (size_t)q * dc_cs + c] = __float2bfloat16(v);
+  }
+}
+
+// network input: channels (R, T, 0 x 14) per node; R advances by r_stride per image (0 = shared)
+__global__ void k_pack_input(const double* R, size_t r_stride, const double* T, size_t t_stride, int N, int images,
+                             bf16* x) {
+  const size_t total = (size_t)images * N;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t img = i / N, q = i - img * N;
+    __align__(16) bf16 v[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) v[c] = __float2bfloat16(0.f);
+    v[0] = __float2bfloat16((float)R[img * r_stride + q]);
+    v[1] = __float2bfloat16((float)T[img * t_stride + q]);
+    uint4* d = reinterpret_cast<uint4*>(x + i * 16);
+    d[0] = reinterpret_cast<const uint4*>(v)[0];
+    d[1] = reinterpret_cast<const uint4*>(v)[1];
+  }
+}
+
+// loss = mean (out - target * scale)^2 over images, nodes, both channels;
+// target [img][2][N] (component planes); gradient into dout (16 channels, 2 used).
+// Per-block partial sums in a fixed order; k_loss_total adds them in block order.
+__global__ void __launch_bounds__(256) k_mse(const float* out, const double* target, double scale, int N, int images,
+                                             bf16* dout, float* part) {
+  __shared__ float red[8];
+  const size_t total = (size_t)images * N;
+  const float inv = 1.f / (float)(2 * total);
+  float s = 0.f;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t img = i / N, q = i - img * N;
+    __align__(16) bf16 g[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) g[c] = __float2bfloat16(0.f);
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const float d = out[i * 2 + c] - (float)(target[(img * 2 + c) * N + q] * scale);
+      s += d * d;
+      g[c] = __float2bfloat16(2.f * d * inv);
+    }
+    uint4* dp = reinterpret_cast<uint4*>(dout + i * 16);
+    dp[0] = reinterpret_cast<const uint4*>(g)[0];
+    dp[1] = reinterpret_cast<const uint4*>(g)[1];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.f;
+    for (int w = 0; w < 8; ++w) t += red[w];
+    part[blockIdx.x] = t * inv;
+  }
+}
+__global__ void k_loss_total(const float* part, int n, float* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    float s = 0.f;
+    for (int i = 0; i < n; ++i) s += part[i];
+    *out = s;
+  }
+}
+
+// network output (pixels of its grid, node-major pairs) -> displacement planes in domain units
+__global__ void k_out_to_phi(const float* out, double scale, int N, int images, double* phi) {
+  const size_t total = (size_t)images * N;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t img = i / N, q = i - img * N;
+    phi[(img * 2) * N + q] = (double)out[i * 2] * scale;
+    phi[(img * 2 + 1) * N + q] = (double)out[i * 2 + 1] * scale;
+  }
+}
+
+// Adam (Kingma & Ba 2015) on the fp32 master parameters
+__global__ void k_adam(float* theta, const float* grad, float* m, float* v, int n, float lr, float b1, float b2,
+                       float eps, float c1, float c2) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float g = grad[i];
+    const float mi = b1 * m[i] + (1.f - b1) * g;
+    const float vi = b2 * v[i] + (1.f - b2) * g * g;
+    m[i] = mi;
+    v[i] = vi;
+    theta[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  }
+}
+
+// bf16 copies of one layer's weights: wf[cout_pad][tap][cin_pad] for the
+// forward pass, wt[cin_pad][tap][cout_pad] for the data gradient
+__global__ void k_pack_weights(const float* w, int cout, int cin, int cout_pad, int cin_pad, bf16* wf, bf16* wt) {
+  const int n = cout_pad * 9 * cin_pad;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int co = i / (9 * cin_pad), r = i - co * 9 * cin_pad;
+    const int tap = r / cin_pad, ci = r - tap * cin_pad;
+    const float v = (co < cout && ci < cin) ? w[((size_t)co * 9 + tap) * cin + ci] : 0.f;
+    const bf16 b = __float2bfloat16(v);
+    wf[i] = b;
+    wt[((size_t)ci * 9 + tap) * cout_pad + co] = b;
+  }
+}
+
+}  // namespace unet
+}  // namespace msg

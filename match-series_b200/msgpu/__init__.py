@@ -93,6 +93,10 @@ EXPORTS = [
     "msgpu_write_displacement", "msgpu_read_arrays_start", "msgpu_io_wait", "msgpu_register_ragged",
     "msgpu_register_ragged_device", "msgpu_lineshift_energy", "msgpu_lineshift_energy_device", "msgpu_xshift_reg",
     "msgpu_xshift_reg_device", "msgpu_find_xshift", "msgpu_find_xshift_device", "msgpu_find_xshift_batch",
+    "msgpu_net_num_params", "msgpu_net_create", "msgpu_net_destroy", "msgpu_net_input_level", "msgpu_net_get_params",
+    "msgpu_net_set_params", "msgpu_net_save", "msgpu_net_load", "msgpu_net_predict_device",
+    "msgpu_net_train_step_device", "msgpu_net_loss_grad", "msgpu_prepare_images_device", "msgpu_register_batch_warm",
+    "msgpu_register_batch_warm_device",
 ]
 
 
@@ -160,6 +164,25 @@ def lib():
                                               ctypes.c_int, _dp, ctypes.c_int]
         L.msgpu_read_arrays_start.restype = ctypes.c_void_p
         L.msgpu_io_wait.argtypes = [ctypes.c_void_p]
+        _fp = ctypes.POINTER(ctypes.c_float)
+        _v = ctypes.c_void_p
+        L.msgpu_net_num_params.restype = ctypes.c_longlong
+        L.msgpu_net_create.argtypes = [_v, ctypes.c_int, ctypes.c_ulonglong, ctypes.POINTER(_v)]
+        L.msgpu_net_destroy.argtypes = [_v]
+        L.msgpu_net_input_level.argtypes = [_v]
+        L.msgpu_net_get_params.argtypes = [_v, _fp]
+        L.msgpu_net_set_params.argtypes = [_v, _fp]
+        L.msgpu_net_save.argtypes = [_v, ctypes.c_char_p]
+        L.msgpu_net_load.argtypes = [_v, ctypes.c_char_p]
+        L.msgpu_net_predict_device.argtypes = [_v, _v, ctypes.c_longlong, _v, ctypes.c_int, _v, _v]
+        L.msgpu_net_train_step_device.argtypes = [_v, _v, ctypes.c_longlong, _v, _v, ctypes.c_int, ctypes.c_float,
+                                                  _fp, _v]
+        L.msgpu_net_loss_grad.argtypes = [_v, _dp, _dp, _dp, ctypes.c_int, _fp, _dp, _fp]
+        L.msgpu_prepare_images_device.argtypes = [_v, ctypes.POINTER(Params), _v, ctypes.c_int, ctypes.c_int, _v, _v]
+        L.msgpu_register_batch_warm.argtypes = [_v, ctypes.POINTER(Params), _v, _dp, _dp, ctypes.c_int, _dp,
+                                                ctypes.c_double, _dp, _dp, _ip, _ip]
+        L.msgpu_register_batch_warm_device.argtypes = [_v, ctypes.POINTER(Params), _v, _v, _v, ctypes.c_int, _v,
+                                                       ctypes.c_double, _v, _v, _v, _ip, _v]
         L.msgpu_lineshift_energy.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp, _dp]
         L.msgpu_lineshift_energy_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
@@ -320,6 +343,45 @@ class Context:
         self._check(lib().msgpu_register_batch_device(self._h, ctypes.byref(params), d_ref, d_templates,
                                                       num_templates, d_init or None, d_phis_out, d_energies or None,
                                                       d_steps or None, stream or None))
+
+    def register_batch_warm(self, params: Params, net: "Net", reference, templates, plain_energies=None,
+                            rel_tol: float = 1e-6):
+        """register_batch started from the network's prediction at its output
+        level (params.start_level stays the plain start, for the fallback);
+        returns (phis[F,2,N], energies[F], steps[F,levels], warm_used[F])."""
+        ref = _f64(reference).reshape(-1)
+        tm = _f64(templates)
+        F = tm.shape[0]
+        tm = tm.reshape(F, -1)
+        N = n_of(params.precision_level) ** 2
+        nlev = params.stop_level - params.start_level + 1
+        phis = np.zeros((F, 2, N))
+        energies = np.zeros(F)
+        steps = np.zeros((F, nlev), dtype=np.int32)
+        used = np.zeros(F, dtype=np.int32)
+        pe = None if plain_energies is None else _f64(plain_energies).reshape(F)
+        self._check(lib().msgpu_register_batch_warm(self._h, ctypes.byref(params), net._h, _p(ref), _p(tm), F,
+                                                    _p(pe) if pe is not None else None, float(rel_tol), _p(phis),
+                                                    _p(energies), steps.ctypes.data_as(_ip),
+                                                    used.ctypes.data_as(_ip)))
+        return phis, energies, steps, used
+
+    def register_batch_warm_device(self, params: Params, net: "Net", d_ref: int, d_templates: int,
+                                   num_templates: int, d_phis_out: int, d_energies: int = 0, d_steps: int = 0,
+                                   d_plain_energies: int = 0, rel_tol: float = 1e-6, stream: int = 0):
+        """Returns warm_used[F] (host)."""
+        used = np.zeros(num_templates, dtype=np.int32)
+        self._check(lib().msgpu_register_batch_warm_device(
+            self._h, ctypes.byref(params), net._h, d_ref, d_templates, num_templates, d_plain_energies or None,
+            float(rel_tol), d_phis_out, d_energies or None, d_steps or None, used.ctypes.data_as(_ip),
+            stream or None))
+        return used
+
+    def prepare_images_device(self, params: Params, d_images: int, count: int, level: int, d_out: int,
+                              stream: int = 0):
+        """The registration path's image preparation, restricted to `level`."""
+        self._check(lib().msgpu_prepare_images_device(self._h, ctypes.byref(params), d_images, count, level, d_out,
+                                                      stream or None))
 
     def warp_mean(self, level: int, frames, phis):
         fr = _f64(frames)
@@ -542,3 +604,70 @@ class Context:
                                          ctypes.byref(st), _p(tr), max_trace))
         steps = st.value
         return px, py, e.value, steps, tr[:min(steps, max_trace)]
+
+
+class Net:
+    """The learned warm start (msgpu_net): a U-Net from the prepared image
+    pair at `input_level` to the displacement at input_level - 1."""
+
+    def __init__(self, ctx: Context, input_level: int = 8, seed: int = 1):
+        self.ctx = ctx
+        self.level = int(input_level)
+        self._h = ctypes.c_void_p()
+        ctx._check(lib().msgpu_net_create(ctx._h, self.level, int(seed), ctypes.byref(self._h)))
+
+    @staticmethod
+    def num_params() -> int:
+        return int(lib().msgpu_net_num_params())
+
+    def close(self):
+        if self._h:
+            lib().msgpu_net_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get_params(self):
+        out = np.zeros(self.num_params(), dtype=np.float32)
+        self.ctx._check(lib().msgpu_net_get_params(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
+
+    def set_params(self, theta):
+        t = np.ascontiguousarray(theta, dtype=np.float32)
+        self.ctx._check(lib().msgpu_net_set_params(self._h, t.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+
+    def save(self, path: str):
+        self.ctx._check(lib().msgpu_net_save(self._h, path.encode()))
+
+    def load(self, path: str):
+        self.ctx._check(lib().msgpu_net_load(self._h, path.encode()))
+
+    def predict_device(self, d_R: int, r_stride: int, d_T: int, batch: int, d_phi_out: int, stream: int = 0):
+        self.ctx._check(lib().msgpu_net_predict_device(self._h, d_R, int(r_stride), d_T, int(batch), d_phi_out,
+                                                       stream or None))
+
+    def train_step_device(self, d_R: int, r_stride: int, d_T: int, d_target: int, batch: int, lr: float,
+                          stream: int = 0, want_loss: bool = True):
+        loss = ctypes.c_float()
+        self.ctx._check(lib().msgpu_net_train_step_device(self._h, d_R, int(r_stride), d_T, d_target, int(batch),
+                                                          float(lr), ctypes.byref(loss) if want_loss else None,
+                                                          stream or None))
+        return loss.value if want_loss else None
+
+    def loss_grad(self, R, T, target):
+        """Host arrays R, T [B, n0, n0], target [B, 2, N1] (domain units):
+        returns (loss, phi [B, 2, N1], flat gradient)."""
+        R = _f64(R)
+        B = R.shape[0]
+        n1 = (1 << (self.level - 1)) + 1
+        phi = np.zeros((B, 2, n1 * n1))
+        grad = np.zeros(self.num_params(), dtype=np.float32)
+        loss = ctypes.c_float()
+        self.ctx._check(lib().msgpu_net_loss_grad(self._h, _p(R), _p(_f64(T)), _p(_f64(target)), B,
+                                                  ctypes.byref(loss), _p(phi),
+                                                  grad.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return loss.value, phi, grad
