@@ -812,6 +812,200 @@ def main_seismic(args, world, rank, local):
     return 0
 
 
+# --- learned warm start (--warm) -------------------------------------------
+WARM_LEVEL, WARM_NET, WARM_START, WARM_FRAMES = 10, 10, 4, 50
+WARM_TRAIN_SERIES, WARM_FPS, WARM_STEPS, WARM_BATCH, WARM_LR = 64, 8, 600, 8, 2e-3
+WARM_TOL = 1e-6
+
+
+def net_forward_flops(n0: int) -> float:
+    """Algorithmic FLOPs of one network forward pass at input grid n0 (real channels)."""
+    spec = [(2, 16, 1, 0), (16, 16, 1, 0), (16, 32, 2, 1), (32, 32, 1, 1), (32, 64, 2, 2), (64, 64, 1, 2),
+            (64, 128, 2, 3), (128, 128, 1, 3), (192, 64, 1, 2), (64, 64, 1, 2), (96, 32, 1, 1), (32, 32, 1, 1),
+            (32, 2, 1, 1)]
+    grids = [n0]
+    for _ in range(3):
+        grids.append((grids[-1] + 1) // 2)
+    return sum(2.0 * 9 * ci * co * grids[g] ** 2 for ci, co, _, g in spec)
+
+
+def main_warm(args, world, rank, local):
+    """--warm: registration started from the learned network's prediction."""
+    import numpy as np
+    import torch
+    import msgpu
+    from msgpu import build as mbuild
+    from msgpu import synthetic as syn
+    from msgpu import warmstart as ws
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    mbuild.build()
+    ctx = msgpu.Context(local)
+    fp64 = not args.fp32
+    # 1. training set from the plain method, training (untimed for the metric, reported)
+    R, T, tgt, t_data = ws.training_set(ctx, level=WARM_LEVEL, net_level=WARM_NET, num_series=WARM_TRAIN_SERIES,
+                                        frames_per_series=WARM_FPS, seed=9000 + 1000 * rank, fp64=fp64)
+    Rv, Tv, tv, _ = ws.training_set(ctx, level=WARM_LEVEL, net_level=WARM_NET, num_series=2,
+                                    frames_per_series=WARM_FPS, seed=9500 + 1000 * rank, fp64=fp64)
+    net = msgpu.Net(ctx, WARM_NET, seed=1)
+    losses, t_train = ws.train(net, R, T, tgt, steps=WARM_STEPS, batch=WARM_BATCH, lr=WARM_LR, seed=rank,
+                               log_every=WARM_STEPS // 4)
+    pred_mse, zero_mse = ws.prediction_error(net, Rv, Tv, tv)
+    train_flops = 3.0 * net_forward_flops(msgpu.n_of(WARM_NET)) * WARM_BATCH * WARM_STEPS
+    del R, T, tgt, Rv, Tv, tv
+    torch.cuda.empty_cache()
+    # 2. the evaluation series (device resident)
+    n = msgpu.n_of(WARM_LEVEL)
+    N = n * n
+    F = WARM_FRAMES
+    spec = syn.random_spec(np.random.default_rng(7000 + rank))
+    frames = syn.make_series_torch(n, F + 1, spec, 7001 + 1000 * rank, dev).reshape(F + 1, N).contiguous()
+    p = msgpu.default_params(precision_level=WARM_LEVEL, input_level=WARM_LEVEL, start_level=WARM_START,
+                             stop_level=WARM_LEVEL, max_gd_iterations=MAX_ITER, use_fp64=int(fp64), lambda_=LAMBDA)
+    nlev = WARM_LEVEL - WARM_START + 1
+    st = torch.cuda.current_stream(dev)
+    outs = {k: (torch.empty((F, 2, N), dtype=torch.float64, device=dev),
+                torch.empty(F, dtype=torch.float64, device=dev),
+                torch.empty((F, nlev), dtype=torch.int32, device=dev)) for k in ("plain", "warm", "fallback")}
+    launches = {}
+
+    def plain():
+        o = outs["plain"]
+        ctx.register_batch_device(p, frames[0].data_ptr(), frames[1].data_ptr(), F, o[0].data_ptr(),
+                                  o[1].data_ptr(), o[2].data_ptr(), stream=st.cuda_stream)
+        launches["plain"] = ctx.stats()["kernel_launches"]
+
+    def warm():
+        o = outs["warm"]
+        ctx.register_batch_warm_device(p, net, frames[0].data_ptr(), frames[1].data_ptr(), F, o[0].data_ptr(),
+                                       o[1].data_ptr(), o[2].data_ptr(), stream=st.cuda_stream)
+        launches["warm"] = ctx.stats()["kernel_launches"]
+
+    def fallback():
+        o = outs["fallback"]
+        used = ctx.register_batch_warm_device(p, net, frames[0].data_ptr(), frames[1].data_ptr(), F,
+                                              o[0].data_ptr(), o[1].data_ptr(), o[2].data_ptr(),
+                                              d_plain_energies=outs["plain"][1].data_ptr(), rel_tol=WARM_TOL,
+                                              stream=st.cuda_stream)
+        launches["fallback"] = ctx.stats()["kernel_launches"]
+        return used
+
+    def timed(fn, reps):
+        for _ in range(max(1, args.warmup - 2)):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            r = fn()
+        e1.record(st)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / reps, r
+
+    barrier(world)
+    with ClockSampler(local) as clocks:
+        t_plain, _ = timed(plain, args.steps)
+        t_warm, _ = timed(warm, args.steps)
+        t_fb, used = timed(fallback, args.steps)
+    # the network alone on the evaluation pairs (prepared images at its input level)
+    prep = torch.empty((F + 1, msgpu.n_of(WARM_NET) ** 2), dtype=torch.float64, device=dev)
+    ctx.prepare_images_device(p, frames.data_ptr(), F + 1, WARM_NET, prep.data_ptr(), st.cuda_stream)
+    pred = torch.empty((F, 2, msgpu.n_of(WARM_NET - 1) ** 2), dtype=torch.float64, device=dev)
+    t_net, _ = timed(lambda: net.predict_device(prep[0].data_ptr(), 0, prep[1].data_ptr(), F, pred.data_ptr(),
+                                                st.cuda_stream), 5)
+    # the plain method one frame at a time (the unbatched plain GPU flow), on 5 frames
+    one = (torch.empty((1, 2, N), dtype=torch.float64, device=dev),)
+
+    def single():
+        for f in range(5):
+            ctx.register_batch_device(p, frames[0].data_ptr(), frames[1 + f].data_ptr(), 1, one[0].data_ptr(),
+                                      stream=st.cuda_stream)
+
+    t_single, _ = timed(single, 1)
+    t_single /= 5
+    # end to end through the host entry point, host buffers (pinned)
+    h_ref = frames[0].cpu().pin_memory()
+    h_tm = frames[1:].cpu().pin_memory()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        wh, we, _, _ = ctx.register_batch_warm(p, net, h_ref.numpy(), h_tm.numpy())
+    t_e2e = (time.perf_counter() - t0) / args.steps
+    t_fb_max = allreduce_max(t_fb, world)
+    ep = outs["plain"][1].cpu().numpy()
+    ew = outs["warm"][1].cpu().numpy()
+    ef = outs["fallback"][1].cpu().numpy()
+    r = (ew - ep) / np.abs(ep)
+    d_px = (outs["warm"][0] - outs["plain"][0]).abs().amax(dim=(1, 2)).cpu().numpy() * (n - 1)
+    steps_w = outs["warm"][2].float().mean(0).cpu().numpy()
+    steps_p = outs["plain"][2].float().mean(0).cpu().numpy()
+    net_flops = net_forward_flops(msgpu.n_of(WARM_NET)) * F
+    peak_tf = None
+    try:
+        peak_tf = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"])
+        peak_kind = "measured"
+    except Exception:
+        peak_tf, peak_kind = 1590.0, "fallback"
+    if rank == 0:
+        clk = clocks.summary()
+        out = {
+            "metric": METRIC, "value": world * F / (t_fb_max * 1e-3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_fb_max, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if fp64 else "f32+f64-reductions",
+            "data": "synthetic lattice series (GPU generator), random lattice per series",
+            "config": {"workload": f"{F} frames {n}x{n} registered to a reference frame, levels {WARM_START}-"
+                                   f"{WARM_LEVEL}, maxGDIterations {MAX_ITER}; warm start: the network (input level "
+                                   f"{WARM_NET}) predicts level {WARM_NET - 1}, the flow refines "
+                                   f"{WARM_NET - 1}-{WARM_LEVEL}; frames whose energy exceeds the plain batch's by "
+                                   f"more than {WARM_TOL} relative are registered again from the plain start "
+                                   f"(counted in the time); a step is the whole batch",
+                       "lattice": {"kind": spec.kind, "spacing_px": round(spec.spacing, 2),
+                                   "peak": round(spec.peak, 1), "max_disp_px": round(spec.max_disp, 2)},
+                       "inputs": "larger than L2 (50 frames of 8.4 MB)",
+                       "parallelism": f"weak, {world} ranks"},
+            "e2e": {"value": world * F / t_e2e, "unit": UNIT, "h2d_bytes_per_step": (F + 1) * N * 8,
+                    "d2h_bytes_per_step": F * 2 * N * 8 + F * 8 + F * nlev * 4,
+                    "note": "warm start without the fallback (the host entry point, pinned host buffers)"},
+            "gpu_launches": launches.get("fallback"),
+            "warm_start": {
+                "plain_batched_frames_per_s": F / (t_plain * 1e-3),
+                "warm_batched_frames_per_s": F / (t_warm * 1e-3),
+                "warm_with_fallback_frames_per_s": F / (t_fb * 1e-3),
+                "plain_single_frame_frames_per_s": 1.0 / (t_single * 1e-3),
+                "gain_vs_plain_batched": t_plain / t_fb,
+                "gain_vs_plain_single_frame": t_single * F / t_fb,
+                "fallback_frames": int(F - int(np.sum(used))),
+                "rel_energy_warm_vs_plain": {"median": float(np.median(r)), "min": float(r.min()),
+                                             "max": float(r.max()), "within_tol": int(np.sum(r <= WARM_TOL)),
+                                             "lower": int(np.sum(r <= 0))},
+                "after_fallback_max_rel_energy": float(np.max((ef - ep) / np.abs(ep))),
+                "max_dphi_px_warm_vs_plain": float(d_px.max()),
+                "steps_per_level_plain": [round(float(x), 1) for x in steps_p],
+                "steps_per_level_warm": [round(float(x), 1) for x in steps_w],
+                "network_ms": t_net,
+                "training": {"pairs": WARM_TRAIN_SERIES * WARM_FPS, "steps": WARM_STEPS, "batch": WARM_BATCH,
+                             "seconds": t_train, "data_seconds": t_data,
+                             "loss": [[k, round(l, 6)] for k, l in losses],
+                             "heldout_mse_px2": pred_mse, "zero_start_mse_px2": zero_mse,
+                             "tflops": train_flops / t_train / 1e12},
+            },
+            "roofline": {"bound": "tensor", "kernel": f"network forward (k_conv and its up/pack kernels), {F} "
+                                                      f"pairs at {msgpu.n_of(WARM_NET)}^2",
+                         "achieved": net_flops / (t_net * 1e-3) / 1e12, "peak": peak_tf, "unit": "TFLOP/s",
+                         "frac": net_flops / (t_net * 1e-3) / 1e12 / peak_tf, "peak_kind": peak_kind,
+                         "traffic": None, "algorithmic_flops_per_launch": net_flops, "avg_launch_ms": t_net},
+            "cpu_baseline": None,
+            "clocks": {k2: clk[k2] for k2 in ("sm_mhz", "sm_max_mhz", "reasons")},
+        }
+        print(json.dumps(out), flush=True)
+    net.close()
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -838,6 +1032,10 @@ def main():
                     help="uneven series of 129^2..1025^2 in one ragged batch (msgpu_register_ragged)")
     ap.add_argument("--files", action="store_true",
                     help="series read from .q2bz files, decoding overlapped with the GPU stages")
+    ap.add_argument("--warm", action="store_true",
+                    help="the learned warm start: train the network, then 50 frames 1025^2 warm-started vs plain")
+    ap.add_argument("--profile-net", type=int, default=0,
+                    help="small case for ncu: this many network training steps at input level 9, batch 4")
     ap.add_argument("--series", action="store_true",
                     help="time matchSeries' whole first stage with accumulated deformations (msgpu_match_series)")
     args = ap.parse_args()
@@ -848,6 +1046,23 @@ def main():
         return profile_case(args.profile_level, args.profile_iters, not args.fp32)
     if args.profile_compose or args.profile_series:
         return profile_series(args.profile_compose, not args.fp32)
+    if args.profile_net:
+        import torch
+        import msgpu
+        from msgpu import build as mbuild
+        mbuild.build()
+        ctx = msgpu.Context(0)
+        net = msgpu.Net(ctx, 9, seed=1)
+        B, n0, n1 = 4, msgpu.n_of(9), msgpu.n_of(8)
+        g = torch.Generator(device="cuda").manual_seed(0)
+        R = torch.rand((B, n0 * n0), dtype=torch.float64, device="cuda", generator=g)
+        T = torch.rand((B, n0 * n0), dtype=torch.float64, device="cuda", generator=g)
+        t = torch.randn((B, 2, n1 * n1), dtype=torch.float64, device="cuda", generator=g) / (n1 - 1)
+        for _ in range(args.profile_net):
+            loss = net.train_step_device(R.data_ptr(), n0 * n0, T.data_ptr(), t.data_ptr(), B, 1e-3)
+        print(json.dumps({"profile_net_steps": args.profile_net, "loss": loss,
+                          "launches_per_step": ctx.stats()["kernel_launches"]}))
+        return 0
     if args.profile_seismic:
         import msgpu
         from msgpu import build as mbuild
@@ -869,6 +1084,8 @@ def main():
         return main_ragged(args, world, rank, local)
     if args.seismic:
         return main_seismic(args, world, rank, local)
+    if args.warm:
+        return main_warm(args, world, rank, local)
 
     import numpy as np
     import torch

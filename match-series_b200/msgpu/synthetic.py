@@ -185,3 +185,69 @@ def psnr(a: np.ndarray, b: np.ndarray) -> float:
     mse = float(np.mean((a - b) ** 2))
     rng = float(b.max() - b.min())
     return float("inf") if mse == 0 else 10.0 * np.log10(rng * rng / mse)
+
+
+# --- the same lattice series generated on the GPU (torch) ----------------------
+# For the learned warm start's training and evaluation sets, which need many
+# large frames: the lattice, displacement and noise model of make_series,
+# evaluated on a CUDA device.  The random numbers differ from make_series'
+# (scalar draws from numpy, per-pixel draws from a torch generator), so the
+# frames follow the same distribution but are not the same frames.
+
+def random_spec(rng: np.random.Generator) -> LatticeSpec:
+    """A lattice of the uneven-series distribution: square or hexagonal,
+    spacing U(8, 16) px, column sigma 0.18 spacing, Poisson peak U(20, 100),
+    displacements up to U(1, 3) px, row jitter U(0.3, 0.7) px."""
+    a = float(rng.uniform(8, 16))
+    return LatticeSpec("hex" if rng.random() < 0.5 else "square", a, 0.18 * a, 0.6, 1.0,
+                       float(rng.uniform(20, 100)), float(rng.uniform(1, 3)), float(rng.uniform(0.3, 0.7)))
+
+
+def make_series_torch(n: int, num_frames: int, spec: LatticeSpec, seed: int, device, noise: bool = True):
+    """make_series on a CUDA device: frames [F, n, n] float64 counts (torch)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    kw = dict(dtype=torch.float64, device=device)
+    y, x = torch.meshgrid(torch.arange(n, **kw), torch.arange(n, **kw), indexing="ij")
+    a1, a2 = _lattice_basis(spec)
+    Binv = np.linalg.inv(np.stack([a1, a2], axis=1))
+    span = int(np.ceil(2.0 * n / spec.spacing)) + 16
+    amps = torch.from_numpy(rng.uniform(spec.amp_lo, spec.amp_hi, size=(2 * span + 1, 2 * span + 1))).to(device)
+    reach = int(np.ceil(4.0 * spec.sigma / (spec.spacing * 0.5))) + 1
+    inv2s2 = 1.0 / (2.0 * spec.sigma * spec.sigma)
+    ox, oy = 3.3, 4.1
+    frames = torch.empty((num_frames, n, n), **kw)
+    for f in range(num_frames):
+        u = torch.zeros((n, n), **kw)
+        v = torch.zeros((n, n), **kw)
+        for _ in range(spec.n_waves):
+            wl, th, ph = rng.uniform(spec.wl_lo, spec.wl_hi), rng.uniform(0, 2 * np.pi), rng.uniform(0, 2 * np.pi)
+            k = 2 * np.pi / wl
+            arg = k * (np.cos(th) * x + np.sin(th) * y) + ph
+            au, av = rng.normal(size=2)
+            s = torch.sin(arg)
+            u += au * s
+            v += av * s
+        m = float(torch.sqrt(u * u + v * v).max())
+        if m > 0:
+            sc = spec.max_disp * rng.uniform(0.5, 1.0) / m
+            u *= sc
+            v *= sc
+        u += torch.randn((n, 1), generator=g, **kw) * spec.jitter
+        px, py = x + u - ox, y + v - oy
+        f1 = Binv[0, 0] * px + Binv[0, 1] * py
+        f2 = Binv[1, 0] * px + Binv[1, 1] * py
+        i0, j0 = torch.floor(f1).long(), torch.floor(f2).long()
+        img = torch.zeros((n, n), **kw)
+        for di in range(-reach, reach + 1):
+            for dj in range(-reach, reach + 1):
+                ii, jj = i0 + di, j0 + dj
+                cx = ii * a1[0] + jj * a2[0]
+                cy = ii * a1[1] + jj * a2[1]
+                d2 = (px - cx) ** 2 + (py - cy) ** 2
+                amp = amps[(ii + span).clamp(0, 2 * span), (jj + span).clamp(0, 2 * span)]
+                img += amp * torch.exp(-d2 * inv2s2)
+        frames[f] = torch.poisson(spec.peak * img, generator=g) if noise else spec.peak * img
+    return frames
