@@ -2829,10 +2829,11 @@ int net_buffers(msgpu_net* net, int batch) {
 
 int net_conv_launch(msgpu_net* net, const msg::unet::ConvArgs& a, int rows, cudaStream_t st) {
   const int bn = tile_of(rows);
-  const dim3 grid((unsigned)((a.total + msg::unet::kBM - 1) / msg::unet::kBM), (unsigned)(rows / bn));
-  if (bn == 64) msg::unet::k_conv<64><<<grid, msg::unet::kThreads, 0, st>>>(a);
-  else if (bn == 32) msg::unet::k_conv<32><<<grid, msg::unet::kThreads, 0, st>>>(a);
-  else msg::unet::k_conv<16><<<grid, msg::unet::kThreads, 0, st>>>(a);
+  namespace u = msg::unet;
+  const dim3 grid((unsigned)((a.total + u::kConvBM - 1) / u::kConvBM), (unsigned)(rows / bn));
+  if (bn == 64) u::k_conv<64><<<grid, u::kThreads, u::conv_smem_bytes<64>(), st>>>(a);
+  else if (bn == 32) u::k_conv<32><<<grid, u::kThreads, u::conv_smem_bytes<32>(), st>>>(a);
+  else u::k_conv<16><<<grid, u::kThreads, u::conv_smem_bytes<16>(), st>>>(a);
   NCK(cudaGetLastError());
   ++net->ctx->stats.kernel_launches;
   return MSGPU_OK;
@@ -2885,16 +2886,15 @@ int net_bwd_weights(msgpu_net* net, int i, const View& in, const View& dy, int B
   chunks = std::min(chunks, std::max(1, total / 256));
   const int chunk = ((total + chunks - 1) / chunks + msg::unet::kBK - 1) / msg::unet::kBK * msg::unet::kBK;
   chunks = (total + chunk - 1) / chunk;
-  const int bchunks = std::min(256, std::max(1, total / 512));
-  const int bchunk = (total + bchunks - 1) / bchunks;
-  const size_t need = (size_t)chunks * l.cout_pad * K + (size_t)bchunks * l.cout;
+  const size_t need = (size_t)chunks * l.cout_pad * (K + 1);
   int rc;
   if ((rc = ensure(net->ctx, net->part, need * sizeof(float)))) return rc;
   float* part = (float*)net->part.p;
+  float* bpart = part + (size_t)chunks * l.cout_pad * K;
   msg::unet::WgradArgs a;
   a.in = in.p; a.in_img = in.img; a.in_n = in.n; a.in_cs = in.cs; a.cin = l.cin_pad;
   a.dy = dy.p; a.dy_img = dy.img; a.dy_n = dy.n; a.dy_cs = dy.cs; a.cout_pad = l.cout_pad;
-  a.stride = l.stride; a.part = part; a.total = total; a.chunk = chunk;
+  a.stride = l.stride; a.part = part; a.bpart = bpart; a.total = total; a.chunk = chunk;
   const dim3 grid((unsigned)xt, (unsigned)yt, (unsigned)chunks);
   if (bm == 64) msg::unet::k_wgrad<64><<<grid, msg::unet::kThreads, 0, st>>>(a);
   else if (bm == 32) msg::unet::k_wgrad<32><<<grid, msg::unet::kThreads, 0, st>>>(a);
@@ -2902,11 +2902,9 @@ int net_bwd_weights(msgpu_net* net, int i, const View& in, const View& dy, int B
   const int nw = l.cout * 9 * l.cin;
   msg::unet::k_wgrad_reduce<<<std::min(1024, (nw + 255) / 256), 256, 0, st>>>(part, chunks, l.cout, l.cout_pad, l.cin,
                                                                               l.cin_pad, net->grad + l.w_off);
-  float* bpart = part + (size_t)chunks * l.cout_pad * K;
-  msg::unet::k_bgrad_part<<<bchunks, 128, 0, st>>>(dy.p, dy.img, dy.n * dy.n, dy.cs, l.cout, total, bchunk, bpart);
-  msg::unet::k_bgrad_reduce<<<1, 128, 0, st>>>(bpart, bchunks, l.cout, net->grad + l.b_off);
+  msg::unet::k_bgrad_reduce<<<1, 128, 0, st>>>(bpart, chunks, l.cout, l.cout_pad, net->grad + l.b_off);
   NCK(cudaGetLastError());
-  net->ctx->stats.kernel_launches += 4;
+  net->ctx->stats.kernel_launches += 3;
   return MSGPU_OK;
 }
 

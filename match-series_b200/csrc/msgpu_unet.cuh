@@ -9,18 +9,20 @@
 //
 // k_conv: one 3x3 convolution as an implicit GEMM on the tensor pipe
 // (mma.sync m16n8k16, bf16 operands, fp32 accumulation).  A block computes
-// 64 output nodes x BN output channels; the reduction runs over
-// (tap, input channel) in stages of 32, staged in shared memory by
-// cp.async with zero fill for taps outside the grid.  mode 0 reads input
+// 128 output nodes x BN output channels; the reduction runs over
+// (tap, input channel) in stages of 32, staged in shared memory by a
+// three-stage cp.async pipeline with zero fill for taps outside the grid,
+// fragments loaded by ldmatrix.  mode 0 reads input
 // node stride*q + d (forward), mode 1 reads (q - d)/stride when that is a
 // node (the data gradient of a forward convolution, with the weights
 // transposed).  The epilogue adds the bias, accumulates into the output,
 // applies ReLU and a ReLU mask as asked.
 //
 // k_wgrad: weight gradient dW[co][(tap, ci)] = sum over nodes of
-// dY[node][co] * X[src(node, tap)][ci], the node sum split into chunks; each
-// block writes its chunk's partial, k_wgrad_reduce adds the partials in
-// chunk order (deterministic training).
+// dY[node][co] * X[src(node, tap)][ci] and the bias gradient, the node sum
+// split into chunks; each block writes its chunk's partial, k_wgrad_reduce
+// and k_bgrad_reduce add the partials in chunk order (deterministic
+// training).
 #pragma once
 
 #include <cuda_bf16.h>
@@ -32,7 +34,6 @@ namespace unet {
 typedef __nv_bfloat16 bf16;
 
 constexpr int kThreads = 128;
-constexpr int kBM = 64;        // output nodes per conv block
 constexpr int kBK = 32;        // reduction elements per stage
 constexpr int kSA = kBK + 8;   // shared-memory row stride (bf16): conflict-free fragment loads
 
@@ -89,22 +90,42 @@ struct ConvArgs {
   int total;             // images * out_n^2
 };
 
+__device__ __forceinline__ void ldsm_x4(uint32_t* r, const void* smem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(s));
+}
+__device__ __forceinline__ void ldsm_x4_trans(uint32_t* r, const void* smem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(s));
+}
+
+constexpr int kConvBM = 128;   // output nodes per conv block (32 per warp)
+constexpr int kStages = 3;
+
+// Block: 128 output nodes x BN channels, 4 warps of 32 nodes each (two m16
+// tiles sharing every B fragment); fragments by ldmatrix from rows of 80
+// bytes (conflict-free); three cp.async stages.
 template <int BN>
 __global__ void __launch_bounds__(kThreads) k_conv(ConvArgs a) {
-  __shared__ __align__(16) bf16 As[2][kBM][kSA];
-  __shared__ __align__(16) bf16 Bs[2][BN][kSA];
+  extern __shared__ __align__(16) unsigned char conv_smem[];
+  bf16 (*As)[kConvBM][kSA] = reinterpret_cast<bf16 (*)[kConvBM][kSA]>(conv_smem);
+  bf16 (*Bs)[BN][kSA] = reinterpret_cast<bf16 (*)[BN][kSA]>(conv_smem + sizeof(bf16) * kStages * kConvBM * kSA);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int p0 = blockIdx.x * kBM;
+  const int p0 = blockIdx.x * kConvBM;
   const int n0 = blockIdx.y * BN;
   const int K = 9 * a.cin;
   const int nk = (K + kBK - 1) / kBK;
   const int outN2 = a.out_n * a.out_n;
-  int r_img[2], r_qy[2], r_qx[2];
-  bool r_ok[2];
+  // the four rows (nodes) this thread loads: row = tid / 4 + 32 i
+  int r_img[4], r_qy[4], r_qx[4];
+  bool r_ok[4];
 #pragma unroll
-  for (int i = 0; i < 2; ++i) {
-    const int row = (tid + i * kThreads) >> 2;
-    const int p = p0 + row;
+  for (int i = 0; i < 4; ++i) {
+    const int p = p0 + (tid >> 2) + 32 * i;
     r_ok[i] = p < a.total;
     const int img = r_ok[i] ? p / outN2 : 0;
     const int q = r_ok[i] ? p - img * outN2 : 0;
@@ -112,87 +133,115 @@ __global__ void __launch_bounds__(kThreads) k_conv(ConvArgs a) {
     r_qy[i] = q / a.out_n;
     r_qx[i] = q - r_qy[i] * a.out_n;
   }
+  const int g = tid & 3;
   auto load_stage = [&](int s, int kt) {
-    const int k0 = kt * kBK;
+    const int k = kt * kBK + g * 8;
+    const bool kin = k < K;
+    int tap = 0, ci = 0;
+    if (kin) {
+      tap = k / a.cin;
+      ci = k - tap * a.cin;
+    }
 #pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const int idx = tid + i * kThreads;
-      const int row = idx >> 2, g = idx & 3;
-      const int k = k0 + g * 8;
+    for (int i = 0; i < 4; ++i) {
       const bf16* src = a.in;
-      bool ok = r_ok[i] && k < K;
+      bool ok = r_ok[i] && kin;
       if (ok) {
-        const int tap = k / a.cin, ci = k - tap * a.cin;
         int sy, sx;
         ok = conv_src(a.mode, a.stride, a.in_n, r_qy[i], r_qx[i], tap / 3 - 1, tap % 3 - 1, sy, sx);
         if (ok) src = a.in + (size_t)r_img[i] * a.in_img + ((size_t)sy * a.in_n + sx) * a.in_cs + ci;
       }
-      cp_async16(&As[s][row][g * 8], src, ok ? 16 : 0);
+      cp_async16(&As[s][(tid >> 2) + 32 * i][g * 8], src, ok ? 16 : 0);
     }
     for (int idx = tid; idx < BN * 4; idx += kThreads) {
-      const int row = idx >> 2, g = idx & 3;
-      const int k = k0 + g * 8;
-      const bool ok = k < K;
-      cp_async16(&Bs[s][row][g * 8], ok ? a.w + (size_t)(n0 + row) * K + k : a.w, ok ? 16 : 0);
+      const int row = idx >> 2, gg = idx & 3;
+      const int kk = kt * kBK + gg * 8;
+      const bool ok = kk < K;
+      cp_async16(&Bs[s][row][gg * 8], ok ? a.w + (size_t)(n0 + row) * K + kk : a.w, ok ? 16 : 0);
     }
-    cp_async_commit();
   };
-  float acc[BN / 8][4];
+  float acc[2][BN / 8][4];
 #pragma unroll
-  for (int j = 0; j < BN / 8; ++j)
-#pragma unroll
-    for (int e = 0; e < 4; ++e) acc[j][e] = 0.f;
-  load_stage(0, 0);
-  for (int kt = 0; kt < nk; ++kt) {
-    if (kt + 1 < nk) {
-      load_stage((kt + 1) & 1, kt + 1);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
-    __syncthreads();
-    const int s = kt & 1;
-#pragma unroll
-    for (int kk = 0; kk < kBK; kk += 16) {
-      const int r = warp * 16 + (lane >> 2), c = kk + 2 * (lane & 3);
-      uint32_t af[4];
-      af[0] = *reinterpret_cast<const uint32_t*>(&As[s][r][c]);
-      af[1] = *reinterpret_cast<const uint32_t*>(&As[s][r + 8][c]);
-      af[2] = *reinterpret_cast<const uint32_t*>(&As[s][r][c + 8]);
-      af[3] = *reinterpret_cast<const uint32_t*>(&As[s][r + 8][c + 8]);
-#pragma unroll
-      for (int j = 0; j < BN / 8; ++j) {
-        const int nr = j * 8 + (lane >> 2);
-        mma_bf16(acc[j], af, *reinterpret_cast<const uint32_t*>(&Bs[s][nr][c]),
-                 *reinterpret_cast<const uint32_t*>(&Bs[s][nr][c + 8]));
-      }
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int p = p0 + warp * 16 + (lane >> 2) + 8 * h;
-    if (p >= a.total) continue;
-    const int img = p / outN2, q = p - img * outN2;
+  for (int m = 0; m < 2; ++m)
 #pragma unroll
     for (int j = 0; j < BN / 8; ++j)
 #pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int co = n0 + j * 8 + 2 * (lane & 3) + e;
-        if (co >= a.cout) continue;
-        float v = acc[j][2 * h + e];
-        if (a.bias) v += a.bias[co];
-        const size_t o = (size_t)img * a.out_img + (size_t)q * a.out_cs + co;
-        if (a.accumulate) v += __bfloat162float(static_cast<const bf16*>(a.out)[o]);
-        if (a.relu) v = fmaxf(v, 0.f);
-        if (a.mask && !(__bfloat162float(a.mask[(size_t)img * a.mask_img + (size_t)q * a.mask_cs + co]) > 0.f))
-          v = 0.f;
-        if (a.out_f32)
-          static_cast<float*>(a.out)[o] = v;
-        else
-          static_cast<bf16*>(a.out)[o] = __float2bfloat16(v);
-      }
+      for (int e = 0; e < 4; ++e) acc[m][j][e] = 0.f;
+#pragma unroll
+  for (int s = 0; s < kStages - 1; ++s) {
+    if (s < nk) load_stage(s, s);
+    cp_async_commit();
   }
+  // ldmatrix lane addresses: A rows r0 + lane % 16, column + 8 (lane / 16);
+  // B rows n + lane % 8 + 8 (lane / 16), column + 8 ((lane / 8) % 2)
+  const int a_row = warp * 32 + (lane & 15), a_col = 8 * (lane >> 4);
+  const int b_row = (lane & 7) + 8 * (lane >> 4), b_col = 8 * ((lane >> 3) & 1);
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_async_wait<kStages - 2>();
+    __syncthreads();
+    {
+      const int kn = kt + kStages - 1;
+      if (kn < nk) load_stage(kn % kStages, kn);
+      cp_async_commit();
+    }
+    const int s = kt % kStages;
+#pragma unroll
+    for (int kk = 0; kk < kBK; kk += 16) {
+      uint32_t af[2][4];
+      ldsm_x4(af[0], &As[s][a_row][kk + a_col]);
+      ldsm_x4(af[1], &As[s][a_row + 16][kk + a_col]);
+#pragma unroll
+      for (int j = 0; j < BN / 8; j += 2) {
+        uint32_t bf[4];
+        ldsm_x4(bf, &Bs[s][j * 8 + b_row][kk + b_col]);
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+          mma_bf16(acc[m][j], af[m], bf[0], bf[1]);
+          mma_bf16(acc[m][j + 1], af[m], bf[2], bf[3]);
+        }
+      }
+    }
+  }
+  cp_async_wait<0>();
+#pragma unroll
+  for (int m = 0; m < 2; ++m)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int p = p0 + warp * 32 + 16 * m + (lane >> 2) + 8 * h;
+      if (p >= a.total) continue;
+      const int img = p / outN2, q = p - img * outN2;
+      const size_t ob = (size_t)img * a.out_img + (size_t)q * a.out_cs;
+      const bf16* mk = a.mask ? a.mask + (size_t)img * a.mask_img + (size_t)q * a.mask_cs : nullptr;
+#pragma unroll
+      for (int j = 0; j < BN / 8; ++j) {
+        const int co = n0 + j * 8 + 2 * (lane & 3);
+        float v[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          v[e] = acc[m][j][2 * h + e];
+          if (co + e >= a.cout) continue;
+          if (a.bias) v[e] += a.bias[co + e];
+          if (a.accumulate) v[e] += __bfloat162float(static_cast<const bf16*>(a.out)[ob + co + e]);
+          if (a.relu) v[e] = fmaxf(v[e], 0.f);
+          if (mk && !(__bfloat162float(mk[co + e]) > 0.f)) v[e] = 0.f;
+        }
+        if (a.out_f32) {
+          float* o = static_cast<float*>(a.out) + ob;
+          if (co < a.cout) o[co] = v[0];
+          if (co + 1 < a.cout) o[co + 1] = v[1];
+        } else if (co + 1 < a.cout) {
+          // co even, channel stride and view offsets multiples of 8: 4-byte aligned
+          *reinterpret_cast<__nv_bfloat162*>(static_cast<bf16*>(a.out) + ob + co) = __floats2bfloat162_rn(v[0], v[1]);
+        } else if (co < a.cout) {
+          static_cast<bf16*>(a.out)[ob + co] = __float2bfloat16(v[0]);
+        }
+      }
+    }
+}
+
+template <int BN>
+constexpr size_t conv_smem_bytes() {
+  return sizeof(bf16) * kStages * (kConvBM + BN) * kSA;
 }
 
 struct WgradArgs {
@@ -204,105 +253,103 @@ struct WgradArgs {
   int dy_n, dy_cs, cout_pad;
   int stride;
   float* part;           // [chunks][cout_pad][9 * cin]
+  float* bpart;          // [chunks][cout_pad]: node sums of dy (the bias gradient)
   int total;             // images * dy_n^2
   int chunk;             // nodes per block (multiple of kBK)
 };
 
 // GEMM dW^T[co][k] over node chunks: rows = output channels (BM per block),
-// columns = 64 reduction indices (tap, ci), inner dimension = nodes.
+// columns = 64 reduction indices (tap, ci), inner dimension = nodes.  Both
+// operands are staged in their natural NHWC layout ([node][channel]) by a
+// three-stage cp.async pipeline and transposed into the mma fragments by
+// ldmatrix.trans.  Blocks of the first column tile also sum dY over their
+// nodes (the bias gradient).
 template <int BM>
 __global__ void __launch_bounds__(kThreads) k_wgrad(WgradArgs a) {
   constexpr int WM = BM / 16, WN = 4 / WM, NT = 64 / WN / 8;
-  constexpr int NA = BM * kBK / 8;   // dY vectors per stage
-  constexpr int RA = (NA + kThreads - 1) / kThreads;
-  __shared__ __align__(16) bf16 As[BM][kSA];   // [co][node]
-  __shared__ __align__(16) bf16 Bs[64][kSA];   // [k][node]
+  constexpr int DS = BM + 8, XS = 64 + 8;   // row strides (bf16): conflict-free ldmatrix
+  __shared__ __align__(16) bf16 Ds[kStages][kBK][DS];   // dY [node][co]
+  __shared__ __align__(16) bf16 Xs[kStages][kBK][XS];   // X  [node][k]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp % WM, wn = warp / WM;
   const int K = 9 * a.cin;
   const int kb = blockIdx.x * 64, cb = blockIdx.y * BM;
   const int pbeg = blockIdx.z * a.chunk;
   const int pend = min(a.total, pbeg + a.chunk);
+  const int nsteps = (pend - pbeg + kBK - 1) / kBK;
   const int dyN2 = a.dy_n * a.dy_n;
+  const bool bias_block = blockIdx.x == 0;
+  auto load_stage = [&](int s, int it) {
+    const int pb = pbeg + it * kBK;
+    for (int idx = tid; idx < kBK * (BM / 8); idx += kThreads) {
+      const int pi = idx / (BM / 8), v = idx - pi * (BM / 8);
+      const int p = pb + pi;
+      const bf16* src = a.dy;
+      const bool ok = p < pend;
+      if (ok) {
+        const int img = p / dyN2, q = p - img * dyN2;
+        src = a.dy + (size_t)img * a.dy_img + (size_t)q * a.dy_cs + cb + 8 * v;
+      }
+      cp_async16(&Ds[s][pi][8 * v], src, ok ? 16 : 0);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int idx = tid + i * kThreads;   // 32 nodes x 8 groups of the 64 columns
+      const int pi = idx >> 3, gg = idx & 7;
+      const int p = pb + pi, k = kb + 8 * gg;
+      const bf16* src = a.in;
+      bool ok = p < pend && k < K;
+      if (ok) {
+        const int img = p / dyN2, q = p - img * dyN2;
+        const int qy = q / a.dy_n, qx = q - qy * a.dy_n;
+        const int tap = k / a.cin, ci = k - tap * a.cin;
+        int sy, sx;
+        ok = conv_src(0, a.stride, a.in_n, qy, qx, tap / 3 - 1, tap % 3 - 1, sy, sx);
+        if (ok) src = a.in + (size_t)img * a.in_img + ((size_t)sy * a.in_n + sx) * a.in_cs + ci;
+      }
+      cp_async16(&Xs[s][pi][8 * gg], src, ok ? 16 : 0);
+    }
+  };
   float acc[NT][4];
 #pragma unroll
   for (int j = 0; j < NT; ++j)
 #pragma unroll
     for (int e = 0; e < 4; ++e) acc[j][e] = 0.f;
-  uint4 ra[RA], rb[2];
-  auto gload = [&](int pb) {
+  float bsum = 0.f;
 #pragma unroll
-    for (int i = 0; i < RA; ++i) {
-      const int idx = tid + i * kThreads;
-      ra[i] = make_uint4(0, 0, 0, 0);
-      if (idx < NA) {
-        const int pi = idx / (BM / 8), v = idx - pi * (BM / 8);
-        const int p = pb + pi;
-        if (p < pend) {
-          const int img = p / dyN2, q = p - img * dyN2;
-          ra[i] = *reinterpret_cast<const uint4*>(a.dy + (size_t)img * a.dy_img + (size_t)q * a.dy_cs + cb + 8 * v);
-        }
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const int idx = tid + i * kThreads;   // 32 nodes x 8 groups
-      const int pi = idx >> 3, g = idx & 7;
-      const int p = pb + pi, k = kb + 8 * g;
-      rb[i] = make_uint4(0, 0, 0, 0);
-      if (p < pend && k < K) {
-        const int img = p / dyN2, q = p - img * dyN2;
-        const int qy = q / a.dy_n, qx = q - qy * a.dy_n;
-        const int tap = k / a.cin, ci = k - tap * a.cin;
-        int sy, sx;
-        if (conv_src(0, a.stride, a.in_n, qy, qx, tap / 3 - 1, tap % 3 - 1, sy, sx))
-          rb[i] = *reinterpret_cast<const uint4*>(a.in + (size_t)img * a.in_img +
-                                                  ((size_t)sy * a.in_n + sx) * a.in_cs + ci);
-      }
-    }
-  };
-  auto sstore = [&]() {
-#pragma unroll
-    for (int i = 0; i < RA; ++i) {
-      const int idx = tid + i * kThreads;
-      if (idx < NA) {
-        const int pi = idx / (BM / 8), v = idx - pi * (BM / 8);
-        const bf16* e = reinterpret_cast<const bf16*>(&ra[i]);
-#pragma unroll
-        for (int t = 0; t < 8; ++t) As[8 * v + t][pi] = e[t];
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const int idx = tid + i * kThreads;
-      const int pi = idx >> 3, g = idx & 7;
-      const bf16* e = reinterpret_cast<const bf16*>(&rb[i]);
-#pragma unroll
-      for (int t = 0; t < 8; ++t) Bs[8 * g + t][pi] = e[t];
-    }
-  };
-  if (pbeg < pend) gload(pbeg);
-  for (int pb = pbeg; pb < pend; pb += kBK) {
-    sstore();
+  for (int s = 0; s < kStages - 1; ++s) {
+    if (s < nsteps) load_stage(s, s);
+    cp_async_commit();
+  }
+  // ldmatrix.trans lane addresses: A (co x node) from Ds rows node, columns co;
+  // B (node x k) from Xs rows node, columns k
+  const int a_node = (lane & 7) + 8 * (lane >> 4), a_co = wm * 16 + 8 * ((lane >> 3) & 1);
+  const int b_node = (lane & 7) + 8 * ((lane >> 3) & 1), b_k = wn * (64 / WN) + 8 * (lane >> 4);
+  for (int it = 0; it < nsteps; ++it) {
+    cp_async_wait<kStages - 2>();
     __syncthreads();
-    if (pb + kBK < pend) gload(pb + kBK);
+    {
+      const int kn = it + kStages - 1;
+      if (kn < nsteps) load_stage(kn % kStages, kn);
+      cp_async_commit();
+    }
+    const int s = it % kStages;
+    if (bias_block && tid < BM)
+      for (int r = 0; r < kBK; ++r) bsum += __bfloat162float(Ds[s][r][tid]);
 #pragma unroll
     for (int kk = 0; kk < kBK; kk += 16) {
-      const int r = wm * 16 + (lane >> 2), c = kk + 2 * (lane & 3);
       uint32_t af[4];
-      af[0] = *reinterpret_cast<const uint32_t*>(&As[r][c]);
-      af[1] = *reinterpret_cast<const uint32_t*>(&As[r + 8][c]);
-      af[2] = *reinterpret_cast<const uint32_t*>(&As[r][c + 8]);
-      af[3] = *reinterpret_cast<const uint32_t*>(&As[r + 8][c + 8]);
+      ldsm_x4_trans(af, &Ds[s][kk + a_node][a_co]);
 #pragma unroll
-      for (int j = 0; j < NT; ++j) {
-        const int nr = wn * (64 / WN) + j * 8 + (lane >> 2);
-        mma_bf16(acc[j], af, *reinterpret_cast<const uint32_t*>(&Bs[nr][c]),
-                 *reinterpret_cast<const uint32_t*>(&Bs[nr][c + 8]));
+      for (int j = 0; j < NT; j += 2) {
+        uint32_t bf[4];
+        ldsm_x4_trans(bf, &Xs[s][kk + b_node][b_k + j * 8]);
+        mma_bf16(acc[j], af, bf[0], bf[1]);
+        mma_bf16(acc[j + 1], af, bf[2], bf[3]);
       }
     }
-    __syncthreads();
   }
+  cp_async_wait<0>();
   float* part = a.part + (size_t)blockIdx.z * a.cout_pad * K;
 #pragma unroll
   for (int j = 0; j < NT; ++j)
@@ -312,6 +359,7 @@ __global__ void __launch_bounds__(kThreads) k_wgrad(WgradArgs a) {
       const int k = kb + wn * (64 / WN) + j * 8 + 2 * (lane & 3) + (e & 1);
       if (k < K) part[(size_t)co * K + k] = acc[j][e];
     }
+  if (bias_block && tid < BM) a.bpart[(size_t)blockIdx.z * a.cout_pad + cb + tid] = bsum;
 }
 
 // dW of one layer from the chunk partials, added in chunk order, into the
@@ -330,24 +378,12 @@ __global__ void k_wgrad_reduce(const float* part, int chunks, int cout, int cout
   }
 }
 
-// bias gradient: per chunk (block) and channel (thread) the node sum, then in chunk order
-__global__ void k_bgrad_part(const bf16* dy, size_t dy_img, int dy_n2, int dy_cs, int cout, int total, int chunk,
-                             float* part) {
-  const int co = threadIdx.x;
-  if (co >= cout) return;
-  const int pbeg = blockIdx.x * chunk, pend = min(total, pbeg + chunk);
-  float s = 0.f;
-  for (int p = pbeg; p < pend; ++p) {
-    const int img = p / dy_n2, q = p - img * dy_n2;
-    s += __bfloat162float(dy[(size_t)img * dy_img + (size_t)q * dy_cs + co]);
-  }
-  part[(size_t)blockIdx.x * cout + co] = s;
-}
-__global__ void k_bgrad_reduce(const float* part, int chunks, int cout, float* grad) {
+// the bias gradient from the chunks' node sums, in chunk order
+__global__ void k_bgrad_reduce(const float* bpart, int chunks, int cout, int cout_pad, float* grad) {
   const int co = blockIdx.x * blockDim.x + threadIdx.x;
   if (co >= cout) return;
   float s = 0.f;
-  for (int c = 0; c < chunks; ++c) s += part[(size_t)c * cout + co];
+  for (int c = 0; c < chunks; ++c) s += bpart[(size_t)c * cout_pad + co];
   grad[co] = s;
 }
 
