@@ -1036,6 +1036,8 @@ def main():
                     help="the learned warm start: train the network, then 50 frames 1025^2 warm-started vs plain")
     ap.add_argument("--profile-net", type=int, default=0,
                     help="small case for ncu: this many network training steps at input level 9, batch 4")
+    ap.add_argument("--profile-predict", type=int, default=0,
+                    help="case for the ncu launch list: network predictions of 8 pairs at 1025^2, this many times")
     ap.add_argument("--series", action="store_true",
                     help="time matchSeries' whole first stage with accumulated deformations (msgpu_match_series)")
     args = ap.parse_args()
@@ -1046,6 +1048,23 @@ def main():
         return profile_case(args.profile_level, args.profile_iters, not args.fp32)
     if args.profile_compose or args.profile_series:
         return profile_series(args.profile_compose, not args.fp32)
+    if args.profile_predict:
+        import torch
+        import msgpu
+        from msgpu import build as mbuild
+        mbuild.build()
+        ctx = msgpu.Context(0)
+        net = msgpu.Net(ctx, 10, seed=1)
+        B, n0, n1 = 8, msgpu.n_of(10), msgpu.n_of(9)
+        g = torch.Generator(device="cuda").manual_seed(0)
+        R = torch.rand((B, n0 * n0), dtype=torch.float64, device="cuda", generator=g)
+        T = torch.rand((B, n0 * n0), dtype=torch.float64, device="cuda", generator=g)
+        phi = torch.empty((B, 2, n1 * n1), dtype=torch.float64, device="cuda")
+        for _ in range(args.profile_predict):
+            net.predict_device(R.data_ptr(), n0 * n0, T.data_ptr(), B, phi.data_ptr())
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_predict": args.profile_predict, "launches": ctx.stats()["kernel_launches"]}))
+        return 0
     if args.profile_net:
         import torch
         import msgpu

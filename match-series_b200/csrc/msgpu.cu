@@ -1744,8 +1744,10 @@ namespace {
 // Mx for Q1 elements with tensor Gauss quadrature), so with the generalised
 // eigenvectors of (K1, M1) -- the cosine modes v_k(i) = cos(k pi i/(n-1)),
 // normalised to v^T M1 v = 1, eigenvalues 6/h^2 (1 - cos t_k)/(2 + cos t_k) --
-// (M + tau L)^{-1} = V (1 + tau (lx_i + ly_j))^{-1} V^T, four dense products
-// per application (cuBLAS DGEMM) and a spectral scaling.  It is the exact
+// (M + tau L)^{-1} = V (1 + tau (lx_i + ly_j))^{-1} V^T: dense products
+// (cuBLAS DGEMM) and a spectral scaling, the x products on the parity-folded
+// halves of each column (k_xfold: even and odd modes separately, half the
+// work of one full product each).  It is the exact
 // inverse that the reference's CholeskyBasedInverseH1Metric computes by a
 // sparse Cholesky factorisation, up to rounding.
 void host_spectral_basis(int n, double h, double* V, double* lam) {
@@ -1770,7 +1772,8 @@ void host_spectral_basis(int n, double h, double* V, double* lam) {
 }
 
 struct XsBufs {
-  double *Vx, *Vy, *lx, *ly;           // spectral basis
+  double *Ve, *Vo, *Vy, *lx, *ly;      // spectral basis: even and odd x modes on half the rows, y modes;
+                                       // lx in the folded order (even modes, then odd modes)
   double *d, *og, *od, *de, *tx, *kphi, *t1, *t2, *part, *scal;
 };
 
@@ -1780,18 +1783,30 @@ int xs_setup(msgpu_context* ctx, int nx, int ny, XsBufs& B, cudaStream_t st) {
     if (cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS) return fail(ctx, MSGPU_ERR_CUDA, "cublasCreate failed");
   }
   if (cublasSetStream(ctx->blas, st) != CUBLAS_STATUS_SUCCESS) return fail(ctx, MSGPU_ERR_CUDA, "cublasSetStream failed");
-  const size_t nb = (size_t)nx * nx + (size_t)ny * ny + nx + ny;
+  const int ne = (nx + 1) / 2, no = nx / 2;
+  const size_t nb = (size_t)ne * ne + (size_t)no * no + (size_t)ny * ny + nx + ny;
   if ((rc = ensure(ctx, ctx->xs_basis, sizeof(double) * nb))) return rc;
-  B.Vx = (double*)ctx->xs_basis.p;
-  B.Vy = B.Vx + (size_t)nx * nx;
+  B.Ve = (double*)ctx->xs_basis.p;
+  B.Vo = B.Ve + (size_t)ne * ne;
+  B.Vy = B.Vo + (size_t)no * no;
   B.lx = B.Vy + (size_t)ny * ny;
   B.ly = B.lx + nx;
   if (ctx->xs_nx != nx || ctx->xs_ny != ny) {
     const double h = 1. / (double)((nx > ny ? nx : ny) - 1);
-    std::vector<double> hb(nb);
-    host_spectral_basis(nx, h, hb.data(), hb.data() + (size_t)nx * nx + (size_t)ny * ny);
-    host_spectral_basis(ny, h, hb.data() + (size_t)nx * nx, hb.data() + (size_t)nx * nx + (size_t)ny * ny + nx);
-    CK(cudaMemcpy(B.Vx, hb.data(), sizeof(double) * nb, cudaMemcpyHostToDevice));
+    std::vector<double> vx((size_t)nx * nx), lxf(nx), hb(nb);
+    host_spectral_basis(nx, h, vx.data(), lxf.data());
+    double* Ve = hb.data();
+    double* Vo = Ve + (size_t)ne * ne;
+    for (int k = 0; k < ne; ++k)
+      for (int i = 0; i < ne; ++i) Ve[i + (size_t)k * ne] = vx[i + (size_t)(2 * k) * nx];
+    for (int k = 0; k < no; ++k)
+      for (int i = 0; i < no; ++i) Vo[i + (size_t)k * no] = vx[i + (size_t)(2 * k + 1) * nx];
+    double* Vy = Vo + (size_t)no * no;
+    double* lx = Vy + (size_t)ny * ny;
+    host_spectral_basis(ny, h, Vy, lx + nx);
+    for (int r = 0; r < ne; ++r) lx[r] = lxf[2 * r];
+    for (int r = 0; r < no; ++r) lx[ne + r] = lxf[2 * r + 1];
+    CK(cudaMemcpy(B.Ve, hb.data(), sizeof(double) * nb, cudaMemcpyHostToDevice));
     ctx->xs_nx = nx;
     ctx->xs_ny = ny;
   }
@@ -1806,16 +1821,27 @@ int xs_setup(msgpu_context* ctx, int nx, int ny, XsBufs& B, cudaStream_t st) {
 int xs_metric(msgpu_context* ctx, const XsBufs& B, int nx, int ny, double sigma, double* g, cudaStream_t st) {
   const double one = 1.0, zero = 0.0;
   const double tau = 0.5 * (sigma * sigma);
-  // column-major view: G is nx x ny (x fastest)
-  if (cublasDgemm(ctx->blas, CUBLAS_OP_T, CUBLAS_OP_N, nx, ny, nx, &one, B.Vx, nx, g, nx, &zero, B.t1, nx) ||
-      cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, nx, ny, ny, &one, B.t1, nx, B.Vy, ny, &zero, B.t2, nx))
-    return fail(ctx, MSGPU_ERR_CUDA, "cublasDgemm failed");
+  const int ne = (nx + 1) / 2, no = nx / 2;
   const int N = nx * ny;
-  k_spectral_scale<<<std::min(2048, (N + 255) / 256), 256, 0, st>>>(B.t2, B.lx, B.ly, tau, nx, ny);
-  if (cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, nx, ny, nx, &one, B.Vx, nx, B.t2, nx, &zero, B.t1, nx) ||
-      cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_T, nx, ny, ny, &one, B.t1, nx, B.Vy, ny, &zero, g, nx))
+  const int gb = std::min(2048, (N + 255) / 256);
+  // column-major view: G is nx x ny (x fastest).  Analysis along x on the
+  // parity-folded columns (even and odd modes), along y with Vy; scaling;
+  // synthesis along y, then along x and unfolded.
+  k_xfold<<<gb, 256, 0, st>>>(g, B.t1, nx, ny);
+  if (cublasDgemm(ctx->blas, CUBLAS_OP_T, CUBLAS_OP_N, ne, ny, ne, &one, B.Ve, ne, B.t1, nx, &zero, B.t2, nx) ||
+      cublasDgemm(ctx->blas, CUBLAS_OP_T, CUBLAS_OP_N, no, ny, no, &one, B.Vo, no, B.t1 + ne, nx, &zero, B.t2 + ne,
+                  nx) ||
+      cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, nx, ny, ny, &one, B.t2, nx, B.Vy, ny, &zero, B.t1, nx))
     return fail(ctx, MSGPU_ERR_CUDA, "cublasDgemm failed");
-  ctx->stats.kernel_launches += 5;
+  k_spectral_scale<<<gb, 256, 0, st>>>(B.t1, B.lx, B.ly, tau, nx, ny);
+  if (cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_T, nx, ny, ny, &one, B.t1, nx, B.Vy, ny, &zero, B.t2, nx) ||
+      cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, ne, ny, ne, &one, B.Ve, ne, B.t2, nx, &zero, B.t1, nx) ||
+      cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, no, ny, no, &one, B.Vo, no, B.t2 + ne, nx, &zero, B.t1 + ne,
+                  nx))
+    return fail(ctx, MSGPU_ERR_CUDA, "cublasDgemm failed");
+  k_xunfold<<<gb, 256, 0, st>>>(B.t1, g, nx, ny);
+  CK(cudaGetLastError());
+  ctx->stats.kernel_launches += 9;
   return MSGPU_OK;
 }
 
@@ -2909,7 +2935,7 @@ int net_bwd_weights(msgpu_net* net, int i, const View& in, const View& dy, int B
 }
 
 int net_up(msgpu_net* net, const View& src, const View& dst, int C, int B, cudaStream_t st) {
-  const size_t total = (size_t)B * dst.n * dst.n * C;
+  const size_t total = (size_t)B * dst.n * dst.n * (C / 8);
   msg::unet::k_up<<<(unsigned)std::min<size_t>(4096, (total + 255) / 256), 256, 0, st>>>(
       src.p, src.img, src.n, src.cs, dst.p, dst.img, dst.cs, C, B);
   NCK(cudaGetLastError());
@@ -2918,7 +2944,7 @@ int net_up(msgpu_net* net, const View& src, const View& dst, int C, int B, cudaS
 }
 
 int net_up_back(msgpu_net* net, const View& df, const View& dc, const View& mask, int C, int B, cudaStream_t st) {
-  const size_t total = (size_t)B * dc.n * dc.n * C;
+  const size_t total = (size_t)B * dc.n * dc.n * (C / 8);
   msg::unet::k_up_back<<<(unsigned)std::min<size_t>(4096, (total + 255) / 256), 256, 0, st>>>(
       df.p, df.img, df.n, df.cs, dc.p, dc.img, dc.cs, mask.p, mask.img, mask.cs, C, B);
   NCK(cudaGetLastError());

@@ -267,6 +267,41 @@ __global__ void k_divide(double* a, double s, int n) {
 __global__ void k_mul(const double* a, double s, double* out, int n) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = a[i] * s;
 }
+// Parity fold of the H1 metric's x transform: the cosine modes satisfy
+// v_k(nx-1-i) = (-1)^k v_k(i), so the transform of column j splits into the
+// even modes applied to S_i = g_i + g_(nx-1-i) (S_mid = g_mid for odd nx) and
+// the odd modes applied to A_i = g_i - g_(nx-1-i): two products of half size.
+// f (nx x ny, column-major, leading dimension nx): rows 0..ne-1 = S, rows
+// ne..nx-1 = A.
+__global__ void k_xfold(const double* g, double* f, int nx, int ny) {
+  const int ne = (nx + 1) / 2, no = nx / 2;
+  const int total = nx * ny;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int j = t / nx, r = t - j * nx;
+    const double* c = g + (size_t)j * nx;
+    double v;
+    if (r < ne) v = (r < no) ? c[r] + c[nx - 1 - r] : c[r];
+    else v = c[r - ne] - c[nx - 1 - (r - ne)];
+    f[(size_t)j * nx + r] = v;
+  }
+}
+// Inverse of the fold after the synthesis products: rows 0..ne-1 hold the
+// even-mode sums E, rows ne..nx-1 the odd-mode sums O; g_i = E_i + O_i,
+// g_(nx-1-i) = E_i - O_i, g_mid = E_mid.
+__global__ void k_xunfold(const double* f, double* g, int nx, int ny) {
+  const int ne = (nx + 1) / 2, no = nx / 2;
+  const int total = nx * ny;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int j = t / nx, i = t - j * nx;
+    const double* c = f + (size_t)j * nx;
+    double v;
+    if (i < no) v = c[i] + c[ne + i];
+    else if (i >= ne) v = c[nx - 1 - i] - c[ne + (nx - 1 - i)];
+    else v = c[i];
+    g[(size_t)j * nx + i] = v;
+  }
+}
+
 // a[i] * b[i] summed per block in a fixed order (partials, then k_sum_part)
 __global__ void __launch_bounds__(256) k_dot_part(const double* a, const double* b, int n, double* part) {
   __shared__ double red[8];

@@ -387,40 +387,55 @@ __global__ void k_bgrad_reduce(const float* bpart, int chunks, int cout, int cou
   grad[co] = s;
 }
 
-// bilinear prolongation of node grids m -> 2m-1, C channels (one thread per node and channel)
+// bilinear prolongation of node grids m -> 2m-1, C channels (C, channel
+// strides and view offsets multiples of 8): one thread per node and group of
+// 8 channels, 16-byte loads and stores
 __global__ void k_up(const bf16* src, size_t src_img, int m, int src_cs, bf16* dst, size_t dst_img, int dst_cs,
                      int C, int images) {
-  const int n = 2 * m - 1;
-  const size_t total = (size_t)images * n * n * C;
+  const int n = 2 * m - 1, G = C / 8;
+  const size_t total = (size_t)images * n * n * G;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-    const int c = (int)(i % C);
-    const size_t node = i / C;
+    const int c = (int)(i % G) * 8;
+    const size_t node = i / G;
     const int img = (int)(node / ((size_t)n * n));
     const int q = (int)(node - (size_t)img * n * n);
     const int y = q / n, x = q - y * n;
     const bf16* s = src + (size_t)img * src_img + c;
     const int y0 = y >> 1, x0 = x >> 1, y1 = y0 + (y & 1), x1 = x0 + (x & 1);
-    float v = __bfloat162float(s[((size_t)y0 * m + x0) * src_cs]);
-    v += __bfloat162float(s[((size_t)y0 * m + x1) * src_cs]);
-    v += __bfloat162float(s[((size_t)y1 * m + x0) * src_cs]);
-    v += __bfloat162float(s[((size_t)y1 * m + x1) * src_cs]);
-    dst[(size_t)img * dst_img + (size_t)q * dst_cs + c] = __float2bfloat16(0.25f * v);
+    uint4 u[4];
+    u[0] = *reinterpret_cast<const uint4*>(s + ((size_t)y0 * m + x0) * src_cs);
+    u[1] = *reinterpret_cast<const uint4*>(s + ((size_t)y0 * m + x1) * src_cs);
+    u[2] = *reinterpret_cast<const uint4*>(s + ((size_t)y1 * m + x0) * src_cs);
+    u[3] = *reinterpret_cast<const uint4*>(s + ((size_t)y1 * m + x1) * src_cs);
+    __align__(16) bf16 o[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      float v = __bfloat162float(reinterpret_cast<const bf16*>(&u[0])[e]);
+      v += __bfloat162float(reinterpret_cast<const bf16*>(&u[1])[e]);
+      v += __bfloat162float(reinterpret_cast<const bf16*>(&u[2])[e]);
+      v += __bfloat162float(reinterpret_cast<const bf16*>(&u[3])[e]);
+      o[e] = __float2bfloat16(0.25f * v);
+    }
+    *reinterpret_cast<uint4*>(dst + (size_t)img * dst_img + (size_t)q * dst_cs + c) =
+        *reinterpret_cast<const uint4*>(o);
   }
 }
 
-// adjoint of k_up, times the ReLU mask of the coarse activation
+// adjoint of k_up, times the ReLU mask of the coarse activation (8 channels per thread)
 __global__ void k_up_back(const bf16* df, size_t df_img, int n, int df_cs, bf16* dc, size_t dc_img, int dc_cs,
                           const bf16* mask, size_t mask_img, int mask_cs, int C, int images) {
-  const int m = (n + 1) / 2;
-  const size_t total = (size_t)images * m * m * C;
+  const int m = (n + 1) / 2, G = C / 8;
+  const size_t total = (size_t)images * m * m * G;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-    const int c = (int)(i % C);
-    const size_t node = i / C;
+    const int c = (int)(i % G) * 8;
+    const size_t node = i / G;
     const int img = (int)(node / ((size_t)m * m));
     const int q = (int)(node - (size_t)img * m * m);
     const int cy = q / m, cx = q - cy * m;
     const bf16* f = df + (size_t)img * df_img + c;
-    float v = 0.f;
+    float v[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) v[e] = 0.f;
 #pragma unroll
     for (int a = -1; a <= 1; ++a)
 #pragma unroll
@@ -428,11 +443,16 @@ __global__ void k_up_back(const bf16* df, size_t df_img, int n, int df_cs, bf16*
         const int y = 2 * cy + a, x = 2 * cx + b;
         if (y < 0 || y >= n || x < 0 || x >= n) continue;
         const float w = (a == 0 ? 1.f : 0.5f) * (b == 0 ? 1.f : 0.5f);
-        v += w * __bfloat162float(f[((size_t)y * n + x) * df_cs]);
+        const uint4 u = *reinterpret_cast<const uint4*>(f + ((size_t)y * n + x) * df_cs);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) v[e] += w * __bfloat162float(reinterpret_cast<const bf16*>(&u)[e]);
       }
-    const size_t mi = (size_t)img * mask_img + (size_t)q * mask_cs + c;
-    if (!(__bfloat162float(mask[mi]) > 0.f)) v = 0.f;
-    dc[(size_t)img * dc_img + (size_t)q * dc_cs + c] = __float2bfloat16(v);
+    const uint4 mu = *reinterpret_cast<const uint4*>(mask + (size_t)img * mask_img + (size_t)q * mask_cs + c);
+    __align__(16) bf16 o[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e)
+      o[e] = __float2bfloat16(__bfloat162float(reinterpret_cast<const bf16*>(&mu)[e]) > 0.f ? v[e] : 0.f);
+    *reinterpret_cast<uint4*>(dc + (size_t)img * dc_img + (size_t)q * dc_cs + c) = *reinterpret_cast<const uint4*>(o);
   }
 }
 
