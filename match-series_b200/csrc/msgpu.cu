@@ -2853,8 +2853,44 @@ int net_buffers(msgpu_net* net, int batch) {
   return MSGPU_OK;
 }
 
+template <int BN, int CIN>
+void net_launch_halo(const msg::unet::ConvArgs& a, int images, int rows, cudaStream_t st) {
+  namespace u = msg::unet;
+  const int tiles = ((a.out_n + u::kHaloY - 1) / u::kHaloY) * ((a.out_n + u::kHaloX - 1) / u::kHaloX);
+  const dim3 grid((unsigned)(images * tiles), (unsigned)(rows / BN));
+  u::k_conv_halo<BN, CIN><<<grid, u::kThreads, u::conv_halo_smem_bytes<BN, CIN>(), st>>>(a);
+}
+
+// shared-memory limits of the halo kernels (above the 48 KB default for the widest)
+int net_kernel_attrs(msgpu_context* ctx) {
+  namespace u = msg::unet;
+  CK(cudaFuncSetAttribute(u::k_conv_halo<64, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)u::conv_halo_smem_bytes<64, 32>()));
+  CK(cudaFuncSetAttribute(u::k_conv_halo<64, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)u::conv_halo_smem_bytes<64, 16>()));
+  CK(cudaFuncSetAttribute(u::k_conv_halo<32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)u::conv_halo_smem_bytes<32, 32>()));
+  return MSGPU_OK;
+}
+
 int net_conv_launch(msgpu_net* net, const msg::unet::ConvArgs& a, int rows, cudaStream_t st) {
   const int bn = tile_of(rows);
+  if (a.stride == 1 && (a.cin == 16 || a.cin == 32)) {
+    // narrow stride-1 layers: every input node fetched once through a halo tile
+    const int images = a.total / (a.out_n * a.out_n);
+    if (a.cin == 16) {
+      if (bn == 64) net_launch_halo<64, 16>(a, images, rows, st);
+      else if (bn == 32) net_launch_halo<32, 16>(a, images, rows, st);
+      else net_launch_halo<16, 16>(a, images, rows, st);
+    } else {
+      if (bn == 64) net_launch_halo<64, 32>(a, images, rows, st);
+      else if (bn == 32) net_launch_halo<32, 32>(a, images, rows, st);
+      else net_launch_halo<16, 32>(a, images, rows, st);
+    }
+    NCK(cudaGetLastError());
+    ++net->ctx->stats.kernel_launches;
+    return MSGPU_OK;
+  }
   namespace u = msg::unet;
   const dim3 grid((unsigned)((a.total + u::kConvBM - 1) / u::kConvBM), (unsigned)(rows / bn));
   if (bn == 64) u::k_conv<64><<<grid, u::kThreads, u::conv_smem_bytes<64>(), st>>>(a);
@@ -3195,6 +3231,7 @@ int msgpu_net_create(msgpu_context* ctx, int input_level, unsigned long long see
                 input_level);
   int rc;
   if ((rc = bind_device(ctx))) return rc;
+  if ((rc = net_kernel_attrs(ctx))) return rc;
   msgpu_net* net = new msgpu_net();
   net->ctx = ctx;
   net->level = input_level;

@@ -244,6 +244,124 @@ constexpr size_t conv_smem_bytes() {
   return sizeof(bf16) * kStages * (kConvBM + BN) * kSA;
 }
 
+// Stride-1 convolution (forward, or the data gradient with transposed
+// weights) of CIN = 16 or 32 input channels from a halo tile: a block
+// computes 8 x 16 output nodes of one image (each warp two rows of 16, one
+// m16 tile per row) x BN channels.  The (8+2) x (16+2) input nodes and all 9
+// taps' weights are staged once in shared memory; every tap's A fragment is
+// read by ldmatrix straight from the halo rows (consecutive nodes of a row,
+// conflict-free), so each input node is fetched once instead of once per
+// tap.  The mma sequence over (tap, channel) is the one k_conv issues, so
+// both give the same results.
+constexpr int kHaloY = 8, kHaloX = 16;
+template <int CIN>
+__host__ __device__ constexpr int halo_stride() { return CIN + 8; }
+template <int BN, int CIN>
+constexpr size_t conv_halo_smem_bytes() {
+  return sizeof(bf16) * ((size_t)(kHaloY + 2) * (kHaloX + 2) * halo_stride<CIN>() + (size_t)9 * BN * halo_stride<CIN>());
+}
+
+template <int BN, int CIN>
+__global__ void __launch_bounds__(kThreads) k_conv_halo(ConvArgs a) {
+  constexpr int HS = halo_stride<CIN>();
+  constexpr int HW = kHaloX + 2, HH = kHaloY + 2;
+  extern __shared__ __align__(16) unsigned char halo_smem[];
+  bf16* H = reinterpret_cast<bf16*>(halo_smem);   // [HH][HW][HS]
+  bf16* W = H + (size_t)HH * HW * HS;             // [9][BN][HS]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tiles_x = (a.out_n + kHaloX - 1) / kHaloX, tiles_y = (a.out_n + kHaloY - 1) / kHaloY;
+  const int img = blockIdx.x / (tiles_x * tiles_y);
+  const int trest = blockIdx.x - img * tiles_x * tiles_y;
+  const int ty0 = (trest / tiles_x) * kHaloY, tx0 = (trest % tiles_x) * kHaloX;
+  const int n0 = blockIdx.y * BN;
+  const int sgn = a.mode == 0 ? 1 : -1;   // mode 0 reads q + d, mode 1 reads q - d
+  const bf16* in = a.in + (size_t)img * a.in_img;
+  // halo nodes (ty0 - 1 .. ty0 + 8, tx0 - 1 .. tx0 + 16), CIN / 8 vectors each, zero outside the grid
+  for (int idx = tid; idx < HH * HW * (CIN / 8); idx += kThreads) {
+    const int v = idx % (CIN / 8), node = idx / (CIN / 8);
+    const int hy = node / HW, hx = node - hy * HW;
+    const int y = ty0 - 1 + hy, x = tx0 - 1 + hx;
+    const bool ok = y >= 0 && y < a.in_n && x >= 0 && x < a.in_n;
+    cp_async16(H + (size_t)node * HS + 8 * v, ok ? in + ((size_t)y * a.in_n + x) * a.in_cs + 8 * v : a.in,
+               ok ? 16 : 0);
+  }
+  for (int idx = tid; idx < 9 * BN * (CIN / 8); idx += kThreads) {
+    const int v = idx % (CIN / 8), r = idx / (CIN / 8);
+    const int tap = r / BN, co = r - tap * BN;
+    cp_async16(W + (size_t)r * HS + 8 * v, a.w + (size_t)(n0 + co) * 9 * CIN + tap * CIN + 8 * v, 16);
+  }
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  float acc[2][BN / 8][4];
+#pragma unroll
+  for (int m = 0; m < 2; ++m)
+#pragma unroll
+    for (int j = 0; j < BN / 8; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[m][j][e] = 0.f;
+  const int a_x = lane & 15, a_col = 8 * (lane >> 4);
+  const int b_row = (lane & 7) + 8 * (lane >> 4), b_col = 8 * ((lane >> 3) & 1);
+#pragma unroll 1
+  for (int tap = 0; tap < 9; ++tap) {
+    const int dy = sgn * (tap / 3 - 1), dx = sgn * (tap % 3 - 1);
+#pragma unroll
+    for (int kk = 0; kk < CIN; kk += 16) {
+      uint32_t af[2][4];
+#pragma unroll
+      for (int m = 0; m < 2; ++m) {
+        const int hy = 2 * warp + m + 1 + dy, hx = a_x + 1 + dx;
+        ldsm_x4(af[m], H + ((size_t)hy * HW + hx) * HS + kk + a_col);
+      }
+#pragma unroll
+      for (int j = 0; j < BN / 8; j += 2) {
+        uint32_t bf[4];
+        ldsm_x4(bf, W + ((size_t)tap * BN + j * 8 + b_row) * HS + kk + b_col);
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+          mma_bf16(acc[m][j], af[m], bf[0], bf[1]);
+          mma_bf16(acc[m][j + 1], af[m], bf[2], bf[3]);
+        }
+      }
+    }
+  }
+  const int outN2 = a.out_n * a.out_n;
+  (void)outN2;
+#pragma unroll
+  for (int m = 0; m < 2; ++m)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int oy = ty0 + 2 * warp + m, ox = tx0 + (lane >> 2) + 8 * h;
+      if (oy >= a.out_n || ox >= a.out_n) continue;
+      const int q = oy * a.out_n + ox;
+      const size_t ob = (size_t)img * a.out_img + (size_t)q * a.out_cs;
+      const bf16* mk = a.mask ? a.mask + (size_t)img * a.mask_img + (size_t)q * a.mask_cs : nullptr;
+#pragma unroll
+      for (int j = 0; j < BN / 8; ++j) {
+        const int co = n0 + j * 8 + 2 * (lane & 3);
+        float v[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          v[e] = acc[m][j][2 * h + e];
+          if (co + e >= a.cout) continue;
+          if (a.bias) v[e] += a.bias[co + e];
+          if (a.accumulate) v[e] += __bfloat162float(static_cast<const bf16*>(a.out)[ob + co + e]);
+          if (a.relu) v[e] = fmaxf(v[e], 0.f);
+          if (mk && !(__bfloat162float(mk[co + e]) > 0.f)) v[e] = 0.f;
+        }
+        if (a.out_f32) {
+          float* o = static_cast<float*>(a.out) + ob;
+          if (co < a.cout) o[co] = v[0];
+          if (co + 1 < a.cout) o[co + 1] = v[1];
+        } else if (co + 1 < a.cout) {
+          *reinterpret_cast<__nv_bfloat162*>(static_cast<bf16*>(a.out) + ob + co) = __floats2bfloat162_rn(v[0], v[1]);
+        } else if (co < a.cout) {
+          static_cast<bf16*>(a.out)[ob + co] = __float2bfloat16(v[0]);
+        }
+      }
+    }
+}
+
 struct WgradArgs {
   const bf16* in;        // forward input view
   size_t in_img;
