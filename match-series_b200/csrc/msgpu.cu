@@ -1774,7 +1774,8 @@ void host_spectral_basis(int n, double h, double* V, double* lam) {
 struct XsBufs {
   double *Ve, *Vo, *Vy, *lx, *ly;      // spectral basis: even and odd x modes on half the rows, y modes;
                                        // lx in the folded order (even modes, then odd modes)
-  double *d, *og, *od, *de, *tx, *kphi, *t1, *t2, *part, *scal;
+  double *d, *og, *od, *de, *tx, *kphi, *t1, *t2, *nr, *part, *scal;
+  unsigned* done;                      // line and regulariser counters of the fused totals
 };
 
 int xs_setup(msgpu_context* ctx, int nx, int ny, XsBufs& B, cudaStream_t st) {
@@ -1811,10 +1812,12 @@ int xs_setup(msgpu_context* ctx, int nx, int ny, XsBufs& B, cudaStream_t st) {
     ctx->xs_ny = ny;
   }
   const size_t N = (size_t)nx * ny;
-  if ((rc = ensure(ctx, ctx->xs_work, sizeof(double) * (9 * N + 4096)))) return rc;
+  if ((rc = ensure(ctx, ctx->xs_work, sizeof(double) * (10 * N + 4096)))) return rc;
   double* w = (double*)ctx->xs_work.p;
   B.d = w; B.og = w + N; B.od = w + 2 * N; B.de = w + 3 * N; B.tx = w + 4 * N; B.kphi = w + 5 * N;
-  B.t1 = w + 6 * N; B.t2 = w + 7 * N; B.part = w + 8 * N; B.scal = B.part + 2048;
+  B.t1 = w + 6 * N; B.t2 = w + 7 * N; B.nr = w + 8 * N; B.part = w + 9 * N; B.scal = B.part + 2048;
+  B.done = (unsigned*)(B.scal + 64);
+  CK(cudaMemsetAsync(B.done, 0, 2 * sizeof(unsigned), st));
   return MSGPU_OK;
 }
 
@@ -1871,15 +1874,15 @@ struct XsSolver {
   // data term and regulariser at p: energies into B.scal[1..2], derivative (if de) into de
   int parts(const double* p, double* de) {
     LineArgs a;
+    memset(&a, 0, sizeof(a));
     a.nx = nx; a.ny = ny; a.img_stride = (size_t)N; a.R = R; a.T = T; a.phi = p;
     a.e_line = (double*)ctx->nccbuf.p; a.de = de; a.t = lt;
+    a.nr_pre = B.nr; a.done = B.done; a.e_total = B.scal + 1;
     const size_t smem = sizeof(double) * 3 * (size_t)nx;
     k_lineshift<<<dim3(ny, 1), kLineThreads, smem, st>>>(a);
-    k_lineshift_total<<<1, 256, 0, st>>>(a.e_line, ny, B.scal + 1);
     const int nb = std::min(1024, (N + 255) / 256);
-    k_xshift_reg<<<dim3(nb, 1), 256, 0, st>>>(rt, nx, ny, (size_t)N, p, B.kphi, B.part);
-    k_xshift_reg_total<<<1, 256, 0, st>>>(B.part, nb, B.scal + 2);
-    ctx->stats.kernel_launches += 4;
+    k_xshift_reg<<<dim3(nb, 1), 256, 0, st>>>(rt, nx, ny, (size_t)N, p, B.kphi, B.part, B.done + 1, B.scal + 2);
+    ctx->stats.kernel_launches += 2;
     CK(cudaGetLastError());
     return MSGPU_OK;
   }
@@ -1959,8 +1962,13 @@ int run_xshift(msgpu_context* ctx, int nx, int ny, const double* R, const double
   S.rt = host_xreg_tables(nx, ny, yreg);
   CK(cudaFuncSetAttribute(k_lineshift, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)(sizeof(double) * 3 * (size_t)nx)));
+  CK(cudaFuncSetAttribute(k_lineshift_prep_ref, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)(sizeof(double) * 3 * (size_t)nx)));
   const int N = S.N, g1 = S.grid1();
   const XsBufs& B = S.B;
+  // the reference lines normalised once for the whole descent
+  k_lineshift_prep_ref<<<dim3(ny, 1), kLineThreads, sizeof(double) * 3 * (size_t)nx, st>>>(R, nx, (size_t)N, S.lt,
+                                                                                         B.nr);
   CK(cudaMemsetAsync(B.og, 0, sizeof(double) * N, st));
   CK(cudaMemsetAsync(B.od, 0, sizeof(double) * N, st));
   const double scale = (double)nx / (double)(nx > ny ? nx : ny);
@@ -2117,6 +2125,7 @@ int msgpu_lineshift_energy_device(msgpu_context* ctx, int nx, int ny, int num_im
   if ((rc = ensure(ctx, ctx->nccbuf, sizeof(double) * (size_t)ny * num_images + 64))) return rc;
   cudaStream_t st = (cudaStream_t)stream;
   LineArgs a;
+  memset(&a, 0, sizeof(a));
   a.nx = nx;
   a.ny = ny;
   a.img_stride = (size_t)nx * ny;
@@ -2169,7 +2178,7 @@ int msgpu_xshift_reg_device(msgpu_context* ctx, int nx, int ny, int num_images, 
   if ((rc = ensure(ctx, ctx->vals, sizeof(double) * (size_t)nb * num_images + 64))) return rc;
   cudaStream_t st = (cudaStream_t)stream;
   k_xshift_reg<<<dim3(nb, num_images), 256, 0, st>>>(host_xreg_tables(nx, ny, yreg), nx, ny, (size_t)N, d_phix,
-                                                     d_kphi_out, (double*)ctx->vals.p);
+                                                     d_kphi_out, (double*)ctx->vals.p, nullptr, nullptr);
   k_xshift_reg_total<<<num_images, 256, 0, st>>>((const double*)ctx->vals.p, nb, d_energy_out);
   CK(cudaGetLastError());
   ctx->stats.kernel_launches = 2;

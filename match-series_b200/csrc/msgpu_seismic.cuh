@@ -38,6 +38,9 @@ struct LineArgs {
   double* e_line;              // ny per image
   double* de;                  // nullable: nx*ny per image
   LineTables t;
+  const double* nr_pre;        // nullable: the reference lines already normalised (k_lineshift_prep_ref)
+  unsigned* done;              // nullable: per-image line counter; the last line's CTA writes the total
+  double* e_total;             // one per image (with done): mean of the line energies in line order
 };
 
 __device__ __forceinline__ double line_block_sum(double v, double* red) {
@@ -86,6 +89,56 @@ __device__ double line_normalize(const LineTables& t, double* v, double* tmp, in
   return var;
 }
 
+// With a.done: the CTA of the image's last finished line adds the line
+// energies in line order (no CTA waits for another: a counter decides who
+// is last) and resets the counter for the next launch.
+// buf: the CTA's line buffer (cap doubles), free again at this point.
+__device__ __forceinline__ void line_total(const LineArgs& a, double* buf, int cap) {
+  if (!a.done) return;
+  __shared__ int last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(a.done + blockIdx.y, 1u) == (unsigned)a.ny - 1) ? 1 : 0;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const double* e = a.e_line + (size_t)blockIdx.y * a.ny;
+  double s = 0.;
+  for (int y0 = 0; y0 < a.ny; y0 += cap) {
+    const int m = min(cap, a.ny - y0);
+    for (int i = threadIdx.x; i < m; i += kLineThreads) buf[i] = __ldcg(e + y0 + i);
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int i = 0; i < m; ++i) s += buf[i];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    a.e_total[blockIdx.y] = s / a.ny;
+    a.done[blockIdx.y] = 0u;
+  }
+}
+
+// The reference lines normalised once (normalizeImageForNCC of
+// registration.h:2137-2193 on each line; R does not change during a
+// descent), for k_lineshift's nr_pre.
+__global__ void __launch_bounds__(kLineThreads) k_lineshift_prep_ref(const double* R, int nx, size_t img_stride,
+                                                                    LineTables t, double* nr_out) {
+  extern __shared__ double lsm[];
+  __shared__ double red[kLineThreads / 32];
+  const int n = nx;
+  const size_t base = (size_t)blockIdx.y * img_stride + (size_t)blockIdx.x * n;
+  double* nr = lsm;
+  double* tmp = lsm + n;
+  if (isnan(R[base])) {
+    for (int i = threadIdx.x; i < n; i += kLineThreads) nr_out[base + i] = R[base + i];
+    return;
+  }
+  for (int i = threadIdx.x; i < n; i += kLineThreads) nr[i] = R[base + i];
+  __syncthreads();
+  line_normalize(t, nr, tmp, n, red);
+  for (int i = threadIdx.x; i < n; i += kLineThreads) nr_out[base + i] = nr[i];
+}
+
 __global__ void __launch_bounds__(kLineThreads) k_lineshift(LineArgs a) {
   extern __shared__ double lsm[];
   __shared__ double red[kLineThreads / 32];
@@ -102,10 +155,11 @@ __global__ void __launch_bounds__(kLineThreads) k_lineshift(LineArgs a) {
     if (threadIdx.x == 0) a.e_line[(size_t)blockIdx.y * a.ny + y] = 0.0;
     if (a.de)
       for (int i = threadIdx.x; i < n; i += kLineThreads) a.de[base + i] = 0.0;
+    line_total(a, lsm, 3 * n);
     return;
   }
   for (int i = threadIdx.x; i < n; i += kLineThreads) {
-    nr[i] = R[i];
+    nr[i] = a.nr_pre ? a.nr_pre[base + i] : R[i];
     // doFastDeformImage<., QC_1D> (deformations.h:111-137), Vector::interpolate (vec.h:461-472)
     double ds = i + phi[i] / t.h;
     ds = ds < 0. ? 0. : (ds > (double)(n - 1) ? (double)(n - 1) : ds);
@@ -114,13 +168,16 @@ __global__ void __launch_bounds__(kLineThreads) k_lineshift(LineArgs a) {
     nt[i] = (p == n - 1) ? T[p] : (1 - pf) * T[p] + pf * T[p + 1];
   }
   __syncthreads();
-  line_normalize(t, nr, tmp, n, red);
+  if (!a.nr_pre) line_normalize(t, nr, tmp, n, red);
   const double var = line_normalize(t, nt, tmp, n, red);
   double part = 0.0;
   for (int i = threadIdx.x; i < n; i += kLineThreads) part += line_mass_row(t, nt, i, n) * nr[i];
   const double energy = -line_block_sum(part, red);
   if (threadIdx.x == 0) a.e_line[(size_t)blockIdx.y * a.ny + y] = energy;
-  if (!a.de) return;
+  if (!a.de) {
+    line_total(a, lsm, 3 * n);
+    return;
+  }
   // VariationOfNormalizedCrossCorrelationEnergy: temp = (normR + normT * E) / var
   for (int i = threadIdx.x; i < n; i += kLineThreads) {
     double v = nr[i];
@@ -167,6 +224,7 @@ __global__ void __launch_bounds__(kLineThreads) k_lineshift(LineArgs a) {
     d /= a.ny;
     a.de[base + i] = d;
   }
+  line_total(a, lsm, 3 * n);
 }
 
 // Sum of the line energies in line order, divided by the line count: one
@@ -210,8 +268,12 @@ struct XRegTables {
   double st[9][3][3];
 };
 
+// With done (one counter per image): the CTA that finishes an image's last
+// block sums its partials like k_xshift_reg_total (E = 1/2 phi.K phi into
+// e_total) and resets the counter.
 __global__ void __launch_bounds__(256) k_xshift_reg(XRegTables tb, int nx, int ny, size_t img_stride,
-                                                    const double* phi, double* kphi, double* part) {
+                                                    const double* phi, double* kphi, double* part,
+                                                    unsigned* done, double* e_total) {
   __shared__ double red[8];
   const double* p = phi + (size_t)blockIdx.y * img_stride;
   double* k = kphi + (size_t)blockIdx.y * img_stride;
@@ -239,6 +301,28 @@ __global__ void __launch_bounds__(256) k_xshift_reg(XRegTables tb, int nx, int n
     double s = 0.0;
     for (int w = 0; w < 8; ++w) s += red[w];
     part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
+  }
+  if (!done) return;
+  __shared__ int last;
+  __shared__ double red2[8];
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(done + blockIdx.y, 1u) == gridDim.x - 1) ? 1 : 0;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const double* pp = part + (size_t)blockIdx.y * gridDim.x;
+  double v = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += 256) v += __ldcg(pp + i);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red2[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 8; ++w) t += red2[w];
+    e_total[blockIdx.y] = 0.5 * t;
+    done[blockIdx.y] = 0u;
   }
 }
 
