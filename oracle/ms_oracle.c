@@ -1497,6 +1497,110 @@ double msor_xshift_reg(int nx, int ny, double yreg, const double* phi, double* k
   return 0.5 * dot(kphi, phi, nx * ny);
 }
 
+/* The regulariser of findXShift for laplaceWeight > 0 (matchSeries.h:828-838):
+ * K = w L M^{-1} L + stiffX + yRegFactor stiffY with L the assembled Q1
+ * stiffness (StiffOp) and M the lumped mass (LumpedMassOp, inverted), the
+ * product formed as qc::assembleLaplaceSquareRegMatrix does
+ * (hyperelastic.h:234-251: rows of L scaled by M^{-1}, then
+ * aol::Matrix::addMatrixProduct, matrix.cpp:414-429, which adds
+ * L[i][k] * (M^{-1}L)[k][j] into entry (i, j) for k in increasing column
+ * order of row i -- aol::SparseRow keeps its entries sorted), scaled by w,
+ * then stiffX and yRegFactor * stiffY added element by element; applied as
+ * the column-sorted CSR_Matrix (sparseMatrices.h CSRMatrix::apply: a
+ * row's sum from 0 in column order).  25-point rows (offsets -2..2).
+ * Returns E = 1/2 phi.(K phi), K phi out.                                  */
+double msor_xshift_reg_laplace(int nx, int ny, double yreg, double w, const double* phi, double* kphi) {
+  const int N = nx * ny;
+  const double h = 1. / (double)((nx > ny ? nx : ny) - 1), vol = sqr(h);
+  quad_t Q;
+  quad_init(&Q, h);
+  /* L: rect_system's stiffness pass alone (StiffOp = FELinScalarWeightedStiffInterface, coefficient 1) */
+  double Ls[4][4];
+  for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) Ls[i][j] = 0.;
+  for (int q = 0; q < 4; ++q)
+    for (int i = 0; i < 4; ++i)
+      for (int j = i; j < 4; ++j) {
+        double d = 0;
+        d += Q.gq[i][q][0] * Q.gq[j][q][0];
+        d += Q.gq[i][q][1] * Q.gq[j][q][1];
+        Ls[i][j] += d * 1. * Q.w;
+      }
+  for (int i = 0; i < 4; ++i)
+    for (int j = i; j < 4; ++j) Ls[j][i] = Ls[i][j] = Ls[i][j] * vol;
+  double* L = (double*)calloc((size_t)N * 9, sizeof(double));
+  double* lm = (double*)calloc((size_t)N, sizeof(double));
+  double lmloc[4] = {0., 0., 0., 0.};
+  for (int q = 0; q < 4; ++q)
+    for (int i = 0; i < 4; ++i) lmloc[i] += 1. * Q.bq[i][q] * Q.w;
+  for (int i = 0; i < 4; ++i) lmloc[i] *= vol;
+  for (int ey = 0; ey < ny - 1; ++ey)
+    for (int ex = 0; ex < nx - 1; ++ex)
+      for (int i = 0; i < 4; ++i) {
+        const int gi = ex + ey * nx + ((i & 1) ? 1 : 0) + ((i & 2) ? nx : 0);
+        lm[gi] += lmloc[i];
+        for (int j = 0; j < 4; ++j) {
+          const int gj = ex + ey * nx + ((j & 1) ? 1 : 0) + ((j & 2) ? nx : 0);
+          const int dx = (gj % nx) - (gi % nx), dy = (gj / nx) - (gi / nx);
+          L[(size_t)gi * 9 + (dy + 1) * 3 + (dx + 1)] += Ls[i][j];
+        }
+      }
+  /* K = w (L M^{-1} L) as 25-point rows, accumulated in increasing k */
+  double* K = (double*)calloc((size_t)N * 25, sizeof(double));
+  for (int r = 0; r < N; ++r) {
+    const int x = r % nx, y = r / nx;
+    double* kr = K + (size_t)r * 25;
+    for (int a = -1; a <= 1; ++a)
+      for (int b = -1; b <= 1; ++b) {
+        const int X = x + b, Y = y + a;
+        if (X < 0 || X >= nx || Y < 0 || Y >= ny) continue;
+        const int k = X + Y * nx;
+        const double lik = L[(size_t)r * 9 + (a + 1) * 3 + (b + 1)];
+        const double minv = 1. / lm[k];
+        for (int c = -1; c <= 1; ++c)
+          for (int d = -1; d <= 1; ++d) {
+            const int X2 = X + d, Y2 = Y + c;
+            if (X2 < 0 || X2 >= nx || Y2 < 0 || Y2 >= ny) continue;
+            const double m2 = L[(size_t)k * 9 + (c + 1) * 3 + (d + 1)] * minv;
+            kr[(a + c + 2) * 5 + (b + d + 2)] += lik * m2;
+          }
+      }
+    for (int e = 0; e < 25; ++e) kr[e] *= w;
+  }
+  /* + stiffX + yRegFactor stiffY, element by element (FEOpMixedDerivative) */
+  for (int pass = 0; pass < 2; ++pass) {
+    const int sd = pass;
+    const double factor = pass == 0 ? 1.0 : yreg;
+    double Lm[4][4];
+    for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) Lm[i][j] = 0.;
+    for (int q = 0; q < 4; ++q)
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) Lm[i][j] += 1. * Q.gq[i][q][sd] * Q.gq[j][q][sd] * Q.w;
+    for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) Lm[i][j] *= vol;
+    for (int ey = 0; ey < ny - 1; ++ey)
+      for (int ex = 0; ex < nx - 1; ++ex)
+        for (int i = 0; i < 4; ++i)
+          for (int j = 0; j < 4; ++j) {
+            const int gi = ex + ey * nx + ((i & 1) ? 1 : 0) + ((i & 2) ? nx : 0);
+            const int gj = ex + ey * nx + ((j & 1) ? 1 : 0) + ((j & 2) ? nx : 0);
+            const int dx = (gj % nx) - (gi % nx), dy = (gj / nx) - (gi / nx);
+            K[(size_t)gi * 25 + (dy + 2) * 5 + (dx + 2)] += factor * Lm[i][j];
+          }
+  }
+  for (int r = 0; r < N; ++r) {
+    const int x = r % nx, y = r / nx;
+    double sum = 0.;
+    for (int a = -2; a <= 2; ++a)
+      for (int b = -2; b <= 2; ++b) {
+        const int X = x + b, Y = y + a;
+        if (X < 0 || X >= nx || Y < 0 || Y >= ny) continue;
+        sum += K[(size_t)r * 25 + (a + 2) * 5 + (b + 2)] * phi[X + Y * nx];
+      }
+    kphi[r] = sum;
+  }
+  free(L); free(lm); free(K);
+  return 0.5 * dot(kphi, phi, N);
+}
+
 /* --- the seismic solve: findXShift (matchSeries.h:805-865) -------------------- */
 /* Nine-point rows of an assembled Q1 operator on the nx x ny rectangular grid
  * (h = 1/(max(nx,ny)-1)): mass (FELinScalarWeightedMassInterface) with factor
@@ -1619,25 +1723,30 @@ void msor_h1_metric(int nx, int ny, double sigma, double* x) {
 typedef struct {
   int nx, ny, N;
   const double *R, *T;
-  double lambda, yreg;
+  double lambda, yreg, lapw;   /* lapw: laplaceWeight (> 0: the Laplace-square regulariser) */
   double rb_tau[2], rb_e[2];
   int rb_pos, evals;
   double e_at_pos;
   double *tx, *w;
 } xs_ctx;
 
+static double xs_reg(xs_ctx* C, const double* phi) {
+  return C->lapw > 0 ? msor_xshift_reg_laplace(C->nx, C->ny, C->yreg, C->lapw, phi, C->w)
+                     : msor_xshift_reg(C->nx, C->ny, C->yreg, phi, C->w);
+}
+
 /* E = EData + lambda * ERegStiff (LinCombOp, matchSeries.h:847-850) */
 static double xs_energy(xs_ctx* C, const double* phi) {
   double e = 0.;
   e += msor_lineshift(C->nx, C->ny, C->R, C->T, phi, NULL);
-  e += C->lambda * msor_xshift_reg(C->nx, C->ny, C->yreg, phi, C->w);
+  e += C->lambda * xs_reg(C, phi);
   return e;
 }
 
 /* DE = DEData + lambda * K phi */
 static void xs_gradient(xs_ctx* C, const double* phi, double* de) {
   msor_lineshift(C->nx, C->ny, C->R, C->T, phi, de);
-  msor_xshift_reg(C->nx, C->ny, C->yreg, phi, C->w);
+  xs_reg(C, phi);
   for (int i = 0; i < C->N; ++i) de[i] += C->lambda * C->w[i];
 }
 
@@ -1684,12 +1793,12 @@ static double xs_armijo(xs_ctx* C, const double* p, const double* d, const doubl
  * ArmijoSearch.h:118-200, as in msor_gd_level_dt, on one component); phix is
  * scaled by nx/max(nx,ny) around the descent (matchSeries.h:860-864).
  * Returns the steps; *energy_out the energy at the end.                    */
-int msor_xshift(int nx, int ny, const double* R, const double* T, double lambda, double yreg, int max_iter,
-                double* phix, double* energy_out, msor_step* trace, int trace_cap) {
+int msor_xshift(int nx, int ny, const double* R, const double* T, double lambda, double yreg, double laplace_weight,
+                int max_iter, double* phix, double* energy_out, msor_step* trace, int trace_cap) {
   const int N = nx * ny;
   xs_ctx C;
   memset(&C, 0, sizeof(C));
-  C.nx = nx; C.ny = ny; C.N = N; C.R = R; C.T = T; C.lambda = lambda; C.yreg = yreg;
+  C.nx = nx; C.ny = ny; C.N = N; C.R = R; C.T = T; C.lambda = lambda; C.yreg = yreg; C.lapw = laplace_weight;
   C.rb_tau[0] = C.rb_tau[1] = NAN;
   double* buf = (double*)calloc((size_t)N * 6, sizeof(double));
   double *d = buf, *og = buf + N, *od = buf + 2 * N, *DE = buf + 3 * N;

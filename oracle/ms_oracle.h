@@ -146,14 +146,18 @@ double msor_lineshift(int nx, int ny, const double* R, const double* T, const do
 /* findXShift's regulariser (laplaceWeight <= 0): K = stiffX + yreg * stiffY
  * on the nx x ny grid; returns 1/2 phi.K phi, K phi into kphi.             */
 double msor_xshift_reg(int nx, int ny, double yreg, const double* phi, double* kphi);
+/* findXShift's regulariser with laplaceWeight w > 0: w L M^{-1} L + stiffX + yreg stiffY */
+double msor_xshift_reg_laplace(int nx, int ny, double yreg, double w, const double* phi, double* kphi);
 /* (M + tau L) x with tau = 0.5 sigma^2 on the nx x ny rectangular grid
  * (InverseH1MetricBase's system matrix), and its exact inverse in place.   */
 void   msor_h1sys_apply(int nx, int ny, double sigma, const double* x, double* y);
 void   msor_h1_metric(int nx, int ny, double sigma, double* x);
-/* findXShift (matchSeries.h:805-865) with laplaceWeight <= 0 and the exact
- * H1 metric: phix (nx*ny) in/out; returns the steps.                      */
+/* findXShift (matchSeries.h:805-865) with the exact H1 metric; laplace_weight
+ * > 0 selects the Laplace-square regulariser: phix (nx*ny) in/out; returns
+ * the steps.                                                               */
 int    msor_xshift(int nx, int ny, const double* R, const double* T, double lambda, double yreg,
-                   int max_iter, double* phix, double* energy_out, msor_step* trace, int trace_cap);
+                   double laplace_weight, int max_iter, double* phix, double* energy_out, msor_step* trace,
+                   int trace_cap);
 /* matchSeries<>() with accumulated deformations, refinement and extra stages
  * (matchSeries.h:87-265, 353-445, 1250-1320); see ms_oracle.c.             */
 void   msor_match_series(int data_term, int level, int start, int stop, double lambda,

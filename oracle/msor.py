@@ -45,6 +45,7 @@ def lib():
         L.msor_ncc_energy.restype = ctypes.c_double
         L.msor_lineshift.restype = ctypes.c_double
         L.msor_xshift_reg.restype = ctypes.c_double
+        L.msor_xshift_reg_laplace.restype = ctypes.c_double
         L.msor_energy_dt.restype = ctypes.c_double
         L.msor_register_dt.restype = ctypes.c_double
         L.msor_gd_level_dt.restype = ctypes.c_int
@@ -201,6 +202,15 @@ def xshift_reg(phix, yreg):
     return float(e), k
 
 
+def xshift_reg_laplace(phix, yreg, w):
+    """findXShift's regulariser with laplaceWeight w > 0: (1/2 phi.K phi, K phi)."""
+    ny, nx = phix.shape
+    k = np.zeros((ny, nx))
+    e = lib().msor_xshift_reg_laplace(nx, ny, ctypes.c_double(yreg), ctypes.c_double(w), _p(_c(phix).reshape(-1)),
+                                      _p(k))
+    return float(e), k
+
+
 def h1sys_apply(x, sigma):
     """(M + 0.5 sigma^2 L) x on the grid of x (ny, nx)."""
     ny, nx = x.shape
@@ -217,7 +227,7 @@ def h1_metric(x, sigma):
     return y
 
 
-def xshift(R, T, lam, yreg, max_iter, phix=None, trace_cap=4096):
+def xshift(R, T, lam, yreg, max_iter, phix=None, trace_cap=4096, laplace_weight=0.0):
     """findXShift: returns (phix, energy, steps, trace rows (iter, energy, tau, sigma, evals))."""
     R = _c(R)
     ny, nx = R.shape
@@ -225,7 +235,8 @@ def xshift(R, T, lam, yreg, max_iter, phix=None, trace_cap=4096):
     e = ctypes.c_double()
     tr = (Step * trace_cap)()
     steps = lib().msor_xshift(nx, ny, _p(R.reshape(-1)), _p(_c(T).reshape(-1)), ctypes.c_double(lam),
-                              ctypes.c_double(yreg), max_iter, _p(ph.reshape(-1)), ctypes.byref(e), tr, trace_cap)
+                              ctypes.c_double(yreg), ctypes.c_double(laplace_weight), max_iter, _p(ph.reshape(-1)),
+                              ctypes.byref(e), tr, trace_cap)
     rows = [(tr[i].iter, tr[i].energy, tr[i].tau, tr[i].sigma, tr[i].evals) for i in range(min(steps, trace_cap))]
     return ph, e.value, steps, rows
 
@@ -346,6 +357,12 @@ class RefRunner:
         ny, nx = phix.shape
         self.run("xshiftreg", nx, ny, repr(float(yreg)), self._w("px", phix), os.path.join(self.dir, "e"),
                  os.path.join(self.dir, "k"))
+        return float(self._r("e")[0]), self._r("k").reshape(ny, nx)
+
+    def xshift_reg_laplace(self, phix, yreg, w):
+        ny, nx = phix.shape
+        self.run("xshiftlap", nx, ny, repr(float(yreg)), repr(float(w)), self._w("px", phix),
+                 os.path.join(self.dir, "e"), os.path.join(self.dir, "k"))
         return float(self._r("e")[0]), self._r("k").reshape(ny, nx)
 
     def h1sys(self, x, sigma):

@@ -15,6 +15,8 @@
 // (registration.h:677-710) and the H1 gradient flow with automatic filter
 // width (gradientDescent.h:632-709).
 #include <registration.h>
+#include <hyperelastic.h>
+#include <CSRMatrix.h>
 #include <configurators.h>
 
 #include <cstdio>
@@ -361,6 +363,7 @@ static int usage ( ) {
     "ms_ref compose L d1 d2 inout | median L F frames phis fill out\n"
     "ms_ref save nx ny in out type | load file out dims | savedef L in mask | loaddef L mask out\n"
     "ms_ref lineshift nx ny R T phix outE outDE | xshiftreg nx ny yRegFactor phix outE outKphi\n"
+    "ms_ref xshiftlap nx ny yRegFactor laplaceWeight phix outE outKphi\n"
     "ms_ref h1sys nx ny sigma x out\n"
     "ms_ref series[_ncc] maxL start stop lambda lambdaFactor maxIter stopEps sat minToZero F framesBin outPhis outMean outTxt\n"
     "ms_ref matchseries[_ncc] maxL start stop lambda lambdaFactor maxIter stopEps sat minToZero refineStart refineStop\n"
@@ -526,6 +529,31 @@ int main ( int argc, char **argv ) {
       DE.apply ( phi, de );
       writeBin ( argv[7], &e[0], 1 );
       writeBin ( argv[8], de.getData ( ), N );
+      return 0;
+    }
+    if ( cmd == "xshiftlap" && argc == 9 ) {
+      // ms_ref xshiftlap nx ny yRegFactor laplaceWeight phix outE outKphi: the regulariser of findXShift with
+      // laplaceWeight > 0 (matchSeries.h:828-838): laplaceWeight L M^-1 L + stiffX + yRegFactor stiffY as CSR
+      typedef qc::RectangularGridConfigurator<RealType, qc::QC_2D, aol::GaussQuadrature<RealType, qc::QC_2D, 3> > RectConf;
+      const int nx = atoi ( argv[2] ), ny = atoi ( argv[3] ), N = nx * ny;
+      ArrayType dummy ( nx, ny );
+      const RectConf::InitType grid ( qc::GridSize<qc::QC_2D>::createFrom ( dummy ) );
+      const aol::FEOpMixedDerivative<RectConf> stiffX ( grid, 0, 0, aol::ONTHEFLY );
+      const aol::FEOpMixedDerivative<RectConf> stiffY ( grid, 1, 1, aol::ONTHEFLY );
+      aol::SparseMatrix<RealType> tempMat ( grid );
+      qc::assembleLaplaceSquareRegMatrix<RectConf> ( grid, tempMat );
+      tempMat *= atof ( argv[5] );
+      stiffX.assembleAddMatrix ( tempMat );
+      stiffY.assembleAddMatrix ( tempMat, atof ( argv[4] ) );
+      const aol::CSR_Matrix<> K ( tempMat );
+      const aol::QuadraticFormOp<aol::Vector<RealType> > EReg ( K );
+      aol::Vector<RealType> phi ( N ), kphi ( N );
+      readBin ( argv[6], phi.getData ( ), N );
+      aol::Scalar<RealType> e;
+      EReg.apply ( phi, e );
+      K.apply ( phi, kphi );
+      writeBin ( argv[7], &e[0], 1 );
+      writeBin ( argv[8], kphi.getData ( ), N );
       return 0;
     }
     if ( cmd == "xshiftreg" && argc == 8 ) {

@@ -260,6 +260,13 @@ def seismic(ref: msor.RefRunner, seed: int):
         d[f"h1x_{tag}"] = x
         d[f"h1sigma_{tag}"] = sg
         d[f"h1y_{tag}"] = ref.h1sys(x, sg)
+    # the regulariser with laplaceWeight > 0 (w L M^-1 L + stiffX + yRegFactor stiffY)
+    for tag, yreg, w in (("a", 0.3, 0.5), ("b", 2.0, 3.0)):
+        elap, klap = ref.xshift_reg_laplace(d[f"phi_{tag}"], yreg, w)
+        d.update({f"lapw_{tag}": w, f"Elap_{tag}": elap, f"Kphilap_{tag}": klap})
+    phi5 = rng.normal(0, 0.2, (5, 7))
+    elap, klap = ref.xshift_reg_laplace(phi5, 1.0, 1.5)
+    d.update({"phi_c": phi5, "yreg_c": 1.0, "lapw_c": 1.5, "Elap_c": elap, "Kphilap_c": klap})
     np.savez_compressed(os.path.join(OUT, "seismic.npz"), **d)
 
 

@@ -57,3 +57,36 @@ def test_xshift_recovers_a_line_shift(oracle):
     assert all(b <= a for a, b in zip(energies, energies[1:]))
     assert rows[-1][3] < rows[0][3]
     assert abs(ph[:, 8:-8].mean() * (nx - 1) - 1.5) < 0.05
+
+
+@pytest.mark.parametrize("tag", ["a", "b", "c"])
+def test_laplace_regulariser_bit_exact(oracle, tag):
+    """findXShift's regulariser with laplaceWeight > 0 (matchSeries.h:828-838):
+    laplaceWeight L M^-1 L (qc::assembleLaplaceSquareRegMatrix) + stiffX +
+    yRegFactor stiffY applied as the reference's CSR matrix, bit for bit."""
+    g = golden("seismic.npz")
+    e, k = oracle.xshift_reg_laplace(g[f"phi_{tag}"], float(g[f"yreg_{tag}"]), float(g[f"lapw_{tag}"]))
+    assert e == float(g[f"Elap_{tag}"])
+    assert np.array_equal(k, g[f"Kphilap_{tag}"])
+
+
+def test_laplace_regulariser_against_the_reference_driver(oracle):
+    if not oracle.have_ref():
+        pytest.skip("the reference driver is not built here")
+    rng = np.random.default_rng(12)
+    phi = rng.normal(0, 0.1, (11, 23))
+    e, k = oracle.xshift_reg_laplace(phi, 0.7, 2.5)
+    re, rk = oracle.RefRunner().xshift_reg_laplace(phi, 0.7, 2.5)
+    assert e == re and np.array_equal(k, rk)
+
+
+def test_xshift_with_laplace_weight_recovers_a_line_shift(oracle):
+    rng = np.random.default_rng(6)
+    nx, ny = 65, 17
+    x = np.arange(nx)
+    R = np.stack([np.sin(x / 4.0 + 0.3 * k) + 0.05 * rng.normal(size=nx) for k in range(ny)])
+    T = np.stack([np.sin((x - 1.5) / 4.0 + 0.3 * k) + 0.05 * rng.normal(size=nx) for k in range(ny)])
+    ph, e, steps, rows = oracle.xshift(R, T, 0.01, 1.0, 60, laplace_weight=0.01)
+    energies = [r[1] for r in rows]
+    assert all(b <= a for a, b in zip(energies, energies[1:]))
+    assert abs(ph[:, 8:-8].mean() * (nx - 1) - 1.5) < 0.1
