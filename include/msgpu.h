@@ -148,15 +148,17 @@ int msgpu_lineshift_energy(msgpu_context* ctx, int nx, int ny, const double* R, 
 int msgpu_lineshift_energy_device(msgpu_context* ctx, int nx, int ny, int num_images, const double* d_R,
                                   const double* d_T, const double* d_phix, double* d_energy_out, double* d_de_out,
                                   void* stream);
-/* findXShift's regulariser with laplaceWeight <= 0 (matchSeries.h:819-845):
- * K = stiffX + yreg * stiffY on the nx x ny grid (h = 1/(max(nx,ny)-1)),
- * energy 1/2 phix.K phix and K phix.                                       */
-int msgpu_xshift_reg(msgpu_context* ctx, int nx, int ny, double yreg, const double* phix, double* energy_out,
-                     double* kphi_out);
-int msgpu_xshift_reg_device(msgpu_context* ctx, int nx, int ny, int num_images, double yreg, const double* d_phix,
-                            double* d_energy_out, double* d_kphi_out, void* stream);
+/* findXShift's regulariser (matchSeries.h:819-845) on the nx x ny grid
+ * (h = 1/(max(nx,ny)-1)): K = stiffX + yreg * stiffY for laplace_weight <= 0,
+ * K = laplace_weight * L M^-1 L + stiffX + yreg * stiffY for laplace_weight
+ * > 0 (qc::assembleLaplaceSquareRegMatrix, hyperelastic.h:234-251; grids of
+ * at least 5 x 5 nodes); energy 1/2 phix.K phix and K phix.                */
+int msgpu_xshift_reg(msgpu_context* ctx, int nx, int ny, double yreg, double laplace_weight, const double* phix,
+                     double* energy_out, double* kphi_out);
+int msgpu_xshift_reg_device(msgpu_context* ctx, int nx, int ny, int num_images, double yreg, double laplace_weight,
+                            const double* d_phix, double* d_energy_out, double* d_kphi_out, void* stream);
 
-/* findXShift (matchSeries.h:805-865) with laplaceWeight <= 0: the gradient
+/* findXShift (matchSeries.h:805-865), laplaceWeight as in msgpu_xshift_reg: the gradient
  * flow with automatic filter width, Fletcher-Reeves NCG and Armijo steps on
  * E = line-shift data term + lambda * 1/2 phix.K phix, in the metric of
  * (M + sigma^2/2 L)^{-1} (CholeskyBasedInverseH1Metric, linearSmoothOp.h:
@@ -166,10 +168,11 @@ int msgpu_xshift_reg_device(msgpu_context* ctx, int nx, int ny, int num_images, 
  *   does).  max_iter: maxGDIterations (the reference's default is 500).
  *   energy_out, steps_out (nullable): host values.                         */
 int msgpu_find_xshift(msgpu_context* ctx, int nx, int ny, const double* R, const double* T, double lambda,
-                      double yreg, int max_iter, double* phix, double* energy_out, int* steps_out);
+                      double yreg, double laplace_weight, int max_iter, double* phix, double* energy_out,
+                      int* steps_out);
 int msgpu_find_xshift_device(msgpu_context* ctx, int nx, int ny, const double* d_R, const double* d_T, double lambda,
-                             double yreg, int max_iter, double* d_phix, double* energy_out, int* steps_out,
-                             void* stream);
+                             double yreg, double laplace_weight, int max_iter, double* d_phix, double* energy_out,
+                             int* steps_out, void* stream);
 
 /* findXShift for num_images images (host buffers, back to back): R is one
  * reference for all (r_per_image = 0, e.g. the mean stack) or one per image;
@@ -179,8 +182,8 @@ int msgpu_find_xshift_device(msgpu_context* ctx, int nx, int ny, const double* d
  * reference, which registers one image at a time).  Kernel-launch counts of
  * all workers are summed in msgpu_get_stats.                               */
 int msgpu_find_xshift_batch(msgpu_context* ctx, int nx, int ny, int num_images, const double* R, int r_per_image,
-                            const double* T, double lambda, double yreg, int max_iter, double* phix,
-                            double* energies_out, int* steps_out, int workers);
+                            const double* T, double lambda, double yreg, double laplace_weight, int max_iter,
+                            double* phix, double* energies_out, int* steps_out, int workers);
 
 /* --- series pipeline ------------------------------------------------------ */
 /* Options of matchSeries<>() beyond the registration keys (parameter-file

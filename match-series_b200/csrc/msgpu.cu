@@ -57,7 +57,7 @@ struct msgpu_context {
 
 namespace {
 
-constexpr int kAbiVersion = 3;
+constexpr int kAbiVersion = 4;
 
 int fail(msgpu_context* ctx, int code, const char* fmt, ...) {
   char buf[512];
@@ -1735,6 +1735,102 @@ XRegTables host_xreg_tables(int nx, int ny, double yreg) {
         for (int i = 0; i < 3; ++i) tb.st[cx + 3 * cy][j][i] = st[(size_t)(rep[cx] + rep[cy] * n) * 9 + j * 3 + i];
   return tb;
 }
+
+// The 25-point rows of laplaceWeight L M^-1 L + stiffX + yreg stiffY for
+// h = 1/(max(nx,ny)-1), formed on a 5 x 5 node patch the way findXShift
+// assembles them (matchSeries.h:828-838): L = StiffOp assembled element by
+// element, M the lumped mass (LumpedMassOp, element-order sums, inverted),
+// rows of L scaled by M^-1, the product added into entry (i, j) over k in
+// increasing column order (aol::Matrix::addMatrixProduct, matrix.cpp:
+// 414-429), scaled by laplaceWeight, then stiffX and yreg * stiffY added
+// element by element.  Every row depends only on its node's class along x
+// and y (first, second, interior, second last, last), so the patch's node
+// c holds class c's row.  Needs nx, ny >= 5.
+XLapTables host_xreg_lap_tables(int nx, int ny, double yreg, double w) {
+  const double h = 1. / (double)((nx > ny ? nx : ny) - 1), vol = h * h;
+  const double g[2] = {0.2113248654051871, 0.7886751345948129};
+  double rc[4][2];
+  for (int i = 0, k = 0; i < 2; ++i)
+    for (int j = 0; j < 2; ++j, ++k) { rc[k][0] = g[i]; rc[k][1] = g[j]; }
+  double gq[4][4][2], bq[4][4];
+  for (int b = 0; b < 4; ++b)
+    for (int q = 0; q < 4; ++q) {
+      host_basis_grad(b, rc[q][0], rc[q][1], h, gq[b][q]);
+      bq[b][q] = host_basis_val(b, rc[q][0], rc[q][1]);
+    }
+  const int n = 5, N = n * n;
+  double Ls[4][4] = {};
+  for (int q = 0; q < 4; ++q)
+    for (int i = 0; i < 4; ++i)
+      for (int j = i; j < 4; ++j) {
+        double d = 0;
+        d += gq[i][q][0] * gq[j][q][0];
+        d += gq[i][q][1] * gq[j][q][1];
+        Ls[i][j] += d * 1. * 0.25;
+      }
+  for (int i = 0; i < 4; ++i)
+    for (int j = i; j < 4; ++j) Ls[j][i] = Ls[i][j] = Ls[i][j] * vol;
+  double lmloc[4] = {0., 0., 0., 0.};
+  for (int q = 0; q < 4; ++q)
+    for (int i = 0; i < 4; ++i) lmloc[i] += 1. * bq[i][q] * 0.25;
+  for (int i = 0; i < 4; ++i) lmloc[i] *= vol;
+  std::vector<double> L((size_t)N * 9, 0.0), lm(N, 0.0), K((size_t)N * 25, 0.0);
+  for (int ey = 0; ey < n - 1; ++ey)
+    for (int ex = 0; ex < n - 1; ++ex)
+      for (int i = 0; i < 4; ++i) {
+        const int gi = ex + ey * n + ((i & 1) ? 1 : 0) + ((i & 2) ? n : 0);
+        lm[gi] += lmloc[i];
+        for (int j = 0; j < 4; ++j) {
+          const int gj = ex + ey * n + ((j & 1) ? 1 : 0) + ((j & 2) ? n : 0);
+          const int dx = (gj % n) - (gi % n), dy = (gj / n) - (gi / n);
+          L[(size_t)gi * 9 + (dy + 1) * 3 + (dx + 1)] += Ls[i][j];
+        }
+      }
+  for (int r = 0; r < N; ++r) {
+    const int x = r % n, y = r / n;
+    double* kr = K.data() + (size_t)r * 25;
+    for (int a = -1; a <= 1; ++a)
+      for (int b = -1; b <= 1; ++b) {
+        const int X = x + b, Y = y + a;
+        if (X < 0 || X >= n || Y < 0 || Y >= n) continue;
+        const int k = X + Y * n;
+        const double lik = L[(size_t)r * 9 + (a + 1) * 3 + (b + 1)];
+        const double minv = 1. / lm[k];
+        for (int c = -1; c <= 1; ++c)
+          for (int d = -1; d <= 1; ++d) {
+            const int X2 = X + d, Y2 = Y + c;
+            if (X2 < 0 || X2 >= n || Y2 < 0 || Y2 >= n) continue;
+            const double m2 = L[(size_t)k * 9 + (c + 1) * 3 + (d + 1)] * minv;
+            kr[(a + c + 2) * 5 + (b + d + 2)] += lik * m2;
+          }
+      }
+    for (int e = 0; e < 25; ++e) kr[e] *= w;
+  }
+  for (int pass = 0; pass < 2; ++pass) {
+    const int sd = pass;
+    const double factor = pass == 0 ? 1.0 : yreg;
+    double Lm[4][4] = {};
+    for (int q = 0; q < 4; ++q)
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) Lm[i][j] += 1. * gq[i][q][sd] * gq[j][q][sd] * 0.25;
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j) Lm[i][j] *= vol;
+    for (int ey = 0; ey < n - 1; ++ey)
+      for (int ex = 0; ex < n - 1; ++ex)
+        for (int i = 0; i < 4; ++i)
+          for (int j = 0; j < 4; ++j) {
+            const int gi = ex + ey * n + ((i & 1) ? 1 : 0) + ((i & 2) ? n : 0);
+            const int gj = ex + ey * n + ((j & 1) ? 1 : 0) + ((j & 2) ? n : 0);
+            const int dx = (gj % n) - (gi % n), dy = (gj / n) - (gi / n);
+            K[(size_t)gi * 25 + (dy + 2) * 5 + (dx + 2)] += factor * Lm[i][j];
+          }
+  }
+  XLapTables tb;
+  for (int cy = 0; cy < 5; ++cy)
+    for (int cx = 0; cx < 5; ++cx)
+      for (int e = 0; e < 25; ++e) tb.st[cx + 5 * cy][e] = K[(size_t)(cx + cy * n) * 25 + e];
+  return tb;
+}
 }  // namespace
 
 namespace {
@@ -1856,6 +1952,8 @@ struct XsSolver {
   double lambda, yreg;
   LineTables lt;
   XRegTables rt;
+  double lapw = 0.;      // laplaceWeight (> 0: the Laplace-square regulariser)
+  XLapTables lapt;
   cudaStream_t st;
   double rb_tau[2], rb_e[2];
   int rb_pos = 0, evals = 0;
@@ -1881,7 +1979,11 @@ struct XsSolver {
     const size_t smem = sizeof(double) * 3 * (size_t)nx;
     k_lineshift<<<dim3(ny, 1), kLineThreads, smem, st>>>(a);
     const int nb = std::min(1024, (N + 255) / 256);
-    k_xshift_reg<<<dim3(nb, 1), 256, 0, st>>>(rt, nx, ny, (size_t)N, p, B.kphi, B.part, B.done + 1, B.scal + 2);
+    if (lapw > 0)
+      k_xshift_reg_lap<<<dim3(nb, 1), 256, 0, st>>>(lapt, nx, ny, (size_t)N, p, B.kphi, B.part, B.done + 1,
+                                                    B.scal + 2);
+    else
+      k_xshift_reg<<<dim3(nb, 1), 256, 0, st>>>(rt, nx, ny, (size_t)N, p, B.kphi, B.part, B.done + 1, B.scal + 2);
     ctx->stats.kernel_launches += 2;
     CK(cudaGetLastError());
     return MSGPU_OK;
@@ -1950,6 +2052,7 @@ struct XsSolver {
 // (gradientDescent.h:295-464, 675-691) on the host, every vector operation on
 // the device; phi (device, nx*ny) in/out.
 int run_xshift(msgpu_context* ctx, int nx, int ny, const double* R, const double* T, double lambda, double yreg,
+               double lapw,
                int max_iter, double* phi, double* energy_out, int* steps_out, cudaStream_t st) {
   XsSolver S;
   S.ctx = ctx; S.nx = nx; S.ny = ny; S.N = nx * ny; S.R = R; S.T = T; S.lambda = lambda; S.yreg = yreg; S.st = st;
@@ -1960,6 +2063,8 @@ int run_xshift(msgpu_context* ctx, int nx, int ny, const double* R, const double
   if ((rc = ensure(ctx, ctx->nccbuf, sizeof(double) * (size_t)ny + 64))) return rc;
   S.lt = host_line_tables(nx);
   S.rt = host_xreg_tables(nx, ny, yreg);
+  S.lapw = lapw;
+  if (lapw > 0) S.lapt = host_xreg_lap_tables(nx, ny, yreg, lapw);
   CK(cudaFuncSetAttribute(k_lineshift, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)(sizeof(double) * 3 * (size_t)nx)));
   CK(cudaFuncSetAttribute(k_lineshift_prep_ref, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2029,22 +2134,26 @@ int run_xshift(msgpu_context* ctx, int nx, int ny, const double* R, const double
 }  // namespace
 
 int msgpu_find_xshift_device(msgpu_context* ctx, int nx, int ny, const double* d_R, const double* d_T, double lambda,
-                             double yreg, int max_iter, double* d_phix, double* energy_out, int* steps_out,
-                             void* stream) {
+                             double yreg, double laplace_weight, int max_iter, double* d_phix, double* energy_out,
+                             int* steps_out, void* stream) {
   if (!ctx) return MSGPU_ERR_INVALID_ARG;
   if (nx < 3 || ny < 3 || max_iter < 0 || !d_R || !d_T || !d_phix)
     return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid find_xshift arguments (grids of at least 3 x 3 nodes)");
+  if (!std::isfinite(laplace_weight) || (laplace_weight > 0 && (nx < 5 || ny < 5)))
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "laplaceWeight %g: finite, and > 0 only on grids of at least 5 x 5 nodes",
+                laplace_weight);
   if (sizeof(double) * 3 * (size_t)nx > 200 * 1024)
     return fail(ctx, MSGPU_ERR_SIZE, "lines of %d samples do not fit shared memory", nx);
   int rc;
   if ((rc = bind_device(ctx))) return rc;
   ctx->stats.kernel_launches = 0;
-  return run_xshift(ctx, nx, ny, d_R, d_T, lambda, yreg, max_iter, d_phix, energy_out, steps_out,
+  return run_xshift(ctx, nx, ny, d_R, d_T, lambda, yreg, laplace_weight, max_iter, d_phix, energy_out, steps_out,
                     (cudaStream_t)stream);
 }
 
 int msgpu_find_xshift(msgpu_context* ctx, int nx, int ny, const double* R, const double* T, double lambda,
-                      double yreg, int max_iter, double* phix, double* energy_out, int* steps_out) {
+                      double yreg, double laplace_weight, int max_iter, double* phix, double* energy_out,
+                      int* steps_out) {
   if (!ctx) return MSGPU_ERR_INVALID_ARG;
   if (!R || !T || !phix) return fail(ctx, MSGPU_ERR_INVALID_ARG, "null buffer");
   int rc;
@@ -2056,8 +2165,8 @@ int msgpu_find_xshift(msgpu_context* ctx, int nx, int ny, const double* R, const
   CK(cudaMemcpyAsync(d, R, sizeof(double) * N, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(d + N, T, sizeof(double) * N, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(d + 2 * N, phix, sizeof(double) * N, cudaMemcpyHostToDevice, st));
-  if ((rc = msgpu_find_xshift_device(ctx, nx, ny, d, d + N, lambda, yreg, max_iter, d + 2 * N, energy_out, steps_out,
-                                     st)))
+  if ((rc = msgpu_find_xshift_device(ctx, nx, ny, d, d + N, lambda, yreg, laplace_weight, max_iter, d + 2 * N,
+                                     energy_out, steps_out, st)))
     return rc;
   CK(cudaMemcpyAsync(phix, d + 2 * N, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
@@ -2065,8 +2174,8 @@ int msgpu_find_xshift(msgpu_context* ctx, int nx, int ny, const double* R, const
 }
 
 int msgpu_find_xshift_batch(msgpu_context* ctx, int nx, int ny, int num_images, const double* R, int r_per_image,
-                            const double* T, double lambda, double yreg, int max_iter, double* phix,
-                            double* energies_out, int* steps_out, int workers) {
+                            const double* T, double lambda, double yreg, double laplace_weight, int max_iter,
+                            double* phix, double* energies_out, int* steps_out, int workers) {
   if (!ctx) return MSGPU_ERR_INVALID_ARG;
   if (num_images < 1 || !R || !T || !phix) return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid find_xshift_batch arguments");
   int rc;
@@ -2089,7 +2198,7 @@ int msgpu_find_xshift_batch(msgpu_context* ctx, int nx, int ny, int num_images, 
       double e = 0;
       int st = 0;
       const int c = msgpu_find_xshift(w, nx, ny, R + (r_per_image ? (size_t)i * N : 0), T + (size_t)i * N, lambda,
-                                      yreg, max_iter, phix + (size_t)i * N, &e, &st);
+                                      yreg, laplace_weight, max_iter, phix + (size_t)i * N, &e, &st);
       if (c) {
         codes[wi] = c;
         msgs[wi] = w->err;
@@ -2166,27 +2275,35 @@ int msgpu_lineshift_energy(msgpu_context* ctx, int nx, int ny, const double* R, 
   return MSGPU_OK;
 }
 
-int msgpu_xshift_reg_device(msgpu_context* ctx, int nx, int ny, int num_images, double yreg, const double* d_phix,
-                            double* d_energy_out, double* d_kphi_out, void* stream) {
+int msgpu_xshift_reg_device(msgpu_context* ctx, int nx, int ny, int num_images, double yreg, double laplace_weight,
+                            const double* d_phix, double* d_energy_out, double* d_kphi_out, void* stream) {
   if (!ctx) return MSGPU_ERR_INVALID_ARG;
   if (nx < 3 || ny < 3 || num_images < 1 || !d_phix || !d_energy_out || !d_kphi_out)
     return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid xshift_reg arguments (grids of at least 3 x 3 nodes)");
+  if (!std::isfinite(laplace_weight) || (laplace_weight > 0 && (nx < 5 || ny < 5)))
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "laplaceWeight %g: finite, and > 0 only on grids of at least 5 x 5 nodes",
+                laplace_weight);
   int rc;
   if ((rc = bind_device(ctx))) return rc;
   const int N = nx * ny;
   const int nb = std::min(1024, (N + 255) / 256);
   if ((rc = ensure(ctx, ctx->vals, sizeof(double) * (size_t)nb * num_images + 64))) return rc;
   cudaStream_t st = (cudaStream_t)stream;
-  k_xshift_reg<<<dim3(nb, num_images), 256, 0, st>>>(host_xreg_tables(nx, ny, yreg), nx, ny, (size_t)N, d_phix,
-                                                     d_kphi_out, (double*)ctx->vals.p, nullptr, nullptr);
+  if (laplace_weight > 0)
+    k_xshift_reg_lap<<<dim3(nb, num_images), 256, 0, st>>>(host_xreg_lap_tables(nx, ny, yreg, laplace_weight), nx, ny,
+                                                           (size_t)N, d_phix, d_kphi_out, (double*)ctx->vals.p,
+                                                           nullptr, nullptr);
+  else
+    k_xshift_reg<<<dim3(nb, num_images), 256, 0, st>>>(host_xreg_tables(nx, ny, yreg), nx, ny, (size_t)N, d_phix,
+                                                       d_kphi_out, (double*)ctx->vals.p, nullptr, nullptr);
   k_xshift_reg_total<<<num_images, 256, 0, st>>>((const double*)ctx->vals.p, nb, d_energy_out);
   CK(cudaGetLastError());
   ctx->stats.kernel_launches = 2;
   return MSGPU_OK;
 }
 
-int msgpu_xshift_reg(msgpu_context* ctx, int nx, int ny, double yreg, const double* phix, double* energy_out,
-                     double* kphi_out) {
+int msgpu_xshift_reg(msgpu_context* ctx, int nx, int ny, double yreg, double laplace_weight, const double* phix,
+                     double* energy_out, double* kphi_out) {
   if (!ctx) return MSGPU_ERR_INVALID_ARG;
   if (!phix || !energy_out || !kphi_out) return fail(ctx, MSGPU_ERR_INVALID_ARG, "null buffer");
   int rc;
@@ -2196,7 +2313,7 @@ int msgpu_xshift_reg(msgpu_context* ctx, int nx, int ny, double yreg, const doub
   double* d = (double*)ctx->io[0].p;
   cudaStream_t st = ctx->stream;
   CK(cudaMemcpyAsync(d, phix, sizeof(double) * N, cudaMemcpyHostToDevice, st));
-  if ((rc = msgpu_xshift_reg_device(ctx, nx, ny, 1, yreg, d, d + 2 * N, d + N, st))) return rc;
+  if ((rc = msgpu_xshift_reg_device(ctx, nx, ny, 1, yreg, laplace_weight, d, d + 2 * N, d + N, st))) return rc;
   CK(cudaMemcpyAsync(energy_out, d + 2 * N, sizeof(double), cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(kphi_out, d + N, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));

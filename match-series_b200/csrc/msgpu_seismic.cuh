@@ -333,6 +333,75 @@ __global__ void __launch_bounds__(256) k_xshift_reg_total(const double* part, in
   if (threadIdx.x == 0) out[blockIdx.x] = 0.5 * s;
 }
 
+// findXShift's regulariser with laplaceWeight > 0 (matchSeries.h:828-838):
+// the 25-point rows of laplaceWeight L M^-1 L + stiffX + yRegFactor stiffY
+// for the 25 node classes (first, second, interior, second last, last along
+// x and y), applied in column order (the reference's CSR rows are sorted by
+// column, i.e. by offset (dy, dx)); partial sums of phi . K phi per block,
+// the image's total by the last block as in k_xshift_reg.
+struct XLapTables {
+  double st[25][25];   // [class cx + 5 cy][(dy + 2) * 5 + (dx + 2)]
+};
+
+__device__ __forceinline__ int lap_class(int x, int n) {
+  return x == 0 ? 0 : (x == 1 ? 1 : (x == n - 1 ? 4 : (x == n - 2 ? 3 : 2)));
+}
+
+__global__ void __launch_bounds__(256) k_xshift_reg_lap(XLapTables tb, int nx, int ny, size_t img_stride,
+                                                        const double* phi, double* kphi, double* part,
+                                                        unsigned* done, double* e_total) {
+  __shared__ double red[8];
+  const double* p = phi + (size_t)blockIdx.y * img_stride;
+  double* k = kphi + (size_t)blockIdx.y * img_stride;
+  const int N = nx * ny;
+  double acc = 0.0;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < N; r += gridDim.x * blockDim.x) {
+    const int x = r % nx, y = r / nx;
+    const double* row = tb.st[lap_class(x, nx) + 5 * lap_class(y, ny)];
+    double d = 0.;
+#pragma unroll
+    for (int j = -2; j <= 2; ++j)
+#pragma unroll
+      for (int i = -2; i <= 2; ++i) {
+        const int X = x + i, Y = y + j;
+        if (X >= 0 && X < nx && Y >= 0 && Y < ny) d += row[(j + 2) * 5 + (i + 2)] * p[X + (size_t)Y * nx];
+      }
+    k[r] = d;
+    acc += d * p[r];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < 8; ++w) s += red[w];
+    part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
+  }
+  if (!done) return;
+  __shared__ int last;
+  __shared__ double red2[8];
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(done + blockIdx.y, 1u) == gridDim.x - 1) ? 1 : 0;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const double* pp = part + (size_t)blockIdx.y * gridDim.x;
+  double v = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += 256) v += __ldcg(pp + i);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red2[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 8; ++w) t += red2[w];
+    e_total[blockIdx.y] = 0.5 * t;
+    done[blockIdx.y] = 0u;
+  }
+}
+
 // --- vector kernels of the seismic descent ----------------------------------
 // out[i] = a[i] + s * b[i]  (also the in-place updates, with out == a)
 __global__ void k_axpy(const double* a, double s, const double* b, double* out, int n) {

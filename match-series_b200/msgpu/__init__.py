@@ -187,18 +187,17 @@ def lib():
         L.msgpu_lineshift_energy_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
-        L.msgpu_xshift_reg.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp]
-        L.msgpu_xshift_reg_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
-                                              ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
-                                              ctypes.c_void_p]
-        L.msgpu_find_xshift.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_double,
-                                        ctypes.c_double, ctypes.c_int, _dp, _dp, _ip]
+        _d = ctypes.c_double
+        L.msgpu_xshift_reg.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _d, _d, _dp, _dp, _dp]
+        L.msgpu_xshift_reg_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _d, _d,
+                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.msgpu_find_xshift.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp, _d, _d, _d,
+                                        ctypes.c_int, _dp, _dp, _ip]
         L.msgpu_find_xshift_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
-                                               ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int,
-                                               ctypes.c_void_p, _dp, _ip, ctypes.c_void_p]
+                                               ctypes.c_void_p, _d, _d, _d, ctypes.c_int, ctypes.c_void_p, _dp, _ip,
+                                               ctypes.c_void_p]
         L.msgpu_find_xshift_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp,
-                                              ctypes.c_int, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp,
-                                              _dp, _ip, ctypes.c_int]
+                                              ctypes.c_int, _dp, _d, _d, _d, ctypes.c_int, _dp, _dp, _ip, ctypes.c_int]
         L.msgpu_register_ragged.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params), ctypes.POINTER(SeriesDesc),
                                             ctypes.c_int]
         L.msgpu_register_ragged_device.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params),
@@ -437,16 +436,17 @@ class Context:
         self._check(lib().msgpu_lineshift_energy_device(self._h, nx, ny, num_images, d_R, d_T, d_phix, d_energy,
                                                         d_de or None, stream))
 
-    def xshift_reg(self, phix, yreg):
+    def xshift_reg(self, phix, yreg, laplace_weight=0.0):
         """findXShift's regulariser: (1/2 phi.K phi, K phi)."""
         phix = _f64(phix)
         ny, nx = phix.shape
         e = ctypes.c_double()
         k = np.zeros((ny, nx))
-        self._check(lib().msgpu_xshift_reg(self._h, nx, ny, float(yreg), _p(phix), ctypes.byref(e), _p(k)))
+        self._check(lib().msgpu_xshift_reg(self._h, nx, ny, float(yreg), float(laplace_weight), _p(phix),
+                                           ctypes.byref(e), _p(k)))
         return e.value, k
 
-    def find_xshift(self, R, T, lam, yreg, max_iter=500, phix=None):
+    def find_xshift(self, R, T, lam, yreg, max_iter=500, phix=None, laplace_weight=0.0):
         """findXShift: returns (phix (ny, nx), energy, steps)."""
         R = _f64(R)
         ny, nx = R.shape
@@ -454,10 +454,11 @@ class Context:
         e = ctypes.c_double()
         steps = ctypes.c_int()
         self._check(lib().msgpu_find_xshift(self._h, nx, ny, _p(R), _p(_f64(T)), float(lam), float(yreg),
+                                            float(laplace_weight),
                                             int(max_iter), _p(ph), ctypes.byref(e), ctypes.byref(steps)))
         return ph, e.value, steps.value
 
-    def find_xshift_batch(self, R, T, lam, yreg, max_iter=500, phix=None, workers=4):
+    def find_xshift_batch(self, R, T, lam, yreg, max_iter=500, phix=None, workers=4, laplace_weight=0.0):
         """findXShift for images T (G, ny, nx) against R (ny, nx) or (G, ny, nx);
         returns (phix (G, ny, nx), energies[G], steps[G])."""
         T = _f64(T)
@@ -468,6 +469,7 @@ class Context:
         en = np.zeros(G)
         st = np.zeros(G, dtype=np.int32)
         self._check(lib().msgpu_find_xshift_batch(self._h, nx, ny, G, _p(R), per, _p(T), float(lam), float(yreg),
+                                                  float(laplace_weight),
                                                   int(max_iter), _p(ph), _p(en), st.ctypes.data_as(_ip),
                                                   int(workers)))
         return ph, en, st

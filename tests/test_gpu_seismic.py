@@ -92,3 +92,31 @@ def test_find_xshift_batch_equals_single_calls(gpu):
     ph2, en2, _ = gpu.find_xshift_batch(R[0], T, 0.01, 1.0, 30, workers=2)
     p1, e1, _ = gpu.find_xshift(R[0], T[3], 0.01, 1.0, 30)
     assert np.array_equal(ph2[3], p1) and en2[3] == e1
+
+
+@pytest.mark.parametrize("tag", ["a", "b", "c"])
+def test_laplace_regulariser_matches_reference(gpu, tag):
+    """laplaceWeight > 0: laplaceWeight L M^-1 L + stiffX + yRegFactor stiffY;
+    K phi bit for bit against the reference's CSR matrix, the energy (a
+    block-parallel sum) within 1e-13."""
+    g = golden("seismic.npz")
+    e, k = gpu.xshift_reg(g[f"phi_{tag}"], float(g[f"yreg_{tag}"]), float(g[f"lapw_{tag}"]))
+    assert np.array_equal(k, g[f"Kphilap_{tag}"])
+    assert abs(e - float(g[f"Elap_{tag}"])) <= 1e-13 * abs(float(g[f"Elap_{tag}"]))
+
+
+def test_find_xshift_with_laplace_weight_matches_oracle(gpu, oracle):
+    nx, ny = 65, 17
+    R, T = _shifted_lines(nx, ny, 1.5, 6)
+    ph, e, steps = gpu.find_xshift(R, T, 0.01, 1.0, 60, laplace_weight=0.01)
+    rph, re, rsteps, _ = oracle.xshift(R, T, 0.01, 1.0, 60, laplace_weight=0.01)
+    assert steps == rsteps
+    assert abs(e - re) <= 1e-9 * abs(re)
+    assert np.abs(ph - rph).max() * (nx - 1) <= 1e-6
+    assert abs(ph[:, 8:-8].mean() * (nx - 1) - 1.5) < 0.1
+
+
+def test_laplace_weight_needs_five_nodes(gpu):
+    import msgpu
+    with pytest.raises(msgpu.MsgpuError, match="5 x 5"):
+        gpu.xshift_reg(np.zeros((4, 9)), 1.0, 0.5)
