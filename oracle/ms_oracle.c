@@ -1728,7 +1728,15 @@ typedef struct {
   int rb_pos, evals;
   double e_at_pos;
   double *tx, *w;
+  int yconst;                  /* findXShiftYConst: the unknown is one shift per line (N = ny) */
+  double *full, *defull;       /* nx*ny scratch of the row-constant mode */
 } xs_ctx;
+
+/* qc::ScalarArray<QC_2D>::setInXDirectionFrom (scalarArray.h:1409-1416) */
+static void yc_expand(const xs_ctx* C, const double* v) {
+  for (int y = 0; y < C->ny; ++y)
+    for (int x = 0; x < C->nx; ++x) C->full[(size_t)y * C->nx + x] = v[y];
+}
 
 static double xs_reg(xs_ctx* C, const double* phi) {
   return C->lapw > 0 ? msor_xshift_reg_laplace(C->nx, C->ny, C->yreg, C->lapw, phi, C->w)
@@ -1737,6 +1745,10 @@ static double xs_reg(xs_ctx* C, const double* phi) {
 
 /* E = EData + lambda * ERegStiff (LinCombOp, matchSeries.h:847-850) */
 static double xs_energy(xs_ctx* C, const double* phi) {
+  if (C->yconst) {   /* PixelWiseToRowWiseOp::apply (quocOps.h:195-199): the data term alone */
+    yc_expand(C, phi);
+    return msor_lineshift(C->nx, C->ny, C->R, C->T, C->full, NULL);
+  }
   double e = 0.;
   e += msor_lineshift(C->nx, C->ny, C->R, C->T, phi, NULL);
   e += C->lambda * xs_reg(C, phi);
@@ -1745,6 +1757,16 @@ static double xs_energy(xs_ctx* C, const double* phi) {
 
 /* DE = DEData + lambda * K phi */
 static void xs_gradient(xs_ctx* C, const double* phi, double* de) {
+  if (C->yconst) {   /* PixelWiseToRowWiseOp::applyDerivative: row sums (sumInXDirectionTo, scalarArray.h:1395-1402) */
+    yc_expand(C, phi);
+    msor_lineshift(C->nx, C->ny, C->R, C->T, C->full, C->defull);
+    for (int y = 0; y < C->ny; ++y) {
+      double sum = 0.;
+      for (int x = 0; x < C->nx; ++x) sum += C->defull[(size_t)y * C->nx + x];
+      de[y] = sum;
+    }
+    return;
+  }
   msor_lineshift(C->nx, C->ny, C->R, C->T, phi, de);
   xs_reg(C, phi);
   for (int i = 0; i < C->N; ++i) de[i] += C->lambda * C->w[i];
@@ -1785,6 +1807,109 @@ static double xs_armijo(xs_ctx* C, const double* p, const double* d, const doubl
     } while ((!finite(fnew) || (G < sigma || f < fnew)) && (tau > tau_min));
   }
   return (tau > tau_min) ? tau : 0.;
+}
+
+/* The template smoothed along x for findXShiftYConst: Template.applyLinearFilterTo
+ * with a (4i+1) x (4i+1) kernel whose middle row is 1/(4i+1) and the other
+ * rows 0 (ScalarArray<QC_2D>::getConvolveValue, scalarArray.cpp:936-965: the
+ * whole window in row order, periodic outside the array, so the zero rows
+ * still carry a NaN of their pixels).                                      */
+void msor_box_x(const double* T, int nx, int ny, int i, double* out) {
+  const int o = 2 * i;
+  const double k = 1. / (double)(2 * o + 1);
+  for (int y = 0; y < ny; ++y)
+    for (int x = 0; x < nx; ++x) {
+      double val = 0.0;
+      for (int oy = -o; oy <= o; ++oy)
+        for (int ox = -o; ox <= o; ++ox) {
+          int X = x + ox, Y = y + oy;
+          if (X < 0) X += nx; else if (X > nx - 1) X = X % nx;
+          if (Y < 0) Y += ny; else if (Y > ny - 1) Y = Y % ny;
+          val += (oy == 0 ? k : 0.0) * T[(size_t)Y * nx + X];
+        }
+      out[(size_t)y * nx + x] = val;
+    }
+}
+
+/* findXShiftYConst (matchSeries.h:873-920): one shift per line, started from
+ * the line means of phix; four descents (GridlessGradientDescent with
+ * Fletcher-Reeves NCG: GradientDescentBase::applySingle, gradientDescent.h:
+ * 295-464, without smoothing or filter widths, stopping when the Armijo step
+ * is 0) against the template smoothed along x by boxes of 13, 9 and 5
+ * samples and then unsmoothed; E = the line-shift data term of the
+ * row-constant shift, DE its derivative summed along each line.  phix
+ * (nx*ny) in/out; returns the steps of the last descent.                  */
+int msor_xshift_yconst(int nx, int ny, const double* R, const double* T, int max_iter, double* phix,
+                       double* energy_out) {
+  const int N = nx * ny;
+  xs_ctx C;
+  memset(&C, 0, sizeof(C));
+  C.nx = nx; C.ny = ny; C.N = ny; C.R = R; C.yconst = 1;
+  double* big = (double*)calloc((size_t)N * 3, sizeof(double));
+  double* Ts = big;
+  C.full = big + N; C.defull = big + 2 * N;
+  double* buf = (double*)calloc((size_t)ny * 7, sizeof(double));
+  double *v = buf, *d = buf + ny, *og = buf + 2 * ny, *od = buf + 3 * ny, *DE = buf + 4 * ny;
+  C.tx = buf + 5 * ny; C.w = buf + 6 * ny;
+  for (int y = 0; y < ny; ++y) {
+    double sum = 0.;
+    for (int x = 0; x < nx; ++x) sum += phix[(size_t)y * nx + x];
+    v[y] = sum;
+  }
+  for (int y = 0; y < ny; ++y) v[y] /= (double)nx;
+  double energy_new = INFINITY;
+  int iter = 0;
+  for (int round = 3; round >= 0; --round) {
+    if (round > 0) msor_box_x(T, nx, ny, round, Ts);
+    else memcpy(Ts, T, sizeof(double) * N);
+    C.T = Ts;
+    C.rb_tau[0] = C.rb_tau[1] = NAN;
+    C.rb_pos = 0;
+    memset(og, 0, sizeof(double) * ny);
+    memset(od, 0, sizeof(double) * ny);
+    double tau = 1.0;
+    double energy = xs_energy(&C, v);
+    energy_new = energy;
+    iter = 0;
+    int go = max_iter > 0;
+    while (go) {
+      iter++;
+      energy = energy_new;
+      C.e_at_pos = energy;
+      C.evals = 0;
+      xs_gradient(&C, v, DE);
+      for (int i = 0; i < ny; ++i) d[i] = DE[i] * -1.;
+      double beta = 0.;
+      if ((iter - 1) % 10) beta = dot(d, d, ny) / dot(og, og, ny);
+      memcpy(og, d, sizeof(double) * ny);
+      for (int i = 0; i < ny; ++i) d[i] += beta * od[i];
+      memcpy(od, d, sizeof(double) * ny);
+      tau = xs_armijo(&C, v, d, DE, tau);
+      for (int i = 0; i < ny; ++i) d[i] *= tau;
+      if (tau == 0) {
+        memcpy(d, og, sizeof(double) * ny);
+        memset(od, 0, sizeof(double) * ny);
+        tau = xs_armijo(&C, v, d, DE, tau);
+        for (int i = 0; i < ny; ++i) d[i] *= tau;
+      }
+      double enew = NAN;
+      if (C.rb_tau[0] == tau) enew = C.rb_e[0];
+      else if (C.rb_tau[1] == tau) enew = C.rb_e[1];
+      else if (tau == 0) enew = energy;
+      if (tau != 0)
+        for (int i = 0; i < ny; ++i) v[i] += d[i];
+      if (isnan(enew)) enew = xs_energy(&C, v);
+      energy_new = enew;
+      go = ((energy - energy_new) > 0.) && (iter < max_iter);
+      if (tau == 0) go = 0;
+    }
+  }
+  for (int y = 0; y < ny; ++y)
+    for (int x = 0; x < nx; ++x) phix[(size_t)y * nx + x] = v[y];
+  if (energy_out) *energy_out = energy_new;
+  free(big);
+  free(buf);
+  return iter;
 }
 
 /* findXShift with laplaceWeight <= 0: GradientDescentWithAutomaticFilterWidth

@@ -158,6 +158,10 @@ void   msor_h1_metric(int nx, int ny, double sigma, double* x);
 int    msor_xshift(int nx, int ny, const double* R, const double* T, double lambda, double yreg,
                    double laplace_weight, int max_iter, double* phix, double* energy_out, msor_step* trace,
                    int trace_cap);
+/* findXShiftYConst (matchSeries.h:873-920): one shift per line; phix in/out */
+int    msor_xshift_yconst(int nx, int ny, const double* R, const double* T, int max_iter, double* phix,
+                          double* energy_out);
+void   msor_box_x(const double* T, int nx, int ny, int i, double* out);
 /* matchSeries<>() with accumulated deformations, refinement and extra stages
  * (matchSeries.h:87-265, 353-445, 1250-1320); see ms_oracle.c.             */
 void   msor_match_series(int data_term, int level, int start, int stop, double lambda,

@@ -241,6 +241,25 @@ def xshift(R, T, lam, yreg, max_iter, phix=None, trace_cap=4096, laplace_weight=
     return ph, e.value, steps, rows
 
 
+def xshift_yconst(R, T, max_iter, phix=None):
+    """findXShiftYConst: returns (phix (one value per line), energy, steps of the last descent)."""
+    R = _c(R)
+    ny, nx = R.shape
+    ph = np.zeros((ny, nx)) if phix is None else _c(phix).copy()
+    e = ctypes.c_double()
+    steps = lib().msor_xshift_yconst(nx, ny, _p(R.reshape(-1)), _p(_c(T).reshape(-1)), max_iter,
+                                     _p(ph.reshape(-1)), ctypes.byref(e))
+    return ph, e.value, steps
+
+
+def box_x(T, i):
+    T = _c(T)
+    ny, nx = T.shape
+    out = np.zeros((ny, nx))
+    lib().msor_box_x(_p(T.reshape(-1)), nx, ny, i, _p(out))
+    return out
+
+
 def warp_median(level, frames, phis, fill):
     N = n_of(level) ** 2
     out = np.zeros(N)
@@ -364,6 +383,12 @@ class RefRunner:
         self.run("xshiftlap", nx, ny, repr(float(yreg)), repr(float(w)), self._w("px", phix),
                  os.path.join(self.dir, "e"), os.path.join(self.dir, "k"))
         return float(self._r("e")[0]), self._r("k").reshape(ny, nx)
+
+    def xshift_yconst(self, R, T, max_iter, phix):
+        ny, nx = R.shape
+        self.run("xshiftyconst", nx, ny, int(max_iter), self._w("R", R), self._w("T", T), self._w("px", phix),
+                 os.path.join(self.dir, "po"), os.path.join(self.dir, "e"))
+        return self._r("po").reshape(ny, nx), float(self._r("e")[0])
 
     def h1sys(self, x, sigma):
         ny, nx = x.shape

@@ -16,6 +16,9 @@
 // width (gradientDescent.h:632-709).
 #include <registration.h>
 #include <hyperelastic.h>
+#include <quocOps.h>
+#include <gradientDescent.h>
+#include <kernel2d.h>
 #include <CSRMatrix.h>
 #include <configurators.h>
 
@@ -364,6 +367,7 @@ static int usage ( ) {
     "ms_ref save nx ny in out type | load file out dims | savedef L in mask | loaddef L mask out\n"
     "ms_ref lineshift nx ny R T phix outE outDE | xshiftreg nx ny yRegFactor phix outE outKphi\n"
     "ms_ref xshiftlap nx ny yRegFactor laplaceWeight phix outE outKphi\n"
+    "ms_ref xshiftyconst nx ny maxIter R T phix outPhi outE\n"
     "ms_ref h1sys nx ny sigma x out\n"
     "ms_ref series[_ncc] maxL start stop lambda lambdaFactor maxIter stopEps sat minToZero F framesBin outPhis outMean outTxt\n"
     "ms_ref matchseries[_ncc] maxL start stop lambda lambdaFactor maxIter stopEps sat minToZero refineStart refineStop\n"
@@ -529,6 +533,46 @@ int main ( int argc, char **argv ) {
       DE.apply ( phi, de );
       writeBin ( argv[7], &e[0], 1 );
       writeBin ( argv[8], de.getData ( ), N );
+      return 0;
+    }
+    if ( cmd == "xshiftyconst" && argc == 10 ) {
+      // ms_ref xshiftyconst nx ny maxIter R T phix outPhi outE: findXShiftYConst (matchSeries.h:873-920), composed
+      // from the same reference components in the same order (the function's header is not among the modules)
+      typedef qc::RectangularGridConfigurator<RealType, qc::QC_2D, aol::GaussQuadrature<RealType, qc::QC_2D, 3> > RectConf;
+      typedef qc::RectangularGridConfigurator<RealType, qc::QC_1D, aol::GaussQuadrature<RealType, qc::QC_1D, 3> > RectConf1D;
+      typedef qc::FELineShiftRegisEnergy<RectConf, RectConf1D, qc::NCCRegistrationConfigurator<RectConf1D> > LineEnergy;
+      const int nx = atoi ( argv[2] ), ny = atoi ( argv[3] ), maxIter = atoi ( argv[4] ), N = nx * ny;
+      ArrayType R ( nx, ny ), T ( nx, ny ), PhiX ( nx, ny );
+      readBin ( argv[5], R.getData ( ), N ); readBin ( argv[6], T.getData ( ), N );
+      readBin ( argv[7], PhiX.getData ( ), N );
+      const RectConf::InitType grid ( qc::GridSize<qc::QC_2D>::createFrom ( R ) );
+      ArrayType temSmoothed ( grid );
+      aol::Vector<RealType> tmp ( grid.getNumY() );
+      PhiX.sumInXDirectionTo ( tmp );
+      tmp /= grid.getNumX();
+      RealType energyVal = aol::NumberTrait<RealType>::Inf;
+      for ( int i = 3; i >= 0; --i ) {
+        if ( i > 0 ) {
+          qc::ModifiableKernel2d<RealType> xAveraginKernel ( 4 * i + 1 );
+          const int offset = xAveraginKernel.getOffset();
+          for ( int X = -offset; X <= offset; X++ )
+            xAveraginKernel.setValue ( X, 0, 1. / ( 2 * offset + 1 ) );
+          T.applyLinearFilterTo ( xAveraginKernel, temSmoothed );
+        } else
+          temSmoothed = T;
+        const LineEnergy EData ( grid, R, temSmoothed );
+        const aol::DerivativeWrapper<RealType, LineEnergy, aol::Vector<RealType> > DEData ( EData );
+        const qc::PixelWiseToRowWiseOp<RectConf> E ( grid, EData, DEData );
+        const aol::DerivativeWrapper<RealType, qc::PixelWiseToRowWiseOp<RectConf>, aol::Vector<RealType> > DE ( E );
+        typedef aol::GridlessGradientDescent<RealType, aol::Vector<RealType> > GDType;
+        GDType gdSolver ( grid, E, DE, maxIter );
+        gdSolver.setConfigurationFlags ( GDType::USE_NONLINEAR_CG );
+        gdSolver.applySingle ( tmp );
+        energyVal = gdSolver.getEnergyAtLastPosition();
+      }
+      PhiX.setInXDirectionFrom ( tmp );
+      writeBin ( argv[8], PhiX.getData ( ), N );
+      writeBin ( argv[9], &energyVal, 1 );
       return 0;
     }
     if ( cmd == "xshiftlap" && argc == 9 ) {

@@ -267,6 +267,17 @@ def seismic(ref: msor.RefRunner, seed: int):
     phi5 = rng.normal(0, 0.2, (5, 7))
     elap, klap = ref.xshift_reg_laplace(phi5, 1.0, 1.5)
     d.update({"phi_c": phi5, "yreg_c": 1.0, "lapw_c": 1.5, "Elap_c": elap, "Kphilap_c": klap})
+    # findXShiftYConst (forceNonDyadicXShiftYConst): one shift per line, the reference's own run
+    for tag, (nx, ny, shift, nan_line) in (("a", (33, 9, 1.3, -1)), ("b", (65, 17, -2.0, 3))):
+        x = np.arange(nx)
+        R = np.stack([np.sin(x / 4.0 + 0.3 * k) + 0.05 * rng.normal(size=nx) for k in range(ny)])
+        T = np.stack([np.sin((x - shift - 0.2 * k / ny) / 4.0 + 0.3 * k) + 0.05 * rng.normal(size=nx)
+                      for k in range(ny)])
+        if nan_line >= 0:
+            R[nan_line, :] = np.nan
+        ph0 = rng.normal(0, 0.3, (ny, nx)) / (nx - 1)
+        ph, e = ref.xshift_yconst(R, T, 60, ph0)
+        d.update({f"ycR_{tag}": R, f"ycT_{tag}": T, f"ycphi0_{tag}": ph0, f"ycphi_{tag}": ph, f"ycE_{tag}": e})
     np.savez_compressed(os.path.join(OUT, "seismic.npz"), **d)
 
 

@@ -90,3 +90,28 @@ def test_xshift_with_laplace_weight_recovers_a_line_shift(oracle):
     energies = [r[1] for r in rows]
     assert all(b <= a for a, b in zip(energies, energies[1:]))
     assert abs(ph[:, 8:-8].mean() * (nx - 1) - 1.5) < 0.1
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_xshift_yconst_bit_exact(oracle, tag):
+    """findXShiftYConst (forceNonDyadicXShiftYConst, matchSeries.h:873-920):
+    one shift per line, four gridless NCG descents against the template
+    smoothed along x; the reference's own run, bit for bit (tag b has a NaN
+    line, whose NaN also reaches the neighbouring lines of the smoothed
+    template through the filter's zero rows)."""
+    g = golden("seismic.npz")
+    ph, e, _ = oracle.xshift_yconst(g[f"ycR_{tag}"], g[f"ycT_{tag}"], 60, g[f"ycphi0_{tag}"])
+    assert e == float(g[f"ycE_{tag}"])
+    assert np.array_equal(ph, g[f"ycphi_{tag}"])
+
+
+def test_box_filter_keeps_lines_and_spreads_nan(oracle):
+    T = np.arange(5 * 11, dtype=float).reshape(5, 11)
+    T[2, 4] = np.nan
+    B = oracle.box_x(T, 1)   # 5-wide box, 5 x 5 window
+    assert np.isnan(B[0:5, 2:7]).all() and np.isfinite(B[:, 8:]).all()
+    ok = T.copy()
+    ok[2, 4] = 0.0
+    B2 = oracle.box_x(ok, 1)
+    x = 6
+    assert B2[1, x] == sum(0.2 * ok[1, (x + k) % 11] for k in range(-2, 3))
