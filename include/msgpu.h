@@ -174,6 +174,20 @@ int msgpu_find_xshift_device(msgpu_context* ctx, int nx, int ny, const double* d
                              double yreg, double laplace_weight, int max_iter, double* d_phix, double* energy_out,
                              int* steps_out, void* stream);
 
+/* findXShiftYConst (matchSeries.h:873-920), the non-dyadic solve of
+ * XShiftNonDyadicRegistrationMultilevelDescent under
+ * forceNonDyadicXShiftYConst (matchSeismicSeries.h:197-201): one shift per
+ * line, started from the line means of phix, by four gradient descents
+ * (GridlessGradientDescent, Fletcher-Reeves NCG, Armijo steps; no metric)
+ * against the template smoothed along x by boxes of 13, 9 and 5 samples and
+ * then unsmoothed, on the line-shift data term alone.  phix (nx*ny) in/out,
+ * returned constant along each line; energy_out, steps_out (nullable, host):
+ * the last descent's energy and steps.                                     */
+int msgpu_find_xshift_yconst(msgpu_context* ctx, int nx, int ny, const double* R, const double* T, int max_iter,
+                             double* phix, double* energy_out, int* steps_out);
+int msgpu_find_xshift_yconst_device(msgpu_context* ctx, int nx, int ny, const double* d_R, const double* d_T,
+                                    int max_iter, double* d_phix, double* energy_out, int* steps_out, void* stream);
+
 /* findXShift for num_images images (host buffers, back to back): R is one
  * reference for all (r_per_image = 0, e.g. the mean stack) or one per image;
  * phix in/out; energies_out, steps_out (nullable) per image.  The images are

@@ -2133,6 +2133,213 @@ int run_xshift(msgpu_context* ctx, int nx, int ny, const double* R, const double
 }
 }  // namespace
 
+namespace {
+// findXShiftYConst (matchSeries.h:873-920): one shift per line v (ny),
+// started from the line means of phix; four GridlessGradientDescent runs
+// with Fletcher-Reeves NCG (GradientDescentBase::applySingle,
+// gradientDescent.h:295-464: no smoothing, no filter widths, stop when the
+// Armijo step is 0) against the template smoothed along x by boxes of 13, 9
+// and 5 samples, then unsmoothed.  E(v) is the line-shift data term of the
+// row-constant shift and DE its derivative summed along each line, both
+// evaluated on the device (k_lineshift in row mode); the ny-long vector
+// algebra and the descent control run on the host in double.
+struct YcSolver {
+  msgpu_context* ctx;
+  int nx, ny;
+  LineArgs a;
+  double *vdev, *derow, *etot;
+  cudaStream_t st;
+  double rb_tau[2] = {NAN, NAN}, rb_e[2] = {NAN, NAN};
+  int rb_pos = 0;
+  double e_at_pos = 0;
+  std::vector<double> tx;
+
+  static double dotv(const double* x, const double* y, int n) {
+    double r = 0;
+    for (int i = 0; i < n; ++i) r += x[i] * y[i];
+    return r;
+  }
+  int eval_device(const double* v, double* e, double* de) {
+    CK(cudaMemcpyAsync(vdev, v, sizeof(double) * ny, cudaMemcpyHostToDevice, st));
+    a.de_row = de ? derow : nullptr;
+    k_lineshift<<<dim3(ny, 1), kLineThreads, sizeof(double) * 3 * (size_t)nx, st>>>(a);
+    CK(cudaGetLastError());
+    ++ctx->stats.kernel_launches;
+    CK(cudaMemcpyAsync(e, etot, sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (de) CK(cudaMemcpyAsync(de, derow, sizeof(double) * ny, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return MSGPU_OK;
+  }
+  int eval(const double* p, const double* d, double tw, double* e) {
+    if (tw == 0) { *e = e_at_pos; return MSGPU_OK; }
+    for (int i = 0; i < ny; ++i) { tx[i] = p[i]; tx[i] += tw * d[i]; }
+    int rc;
+    if ((rc = eval_device(tx.data(), e, nullptr))) return rc;
+    rb_tau[rb_pos] = tw;
+    rb_e[rb_pos] = *e;
+    rb_pos ^= 1;
+    return MSGPU_OK;
+  }
+  // getTimestepWidthWithArmijoLineSearch (ArmijoSearch.h:118-200)
+  int armijo(const double* p, const double* d, const double* DE, double old_tau, double* out) {
+    const double sg = 0.5, tau_min = std::pow(2., -30.), tau_max = std::pow(2., 25.);
+    double tau = old_tau < tau_min ? tau_min : (old_tau > tau_max ? tau_max : old_tau);
+    double f, fnew;
+    int rc;
+    if ((rc = eval(p, d, 0., &f)) || (rc = eval(p, d, tau, &fnew))) return rc;
+    const double Df = dotv(DE, d, ny);
+    double G = (fnew - f) / (Df * tau);
+    if (Df >= 0 || !std::isfinite(f)) { *out = 0; return MSGPU_OK; }
+    if (G >= sg && f >= fnew) {
+      do {
+        tau *= 2.;
+        if ((rc = eval(p, d, tau, &fnew))) return rc;
+        G = (fnew - f) / (Df * tau);
+      } while (G >= sg && f >= fnew && tau <= tau_max);
+      tau *= 0.5;
+    } else {
+      do {
+        if (tau > tau_min) tau *= 0.5;
+        if ((rc = eval(p, d, tau, &fnew))) return rc;
+        G = (fnew - f) / (Df * tau);
+      } while ((!std::isfinite(fnew) || (G < sg || f < fnew)) && (tau > tau_min));
+    }
+    *out = (tau > tau_min) ? tau : 0.;
+    return MSGPU_OK;
+  }
+};
+
+int run_xshift_yconst(msgpu_context* ctx, int nx, int ny, const double* R, const double* T, int max_iter,
+                      double* phix, double* energy_out, int* steps_out, cudaStream_t st) {
+  const size_t N = (size_t)nx * ny;
+  int rc;
+  if ((rc = ensure(ctx, ctx->xs_work, sizeof(double) * (2 * N + 3 * (size_t)ny + 64)))) return rc;
+  double* w = (double*)ctx->xs_work.p;
+  double* Ts = w;
+  double* nr = w + N;
+  YcSolver S;
+  S.ctx = ctx; S.nx = nx; S.ny = ny; S.st = st;
+  S.vdev = w + 2 * N;
+  S.derow = S.vdev + ny;
+  double* eline = S.derow + ny;
+  S.etot = eline + ny;
+  unsigned* done = (unsigned*)(S.etot + 8);
+  S.tx.assign(ny, 0.);
+  CK(cudaMemsetAsync(done, 0, sizeof(unsigned), st));
+  const LineTables lt = host_line_tables(nx);
+  const size_t smem = sizeof(double) * 3 * (size_t)nx;
+  CK(cudaFuncSetAttribute(k_lineshift, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(cudaFuncSetAttribute(k_lineshift_prep_ref, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_lineshift_prep_ref<<<dim3(ny, 1), kLineThreads, smem, st>>>(R, nx, N, lt, nr);
+  memset(&S.a, 0, sizeof(S.a));
+  S.a.nx = nx; S.a.ny = ny; S.a.img_stride = N; S.a.R = R; S.a.T = Ts; S.a.phi = S.vdev;
+  S.a.e_line = eline; S.a.t = lt; S.a.nr_pre = nr; S.a.done = done; S.a.e_total = S.etot;
+  S.a.phi_row = S.vdev;
+  ++ctx->stats.kernel_launches;
+  // the line means of phix (sumInXDirectionTo, then / numX)
+  std::vector<double> ph(N), v(ny), d(ny), og(ny), od(ny), DE(ny);
+  CK(cudaMemcpyAsync(ph.data(), phix, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  for (int y = 0; y < ny; ++y) {
+    double sum = 0.;
+    for (int x = 0; x < nx; ++x) sum += ph[(size_t)y * nx + x];
+    v[y] = sum;
+  }
+  for (int y = 0; y < ny; ++y) v[y] /= (double)nx;
+  double energy_new = INFINITY;
+  int iter = 0;
+  for (int round = 3; round >= 0; --round) {
+    if (round > 0) {
+      k_box_x<<<(unsigned)std::min<size_t>(2048, (N + 255) / 256), 256, 0, st>>>(T, nx, ny, 2 * round, Ts);
+      ++ctx->stats.kernel_launches;
+    } else {
+      CK(cudaMemcpyAsync(Ts, T, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+    }
+    S.rb_tau[0] = S.rb_tau[1] = NAN;
+    S.rb_pos = 0;
+    std::fill(og.begin(), og.end(), 0.);
+    std::fill(od.begin(), od.end(), 0.);
+    double tau = 1.0, energy;
+    if ((rc = S.eval_device(v.data(), &energy, nullptr))) return rc;
+    energy_new = energy;
+    iter = 0;
+    bool go = max_iter > 0;
+    while (go) {
+      iter++;
+      energy = energy_new;
+      S.e_at_pos = energy;
+      double e_pos;
+      if ((rc = S.eval_device(v.data(), &e_pos, DE.data()))) return rc;
+      for (int i = 0; i < ny; ++i) d[i] = DE[i] * -1.;
+      double beta = 0.;
+      if ((iter - 1) % 10) beta = YcSolver::dotv(d.data(), d.data(), ny) / YcSolver::dotv(og.data(), og.data(), ny);
+      og = d;
+      for (int i = 0; i < ny; ++i) d[i] += beta * od[i];
+      od = d;
+      if ((rc = S.armijo(v.data(), d.data(), DE.data(), tau, &tau))) return rc;
+      for (int i = 0; i < ny; ++i) d[i] *= tau;
+      if (tau == 0) {
+        d = og;
+        std::fill(od.begin(), od.end(), 0.);
+        if ((rc = S.armijo(v.data(), d.data(), DE.data(), tau, &tau))) return rc;
+        for (int i = 0; i < ny; ++i) d[i] *= tau;
+      }
+      double enew = NAN;
+      if (S.rb_tau[0] == tau) enew = S.rb_e[0];
+      else if (S.rb_tau[1] == tau) enew = S.rb_e[1];
+      else if (tau == 0) enew = energy;
+      if (tau != 0)
+        for (int i = 0; i < ny; ++i) v[i] += d[i];
+      if (std::isnan(enew) && (rc = S.eval_device(v.data(), &enew, nullptr))) return rc;
+      energy_new = enew;
+      go = ((energy - energy_new) > 0.) && (iter < max_iter);
+      if (tau == 0) go = false;
+    }
+  }
+  for (int y = 0; y < ny; ++y)
+    for (int x = 0; x < nx; ++x) ph[(size_t)y * nx + x] = v[y];
+  CK(cudaMemcpyAsync(phix, ph.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st));
+  if (energy_out) *energy_out = energy_new;
+  if (steps_out) *steps_out = iter;
+  return MSGPU_OK;
+}
+}  // namespace
+
+int msgpu_find_xshift_yconst_device(msgpu_context* ctx, int nx, int ny, const double* d_R, const double* d_T,
+                                    int max_iter, double* d_phix, double* energy_out, int* steps_out, void* stream) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (nx < 3 || ny < 1 || max_iter < 0 || !d_R || !d_T || !d_phix)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid find_xshift_yconst arguments (lines of at least 3 samples)");
+  if (sizeof(double) * 3 * (size_t)nx > 200 * 1024)
+    return fail(ctx, MSGPU_ERR_SIZE, "lines of %d samples do not fit shared memory", nx);
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  ctx->stats.kernel_launches = 0;
+  return run_xshift_yconst(ctx, nx, ny, d_R, d_T, max_iter, d_phix, energy_out, steps_out, (cudaStream_t)stream);
+}
+
+int msgpu_find_xshift_yconst(msgpu_context* ctx, int nx, int ny, const double* R, const double* T, int max_iter,
+                             double* phix, double* energy_out, int* steps_out) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (!R || !T || !phix) return fail(ctx, MSGPU_ERR_INVALID_ARG, "null buffer");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  const size_t N = (size_t)nx * ny;
+  if ((rc = ensure(ctx, ctx->io[0], sizeof(double) * 3 * N))) return rc;
+  double* dd = (double*)ctx->io[0].p;
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(dd, R, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dd + N, T, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dd + 2 * N, phix, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+  if ((rc = msgpu_find_xshift_yconst_device(ctx, nx, ny, dd, dd + N, max_iter, dd + 2 * N, energy_out, steps_out,
+                                            st)))
+    return rc;
+  CK(cudaMemcpyAsync(phix, dd + 2 * N, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return MSGPU_OK;
+}
+
 int msgpu_find_xshift_device(msgpu_context* ctx, int nx, int ny, const double* d_R, const double* d_T, double lambda,
                              double yreg, double laplace_weight, int max_iter, double* d_phix, double* energy_out,
                              int* steps_out, void* stream) {

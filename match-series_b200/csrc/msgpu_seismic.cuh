@@ -39,6 +39,8 @@ struct LineArgs {
   double* de;                  // nullable: nx*ny per image
   LineTables t;
   const double* nr_pre;        // nullable: the reference lines already normalised (k_lineshift_prep_ref)
+  const double* phi_row;       // nullable: one shift per line (phi = phi_row[y] on the whole line)
+  double* de_row;              // nullable (with phi_row): the derivative summed along each line, in x order
   unsigned* done;              // nullable: per-image line counter; the last line's CTA writes the total
   double* e_total;             // one per image (with done): mean of the line energies in line order
 };
@@ -146,7 +148,8 @@ __global__ void __launch_bounds__(kLineThreads) k_lineshift(LineArgs a) {
   const size_t base = (size_t)blockIdx.y * a.img_stride + (size_t)y * n;
   const double* R = a.R + base;
   const double* T = a.T + base;
-  const double* phi = a.phi + base;
+  const double* phi = a.phi_row ? nullptr : a.phi + base;
+  const double prow = a.phi_row ? a.phi_row[(size_t)blockIdx.y * a.ny + y] : 0.0;
   double* nr = lsm;            // normalised reference line
   double* nt = lsm + n;        // deformed, then normalised template line
   double* tmp = lsm + 2 * n;   // (M nt), then the force weights
@@ -155,13 +158,14 @@ __global__ void __launch_bounds__(kLineThreads) k_lineshift(LineArgs a) {
     if (threadIdx.x == 0) a.e_line[(size_t)blockIdx.y * a.ny + y] = 0.0;
     if (a.de)
       for (int i = threadIdx.x; i < n; i += kLineThreads) a.de[base + i] = 0.0;
+    if (a.de_row && threadIdx.x == 0) a.de_row[(size_t)blockIdx.y * a.ny + y] = 0.0;
     line_total(a, lsm, 3 * n);
     return;
   }
   for (int i = threadIdx.x; i < n; i += kLineThreads) {
     nr[i] = a.nr_pre ? a.nr_pre[base + i] : R[i];
     // doFastDeformImage<., QC_1D> (deformations.h:111-137), Vector::interpolate (vec.h:461-472)
-    double ds = i + phi[i] / t.h;
+    double ds = i + (phi ? phi[i] : prow) / t.h;
     ds = ds < 0. ? 0. : (ds > (double)(n - 1) ? (double)(n - 1) : ds);
     const int p = (int)ds;
     const double pf = ds - p;
@@ -174,7 +178,7 @@ __global__ void __launch_bounds__(kLineThreads) k_lineshift(LineArgs a) {
   for (int i = threadIdx.x; i < n; i += kLineThreads) part += line_mass_row(t, nt, i, n) * nr[i];
   const double energy = -line_block_sum(part, red);
   if (threadIdx.x == 0) a.e_line[(size_t)blockIdx.y * a.ny + y] = energy;
-  if (!a.de) {
+  if (!a.de && !a.de_row) {
     line_total(a, lsm, 3 * n);
     return;
   }
@@ -193,8 +197,8 @@ __global__ void __launch_bounds__(kLineThreads) k_lineshift(LineArgs a) {
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
       double off = 0.;
-      off += phi[e] * t.bq[0][q];
-      off += phi[e + 1] * t.bq[1][q];
+      off += (phi ? phi[e] : prow) * t.bq[0][q];
+      off += (phi ? phi[e + 1] : prow) * t.bq[1][q];
       const double tc = ((double)e + t.g[q]) + off / t.h;
       int el = (short)tc;
       double loc = tc - el;
@@ -222,7 +226,17 @@ __global__ void __launch_bounds__(kLineThreads) k_lineshift(LineArgs a) {
     if (i > 0) d += elem(i - 1, 1);
     if (i < n - 1) d += elem(i, 0);
     d /= a.ny;
-    a.de[base + i] = d;
+    if (a.de) a.de[base + i] = d;
+    if (a.de_row) nr[i] = d;   // nr is free once tmp holds the force weights
+  }
+  if (a.de_row) {
+    // ScalarArray<QC_2D>::sumInXDirectionTo (scalarArray.h:1395-1402): from 0, in x order
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double sum = 0.;
+      for (int i = 0; i < n; ++i) sum += nr[i];
+      a.de_row[(size_t)blockIdx.y * a.ny + y] = sum;
+    }
   }
   line_total(a, lsm, 3 * n);
 }
@@ -399,6 +413,30 @@ __global__ void __launch_bounds__(256) k_xshift_reg_lap(XLapTables tb, int nx, i
     for (int w = 0; w < 8; ++w) t += red2[w];
     e_total[blockIdx.y] = 0.5 * t;
     done[blockIdx.y] = 0u;
+  }
+}
+
+// The template smoothed along x for findXShiftYConst (matchSeries.h:886-896):
+// ScalarArray<QC_2D>::applyLinearFilterTo with a (2o+1) x (2o+1) kernel whose
+// middle row is 1/(2o+1) and the other rows 0 (scalarArray.cpp:936-965: the
+// whole window in row order, periodic outside the array, so the zero rows
+// still carry a NaN or Inf of their pixels).
+__global__ void k_box_x(const double* T, int nx, int ny, int o, double* out) {
+  const double k = 1. / (double)(2 * o + 1);
+  const int N = nx * ny;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < N; r += gridDim.x * blockDim.x) {
+    const int x = r % nx, y = r / nx;
+    double val = 0.0;
+    for (int oy = -o; oy <= o; ++oy) {
+      int Y = y + oy;
+      if (Y < 0) Y += ny; else if (Y > ny - 1) Y = Y % ny;
+      for (int ox = -o; ox <= o; ++ox) {
+        int X = x + ox;
+        if (X < 0) X += nx; else if (X > nx - 1) X = X % nx;
+        val += (oy == 0 ? k : 0.0) * T[(size_t)Y * nx + X];
+      }
+    }
+    out[r] = val;
   }
 }
 

@@ -96,7 +96,7 @@ EXPORTS = [
     "msgpu_net_num_params", "msgpu_net_create", "msgpu_net_destroy", "msgpu_net_input_level", "msgpu_net_get_params",
     "msgpu_net_set_params", "msgpu_net_save", "msgpu_net_load", "msgpu_net_predict_device",
     "msgpu_net_train_step_device", "msgpu_net_loss_grad", "msgpu_prepare_images_device", "msgpu_register_batch_warm",
-    "msgpu_register_batch_warm_device",
+    "msgpu_register_batch_warm_device", "msgpu_find_xshift_yconst", "msgpu_find_xshift_yconst_device",
 ]
 
 
@@ -196,6 +196,11 @@ def lib():
         L.msgpu_find_xshift_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                                ctypes.c_void_p, _d, _d, _d, ctypes.c_int, ctypes.c_void_p, _dp, _ip,
                                                ctypes.c_void_p]
+        L.msgpu_find_xshift_yconst.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp, ctypes.c_int,
+                                               _dp, _dp, _ip]
+        L.msgpu_find_xshift_yconst_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                                      ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, _dp, _ip,
+                                                      ctypes.c_void_p]
         L.msgpu_find_xshift_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp,
                                               ctypes.c_int, _dp, _d, _d, _d, ctypes.c_int, _dp, _dp, _ip, ctypes.c_int]
         L.msgpu_register_ragged.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params), ctypes.POINTER(SeriesDesc),
@@ -456,6 +461,17 @@ class Context:
         self._check(lib().msgpu_find_xshift(self._h, nx, ny, _p(R), _p(_f64(T)), float(lam), float(yreg),
                                             float(laplace_weight),
                                             int(max_iter), _p(ph), ctypes.byref(e), ctypes.byref(steps)))
+        return ph, e.value, steps.value
+
+    def find_xshift_yconst(self, R, T, max_iter=500, phix=None):
+        """findXShiftYConst: returns (phix (ny, nx), one value per line; energy; steps of the last descent)."""
+        R = _f64(R)
+        ny, nx = R.shape
+        ph = np.zeros((ny, nx)) if phix is None else _f64(phix).copy()
+        e = ctypes.c_double()
+        steps = ctypes.c_int()
+        self._check(lib().msgpu_find_xshift_yconst(self._h, nx, ny, _p(R), _p(_f64(T)), int(max_iter), _p(ph),
+                                                   ctypes.byref(e), ctypes.byref(steps)))
         return ph, e.value, steps.value
 
     def find_xshift_batch(self, R, T, lam, yreg, max_iter=500, phix=None, workers=4, laplace_weight=0.0):

@@ -120,3 +120,18 @@ def test_laplace_weight_needs_five_nodes(gpu):
     import msgpu
     with pytest.raises(msgpu.MsgpuError, match="5 x 5"):
         gpu.xshift_reg(np.zeros((4, 9)), 1.0, 0.5)
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_find_xshift_yconst_matches_reference(gpu, tag):
+    """findXShiftYConst on the GPU (line-shift kernel in row mode, control
+    on the host) against the reference's own run: the same iterates, so the
+    shifts and the energy agree to rounding of the device sums."""
+    g = golden("seismic.npz")
+    R, T = g[f"ycR_{tag}"], g[f"ycT_{tag}"]
+    nx = R.shape[1]
+    ph, e, steps = gpu.find_xshift_yconst(R, T, 60, g[f"ycphi0_{tag}"])
+    ref = g[f"ycphi_{tag}"]
+    assert np.all(ph == ph[:, :1])
+    assert np.abs(ph - ref).max() * (nx - 1) <= 1e-9
+    assert abs(e - float(g[f"ycE_{tag}"])) <= 1e-12 * abs(float(g[f"ycE_{tag}"]))
