@@ -3186,23 +3186,26 @@ int net_buffers(msgpu_net* net, int batch) {
   return MSGPU_OK;
 }
 
+// 16-channel outputs: 16 rows per block (four m16 tiles per warp), wider: 8 rows
 template <int BN, int CIN>
 void net_launch_halo(const msg::unet::ConvArgs& a, int images, int rows, cudaStream_t st) {
   namespace u = msg::unet;
-  const int tiles = ((a.out_n + u::kHaloY - 1) / u::kHaloY) * ((a.out_n + u::kHaloX - 1) / u::kHaloX);
+  constexpr int MT = BN == 16 ? 4 : 2;
+  const int ty = 4 * MT;
+  const int tiles = ((a.out_n + ty - 1) / ty) * ((a.out_n + u::kHaloX - 1) / u::kHaloX);
   const dim3 grid((unsigned)(images * tiles), (unsigned)(rows / BN));
-  u::k_conv_halo<BN, CIN><<<grid, u::kThreads, u::conv_halo_smem_bytes<BN, CIN>(), st>>>(a);
+  u::k_conv_halo<BN, CIN, MT><<<grid, u::kThreads, u::conv_halo_smem_bytes<BN, CIN, MT>(), st>>>(a);
 }
 
 // shared-memory limits of the halo kernels (above the 48 KB default for the widest)
 int net_kernel_attrs(msgpu_context* ctx) {
   namespace u = msg::unet;
-  CK(cudaFuncSetAttribute(u::k_conv_halo<64, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)u::conv_halo_smem_bytes<64, 32>()));
-  CK(cudaFuncSetAttribute(u::k_conv_halo<64, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)u::conv_halo_smem_bytes<64, 16>()));
-  CK(cudaFuncSetAttribute(u::k_conv_halo<32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)u::conv_halo_smem_bytes<32, 32>()));
+  CK(cudaFuncSetAttribute(u::k_conv_halo<64, 32, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)u::conv_halo_smem_bytes<64, 32, 2>()));
+  CK(cudaFuncSetAttribute(u::k_conv_halo<64, 16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)u::conv_halo_smem_bytes<64, 16, 2>()));
+  CK(cudaFuncSetAttribute(u::k_conv_halo<32, 32, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)u::conv_halo_smem_bytes<32, 32, 2>()));
   return MSGPU_OK;
 }
 

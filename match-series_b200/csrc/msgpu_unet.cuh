@@ -246,24 +246,25 @@ constexpr size_t conv_smem_bytes() {
 
 // Stride-1 convolution (forward, or the data gradient with transposed
 // weights) of CIN = 16 or 32 input channels from a halo tile: a block
-// computes 8 x 16 output nodes of one image (each warp two rows of 16, one
-// m16 tile per row) x BN channels.  The (8+2) x (16+2) input nodes and all 9
+// computes (4 MT) x 16 output nodes of one image (each warp MT rows of 16,
+// one m16 tile per row) x BN channels.  The (4MT+2) x (16+2) input nodes and all 9
 // taps' weights are staged once in shared memory; every tap's A fragment is
 // read by ldmatrix straight from the halo rows (consecutive nodes of a row,
 // conflict-free), so each input node is fetched once instead of once per
 // tap.  The mma sequence over (tap, channel) is the one k_conv issues, so
 // both give the same results.
-constexpr int kHaloY = 8, kHaloX = 16;
+constexpr int kHaloX = 16;
 template <int CIN>
 __host__ __device__ constexpr int halo_stride() { return CIN + 8; }
-template <int BN, int CIN>
+template <int BN, int CIN, int MT>
 constexpr size_t conv_halo_smem_bytes() {
-  return sizeof(bf16) * ((size_t)(kHaloY + 2) * (kHaloX + 2) * halo_stride<CIN>() + (size_t)9 * BN * halo_stride<CIN>());
+  return sizeof(bf16) * ((size_t)(4 * MT + 2) * (kHaloX + 2) * halo_stride<CIN>() + (size_t)9 * BN * halo_stride<CIN>());
 }
 
-template <int BN, int CIN>
+template <int BN, int CIN, int MT>
 __global__ void __launch_bounds__(kThreads) k_conv_halo(ConvArgs a) {
   constexpr int HS = halo_stride<CIN>();
+  constexpr int kHaloY = 4 * MT;
   constexpr int HW = kHaloX + 2, HH = kHaloY + 2;
   extern __shared__ __align__(16) unsigned char halo_smem[];
   bf16* H = reinterpret_cast<bf16*>(halo_smem);   // [HH][HW][HS]
@@ -293,9 +294,9 @@ __global__ void __launch_bounds__(kThreads) k_conv_halo(ConvArgs a) {
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
-  float acc[2][BN / 8][4];
+  float acc[MT][BN / 8][4];
 #pragma unroll
-  for (int m = 0; m < 2; ++m)
+  for (int m = 0; m < MT; ++m)
 #pragma unroll
     for (int j = 0; j < BN / 8; ++j)
 #pragma unroll
@@ -307,10 +308,10 @@ __global__ void __launch_bounds__(kThreads) k_conv_halo(ConvArgs a) {
     const int dy = sgn * (tap / 3 - 1), dx = sgn * (tap % 3 - 1);
 #pragma unroll
     for (int kk = 0; kk < CIN; kk += 16) {
-      uint32_t af[2][4];
+      uint32_t af[MT][4];
 #pragma unroll
-      for (int m = 0; m < 2; ++m) {
-        const int hy = 2 * warp + m + 1 + dy, hx = a_x + 1 + dx;
+      for (int m = 0; m < MT; ++m) {
+        const int hy = MT * warp + m + 1 + dy, hx = a_x + 1 + dx;
         ldsm_x4(af[m], H + ((size_t)hy * HW + hx) * HS + kk + a_col);
       }
 #pragma unroll
@@ -318,7 +319,7 @@ __global__ void __launch_bounds__(kThreads) k_conv_halo(ConvArgs a) {
         uint32_t bf[4];
         ldsm_x4(bf, W + ((size_t)tap * BN + j * 8 + b_row) * HS + kk + b_col);
 #pragma unroll
-        for (int m = 0; m < 2; ++m) {
+        for (int m = 0; m < MT; ++m) {
           mma_bf16(acc[m][j], af[m], bf[0], bf[1]);
           mma_bf16(acc[m][j + 1], af[m], bf[2], bf[3]);
         }
@@ -328,10 +329,10 @@ __global__ void __launch_bounds__(kThreads) k_conv_halo(ConvArgs a) {
   const int outN2 = a.out_n * a.out_n;
   (void)outN2;
 #pragma unroll
-  for (int m = 0; m < 2; ++m)
+  for (int m = 0; m < MT; ++m)
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const int oy = ty0 + 2 * warp + m, ox = tx0 + (lane >> 2) + 8 * h;
+      const int oy = ty0 + MT * warp + m, ox = tx0 + (lane >> 2) + 8 * h;
       if (oy >= a.out_n || ox >= a.out_n) continue;
       const int q = oy * a.out_n + ox;
       const size_t ob = (size_t)img * a.out_img + (size_t)q * a.out_cs;
