@@ -195,6 +195,9 @@ int ensure_tables(msgpu_context* ctx) {
   FeTables t;
   host_fe_tables(t);
   CK(cudaMemcpyToSymbol(c_fe, &t, sizeof(t)));
+  // a copy from pageable memory may return before it lands; the kernels that
+  // read the tables run on non-blocking streams, which do not wait for it
+  CK(cudaDeviceSynchronize());
   if (dev < 64) g_tables_ready[dev] = true;
   return MSGPU_OK;
 }
@@ -1903,7 +1906,7 @@ int xs_setup(msgpu_context* ctx, int nx, int ny, XsBufs& B, cudaStream_t st) {
     host_spectral_basis(ny, h, Vy, lx + nx);
     for (int r = 0; r < ne; ++r) lx[r] = lxf[2 * r];
     for (int r = 0; r < no; ++r) lx[ne + r] = lxf[2 * r + 1];
-    CK(cudaMemcpy(B.Ve, hb.data(), sizeof(double) * nb, cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(B.Ve, hb.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, st));
     ctx->xs_nx = nx;
     ctx->xs_ny = ny;
   }
@@ -2978,6 +2981,8 @@ int noalloc_setup(int dev, NoAllocDevice** out) {
     FeTables t;
     host_fe_tables(t);
     if (cudaMemcpyToSymbol(c_fe, &t, sizeof(t)) != cudaSuccess) return MSGPU_ERR_CUDA;
+    // the upload must have landed before kernels on the caller's stream read it
+    if (cudaDeviceSynchronize() != cudaSuccess) return MSGPU_ERR_CUDA;
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
       return MSGPU_ERR_CUDA;
@@ -3157,7 +3162,7 @@ int net_pack(msgpu_net* net, cudaStream_t st) {
 }
 
 // Activation buffers for `batch` images.
-int net_buffers(msgpu_net* net, int batch) {
+int net_buffers(msgpu_net* net, int batch, cudaStream_t st) {
   if (batch <= net->batch) return MSGPU_OK;
   const size_t N[4] = {(size_t)net->n[0] * net->n[0], (size_t)net->n[1] * net->n[1], (size_t)net->n[2] * net->n[2],
                        (size_t)net->n[3] * net->n[3]};
@@ -3181,7 +3186,7 @@ int net_buffers(msgpu_net* net, int batch) {
   }
   net->out = (float*)p;
   // zero once: padding channels of the input and of the loss gradient stay zero
-  NCK(cudaMemset(net->act.p, 0, total * sizeof(bf16) + out_floats * sizeof(float)));
+  NCK(cudaMemsetAsync(net->act.p, 0, total * sizeof(bf16) + out_floats * sizeof(float), st));
   net->batch = batch;
   return MSGPU_OK;
 }
@@ -3382,7 +3387,7 @@ int net_backward(msgpu_net* net, int B, cudaStream_t st) {
 int net_input(msgpu_net* net, const double* R, size_t r_stride, const double* T, size_t t_stride, int B,
               cudaStream_t st) {
   int rc;
-  if ((rc = net_buffers(net, B))) return rc;
+  if ((rc = net_buffers(net, B, st))) return rc;
   const size_t total = (size_t)B * net->n[0] * net->n[0];
   msg::unet::k_pack_input<<<(unsigned)std::min<size_t>(4096, (total + 255) / 256), 256, 0, st>>>(
       R, r_stride, T, t_stride, net->n[0] * net->n[0], B, net->x0.p);
@@ -3457,9 +3462,10 @@ void net_init_host(const msgpu_net* net, unsigned long long seed, std::vector<fl
 }
 
 int net_set_params_dev(msgpu_net* net, const float* host) {
-  NCK(cudaMemcpy(net->theta, host, sizeof(float) * net->nparams, cudaMemcpyHostToDevice));
-  NCK(cudaMemset(net->m, 0, sizeof(float) * net->nparams));
-  NCK(cudaMemset(net->v, 0, sizeof(float) * net->nparams));
+  const cudaStream_t st = net->ctx->stream;
+  NCK(cudaMemcpyAsync(net->theta, host, sizeof(float) * net->nparams, cudaMemcpyHostToDevice, st));
+  NCK(cudaMemsetAsync(net->m, 0, sizeof(float) * net->nparams, st));
+  NCK(cudaMemsetAsync(net->v, 0, sizeof(float) * net->nparams, st));
   net->step = 0;
   int rc;
   if ((rc = net_pack(net, net->ctx->stream))) return rc;
@@ -3620,7 +3626,7 @@ int msgpu_net_get_params(msgpu_net* net, float* out) {
   if (!net || !out) return MSGPU_ERR_INVALID_ARG;
   int rc;
   if ((rc = bind_device(net->ctx))) return rc;
-  NCK(cudaStreamSynchronize(net->ctx->stream));
+  NCK(cudaDeviceSynchronize());   // training steps may have run on any stream
   NCK(cudaMemcpy(out, net->theta, sizeof(float) * net->nparams, cudaMemcpyDeviceToHost));
   return MSGPU_OK;
 }
