@@ -3387,6 +3387,10 @@ int net_backward(msgpu_net* net, int B, cudaStream_t st) {
 int net_input(msgpu_net* net, const double* R, size_t r_stride, const double* T, size_t t_stride, int B,
               cudaStream_t st) {
   int rc;
+  // the kernels index nodes of the whole batch with 32-bit integers
+  if ((double)B * net->n[0] * net->n[0] * 16.0 > 2147483647.0)
+    return fail(net->ctx, MSGPU_ERR_SIZE, "a batch of %d images of %d^2 nodes is too large for one network pass", B,
+                net->n[0]);
   if ((rc = net_buffers(net, B, st))) return rc;
   const size_t total = (size_t)B * net->n[0] * net->n[0];
   msg::unet::k_pack_input<<<(unsigned)std::min<size_t>(4096, (total + 255) / 256), 256, 0, st>>>(
