@@ -3126,7 +3126,7 @@ struct msgpu_net {
   bf16 *wf = nullptr, *wt = nullptr;
   long long step = 0;
   int batch = 0;                         // images the activation buffers hold
-  msgpu_context::Buf act, part, small, phi, gather;
+  msgpu_context::Buf act, part, small, phi, gather, phiall;
   // activations and their gradients (views into act)
   View x0, a0, a1, b0, cat1, c0, cat2, d0, d1, g0, g1, h0, h1;
   View dout, dh1, dh0, dcat1, dg1, dg0, dcat2, dd1, dd0, dc0, db0, da1, da0;
@@ -3483,7 +3483,20 @@ int net_set_params_dev(msgpu_net* net, const float* host) {
 int warm_start_phi(msgpu_net* net, const double* pyr, const std::vector<size_t>& poff, size_t pstride, int F,
                    cudaStream_t st, double** phi) {
   const int l0 = net->level;
-  return net_predict(net, pyr + poff[l0], 0, pyr + pstride + poff[l0], pstride, F, st, phi);
+  const size_t N1 = (size_t)net->n[1] * net->n[1];
+  int rc;
+  if ((rc = ensure(net->ctx, net->phiall, sizeof(double) * 2 * N1 * F))) return rc;
+  double* all = (double*)net->phiall.p;
+  // at most 64 frames per network pass (activation memory and 32-bit node indices)
+  for (int f0 = 0; f0 < F; f0 += 64) {
+    const int m = std::min(64, F - f0);
+    double* part;
+    if ((rc = net_predict(net, pyr + poff[l0], 0, pyr + (size_t)(1 + f0) * pstride + poff[l0], pstride, m, st, &part)))
+      return rc;
+    NCK(cudaMemcpyAsync(all + 2 * N1 * f0, part, sizeof(double) * 2 * N1 * m, cudaMemcpyDeviceToDevice, st));
+  }
+  *phi = all;
+  return MSGPU_OK;
 }
 
 // msgpu_register_batch_warm_device; warm_used (host, nullable).
@@ -3618,7 +3631,7 @@ int msgpu_net_destroy(msgpu_net* net) {
   cudaSetDevice(net->ctx->device);
   cudaFree(net->theta);
   cudaFree(net->wf);
-  for (msgpu_context::Buf* b : {&net->act, &net->part, &net->small, &net->phi, &net->gather})
+  for (msgpu_context::Buf* b : {&net->act, &net->part, &net->small, &net->phi, &net->gather, &net->phiall})
     if (b->p) cudaFree(b->p);
   delete net;
   return MSGPU_OK;

@@ -180,3 +180,22 @@ def test_warm_batch_and_fallback(gpu):
     with pytest.raises(msgpu.MsgpuError, match="network input level"):
         gpu.register_batch_warm(bad, net, ref, tm)
     net.close()
+
+
+def test_warm_batch_larger_than_one_network_pass(gpu):
+    """70 frames: the prediction runs in passes of 64; every frame's result
+    equals the one it gets in a batch of 5 (neither the network nor the
+    registration depends on the batch a frame is in)."""
+    import msgpu
+    from msgpu import synthetic as syn
+    lvl = 5
+    n = (1 << lvl) + 1
+    frames, _, _ = syn.make_series(n, 71, syn.SQUARE_257, seed=77)
+    p = msgpu.default_params(precision_level=lvl, input_level=lvl, start_level=2, stop_level=lvl,
+                             max_gd_iterations=5, use_fp64=1)
+    net = msgpu.Net(gpu, 5, seed=9)   # predicts level 4
+    ph, e, _, _ = gpu.register_batch_warm(p, net, frames[0], frames[1:])
+    for f0 in (0, 63, 65):
+        ph5, e5, _, _ = gpu.register_batch_warm(p, net, frames[0], frames[1 + f0:6 + f0])
+        assert np.array_equal(ph5, ph[f0:f0 + 5]) and np.array_equal(e5, e[f0:f0 + 5])
+    net.close()
