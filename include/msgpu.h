@@ -174,6 +174,17 @@ int msgpu_find_xshift_device(msgpu_context* ctx, int nx, int ny, const double* d
                              double yreg, double laplace_weight, int max_iter, double* d_phix, double* energy_out,
                              int* steps_out, void* stream);
 
+/* replaceEmptyLinesWithNaN (matchSeismicSeries.h:141-157), which
+ * XShiftNonDyadicRegistrationMultilevelDescent applies to its reference and
+ * template before the non-dyadic solve (matchSeismicSeries.h:179-185,
+ * 211-228): every line of the num_images images (nx*ny each, back to back)
+ * whose squared norm is 0 is overwritten in place by quiet NaNs, so that the
+ * line-shift data term skips it (registration.h:2150-2151).  replaced_out
+ * (nullable, host): the number of lines replaced.                          */
+int msgpu_empty_lines_to_nan(msgpu_context* ctx, int nx, int ny, int num_images, double* img, int* replaced_out);
+int msgpu_empty_lines_to_nan_device(msgpu_context* ctx, int nx, int ny, int num_images, double* d_img,
+                                    int* replaced_out, void* stream);
+
 /* findXShiftYConst (matchSeries.h:873-920), the non-dyadic solve of
  * XShiftNonDyadicRegistrationMultilevelDescent under
  * forceNonDyadicXShiftYConst (matchSeismicSeries.h:197-201): one shift per

@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <climits>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -2428,6 +2429,51 @@ int msgpu_find_xshift_batch(msgpu_context* ctx, int nx, int ny, int num_images, 
   ctx->stats.kernel_launches = launches;
   for (int t = 0; t < nw; ++t)
     if (codes[t]) return fail(ctx, codes[t], "%s", msgs[t].c_str());
+  return MSGPU_OK;
+}
+
+int msgpu_empty_lines_to_nan_device(msgpu_context* ctx, int nx, int ny, int num_images, double* d_img,
+                                    int* replaced_out, void* stream) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (nx < 1 || ny < 1 || num_images < 1 || !d_img)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid empty_lines_to_nan arguments");
+  if ((size_t)ny * num_images > (size_t)INT_MAX)
+    return fail(ctx, MSGPU_ERR_SIZE, "%d images of %d lines exceed the grid", num_images, ny);
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  ctx->stats.kernel_launches = 0;
+  cudaStream_t st = (cudaStream_t)stream;
+  int* cnt = nullptr;
+  if (replaced_out) {
+    if ((rc = ensure(ctx, ctx->io[5], 64))) return rc;
+    cnt = (int*)ctx->io[5].p;
+    CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
+  }
+  msg::k_empty_lines_nan<<<ny * num_images, 256, 0, st>>>(d_img, nx, cnt);
+  CK(cudaGetLastError());
+  ctx->stats.kernel_launches = 1;
+  if (replaced_out) {
+    CK(cudaMemcpyAsync(replaced_out, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+  }
+  return MSGPU_OK;
+}
+
+int msgpu_empty_lines_to_nan(msgpu_context* ctx, int nx, int ny, int num_images, double* img, int* replaced_out) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (!img) return fail(ctx, MSGPU_ERR_INVALID_ARG, "null buffer");
+  if (nx < 1 || ny < 1 || num_images < 1)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid empty_lines_to_nan arguments");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  const size_t N = (size_t)nx * ny * num_images;
+  if ((rc = ensure(ctx, ctx->io[0], sizeof(double) * N))) return rc;
+  double* d = (double*)ctx->io[0].p;
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(d, img, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+  if ((rc = msgpu_empty_lines_to_nan_device(ctx, nx, ny, num_images, d, replaced_out, st))) return rc;
+  CK(cudaMemcpyAsync(img, d, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
   return MSGPU_OK;
 }
 

@@ -442,6 +442,23 @@ __global__ void k_box_x(const double* T, int nx, int ny, int o, double* out) {
 
 // --- vector kernels of the seismic descent ----------------------------------
 // out[i] = a[i] + s * b[i]  (also the in-place updates, with out == a)
+// replaceEmptyLinesWithNaN (matchSeismicSeries.h:141-157): a line whose
+// squared norm is 0 becomes quiet NaNs.  The norm of the reference is a sum of
+// rounded squares, which are never negative, so it is 0 exactly when every
+// square rounds to 0, whatever the order of the additions (a NaN sample makes
+// it NaN and keeps the line): one block per line tests each square.
+__global__ void __launch_bounds__(256) k_empty_lines_nan(double* img, int nx, int* replaced) {
+  double* line = img + (size_t)blockIdx.x * nx;
+  int nonzero = 0;
+  for (int i = threadIdx.x; i < nx; i += 256) {
+    const double v = line[i];
+    nonzero |= !(v * v == 0.0);
+  }
+  if (__syncthreads_or(nonzero)) return;
+  for (int i = threadIdx.x; i < nx; i += 256) line[i] = __longlong_as_double(0x7ff8000000000000LL);
+  if (threadIdx.x == 0 && replaced) atomicAdd(replaced, 1);
+}
+
 __global__ void k_axpy(const double* a, double s, const double* b, double* out, int n) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     double v = a[i];

@@ -97,6 +97,7 @@ EXPORTS = [
     "msgpu_net_set_params", "msgpu_net_save", "msgpu_net_load", "msgpu_net_predict_device",
     "msgpu_net_train_step_device", "msgpu_net_loss_grad", "msgpu_prepare_images_device", "msgpu_register_batch_warm",
     "msgpu_register_batch_warm_device", "msgpu_find_xshift_yconst", "msgpu_find_xshift_yconst_device",
+    "msgpu_empty_lines_to_nan", "msgpu_empty_lines_to_nan_device",
 ]
 
 
@@ -201,6 +202,9 @@ def lib():
         L.msgpu_find_xshift_yconst_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                                       ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, _dp, _ip,
                                                       ctypes.c_void_p]
+        L.msgpu_empty_lines_to_nan.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _ip]
+        L.msgpu_empty_lines_to_nan_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                      ctypes.c_void_p, _ip, ctypes.c_void_p]
         L.msgpu_find_xshift_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp,
                                               ctypes.c_int, _dp, _d, _d, _d, ctypes.c_int, _dp, _dp, _ip, ctypes.c_int]
         L.msgpu_register_ragged.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params), ctypes.POINTER(SeriesDesc),
@@ -473,6 +477,21 @@ class Context:
         self._check(lib().msgpu_find_xshift_yconst(self._h, nx, ny, _p(R), _p(_f64(T)), int(max_iter), _p(ph),
                                                    ctypes.byref(e), ctypes.byref(steps)))
         return ph, e.value, steps.value
+
+    def empty_lines_to_nan(self, img):
+        """replaceEmptyLinesWithNaN on a copy of img (ny, nx) or (G, ny, nx); returns (copy, lines replaced)."""
+        out = _f64(img).copy()
+        nx, ny = out.shape[-1], out.shape[-2]
+        n = ctypes.c_int()
+        self._check(lib().msgpu_empty_lines_to_nan(self._h, nx, ny, out.size // (nx * ny), _p(out), ctypes.byref(n)))
+        return out, n.value
+
+    def empty_lines_to_nan_device(self, d_img, nx, ny, num_images, stream):
+        """In place on device memory; returns the number of lines replaced."""
+        n = ctypes.c_int()
+        self._check(lib().msgpu_empty_lines_to_nan_device(self._h, nx, ny, num_images, d_img, ctypes.byref(n),
+                                                          stream))
+        return n.value
 
     def find_xshift_batch(self, R, T, lam, yreg, max_iter=500, phix=None, workers=4, laplace_weight=0.0):
         """findXShift for images T (G, ny, nx) against R (ny, nx) or (G, ny, nx);

@@ -1831,6 +1831,24 @@ void msor_box_x(const double* T, int nx, int ny, int i, double* out) {
     }
 }
 
+/* replaceEmptyLinesWithNaN (matchSeismicSeries.h:141-157): a line whose
+ * squared norm (Vector::normSqr, the sum of the squares in index order) is 0
+ * is overwritten by quiet NaNs.  A NaN sample makes the norm NaN, so such a
+ * line is kept.                                                            */
+int msor_empty_lines_to_nan(double* img, int nx, int ny) {
+  int replaced = 0;
+  for (int y = 0; y < ny; ++y) {
+    double* line = img + (size_t)y * nx;
+    double s = 0.0;
+    for (int x = 0; x < nx; ++x) s += line[x] * line[x];
+    if (s == 0.0) {
+      for (int x = 0; x < nx; ++x) line[x] = NAN;
+      ++replaced;
+    }
+  }
+  return replaced;
+}
+
 /* findXShiftYConst (matchSeries.h:873-920): one shift per line, started from
  * the line means of phix; four descents (GridlessGradientDescent with
  * Fletcher-Reeves NCG: GradientDescentBase::applySingle, gradientDescent.h:

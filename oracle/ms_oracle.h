@@ -162,6 +162,9 @@ int    msor_xshift(int nx, int ny, const double* R, const double* T, double lamb
 int    msor_xshift_yconst(int nx, int ny, const double* R, const double* T, int max_iter, double* phix,
                           double* energy_out);
 void   msor_box_x(const double* T, int nx, int ny, int i, double* out);
+/* replaceEmptyLinesWithNaN (matchSeismicSeries.h:141-157) on ny lines of nx
+ * samples, in place; returns the number of lines replaced                 */
+int    msor_empty_lines_to_nan(double* img, int nx, int ny);
 /* matchSeries<>() with accumulated deformations, refinement and extra stages
  * (matchSeries.h:87-265, 353-445, 1250-1320); see ms_oracle.c.             */
 void   msor_match_series(int data_term, int level, int start, int stop, double lambda,

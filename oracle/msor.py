@@ -260,6 +260,14 @@ def box_x(T, i):
     return out
 
 
+def empty_lines_to_nan(img):
+    """replaceEmptyLinesWithNaN on a copy of img (..., ny, nx); returns (copy, lines replaced)."""
+    out = _c(img).copy()
+    nx = out.shape[-1]
+    n = lib().msor_empty_lines_to_nan(_p(out.reshape(-1)), nx, out.size // nx)
+    return out, n
+
+
 def warp_median(level, frames, phis, fill):
     N = n_of(level) ** 2
     out = np.zeros(N)
@@ -389,6 +397,12 @@ class RefRunner:
         self.run("xshiftyconst", nx, ny, int(max_iter), self._w("R", R), self._w("T", T), self._w("px", phix),
                  os.path.join(self.dir, "po"), os.path.join(self.dir, "e"))
         return self._r("po").reshape(ny, nx), float(self._r("e")[0])
+
+    def empty_lines_to_nan(self, img):
+        img = _c(img)
+        ny, nx = img.shape
+        self.run("emptynan", nx, ny, self._w("img", img), os.path.join(self.dir, "out"))
+        return self._r("out").reshape(ny, nx)
 
     def h1sys(self, x, sigma):
         ny, nx = x.shape

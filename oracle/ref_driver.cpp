@@ -367,7 +367,7 @@ static int usage ( ) {
     "ms_ref save nx ny in out type | load file out dims | savedef L in mask | loaddef L mask out\n"
     "ms_ref lineshift nx ny R T phix outE outDE | xshiftreg nx ny yRegFactor phix outE outKphi\n"
     "ms_ref xshiftlap nx ny yRegFactor laplaceWeight phix outE outKphi\n"
-    "ms_ref xshiftyconst nx ny maxIter R T phix outPhi outE\n"
+    "ms_ref xshiftyconst nx ny maxIter R T phix outPhi outE | emptynan nx ny img out\n"
     "ms_ref h1sys nx ny sigma x out\n"
     "ms_ref series[_ncc] maxL start stop lambda lambdaFactor maxIter stopEps sat minToZero F framesBin outPhis outMean outTxt\n"
     "ms_ref matchseries[_ncc] maxL start stop lambda lambdaFactor maxIter stopEps sat minToZero refineStart refineStop\n"
@@ -533,6 +533,23 @@ int main ( int argc, char **argv ) {
       DE.apply ( phi, de );
       writeBin ( argv[7], &e[0], 1 );
       writeBin ( argv[8], de.getData ( ), N );
+      return 0;
+    }
+    if ( cmd == "emptynan" && argc == 6 ) {
+      // ms_ref emptynan nx ny img out: replaceEmptyLinesWithNaN (matchSeismicSeries.h:141-157), composed from the
+      // same reference components (getLine, Vector::normSqr, putLine), as the function's header is not among the
+      // modules
+      const int nx = atoi ( argv[2] ), ny = atoi ( argv[3] );
+      ArrayType img ( nx, ny );
+      readBin ( argv[4], img.getData ( ), nx * ny );
+      qc::ScalarArray<RealType, qc::QC_1D> imageLine ( nx ), nanLine ( nx );
+      nanLine.setAll ( aol::NumberTrait<RealType>::NaN );
+      for ( int line = 0; line < ny; ++line ) {
+        img.getLine ( qc::QC_Y, line, imageLine );
+        if ( imageLine.normSqr ( ) == 0 )
+          img.putLine ( qc::QC_Y, line, nanLine );
+      }
+      writeBin ( argv[5], img.getData ( ), nx * ny );
       return 0;
     }
     if ( cmd == "xshiftyconst" && argc == 10 ) {

@@ -278,6 +278,19 @@ def seismic(ref: msor.RefRunner, seed: int):
         ph0 = rng.normal(0, 0.3, (ny, nx)) / (nx - 1)
         ph, e = ref.xshift_yconst(R, T, 60, ph0)
         d.update({f"ycR_{tag}": R, f"ycT_{tag}": T, f"ycphi0_{tag}": ph0, f"ycphi_{tag}": ph, f"ycE_{tag}": e})
+    # replaceEmptyLinesWithNaN: zero lines (also -0.0 and squares that underflow to 0) become NaN; a line with
+    # a NaN, a subnormal square or one non-zero sample stays
+    img = rng.normal(size=(12, 21))
+    img[[0, 5, 11], :] = 0.0
+    img[2, :] = -0.0
+    img[3, :] = 1e-170
+    img[4, :] = 0.0
+    img[4, 7] = np.nan
+    img[6, :] = 0.0
+    img[6, 20] = 1e-160
+    img[7, :] = 0.0
+    img[7, 0] = -3.0
+    d.update({"enR": img, "enOut": ref.empty_lines_to_nan(img)})
     np.savez_compressed(os.path.join(OUT, "seismic.npz"), **d)
 
 

@@ -135,3 +135,34 @@ def test_find_xshift_yconst_matches_reference(gpu, tag):
     assert np.all(ph == ph[:, :1])
     assert np.abs(ph - ref).max() * (nx - 1) <= 1e-9
     assert abs(e - float(g[f"ycE_{tag}"])) <= 1e-12 * abs(float(g[f"ycE_{tag}"]))
+
+
+def test_empty_lines_to_nan_matches_reference(gpu):
+    """replaceEmptyLinesWithNaN on the GPU against the reference's own run
+    (zero and -0.0 lines, squares that underflow to 0, a NaN line, a
+    subnormal square), NaN for NaN, bit for bit."""
+    g = golden("seismic.npz")
+    out, n = gpu.empty_lines_to_nan(g["enR"])
+    assert n == 5
+    assert np.array_equal(out.view(np.uint64), g["enOut"].view(np.uint64))
+
+
+def test_empty_lines_to_nan_batched_on_device_then_skipped_by_the_energy(gpu, oracle):
+    """Three images in one launch on device memory; the lines it turns into
+    NaN then contribute nothing to the line-shift energy, as in the
+    reference (registration.h:2150-2151)."""
+    import torch
+    rng = np.random.default_rng(31)
+    imgs = rng.normal(size=(3, 9, 40))
+    imgs[0, 2] = 0.0
+    imgs[2, [0, 8]] = 0.0
+    d = torch.from_numpy(imgs).cuda()
+    n = gpu.empty_lines_to_nan_device(d.data_ptr(), 40, 9, 3, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    out = d.cpu().numpy()
+    ref = np.stack([oracle.empty_lines_to_nan(im)[0] for im in imgs])
+    assert n == 3 and np.array_equal(out.view(np.uint64), ref.view(np.uint64))
+    phi = rng.normal(0, 0.02, (9, 40))
+    e, _ = gpu.lineshift_energy(out[1], out[0], phi)
+    eo, _ = oracle.lineshift(out[1], out[0], phi)
+    assert np.isfinite(e) and abs(e - eo) <= 1e-12 * abs(eo)

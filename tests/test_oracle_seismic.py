@@ -115,3 +115,11 @@ def test_box_filter_keeps_lines_and_spreads_nan(oracle):
     B2 = oracle.box_x(ok, 1)
     x = 6
     assert B2[1, x] == sum(0.2 * ok[1, (x + k) % 11] for k in range(-2, 3))
+
+
+def test_empty_lines_to_nan_matches_the_reference(oracle):
+    """replaceEmptyLinesWithNaN (matchSeismicSeries.h:141-157): the reference's own run, NaN for NaN."""
+    g = golden("seismic.npz")
+    out, n = oracle.empty_lines_to_nan(g["enR"])
+    assert np.array_equal(out, g["enOut"], equal_nan=True)
+    assert n == 5
