@@ -493,6 +493,23 @@ class Context:
                                                           stream))
         return n.value
 
+    def update_non_dyadic_xshift(self, R, T, lam, yreg, phix, laplace_weight=0.0, max_iter=500,
+                                 force_yconst=False):
+        """The non-dyadic step of XShiftNonDyadicRegistrationMultilevelDescent:
+        the empty lines of R and T become NaN (replaceEmptyLinesWithNaN,
+        matchSeismicSeries.h:141-157, 179-185), and unless every sample of
+        R + T is NaN (matchSeries.h:1217-1221) phix (ny, nx) is refined by
+        findXShift, or by findXShiftYConst under forceNonDyadicXShiftYConst
+        (matchSeismicSeries.h:195-202).  Returns (phix, energy, steps); with
+        nothing to register, phix unchanged, NaN and 0."""
+        R, _ = self.empty_lines_to_nan(R)
+        T, _ = self.empty_lines_to_nan(T)
+        if np.isnan(R + T).all():
+            return _f64(phix).copy(), float("nan"), 0
+        if force_yconst:
+            return self.find_xshift_yconst(R, T, max_iter, phix)
+        return self.find_xshift(R, T, lam, yreg, max_iter, phix, laplace_weight=laplace_weight)
+
     def find_xshift_batch(self, R, T, lam, yreg, max_iter=500, phix=None, workers=4, laplace_weight=0.0):
         """findXShift for images T (G, ny, nx) against R (ny, nx) or (G, ny, nx);
         returns (phix (G, ny, nx), energies[G], steps[G])."""

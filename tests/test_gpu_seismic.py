@@ -166,3 +166,29 @@ def test_empty_lines_to_nan_batched_on_device_then_skipped_by_the_energy(gpu, or
     e, _ = gpu.lineshift_energy(out[1], out[0], phi)
     eo, _ = oracle.lineshift(out[1], out[0], phi)
     assert np.isfinite(e) and abs(e - eo) <= 1e-12 * abs(eo)
+
+
+def test_non_dyadic_update_with_empty_lines_matches_oracle(gpu, oracle):
+    """updateNonDyadicDeformation of the seismic descent: empty lines (here a
+    gap at the top and one inside) become NaN and drop out of the data term;
+    findXShift then matches the oracle run on the same NaN-lined images."""
+    nx, ny = 65, 17
+    R, T = _shifted_lines(nx, ny, 1.0, 41)
+    R[0] = 0.0
+    T[9] = 0.0
+    ph0 = np.zeros((ny, nx))
+    ph, e, steps = gpu.update_non_dyadic_xshift(R, T, 0.01, 1.0, ph0, max_iter=40)
+    Rn, n_r = oracle.empty_lines_to_nan(R)
+    Tn, n_t = oracle.empty_lines_to_nan(T)
+    assert (n_r, n_t) == (1, 1)
+    rph, re, rsteps, _ = oracle.xshift(Rn, Tn, 0.01, 1.0, 40)
+    assert steps == rsteps and np.isfinite(e)
+    assert abs(e - re) <= 1e-9 * abs(re)
+    assert np.abs(ph - rph).max() * (nx - 1) <= 1e-6
+    # forceNonDyadicXShiftYConst takes the one-shift-per-line solve instead
+    phy, ey, _ = gpu.update_non_dyadic_xshift(R, T, 0.01, 1.0, ph0, max_iter=40, force_yconst=True)
+    assert np.all(phy == phy[:, :1]) and np.isfinite(ey)
+    # nothing to register: every sample of R + T is NaN
+    Z = np.zeros((ny, nx))
+    phz, ez, sz = gpu.update_non_dyadic_xshift(Z, T, 0.01, 1.0, ph0 + 0.25, max_iter=40)
+    assert np.all(phz == 0.25) and np.isnan(ez) and sz == 0
