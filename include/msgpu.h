@@ -185,6 +185,21 @@ int msgpu_empty_lines_to_nan(msgpu_context* ctx, int nx, int ny, int num_images,
 int msgpu_empty_lines_to_nan_device(msgpu_context* ctx, int nx, int ny, int num_images, double* d_img,
                                     int* replaced_out, void* stream);
 
+/* removeEmptyLinesFromImage (matchSeismicSeries.h:101-136), the input of the
+ * dyadic pre-stage (initMLADroppingEmptyLines, matchSeismicSeries.h:
+ * 187-192): out (capacity nx*ny; not the input) receives the lines of img
+ * whose squared norm is not 0 and which are not all NaN, in order; with
+ * keep_top_bottom (keepEmptyTopBottomBlocks) preceded and followed by zero
+ * lines for the empty blocks at the top and bottom, counted in units of the
+ * non-empty lines' mean distance.  *out_ny: the lines written.  Only empty
+ * lines: MSGPU_ERR_INVALID_ARG "Input contains only empty lines"; the same
+ * code for keep_top_bottom with a single non-empty line, where the reference
+ * divides by zero.                                                         */
+int msgpu_remove_empty_lines(msgpu_context* ctx, int nx, int ny, const double* img, int keep_top_bottom, double* out,
+                             int* out_ny);
+int msgpu_remove_empty_lines_device(msgpu_context* ctx, int nx, int ny, const double* d_img, int keep_top_bottom,
+                                    double* d_out, int* out_ny, void* stream);
+
 /* findXShiftYConst (matchSeries.h:873-920), the non-dyadic solve of
  * XShiftNonDyadicRegistrationMultilevelDescent under
  * forceNonDyadicXShiftYConst (matchSeismicSeries.h:197-201): one shift per

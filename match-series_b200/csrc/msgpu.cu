@@ -2459,6 +2459,67 @@ int msgpu_empty_lines_to_nan_device(msgpu_context* ctx, int nx, int ny, int num_
   return MSGPU_OK;
 }
 
+int msgpu_remove_empty_lines_device(msgpu_context* ctx, int nx, int ny, const double* d_img, int keep_top_bottom,
+                                    double* d_out, int* out_ny, void* stream) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (nx < 1 || ny < 1 || !d_img || !d_out || !out_ny || d_img == d_out)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid remove_empty_lines arguments");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((rc = ensure(ctx, ctx->io[5], sizeof(int) * 2 * (size_t)ny))) return rc;
+  int* kept_d = (int*)ctx->io[5].p;
+  int* map_d = kept_d + ny;
+  msg::k_line_kept<<<ny, 256, 0, st>>>(d_img, nx, kept_d);
+  CK(cudaGetLastError());
+  std::vector<int> kept(ny), lines;
+  CK(cudaMemcpyAsync(kept.data(), kept_d, sizeof(int) * ny, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  for (int y = 0; y < ny; ++y)
+    if (kept[y]) lines.push_back(y);
+  ctx->stats.kernel_launches = 1;
+  if (lines.empty()) return fail(ctx, MSGPU_ERR_INVALID_ARG, "Input contains only empty lines");
+  const int count = (int)lines.size(), first = lines.front(), last = lines.back();
+  int top = 0, bottom = 0;
+  if (keep_top_bottom) {
+    if (count == 1)
+      return fail(ctx, MSGPU_ERR_INVALID_ARG, "keeping the empty top and bottom blocks needs two non-empty lines");
+    // aol::Rint (aol.h:422) of the mean distance of the non-empty lines
+    const double d = (last - first) / (double)(count - 1);
+    const int dist = d >= 0 ? (int)(d + 0.5) : (int)(d - 0.5);
+    top = first / dist;
+    bottom = (ny - 1 - last) / dist;
+  }
+  const int n = count + top + bottom;
+  std::vector<int> map(n, -1);
+  for (int k = 0; k < count; ++k) map[top + k] = lines[k];
+  CK(cudaMemcpyAsync(map_d, map.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+  msg::k_gather_lines<<<n, 256, 0, st>>>(d_img, nx, map_d, d_out);
+  CK(cudaGetLastError());
+  ctx->stats.kernel_launches = 2;
+  CK(cudaStreamSynchronize(st));
+  *out_ny = n;
+  return MSGPU_OK;
+}
+
+int msgpu_remove_empty_lines(msgpu_context* ctx, int nx, int ny, const double* img, int keep_top_bottom, double* out,
+                             int* out_ny) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (!img || !out || !out_ny) return fail(ctx, MSGPU_ERR_INVALID_ARG, "null buffer");
+  if (nx < 1 || ny < 1) return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid remove_empty_lines arguments");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  const size_t N = (size_t)nx * ny;
+  if ((rc = ensure(ctx, ctx->io[0], sizeof(double) * 2 * N))) return rc;
+  double* d = (double*)ctx->io[0].p;
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(d, img, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+  if ((rc = msgpu_remove_empty_lines_device(ctx, nx, ny, d, keep_top_bottom, d + N, out_ny, st))) return rc;
+  CK(cudaMemcpyAsync(out, d + N, sizeof(double) * nx * (size_t)*out_ny, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return MSGPU_OK;
+}
+
 int msgpu_empty_lines_to_nan(msgpu_context* ctx, int nx, int ny, int num_images, double* img, int* replaced_out) {
   if (!ctx) return MSGPU_ERR_INVALID_ARG;
   if (!img) return fail(ctx, MSGPU_ERR_INVALID_ARG, "null buffer");

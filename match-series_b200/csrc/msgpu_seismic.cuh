@@ -459,6 +459,29 @@ __global__ void __launch_bounds__(256) k_empty_lines_nan(double* img, int nx, in
   if (threadIdx.x == 0 && replaced) atomicAdd(replaced, 1);
 }
 
+// removeEmptyLinesFromImage (matchSeismicSeries.h:101-136), first pass: a
+// line is kept unless its squared norm is 0 (every square rounds to 0, see
+// k_empty_lines_nan) or it holds NaNs only; one block per line.
+__global__ void __launch_bounds__(256) k_line_kept(const double* img, int nx, int* kept) {
+  const double* line = img + (size_t)blockIdx.x * nx;
+  int nonzero = 0, number = 0;
+  for (int i = threadIdx.x; i < nx; i += 256) {
+    const double v = line[i];
+    nonzero |= !(v * v == 0.0);
+    number |= !isnan(v);
+  }
+  const int nz = __syncthreads_or(nonzero);
+  const int nn = __syncthreads_or(number);
+  if (threadIdx.x == 0) kept[blockIdx.x] = nz && nn;
+}
+
+// Second pass: output line y copies source line map[y], or is zero for -1.
+__global__ void __launch_bounds__(256) k_gather_lines(const double* img, int nx, const int* map, double* out) {
+  const int src = map[blockIdx.x];
+  double* o = out + (size_t)blockIdx.x * nx;
+  for (int i = threadIdx.x; i < nx; i += 256) o[i] = src >= 0 ? img[(size_t)src * nx + i] : 0.0;
+}
+
 __global__ void k_axpy(const double* a, double s, const double* b, double* out, int n) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     double v = a[i];

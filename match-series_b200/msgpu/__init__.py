@@ -97,7 +97,8 @@ EXPORTS = [
     "msgpu_net_set_params", "msgpu_net_save", "msgpu_net_load", "msgpu_net_predict_device",
     "msgpu_net_train_step_device", "msgpu_net_loss_grad", "msgpu_prepare_images_device", "msgpu_register_batch_warm",
     "msgpu_register_batch_warm_device", "msgpu_find_xshift_yconst", "msgpu_find_xshift_yconst_device",
-    "msgpu_empty_lines_to_nan", "msgpu_empty_lines_to_nan_device",
+    "msgpu_empty_lines_to_nan", "msgpu_empty_lines_to_nan_device", "msgpu_remove_empty_lines",
+    "msgpu_remove_empty_lines_device",
 ]
 
 
@@ -205,6 +206,10 @@ def lib():
         L.msgpu_empty_lines_to_nan.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _ip]
         L.msgpu_empty_lines_to_nan_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                       ctypes.c_void_p, _ip, ctypes.c_void_p]
+        L.msgpu_remove_empty_lines.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _dp,
+                                               _ip]
+        L.msgpu_remove_empty_lines_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                                      ctypes.c_int, ctypes.c_void_p, _ip, ctypes.c_void_p]
         L.msgpu_find_xshift_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp,
                                               ctypes.c_int, _dp, _d, _d, _d, ctypes.c_int, _dp, _dp, _ip, ctypes.c_int]
         L.msgpu_register_ragged.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params), ctypes.POINTER(SeriesDesc),
@@ -485,6 +490,16 @@ class Context:
         n = ctypes.c_int()
         self._check(lib().msgpu_empty_lines_to_nan(self._h, nx, ny, out.size // (nx * ny), _p(out), ctypes.byref(n)))
         return out, n.value
+
+    def remove_empty_lines(self, img, keep_top_bottom=False):
+        """removeEmptyLinesFromImage of img (ny, nx); returns the cleaned image (lines, nx)."""
+        img = _f64(img)
+        ny, nx = img.shape
+        out = np.zeros((ny, nx))
+        n = ctypes.c_int()
+        self._check(lib().msgpu_remove_empty_lines(self._h, nx, ny, _p(img), int(bool(keep_top_bottom)), _p(out),
+                                                   ctypes.byref(n)))
+        return out[:n.value].copy()
 
     def empty_lines_to_nan_device(self, d_img, nx, ny, num_images, stream):
         """In place on device memory; returns the number of lines replaced."""

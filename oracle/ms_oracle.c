@@ -1849,6 +1849,53 @@ int msor_empty_lines_to_nan(double* img, int nx, int ny) {
   return replaced;
 }
 
+/* removeEmptyLinesFromImage (matchSeismicSeries.h:101-136): a line is empty
+ * when its squared norm is 0 or it holds NaNs only.  The kept top and bottom
+ * blocks count the empty lines there in units of the mean distance of the
+ * non-empty lines, rounded by aol::Rint (aol.h:422).  The reference divides
+ * by that distance, which is 0 for a single non-empty line: -2 here.      */
+int msor_remove_empty_lines(const double* img, int nx, int ny, int keep_top_bottom, double* out) {
+  int count = 0, first = -1, last = -1;
+  for (int y = 0; y < ny; ++y) {
+    const double* line = img + (size_t)y * nx;
+    double s = 0.0;
+    int non_nan = 0;
+    for (int x = 0; x < nx; ++x) {
+      s += line[x] * line[x];
+      if (!isnan(line[x])) ++non_nan;
+    }
+    if (s == 0.0 || non_nan == 0) continue;
+    if (first < 0) first = y;
+    last = y;
+    ++count;
+  }
+  if (count == 0) return -1;
+  int top = 0, bottom = 0;
+  if (keep_top_bottom) {
+    if (count == 1) return -2;
+    const double d = (last - first) / (double)(count - 1);
+    const int dist = d >= 0 ? (int)(d + 0.5) : (int)(d - 0.5);
+    top = first / dist;
+    bottom = (ny - 1 - last) / dist;
+  }
+  const int out_ny = count + top + bottom;
+  memset(out, 0, sizeof(double) * (size_t)nx * out_ny);
+  int k = top;
+  for (int y = 0; y < ny; ++y) {
+    const double* line = img + (size_t)y * nx;
+    double s = 0.0;
+    int non_nan = 0;
+    for (int x = 0; x < nx; ++x) {
+      s += line[x] * line[x];
+      if (!isnan(line[x])) ++non_nan;
+    }
+    if (s == 0.0 || non_nan == 0) continue;
+    memcpy(out + (size_t)k * nx, line, sizeof(double) * nx);
+    ++k;
+  }
+  return out_ny;
+}
+
 /* findXShiftYConst (matchSeries.h:873-920): one shift per line, started from
  * the line means of phix; four descents (GridlessGradientDescent with
  * Fletcher-Reeves NCG: GradientDescentBase::applySingle, gradientDescent.h:

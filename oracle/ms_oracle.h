@@ -165,6 +165,11 @@ void   msor_box_x(const double* T, int nx, int ny, int i, double* out);
 /* replaceEmptyLinesWithNaN (matchSeismicSeries.h:141-157) on ny lines of nx
  * samples, in place; returns the number of lines replaced                 */
 int    msor_empty_lines_to_nan(double* img, int nx, int ny);
+/* removeEmptyLinesFromImage (matchSeismicSeries.h:101-136): out (ny lines
+ * at most) gets the non-empty lines, with keep_top_bottom the empty blocks at
+ * the top and bottom as zero lines; returns its line count, -1 when every
+ * line is empty, -2 when keep_top_bottom meets a single non-empty line     */
+int    msor_remove_empty_lines(const double* img, int nx, int ny, int keep_top_bottom, double* out);
 /* matchSeries<>() with accumulated deformations, refinement and extra stages
  * (matchSeries.h:87-265, 353-445, 1250-1320); see ms_oracle.c.             */
 void   msor_match_series(int data_term, int level, int start, int stop, double lambda,

@@ -260,6 +260,15 @@ def box_x(T, i):
     return out
 
 
+def remove_empty_lines(img, keep_top_bottom=False):
+    """removeEmptyLinesFromImage of img (ny, nx); returns the cleaned image, or the code -1 / -2."""
+    img = _c(img)
+    ny, nx = img.shape
+    out = np.zeros((ny, nx))
+    n = lib().msor_remove_empty_lines(_p(img.reshape(-1)), nx, ny, int(keep_top_bottom), _p(out))
+    return out[:n] if n >= 0 else n
+
+
 def empty_lines_to_nan(img):
     """replaceEmptyLinesWithNaN on a copy of img (..., ny, nx); returns (copy, lines replaced)."""
     out = _c(img).copy()
@@ -403,6 +412,13 @@ class RefRunner:
         ny, nx = img.shape
         self.run("emptynan", nx, ny, self._w("img", img), os.path.join(self.dir, "out"))
         return self._r("out").reshape(ny, nx)
+
+    def remove_empty_lines(self, img, keep_top_bottom=False):
+        img = _c(img)
+        ny, nx = img.shape
+        self.run("rmempty", nx, ny, int(keep_top_bottom), self._w("img", img), os.path.join(self.dir, "out"))
+        out = self._r("out")
+        return out.reshape(-1, nx)
 
     def h1sys(self, x, sigma):
         ny, nx = x.shape

@@ -368,6 +368,7 @@ static int usage ( ) {
     "ms_ref lineshift nx ny R T phix outE outDE | xshiftreg nx ny yRegFactor phix outE outKphi\n"
     "ms_ref xshiftlap nx ny yRegFactor laplaceWeight phix outE outKphi\n"
     "ms_ref xshiftyconst nx ny maxIter R T phix outPhi outE | emptynan nx ny img out\n"
+    "ms_ref rmempty nx ny keepTopBottom img out\n"
     "ms_ref h1sys nx ny sigma x out\n"
     "ms_ref series[_ncc] maxL start stop lambda lambdaFactor maxIter stopEps sat minToZero F framesBin outPhis outMean outTxt\n"
     "ms_ref matchseries[_ncc] maxL start stop lambda lambdaFactor maxIter stopEps sat minToZero refineStart refineStop\n"
@@ -550,6 +551,33 @@ int main ( int argc, char **argv ) {
           img.putLine ( qc::QC_Y, line, nanLine );
       }
       writeBin ( argv[5], img.getData ( ), nx * ny );
+      return 0;
+    }
+    if ( cmd == "rmempty" && argc == 7 ) {
+      // ms_ref rmempty nx ny keepTopBottom img out: removeEmptyLinesFromImage (matchSeismicSeries.h:101-136),
+      // composed from the same reference components (getLine, normSqr, numNonNaNs, Rint, reallocate, putLine)
+      const int nx = atoi ( argv[2] ), ny = atoi ( argv[3] );
+      const bool keep = atoi ( argv[4] ) != 0;
+      ArrayType img ( nx, ny ), cleaned;
+      readBin ( argv[5], img.getData ( ), nx * ny );
+      qc::ScalarArray<RealType, qc::QC_1D> imageLine ( nx );
+      aol::Vector<int> emptyLines, nonEmptyLines;
+      for ( int line = 0; line < ny; ++line ) {
+        img.getLine ( qc::QC_Y, line, imageLine );
+        if ( ( imageLine.normSqr ( ) == 0 ) || ( aol::VectorHelper<aol::Vector<RealType> >::numNonNaNs ( imageLine ) == 0 ) )
+          emptyLines.pushBack ( line );
+        else
+          nonEmptyLines.pushBack ( line );
+      }
+      const int first = nonEmptyLines[0], last = nonEmptyLines[nonEmptyLines.size ( ) - 1];
+      const int dist = aol::Rint ( ( last - first ) / static_cast<RealType> ( nonEmptyLines.size ( ) - 1 ) );
+      const int top = keep ? ( first / dist ) : 0, bottom = keep ? ( ( ny - 1 - last ) / dist ) : 0;
+      cleaned.reallocate ( nx, nonEmptyLines.size ( ) + top + bottom );
+      for ( int line = 0; line < nonEmptyLines.size ( ); ++line ) {
+        img.getLine ( qc::QC_Y, nonEmptyLines[line], imageLine );
+        cleaned.putLine ( qc::QC_Y, line + top, imageLine );
+      }
+      writeBin ( argv[6], cleaned.getData ( ), cleaned.size ( ) );
       return 0;
     }
     if ( cmd == "xshiftyconst" && argc == 10 ) {

@@ -291,6 +291,14 @@ def seismic(ref: msor.RefRunner, seed: int):
     img[7, :] = 0.0
     img[7, 0] = -3.0
     d.update({"enR": img, "enOut": ref.empty_lines_to_nan(img)})
+    # removeEmptyLinesFromImage: every third line recorded (the others empty, one all NaN), an empty block at
+    # the top and at the bottom, without and with keepEmptyTopBottomBlocks
+    rm = np.zeros((31, 17))
+    rm[4:26:3] = rng.normal(size=(8, 17))
+    rm[7, :] = np.nan
+    rm[5, :] = np.nan
+    rm[5, 3] = 0.5
+    d.update({"rmR": rm, "rmOut0": ref.remove_empty_lines(rm, False), "rmOut1": ref.remove_empty_lines(rm, True)})
     np.savez_compressed(os.path.join(OUT, "seismic.npz"), **d)
 
 

@@ -192,3 +192,28 @@ def test_non_dyadic_update_with_empty_lines_matches_oracle(gpu, oracle):
     Z = np.zeros((ny, nx))
     phz, ez, sz = gpu.update_non_dyadic_xshift(Z, T, 0.01, 1.0, ph0 + 0.25, max_iter=40)
     assert np.all(phz == 0.25) and np.isnan(ez) and sz == 0
+
+
+@pytest.mark.parametrize("keep", [0, 1])
+def test_remove_empty_lines_matches_reference(gpu, keep):
+    """removeEmptyLinesFromImage on the GPU against the reference's own run
+    (an all-NaN line dropped, a line with one number kept), bit for bit."""
+    g = golden("seismic.npz")
+    out = gpu.remove_empty_lines(g["rmR"], bool(keep))
+    ref = g[f"rmOut{keep}"]
+    assert out.shape == ref.shape and np.array_equal(out.view(np.uint64), ref.view(np.uint64))
+
+
+def test_remove_empty_lines_errors_and_larger_image(gpu, oracle):
+    import msgpu
+    with pytest.raises(msgpu.MsgpuError, match="only empty lines"):
+        gpu.remove_empty_lines(np.zeros((6, 300)))
+    one = np.zeros((6, 300))
+    one[3] = 2.0
+    with pytest.raises(msgpu.MsgpuError):
+        gpu.remove_empty_lines(one, True)
+    rng = np.random.default_rng(33)
+    img = np.zeros((513, 1000))
+    img[7:500:4] = rng.normal(size=(124, 1000))
+    for keep in (False, True):
+        assert np.array_equal(gpu.remove_empty_lines(img, keep), oracle.remove_empty_lines(img, keep))

@@ -123,3 +123,20 @@ def test_empty_lines_to_nan_matches_the_reference(oracle):
     out, n = oracle.empty_lines_to_nan(g["enR"])
     assert np.array_equal(out, g["enOut"], equal_nan=True)
     assert n == 5
+
+
+@pytest.mark.parametrize("keep", [0, 1])
+def test_remove_empty_lines_matches_the_reference(oracle, keep):
+    """removeEmptyLinesFromImage (matchSeismicSeries.h:101-136): the reference's own run, bit for bit."""
+    g = golden("seismic.npz")
+    out = oracle.remove_empty_lines(g["rmR"], bool(keep))
+    ref = g[f"rmOut{keep}"]
+    assert out.shape == ref.shape and np.array_equal(out.view(np.uint64), ref.view(np.uint64))
+
+
+def test_remove_empty_lines_error_codes(oracle):
+    assert oracle.remove_empty_lines(np.zeros((4, 5))) == -1
+    one = np.zeros((4, 5))
+    one[2] = 1.0
+    assert oracle.remove_empty_lines(one, True) == -2
+    assert oracle.remove_empty_lines(one, False).shape == (1, 5)
