@@ -6,7 +6,10 @@
  * on failure msgpu_last_error() gives the message (the reference throws
  * aol::Exception with file and line; a C++ adapter rethrows this text).
  * A context is bound to one CUDA device and is not shared between threads.
- * Host-pointer entry points are synchronous.  Images are (2^l+1)^2 float64
+ * Host-pointer entry points are synchronous.  They refuse input images that
+ * hold NaN or Inf with MSGPU_ERR_INVALID_ARG (the reference's saturated
+ * min/max sorts the image, and with NaN the order is unspecified); with the
+ * device entry points such results are unspecified.  Images are (2^l+1)^2 float64
  * arrays, x fastest (quoc ILex order); displacements are in domain units
  * (pixel shift = phi * 2^l) and stored as [phi_x, phi_y] per frame.
  */
@@ -53,6 +56,17 @@ typedef struct {
 
 void msgpu_params_default(msgpu_params* p);
 int  msgpu_abi_version(void);
+
+/* Bounds of the device-side waits, in seconds, for every context of the
+ * process (no counterpart in the reference, which has no device waits):
+ * level_wait_s bounds one wait of a level-kernel worker for work (default
+ * 4 s), barrier_wait_s one grid-barrier wait of the composition kernel
+ * (default 2 s); a value <= 0 restores the default.  A kernel whose wait runs
+ * out sets an error flag and returns; the synchronous entry points then
+ * report MSGPU_ERR_CUDA and the context stays usable.  A diagnostic hook:
+ * shorter bounds make the waits run out on purpose, so that these error
+ * paths can be checked without a stuck kernel.                             */
+int  msgpu_set_wait_limits(double level_wait_s, double barrier_wait_s);
 
 int  msgpu_create(int device, msgpu_context** out);
 /* Data term (0 SSD, 1 NCC) of the single-operator entry points msgpu_energy
@@ -385,8 +399,14 @@ int msgpu_gd_level(msgpu_context* ctx, int level, const double* R, const double*
  * Every call on a device shares the one scratch array and leaves its
  * contents behind (each call clears what must start at zero); calls whose
  * work overlaps on the GPU (other streams, other host threads) race on it,
- * so serialise them.  Errors are status codes only (no context holds a
- * message): MSGPU_ERR_INVALID_ARG, MSGPU_ERR_SIZE, MSGPU_ERR_CUDA.          */
+ * so serialise them.  The set-up is cached per device for the life of the
+ * process: cudaDeviceReset on that device after the first call is not
+ * supported (the cached address and the uploaded tables would be stale).
+ * Errors are status codes only (no context holds a message):
+ * MSGPU_ERR_INVALID_ARG, MSGPU_ERR_SIZE, MSGPU_ERR_CUDA.  Because the call
+ * returns before the GPU runs, a solve whose scheduler gave up waiting (see
+ * msgpu_set_wait_limits) is reported in its outputs: *d_steps_out = -1 and
+ * *d_energy_out = NaN, with d_phi holding an unfinished displacement.        */
 int msgpu_gd_level_noalloc(int level, const double* d_R, const double* d_T, double* d_phi, double lambda,
                            int max_iter, double stop_eps, int use_fp64, double* d_energy_out, int* d_steps_out,
                            void* stream);

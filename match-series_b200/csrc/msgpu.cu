@@ -58,7 +58,14 @@ struct msgpu_context {
 
 namespace {
 
-constexpr int kAbiVersion = 4;
+constexpr int kAbiVersion = 5;
+
+// Bounds of the device-side waits (global-timer nanoseconds), process-wide:
+// a level-kernel worker waiting for work, a composition grid barrier.
+// msgpu_set_wait_limits changes them (a diagnostic hook: shorter bounds make
+// a wait run out on purpose, so that the error path can be checked).
+std::atomic<unsigned long long> g_level_wait_ns{kMaxIdleNs};
+std::atomic<unsigned long long> g_barrier_wait_ns{kExtBarrierNs};
 
 int fail(msgpu_context* ctx, int code, const char* fmt, ...) {
   char buf[512];
@@ -259,6 +266,19 @@ __global__ void __launch_bounds__(kSelThreads) k_select2(const double* __restric
     __syncthreads();
   }
   if (threadIdx.x < 2) out[2 * blockIdx.x + threadIdx.x] = dkey_inv(prefix[threadIdx.x]);
+}
+
+// Sets *flag when an image holds NaN or Inf.  The reference sorts such an
+// image for its saturated min/max (vec.h:864-871), whose result is then
+// unspecified, so the synchronous entry points refuse it after the call.
+__global__ void k_finite_check(const double* __restrict__ img, size_t stride, int count, int* flag) {
+  const double* a = img + (size_t)blockIdx.y * stride;
+  bool bad = false;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const double v = a[i];
+    bad |= !(fabs(v) <= 1.7976931348623157e308);
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
 }
 
 // min and max of every image (deterministic: min/max are order independent).
@@ -627,6 +647,7 @@ template <typename Real>
 cudaError_t launch_level_core(LevelArgs<Real>& a, void* sched_mem, int* error_flag, int sms, cudaStream_t st,
                               int* grid_out) {
   const int max_tiles = level_max_tiles(a.level);
+  a.idle_ns = g_level_wait_ns.load();
   size_t zb = 0;
   SchedPtrs<Real> sp = carve_sched<Real>(sched_mem, a.num_inst, max_tiles, &zb);
   sp.error = error_flag;
@@ -671,17 +692,19 @@ int sched_error_reset(msgpu_context* ctx, cudaStream_t st) {
     if ((rc = ensure(ctx, ctx->flags, 256))) return rc;
     ctx->sched_error = (int*)ctx->flags.p;
   }
-  CK(cudaMemsetAsync(ctx->sched_error, 0, 2 * sizeof(int), st));
+  CK(cudaMemsetAsync(ctx->sched_error, 0, 3 * sizeof(int), st));
   return MSGPU_OK;
 }
 
-// After the call's work has completed: reports a kernel that gave up waiting.
+// After the call's work has completed: reports a kernel that gave up waiting
+// and input images holding NaN or Inf (word 2, set by k_finite_check).
 int sched_error_check(msgpu_context* ctx) {
-  int h[2] = {0, 0};
+  int h[3] = {0, 0, 0};
   if (!ctx->sched_error) return MSGPU_OK;
   CK(cudaMemcpy(h, ctx->sched_error, sizeof(h), cudaMemcpyDeviceToHost));
   if (h[0]) return fail(ctx, MSGPU_ERR_CUDA, "level kernel: a worker waited too long for work (scheduler stalled)");
   if (h[1]) return fail(ctx, MSGPU_ERR_CUDA, "composition: a grid-barrier wait timed out");
+  if (h[2]) return fail(ctx, MSGPU_ERR_INVALID_ARG, "an input image holds a non-finite value (NaN or Inf)");
   return MSGPU_OK;
 }
 
@@ -698,6 +721,11 @@ int prepare_pyramid(msgpu_context* ctx, const msgpu_params& p, double* pyr, cons
   const int Lin = p.input_level;
   const size_t Nin = lvl_N(Lin);
   int& launches = ctx->stats.kernel_launches;
+  if (ctx->sched_error) {
+    k_finite_check<<<dim3((unsigned)std::min<size_t>(256, (Nin + 255) / 256), nimg), 256, 0, st>>>(
+        pyr + poff[Lin], pstride, (int)Nin, ctx->sched_error + 2);
+    ++launches;
+  }
   if (!p.dont_normalize_input) {
     if (p.saturation_percent >= 0) {
       const int m1 = (int)Nin - 1;
@@ -985,6 +1013,11 @@ int prepare_series(msgpu_context* ctx, const msgpu_params& p, const RaggedSeries
                        1, cudaMemcpyDeviceToDevice, st));
   CK(cudaMemcpy2DAsync(pyr + pstride + poff[Lin], pstride * sizeof(double), S.tmpl, Nin * sizeof(double),
                        Nin * sizeof(double), F, cudaMemcpyDeviceToDevice, st));
+  if (ctx->sched_error) {
+    k_finite_check<<<dim3((unsigned)std::min<size_t>(256, (Nin + 255) / 256), nimg), 256, 0, st>>>(
+        pyr + poff[Lin], pstride, (int)Nin, ctx->sched_error + 2);
+    ++launches;
+  }
   if (!p.dont_normalize_input) {
     if (p.saturation_percent >= 0) {
       const int m1 = (int)Nin - 1;
@@ -1224,6 +1257,7 @@ int compose_device(msgpu_context* ctx, int level, const double* d1, const double
   a.defined = (unsigned char*)(base + nd) + 64;
   a.error = ctx->sched_error + 1;
   a.level = level;
+  a.bar_ns = g_barrier_wait_ns.load();
   CK(cudaMemsetAsync(a.bar, 0, 2 * sizeof(unsigned), st));
   k_compose_prep<<<(unsigned)std::min<size_t>(2048, (N + 255) / 256), 256, 0, st>>>(a);
   CK(cudaGetLastError());
@@ -1412,6 +1446,18 @@ void msgpu_params_default(msgpu_params* p) {
 }
 
 int msgpu_abi_version(void) { return kAbiVersion; }
+
+int msgpu_set_wait_limits(double level_wait_s, double barrier_wait_s) {
+  if (std::isnan(level_wait_s) || std::isnan(barrier_wait_s)) return MSGPU_ERR_INVALID_ARG;
+  auto ns = [](double s, unsigned long long dflt) {
+    if (s <= 0) return dflt;
+    const double v = s * 1e9;
+    return v >= 1.8e19 ? dflt : (unsigned long long)v;
+  };
+  g_level_wait_ns.store(ns(level_wait_s, kMaxIdleNs));
+  g_barrier_wait_ns.store(ns(barrier_wait_s, kExtBarrierNs));
+  return MSGPU_OK;
+}
 
 int msgpu_set_data_term(msgpu_context* ctx, int data_term) {
   if (!ctx) return MSGPU_ERR_INVALID_ARG;
@@ -3101,6 +3147,14 @@ int noalloc_setup(int dev, NoAllocDevice** out) {
   return MSGPU_OK;
 }
 
+// Marks the outputs of a level solve whose scheduler gave up (error flag set).
+__global__ void k_noalloc_status(const int* err, double* energy, int* steps) {
+  if (threadIdx.x == 0 && *err) {
+    *steps = -1;
+    *energy = __longlong_as_double(0x7ff8000000000000ll);
+  }
+}
+
 #define NA_CK(call)                                \
   do {                                             \
     if ((call) != cudaSuccess) return MSGPU_ERR_CUDA; \
@@ -3161,6 +3215,9 @@ int noalloc_level(const NoAllocDevice& dv, int level, const double* d_R, const d
   // result: [phi_x, phi_y] dense, from whichever buffer the solve ended in
   k_phi_out<Real><<<dim3(gx, 1), 256, 0, st>>>(arena, L.stride, L.off_phi[0], L.off_phi[1], level, i_slot + 1,
                                                d_phi);
+  // a worker that gave up waiting leaves an unfinished solve: mark it in the
+  // outputs (steps -1, energy NaN), since the call does not wait for the GPU
+  k_noalloc_status<<<1, 32, 0, st>>>(err, a.out_energy, a.out_steps);
   NA_CK(cudaGetLastError());
   return MSGPU_OK;
 }

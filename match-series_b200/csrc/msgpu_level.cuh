@@ -98,6 +98,9 @@ struct LevelArgs {
   const int* inst_ref;
   size_t ref_stride;
   const double* lambda_inst;
+  // bound of one wait for work, in nanoseconds of the global timer; a worker
+  // that waits longer sets the error flag and every worker returns
+  unsigned long long idle_ns;
 };
 
 // A 2-component array of level k occupies 2 * comp_stride(k) elements.
@@ -1730,8 +1733,9 @@ __device__ bool try_take(const LevelArgs<Real>& a, const SchedPtrs<Real>& sp, in
   return false;
 }
 
-// Upper bound on one wait for work (nanoseconds of the global timer); beyond
-// it the worker sets the error flag and every worker returns.
+// Default bound on one wait for work (nanoseconds of the global timer, see
+// LevelArgs::idle_ns); beyond it the worker sets the error flag and every
+// worker returns.
 constexpr unsigned long long kMaxIdleNs = 4000000000ull;
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
@@ -1785,7 +1789,7 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
           int stop = 0;
           if (threadIdx.x == 0) {
             if (*(volatile int*)sp.error || *(volatile int*)sp.finished >= a.num_inst) stop = 2;
-            else if (global_ns() - t_begin > kMaxIdleNs) {
+            else if (global_ns() - t_begin > a.idle_ns) {
               atomicExch(sp.error, 1);
               stop = 2;
             }

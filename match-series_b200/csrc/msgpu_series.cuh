@@ -27,7 +27,7 @@ constexpr int kExtWX = kExtTX + 2, kExtWY = kExtTY + 2;       // with its one-no
 constexpr int kExtWin = kExtWX * kExtWY;
 constexpr int kExtMaxIter = 1000;
 constexpr double kExtEps = 1e-16;
-constexpr unsigned long long kExtBarrierNs = 2000000000ull;   // bound of one grid-barrier wait
+constexpr unsigned long long kExtBarrierNs = 2000000000ull;   // default bound of one grid-barrier wait
 
 // Scratch of one composition (doubles unless noted), N = nodes of the level.
 struct ExtArgs {
@@ -45,6 +45,7 @@ struct ExtArgs {
   int* error;              // set when a barrier wait gave up
   int* iters_out;          // 2: PCG steps per component
   int level;
+  unsigned long long bar_ns;  // bound of one grid-barrier wait (global-timer nanoseconds)
 };
 
 // DeformImage with an extension image of NaN (deformations.h:225-253), then
@@ -69,8 +70,8 @@ __global__ void k_compose_prep(ExtArgs a) {
 }
 
 // Grid-wide barrier with a bounded wait: returns false (and sets *error) when
-// the other CTAs did not arrive within kExtBarrierNs or another CTA gave up.
-__device__ __forceinline__ bool ext_grid_sync(unsigned* bar, int* error) {
+// the other CTAs did not arrive within limit_ns or another CTA gave up.
+__device__ __forceinline__ bool ext_grid_sync(unsigned* bar, int* error, unsigned long long limit_ns) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -86,7 +87,7 @@ __device__ __forceinline__ bool ext_grid_sync(unsigned* bar, int* error) {
     } else {
       const unsigned long long t0 = global_ns();
       while (*vgen == gen) {
-        if (*(volatile int*)error || global_ns() - t0 > kExtBarrierNs) {
+        if (*(volatile int*)error || global_ns() - t0 > limit_ns) {
           atomicExch(error, 1);
           good = 0;
           break;
@@ -226,7 +227,7 @@ __global__ void __launch_bounds__(kExtThreads) k_extend_pcg(ExtArgs a) {
   ext_block_sum(part, wbuf);
   if (threadIdx.x == 0)
     for (int k = 0; k < 4; ++k) __stcg(a.partials + (size_t)blockIdx.x * 4 + k, part[k]);
-  if (!ext_grid_sync(a.bar, a.error)) return;
+  if (!ext_grid_sync(a.bar, a.error, a.bar_ns)) return;
   double tot[4];
   ext_grid_total(a.partials, 4, tot, wbuf);
   double an[2] = {tot[0], tot[1]}, spn[2] = {tot[2], tot[3]}, q[2] = {0.0, 0.0};
@@ -285,7 +286,7 @@ __global__ void __launch_bounds__(kExtThreads) k_extend_pcg(ExtArgs a) {
     ext_block_sum(pa, wbuf);
     if (threadIdx.x == 0)
       for (int c = 0; c < 2; ++c) __stcg(a.partials + (size_t)blockIdx.x * 4 + c, pa[c]);
-    if (!ext_grid_sync(a.bar, a.error)) return;
+    if (!ext_grid_sync(a.bar, a.error, a.bar_ns)) return;
     ext_grid_total(a.partials, 2, tot, wbuf);
     double alpha[2];
     for (int c = 0; c < 2; ++c) alpha[c] = an[c] / tot[c];
@@ -314,7 +315,7 @@ __global__ void __launch_bounds__(kExtThreads) k_extend_pcg(ExtArgs a) {
     ext_block_sum(pb, wbuf);
     if (threadIdx.x == 0)
       for (int k2 = 0; k2 < 4; ++k2) __stcg(a.partials + (size_t)blockIdx.x * 4 + k2, pb[k2]);
-    if (!ext_grid_sync(a.bar, a.error)) return;
+    if (!ext_grid_sync(a.bar, a.error, a.bar_ns)) return;
     ext_grid_total(a.partials, 4, tot, wbuf);
     for (int c = 0; c < 2; ++c) {
       if (!act[c]) continue;

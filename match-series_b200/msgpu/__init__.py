@@ -98,7 +98,7 @@ EXPORTS = [
     "msgpu_net_train_step_device", "msgpu_net_loss_grad", "msgpu_prepare_images_device", "msgpu_register_batch_warm",
     "msgpu_register_batch_warm_device", "msgpu_find_xshift_yconst", "msgpu_find_xshift_yconst_device",
     "msgpu_empty_lines_to_nan", "msgpu_empty_lines_to_nan_device", "msgpu_remove_empty_lines",
-    "msgpu_remove_empty_lines_device",
+    "msgpu_remove_empty_lines_device", "msgpu_set_wait_limits",
 ]
 
 
@@ -216,8 +216,17 @@ def lib():
                                             ctypes.c_int]
         L.msgpu_register_ragged_device.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params),
                                                    ctypes.POINTER(SeriesDesc), ctypes.c_int, ctypes.c_void_p]
+        L.msgpu_set_wait_limits.argtypes = [ctypes.c_double, ctypes.c_double]
         _lib = L
     return _lib
+
+
+def set_wait_limits(level_wait_s: float = 0.0, barrier_wait_s: float = 0.0) -> None:
+    """Bounds of the device-side waits for the whole process (<= 0: defaults
+    of 4 s and 2 s); shorter bounds make the waits run out on purpose."""
+    st = lib().msgpu_set_wait_limits(level_wait_s, barrier_wait_s)
+    if st:
+        raise MsgpuError(st, "invalid wait limits")
 
 
 def default_params(**kw) -> Params:
@@ -509,18 +518,20 @@ class Context:
         return n.value
 
     def update_non_dyadic_xshift(self, R, T, lam, yreg, phix, laplace_weight=0.0, max_iter=500,
-                                 force_yconst=False):
+                                 force_yconst=False, prev_energy=float("nan")):
         """The non-dyadic step of XShiftNonDyadicRegistrationMultilevelDescent:
         the empty lines of R and T become NaN (replaceEmptyLinesWithNaN,
         matchSeismicSeries.h:141-157, 179-185), and unless every sample of
         R + T is NaN (matchSeries.h:1217-1221) phix (ny, nx) is refined by
         findXShift, or by findXShiftYConst under forceNonDyadicXShiftYConst
-        (matchSeismicSeries.h:195-202).  Returns (phix, energy, steps); with
-        nothing to register, phix unchanged, NaN and 0."""
+        (matchSeismicSeries.h:195-202).  Returns (phix, energy, steps).  With
+        nothing to register the reference skips updateNonDyadicDeformation, so
+        its energy of the last solution keeps its previous value: phix comes
+        back unchanged with prev_energy (the caller's last energy) and 0 steps."""
         R, _ = self.empty_lines_to_nan(R)
         T, _ = self.empty_lines_to_nan(T)
         if np.isnan(R + T).all():
-            return _f64(phix).copy(), float("nan"), 0
+            return _f64(phix).copy(), float(prev_energy), 0
         if force_yconst:
             return self.find_xshift_yconst(R, T, max_iter, phix)
         return self.find_xshift(R, T, lam, yreg, max_iter, phix, laplace_weight=laplace_weight)

@@ -192,6 +192,9 @@ def test_non_dyadic_update_with_empty_lines_matches_oracle(gpu, oracle):
     Z = np.zeros((ny, nx))
     phz, ez, sz = gpu.update_non_dyadic_xshift(Z, T, 0.01, 1.0, ph0 + 0.25, max_iter=40)
     assert np.all(phz == 0.25) and np.isnan(ez) and sz == 0
+    # the reference then keeps its previous energy of the last solution
+    phz, ez, sz = gpu.update_non_dyadic_xshift(Z, T, 0.01, 1.0, ph0 + 0.25, max_iter=40, prev_energy=e)
+    assert np.all(phz == 0.25) and ez == e and sz == 0
 
 
 @pytest.mark.parametrize("keep", [0, 1])

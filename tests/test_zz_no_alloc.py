@@ -53,7 +53,8 @@ def _noalloc(f, level, R, T, phix, phiy, lam, max_iter, fp64):
 @pytest.mark.parametrize("order", ["large_then_small", "small_then_large"])
 def test_noalloc_matches_gd_level_on_calls_in_a_row(gpu, order):
     f = _entry()
-    cases = [(7, 21, 1, 12), (6, 22, 1, 10), (6, 23, 0, 10)]
+    # level 8 in FP64 is the largest solve the scratch array holds
+    cases = [(8, 24, 1, 6), (7, 21, 1, 12), (6, 22, 1, 10), (8, 25, 0, 6), (6, 23, 0, 10)]
     if order == "small_then_large":
         cases = cases[::-1]
     for level, seed, fp64, iters in cases:
@@ -78,6 +79,28 @@ def test_noalloc_rejects_levels_beyond_its_scratch(gpu):
     n = (1 << level) + 1
     R, T = _images(gpu, level, 5)
     z = np.zeros(n * n)
+    qx, qy, e0, s0, _ = gpu.gd_level(level, R, T, z, z, 0.1, 6, fp64=1)
+    px, py, e, s = _noalloc(f, level, R, T, z, z, 0.1, 6, 1)
+    assert s == s0 and abs(e - e0) / e0 <= 1e-9
+    assert max(np.abs(px - qx).max(), np.abs(py - qy).max()) * (n - 1) <= 1e-6
+
+
+def test_noalloc_reports_a_stalled_solve_in_its_outputs(gpu):
+    """The call returns before the GPU runs, so a scheduler that gave up
+    waiting (its wait bound shortened on purpose) is reported in the outputs:
+    steps -1 and energy NaN.  With the default bound the next call is whole."""
+    import msgpu
+    f = _entry()
+    level = 6
+    n = (1 << level) + 1
+    R, T = _images(gpu, level, 27)
+    z = np.zeros(n * n)
+    msgpu.set_wait_limits(1e-9, 0.0)
+    try:
+        _, _, e, s = _noalloc(f, level, R, T, z, z, 0.1, 6, 1)
+    finally:
+        msgpu.set_wait_limits(0.0, 0.0)
+    assert s == -1 and np.isnan(e)
     qx, qy, e0, s0, _ = gpu.gd_level(level, R, T, z, z, 0.1, 6, fp64=1)
     px, py, e, s = _noalloc(f, level, R, T, z, z, 0.1, 6, 1)
     assert s == s0 and abs(e - e0) / e0 <= 1e-9
