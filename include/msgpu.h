@@ -52,6 +52,17 @@ typedef struct {
                                   (SSDRegistrationConfigurator), 1 normalized
                                   cross-correlation (NCCRegistrationConfigurator,
                                   registration.h:1766-1780, 1909-2018)        */
+  int sum_order;               /* order of the global FP64 sums of a level
+                                  solve (no parameter-file key; the reference
+                                  has only its own order): 0 (default) the
+                                  reference's sequential order, every sum the
+                                  reference's double bit for bit, so the
+                                  gradient flow takes the reference's steps;
+                                  1 a fixed parallel order (deterministic, a
+                                  little faster, sums within rounding of the
+                                  reference's).  Applies with use_fp64 = 1
+                                  and data_term = 0; otherwise the parallel
+                                  order is used.                            */
 } msgpu_params;
 
 void msgpu_params_default(msgpu_params* p);
@@ -73,6 +84,9 @@ int  msgpu_create(int device, msgpu_context** out);
  * and msgpu_gd_level of this context; the batch entry points take it from
  * msgpu_params.data_term.                                                  */
 int  msgpu_set_data_term(msgpu_context* ctx, int data_term);
+/* Order of the global sums (msgpu_params.sum_order) of the single-operator
+ * entry points msgpu_energy and msgpu_gd_level of this context (default 0). */
+int  msgpu_set_sum_order(msgpu_context* ctx, int sum_order);
 int  msgpu_destroy(msgpu_context* ctx);
 const char* msgpu_last_error(const msgpu_context* ctx);
 
@@ -378,8 +392,10 @@ int msgpu_gd_level(msgpu_context* ctx, int level, const double* R, const double*
                    double* energy_out, int* steps_out, double* trace, int max_trace);
 
 /* --- allocation-free level solve ----------------------------------------
- * No counterpart in the reference.  The same level solve as msgpu_gd_level,
- * for callers that cannot allocate device memory: applications whose device
+ * No counterpart in the reference.  The same level solve as msgpu_gd_level
+ * with its global sums in the fixed parallel order (sum order 1; the term
+ * blocks of the reference order would not fit the static array), for
+ * callers that cannot allocate device memory: applications whose device
  * memory belongs to their own pool allocator (cudaMalloc/cudaFree from other
  * code would synchronise the device and fragment the pool), or hosts that
  * admit only a fixed, known device footprint.  It needs no context and

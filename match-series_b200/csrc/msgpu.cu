@@ -23,6 +23,7 @@
 #include <atomic>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/msgpu.h"
@@ -42,6 +43,8 @@ struct msgpu_context {
   struct Buf { void* p = nullptr; size_t cap = 0; };
   Buf arena, shared_real, dscratch, small, phis_d, io[6], prof, sched, flags, nccbuf, ext, series, vals;
   int data_term = 0;           // data term of the single-operator entry points
+  int sum_order = 0;           // order of the global sums of the single-operator entry points
+  Buf xsum;                    // exact sums: per-instance term blocks and chunk summaries
   int* sched_error = nullptr;  // device flag of the level scheduler (in flags)
   // statistics of the last batch call
   bool profiling = false;
@@ -683,6 +686,22 @@ int launch_level(msgpu_context* ctx, LevelArgs<Real>& a, cudaStream_t st) {
   return MSGPU_OK;
 }
 
+// Exact sums of a level launch (FP64, SSD, sum order 0): per-instance
+// regions of XsLayout(n).stride doubles for num_inst instances; otherwise the
+// launch adds its sums in the fixed parallel order of the tile partials.
+template <typename Real>
+int xs_attach(msgpu_context* ctx, LevelArgs<Real>& a, bool exact, int max_level, int num_inst) {
+  a.xs = nullptr;
+  a.xs_stride = 0;
+  if (!exact || !std::is_same<Real, double>::value || a.ncc) return MSGPU_OK;
+  int rc;
+  const size_t cap = XsLayout(lvl_n(max_level)).stride * (size_t)num_inst;
+  if ((rc = ensure(ctx, ctx->xsum, sizeof(double) * cap))) return rc;
+  a.xs = (double*)ctx->xsum.p;
+  a.xs_stride = XsLayout(a.n).stride;
+  return MSGPU_OK;
+}
+
 // Clears the error flags at the start of an API call: word 0 is set by a
 // level-kernel worker that gave up waiting for work, word 1 by the
 // composition kernel when a grid-barrier wait gave up.
@@ -927,6 +946,7 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
       a.pass_cycles = (unsigned long long*)ctx->prof.p + prof_n * (l - start);
       CK(cudaMemsetAsync(a.pass_cycles, 0, sizeof(unsigned long long) * prof_n, st));
     }
+    if ((rc = xs_attach<Real>(ctx, a, p.sum_order == 0, stop, F))) return rc;
     if (ctx->profiling && l - start < 16) CK(cudaEventRecord(ctx->ev[2 * (l - start)], st));
     if ((rc = launch_level<Real>(ctx, a, st))) return rc;
     if (l - start < 16) ctx->stats.level_cluster[l - start] = ctx->last_grid;
@@ -1166,6 +1186,7 @@ int run_ragged(msgpu_context* ctx, const msgpu_params& p, std::vector<RaggedSeri
     a.out_steps = steps;
     a.out_evals = evals;
     a.out_phi_buf = bin;
+    if ((rc = xs_attach<Real>(ctx, a, p.sum_order == 0, Lmax, Ftot))) return rc;
     if ((rc = launch_level<Real>(ctx, a, st))) return rc;
     ++launches;
     // series finishing at this level: displacements and energies out
@@ -1205,6 +1226,8 @@ int check_params(msgpu_context* ctx, const msgpu_params* p) {
   if (p->max_gd_iterations < 0) return fail(ctx, MSGPU_ERR_INVALID_ARG, "maxGDIterations < 0");
   if (p->data_term != 0 && p->data_term != 1)
     return fail(ctx, MSGPU_ERR_INVALID_ARG, "data_term %d: 0 (SSD) or 1 (NCC)", p->data_term);
+  if (p->sum_order != 0 && p->sum_order != 1)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "sum_order %d: 0 (reference order) or 1 (parallel order)", p->sum_order);
   return MSGPU_OK;
 }
 
@@ -1456,6 +1479,13 @@ int msgpu_set_wait_limits(double level_wait_s, double barrier_wait_s) {
   };
   g_level_wait_ns.store(ns(level_wait_s, kMaxIdleNs));
   g_barrier_wait_ns.store(ns(barrier_wait_s, kExtBarrierNs));
+  return MSGPU_OK;
+}
+
+int msgpu_set_sum_order(msgpu_context* ctx, int sum_order) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (sum_order != 0 && sum_order != 1) return fail(ctx, MSGPU_ERR_INVALID_ARG, "sum_order must be 0 or 1");
+  ctx->sum_order = sum_order;
   return MSGPU_OK;
 }
 
@@ -2936,6 +2966,7 @@ int single_level(msgpu_context* ctx, int level, int mode, const double* R, const
   a.out_phi_buf = d_i + 1;
   a.trace = trace ? d_trace : nullptr;
   a.max_trace = max_trace;
+  if ((rc = xs_attach<Real>(ctx, a, ctx->sum_order == 0 && mode != MODE_SMOOTH, level, 1))) return rc;
   if ((rc = sched_error_reset(ctx, st))) return rc;
   if ((rc = launch_level<Real>(ctx, a, st))) return rc;
   CK(cudaGetLastError());

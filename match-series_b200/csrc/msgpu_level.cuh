@@ -27,6 +27,7 @@
 #pragma once
 
 #include "msgpu_fe.cuh"
+#include "msgpu_xsum.cuh"
 
 namespace msg {
 
@@ -101,6 +102,10 @@ struct LevelArgs {
   // bound of one wait for work, in nanoseconds of the global timer; a worker
   // that waits longer sets the error flag and every worker returns
   unsigned long long idle_ns;
+  // exact sums (FP64, SSD): every global sum in the reference's sequential
+  // order (msgpu_xsum.cuh); per-instance regions of xs_stride doubles, or null
+  double* xs;
+  size_t xs_stride;
 };
 
 // A 2-component array of level k occupies 2 * comp_stride(k) elements.
@@ -250,12 +255,14 @@ struct EnergyPass {
   int nwin;
   double* part;
   Tiles tl;
+  double* xs;   // exact sums: the instance's region (Real = double), or null
 
   __device__ EnergyPass(const Inst<Real>& I_, int kind_, Real tau_, Real beta_, bool odz, const Real* phx_,
                         const Real* phy_, const Real* dx_, const Real* dy_, const Real* sx_, const Real* sy_,
-                        const Real* dex_, const Real* dey_, Real* wdx_, Real* wdy_, Real* sm_, double* part_)
+                        const Real* dex_, const Real* dey_, Real* wdx_, Real* wdy_, Real* sm_, double* part_,
+                        double* xs_ = nullptr)
       : I(I_), kind(kind_), tau(tau_), beta(beta_), od_zero(odz), phx(phx_), phy(phy_), dx(dx_), dy(dy_),
-        sx(sx_), sy(sy_), dex(dex_), dey(dey_), wdx(wdx_), wdy(wdy_), sm(sm_), part(part_), tl(I_.n) {
+        sx(sx_), sy(sy_), dex(dex_), dey(dey_), wdx(wdx_), wdy(wdy_), sm(sm_), part(part_), tl(I_.n), xs(xs_) {
     nwin = (kind == 0) ? 3 : (kind == 1 ? 5 : 7);
   }
   __device__ Real* win(int stage, int k) const { return sm + ((size_t)stage * nwin + k) * EWIN; }
@@ -282,7 +289,131 @@ struct EnergyPass {
     load_window(win(stage, k), I.R, n, P, wx0, wy0, EWX, EWY);
   }
 
+  // Exact-sum variant: the terms of E_data (per element), of phi . L phi at
+  // the evaluated position (per node and component) and, for the NCG pass,
+  // of DE . d go to the instance's term blocks in the reference's order
+  // (msgpu_xsum.cuh); the completing CTA adds them exactly.  The evaluated
+  // position newPosition = phi + tau d (gradientDescent.h:176-178) is formed
+  // on the whole window first, and E_reg = 1/2 (p_x . L p_x + p_y . L p_y)
+  // is evaluated there as DisplacementLengthEnergy does (hyperelastic.h:
+  // 178-183), not by the quadratic expansion of the fast path.
+  __device__ void compute_exact(int t, int stage) {
+    int x0, x1, y0, y1;
+    tl.rect(t, x0, x1, y0, y1);
+    const int n = I.n;
+    Real* Wpx = win(stage, 0);
+    Real* Wpy = win(stage, 1);
+    const Real* Wr = win(stage, nwin - 1);
+    Real* Wa = (kind != 0) ? win(stage, 2) : nullptr;
+    Real* Wb = (kind != 0) ? win(stage, 3) : nullptr;
+    const Real* Wox = (kind == 2) ? win(stage, 4) : nullptr;
+    const Real* Woy = (kind == 2) ? win(stage, 5) : nullptr;
+    if (kind != 0) {
+      for (int i = threadIdx.x; i < EWIN; i += kThreads) {
+        Real ddx = Wa[i], ddy = Wb[i];
+        if (kind == 2 && !od_zero) {
+          // d = s + beta od (gradientDescent.h:221-229)
+          ddx = ddx + beta * Wox[i];
+          ddy = ddy + beta * Woy[i];
+          Wa[i] = ddx;
+          Wb[i] = ddy;
+        }
+        Real vx = Wpx[i], vy = Wpy[i];
+        vx += tau * ddx;
+        vy += tau * ddy;
+        Wpx[i] = vx;
+        Wpy[i] = vy;
+      }
+      __syncthreads();
+    }
+    auto at = [&](int x, int y) { return (y - (y0 - 1)) * EWX + (x - (x0 - 4)); };
+    const XsGeom g(n);
+    const int tx = t % g.nx;
+    const int lx = threadIdx.x & 63, ly = threadIdx.x >> 6, half = lx >> 5, lane = threadIdx.x & 31;
+    // elements owned by the tile: E_data terms
+    {
+      const XsSum s0 = xs_sum(xs, n, 0, true);
+      double* B0 = xs_block(s0, t);
+      const int ex1 = (x1 < n - 1) ? x1 : n - 1, ey1 = (y1 < n - 1) ? y1 : n - 1;
+      const int ew = ex1 - x0, eh = ey1 - y0;
+      for (int iy = ly; iy < eh; iy += kThreads / 64) {
+        double acc = 0.0;
+        for (int ix = lx; ix < ew; ix += 64) {
+          const int ex = x0 + ix, ey = y0 + iy;
+          const int c0 = at(ex, ey);
+          const int idx[4] = {c0, c0 + 1, c0 + EWX, c0 + EWX + 1};
+          Real px[4], py[4], r[4];
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            r[b] = Wr[idx[b]];
+            px[b] = Wpx[idx[b]];
+            py[b] = Wpy[idx[b]];
+          }
+          const double v = (double)element_ssd(I.T, n, I.P, I.h, ex, ey, px, py, r);
+          B0[xs_at(ix, iy)] = v;
+          acc += v;
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) s0.tot[((y0 + iy) * g.nx + tx) * 2 + half] = acc;
+      }
+    }
+    // owned nodes: p . L p per component; NCG also DE . d and the direction
+    {
+      const XsSum s1 = xs_sum(xs, n, 1, false), s2 = xs_sum(xs, n, 2, false);
+      const XsSum s3 = xs_sum(xs, n, 3, false), s4 = xs_sum(xs, n, 4, false);
+      double* B1 = xs_block(s1, t);
+      double* B2 = xs_block(s2, t);
+      double* B3 = xs_block(s3, t);
+      double* B4 = xs_block(s4, t);
+      const int nw = x1 - x0, nh = y1 - y0;
+      for (int iy = ly; iy < nh; iy += kThreads / 64) {
+        double a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0;
+        for (int ix = lx; ix < nw; ix += 64) {
+          const int x = x0 + ix, y = y0 + iy;
+          const int c = at(x, y);
+          const Real lx_ = stiff_row<Real>(x, y, n, [&](int X, int Y) { return Wpx[at(X, Y)]; });
+          const Real ly_ = stiff_row<Real>(x, y, n, [&](int X, int Y) { return Wpy[at(X, Y)]; });
+          const double t1 = (double)(Wpx[c] * lx_), t2 = (double)(Wpy[c] * ly_);
+          B1[xs_at(ix, iy)] = t1;
+          B2[xs_at(ix, iy)] = t2;
+          a1 += t1;
+          a2 += t2;
+          if (kind == 2) {
+            const Real ddx = Wa[c], ddy = Wb[c];
+            const size_t gg = (size_t)y * I.P + x;
+            wdx[gg] = ddx;
+            wdy[gg] = ddy;
+            const double t3 = (double)(__ldcg(dex + gg) * ddx), t4 = (double)(__ldcg(dey + gg) * ddy);
+            B3[xs_at(ix, iy)] = t3;
+            B4[xs_at(ix, iy)] = t4;
+            a3 += t3;
+            a4 += t4;
+          }
+        }
+        a1 = warp_sum(a1);
+        a2 = warp_sum(a2);
+        if (kind == 2) {
+          a3 = warp_sum(a3);
+          a4 = warp_sum(a4);
+        }
+        if (lane == 0) {
+          const int j2 = ((y0 + iy) * g.nx + tx) * 2 + half;
+          s1.tot[j2] = a1;
+          s2.tot[j2] = a2;
+          if (kind == 2) {
+            s3.tot[j2] = a3;
+            s4.tot[j2] = a4;
+          }
+        }
+      }
+    }
+  }
+
   __device__ void compute(int t, int stage) {
+    if (xs) {
+      compute_exact(t, stage);
+      return;
+    }
     int x0, x1, y0, y1;
     tl.rect(t, x0, x1, y0, y1);
     const int n = I.n;
@@ -840,13 +971,14 @@ struct UpPass {
   bool want_norm;
   double* part;
   Tiles tl;
+  double* xs;   // exact sums of |s|^2 (want_norm, Real = double), or null
   static constexpr size_t kStage = 4 * VWIN + 2 * CWIN;
   __device__ UpPass(int n_, const Real* rx_, const Real* ry_, Real sgn_, const Real* x2x_, const Real* x2y_,
                     const Real* xcx_, const Real* xcy_, Real* ox_, Real* oy_, Real hsq_, Real diag_, Real* sm_,
-                    bool wn, double* part_)
+                    bool wn, double* part_, double* xs_ = nullptr)
       : n(n_), P(pitch_of(n_)), cw((n_ >> 1) + 1), cP(pitch_of((n_ >> 1) + 1)), rx(rx_), ry(ry_), x2x(x2x_),
         x2y(x2y_), xcx(xcx_), xcy(xcy_), sgn(sgn_), ox(ox_), oy(oy_), hsq(hsq_), diag(diag_), sm(sm_),
-        want_norm(wn), part(part_), tl(n_, VTX, VTY) {}
+        want_norm(wn), part(part_), tl(n_, VTX, VTY), xs(xs_) {}
   __device__ Real* rhs(int stage, int c) const { return sm + stage * kStage + (size_t)c * VWIN; }
   __device__ Real* x2(int stage, int c) const { return sm + stage * kStage + (size_t)(2 + c) * VWIN; }
   __device__ Real* xc(int stage, int c) const { return sm + stage * kStage + 4 * VWIN + (size_t)c * CWIN; }
@@ -893,7 +1025,55 @@ struct UpPass {
     }
     __syncthreads();
     // x5 on the owned nodes
-    {
+    if (xs && want_norm) {
+      // the smoothed direction s and the terms s_c * s_c of |s|^2 = s_x . s_x +
+      // s_y . s_y (gradientDescent.h:221-226), node sums of the element-pass
+      // geometry: a 32-wide tile is one half of a 64-wide chunk
+      const int w = x1 - x0, h = y1 - y0;
+      const XsGeom g(n);
+      const XsSum s0 = xs_sum(xs, n, 0, false), s1 = xs_sum(xs, n, 1, false);
+      const int txE = x0 / 64, kb = x0 - txE * 64, half = (x0 >> 5) & 1;
+      const bool whole = (tl.nx == 1);   // this tile covers its chunk: no second half
+      const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
+      for (int iy = ly; iy < h; iy += kThreads / 32) {
+        const int y = y0 + iy;
+        int tyE = y / 8;
+        if (tyE > g.ny - 1) tyE = g.ny - 1;
+        const int r = y - tyE * 8;
+        double* B0 = xs_block(s0, tyE * g.nx + txE);
+        double* B1 = xs_block(s1, tyE * g.nx + txE);
+        double a0 = 0.0, a1 = 0.0;
+        for (int ix = lx; ix < w; ix += 32) {
+          const int x = x0 + ix;
+          Real o[2];
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            const Real* X4 = x4(c);
+            const Real ax = heat_row<Real>(x, y, n, hsq, [&](int a, int b) { return X4[at(a, b)]; });
+            o[c] = jacobi_update(X4[at(x, y)], rhs(stage, c)[at(x, y)] * sgn, ax, diag);
+          }
+          const size_t gg = (size_t)y * P + x;
+          ox[gg] = o[0];
+          oy[gg] = o[1];
+          const double t0 = (double)(o[0] * o[0]), t1 = (double)(o[1] * o[1]);
+          B0[xs_at(kb + ix, r)] = t0;
+          B1[xs_at(kb + ix, r)] = t1;
+          a0 += t0;
+          a1 += t1;
+        }
+        a0 = warp_sum(a0);
+        a1 = warp_sum(a1);
+        if (lx == 0) {
+          const int j = y * g.nx + txE;
+          s0.tot[2 * j + half] = a0;
+          s1.tot[2 * j + half] = a1;
+          if (whole) {
+            s0.tot[2 * j + 1] = 0.0;
+            s1.tot[2 * j + 1] = 0.0;
+          }
+        }
+      }
+    } else {
       const int w = x1 - x0, h = y1 - y0;
       for_rect(w, h, [&](int ix, int iy) {
         const int x = x0 + ix, y = y0 + iy;
@@ -1020,7 +1200,7 @@ struct Coarse {
 
 template <typename Real>
 __device__ void coarse_vcycle(int lc, double tau, Real* sm, const Real* bx, const Real* by, Real sgn, Real* outx,
-                              Real* outy, bool want_norm, double part[kRedSlots]) {
+                              Real* outy, bool want_norm, double part[kRedSlots], double* xs = nullptr) {
   Coarse<Real> C{sm, tau};
   const int wl = (1 << lc) + 1, Pl = pitch_of(wl);
   {
@@ -1038,6 +1218,39 @@ __device__ void coarse_vcycle(int lc, double tau, Real* sm, const Real* bx, cons
   C.bottom();
   for (int k = 1; k <= lc; ++k) C.up(k);
   const Real *s0 = C.S(lc, C.slot(lc), 0), *s1 = C.S(lc, C.slot(lc), 1);
+  if (xs && want_norm) {
+    // exact sums of |s|^2 in the element-pass geometry (one chunk per row)
+    const XsGeom g(wl);
+    const XsSum q0 = xs_sum(xs, wl, 0, false), q1 = xs_sum(xs, wl, 1, false);
+    const int lx = threadIdx.x & 63, ly = threadIdx.x >> 6, half = lx >> 5;
+    for (int y = ly; y < wl; y += kThreads / 64) {
+      int ty = y / 8;
+      if (ty > g.ny - 1) ty = g.ny - 1;
+      const int r = y - ty * 8;
+      double* B0 = xs_block(q0, ty * g.nx);
+      double* B1 = xs_block(q1, ty * g.nx);
+      double a0 = 0.0, a1 = 0.0;
+      for (int x = lx; x < wl; x += 64) {
+        const int id = y * wl + x;
+        const Real a = s0[id], b = s1[id];
+        const size_t gg = (size_t)y * Pl + x;
+        outx[gg] = a;
+        outy[gg] = b;
+        const double t0 = (double)(a * a), t1 = (double)(b * b);
+        B0[xs_at(x, r)] = t0;
+        B1[xs_at(x, r)] = t1;
+        a0 += t0;
+        a1 += t1;
+      }
+      a0 = warp_sum(a0);
+      a1 = warp_sum(a1);
+      if ((threadIdx.x & 31) == 0) {
+        q0.tot[2 * y * g.nx + half] = a0;
+        q1.tot[2 * y * g.nx + half] = a1;
+      }
+    }
+    return;
+  }
   for_rect(wl, wl, [&](int x, int y) {
     const int id = y * wl + x;
     const Real a = s0[id], b = s1[id];
@@ -1209,17 +1422,18 @@ struct TaskRunner {
     Real* phi = I.arr(a.off_phi[d.cur]);
     Real* de = I.arr(a.off_de);
     Real* s = I.arr(a.off_s);
+    double* xs = a.xs ? a.xs + (size_t)inst * a.xs_stride : nullptr;
     switch (d.kind) {
       case TK_E0: {
         EnergyPass<Real> ps(I, 0, Real(0), Real(0), false, phi, phi + cs, nullptr, nullptr, nullptr, nullptr, nullptr,
-                            nullptr, nullptr, nullptr, smem, part);
+                            nullptr, nullptr, nullptr, smem, part, xs);
         f(ps);
         break;
       }
       case TK_TRIAL: {
         const Real* dd = I.arr(a.off_d[d.dcur]);
         EnergyPass<Real> ps(I, 1, (Real)d.t, Real(0), false, phi, phi + cs, dd, dd + cs, nullptr, nullptr, nullptr,
-                            nullptr, nullptr, nullptr, smem, part);
+                            nullptr, nullptr, nullptr, smem, part, xs);
         f(ps);
         break;
       }
@@ -1227,7 +1441,7 @@ struct TaskRunner {
         const Real* od = I.arr(a.off_d[d.dcur]);
         Real* wd = I.arr(a.off_d[d.dn]);
         EnergyPass<Real> ps(I, 2, (Real)d.t, (Real)d.beta, (d.flags & PF_ODZERO) != 0, phi, phi + cs, od, od + cs, s,
-                            s + cs, de, de + cs, wd, wd + cs, smem, part);
+                            s + cs, de, de + cs, wd, wd + cs, smem, part, xs);
         f(ps);
         break;
       }
@@ -1286,7 +1500,8 @@ struct TaskRunner {
         Real* o = (k == L) ? s : I.arr(a.off_x5[k]);
         Real* oy = (k == L) ? s + cs : o + comp_stride(k);
         UpPass<Real> ps(w, rx, ry, (k == L) ? Real(-1) : Real(1), x2, x2 + comp_stride(k), xc,
-                        xc + comp_stride(k - 1), o, oy, hsq, diag, smem, k == L, part);
+                        xc + comp_stride(k - 1), o, oy, hsq, diag, smem, k == L, part,
+                        (k == L && a.mode != MODE_SMOOTH) ? xs : nullptr);
         f(ps);
         break;
       }
@@ -1311,7 +1526,8 @@ struct TaskRunner {
       const Real* by = (L == lc) ? de + cs : bx + comp_stride(lc);
       Real* out = (L == lc) ? s : I.arr(a.off_x5[lc]);
       Real* outy = (L == lc) ? s + cs : out + comp_stride(lc);
-      coarse_vcycle<Real>(lc, d.vtau, smem, bx, by, (L == lc) ? Real(-1) : Real(1), out, outy, L == lc, part);
+      double* xs = (a.xs && L == lc && a.mode != MODE_SMOOTH) ? a.xs + (size_t)inst * a.xs_stride : nullptr;
+      coarse_vcycle<Real>(lc, d.vtau, smem, bx, by, (L == lc) ? Real(-1) : Real(1), out, outy, L == lc, part, xs);
       return;
     }
     if (d.kind == TK_FLUSH) {
@@ -1367,7 +1583,7 @@ __device__ __forceinline__ void block_sum(const double part[kRedSlots], double (
 // (gradientDescent.h:200-236) and ArmijoLineSearchUsingOp
 // (ArmijoSearch.h:118-200).
 template <typename Real>
-__device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const double* tot) {
+__device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const double* tot, const double* xr) {
   const double lam = a.lambda_inst ? a.lambda_inst[inst] : a.lambda;
   const double tau_min = 9.313225746154785e-10;  // 2^-30 (ArmijoSearch.h:77)
   const double tau_max = 33554432.0;             // 2^25  (ArmijoSearch.h:67)
@@ -1381,6 +1597,14 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
     return e;
   };
   auto quad = [&](double tt) { return 0.5 * ((c.A + 2.0 * tt * c.Bd) + tt * tt * c.Cd); };
+  // exact sums (xr): E_reg = 1/2 (0 + p_x . L p_x + p_y . L p_y), the order of
+  // DisplacementLengthEnergy::apply (hyperelastic.h:178-183)
+  auto ereg_exact = [&]() {
+    double dd = 0.0;
+    dd += xr[1];
+    dd += xr[2];
+    return 0.5 * dd;
+  };
   // the next pass is an energy-type pass: with the NCC data term it starts
   // with energy sub 1 and remembers what it stands for
   auto to = [&](int kind) {
@@ -1525,7 +1749,7 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
   switch (d.kind) {
     case TK_E0: {
       c.A = tot[1];
-      c.energy = energy_of(tot[0], 0.5 * c.A);
+      c.energy = xr ? energy_of(xr[0], ereg_exact()) : energy_of(tot[0], 0.5 * c.A);
       c.energy_new = c.energy;
       if (a.mode == MODE_ENERGY) {
         to(TK_GRAD);
@@ -1567,7 +1791,12 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
         d.kind = TK_DONE;
         break;
       }
-      const double s2 = tot[0];
+      double s2 = tot[0];
+      if (xr) {   // 0 + s_x . s_x + s_y . s_y in the reference's order
+        s2 = 0.0;
+        s2 += xr[0];
+        s2 += xr[1];
+      }
       c.beta = ((c.iter - 1) % 10) ? (s2 / c.og2) : 0.0;
       c.og2 = s2;
       c.attempt = 0;
@@ -1579,8 +1808,13 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
       c.Df = tot[1];
       c.Bd = tot[2];
       c.Cd = tot[3];
+      if (xr) {   // 0 + DE_x . d_x + DE_y . d_y (ArmijoSearch.h:129-131)
+        c.Df = 0.0;
+        c.Df += xr[3];
+        c.Df += xr[4];
+      }
       const double t = c.t, f = c.f;
-      const double fnew = energy_of(tot[0], quad(t));
+      const double fnew = xr ? energy_of(xr[0], ereg_exact()) : energy_of(tot[0], quad(t));
       push_ring(t, fnew);
       const double G = (fnew - f) / (c.Df * t);
       if (c.Df >= 0 || !finite_d(f)) {
@@ -1594,7 +1828,7 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
     }
     case TK_TRIAL: {
       const double t = c.t, f = c.f;
-      const double fnew = energy_of(tot[0], quad(t));
+      const double fnew = xr ? energy_of(xr[0], ereg_exact()) : energy_of(tot[0], quad(t));
       push_ring(t, fnew);
       if (c.ls == 2) {
         end_iteration(fnew);
@@ -1743,6 +1977,22 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
+// Exact sums a completed pass leaves to add (0: none): the energy passes
+// E_data and p . L p per component, the NCG pass also DE . d per component,
+// the top of the V-cycle |s|^2 per component.
+template <typename Real>
+__device__ __forceinline__ int xs_count(const LevelArgs<Real>& a, const PassDesc& d) {
+  if (a.mode == MODE_SMOOTH) return 0;
+  switch (d.kind) {
+    case TK_E0:
+    case TK_TRIAL: return 3;
+    case TK_NCG: return 5;
+    case TK_VUP: return d.k == a.level ? 2 : 0;
+    case TK_COARSE: return a.level == a.lc ? 2 : 0;
+    default: return 0;
+  }
+}
+
 template <typename Real>
 __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, SchedPtrs<Real> sp) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -1752,6 +2002,8 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
   __shared__ TaskSlot slot[2];
   __shared__ int flag_wait, flag_next, flag_last;
   __shared__ InstCtl cs;
+  __shared__ XsSum xss[kXsSlots];
+  __shared__ double xres[kXsSlots], xwtot[kThreads / 32];
   PassTimer pt{a.pass_cycles ? a.pass_cycles + (size_t)blockIdx.x * kPassKinds : nullptr, 0};
   const TaskRunner<Real> run(a, smem);
 
@@ -1867,9 +2119,20 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
         for (int k = 0; k < kRedSlots; ++k) acc[k] += __ldcg(pp + (size_t)i * kRedSlots + k);
       }
       block_sum(acc, wbuf, tot);
+      // exact sums of the pass, in the reference's order
+      const int nxs = a.xs ? xs_count(a, t.desc) : 0;
+      if (nxs) {
+        if (threadIdx.x < nxs) {
+          const bool el = (threadIdx.x == 0) && (t.desc.kind == TK_E0 || t.desc.kind == TK_TRIAL ||
+                                                 t.desc.kind == TK_NCG);
+          xss[threadIdx.x] = xs_sum(a.xs + (size_t)t.inst * a.xs_stride, a.n, threadIdx.x, el);
+        }
+        __syncthreads();
+        xs_reduce(xss, nxs, XsGeom(a.n), xres, xwtot);
+      }
       if (threadIdx.x == 0) {
         ctl_load(cs, sp.ctl + t.inst);
-        advance(a, t.inst, cs, tot);
+        advance(a, t.inst, cs, tot, nxs ? xres : nullptr);
         publish(a, sp, t.inst, cs);
       }
       __syncthreads();

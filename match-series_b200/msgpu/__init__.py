@@ -38,6 +38,7 @@ class Params(ctypes.Structure):
         ("resample_deformation", ctypes.c_int),
         ("use_fp64", ctypes.c_int),
         ("data_term", ctypes.c_int),
+        ("sum_order", ctypes.c_int),
     ]
 
 
@@ -98,7 +99,7 @@ EXPORTS = [
     "msgpu_net_train_step_device", "msgpu_net_loss_grad", "msgpu_prepare_images_device", "msgpu_register_batch_warm",
     "msgpu_register_batch_warm_device", "msgpu_find_xshift_yconst", "msgpu_find_xshift_yconst_device",
     "msgpu_empty_lines_to_nan", "msgpu_empty_lines_to_nan_device", "msgpu_remove_empty_lines",
-    "msgpu_remove_empty_lines_device", "msgpu_set_wait_limits",
+    "msgpu_remove_empty_lines_device", "msgpu_set_wait_limits", "msgpu_set_sum_order",
 ]
 
 
@@ -139,6 +140,7 @@ def lib():
                                                       ctypes.c_void_p, ctypes.c_void_p]
         L.msgpu_set_profiling.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.msgpu_set_data_term.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.msgpu_set_sum_order.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.msgpu_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(Stats)]
         L.msgpu_series_params_default.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(SeriesParams)]
         L.msgpu_series_params_default.restype = None
@@ -672,6 +674,11 @@ class Context:
     def set_data_term(self, data_term: int):
         """0: SSD, 1: normalized cross-correlation, for energy() and gd_level()."""
         self._check(lib().msgpu_set_data_term(self._h, int(data_term)))
+
+    def set_sum_order(self, sum_order: int):
+        """0: the reference's sequential order (default), 1: a fixed parallel
+        order, for the FP64 sums of energy() and gd_level()."""
+        self._check(lib().msgpu_set_sum_order(self._h, int(sum_order)))
 
     def gd_level(self, level, R, T, phix, phiy, lam, max_iter, stop_eps=0.0, fp64=False, max_trace=256):
         px = _f64(phix).copy()

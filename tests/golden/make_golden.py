@@ -10,7 +10,8 @@ CPU oracle and the CUDA path.  Run from the repository root:
 
 (--ncc-only regenerates only the fixtures of the cross-correlation data term,
 --series-only those of the series pipeline: composition, median, stages;
---io-only the array files written by the reference's savers.)
+--io-only the array files written by the reference's savers, --l9-only the
+full-size registration of the benchmark configuration.)
 """
 from __future__ import annotations
 
@@ -302,10 +303,50 @@ def seismic(ref: msor.RefRunner, seed: int):
     np.savez_compressed(os.path.join(OUT, "seismic.npz"), **d)
 
 
+def phi_digest(px, py) -> str:
+    """SHA-256 of a displacement's bytes ([phi_x, phi_y], little-endian float64)."""
+    import hashlib
+    return hashlib.sha256(np.concatenate([px, py]).astype("<f8").tobytes()).hexdigest()
+
+
+def exact_l9(seed: int, frames_n: int = 4):
+    """The benchmark configuration at full size: templates 1..3 of a 513^2
+    hexagonal-lattice series registered to frame 0 on levels 5..9 with 30
+    gradient-flow steps per level, by the reference itself.  The raw frames
+    are Poisson counts (integers), stored as uint8; the displacements (2 x
+    263169 doubles per template) are too large to commit, so the fixture keeps
+    their SHA-256 (a bit-for-bit comparison), every 16th node for
+    diagnostics, and the exact final energies."""
+    from concurrent.futures import ThreadPoolExecutor
+    level, n = 9, n_of(9)
+    fr, _, _ = syn.make_series(n, frames_n, syn.HEX_513, seed=seed)
+    raw = fr.reshape(frames_n, -1)
+    assert np.all(raw == np.round(raw)) and raw.min() >= 0 and raw.max() < 256
+    raw8 = raw.astype(np.uint8)
+    R = msor.RefRunner().normalize(level, raw8[0].astype(np.float64))
+
+    def one(i):
+        ref = msor.RefRunner()
+        T = ref.normalize(level, raw8[i].astype(np.float64))
+        return ref.register(level, 5, 9, R, T, lam=0.1, lam_factor=1.0, max_iter=30)
+
+    with ThreadPoolExecutor(frames_n - 1) as ex:
+        res = list(ex.map(one, range(1, frames_n)))
+    sub = np.s_[::16, ::16]
+    np.savez_compressed(os.path.join(OUT, "exact_L9.npz"), level=level, start=5, stop=9, lam=0.1, max_iter=30,
+                        raw=raw8, energies=np.array([e for _, _, e in res]),
+                        digests=np.array([phi_digest(px, py) for px, py, _ in res]),
+                        phi_sub=np.stack([np.stack([px.reshape(n, n)[sub], py.reshape(n, n)[sub]])
+                                          for px, py, _ in res]))
+
+
 def main():
     if not msor.have_ref():
         raise SystemExit("oracle/_ref/ms_ref is missing: make -f oracle/Makefile.ref")
     ref = msor.RefRunner()
+    if "--l9-only" in sys.argv:
+        exact_l9(9001)
+        return
     if "--seismic-only" in sys.argv:
         seismic(ref, 801)
         return
@@ -336,6 +377,7 @@ def main():
     match_series_conditioned(ref, 6, 4, 623)
     io_files(ref, 701)
     seismic(ref, 801)
+    exact_l9(9001)
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(OUT, f)))

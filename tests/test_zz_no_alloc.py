@@ -1,11 +1,14 @@
 """msgpu_gd_level_noalloc, the level solve for callers that cannot allocate
 device memory, against msgpu_gd_level (the allocating entry point).
 
-Both run the same level kernel, so the results are held to the parity
-tolerances of the FP64 path: displacements within 1e-6 px, energies within
-1e-9 relative, identical step counts.  Several calls in a row share the one
-static scratch array; a smaller level after a larger one checks that
-leftovers of the previous call do not leak into the next."""
+Both run the same level kernel with the global sums in the fixed parallel
+order (the allocating entry point set to sum order 1 for the comparison; the
+exact-sum scratch of the reference order does not fit the static array), so
+the results are held to the parity tolerances of the FP64 path: displacements
+within 1e-6 px, energies within 1e-9 relative, identical step counts.  Several
+calls in a row share the one static scratch array; a smaller level after a
+larger one checks that leftovers of the previous call do not leak into the
+next."""
 import ctypes
 
 import numpy as np
@@ -23,6 +26,13 @@ def _entry():
                   ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     f.restype = ctypes.c_int
     return f
+
+
+@pytest.fixture
+def gpu_parallel_sums(gpu):
+    gpu.set_sum_order(1)
+    yield gpu
+    gpu.set_sum_order(0)
 
 
 def _images(gpu, level, seed):
@@ -51,7 +61,8 @@ def _noalloc(f, level, R, T, phix, phiy, lam, max_iter, fp64):
 
 
 @pytest.mark.parametrize("order", ["large_then_small", "small_then_large"])
-def test_noalloc_matches_gd_level_on_calls_in_a_row(gpu, order):
+def test_noalloc_matches_gd_level_on_calls_in_a_row(gpu_parallel_sums, order):
+    gpu = gpu_parallel_sums
     f = _entry()
     # level 8 in FP64 is the largest solve the scratch array holds
     cases = [(8, 24, 1, 6), (7, 21, 1, 12), (6, 22, 1, 10), (8, 25, 0, 6), (6, 23, 0, 10)]
@@ -70,7 +81,8 @@ def test_noalloc_matches_gd_level_on_calls_in_a_row(gpu, order):
         assert max(np.abs(px - qx).max(), np.abs(py - qy).max()) * (n - 1) <= 1e-6, (level, fp64)
 
 
-def test_noalloc_rejects_levels_beyond_its_scratch(gpu):
+def test_noalloc_rejects_levels_beyond_its_scratch(gpu_parallel_sums):
+    gpu = gpu_parallel_sums
     f = _entry()
     # level 9 needs more than the 12 MiB scratch: refused before any device work
     assert f(9, 16, 16, 16, 0.1, 1, 0.0, 1, None, None, None) == MSGPU_ERR_SIZE
@@ -85,7 +97,8 @@ def test_noalloc_rejects_levels_beyond_its_scratch(gpu):
     assert max(np.abs(px - qx).max(), np.abs(py - qy).max()) * (n - 1) <= 1e-6
 
 
-def test_noalloc_reports_a_stalled_solve_in_its_outputs(gpu):
+def test_noalloc_reports_a_stalled_solve_in_its_outputs(gpu_parallel_sums):
+    gpu = gpu_parallel_sums
     """The call returns before the GPU runs, so a scheduler that gave up
     waiting (its wait bound shortened on purpose) is reported in the outputs:
     steps -1 and energy NaN.  With the default bound the next call is whole."""
