@@ -64,18 +64,27 @@ DATA_TERM = 0   # 0: SSD (deformationModel 22); 1: normalized cross-correlation 
 
 
 def workload(rank: int):
+    """One series: frame FRAMES is the stage's reference on every rank; rank
+    0 registers frames 0..FRAMES-1, rank r > 0 the next FRAMES frames after
+    the reference (a shard of one series of FRAMES * world + 1 frames)."""
     from msgpu import synthetic as syn
     n = (1 << LEVEL) + 1
-    frames, clean, _ = syn.make_series(n, FRAMES + 1, syn.HEX_513, seed=2000 + 1000 * rank)
-    ref = frames[FRAMES].reshape(-1).copy()   # the reference frame of the stage
-    tmpl = frames[:FRAMES].reshape(FRAMES, -1).copy()
-    return ref, tmpl, clean[FRAMES]
+    if rank == 0:
+        frames, clean, _ = syn.make_series(n, FRAMES + 1, syn.HEX_513, seed=2000)
+        return frames[FRAMES].reshape(-1).copy(), frames[:FRAMES].reshape(FRAMES, -1).copy(), clean[FRAMES]
+    rf, rc, _ = syn.make_series(n, 1, syn.HEX_513, seed=2000, first=FRAMES)
+    frames, _, _ = syn.make_series(n, FRAMES, syn.HEX_513, seed=2000, first=FRAMES + 1 + FRAMES * (rank - 1))
+    return rf[0].reshape(-1).copy(), frames.reshape(FRAMES, -1).copy(), rc[0]
+
+
+SUM_ORDER = 0   # 0: the reference's sequential order (bit-exact); 1: parallel order (--sum-order 1)
 
 
 def params(fp64: bool):
     import msgpu
     return msgpu.default_params(precision_level=LEVEL, input_level=LEVEL, start_level=START, stop_level=LEVEL,
-                                max_gd_iterations=MAX_ITER, use_fp64=int(fp64), data_term=DATA_TERM)
+                                max_gd_iterations=MAX_ITER, use_fp64=int(fp64), data_term=DATA_TERM,
+                                sum_order=SUM_ORDER)
 
 
 class ClockSampler:
@@ -233,7 +242,7 @@ def dist_setup():
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
     return world, rank, local
 
 
@@ -291,7 +300,7 @@ def profile_case(level: int, iters: int, fp64: bool):
     frames, _, _ = syn.make_series(n, FRAMES + 1, syn.HEX_513, seed=2000)
     ctx = msgpu.Context(0)
     p = msgpu.default_params(precision_level=level, input_level=level, start_level=level, stop_level=level,
-                             max_gd_iterations=iters, use_fp64=int(fp64), data_term=DATA_TERM)
+                             max_gd_iterations=iters, use_fp64=int(fp64), data_term=DATA_TERM, sum_order=SUM_ORDER)
     ctx.set_profiling(True)
     ctx.register_batch(p, frames[FRAMES], frames[:FRAMES])
     print(json.dumps({"profile_level": level, "frames": FRAMES, "iters": iters, "fp64": fp64,
@@ -447,7 +456,9 @@ def main_series(args, world, rank, local):
                                    f"refinement (levels {START}-{LEVEL}) per template, average and median; "
                                    f"maxGDIterations {MAX_ITER}, lambda {LAMBDA}, "
                                    f"{'NCC' if DATA_TERM else 'SSD'} data term",
-                       "data_term": "ncc" if DATA_TERM else "ssd", "templates_per_gpu": m, "level": LEVEL,
+                       "data_term": "ncc" if DATA_TERM else "ssd",
+                       "sum_order": "reference sequential order (bit-exact)"
+                       if (SUM_ORDER == 0 and fp64 and not DATA_TERM) else "parallel order", "templates_per_gpu": m, "level": LEVEL,
                        "l2": "no flush: per-step working set exceeds the 126 MB L2",
                        "parallelism": f"weak, {world} independent series"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -1013,6 +1024,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--fp32", action="store_true", help="FP32 bulk with FP64 reductions (outside the energy tol)")
+    ap.add_argument("--sum-order", type=int, default=0, choices=[0, 1],
+                    help="0: global sums in the reference's sequential order (bit-exact, default); "
+                         "1: fixed parallel order")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ncc", action="store_true",
                     help="normalized cross-correlation data term (matchSeries' default model) instead of SSD")
@@ -1042,8 +1056,9 @@ def main():
                     help="time matchSeries' whole first stage with accumulated deformations (msgpu_match_series)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    global DATA_TERM
+    global DATA_TERM, SUM_ORDER
     DATA_TERM = 1 if args.ncc else 0
+    SUM_ORDER = args.sum_order
     if args.profile_level:
         return profile_case(args.profile_level, args.profile_iters, not args.fp32)
     if args.profile_compose or args.profile_series:
@@ -1128,13 +1143,30 @@ def main():
     d_e = torch.empty(FRAMES, dtype=torch.float64, device=dev)
     d_s = torch.empty((FRAMES, nlev), dtype=torch.int32, device=dev)
     d_mean = torch.empty(N, dtype=torch.float64, device=dev)
-    d_count = torch.empty(N, dtype=torch.float64, device=dev)
+    d_count = torch.empty(N + 1, dtype=torch.float64, device=dev)   # slot N: fill of pixels without samples
+    d_sum = torch.empty(N, dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream(dev)
 
     def step():
-        ctx.match_series_stage_device(p, d_ref.data_ptr(), d_tmpl.data_ptr(), FRAMES, d_phis.data_ptr(),
-                                      d_e.data_ptr(), d_s.data_ptr(), d_mean.data_ptr(), d_count.data_ptr(),
-                                      stream.cuda_stream)
+        if world == 1:
+            ctx.match_series_stage_device(p, d_ref.data_ptr(), d_tmpl.data_ptr(), FRAMES, d_phis.data_ptr(),
+                                          d_e.data_ptr(), d_s.data_ptr(), d_mean.data_ptr(), d_count.data_ptr(),
+                                          stream.cuda_stream)
+            return
+        # sharded stage: every rank registers its frames; the average needs the
+        # ranks' per-pixel sums and counts added (one NCCL all-reduce each)
+        import torch.distributed as dist
+        ctx.register_batch_device(p, d_ref.data_ptr(), d_tmpl.data_ptr(), FRAMES, d_phis.data_ptr(), d_e.data_ptr(),
+                                  d_s.data_ptr(), 0, stream.cuda_stream)
+        last = rank == world - 1   # holds the series' last frame: its mean fills empty pixels
+        ctx.warp_sum_device(LEVEL, d_tmpl.data_ptr(), d_phis.data_ptr(), FRAMES, d_sum.data_ptr(), d_count.data_ptr(),
+                            d_count[N:].data_ptr() if last else 0, stream.cuda_stream)
+        if not last:
+            d_count[N:].zero_()
+        dist.all_reduce(d_sum)
+        dist.all_reduce(d_count)
+        ctx.mean_from_sums_device(LEVEL, d_sum.data_ptr(), d_count.data_ptr(), d_count[N:].data_ptr(),
+                                  d_mean.data_ptr(), stream.cuda_stream)
 
     for _ in range(args.warmup):
         step()
@@ -1175,11 +1207,25 @@ def main():
             torch.zeros((FRAMES, nlev), dtype=torch.int32).pin_memory().numpy(),
             torch.zeros(N, dtype=torch.float64).pin_memory().numpy(),
             torch.zeros(N, dtype=torch.float64).pin_memory().numpy())
-    ctx.match_series_stage(p, h_ref, h_tmpl, out=outs)
+    def e2e_step():
+        if world == 1:
+            ctx.match_series_stage(p, h_ref, h_tmpl, out=outs)
+            return
+        # host buffers in and out around the sharded device step
+        d_ref.copy_(torch.from_numpy(h_ref), non_blocking=True)
+        d_tmpl.copy_(torch.from_numpy(h_tmpl), non_blocking=True)
+        step()
+        outs[0][...] = d_phis.cpu().numpy()
+        outs[1][...] = d_e.cpu().numpy()
+        outs[2][...] = d_s.cpu().numpy()
+        outs[3][...] = d_mean.cpu().numpy()
+        outs[4][...] = d_count[:N].cpu().numpy()
+
+    e2e_step()
     barrier(world)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        ctx.match_series_stage(p, h_ref, h_tmpl, out=outs)
+        e2e_step()
     e2e_s = allreduce_max(time.perf_counter() - t0, world)
     e2e_value = world * FRAMES * args.steps / e2e_s
     h2d = (1 + FRAMES) * N * 8
@@ -1205,6 +1251,8 @@ def main():
                              f"registration phase {secs:.1f} s"}
             dphi = float(np.abs(phis[:nfr] - rphis).max()) * (n - 1)
             rel = float(np.max(np.abs(energies[:nfr] - renergies) / np.abs(renergies)))
+            identical = int(sum(np.array_equal(phis[f], rphis[f]) and energies[f] == renergies[f]
+                                for f in range(nfr)))
             # the reference's own sensitivity: the same frames with every pixel
             # of the reference frame moved by one ulp in a random direction (a
             # perturbation of the size of a reordered floating-point sum)
@@ -1215,7 +1263,8 @@ def main():
                 _, _, pphis, penergies, _, _ = run_reference_sample(ref_p, tmpl, procs, wd)
             sp_dphi = float(np.abs(pphis - rphis).max()) * (n - 1)
             sp_rel = float(np.max(np.abs(penergies - renergies) / np.abs(renergies)))
-            accuracy = {"frames_checked": nfr, "max_dphi_px": dphi, "max_rel_energy": rel,
+            accuracy = {"frames_checked": nfr, "frames_bit_identical": identical,
+                        "max_dphi_px": dphi, "max_rel_energy": rel,
                         "tolerance": {"dphi_px": 1e-3, "rel_energy": 1e-6},
                         "within_tolerance": bool(dphi <= 1e-3 and rel <= 1e-6),
                         "reference_1ulp_spread": {"max_dphi_px": sp_dphi, "max_rel_energy": sp_rel,
@@ -1234,7 +1283,10 @@ def main():
                        "frames_per_gpu": FRAMES, "level": LEVEL, "start_level": START,
                        "max_gd_iterations": MAX_ITER, "lambda": LAMBDA,
                        "l2": "no flush: per-step working set (~0.6 GB) exceeds the 126 MB L2",
-                       "parallelism": f"weak, {world} independent series"},
+                       "parallelism": ("one GPU" if world == 1 else
+                                       f"weak: {world} ranks register {FRAMES} frames each of one series against "
+                                       f"its reference; the average adds the ranks' per-pixel sums and counts "
+                                       f"(NCCL all-reduce)")},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": f"level_kernel<{'double' if fp64 else 'float'}> level {LEVEL}",

@@ -124,6 +124,22 @@ int msgpu_warp_mean(msgpu_context* ctx, int level, const double* frames, const d
 int msgpu_warp_mean_device(msgpu_context* ctx, int level, const double* d_frames, const double* d_phis,
                            int num_frames, double* d_mean_out, double* d_count_out, void* stream);
 
+/* The average of a stage whose frames are sharded over several GPUs (no
+ * single counterpart in the reference, which averages in one process):
+ * msgpu_warp_sum_device gives, for this rank's frames, the per-pixel sum of
+ * the finite warped samples and their number (averageSeries,
+ * matchSeries.h:410-425) and, when d_last_mean_out is not NULL, the mean of
+ * its last frame (the fill of pixels without samples when this rank holds
+ * the series' last frame); the caller adds the ranks' sums and counts (one
+ * all-reduce, e.g. NCCL) and msgpu_mean_from_sums_device divides:
+ * mean = sum / count, or *d_fill where count is 0.  The result equals
+ * msgpu_warp_mean over all frames up to the order of the per-pixel sums.   */
+int msgpu_warp_sum_device(msgpu_context* ctx, int level, const double* d_frames, const double* d_phis,
+                          int num_frames, double* d_sum_out, double* d_count_out, double* d_last_mean_out,
+                          void* stream);
+int msgpu_mean_from_sums_device(msgpu_context* ctx, int level, const double* d_sum, const double* d_count,
+                                const double* d_fill, double* d_mean_out, void* stream);
+
 /* One stage of series matching in one call: msgpu_register_batch followed by
  * msgpu_warp_mean of the raw templates with their displacements (the stage
  * loop of matchSeries<>(), matchSeries.h:1284-1316, with averageSeries).

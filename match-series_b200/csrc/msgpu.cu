@@ -543,6 +543,44 @@ __global__ void k_warp_mean(const double* __restrict__ frames, const double* __r
   }
 }
 
+// The per-rank part of the average of a sharded stage: per pixel the sum of
+// the finite warped samples of this rank's frames (in frame order) and their
+// number, as k_warp_mean accumulates them (averageSeries, matchSeries.h:
+// 410-425); the ranks' sums and counts are then added by one all-reduce.
+__global__ void k_warp_sum(const double* __restrict__ frames, const double* __restrict__ phis, int F, int level,
+                           double* sum, double* count) {
+  const int n = lvl_n(level);
+  const int N = n * n;
+  const double h = 1.0 / (double)(n - 1);
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < N; j += gridDim.x * blockDim.x) {
+    const int x = j % n, y = j / n;
+    double acc = 0;
+    int k = 0;
+    for (int f = 0; f < F; ++f) {
+      const double* ph = phis + (size_t)f * 2 * N;
+      const double d0 = x + ph[j] / h, d1 = y + ph[N + j] / h;
+      bool in = true;
+      if (d0 < 0. || d0 > (double)(n - 1) || isnan(d0)) in = false;
+      if (d1 < 0. || d1 > (double)(n - 1) || isnan(d1)) in = false;
+      const double v = in ? interp_d(frames + (size_t)f * N, n, d0, d1) : INFINITY;
+      if (v != INFINITY) {
+        acc += v;
+        ++k;
+      }
+    }
+    sum[j] = acc;
+    count[j] = k;
+  }
+}
+
+// mean = sum / count where a pixel has samples, else *fill.
+__global__ void k_mean_from_sums(const double* sum, const double* count, int N, const double* fill, double* mean) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < N; j += gridDim.x * blockDim.x) {
+    const double k = count[j];
+    mean[j] = (k > 0) ? sum[j] / k : *fill;
+  }
+}
+
 __global__ void k_mean(const double* a, int N, double* out) {
   __shared__ double sm[32];
   double s = 0;
@@ -1608,6 +1646,43 @@ int msgpu_warp_mean_device(msgpu_context* ctx, int level, const double* d_frames
                                                                d_count_out);
   CK(cudaGetLastError());
   ctx->stats.kernel_launches += 2;
+  return MSGPU_OK;
+}
+
+int msgpu_warp_sum_device(msgpu_context* ctx, int level, const double* d_frames, const double* d_phis,
+                          int num_frames, double* d_sum_out, double* d_count_out, double* d_last_mean_out,
+                          void* stream) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (level < 1 || level > kMaxLevel || num_frames < 0 || (num_frames > 0 && (!d_frames || !d_phis)) ||
+      !d_sum_out || !d_count_out)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid warp_sum arguments");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int N = (int)lvl_N(level);
+  if (num_frames > 0 && d_last_mean_out) {
+    k_mean<<<1, 1024, 0, st>>>(d_frames + (size_t)(num_frames - 1) * N, N, d_last_mean_out);
+    ++ctx->stats.kernel_launches;
+  }
+  k_warp_sum<<<std::min(2048, (N + 255) / 256), 256, 0, st>>>(d_frames, d_phis, num_frames, level, d_sum_out,
+                                                              d_count_out);
+  CK(cudaGetLastError());
+  ++ctx->stats.kernel_launches;
+  return MSGPU_OK;
+}
+
+int msgpu_mean_from_sums_device(msgpu_context* ctx, int level, const double* d_sum, const double* d_count,
+                                const double* d_fill, double* d_mean_out, void* stream) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (level < 1 || level > kMaxLevel || !d_sum || !d_count || !d_fill || !d_mean_out)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid mean_from_sums arguments");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  const int N = (int)lvl_N(level);
+  k_mean_from_sums<<<std::min(2048, (N + 255) / 256), 256, 0, (cudaStream_t)stream>>>(d_sum, d_count, N, d_fill,
+                                                                                       d_mean_out);
+  CK(cudaGetLastError());
+  ++ctx->stats.kernel_launches;
   return MSGPU_OK;
 }
 

@@ -99,7 +99,8 @@ EXPORTS = [
     "msgpu_net_train_step_device", "msgpu_net_loss_grad", "msgpu_prepare_images_device", "msgpu_register_batch_warm",
     "msgpu_register_batch_warm_device", "msgpu_find_xshift_yconst", "msgpu_find_xshift_yconst_device",
     "msgpu_empty_lines_to_nan", "msgpu_empty_lines_to_nan_device", "msgpu_remove_empty_lines",
-    "msgpu_remove_empty_lines_device", "msgpu_set_wait_limits", "msgpu_set_sum_order",
+    "msgpu_remove_empty_lines_device", "msgpu_set_wait_limits", "msgpu_set_sum_order", "msgpu_warp_sum_device",
+    "msgpu_mean_from_sums_device",
 ]
 
 
@@ -219,6 +220,11 @@ def lib():
         L.msgpu_register_ragged_device.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params),
                                                    ctypes.POINTER(SeriesDesc), ctypes.c_int, ctypes.c_void_p]
         L.msgpu_set_wait_limits.argtypes = [ctypes.c_double, ctypes.c_double]
+        L.msgpu_warp_sum_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_void_p]
+        L.msgpu_mean_from_sums_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -421,6 +427,18 @@ class Context:
                          stream: int = 0):
         self._check(lib().msgpu_warp_mean_device(self._h, level, d_frames, d_phis, num_frames, d_mean, d_count,
                                                  stream or None))
+
+    def warp_sum_device(self, level: int, d_frames: int, d_phis: int, num_frames: int, d_sum: int, d_count: int,
+                        d_last_mean: int = 0, stream: int = 0):
+        """Per-pixel sums of the finite warped samples and their counts of
+        this rank's frames (device pointers); see msgpu_warp_sum_device."""
+        self._check(lib().msgpu_warp_sum_device(self._h, level, d_frames, d_phis, num_frames, d_sum, d_count,
+                                                d_last_mean or None, stream or None))
+
+    def mean_from_sums_device(self, level: int, d_sum: int, d_count: int, d_fill: int, d_mean: int,
+                              stream: int = 0):
+        self._check(lib().msgpu_mean_from_sums_device(self._h, level, d_sum, d_count, d_fill, d_mean,
+                                                      stream or None))
 
     def match_series_stage(self, params: Params, reference, templates, out=None):
         """register_batch + warp_mean in one call; returns (phis, energies, steps, mean, count).

@@ -6,7 +6,10 @@ ranks without any exchange.  The only collective is the reconstruction: each
 rank warps its own frames and the per-pixel sums of finite samples and their
 counts are summed over ranks with one all-reduce (averageSeries,
 matchSeries.h:410-425); pixels without any sample take the mean of the
-series' last frame.
+series' last frame.  On the GPU the per-rank part is msgpu_warp_sum_device
+and the division msgpu_mean_from_sums_device (Context.warp_sum_device,
+Context.mean_from_sums_device); the helpers below are the same steps on host
+arrays.
 """
 from __future__ import annotations
 

@@ -98,24 +98,26 @@ def smooth_displacement(n: int, spec: LatticeSpec, rng: np.random.Generator):
 
 
 def make_series(n: int, num_frames: int, spec: LatticeSpec = HEX_513, seed: int = 2000,
-                noise: bool = True):
+                noise: bool = True, first: int = 0):
     """Returns (frames[F, n, n] float64 counts, clean[F, n, n], disp[F, 2, n, n]).
 
     Frame f uses the generator seeded with ``seed + f``; the lattice amplitudes
-    are shared by the series (seeded with ``seed``)."""
+    are shared by the series (seeded with ``seed``).  ``first`` > 0 returns
+    frames first .. first + num_frames - 1 of the same series (a shard)."""
     y, x = np.mgrid[0:n, 0:n].astype(np.float64)
     frames = np.empty((num_frames, n, n))
     clean = np.empty((num_frames, n, n))
     disp = np.empty((num_frames, 2, n, n))
-    for f in range(num_frames):
+    for i in range(num_frames):
+        f = first + i
         rng = np.random.default_rng(seed + f)
         u, v = smooth_displacement(n, spec, rng)
         u = u + rng.normal(0.0, spec.jitter, size=(n, 1))
         img = clean_image(n, spec, x + u, y + v, amp_seed=seed)
-        clean[f] = spec.peak * img
-        disp[f, 0] = u
-        disp[f, 1] = v
-        frames[f] = rng.poisson(spec.peak * img).astype(np.float64) if noise else spec.peak * img
+        clean[i] = spec.peak * img
+        disp[i, 0] = u
+        disp[i, 1] = v
+        frames[i] = rng.poisson(spec.peak * img).astype(np.float64) if noise else spec.peak * img
     return frames, clean, disp
 
 
