@@ -380,8 +380,18 @@ typedef struct {
    * V-cycle, V-cycle up, NCG + first trial, further line-search trials,
    * waiting for work and completing passes                                 */
   long long level_pass_cycles[16][8];
+  int graph_replayed;           /* 1: the last device batch call replayed a
+                                   captured CUDA graph (one launch)          */
 } msgpu_stats;
 int msgpu_set_profiling(msgpu_context* ctx, int on);
+/* CUDA graphs for msgpu_register_batch_device (and the stage entry points
+ * built on it), default on: the second call with the same parameters and
+ * buffers captures the batch's launches (per level: the level kernel, the
+ * collection of the results, the prolongation; before them the image
+ * preparation) into one graph, later such calls replay it as a single
+ * launch.  The first call after a change of parameters or buffers runs
+ * directly.  No counterpart in the reference.                             */
+int msgpu_set_graphs(msgpu_context* ctx, int on);
 int msgpu_get_stats(const msgpu_context* ctx, msgpu_stats* out);
 
 /* --- single operators of the path (parity entry points) ----------------- */

@@ -45,6 +45,19 @@ struct msgpu_context {
   int data_term = 0;           // data term of the single-operator entry points
   int sum_order = 0;           // order of the global sums of the single-operator entry points
   Buf xsum;                    // exact sums: per-instance term blocks and chunk summaries
+  // CUDA graph of the last device batch call (msgpu_register_batch_device):
+  // captured on the second call with the same parameters and buffers, then
+  // replayed as one launch while they stay the same
+  struct Graph {
+    std::vector<unsigned char> key;
+    int seen = 0;                // calls with this key so far
+    cudaGraphExec_t exec = nullptr;
+    int launches = 0;            // kernels in the graph
+    unsigned long long epoch = 0;  // alloc_epoch when it was captured
+  } graph;
+  unsigned long long alloc_epoch = 0;   // counts reallocations of the context's buffers
+  bool use_graphs = true;
+  cudaStream_t graph_stream = nullptr;
   int* sched_error = nullptr;  // device flag of the level scheduler (in flags)
   // statistics of the last batch call
   bool profiling = false;
@@ -90,6 +103,7 @@ int fail(msgpu_context* ctx, int code, const char* fmt, ...) {
 
 int ensure(msgpu_context* ctx, msgpu_context::Buf& b, size_t bytes) {
   if (b.cap >= bytes) return MSGPU_OK;
+  ++ctx->alloc_epoch;   // a captured graph holding the old address is stale now
   if (b.p) CK(cudaFree(b.p));
   b.p = nullptr;
   b.cap = 0;
@@ -1046,6 +1060,62 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
   return MSGPU_OK;
 }
 
+// One device batch through a CUDA graph.  The first call with a given set of
+// parameters and buffers runs directly (and sizes every buffer); the second
+// captures the same work on the context's capture stream and replays it; later
+// calls with the same key replay the instantiated graph on the caller's
+// stream as a single launch.  A capture that fails (an operation the graph
+// cannot hold) turns graphs off for the context and the call runs directly.
+int run_batch_graph(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& io, cudaStream_t st) {
+  auto direct = [&]() {
+    return p.use_fp64 ? run_batch<double>(ctx, p, F, io, st) : run_batch<float>(ctx, p, F, io, st);
+  };
+  std::vector<unsigned char> key(sizeof(p) + sizeof(F) + sizeof(io));
+  memcpy(key.data(), &p, sizeof(p));
+  memcpy(key.data() + sizeof(p), &F, sizeof(F));
+  memcpy(key.data() + sizeof(p) + sizeof(F), &io, sizeof(io));
+  msgpu_context::Graph& g = ctx->graph;
+  if (g.key != key || (g.exec && g.epoch != ctx->alloc_epoch)) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+    g.key = key;
+    g.seen = 0;
+  }
+  if (g.exec) {
+    CK(cudaGraphLaunch(g.exec, st));
+    ctx->stats.kernel_launches = g.launches;
+    ctx->stats.graph_replayed = 1;
+    return MSGPU_OK;
+  }
+  if (++g.seen < 2) return direct();
+  if (!ctx->graph_stream) CK(cudaStreamCreateWithFlags(&ctx->graph_stream, cudaStreamNonBlocking));
+  const unsigned long long epoch = ctx->alloc_epoch;
+  CK(cudaStreamBeginCapture(ctx->graph_stream, cudaStreamCaptureModeThreadLocal));
+  const int rc = p.use_fp64 ? run_batch<double>(ctx, p, F, io, ctx->graph_stream)
+                            : run_batch<float>(ctx, p, F, io, ctx->graph_stream);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(ctx->graph_stream, &graph);
+  cudaGraphExec_t exec = nullptr;
+  // a buffer that grew during the capture (it must not: the first call sized
+  // them) would leave the graph with a freed address
+  const bool ok = rc == MSGPU_OK && ce == cudaSuccess && graph && epoch == ctx->alloc_epoch &&
+                  cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+  if (graph) cudaGraphDestroy(graph);
+  if (!ok) {
+    if (exec) cudaGraphExecDestroy(exec);
+    cudaGetLastError();   // a refused capture leaves a sticky-free error state
+    ctx->use_graphs = false;
+    g.key.clear();
+    return direct();
+  }
+  g.exec = exec;
+  g.epoch = epoch;
+  g.launches = ctx->stats.kernel_launches;
+  CK(cudaGraphLaunch(g.exec, st));
+  ctx->stats.graph_replayed = 1;
+  return MSGPU_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Ragged batches: series of different sizes, each registered to its own
 // reference, one level-kernel launch per level for all of them.
@@ -1520,6 +1590,18 @@ int msgpu_set_wait_limits(double level_wait_s, double barrier_wait_s) {
   return MSGPU_OK;
 }
 
+int msgpu_set_graphs(msgpu_context* ctx, int on) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  ctx->use_graphs = on != 0;
+  if (!ctx->use_graphs && ctx->graph.exec) {
+    cudaGraphExecDestroy(ctx->graph.exec);
+    ctx->graph.exec = nullptr;
+  }
+  ctx->graph.key.clear();
+  ctx->graph.seen = 0;
+  return MSGPU_OK;
+}
+
 int msgpu_set_sum_order(msgpu_context* ctx, int sum_order) {
   if (!ctx) return MSGPU_ERR_INVALID_ARG;
   if (sum_order != 0 && sum_order != 1) return fail(ctx, MSGPU_ERR_INVALID_ARG, "sum_order must be 0 or 1");
@@ -1560,7 +1642,10 @@ int msgpu_destroy(msgpu_context* ctx) {
   msgpu_context::Buf* bufs[] = {&ctx->arena, &ctx->shared_real, &ctx->dscratch, &ctx->small, &ctx->phis_d,
                                 &ctx->io[0], &ctx->io[1],   &ctx->io[2],    &ctx->io[3], &ctx->io[4],
                                 &ctx->io[5], &ctx->prof,    &ctx->sched,    &ctx->flags, &ctx->nccbuf,
-                                &ctx->ext,   &ctx->series,  &ctx->vals,  &ctx->xs_basis, &ctx->xs_work};
+                                &ctx->ext,   &ctx->series,  &ctx->vals,  &ctx->xs_basis, &ctx->xs_work,
+                                &ctx->xsum};
+  if (ctx->graph.exec) cudaGraphExecDestroy(ctx->graph.exec);
+  if (ctx->graph_stream) cudaStreamDestroy(ctx->graph_stream);
   for (auto* b : bufs)
     if (b->p) cudaFree(b->p);
   if (ctx->ev_ready)
@@ -1586,6 +1671,8 @@ int msgpu_register_batch_device(msgpu_context* ctx, const msgpu_params* p, const
   if ((rc = bind_device(ctx))) return rc;
   BatchIO io{d_reference, d_templates, d_initial_phis, d_phis_out, d_energies_out, d_steps_out};
   cudaStream_t st = (cudaStream_t)stream;
+  ctx->stats.graph_replayed = 0;
+  if (ctx->use_graphs && !ctx->profiling) return run_batch_graph(ctx, *p, num_templates, io, st);
   return p->use_fp64 ? run_batch<double>(ctx, *p, num_templates, io, st)
                      : run_batch<float>(ctx, *p, num_templates, io, st);
 }

@@ -70,7 +70,7 @@ class Stats(ctypes.Structure):
     _fields_ = [("kernel_launches", ctypes.c_int), ("num_levels", ctypes.c_int), ("first_level", ctypes.c_int),
                 ("level_ms", ctypes.c_float * 16), ("level_steps", ctypes.c_longlong * 16),
                 ("level_evals", ctypes.c_longlong * 16), ("level_cluster", ctypes.c_int * 16),
-                ("level_pass_cycles", (ctypes.c_longlong * 8) * 16)]
+                ("level_pass_cycles", (ctypes.c_longlong * 8) * 16), ("graph_replayed", ctypes.c_int)]
 
 PASS_KINDS = ["energy0", "gradient", "vdown", "vcoarse", "vup", "ncg", "energy", "sync"]
 
@@ -100,7 +100,7 @@ EXPORTS = [
     "msgpu_register_batch_warm_device", "msgpu_find_xshift_yconst", "msgpu_find_xshift_yconst_device",
     "msgpu_empty_lines_to_nan", "msgpu_empty_lines_to_nan_device", "msgpu_remove_empty_lines",
     "msgpu_remove_empty_lines_device", "msgpu_set_wait_limits", "msgpu_set_sum_order", "msgpu_warp_sum_device",
-    "msgpu_mean_from_sums_device",
+    "msgpu_mean_from_sums_device", "msgpu_set_graphs",
 ]
 
 
@@ -140,6 +140,7 @@ def lib():
                                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                       ctypes.c_void_p, ctypes.c_void_p]
         L.msgpu_set_profiling.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.msgpu_set_graphs.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.msgpu_set_data_term.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.msgpu_set_sum_order.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.msgpu_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(Stats)]
@@ -650,6 +651,10 @@ class Context:
     def set_profiling(self, on: bool):
         self._check(lib().msgpu_set_profiling(self._h, int(bool(on))))
 
+    def set_graphs(self, on: bool):
+        """CUDA-graph capture and replay of the device batch calls (default on)."""
+        self._check(lib().msgpu_set_graphs(self._h, int(bool(on))))
+
     def stats(self) -> dict:
         s = Stats()
         self._check(lib().msgpu_get_stats(self._h, ctypes.byref(s)))
@@ -657,7 +662,8 @@ class Context:
         return {"kernel_launches": s.kernel_launches, "first_level": s.first_level,
                 "level_ms": list(s.level_ms[:k]), "level_steps": list(s.level_steps[:k]),
                 "level_evals": list(s.level_evals[:k]), "level_cluster": list(s.level_cluster[:k]),
-                "level_pass_cycles": [dict(zip(PASS_KINDS, list(s.level_pass_cycles[i]))) for i in range(k)]}
+                "level_pass_cycles": [dict(zip(PASS_KINDS, list(s.level_pass_cycles[i]))) for i in range(k)],
+                "graph_replayed": bool(s.graph_replayed)}
 
     # --- single operators ------------------------------------------------
     def energy(self, level, R, T, phix, phiy, lam, fp64=False):

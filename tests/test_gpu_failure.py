@@ -110,6 +110,12 @@ def test_constant_frame_under_ncc_follows_the_reference_trace(gpu, oracle, which
     rx, ry, re, rsteps, rtr = oracle.gd_level(level, R, T, z, z, 0.1, 10, ncc=True)
     assert steps == rsteps and e == re == 0.0
     assert np.array_equal(px, rx) and np.array_equal(py, ry) and not px.any()
-    got = [(row[1], row[2], int(row[3])) for row in tr]
-    want = [(t[2], t[3], t[4]) for t in rtr]
-    assert got == want
+    # accepted tau (0) and the filter width of every step as in the reference
+    assert [(row[1], row[2]) for row in tr] == [(t[2], t[3]) for t in rtr]
+    if which == "template":
+        # and the number of line-search evaluations
+        assert [int(row[3]) for row in tr] == [t[4] for t in rtr]
+    # (a constant reference is normalised to rounding noise: its mean differs
+    # from the constant in the last bits, so the descent direction is noise
+    # of the order of the unit roundoff and the length of each futile line
+    # search depends on the order of the normalisation's sums)
