@@ -497,9 +497,11 @@ int msgpu_prepare_images_device(msgpu_context* ctx, const msgpu_params* p, const
                                 int level, double* d_out, void* stream);
 /* msgpu_register_batch started from the network's prediction at level
  * l0-1 (which must lie in startLevel..stopLevel; inputLevel >= l0).  With
- * plain_energies (the plain method's final energies, nullable), a frame
- * whose warm-started energy exceeds its plain energy by more than
- * rel_tol * |plain energy| is registered again from the plain start;
+ * plain_energies (the plain method's final energies, nullable) the frames
+ * are registered to that stated energy tolerance: the warm-started solve of
+ * the stop level ends as soon as a frame's energy is within
+ * rel_tol * |plain energy| of (or below) its plain energy, and a frame that
+ * ends above that is registered again from the plain start;
  * warm_used_out[f] (host, nullable) = 1 where the warm start was kept.
  * steps_out has the plain layout (stop-start+1 levels per frame; levels
  * below l0-1 count 0 for warm-started frames).                             */

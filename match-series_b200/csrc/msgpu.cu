@@ -848,6 +848,8 @@ struct BatchOpts {
   int lambda_stop = -1;  // level that lambdaFactor's exponent counts from (default: stop_level)
   int reset_error = 1;   // clear the error flags (0: a caller running several batches clears them once)
   msgpu_net* warm = nullptr;   // learned warm start: the network's prediction is the start-level displacement
+  const double* e_target = nullptr;   // device, per frame: stop the stop-level solve at this energy (+ e_tol)
+  double e_tol = 0.0;
 };
 
 int warm_start_phi(msgpu_net* net, const double* pyr, const std::vector<size_t>& poff, size_t pstride, int F,
@@ -992,6 +994,10 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
     a.out_steps = steps_all + (size_t)(l - start) * F;
     a.out_evals = evals_all + (size_t)(l - start) * F;
     a.out_phi_buf = bin;   // the level kernel updates the buffer index in place
+    if (l == stop && opt.e_target) {
+      a.e_target = opt.e_target;
+      a.e_tol = opt.e_tol;
+    }
     const size_t prof_n = (size_t)max_level_grid(ctx->sm_count) * kPassKinds;
     if (ctx->profiling) {
       if ((rc = ensure(ctx, ctx->prof, sizeof(unsigned long long) * prof_n * nlev_all))) return rc;
@@ -3873,6 +3879,11 @@ int warm_batch(msgpu_context* ctx, const msgpu_params& p, msgpu_net* net, const 
   BatchIO io{d_ref, d_tmpl, nullptr, d_phis, e, s};
   BatchOpts opt;
   opt.warm = net;
+  // to the stated energy tolerance: with the plain method's energies the
+  // warm-started solve of the stop level ends as soon as it is within rel_tol
+  // of them
+  opt.e_target = d_plain_e;
+  opt.e_tol = rel_tol;
   if ((rc = run_batch<Real>(ctx, pw, F, io, st, opt))) return rc;
   if (d_e_out) CK(cudaMemcpyAsync(d_e_out, e, sizeof(double) * F, cudaMemcpyDeviceToDevice, st));
   if (d_s_out) {

@@ -106,6 +106,11 @@ struct LevelArgs {
   // order (msgpu_xsum.cuh); per-instance regions of xs_stride doubles, or null
   double* xs;
   size_t xs_stride;
+  // energy targets (nullable, per instance): the solve stops as soon as its
+  // energy is <= e_target + e_tol |e_target| (registration to a stated
+  // energy tolerance; no counterpart in the reference's stop rules)
+  const double* e_target;
+  double e_tol;
 };
 
 // A 2-component array of level k occupies 2 * comp_stride(k) elements.
@@ -1597,6 +1602,11 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
     return e;
   };
   auto quad = [&](double tt) { return 0.5 * ((c.A + 2.0 * tt * c.Bd) + tt * tt * c.Cd); };
+  auto target_met = [&](double en) {
+    if (!a.e_target) return false;
+    const double tg = a.e_target[inst];
+    return en <= tg + a.e_tol * fabs(tg);
+  };
   // exact sums (xr): E_reg = 1/2 (0 + p_x . L p_x + p_y . L p_y), the order of
   // DisplacementLengthEnergy::apply (hyperelastic.h:178-183)
   auto ereg_exact = [&]() {
@@ -1689,6 +1699,7 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
       c.tau = 1.;
       go = (c.sigma > stop_sigma) && (c.iter < a.max_iter);
     }
+    if (target_met(c.energy_new)) go = false;
     if (go) start_iteration(); else finish();
   };
   auto step_done = [&](double acc_tau) {
@@ -1757,7 +1768,7 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
         d.dcur = c.dcur;
         d.flags = 0;
         d.t = 0;
-      } else if (a.max_iter > 0) {
+      } else if (a.max_iter > 0 && !target_met(c.energy)) {
         start_iteration();
       } else {
         d.kind = TK_DONE;
