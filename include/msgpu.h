@@ -32,6 +32,18 @@ typedef enum {
 
 typedef struct msgpu_context msgpu_context;
 
+/* Scheduling of the level kernel on one level (no counterpart in the
+ * reference).  The results do not depend on it: every tile keeps its own
+ * partial sums and a pass adds them in a fixed order.                      */
+typedef struct {
+  int chunk_div;     /* a pass is handed out in chunks of ntiles / chunk_div
+                        tiles (0: default 24)                                */
+  int chunk_max;     /* at most chunk_max tiles per chunk (0: default 16)    */
+  int ctas_per_sm;   /* CTAs of the persistent grid per SM (0: as many as
+                        fit, which is 2)                                    */
+  float ms;          /* msgpu_autotune_device: the level's measured time    */
+} msgpu_level_tuning;
+
 /* The parameter-file keys of the registration path (names as in the
  * reference's .par files; see msgpu_params_default for the defaults).       */
 typedef struct {
@@ -382,6 +394,11 @@ typedef struct {
   long long level_pass_cycles[16][8];
   int graph_replayed;           /* 1: the last device batch call replayed a
                                    captured CUDA graph (one launch)          */
+  /* exact sums (sum order 0) per level: completed passes that added sums,
+   * clock cycles of their three steps (binade predictions, chunk summaries,
+   * the ordered walk; summed over the passes), chunks walked, chunks added
+   * term by term                                                            */
+  long long level_xs[16][6];
 } msgpu_stats;
 int msgpu_set_profiling(msgpu_context* ctx, int on);
 /* CUDA graphs for msgpu_register_batch_device (and the stage entry points
@@ -392,6 +409,18 @@ int msgpu_set_profiling(msgpu_context* ctx, int on);
  * launch.  The first call after a change of parameters or buffers runs
  * directly.  No counterpart in the reference.                             */
 int msgpu_set_graphs(msgpu_context* ctx, int on);
+
+/* The scheduling table of a context, per precision (use_fp64 0 or 1) and
+ * level, and its autotuner: msgpu_autotune_device runs the batch of
+ * msgpu_register_batch_device (same arguments; d_phis_scratch receives
+ * num_templates * 2 * N doubles) once per candidate setting (chunk_div in
+ * {12, 24, 48}, chunk_max in {8, 16, 32}, 1 or 2 CTAs per SM), times every
+ * level's launch with CUDA events, and keeps for each level startLevel ..
+ * stopLevel the fastest setting.  Synchronous.                            */
+int msgpu_get_tuning(const msgpu_context* ctx, int use_fp64, int level, msgpu_level_tuning* out);
+int msgpu_set_tuning(msgpu_context* ctx, int use_fp64, int level, const msgpu_level_tuning* t);
+int msgpu_autotune_device(msgpu_context* ctx, const msgpu_params* p, const double* d_reference,
+                          const double* d_templates, int num_templates, double* d_phis_scratch, void* stream);
 int msgpu_get_stats(const msgpu_context* ctx, msgpu_stats* out);
 
 /* --- single operators of the path (parity entry points) ----------------- */

@@ -58,6 +58,9 @@ struct msgpu_context {
   unsigned long long alloc_epoch = 0;   // counts reallocations of the context's buffers
   bool use_graphs = true;
   cudaStream_t graph_stream = nullptr;
+  // scheduling of the level kernel per precision (FP32, FP64) and level;
+  // zeros are the defaults (msgpu_autotune fills it)
+  msgpu_level_tuning tuning[2][kMaxLevel + 1] = {};
   int* sched_error = nullptr;  // device flag of the level scheduler (in flags)
   // statistics of the last batch call
   bool profiling = false;
@@ -75,6 +78,8 @@ struct msgpu_context {
 namespace {
 
 constexpr int kAbiVersion = 5;
+// default chunking of the level scheduler: a 24th of a pass, at most 16 tiles
+constexpr int kChunkDiv = 24, kChunkMax = 16;
 
 // Bounds of the device-side waits (global-timer nanoseconds), process-wide:
 // a level-kernel worker waiting for work, a composition grid barrier.
@@ -700,9 +705,11 @@ SchedPtrs<Real> carve_sched(void* mem, int num_inst, int max_tiles, size_t* zero
 // is cleared by the caller at the start of an API call, not per launch.
 template <typename Real>
 cudaError_t launch_level_core(LevelArgs<Real>& a, void* sched_mem, int* error_flag, int sms, cudaStream_t st,
-                              int* grid_out) {
+                              int* grid_out, int want_per_sm = 0) {
   const int max_tiles = level_max_tiles(a.level);
   a.idle_ns = g_level_wait_ns.load();
+  if (a.chunk_div <= 0) a.chunk_div = kChunkDiv;
+  if (a.chunk_max <= 0) a.chunk_max = kChunkMax;
   size_t zb = 0;
   SchedPtrs<Real> sp = carve_sched<Real>(sched_mem, a.num_inst, max_tiles, &zb);
   sp.error = error_flag;
@@ -715,6 +722,7 @@ cudaError_t launch_level_core(LevelArgs<Real>& a, void* sched_mem, int* error_fl
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, level_kernel<Real>, kThreads, smem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  if (want_per_sm > 0 && want_per_sm < per_sm) per_sm = want_per_sm;
   const int grid = per_sm * sms;
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
@@ -734,7 +742,11 @@ template <typename Real>
 int launch_level(msgpu_context* ctx, LevelArgs<Real>& a, cudaStream_t st) {
   int rc;
   if ((rc = ensure(ctx, ctx->sched, sched_bytes(a.num_inst, level_max_tiles(a.level))))) return rc;
-  CK(launch_level_core<Real>(a, ctx->sched.p, ctx->sched_error, ctx->sm_count, st, &ctx->last_grid));
+  const msgpu_level_tuning& t = ctx->tuning[sizeof(Real) == 8 ? 1 : 0][a.level];
+  a.chunk_div = t.chunk_div;
+  a.chunk_max = t.chunk_max;
+  CK(launch_level_core<Real>(a, ctx->sched.p, ctx->sched_error, ctx->sm_count, st, &ctx->last_grid,
+                             t.ctas_per_sm));
   return MSGPU_OK;
 }
 
@@ -1000,9 +1012,11 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
     }
     const size_t prof_n = (size_t)max_level_grid(ctx->sm_count) * kPassKinds;
     if (ctx->profiling) {
-      if ((rc = ensure(ctx, ctx->prof, sizeof(unsigned long long) * prof_n * nlev_all))) return rc;
+      if ((rc = ensure(ctx, ctx->prof, sizeof(unsigned long long) * (prof_n + 8) * nlev_all))) return rc;
       a.pass_cycles = (unsigned long long*)ctx->prof.p + prof_n * (l - start);
+      a.xs_prof = (unsigned long long*)ctx->prof.p + prof_n * nlev_all + 8 * (l - start);
       CK(cudaMemsetAsync(a.pass_cycles, 0, sizeof(unsigned long long) * prof_n, st));
+      CK(cudaMemsetAsync(a.xs_prof, 0, sizeof(unsigned long long) * 8, st));
     }
     if ((rc = xs_attach<Real>(ctx, a, p.sum_order == 0, stop, F))) return rc;
     if (ctx->profiling && l - start < 16) CK(cudaEventRecord(ctx->ev[2 * (l - start)], st));
@@ -1061,6 +1075,10 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
         const unsigned long long mx = nctas > 0 ? sum / (unsigned long long)nctas : 0ull;
         ctx->stats.level_pass_cycles[k][q] = (long long)mx;
       }
+      unsigned long long xp[8];
+      CK(cudaMemcpy(xp, (unsigned long long*)ctx->prof.p + prof_n * nlev_all + 8 * k, sizeof(xp),
+                    cudaMemcpyDeviceToHost));
+      for (int q = 0; q < 6; ++q) ctx->stats.level_xs[k][q] = (long long)xp[q];
     }
   }
   return MSGPU_OK;
@@ -1594,6 +1612,58 @@ int msgpu_set_wait_limits(double level_wait_s, double barrier_wait_s) {
   g_level_wait_ns.store(ns(level_wait_s, kMaxIdleNs));
   g_barrier_wait_ns.store(ns(barrier_wait_s, kExtBarrierNs));
   return MSGPU_OK;
+}
+
+int msgpu_get_tuning(const msgpu_context* ctx, int use_fp64, int level, msgpu_level_tuning* out) {
+  if (!ctx || !out || level < 0 || level > kMaxLevel) return MSGPU_ERR_INVALID_ARG;
+  *out = ctx->tuning[use_fp64 ? 1 : 0][level];
+  return MSGPU_OK;
+}
+
+int msgpu_set_tuning(msgpu_context* ctx, int use_fp64, int level, const msgpu_level_tuning* t) {
+  if (!ctx || !t || level < 0 || level > kMaxLevel) return MSGPU_ERR_INVALID_ARG;
+  if (t->chunk_div < 0 || t->chunk_max < 0 || t->ctas_per_sm < 0)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "tuning values must be >= 0");
+  ctx->tuning[use_fp64 ? 1 : 0][level] = *t;
+  ctx->graph.key.clear();   // a captured graph holds the old launch settings
+  return MSGPU_OK;
+}
+
+int msgpu_autotune_device(msgpu_context* ctx, const msgpu_params* p, const double* d_reference,
+                          const double* d_templates, int num_templates, double* d_phis_scratch, void* stream) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  int rc;
+  if ((rc = check_params(ctx, p))) return rc;
+  if (num_templates < 1 || !d_reference || !d_templates || !d_phis_scratch)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid autotune arguments");
+  if (p->stop_level - p->start_level + 1 > 16) return fail(ctx, MSGPU_ERR_UNSUPPORTED, "more than 16 levels");
+  if ((rc = bind_device(ctx))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int fp = p->use_fp64 ? 1 : 0;
+  const int divs[3] = {12, 24, 48}, maxs[3] = {8, 16, 32}, ctas[2] = {2, 1};
+  const bool prof = ctx->profiling;
+  ctx->profiling = true;
+  msgpu_level_tuning best[kMaxLevel + 1];
+  for (int l = 0; l <= kMaxLevel; ++l) best[l] = ctx->tuning[fp][l], best[l].ms = 1e30f;
+  BatchIO io{d_reference, d_templates, nullptr, d_phis_scratch, nullptr, nullptr};
+  for (int c = 0; c < 2 && rc == MSGPU_OK; ++c)
+    for (int i = 0; i < 3 && rc == MSGPU_OK; ++i)
+      for (int j = 0; j < 3 && rc == MSGPU_OK; ++j) {
+        const msgpu_level_tuning cand = {divs[i], maxs[j], ctas[c], 0.f};
+        for (int l = p->start_level; l <= p->stop_level; ++l) ctx->tuning[fp][l] = cand;
+        rc = fp ? run_batch<double>(ctx, *p, num_templates, io, st) : run_batch<float>(ctx, *p, num_templates, io, st);
+        if (rc) break;
+        for (int l = p->start_level; l <= p->stop_level; ++l) {
+          const float ms = ctx->stats.level_ms[l - p->start_level];
+          if (ms < best[l].ms) best[l] = cand, best[l].ms = ms;
+        }
+      }
+  ctx->profiling = prof;
+  for (int l = p->start_level; l <= p->stop_level; ++l) ctx->tuning[fp][l] = best[l];
+  ctx->graph.key.clear();
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(st));
+  return sched_error_check(ctx);
 }
 
 int msgpu_set_graphs(msgpu_context* ctx, int on) {

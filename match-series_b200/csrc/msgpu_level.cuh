@@ -111,6 +111,12 @@ struct LevelArgs {
   // energy tolerance; no counterpart in the reference's stop rules)
   const double* e_target;
   double e_tol;
+  // scheduling (tuned per level, results do not depend on them): a pass is
+  // handed out in chunks of ntiles / chunk_div tiles, at most chunk_max
+  int chunk_div, chunk_max;
+  // optional profile of the exact sums: calls, cycles of their three steps,
+  // chunks walked, chunks added term by term
+  unsigned long long* xs_prof;
 };
 
 // A 2-component array of level k occupies 2 * comp_stride(k) elements.
@@ -1403,9 +1409,9 @@ __device__ __forceinline__ int pass_tiles(int kind, int k, int level, int n) {
 // still running spread over the grid, so that the pass of a lone instance
 // still spreads over every CTA.  Every tile stores its own partial sums and
 // a pass adds them in tile order, so the chunking never changes a result.
-__device__ __forceinline__ int chunk_tiles(int ntiles, int active) {
-  int c = ntiles / 24;
-  c = c < 1 ? 1 : (c > 16 ? 16 : c);
+__device__ __forceinline__ int chunk_tiles(int ntiles, int active, int div, int cmax) {
+  int c = ntiles / div;
+  c = c < 1 ? 1 : (c > cmax ? cmax : c);
   const long long work = (long long)ntiles * (active < 1 ? 1 : active);
   const int spread = (int)((work + gridDim.x - 1) / gridDim.x);
   return spread < c ? (spread < 1 ? 1 : spread) : c;
@@ -1915,7 +1921,7 @@ __device__ void publish(const LevelArgs<Real>& a, const SchedPtrs<Real>& sp, int
     return;
   }
   c.desc.ntiles = pass_tiles(c.desc.kind, c.desc.k, a.level, a.n);
-  c.desc.chunk = chunk_tiles(c.desc.ntiles, a.num_inst - *(volatile int*)sp.finished);
+  c.desc.chunk = chunk_tiles(c.desc.ntiles, a.num_inst - *(volatile int*)sp.finished, a.chunk_div, a.chunk_max);
   const int nchunks = (c.desc.ntiles + c.desc.chunk - 1) / c.desc.chunk;
   c.done = 0;
   ctl_store(sp.ctl + inst, c);
@@ -2139,7 +2145,7 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
           xss[threadIdx.x] = xs_sum(a.xs + (size_t)t.inst * a.xs_stride, a.n, threadIdx.x, el);
         }
         __syncthreads();
-        xs_reduce(xss, nxs, XsGeom(a.n), xres, xwtot);
+        xs_reduce(xss, nxs, XsGeom(a.n), xres, xwtot, a.xs_prof);
       }
       if (threadIdx.x == 0) {
         ctl_load(cs, sp.ctl + t.inst);

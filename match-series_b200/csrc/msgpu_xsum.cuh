@@ -214,8 +214,60 @@ __device__ __forceinline__ void xs_chunk(const XsSum& s, const XsGeom& g, int j,
   len = (tx == g.nx - 1) ? s.items - x0 : 64;
 }
 
-// fl(... fl(fl(S + p_0) + p_1) ... + p_{len-1}) for chunk j, by the warp
-// (every lane returns the same value).
+__device__ __forceinline__ bool xs_in_range(long long v, bool neg) {
+  constexpr long long lo = (1ll << 52) + 1, hi = (1ll << 53) - 1;
+  return neg ? (v >= -hi && v <= -lo) : (v >= lo && v <= hi);
+}
+
+// S + t_0 + ... + t_{cnt-1} in sequence, the terms one per lane (lane k holds
+// t_k), by the warp: at the exponent of the exact running sum every lane
+// converts its term to units of the ulp, a prefix sum over the lanes gives
+// the running mantissa after every term, and the run stops at the first term
+// whose sum leaves the binade or is a tie (or whose running sum cannot be
+// split); that one term is added in floating point, and the walk goes on
+// from the next term.  Every lane returns the same value.
+__device__ __forceinline__ double xs_add_lanes(double S, double v, int cnt) {
+  const int lane = threadIdx.x & 31;
+  int pos = 0;
+  while (pos < cnt) {
+    int E;
+    long long m;
+    if (!xs_split(S, E, m)) {
+      S = __dadd_rn(S, __shfl_sync(0xffffffffu, v, pos));
+      ++pos;
+      continue;
+    }
+    const bool act = lane >= pos && lane < cnt;
+    const double q = v * xs_pow2(-E);
+    bool ok = act && fabs(q) < 36028797018963968.0;
+    long long c = 0;
+    if (ok) {
+      c = __double2ll_rn(q);
+      ok = fabs(q - (double)c) != 0.5;
+    }
+    unsigned long long inc = act ? (unsigned long long)c : 0ull;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += t;
+    }
+    const long long mi = m + (long long)inc;   // mantissa after this lane's term
+    const bool good = ok && xs_in_range(mi, m < 0);
+    const unsigned bad = __ballot_sync(0xffffffffu, act && !good);
+    const int first = bad ? __ffs(bad) - 1 : cnt;
+    if (first > pos) S = (double)__shfl_sync(0xffffffffu, mi, first - 1) * xs_pow2(E);
+    if (first < cnt) {
+      S = __dadd_rn(S, __shfl_sync(0xffffffffu, v, first));
+      pos = first + 1;
+    } else {
+      pos = cnt;
+    }
+  }
+  return S;
+}
+
+// fl(... fl(fl(S + p_0) + p_1) ... + p_{len-1}) for chunk j, by the warp in
+// segments of 32 terms (every lane returns the same value).
 __device__ __forceinline__ double xs_add_chunk(const XsSum& s, const XsGeom& g, int j, double S) {
   const int lane = threadIdx.x & 31;
   int tile, r, len;
@@ -224,21 +276,16 @@ __device__ __forceinline__ double xs_add_chunk(const XsSum& s, const XsGeom& g, 
   const double v0 = (lane < len) ? __ldcg(p + xs_at(lane, 0)) : 0.0;
   const double v1 = (lane + 32 < len) ? __ldcg(p + xs_at(lane + 32, 0)) : 0.0;
   const double v2 = (lane + 64 < len) ? __ldcg(p + xs_at(lane + 64, 0)) : 0.0;
-  const int l0 = len < 32 ? len : 32;
-  for (int k = 0; k < l0; ++k) S = __dadd_rn(S, __shfl_sync(0xffffffffu, v0, k));
-  for (int k = 32; k < len && k < 64; ++k) S = __dadd_rn(S, __shfl_sync(0xffffffffu, v1, k - 32));
-  for (int k = 64; k < len; ++k) S = __dadd_rn(S, __shfl_sync(0xffffffffu, v2, k - 64));
+  S = xs_add_lanes(S, v0, len < 32 ? len : 32);
+  if (len > 32) S = xs_add_lanes(S, v1, len < 64 ? len - 32 : 32);
+  if (len > 64) S = xs_add_lanes(S, v2, len - 64);
   return S;
-}
-
-__device__ __forceinline__ bool xs_in_range(long long v, bool neg) {
-  constexpr long long lo = (1ll << 52) + 1, hi = (1ll << 53) - 1;
-  return neg ? (v >= -hi && v <= -lo) : (v >= lo && v <= hi);
 }
 
 // The sequential sum 0 + t_0 + t_1 + ... of one sum, by one warp (every lane
 // returns it).  Needs the summaries of every chunk.
-__device__ double xs_drive(const XsSum& s, const XsGeom& g) {
+__device__ double xs_drive(const XsSum& s, const XsGeom& g, unsigned long long* prof) {
+  unsigned long long slow = 0;
   const int lane = threadIdx.x & 31;
   const int nch = s.rows * g.nx;
   double S = 0.0;
@@ -266,6 +313,7 @@ __device__ double xs_drive(const XsSum& s, const XsGeom& g) {
       long long m;
       if (!xs_split(S, E, m)) {
         S = xs_add_chunk(s, g, j, S);
+        ++slow;
         ++j;
         continue;
       }
@@ -309,10 +357,17 @@ __device__ double xs_drive(const XsSum& s, const XsGeom& g) {
             done = true;
           }
         }
-        if (!done) S = xs_add_chunk(s, g, j, S);
+        if (!done) {
+          S = xs_add_chunk(s, g, j, S);
+          ++slow;
+        }
         ++j;
       }
     }
+  }
+  if (prof && (threadIdx.x & 31) == 0) {
+    atomicAdd(prof + 4, (unsigned long long)nch);
+    atomicAdd(prof + 5, slow);
   }
   return S;
 }
@@ -340,8 +395,9 @@ __device__ __forceinline__ double xs_block_excl(double v, double* wtot /* [8] sh
 // start, chunk summaries at the predicted exponents, then one warp per sum
 // walks its chunks in order.
 __device__ void xs_reduce(const XsSum* sums, int ns, const XsGeom& g, double* out /* shared [ns] */,
-                          double* wtot /* shared [8] */) {
+                          double* wtot /* shared [8] */, unsigned long long* prof = nullptr) {
   const int nthr = blockDim.x;
+  long long t0 = clock64();
   // 1. predicted ulp exponent at every chunk start
   for (int k = 0; k < ns; ++k) {
     const XsSum& s = sums[k];
@@ -360,6 +416,12 @@ __device__ void xs_reduce(const XsSum* sums, int ns, const XsGeom& g, double* ou
   }
   __threadfence();
   __syncthreads();
+  if (prof && threadIdx.x == 0) {
+    const long long t1 = clock64();
+    atomicAdd(prof + 0, 1ull);
+    atomicAdd(prof + 1, (unsigned long long)(t1 - t0));
+    t0 = t1;
+  }
   // 2. summaries: lanes of a warp take the rows of 3 tiles (9 rows each)
   {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = nthr >> 5;
@@ -392,13 +454,19 @@ __device__ void xs_reduce(const XsSum* sums, int ns, const XsGeom& g, double* ou
   }
   __threadfence();
   __syncthreads();
+  if (prof && threadIdx.x == 0) {
+    const long long t1 = clock64();
+    atomicAdd(prof + 2, (unsigned long long)(t1 - t0));
+    t0 = t1;
+  }
   // 3. one warp per sum
   const int warp = threadIdx.x >> 5;
   if (warp < ns) {
-    const double v = xs_drive(sums[warp], g);
+    const double v = xs_drive(sums[warp], g, prof);
     if ((threadIdx.x & 31) == 0) out[warp] = v;
   }
   __syncthreads();
+  if (prof && threadIdx.x == 0) atomicAdd(prof + 3, (unsigned long long)(clock64() - t0));
 }
 
 }  // namespace msg

@@ -66,11 +66,18 @@ class SeriesDesc(ctypes.Structure):
     ]
 
 
+class LevelTuning(ctypes.Structure):
+    """msgpu_level_tuning: scheduling of the level kernel on one level."""
+    _fields_ = [("chunk_div", ctypes.c_int), ("chunk_max", ctypes.c_int), ("ctas_per_sm", ctypes.c_int),
+                ("ms", ctypes.c_float)]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("kernel_launches", ctypes.c_int), ("num_levels", ctypes.c_int), ("first_level", ctypes.c_int),
                 ("level_ms", ctypes.c_float * 16), ("level_steps", ctypes.c_longlong * 16),
                 ("level_evals", ctypes.c_longlong * 16), ("level_cluster", ctypes.c_int * 16),
-                ("level_pass_cycles", (ctypes.c_longlong * 8) * 16), ("graph_replayed", ctypes.c_int)]
+                ("level_pass_cycles", (ctypes.c_longlong * 8) * 16), ("graph_replayed", ctypes.c_int),
+                ("level_xs", (ctypes.c_longlong * 6) * 16)]
 
 PASS_KINDS = ["energy0", "gradient", "vdown", "vcoarse", "vup", "ncg", "energy", "sync"]
 
@@ -100,7 +107,8 @@ EXPORTS = [
     "msgpu_register_batch_warm_device", "msgpu_find_xshift_yconst", "msgpu_find_xshift_yconst_device",
     "msgpu_empty_lines_to_nan", "msgpu_empty_lines_to_nan_device", "msgpu_remove_empty_lines",
     "msgpu_remove_empty_lines_device", "msgpu_set_wait_limits", "msgpu_set_sum_order", "msgpu_warp_sum_device",
-    "msgpu_mean_from_sums_device", "msgpu_set_graphs",
+    "msgpu_mean_from_sums_device", "msgpu_set_graphs", "msgpu_get_tuning", "msgpu_set_tuning",
+    "msgpu_autotune_device",
 ]
 
 
@@ -141,6 +149,10 @@ def lib():
                                                       ctypes.c_void_p, ctypes.c_void_p]
         L.msgpu_set_profiling.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.msgpu_set_graphs.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.msgpu_get_tuning.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(LevelTuning)]
+        L.msgpu_set_tuning.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(LevelTuning)]
+        L.msgpu_autotune_device.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params), ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
         L.msgpu_set_data_term.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.msgpu_set_sum_order.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.msgpu_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(Stats)]
@@ -651,6 +663,36 @@ class Context:
     def set_profiling(self, on: bool):
         self._check(lib().msgpu_set_profiling(self._h, int(bool(on))))
 
+    def tuning(self, fp64: bool, level: int) -> dict:
+        t = LevelTuning()
+        self._check(lib().msgpu_get_tuning(self._h, int(bool(fp64)), level, ctypes.byref(t)))
+        return {"chunk_div": t.chunk_div, "chunk_max": t.chunk_max, "ctas_per_sm": t.ctas_per_sm, "ms": t.ms}
+
+    def set_tuning(self, fp64: bool, level: int, chunk_div: int = 0, chunk_max: int = 0, ctas_per_sm: int = 0,
+                   ms: float = 0.0):
+        t = LevelTuning(int(chunk_div), int(chunk_max), int(ctas_per_sm), float(ms))
+        self._check(lib().msgpu_set_tuning(self._h, int(bool(fp64)), level, ctypes.byref(t)))
+
+    def load_tuning(self, path: str = None):
+        """Loads a tuning table (JSON written from msgpu_autotune_device's
+        results; default: the table measured on B200 that ships with the
+        package) into the context."""
+        import json
+        path = path or os.path.join(HERE, "tuning_b200.json")
+        d = json.load(open(path))
+        for prec, levels in d["levels"].items():
+            for lv, t in levels.items():
+                self.set_tuning(prec == "fp64", int(lv), t["chunk_div"], t["chunk_max"], t["ctas_per_sm"],
+                                t.get("ms", 0.0))
+
+    def autotune_device(self, params: Params, d_ref: int, d_templates: int, num_templates: int,
+                        d_phis_scratch: int, stream: int = 0) -> dict:
+        """msgpu_autotune_device; returns the chosen setting per level."""
+        self._check(lib().msgpu_autotune_device(self._h, ctypes.byref(params), d_ref, d_templates, num_templates,
+                                                d_phis_scratch, stream or None))
+        return {lv: self.tuning(bool(params.use_fp64), lv)
+                for lv in range(params.start_level, params.stop_level + 1)}
+
     def set_graphs(self, on: bool):
         """CUDA-graph capture and replay of the device batch calls (default on)."""
         self._check(lib().msgpu_set_graphs(self._h, int(bool(on))))
@@ -663,7 +705,10 @@ class Context:
                 "level_ms": list(s.level_ms[:k]), "level_steps": list(s.level_steps[:k]),
                 "level_evals": list(s.level_evals[:k]), "level_cluster": list(s.level_cluster[:k]),
                 "level_pass_cycles": [dict(zip(PASS_KINDS, list(s.level_pass_cycles[i]))) for i in range(k)],
-                "graph_replayed": bool(s.graph_replayed)}
+                "graph_replayed": bool(s.graph_replayed),
+                "level_exact_sums": [dict(zip(["passes", "cycles_predict", "cycles_summaries", "cycles_walk",
+                                               "chunks", "chunks_term_by_term"], list(s.level_xs[i])))
+                                     for i in range(k)]}
 
     # --- single operators ------------------------------------------------
     def energy(self, level, R, T, phix, phiy, lam, fp64=False):
