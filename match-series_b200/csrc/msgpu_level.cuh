@@ -1318,6 +1318,7 @@ __device__ __forceinline__ bool finite_d(double x) { return !isnan(x) && !isinf(
 enum TaskKind : int {
   TK_E0 = 0, TK_GRAD, TK_VDOWN, TK_COARSE, TK_VUP, TK_NCG, TK_TRIAL, TK_FLUSH,
   TK_N1, TK_N2, TK_N3, TK_NF,   // NCC data term: energy subs 1-3, variation
+  TK_XSUM,                      // exact sums: chunk summaries of the pass it stands for (purpose)
   TK_DONE
 };
 __device__ __forceinline__ int task_pass_kind(int kind) {
@@ -1329,6 +1330,7 @@ __device__ __forceinline__ int task_pass_kind(int kind) {
     case TK_VUP: return PK_VUP;
     case TK_NCG: return PK_NCG;
     case TK_NF: return PK_GRAD;
+    case TK_XSUM: return PK_REDUCE;
     default: return PK_ENERGY;
   }
 }
@@ -1338,7 +1340,8 @@ constexpr int PF_ODZERO = 2;   // NCG: the old direction is zero (d = s)
 struct PassDesc {
   int kind, k, cur, dcur, dn, flags;
   int ntiles, chunk;   // tiles of the pass, tiles per dispensed chunk
-  int purpose;   // NCC energy subs: the pass they stand for (TK_E0, TK_GRAD, TK_TRIAL, TK_NCG)
+  int purpose;   // NCC energy subs, TK_XSUM: the pass they stand for (TK_E0, TK_GRAD, TK_TRIAL, TK_NCG, ...)
+  int xn;        // TK_XSUM: exact sums of that pass
   double t;      // trial step (NCG, TRIAL) or pending step (GRAD, FLUSH)
   double beta;   // Fletcher-Reeves factor (NCG)
   double vtau;   // tau of the V-cycle passes
@@ -1387,8 +1390,18 @@ __device__ __forceinline__ Inst<Real> make_inst(const LevelArgs<Real>& a, int in
   return I;
 }
 
-__device__ __forceinline__ int pass_tiles(int kind, int k, int level, int n) {
+// The exact sums of a pass of kind `kind` for instance inst: slot 0 is the
+// element sum E_data for the energy passes, every other slot a node sum.
+template <typename Real>
+__device__ __forceinline__ void xs_pass_sums(const LevelArgs<Real>& a, int inst, int kind, int ns, XsSum* out) {
+  double* base = a.xs + (size_t)inst * a.xs_stride;
+  const bool energy = (kind == TK_E0 || kind == TK_TRIAL || kind == TK_NCG);
+  for (int k = 0; k < ns; ++k) out[k] = xs_sum(base, a.n, k, energy && k == 0);
+}
+
+__device__ __forceinline__ int pass_tiles(int kind, int k, int level, int n, int xn) {
   switch (kind) {
+    case TK_XSUM: return xs_summary_tasks(xn, n);
     case TK_VDOWN:
     case TK_VUP: {
       const int w = (1 << k) + 1;
@@ -1521,12 +1534,25 @@ struct TaskRunner {
   }
 
   __device__ void issue(int inst, const PassDesc& d, int tile, int stage) const {
-    if (d.kind == TK_COARSE || d.kind == TK_FLUSH) return;  // these read global memory directly
+    if (d.kind == TK_COARSE || d.kind == TK_FLUSH || d.kind == TK_XSUM) return;  // these read global memory directly
     double dummy[kRedSlots];
     with_pass(inst, d, dummy, [&](auto& ps) { ps.issue(tile, stage); });
   }
 
   __device__ void compute(int inst, const PassDesc& d, int tile, int stage, double* part) const {
+    if (d.kind == TK_XSUM) {
+      // thread (block b, row r) of task tile `tile`: blocks of all sums in turn
+      if ((int)threadIdx.x >= kXsTilesPerTask * kXsBR) return;
+      const XsGeom g(a.n);
+      const int ntiles = g.nx * g.ny;
+      const int b = tile * kXsTilesPerTask + (int)threadIdx.x / kXsBR, r = (int)threadIdx.x % kXsBR;
+      const int k = b / ntiles;
+      if (k >= d.xn) return;
+      const bool energy = (d.purpose == TK_E0 || d.purpose == TK_TRIAL || d.purpose == TK_NCG);
+      const XsSum s = xs_sum(a.xs + (size_t)inst * a.xs_stride, a.n, k, energy && k == 0);
+      xs_summary_row(s, g, b - k * ntiles, r);
+      return;
+    }
     if (d.kind == TK_COARSE) {
       const Inst<Real> I = make_inst(a, inst);
       const int L = a.level, lc = a.lc;
@@ -1920,7 +1946,7 @@ __device__ void publish(const LevelArgs<Real>& a, const SchedPtrs<Real>& sp, int
     atomicAdd(sp.finished, 1);
     return;
   }
-  c.desc.ntiles = pass_tiles(c.desc.kind, c.desc.k, a.level, a.n);
+  c.desc.ntiles = pass_tiles(c.desc.kind, c.desc.k, a.level, a.n, c.desc.xn);
   c.desc.chunk = chunk_tiles(c.desc.ntiles, a.num_inst - *(volatile int*)sp.finished, a.chunk_div, a.chunk_max);
   const int nchunks = (c.desc.ntiles + c.desc.chunk - 1) / c.desc.chunk;
   c.done = 0;
@@ -1932,7 +1958,7 @@ __device__ void publish(const LevelArgs<Real>& a, const SchedPtrs<Real>& sp, int
 // Two passes whose tiles use the same shared-memory layout (so the first
 // tile of one can be prefetched while the other computes).
 __device__ __forceinline__ bool same_layout(const PassDesc& a, const PassDesc& b) {
-  if (a.kind != b.kind || a.kind == TK_COARSE || a.kind == TK_FLUSH) return false;
+  if (a.kind != b.kind || a.kind == TK_COARSE || a.kind == TK_FLUSH || a.kind == TK_XSUM) return false;
   if (a.kind == TK_N1) return a.purpose == b.purpose && a.flags == b.flags;
   return true;
 }
@@ -2136,20 +2162,30 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
         for (int k = 0; k < kRedSlots; ++k) acc[k] += __ldcg(pp + (size_t)i * kRedSlots + k);
       }
       block_sum(acc, wbuf, tot);
-      // exact sums of the pass, in the reference's order
-      const int nxs = a.xs ? xs_count(a, t.desc) : 0;
-      if (nxs) {
-        if (threadIdx.x < nxs) {
-          const bool el = (threadIdx.x == 0) && (t.desc.kind == TK_E0 || t.desc.kind == TK_TRIAL ||
-                                                 t.desc.kind == TK_NCG);
-          xss[threadIdx.x] = xs_sum(a.xs + (size_t)t.inst * a.xs_stride, a.n, threadIdx.x, el);
-        }
+      // exact sums of the pass, in the reference's order: predictions here,
+      // then a summary pass over the grid, whose completing CTA walks the
+      // chunks and takes the control step of the pass it stands for
+      const int nxs = (a.xs && t.desc.kind != TK_XSUM) ? xs_count(a, t.desc) : 0;
+      if (t.desc.kind == TK_XSUM || nxs) {
+        const int kind = (t.desc.kind == TK_XSUM) ? t.desc.purpose : t.desc.kind;
+        const int ns = (t.desc.kind == TK_XSUM) ? t.desc.xn : nxs;
+        if (threadIdx.x == 0) xs_pass_sums(a, t.inst, kind, ns, xss);
         __syncthreads();
-        xs_reduce(xss, nxs, XsGeom(a.n), xres, xwtot, a.xs_prof);
+        if (t.desc.kind == TK_XSUM) xs_walk(xss, ns, XsGeom(a.n), xres, a.xs_prof);
+        else xs_predict(xss, ns, XsGeom(a.n), xwtot, a.xs_prof);
       }
       if (threadIdx.x == 0) {
         ctl_load(cs, sp.ctl + t.inst);
-        advance(a, t.inst, cs, tot, nxs ? xres : nullptr);
+        if (nxs) {
+          cs.desc.purpose = cs.desc.kind;
+          cs.desc.xn = nxs;
+          cs.desc.kind = TK_XSUM;
+        } else if (t.desc.kind == TK_XSUM) {
+          cs.desc.kind = cs.desc.purpose;
+          advance(a, t.inst, cs, tot, xres);
+        } else {
+          advance(a, t.inst, cs, tot, nullptr);
+        }
         publish(a, sp, t.inst, cs);
       }
       __syncthreads();

@@ -287,26 +287,30 @@ __device__ __forceinline__ double xs_add_chunk(const XsSum& s, const XsGeom& g, 
 __device__ double xs_drive(const XsSum& s, const XsGeom& g, unsigned long long* prof) {
   unsigned long long slow = 0;
   const int lane = threadIdx.x & 31;
+  const unsigned lt_mask = (1u << lane) - 1u;   // lanes below this one
   const int nch = s.rows * g.nx;
   double S = 0.0;
   int j = 0;
   // the records of the next window are loaded while the current one is walked
-  int nef = (lane < nch) ? __ldcg(s.ef + lane) : 0;
-  long long nX = (lane < nch) ? __ldcg(s.X + lane) : 0, nlo = (lane < nch) ? __ldcg(s.mnB + lane) : 0,
-            nhi = (lane < nch) ? __ldcg(s.mxB + lane) : 0;
+  auto load = [&](int jn, int& ef, long long& X, long long& lo, long long& hi, long long& R, long long& loA,
+                  long long& hiA) {
+    const bool in = jn < nch;
+    ef = in ? __ldcg(s.ef + jn) : 0;
+    X = in ? __ldcg(s.X + jn) : 0;
+    lo = in ? __ldcg(s.mnB + jn) : 0;
+    hi = in ? __ldcg(s.mxB + jn) : 0;
+    R = in ? __ldcg(s.R + jn) : 0;
+    loA = in ? __ldcg(s.mnA + jn) : 0;
+    hiA = in ? __ldcg(s.mxA + jn) : 0;
+  };
+  int nef;
+  long long nX, nlo, nhi, nR, nloA, nhiA;
+  load(lane, nef, nX, nlo, nhi, nR, nloA, nhiA);
   for (int jb = 0; jb < nch; jb += 32) {
-    const int jl = jb + lane;
-    const bool in = jl < nch;
+    const bool in = jb + lane < nch;
     const int ef = nef;
-    const long long X = nX, lo = nlo, hi = nhi;
-    {
-      const int jn = jl + 32;
-      const bool inn = jn < nch;
-      nef = inn ? __ldcg(s.ef + jn) : 0;
-      nX = inn ? __ldcg(s.X + jn) : 0;
-      nlo = inn ? __ldcg(s.mnB + jn) : 0;
-      nhi = inn ? __ldcg(s.mxB + jn) : 0;
-    }
+    const long long X = nX, lo = nlo, hi = nhi, R = nR, loA = nloA, hiA = nhiA;
+    load(jb + lane + 32, nef, nX, nlo, nhi, nR, nloA, nhiA);
     while (j < jb + 32 && j < nch) {
       if (isnan(S)) return S;
       int E;
@@ -320,47 +324,45 @@ __device__ double xs_drive(const XsSum& s, const XsGeom& g, unsigned long long* 
       const bool neg = m < 0;
       const int o = j - jb;
       const bool act = lane >= o && in;
-      const bool plain = act && (ef & 3) == kXsValid && xs_exp(ef) == E;
-      const unsigned long long dl = plain ? (unsigned long long)X : 0ull;
-      // exclusive prefix of the chunk sums over the lanes
-      unsigned long long inc = dl;
+      const bool use = act && (ef & kXsValid) && xs_exp(ef) == E;
+      const bool tie = use && (ef & kXsTie);
+      // parity of the mantissa entering every lane's chunk: after a tie chunk
+      // it is the parity of that chunk's R (its mantissa at the first tie is
+      // even), before any tie the parity of m; the chunks in between add X
+      const unsigned ties = __ballot_sync(0xffffffffu, tie);
+      const unsigned odd = __ballot_sync(0xffffffffu, use && !tie && (X & 1));
+      const unsigned tb = ties & lt_mask;
+      const int t = tb ? 31 - __clz(tb) : -1;   // last tie chunk below this lane
+      const long long Rt = __shfl_sync(0xffffffffu, R, t < 0 ? 0 : t);
+      const unsigned between = lt_mask & (t < 0 ? ~((1u << o) - 1u) : ~((2u << t) - 1u));
+      const int par_in = ((t < 0 ? (int)(m & 1) : (int)(Rt & 1)) + __popc(odd & between)) & 1;
+      const long long b = (long long)((par_in + (int)(X & 1)) & 1);
+      const long long delta = use ? (tie ? X + b + R : X) : 0;
+      // exclusive prefix of the chunk deltas over the lanes
+      unsigned long long inc = (unsigned long long)delta;
 #pragma unroll
       for (int o2 = 1; o2 < 32; o2 <<= 1) {
-        const unsigned long long t = __shfl_up_sync(0xffffffffu, inc, o2);
-        if (lane >= o2) inc += t;
+        const unsigned long long tt = __shfl_up_sync(0xffffffffu, inc, o2);
+        if (lane >= o2) inc += tt;
       }
-      const long long mi = m + (long long)(inc - dl);
-      const bool good = plain && xs_in_range(mi + lo, neg) && xs_in_range(mi + hi, neg);
+      const long long mi = m + (long long)(inc - (unsigned long long)delta);
+      bool good = use && xs_in_range(mi + lo, neg) && xs_in_range(mi + hi, neg);
+      if (tie) {
+        const long long m1 = mi + X + b;
+        good = good && xs_in_range(m1 + loA, neg) && xs_in_range(m1 + hiA, neg);
+      }
       const unsigned bad = __ballot_sync(0xffffffffu, act && !good);
       const int last = (nch - jb < 32 ? nch - jb : 32);   // lanes with a chunk
       const int first = bad ? __ffs(bad) - 1 : last;
       // mantissa at the start of chunk jb + first
-      const long long mf = __shfl_sync(0xffffffffu, mi + (long long)dl, (first > 0 ? first : 1) - 1);
+      const long long mf = __shfl_sync(0xffffffffu, mi + delta, (first > 0 ? first : 1) - 1);
       if (first > o) S = (double)mf * xs_pow2(E);
       j = jb + first;
       if (j < jb + 32 && j < nch) {
-        // chunk j interrupts the run: a tie chunk at this exponent, or one
-        // whose sums leave the binade (or that has no usable summary)
-        const int efj = __shfl_sync(0xffffffffu, ef, first);
-        bool done = false;
-        if ((efj & kXsValid) && (efj & kXsTie) && xs_exp(efj) == E) {
-          long long mm;
-          int EE;
-          xs_split(S, EE, mm);
-          const long long Xj = __shfl_sync(0xffffffffu, X, first);
-          const long long loj = __shfl_sync(0xffffffffu, lo, first), hij = __shfl_sync(0xffffffffu, hi, first);
-          const long long Rj = __ldcg(s.R + j), loA = __ldcg(s.mnA + j), hiA = __ldcg(s.mxA + j);
-          const long long m1 = mm + Xj + ((mm + Xj) & 1);
-          if (xs_in_range(mm + loj, neg) && xs_in_range(mm + hij, neg) && xs_in_range(m1 + loA, neg) &&
-              xs_in_range(m1 + hiA, neg)) {
-            S = (double)(m1 + Rj) * xs_pow2(E);
-            done = true;
-          }
-        }
-        if (!done) {
-          S = xs_add_chunk(s, g, j, S);
-          ++slow;
-        }
+        // chunk j interrupts the run (its sums leave the binade, or it has no
+        // summary at this exponent): added term by term
+        S = xs_add_chunk(s, g, j, S);
+        ++slow;
         ++j;
       }
     }
@@ -390,76 +392,75 @@ __device__ __forceinline__ double xs_block_excl(double v, double* wtot /* [8] sh
   return base + inc - v;
 }
 
-// The exact sums of ns sums of a completed pass, by the whole CTA (256
-// threads): out[k] for sum k.  Three steps: predicted binade of every chunk
-// start, chunk summaries at the predicted exponents, then one warp per sum
-// walks its chunks in order.
-__device__ void xs_reduce(const XsSum* sums, int ns, const XsGeom& g, double* out /* shared [ns] */,
-                          double* wtot /* shared [8] */, unsigned long long* prof = nullptr) {
+// The exact sums of a completed pass in three steps.  1 (xs_predict, the
+// CTA that completed the pass): the predicted binade at every chunk start.
+// 2 (xs_summary_row, a pass of its own spread over the grid): the chunk
+// summaries at the predicted exponents, one chunk per thread.  3 (xs_walk,
+// the CTA that completed step 2): one warp per sum walks its chunks in order.
+constexpr int kXsTilesPerTask = 256 / kXsBR;   // term blocks per task tile of step 2 (9 rows each)
+
+// Profile counters (nullable): [0] passes, [1..3] cycles of the steps,
+// [4] chunks walked, [5] chunks added term by term.
+__device__ void xs_predict(const XsSum* sums, int ns, const XsGeom& g, double* wtot /* shared [8] */,
+                           unsigned long long* prof) {
   const int nthr = blockDim.x;
-  long long t0 = clock64();
-  // 1. predicted ulp exponent at every chunk start
+  const long long t0 = clock64();
   for (int k = 0; k < ns; ++k) {
     const XsSum& s = sums[k];
     const int nch = s.rows * g.nx;
     const int per = (nch + nthr - 1) / nthr;
     const int c0 = threadIdx.x * per, c1 = min(c0 + per, nch);
     double loc = 0.0;
+#pragma unroll 8
     for (int j = c0; j < c1; ++j) loc += __ldcg(s.tot + 2 * j) + __ldcg(s.tot + 2 * j + 1);
     double run = xs_block_excl(loc, wtot);
+#pragma unroll 8
     for (int j = c0; j < c1; ++j) {
       int E;
       long long m;
-      s.ef[j] = xs_split(run, E, m) ? xs_pack(E, 0) : kXsNoExp;
+      __stcg(s.ef + j, xs_split(run, E, m) ? xs_pack(E, 0) : kXsNoExp);
       run += __ldcg(s.tot + 2 * j) + __ldcg(s.tot + 2 * j + 1);
     }
   }
   __threadfence();
   __syncthreads();
   if (prof && threadIdx.x == 0) {
-    const long long t1 = clock64();
     atomicAdd(prof + 0, 1ull);
-    atomicAdd(prof + 1, (unsigned long long)(t1 - t0));
-    t0 = t1;
+    atomicAdd(prof + 1, (unsigned long long)(clock64() - t0));
   }
-  // 2. summaries: lanes of a warp take the rows of 3 tiles (9 rows each)
-  {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = nthr >> 5;
-    const int grp = lane / kXsBR, r = lane - grp * kXsBR;
-    const int ntiles = g.nx * g.ny;
-    for (int k = 0; k < ns; ++k) {
-      const XsSum& s = sums[k];
-      for (int t0 = warp * 3; t0 < ntiles; t0 += nwarps * 3) {
-        const int t = t0 + grp;
-        if (grp >= 3 || t >= ntiles) continue;
-        const int ty = t / g.nx, tx = t - ty * g.nx;
-        const int y = ty * 8 + r;
-        const int rows_t = (ty == g.ny - 1) ? s.rows - ty * 8 : 8;
-        if (r >= rows_t) continue;
-        const int x0 = tx * 64;
-        const int len = (tx == g.nx - 1) ? s.items - x0 : 64;
-        const int j = y * g.nx + tx;
-        long long X, R, lo, hi, loA, hiA;
-        int ef;
-        xs_summarise(xs_block(s, t) + r, kXsBR, len, __ldcg(s.ef + j), X, R, lo, hi, loA, hiA, ef);
-        __stcg(s.X + j, X);
-        __stcg(s.R + j, R);
-        __stcg(s.mnB + j, lo);
-        __stcg(s.mxB + j, hi);
-        __stcg(s.mnA + j, loA);
-        __stcg(s.mxA + j, hiA);
-        __stcg(s.ef + j, ef);
-      }
-    }
-  }
-  __threadfence();
-  __syncthreads();
-  if (prof && threadIdx.x == 0) {
-    const long long t1 = clock64();
-    atomicAdd(prof + 2, (unsigned long long)(t1 - t0));
-    t0 = t1;
-  }
-  // 3. one warp per sum
+}
+
+// Step 2: the summary of chunk row r of term block t of sum s (one thread).
+__device__ __forceinline__ void xs_summary_row(const XsSum& s, const XsGeom& g, int t, int r) {
+  const int ty = t / g.nx, tx = t - ty * g.nx;
+  const int rows_t = (ty == g.ny - 1) ? s.rows - ty * 8 : 8;
+  if (r >= rows_t) return;
+  const int y = ty * 8 + r;
+  const int x0 = tx * 64;
+  const int len = (tx == g.nx - 1) ? s.items - x0 : 64;
+  const int j = y * g.nx + tx;
+  long long X, R, lo, hi, loA, hiA;
+  int ef;
+  xs_summarise(xs_block(s, t) + r, kXsBR, len, __ldcg(s.ef + j), X, R, lo, hi, loA, hiA, ef);
+  __stcg(s.X + j, X);
+  __stcg(s.R + j, R);
+  __stcg(s.mnB + j, lo);
+  __stcg(s.mxB + j, hi);
+  __stcg(s.mnA + j, loA);
+  __stcg(s.mxA + j, hiA);
+  __stcg(s.ef + j, ef);
+}
+
+// Task tiles of the summary pass.
+__host__ __device__ inline int xs_summary_tasks(int ns, int n) {
+  const XsGeom g(n);
+  return (ns * g.nx * g.ny + kXsTilesPerTask - 1) / kXsTilesPerTask;
+}
+
+// Step 3: out[k] = the sequential sum k (one warp per sum).
+__device__ void xs_walk(const XsSum* sums, int ns, const XsGeom& g, double* out /* shared [ns] */,
+                        unsigned long long* prof) {
+  const long long t0 = clock64();
   const int warp = threadIdx.x >> 5;
   if (warp < ns) {
     const double v = xs_drive(sums[warp], g, prof);
