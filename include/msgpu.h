@@ -446,6 +446,16 @@ int msgpu_gd_level(msgpu_context* ctx, int level, const double* R, const double*
                    double* phiy, double lambda, int max_iter, double stop_eps, int use_fp64,
                    double* energy_out, int* steps_out, double* trace, int max_trace);
 
+/* msgpu_gd_level with the reference's per-level energy log instead of the
+ * trace: energy_log receives min(steps, max_rows - 1) + 1 rows of
+ * (iteration - 1, lambda * E_reg of the last energy evaluation, energy at
+ * the new position), the first row (-1) for the initial position -- the
+ * columns the reference writes to energy_%02d.txt (gradientDescent.h:
+ * 254-272, through findTransformation, registration.h:967-1000).           */
+int msgpu_gd_level_log(msgpu_context* ctx, int level, const double* R, const double* T, double* phix,
+                       double* phiy, double lambda, int max_iter, double stop_eps, int use_fp64, double* energy_out,
+                       int* steps_out, double* energy_log, int max_rows);
+
 /* --- allocation-free level solve ----------------------------------------
  * No counterpart in the reference.  The same level solve as msgpu_gd_level
  * with its global sums in the fixed parallel order (sum order 1; the term

@@ -21,6 +21,7 @@
 
 #include <registration.h>
 
+#include <fstream>
 #include <vector>
 
 #include "msgpu.h"
@@ -67,12 +68,20 @@ class GpuSSDRegistrationMultilevelDescent
     const double stopEps = P.hasVariable("stopEpsilon") ? P.getDouble("stopEpsilon") : 0.;
     double energy = 0.;
     int steps = 0;
-    check(msgpu_gd_level(_ctx, this->_curLevel, this->_org_reference[this->_curLevel].getData(),
-                         this->_org_template[this->_curLevel].getData(), phi[0].getData(), phi[1].getData(), lambda,
-                         maxIter, stopEps, /* use_fp64 */ 1, &energy, &steps, NULL, 0),
+    std::vector<double> log(3 * (size_t)(maxIter + 1));
+    check(msgpu_gd_level_log(_ctx, this->_curLevel, this->_org_reference[this->_curLevel].getData(),
+                             this->_org_template[this->_curLevel].getData(), phi[0].getData(), phi[1].getData(),
+                             lambda, maxIter, stopEps, /* use_fp64 */ 1, &energy, &steps, &log[0], maxIter + 1),
           __FILE__, __LINE__);
     this->_energyOfLastSolution = energy;
-    if (this->_disableSaving == false) regisConfig.writeCurrentRegistration(*this, phi);
+    if (this->_disableSaving == false) {
+      // the per-level energy log the reference's gradient descent writes
+      // (gradientDescent.h:254-272): iteration - 1, lambda * E_reg, energy
+      std::ofstream out(aol::strprintf("%senergy_%02d.txt", this->getSaveDirectory(), this->_curLevel).c_str());
+      for (int i = 0; i <= steps && i <= maxIter; ++i)
+        out << static_cast<int>(log[3 * i]) << " " << log[3 * i + 1] << " " << log[3 * i + 2] << std::endl;
+      regisConfig.writeCurrentRegistration(*this, phi);
+    }
   }
 };
 

@@ -3136,7 +3136,7 @@ template <typename Real>
 int single_level(msgpu_context* ctx, int level, int mode, const double* R, const double* T, const double* phix,
                  const double* phiy, const double* de_in, double lambda, int max_iter, double stop_eps,
                  double sigma, double* energy_out, int* steps_out, double* phix_out, double* phiy_out,
-                 double* de_out, double* trace, int max_trace) {
+                 double* de_out, double* trace, int max_trace, double* elog_out = nullptr) {
   int rc;
   if ((rc = ensure_tables(ctx))) return rc;
   const bool ncc = ctx->data_term == 1 && mode != MODE_SMOOTH;
@@ -3147,7 +3147,8 @@ int single_level(msgpu_context* ctx, int level, int mode, const double* R, const
   if ((rc = ensure(ctx, ctx->shared_real, sizeof(Real) * (comp_stride(level) + 64)))) return rc;
   if ((rc = ensure(ctx, ctx->io[0], sizeof(double) * 6 * N))) return rc;
   const size_t trace_n = (size_t)std::max(1, max_trace) * 4;
-  if ((rc = ensure(ctx, ctx->small, sizeof(double) * (8 + trace_n) + 64))) return rc;
+  const size_t elog_n = (size_t)(std::max(0, max_trace) + 1) * 3;
+  if ((rc = ensure(ctx, ctx->small, sizeof(double) * (8 + trace_n + elog_n) + 64))) return rc;
   cudaStream_t st = ctx->stream;
   Real* arena = (Real*)ctx->arena.p;
   Real* Rd = (Real*)ctx->shared_real.p;
@@ -3204,6 +3205,7 @@ int single_level(msgpu_context* ctx, int level, int mode, const double* R, const
   a.out_phi_buf = d_i + 1;
   a.trace = trace ? d_trace : nullptr;
   a.max_trace = max_trace;
+  a.elog = elog_out ? d_trace + trace_n : nullptr;
   if ((rc = xs_attach<Real>(ctx, a, ctx->sum_order == 0 && mode != MODE_SMOOTH, level, 1))) return rc;
   if ((rc = sched_error_reset(ctx, st))) return rc;
   if ((rc = launch_level<Real>(ctx, a, st))) return rc;
@@ -3238,6 +3240,10 @@ int single_level(msgpu_context* ctx, int level, int mode, const double* R, const
   if (trace && max_trace > 0) {
     const int rows = std::min(hi[0], max_trace);
     CK(cudaMemcpy(trace, d_trace, sizeof(double) * 4 * rows, cudaMemcpyDeviceToHost));
+  }
+  if (elog_out) {
+    const int rows = std::min(hi[0], max_trace) + 1;
+    CK(cudaMemcpy(elog_out, d_trace + trace_n, sizeof(double) * 3 * rows, cudaMemcpyDeviceToHost));
   }
   return MSGPU_OK;
 }
@@ -3285,6 +3291,23 @@ int msgpu_gd_level(msgpu_context* ctx, int level, const double* R, const double*
                                          stop_eps, 0, energy_out, steps_out, phix, phiy, nullptr, trace, max_trace)
                   : single_level<float>(ctx, level, MODE_SOLVE, R, T, phix, phiy, nullptr, lambda, max_iter,
                                         stop_eps, 0, energy_out, steps_out, phix, phiy, nullptr, trace, max_trace);
+}
+
+int msgpu_gd_level_log(msgpu_context* ctx, int level, const double* R, const double* T, double* phix,
+                       double* phiy, double lambda, int max_iter, double stop_eps, int use_fp64, double* energy_out,
+                       int* steps_out, double* energy_log, int max_rows) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (level < 1 || level > kMaxLevel || !R || !T || !phix || !phiy || max_iter < 0 || !energy_log || max_rows < 1)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid gd_level_log arguments");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  const int mt = max_rows - 1;
+  return use_fp64 ? single_level<double>(ctx, level, MODE_SOLVE, R, T, phix, phiy, nullptr, lambda, max_iter,
+                                         stop_eps, 0, energy_out, steps_out, phix, phiy, nullptr, nullptr, mt,
+                                         energy_log)
+                  : single_level<float>(ctx, level, MODE_SOLVE, R, T, phix, phiy, nullptr, lambda, max_iter,
+                                        stop_eps, 0, energy_out, steps_out, phix, phiy, nullptr, nullptr, mt,
+                                        energy_log);
 }
 
 int msgpu_restrict(msgpu_context* ctx, int fine_level, const double* in, double* out) {

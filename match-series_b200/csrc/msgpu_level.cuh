@@ -82,6 +82,11 @@ struct LevelArgs {
   int* out_phi_buf;         // per instance: buffer holding the result
   double* trace;            // optional: per instance max_trace rows of (energy, tau, sigma, evals)
   int max_trace;
+  // optional energy log of the reference's per-level file (energy_%02d.txt,
+  // gradientDescent.h:254-272): per instance max_trace + 1 rows of
+  // (iteration - 1, lambda * E_reg of the last evaluation, energy), the
+  // first row (-1) for the initial position
+  double* elog;
   unsigned long long* pass_cycles;  // optional: per CTA kPassKinds clock64 totals
   // normalized cross-correlation data term (ncc != 0)
   int ncc;
@@ -1355,6 +1360,7 @@ struct InstCtl {
   int ls;              // TRIAL role: 0 doubling, 1 halving, 2 energy at the accepted step
   int iter, evals, total_evals, attempt, rb_pos, pending, od_zero, cur, dcur;
   double energy, energy_new, f, sigma, sigma_used, tau, og2, A, Bd, Cd, Df, t, beta, tau_p;
+  double last_ereg;    // E_reg of the last energy evaluation (the energy log)
   double rb_tau[2], rb_e[2];
   double n1[kRedSlots];      // NCC: totals of energy sub 1 (mean, then A or Df B C)
 };
@@ -1711,6 +1717,14 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
     c.rb_pos ^= 1;
     c.evals++;
   };
+  auto log_row = [&](int row, double en) {
+    if (a.elog && row <= a.max_trace) {
+      double* lg = a.elog + ((size_t)inst * (a.max_trace + 1) + row) * 3;
+      lg[0] = (double)(row - 1);
+      lg[1] = lam * c.last_ereg;
+      lg[2] = en;
+    }
+  };
   auto end_iteration = [&](double en) {
     if (c.tau != 0) {
       c.pending = 1;
@@ -1718,6 +1732,7 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
     }
     c.energy_new = en;
     c.total_evals += c.evals;
+    log_row(c.iter, en);
     if (a.trace && c.iter <= a.max_trace) {
       double* tr = a.trace + ((size_t)inst * a.max_trace + (c.iter - 1)) * 4;
       tr[0] = c.energy_new;
@@ -1792,8 +1807,10 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
   switch (d.kind) {
     case TK_E0: {
       c.A = tot[1];
-      c.energy = xr ? energy_of(xr[0], ereg_exact()) : energy_of(tot[0], 0.5 * c.A);
+      c.last_ereg = xr ? ereg_exact() : 0.5 * c.A;
+      c.energy = energy_of(xr ? xr[0] : tot[0], c.last_ereg);
       c.energy_new = c.energy;
+      log_row(0, c.energy);
       if (a.mode == MODE_ENERGY) {
         to(TK_GRAD);
         d.cur = c.cur;
@@ -1857,7 +1874,8 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
         c.Df += xr[4];
       }
       const double t = c.t, f = c.f;
-      const double fnew = xr ? energy_of(xr[0], ereg_exact()) : energy_of(tot[0], quad(t));
+      c.last_ereg = xr ? ereg_exact() : quad(t);
+      const double fnew = energy_of(xr ? xr[0] : tot[0], c.last_ereg);
       push_ring(t, fnew);
       const double G = (fnew - f) / (c.Df * t);
       if (c.Df >= 0 || !finite_d(f)) {
@@ -1871,7 +1889,8 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
     }
     case TK_TRIAL: {
       const double t = c.t, f = c.f;
-      const double fnew = xr ? energy_of(xr[0], ereg_exact()) : energy_of(tot[0], quad(t));
+      c.last_ereg = xr ? ereg_exact() : quad(t);
+      const double fnew = energy_of(xr ? xr[0] : tot[0], c.last_ereg);
       push_ring(t, fnew);
       if (c.ls == 2) {
         end_iteration(fnew);

@@ -108,7 +108,7 @@ EXPORTS = [
     "msgpu_empty_lines_to_nan", "msgpu_empty_lines_to_nan_device", "msgpu_remove_empty_lines",
     "msgpu_remove_empty_lines_device", "msgpu_set_wait_limits", "msgpu_set_sum_order", "msgpu_warp_sum_device",
     "msgpu_mean_from_sums_device", "msgpu_set_graphs", "msgpu_get_tuning", "msgpu_set_tuning",
-    "msgpu_autotune_device",
+    "msgpu_autotune_device", "msgpu_gd_level_log",
 ]
 
 
@@ -141,6 +141,7 @@ def lib():
         L.msgpu_normalize.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp]
         L.msgpu_gd_level.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_double,
                                      ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp, _ip, _dp, ctypes.c_int]
+        L.msgpu_gd_level_log.argtypes = L.msgpu_gd_level.argtypes
         L.msgpu_match_series_stage.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params), _dp, _dp, ctypes.c_int,
                                                _dp, _dp, _ip, _dp, _dp]
         L.msgpu_match_series_stage_device.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params), ctypes.c_void_p,
@@ -760,6 +761,19 @@ class Context:
                                          ctypes.byref(st), _p(tr), max_trace))
         steps = st.value
         return px, py, e.value, steps, tr[:min(steps, max_trace)]
+
+    def gd_level_log(self, level, R, T, phix, phiy, lam, max_iter, stop_eps=0.0, fp64=True):
+        """gd_level with the reference's per-level energy log: rows of
+        (iteration - 1, lambda * E_reg of the last evaluation, energy)."""
+        px = _f64(phix).copy()
+        py = _f64(phiy).copy()
+        e = ctypes.c_double()
+        st = ctypes.c_int()
+        lg = np.zeros((max_iter + 1, 3))
+        self._check(lib().msgpu_gd_level_log(self._h, level, _p(_f64(R)), _p(_f64(T)), _p(px), _p(py), float(lam),
+                                             int(max_iter), float(stop_eps), int(fp64), ctypes.byref(e),
+                                             ctypes.byref(st), _p(lg), max_iter + 1))
+        return px, py, e.value, st.value, lg[:st.value + 1]
 
 
 class Net:
