@@ -417,6 +417,12 @@ int msgpu_set_graphs(msgpu_context* ctx, int on);
  * {12, 24, 48}, chunk_max in {8, 16, 32}, 1 or 2 CTAs per SM), times every
  * level's launch with CUDA events, and keeps for each level startLevel ..
  * stopLevel the fastest setting.  Synchronous.                            */
+/* The reference-order sum of the level solve on its own (no counterpart in
+ * the reference; exposed so that it can be checked on any data): *d_out =
+ * the sequentially rounded 0 + t_0 + t_1 + ... of the (2^level+1)^2 doubles
+ * at d_terms, in their order.  Device pointers, enqueued on `stream`.     */
+int msgpu_exact_sum_device(msgpu_context* ctx, int level, const double* d_terms, double* d_out, void* stream);
+
 int msgpu_get_tuning(const msgpu_context* ctx, int use_fp64, int level, msgpu_level_tuning* out);
 int msgpu_set_tuning(msgpu_context* ctx, int use_fp64, int level, const msgpu_level_tuning* t);
 int msgpu_autotune_device(msgpu_context* ctx, const msgpu_params* p, const double* d_reference,

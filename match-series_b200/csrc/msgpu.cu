@@ -1084,6 +1084,49 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
   return MSGPU_OK;
 }
 
+// The exact sequential sum of the level solve (msgpu_xsum.cuh) on its own,
+// for an n x n array of terms in row-major order (a node sum): the terms go
+// to the term blocks with their chunk totals, then the three steps run as
+// kernels of their own.
+__global__ void k_xs_fill(const double* __restrict__ t, int n, XsSum s) {
+  const XsGeom g(n);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n * n; i += gridDim.x * blockDim.x) {
+    const int y = i / n, x = i - y * n;
+    int tx = x / 64;
+    if (tx > g.nx - 1) tx = g.nx - 1;
+    int ty = y / 8;
+    if (ty > g.ny - 1) ty = g.ny - 1;
+    xs_block(s, ty * g.nx + tx)[xs_at(x - 64 * tx, y - 8 * ty)] = t[i];
+  }
+}
+__global__ void k_xs_totals(const double* __restrict__ t, int n, XsSum s) {
+  const XsGeom g(n);
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n * g.nx; j += gridDim.x * blockDim.x) {
+    const int y = j / g.nx, tx = j - y * g.nx;
+    const int x0 = 64 * tx, x1 = (tx == g.nx - 1) ? n : x0 + 64;
+    double a = 0.0;
+    for (int x = x0; x < x1; ++x) a += t[(size_t)y * n + x];
+    s.tot[2 * j] = a;
+    s.tot[2 * j + 1] = 0.0;
+  }
+}
+__global__ void k_xs_predict(XsSum s, int n) {
+  __shared__ double wtot[32];
+  xs_predict(&s, 1, XsGeom(n), wtot, nullptr);
+}
+__global__ void k_xs_summaries(XsSum s, int n) {
+  const XsGeom g(n);
+  if ((int)threadIdx.x >= kXsTilesPerTask * kXsBR) return;
+  const int b = blockIdx.x * kXsTilesPerTask + (int)threadIdx.x / kXsBR;
+  if (b >= g.nx * g.ny) return;
+  xs_summary_row(s, g, b, (int)threadIdx.x % kXsBR);
+}
+__global__ void k_xs_walk(XsSum s, int n, double* out) {
+  __shared__ double r[1];
+  xs_walk(&s, 1, XsGeom(n), r, nullptr);
+  if (threadIdx.x == 0) *out = r[0];
+}
+
 // One device batch through a CUDA graph.  The first call with a given set of
 // parameters and buffers runs directly (and sizes every buffer); the second
 // captures the same work on the context's capture stream and replays it; later
@@ -1664,6 +1707,28 @@ int msgpu_autotune_device(msgpu_context* ctx, const msgpu_params* p, const doubl
   if (rc) return rc;
   CK(cudaStreamSynchronize(st));
   return sched_error_check(ctx);
+}
+
+int msgpu_exact_sum_device(msgpu_context* ctx, int level, const double* d_terms, double* d_out, void* stream) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (level < 1 || level > kMaxLevel || !d_terms || !d_out)
+    return fail(ctx, MSGPU_ERR_INVALID_ARG, "invalid exact_sum arguments");
+  int rc;
+  if ((rc = bind_device(ctx))) return rc;
+  const int n = lvl_n(level);
+  const XsLayout L(n);
+  if ((rc = ensure(ctx, ctx->xsum, sizeof(double) * L.stride))) return rc;
+  const XsSum s = xs_sum((double*)ctx->xsum.p, n, 0, false);
+  cudaStream_t st = (cudaStream_t)stream;
+  const XsGeom g(n);
+  k_xs_fill<<<std::min(2048, (n * n + 255) / 256), 256, 0, st>>>(d_terms, n, s);
+  k_xs_totals<<<std::min(2048, (n * g.nx + 255) / 256), 256, 0, st>>>(d_terms, n, s);
+  k_xs_predict<<<1, 256, 0, st>>>(s, n);
+  k_xs_summaries<<<(g.nx * g.ny + kXsTilesPerTask - 1) / kXsTilesPerTask, 256, 0, st>>>(s, n);
+  k_xs_walk<<<1, 32, 0, st>>>(s, n, d_out);
+  CK(cudaGetLastError());
+  ctx->stats.kernel_launches += 5;
+  return MSGPU_OK;
 }
 
 int msgpu_set_graphs(msgpu_context* ctx, int on) {

@@ -108,7 +108,7 @@ EXPORTS = [
     "msgpu_empty_lines_to_nan", "msgpu_empty_lines_to_nan_device", "msgpu_remove_empty_lines",
     "msgpu_remove_empty_lines_device", "msgpu_set_wait_limits", "msgpu_set_sum_order", "msgpu_warp_sum_device",
     "msgpu_mean_from_sums_device", "msgpu_set_graphs", "msgpu_get_tuning", "msgpu_set_tuning",
-    "msgpu_autotune_device", "msgpu_gd_level_log",
+    "msgpu_autotune_device", "msgpu_gd_level_log", "msgpu_exact_sum_device",
 ]
 
 
@@ -142,6 +142,8 @@ def lib():
         L.msgpu_gd_level.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_double,
                                      ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp, _ip, _dp, ctypes.c_int]
         L.msgpu_gd_level_log.argtypes = L.msgpu_gd_level.argtypes
+        L.msgpu_exact_sum_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_void_p]
         L.msgpu_match_series_stage.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params), _dp, _dp, ctypes.c_int,
                                                _dp, _dp, _ip, _dp, _dp]
         L.msgpu_match_series_stage_device.argtypes = [ctypes.c_void_p, ctypes.POINTER(Params), ctypes.c_void_p,
@@ -693,6 +695,10 @@ class Context:
                                                 d_phis_scratch, stream or None))
         return {lv: self.tuning(bool(params.use_fp64), lv)
                 for lv in range(params.start_level, params.stop_level + 1)}
+
+    def exact_sum_device(self, level: int, d_terms: int, d_out: int, stream: int = 0):
+        """The reference-order (sequentially rounded) sum of (2^level+1)^2 doubles."""
+        self._check(lib().msgpu_exact_sum_device(self._h, level, d_terms, d_out, stream or None))
 
     def set_graphs(self, on: bool):
         """CUDA-graph capture and replay of the device batch calls (default on)."""

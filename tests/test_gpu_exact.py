@@ -145,3 +145,53 @@ def test_parallel_sum_order_stays_within_rounding(gpu, oracle):
     finally:
         gpu.set_sum_order(0)
     assert abs(e - d["E"][2]) <= 1e-13 * abs(d["E"][2])
+
+
+def _sequential(t):
+    s = 0.0
+    for v in t.tolist():
+        s += v
+    return s
+
+
+@pytest.mark.parametrize("level", [6, 9])
+def test_exact_sum_is_the_sequential_sum_on_hard_data(level):
+    """The reference-order sum on its own (msgpu_exact_sum_device) against a
+    plain left-to-right loop, on data made to defeat it: mixed signs, a huge
+    dynamic range, dyadic terms that make round-half-even ties frequent,
+    cancellations back to zero, signed zeros and subnormals, terms that keep
+    the sum crossing binades, and non-finite terms."""
+    import torch
+    import msgpu
+    n = (1 << level) + 1
+    N = n * n
+    rng = np.random.default_rng(level)
+    cases = {
+        "normal": rng.normal(size=N),
+        "range": np.exp(rng.uniform(-40, 40, N)) * rng.choice([-1.0, 1.0], N),
+        "dyadic_ties": rng.integers(-1000, 1000, N) * np.ldexp(1.0, rng.integers(-60, 0, N)),
+        "positive_dyadic": rng.integers(1, 8, N) * np.ldexp(1.0, rng.integers(-53, -40, N)),
+        "cancel": np.repeat(rng.normal(size=N // 2 + 1), 2)[:N] * np.resize([1.0, -1.0], N),
+        "zeros": np.where(rng.random(N) < 0.5, rng.choice([0.0, -0.0, 5e-324, -5e-324], N), rng.normal(size=N)),
+        "binades": np.where(np.arange(N) % 3 == 0, 1.0, -np.ldexp(1.0, -rng.integers(1, 60, N))),
+    }
+    nan = rng.normal(size=N)
+    nan[N // 2] = np.nan
+    inf = rng.normal(size=N)
+    inf[N // 3] = np.inf
+    cases["nan"], cases["inf"] = nan, inf
+    ctx = msgpu.Context(0)
+    try:
+        dev = torch.device("cuda", 0)
+        out = torch.empty(1, dtype=torch.float64, device=dev)
+        for name, t in cases.items():
+            d = torch.from_numpy(np.ascontiguousarray(t, dtype=np.float64)).to(dev)
+            ctx.exact_sum_device(level, d.data_ptr(), out.data_ptr())
+            torch.cuda.synchronize(dev)
+            got, want = float(out.item()), _sequential(t)
+            if np.isnan(want):
+                assert np.isnan(got), name
+            else:
+                assert got == want and np.signbit(got) == np.signbit(want), (name, got, want)
+    finally:
+        ctx.close()
