@@ -454,8 +454,8 @@ int msgpu_gd_level(msgpu_context* ctx, int level, const double* R, const double*
 
 /* msgpu_gd_level with the reference's per-level energy log instead of the
  * trace: energy_log receives min(steps, max_rows - 1) + 1 rows of
- * (iteration - 1, lambda * E_reg of the last energy evaluation, energy at
- * the new position), the first row (-1) for the initial position -- the
+ * (iteration - 1, lambda * E_reg at the new position, energy at the new
+ * position), the first row (-1) for the initial position -- the
  * columns the reference writes to energy_%02d.txt (gradientDescent.h:
  * 254-272, through findTransformation, registration.h:967-1000).           */
 int msgpu_gd_level_log(msgpu_context* ctx, int level, const double* R, const double* T, double* phix,

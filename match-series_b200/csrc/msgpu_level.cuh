@@ -84,7 +84,7 @@ struct LevelArgs {
   int max_trace;
   // optional energy log of the reference's per-level file (energy_%02d.txt,
   // gradientDescent.h:254-272): per instance max_trace + 1 rows of
-  // (iteration - 1, lambda * E_reg of the last evaluation, energy), the
+  // (iteration - 1, lambda * E_reg at the new position, energy), the
   // first row (-1) for the initial position
   double* elog;
   unsigned long long* pass_cycles;  // optional: per CTA kPassKinds clock64 totals
@@ -1360,7 +1360,9 @@ struct InstCtl {
   int ls;              // TRIAL role: 0 doubling, 1 halving, 2 energy at the accepted step
   int iter, evals, total_evals, attempt, rb_pos, pending, od_zero, cur, dcur;
   double energy, energy_new, f, sigma, sigma_used, tau, og2, A, Bd, Cd, Df, t, beta, tau_p;
-  double last_ereg;    // E_reg of the last energy evaluation (the energy log)
+  double last_ereg;    // E_reg of the last energy evaluation
+  double ereg_pos;     // E_reg at the current position (the energy log)
+  double rb_r[2];      // E_reg of the ring buffer's evaluations
   double rb_tau[2], rb_e[2];
   double n1[kRedSlots];      // NCC: totals of energy sub 1 (mean, then A or Df B C)
 };
@@ -1714,18 +1716,23 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
   auto push_ring = [&](double t, double e) {
     c.rb_tau[c.rb_pos] = t;
     c.rb_e[c.rb_pos] = e;
+    c.rb_r[c.rb_pos] = c.last_ereg;
     c.rb_pos ^= 1;
     c.evals++;
   };
+  // the reference's energy log holds lambda * E_reg at the new position
+  // (with a log file it evaluates the energy there again, gradientDescent.h:
+  // 364-369, and writes the last evaluation's components)
   auto log_row = [&](int row, double en) {
     if (a.elog && row <= a.max_trace) {
       double* lg = a.elog + ((size_t)inst * (a.max_trace + 1) + row) * 3;
       lg[0] = (double)(row - 1);
-      lg[1] = lam * c.last_ereg;
+      lg[1] = lam * c.ereg_pos;
       lg[2] = en;
     }
   };
-  auto end_iteration = [&](double en) {
+  auto end_iteration = [&](double en, double er) {
+    c.ereg_pos = er;
     if (c.tau != 0) {
       c.pending = 1;
       c.tau_p = c.tau;
@@ -1752,15 +1759,15 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
   auto step_done = [&](double acc_tau) {
     c.tau = acc_tau;
     // energy at the new position (gradientDescent.h:365-395)
-    double en = nan("");
-    if (c.rb_tau[0] == c.tau) en = c.rb_e[0];
-    else if (c.rb_tau[1] == c.tau) en = c.rb_e[1];
+    double en = nan(""), er = c.ereg_pos;
+    if (c.rb_tau[0] == c.tau) en = c.rb_e[0], er = c.rb_r[0];
+    else if (c.rb_tau[1] == c.tau) en = c.rb_e[1], er = c.rb_r[1];
     else if (c.tau == 0) en = c.energy;
     if (isnan(en) && c.tau != 0) {
       trial(c.tau, 2);
       return;
     }
-    end_iteration(en);
+    end_iteration(en, er);
   };
   auto attempt_done = [&](double res) {
     const bool fallback = (c.attempt == 1);
@@ -1810,6 +1817,7 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
       c.last_ereg = xr ? ereg_exact() : 0.5 * c.A;
       c.energy = energy_of(xr ? xr[0] : tot[0], c.last_ereg);
       c.energy_new = c.energy;
+      c.ereg_pos = c.last_ereg;
       log_row(0, c.energy);
       if (a.mode == MODE_ENERGY) {
         to(TK_GRAD);
@@ -1893,7 +1901,7 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
       const double fnew = energy_of(xr ? xr[0] : tot[0], c.last_ereg);
       push_ring(t, fnew);
       if (c.ls == 2) {
-        end_iteration(fnew);
+        end_iteration(fnew, c.last_ereg);
         break;
       }
       const double G = (fnew - f) / (c.Df * t);

@@ -258,12 +258,46 @@ __device__ __forceinline__ double xs_add_lanes(double S, double v, int cnt) {
     if (first > pos) S = (double)__shfl_sync(0xffffffffu, mi, first - 1) * xs_pow2(E);
     if (first < cnt) {
       S = __dadd_rn(S, __shfl_sync(0xffffffffu, v, first));
+      if (first == pos) {
+        // no run at all: the sum changes binade term after term here, so
+        // the rest of the segment goes one addition after the other
+        for (int k = first + 1; k < cnt; ++k) S = __dadd_rn(S, __shfl_sync(0xffffffffu, v, k));
+        return S;
+      }
       pos = first + 1;
     } else {
       pos = cnt;
     }
   }
   return S;
+}
+
+// S + t_0 + ... + t_{cnt-1} one addition after the other (lane k holds t_k);
+// the shuffles do not depend on S, so they are issued ahead of the additions.
+__device__ __forceinline__ double xs_add_seq(double S, double v, int cnt) {
+#pragma unroll
+  for (int k0 = 0; k0 < 32; k0 += 8) {
+    if (k0 >= cnt) break;
+    double t[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) t[i] = __shfl_sync(0xffffffffu, v, k0 + i);
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+      if (k0 + i < cnt) S = __dadd_rn(S, t[i]);
+  }
+  return S;
+}
+
+// One segment of up to 32 terms: where the terms are not small against the
+// running sum (its binade would change at many of them) one addition after
+// the other, else the binade runs of xs_add_lanes.
+__device__ __forceinline__ double xs_add_segment(double S, double v, int cnt) {
+  const int lane = threadIdx.x & 31;
+  double a = lane < cnt ? fabs(v) : 0.0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  if (!(a < fabs(S) * 0.015625)) return xs_add_seq(S, v, cnt);   // also for S = 0 and non-finite values
+  return xs_add_lanes(S, v, cnt);
 }
 
 // fl(... fl(fl(S + p_0) + p_1) ... + p_{len-1}) for chunk j, by the warp in
@@ -276,9 +310,9 @@ __device__ __forceinline__ double xs_add_chunk(const XsSum& s, const XsGeom& g, 
   const double v0 = (lane < len) ? __ldcg(p + xs_at(lane, 0)) : 0.0;
   const double v1 = (lane + 32 < len) ? __ldcg(p + xs_at(lane + 32, 0)) : 0.0;
   const double v2 = (lane + 64 < len) ? __ldcg(p + xs_at(lane + 64, 0)) : 0.0;
-  S = xs_add_lanes(S, v0, len < 32 ? len : 32);
-  if (len > 32) S = xs_add_lanes(S, v1, len < 64 ? len - 32 : 32);
-  if (len > 64) S = xs_add_lanes(S, v2, len - 64);
+  S = xs_add_segment(S, v0, len < 32 ? len : 32);
+  if (len > 32) S = xs_add_segment(S, v1, len < 64 ? len - 32 : 32);
+  if (len > 64) S = xs_add_seq(S, v2, len - 64);
   return S;
 }
 
@@ -403,23 +437,42 @@ constexpr int kXsTilesPerTask = 256 / kXsBR;   // term blocks per task tile of s
 // [4] chunks walked, [5] chunks added term by term.
 __device__ void xs_predict(const XsSum* sums, int ns, const XsGeom& g, double* wtot /* shared [8] */,
                            unsigned long long* prof) {
-  const int nthr = blockDim.x;
   const long long t0 = clock64();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int k = 0; k < ns; ++k) {
     const XsSum& s = sums[k];
     const int nch = s.rows * g.nx;
-    const int per = (nch + nthr - 1) / nthr;
-    const int c0 = threadIdx.x * per, c1 = min(c0 + per, nch);
+    // warp w takes the contiguous range [c0, c1) in rounds of 32 chunks,
+    // lane l chunk c0 + 32 i + l (coalesced loads of the two partial totals)
+    const int per = ((nch + nw - 1) / nw + 31) & ~31;
+    const int c0 = warp * per, c1 = min(c0 + per, nch);
     double loc = 0.0;
-#pragma unroll 8
-    for (int j = c0; j < c1; ++j) loc += __ldcg(s.tot + 2 * j) + __ldcg(s.tot + 2 * j + 1);
-    double run = xs_block_excl(loc, wtot);
-#pragma unroll 8
-    for (int j = c0; j < c1; ++j) {
+    for (int c = c0 + lane; c < c1; c += 32) {
+      const double2 tt = __ldcg(reinterpret_cast<const double2*>(s.tot) + c);
+      loc += tt.x + tt.y;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) loc += __shfl_xor_sync(0xffffffffu, loc, o);
+    if (lane == 0) wtot[warp] = loc;
+    __syncthreads();
+    double run = 0.0;
+    for (int w = 0; w < warp; ++w) run += wtot[w];
+    __syncthreads();
+    for (int cb = c0; cb < c1; cb += 32) {
+      const int c = cb + lane;
+      const double2 tt = c < c1 ? __ldcg(reinterpret_cast<const double2*>(s.tot) + c) : make_double2(0.0, 0.0);
+      const double v = tt.x + tt.y;
+      double inc = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const double u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += u;
+      }
+      const double start = run + (inc - v);   // estimated running sum at the chunk start
       int E;
       long long m;
-      __stcg(s.ef + j, xs_split(run, E, m) ? xs_pack(E, 0) : kXsNoExp);
-      run += __ldcg(s.tot + 2 * j) + __ldcg(s.tot + 2 * j + 1);
+      if (c < c1) __stcg(s.ef + c, xs_split(start, E, m) ? xs_pack(E, 0) : kXsNoExp);
+      run += __shfl_sync(0xffffffffu, inc, 31);
     }
   }
   __threadfence();

@@ -770,7 +770,7 @@ class Context:
 
     def gd_level_log(self, level, R, T, phix, phiy, lam, max_iter, stop_eps=0.0, fp64=True):
         """gd_level with the reference's per-level energy log: rows of
-        (iteration - 1, lambda * E_reg of the last evaluation, energy)."""
+        (iteration - 1, lambda * E_reg at the new position, energy)."""
         px = _f64(phix).copy()
         py = _f64(phiy).copy()
         e = ctypes.c_double()

@@ -91,7 +91,14 @@ def test_reference_program_with_gpu_registration_writes_the_reference_files(tmp_
     assert "stage1/average.q2bz" in ref_files and "stage1/energies.txt" in ref_files
     assert any(os.path.basename(f).startswith("energy_") for f in ref_files)
     for f in ref_files:
-        assert filecmp.cmp(os.path.join(ref_out, f), os.path.join(gpu_out, f), shallow=False), f
+        a, b = os.path.join(ref_out, f), os.path.join(gpu_out, f)
+        if not filecmp.cmp(a, b, shallow=False):
+            if f.endswith(".txt"):
+                import difflib
+                diff = "".join(list(difflib.unified_diff(open(a).readlines(), open(b).readlines()))[:20])
+            else:
+                diff = ""
+            raise AssertionError(f"{f} differs\n{diff}")
     # the displacements are not trivial
     phi = msgpu.read_displacement(os.path.join(gpu_out, "stage1", "1", f"deformation_{level:02d}_%d.dat.bz2"), n)
     assert np.abs(phi).max() * (n - 1) > 0.05
