@@ -10,7 +10,6 @@
 //      (quocDescent.h:83-105, registration.h:510-521)
 //   4. prolongation to the precision level (registration.h:462-467)
 // and msgpu_warp_mean the warped-frame average (matchSeries.h:385-425).
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -68,8 +67,7 @@ struct msgpu_context {
   cudaEvent_t ev[32] = {};
   bool ev_ready = false;
   int last_grid = 0;        // CTAs of the last level launch
-  // seismic line-shift solve: cuBLAS for the H1 metric, its spectral basis
-  cublasHandle_t blas = nullptr;
+  // seismic line-shift solve: the spectral basis of its H1 metric
   int xs_nx = 0, xs_ny = 0;
   Buf xs_basis, xs_work;
   std::vector<msgpu_context*> workers;   // contexts of the batch workers (own streams and buffers)
@@ -1793,7 +1791,6 @@ int msgpu_destroy(msgpu_context* ctx) {
     for (int i = 0; i < 32; ++i) cudaEventDestroy(ctx->ev[i]);
   for (msgpu_context* w : ctx->workers) msgpu_destroy(w);
   ctx->workers.clear();
-  if (ctx->blas) cublasDestroy(ctx->blas);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return MSGPU_OK;
@@ -2259,10 +2256,7 @@ struct XsBufs {
 
 int xs_setup(msgpu_context* ctx, int nx, int ny, XsBufs& B, cudaStream_t st) {
   int rc;
-  if (!ctx->blas) {
-    if (cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS) return fail(ctx, MSGPU_ERR_CUDA, "cublasCreate failed");
-  }
-  if (cublasSetStream(ctx->blas, st) != CUBLAS_STATUS_SUCCESS) return fail(ctx, MSGPU_ERR_CUDA, "cublasSetStream failed");
+  (void)st;
   const int ne = (nx + 1) / 2, no = nx / 2;
   const size_t nb = (size_t)ne * ne + (size_t)no * no + (size_t)ny * ny + nx + ny;
   if ((rc = ensure(ctx, ctx->xs_basis, sizeof(double) * nb))) return rc;
@@ -2300,8 +2294,18 @@ int xs_setup(msgpu_context* ctx, int nx, int ny, XsBufs& B, cudaStream_t st) {
   return MSGPU_OK;
 }
 
+// C = op(A) op(B), column-major, by k_dgemm (FP64 on the tensor pipe).
+cudaError_t dgemm(cudaStream_t st, bool ta, bool tb, int M, int N, int K, const double* A, int lda,
+                  const double* B, int ldb, double* C, int ldc) {
+  const dim3 grid((unsigned)((M + kGemmBM - 1) / kGemmBM), (unsigned)((N + kGemmBN - 1) / kGemmBN));
+  if (ta && tb) k_dgemm<true, true><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, C, ldc);
+  else if (ta) k_dgemm<true, false><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, C, ldc);
+  else if (tb) k_dgemm<false, true><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, C, ldc);
+  else k_dgemm<false, false><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, C, ldc);
+  return cudaGetLastError();
+}
+
 int xs_metric(msgpu_context* ctx, const XsBufs& B, int nx, int ny, double sigma, double* g, cudaStream_t st) {
-  const double one = 1.0, zero = 0.0;
   const double tau = 0.5 * (sigma * sigma);
   const int ne = (nx + 1) / 2, no = nx / 2;
   const int N = nx * ny;
@@ -2310,17 +2314,13 @@ int xs_metric(msgpu_context* ctx, const XsBufs& B, int nx, int ny, double sigma,
   // parity-folded columns (even and odd modes), along y with Vy; scaling;
   // synthesis along y, then along x and unfolded.
   k_xfold<<<gb, 256, 0, st>>>(g, B.t1, nx, ny);
-  if (cublasDgemm(ctx->blas, CUBLAS_OP_T, CUBLAS_OP_N, ne, ny, ne, &one, B.Ve, ne, B.t1, nx, &zero, B.t2, nx) ||
-      cublasDgemm(ctx->blas, CUBLAS_OP_T, CUBLAS_OP_N, no, ny, no, &one, B.Vo, no, B.t1 + ne, nx, &zero, B.t2 + ne,
-                  nx) ||
-      cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, nx, ny, ny, &one, B.t2, nx, B.Vy, ny, &zero, B.t1, nx))
-    return fail(ctx, MSGPU_ERR_CUDA, "cublasDgemm failed");
+  CK(dgemm(st, true, false, ne, ny, ne, B.Ve, ne, B.t1, nx, B.t2, nx));
+  CK(dgemm(st, true, false, no, ny, no, B.Vo, no, B.t1 + ne, nx, B.t2 + ne, nx));
+  CK(dgemm(st, false, false, nx, ny, ny, B.t2, nx, B.Vy, ny, B.t1, nx));
   k_spectral_scale<<<gb, 256, 0, st>>>(B.t1, B.lx, B.ly, tau, nx, ny);
-  if (cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_T, nx, ny, ny, &one, B.t1, nx, B.Vy, ny, &zero, B.t2, nx) ||
-      cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, ne, ny, ne, &one, B.Ve, ne, B.t2, nx, &zero, B.t1, nx) ||
-      cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, no, ny, no, &one, B.Vo, no, B.t2 + ne, nx, &zero, B.t1 + ne,
-                  nx))
-    return fail(ctx, MSGPU_ERR_CUDA, "cublasDgemm failed");
+  CK(dgemm(st, false, true, nx, ny, ny, B.t1, nx, B.Vy, ny, B.t2, nx));
+  CK(dgemm(st, false, false, ne, ny, ne, B.Ve, ne, B.t2, nx, B.t1, nx));
+  CK(dgemm(st, false, false, no, ny, no, B.Vo, no, B.t2 + ne, nx, B.t1 + ne, nx));
   k_xunfold<<<gb, 256, 0, st>>>(B.t1, g, nx, ny);
   CK(cudaGetLastError());
   ctx->stats.kernel_launches += 9;

@@ -562,4 +562,77 @@ __global__ void k_spectral_scale(double* z, const double* lx, const double* ly, 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Dense FP64 products of the H1 metric's cosine-basis transforms, on the
+// tensor pipe: C = op(A) op(B), column-major (the layout of the transforms:
+// an nx x ny image with x fastest is an nx x ny column-major matrix), op a
+// transpose when TA / TB.  A 64 x 64 tile of C per CTA (256 threads, 8 warps
+// of 32 x 16), k in steps of 16 through shared memory, each warp issuing
+// mma.sync m8n8k4 FP64 (DMMA) on fragments read from shared memory.
+constexpr int kGemmBM = 64, kGemmBN = 64, kGemmBK = 16, kGemmPad = 2;
+
+__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(256) k_dgemm(int M, int N, int K, const double* __restrict__ A, int lda,
+                                              const double* __restrict__ B, int ldb, double* __restrict__ C,
+                                              int ldc) {
+  __shared__ double As[kGemmBK][kGemmBM + kGemmPad];   // As[k][m] = op(A)(m, k)
+  __shared__ double Bs[kGemmBK][kGemmBN + kGemmPad];   // Bs[k][n] = op(B)(k, n)
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int bm = blockIdx.x * kGemmBM, bn = blockIdx.y * kGemmBN;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+  double acc[4][2][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  for (int k0 = 0; k0 < K; k0 += kGemmBK) {
+    // op(A) tile (64 x 16) and op(B) tile (16 x 64), zero outside the matrices
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int i = tid + 256 * r;
+      int m, k;
+      if (TA) { k = i % kGemmBK; m = i / kGemmBK; } else { m = i % kGemmBM; k = i / kGemmBM; }
+      const int gm = bm + m, gk = k0 + k;
+      double v = 0.0;
+      if (gm < M && gk < K) v = TA ? A[gk + (size_t)gm * lda] : A[gm + (size_t)gk * lda];
+      As[k][m] = v;
+      int n;
+      if (TB) { n = i % kGemmBN; k = i / kGemmBN; } else { k = i % kGemmBK; n = i / kGemmBK; }
+      const int gn = bn + n, gk2 = k0 + k;
+      double w = 0.0;
+      if (gn < N && gk2 < K) w = TB ? B[gn + (size_t)gk2 * ldb] : B[gk2 + (size_t)gn * ldb];
+      Bs[k][n] = w;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kGemmBK; kk += 4) {
+      double a[4], b[2];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[kk + (lane & 3)][wm + 8 * i + (lane >> 2)];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) b[j] = Bs[kk + (lane & 3)][wn + 8 * j + (lane >> 2)];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int m = bm + wm + 8 * i + (lane >> 2), n = bn + wn + 8 * j + (lane & 3) * 2 + e;
+        if (m < M && n < N) C[m + (size_t)n * ldc] = acc[i][j][e];
+      }
+}
+
 }  // namespace msg

@@ -17,9 +17,8 @@ DEPS = SOURCES + [os.path.join(CSRC, f) for f in ("msgpu_level.cuh", "msgpu_fe.c
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
               "-Xcompiler", "-fPIC", "-shared"]
 # bzip2 (the image has the shared library without its development symlink)
-# and zlib for the compressed array files of msgpu_io.cpp; cuBLAS for the
-# dense products of the seismic model's H1 metric
-LIBS = ["-l:libbz2.so.1.0", "-lz", "-lcublas"]
+# and zlib for the compressed array files of msgpu_io.cpp
+LIBS = ["-l:libbz2.so.1.0", "-lz"]
 
 
 def nvcc() -> str:
