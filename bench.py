@@ -63,6 +63,12 @@ LEVEL, START, FRAMES, MAX_ITER, LAMBDA = 9, 5, 20, 30, 0.1
 DATA_TERM = 0   # 0: SSD (deformationModel 22); 1: normalized cross-correlation (--ncc)
 
 
+def use_tuning(ctx):
+    """Loads the committed scheduler table (measured on B200) when it exists."""
+    if os.path.exists(os.path.join(ROOT, "match-series_b200", "msgpu", "tuning_b200.json")):
+        ctx.load_tuning()
+
+
 def workload(rank: int):
     """One series: frame FRAMES is the stage's reference on every rank; rank
     0 registers frames 0..FRAMES-1, rank r > 0 the next FRAMES frames after
@@ -367,6 +373,7 @@ def main_series(args, world, rank, local):
     n = (1 << LEVEL) + 1
     N = n * n
     ctx = msgpu.Context(local)
+    use_tuning(ctx)
     dev = torch.device("cuda", local)
     d_frames = torch.from_numpy(frames).to(dev)
     d_phis = torch.empty((m, 2, N), dtype=torch.float64, device=dev)
@@ -501,6 +508,7 @@ def main_files(args, world, rank, local):
     nlev = LEVEL - START + 1
     threads = cpu_procs()
     ctx = msgpu.Context(local)
+    use_tuning(ctx)
     with tempfile.TemporaryDirectory() as wd:
         # --- the files (untimed): FILE_SERIES series, reference frame first
         series = []
@@ -619,6 +627,7 @@ def main_ragged(args, world, rank, local):
     total = sum(F)
     p = msgpu.default_params(start_level=4, max_gd_iterations=MAX_ITER, use_fp64=int(fp64), lambda_=LAMBDA)
     ctx = msgpu.Context(local)
+    use_tuning(ctx)
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
     keep, descs = [], []
@@ -1037,6 +1046,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--fp32", action="store_true", help="FP32 bulk with FP64 reductions (outside the energy tol)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="tune the level scheduler on the workload first (msgpu_autotune_device); writes the table "
+                         "to gpurun_out/tuning.json when that folder exists")
     ap.add_argument("--sum-order", type=int, default=0, choices=[0, 1],
                     help="0: global sums in the reference's sequential order (bit-exact, default); "
                          "1: fixed parallel order")
@@ -1161,6 +1173,20 @@ def main():
     d_count = torch.empty(N + 1, dtype=torch.float64, device=dev)   # slot N: fill of pixels without samples
     d_sum = torch.empty(N, dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream(dev)
+
+    tuned = None
+    if args.autotune:
+        scratch = torch.empty_like(d_phis)
+        tuned = ctx.autotune_device(p, d_ref.data_ptr(), d_tmpl.data_ptr(), FRAMES, scratch.data_ptr(),
+                                    stream.cuda_stream)
+        if rank == 0 and os.path.isdir(os.path.join(ROOT, "gpurun_out")):
+            key = "fp64" if fp64 else "fp32"
+            json.dump({"device": torch.cuda.get_device_name(dev),
+                       "workload": f"{FRAMES} frames 513x513, levels {START}-{LEVEL}, sum order {SUM_ORDER}",
+                       "levels": {key: {str(k): v for k, v in tuned.items()}}},
+                      open(os.path.join(ROOT, "gpurun_out", "tuning.json"), "w"), indent=1)
+    elif os.path.exists(os.path.join(ROOT, "match-series_b200", "msgpu", "tuning_b200.json")):
+        ctx.load_tuning()
 
     def step():
         if world == 1:
@@ -1304,6 +1330,8 @@ def main():
                                        f"(NCCL all-reduce)")},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
+            "tuning": tuned if tuned is not None else "table" if os.path.exists(
+                os.path.join(ROOT, "match-series_b200", "msgpu", "tuning_b200.json")) else "defaults",
             "roofline": {"bound": "hbm", "kernel": f"level_kernel<{'double' if fp64 else 'float'}> level {LEVEL}",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "traffic": traffic,

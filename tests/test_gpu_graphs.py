@@ -82,3 +82,26 @@ def test_reallocated_buffers_invalidate_the_graph():
         assert np.array_equal(phi, want_phi) and np.array_equal(e, want_e)
     finally:
         ctx.close()
+
+
+def test_autotuner_fills_the_table_and_keeps_the_results():
+    """msgpu_autotune_device times every level under each candidate setting
+    and keeps the fastest; a batch under the tuned settings gives the same
+    bits as under the defaults (the scheduling never changes a result)."""
+    import torch
+    import msgpu
+    ctx = msgpu.Context(0)
+    try:
+        p, d_ref, d_tmpl, d_phis, d_e = _setup(7, 3, 7304)
+        ctx.set_graphs(False)
+        want_phi, want_e, _ = _call(ctx, p, d_ref, d_tmpl, d_phis, d_e)
+        scratch = torch.empty_like(d_phis)
+        table = ctx.autotune_device(p, d_ref.data_ptr(), d_tmpl.data_ptr(), d_tmpl.shape[0], scratch.data_ptr())
+        assert sorted(table) == list(range(p.start_level, p.stop_level + 1))
+        for lv, t in table.items():
+            assert t["chunk_div"] in (12, 24, 48) and t["chunk_max"] in (8, 16, 32)
+            assert t["ctas_per_sm"] in (1, 2) and 0 < t["ms"] < 1e4
+        phi, e, _ = _call(ctx, p, d_ref, d_tmpl, d_phis, d_e)
+        assert np.array_equal(phi, want_phi) and np.array_equal(e, want_e)
+    finally:
+        ctx.close()
