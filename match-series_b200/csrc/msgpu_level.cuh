@@ -2193,17 +2193,36 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
       // then a summary pass over the grid, whose completing CTA walks the
       // chunks and takes the control step of the pass it stands for
       const int nxs = (a.xs && t.desc.kind != TK_XSUM) ? xs_count(a, t.desc) : 0;
+      // small levels: the summaries by this CTA right away (a pass of its own
+      // would cost more in latency than its work)
+      const XsGeom xg(a.n);
+      const bool xs_inline = nxs && nxs * xg.nx * xg.ny * kXsBR <= 6 * kThreads;
       if (t.desc.kind == TK_XSUM || nxs) {
         const int kind = (t.desc.kind == TK_XSUM) ? t.desc.purpose : t.desc.kind;
         const int ns = (t.desc.kind == TK_XSUM) ? t.desc.xn : nxs;
         if (threadIdx.x == 0) xs_pass_sums(a, t.inst, kind, ns, xss);
         __syncthreads();
-        if (t.desc.kind == TK_XSUM) xs_walk(xss, ns, XsGeom(a.n), xres, a.xs_prof);
-        else xs_predict(xss, ns, XsGeom(a.n), xwtot, a.xs_prof);
+        if (t.desc.kind == TK_XSUM) {
+          xs_walk(xss, ns, xg, xres, a.xs_prof);
+        } else {
+          xs_predict(xss, ns, xg, xwtot, a.xs_prof);
+          if (xs_inline) {
+            const int per = xg.nx * xg.ny * kXsBR;
+            for (int job = threadIdx.x; job < ns * per; job += kThreads) {
+              const int k = job / per, rem = job - k * per;
+              xs_summary_row(xss[k], xg, rem / kXsBR, rem % kXsBR);
+            }
+            __threadfence();
+            __syncthreads();
+            xs_walk(xss, ns, xg, xres, a.xs_prof);
+          }
+        }
       }
       if (threadIdx.x == 0) {
         ctl_load(cs, sp.ctl + t.inst);
-        if (nxs) {
+        if (xs_inline) {
+          advance(a, t.inst, cs, tot, xres);
+        } else if (nxs) {
           cs.desc.purpose = cs.desc.kind;
           cs.desc.xn = nxs;
           cs.desc.kind = TK_XSUM;

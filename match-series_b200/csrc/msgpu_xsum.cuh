@@ -300,20 +300,34 @@ __device__ __forceinline__ double xs_add_segment(double S, double v, int cnt) {
   return xs_add_lanes(S, v, cnt);
 }
 
-// fl(... fl(fl(S + p_0) + p_1) ... + p_{len-1}) for chunk j, by the warp in
-// segments of 32 terms (every lane returns the same value).
-__device__ __forceinline__ double xs_add_chunk(const XsSum& s, const XsGeom& g, int j, double S) {
+// The terms of chunk j, lane k holding terms k, k + 32 and k + 64.
+struct XsChunkTerms {
+  double v0, v1, v2;
+  int len;
+};
+__device__ __forceinline__ XsChunkTerms xs_load_chunk(const XsSum& s, const XsGeom& g, int j) {
   const int lane = threadIdx.x & 31;
   int tile, r, len;
   xs_chunk(s, g, j, tile, r, len);
   const double* p = xs_block(s, tile) + r;
-  const double v0 = (lane < len) ? __ldcg(p + xs_at(lane, 0)) : 0.0;
-  const double v1 = (lane + 32 < len) ? __ldcg(p + xs_at(lane + 32, 0)) : 0.0;
-  const double v2 = (lane + 64 < len) ? __ldcg(p + xs_at(lane + 64, 0)) : 0.0;
-  S = xs_add_segment(S, v0, len < 32 ? len : 32);
-  if (len > 32) S = xs_add_segment(S, v1, len < 64 ? len - 32 : 32);
-  if (len > 64) S = xs_add_seq(S, v2, len - 64);
+  XsChunkTerms c;
+  c.len = len;
+  c.v0 = (lane < len) ? __ldcg(p + xs_at(lane, 0)) : 0.0;
+  c.v1 = (lane + 32 < len) ? __ldcg(p + xs_at(lane + 32, 0)) : 0.0;
+  c.v2 = (lane + 64 < len) ? __ldcg(p + xs_at(lane + 64, 0)) : 0.0;
+  return c;
+}
+
+// fl(... fl(fl(S + p_0) + p_1) ... + p_{len-1}) for a chunk's terms, by the
+// warp in segments of 32 terms (every lane returns the same value).
+__device__ __forceinline__ double xs_add_terms(double S, const XsChunkTerms& c) {
+  S = xs_add_segment(S, c.v0, c.len < 32 ? c.len : 32);
+  if (c.len > 32) S = xs_add_segment(S, c.v1, c.len < 64 ? c.len - 32 : 32);
+  if (c.len > 64) S = xs_add_seq(S, c.v2, c.len - 64);
   return S;
+}
+__device__ __forceinline__ double xs_add_chunk(const XsSum& s, const XsGeom& g, int j, double S) {
+  return xs_add_terms(S, xs_load_chunk(s, g, j));
 }
 
 // The sequential sum 0 + t_0 + t_1 + ... of one sum, by one warp (every lane
@@ -345,12 +359,32 @@ __device__ double xs_drive(const XsSum& s, const XsGeom& g, unsigned long long* 
     const int ef = nef;
     const long long X = nX, lo = nlo, hi = nhi, R = nR, loA = nloA, hiA = nhiA;
     load(jb + lane + 32, nef, nX, nlo, nhi, nR, nloA, nhiA);
+    // chunks where the predicted binade of the next chunk differs (the sum
+    // crosses a binade inside) or without a usable summary: added term by
+    // term, so their terms are fetched ahead, the first one now
+    const int efn = __shfl_down_sync(0xffffffffu, ef, 1);
+    const unsigned slowm =
+        __ballot_sync(0xffffffffu, in && (!(ef & kXsValid) || (lane < 31 && jb + lane + 1 < nch &&
+                                                                   xs_exp(efn) != xs_exp(ef))));
+    auto next_slow = [&](int from) -> int {
+      const unsigned m = from >= 32 ? 0u : (slowm & ~((1u << from) - 1u));
+      return m ? __ffs(m) - 1 : -1;
+    };
+    int pf = next_slow(j - jb);
+    XsChunkTerms pt;
+    if (pf >= 0) pt = xs_load_chunk(s, g, jb + pf);
     while (j < jb + 32 && j < nch) {
       if (isnan(S)) return S;
       int E;
       long long m;
       if (!xs_split(S, E, m)) {
-        S = xs_add_chunk(s, g, j, S);
+        if (j - jb == pf) {
+          S = xs_add_terms(S, pt);
+          pf = next_slow(pf + 1);
+          if (pf >= 0) pt = xs_load_chunk(s, g, jb + pf);
+        } else {
+          S = xs_add_chunk(s, g, j, S);
+        }
         ++slow;
         ++j;
         continue;
@@ -395,7 +429,17 @@ __device__ double xs_drive(const XsSum& s, const XsGeom& g, unsigned long long* 
       if (j < jb + 32 && j < nch) {
         // chunk j interrupts the run (its sums leave the binade, or it has no
         // summary at this exponent): added term by term
-        S = xs_add_chunk(s, g, j, S);
+        if (first == pf) {
+          S = xs_add_terms(S, pt);
+          pf = next_slow(pf + 1);
+          if (pf >= 0) pt = xs_load_chunk(s, g, jb + pf);
+        } else {
+          S = xs_add_chunk(s, g, j, S);
+          if (pf >= 0 && pf < first) {   // the fetched chunk was passed by the run
+            pf = next_slow(first + 1);
+            if (pf >= 0) pt = xs_load_chunk(s, g, jb + pf);
+          }
+        }
         ++slow;
         ++j;
       }
@@ -435,7 +479,7 @@ constexpr int kXsTilesPerTask = 256 / kXsBR;   // term blocks per task tile of s
 
 // Profile counters (nullable): [0] passes, [1..3] cycles of the steps,
 // [4] chunks walked, [5] chunks added term by term.
-__device__ void xs_predict(const XsSum* sums, int ns, const XsGeom& g, double* wtot /* shared [8] */,
+__device__ __noinline__ void xs_predict(const XsSum* sums, int ns, const XsGeom& g, double* wtot /* shared [8] */,
                            unsigned long long* prof) {
   const long long t0 = clock64();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -447,9 +491,14 @@ __device__ void xs_predict(const XsSum* sums, int ns, const XsGeom& g, double* w
     const int per = ((nch + nw - 1) / nw + 31) & ~31;
     const int c0 = warp * per, c1 = min(c0 + per, nch);
     double loc = 0.0;
-    for (int c = c0 + lane; c < c1; c += 32) {
-      const double2 tt = __ldcg(reinterpret_cast<const double2*>(s.tot) + c);
-      loc += tt.x + tt.y;
+    const double2* tot2 = reinterpret_cast<const double2*>(s.tot);
+    for (int c = c0 + lane; c < c1; c += 128) {
+      double2 tt[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        tt[u] = (c + 32 * u < c1) ? __ldcg(tot2 + c + 32 * u) : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) loc += tt[u].x + tt[u].y;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) loc += __shfl_xor_sync(0xffffffffu, loc, o);
@@ -458,9 +507,11 @@ __device__ void xs_predict(const XsSum* sums, int ns, const XsGeom& g, double* w
     double run = 0.0;
     for (int w = 0; w < warp; ++w) run += wtot[w];
     __syncthreads();
+    double2 nxt = (c0 + lane < c1) ? __ldcg(tot2 + c0 + lane) : make_double2(0.0, 0.0);
     for (int cb = c0; cb < c1; cb += 32) {
       const int c = cb + lane;
-      const double2 tt = c < c1 ? __ldcg(reinterpret_cast<const double2*>(s.tot) + c) : make_double2(0.0, 0.0);
+      const double2 tt = nxt;
+      nxt = (c + 32 < c1) ? __ldcg(tot2 + c + 32) : make_double2(0.0, 0.0);
       const double v = tt.x + tt.y;
       double inc = v;
 #pragma unroll
@@ -484,7 +535,7 @@ __device__ void xs_predict(const XsSum* sums, int ns, const XsGeom& g, double* w
 }
 
 // Step 2: the summary of chunk row r of term block t of sum s (one thread).
-__device__ __forceinline__ void xs_summary_row(const XsSum& s, const XsGeom& g, int t, int r) {
+__device__ __noinline__ void xs_summary_row(const XsSum& s, const XsGeom& g, int t, int r) {
   const int ty = t / g.nx, tx = t - ty * g.nx;
   const int rows_t = (ty == g.ny - 1) ? s.rows - ty * 8 : 8;
   if (r >= rows_t) return;
@@ -511,7 +562,7 @@ __host__ __device__ inline int xs_summary_tasks(int ns, int n) {
 }
 
 // Step 3: out[k] = the sequential sum k (one warp per sum).
-__device__ void xs_walk(const XsSum* sums, int ns, const XsGeom& g, double* out /* shared [ns] */,
+__device__ __noinline__ void xs_walk(const XsSum* sums, int ns, const XsGeom& g, double* out /* shared [ns] */,
                         unsigned long long* prof) {
   const long long t0 = clock64();
   const int warp = threadIdx.x >> 5;
