@@ -852,6 +852,79 @@ def net_forward_flops(n0: int) -> float:
     return sum(2.0 * 9 * ci * co * grids[g] ** 2 for ci, co, _, g in spec)
 
 
+def metric_legs(ctx, p, d_ref, d_tmpl, F, plain_ms, plain_e, fp64, local, rank):
+    """The metric's two legs on the stage's own frames (one GPU): the plain
+    GPU gradient flow one frame at a time, and warm start + batch to the
+    stated energy tolerance (the plain batch's final energies + WARM_TOL
+    relative; a frame that does not reach it is registered again from the
+    plain start, counted in the time).  The network (input 513^2, output
+    level 8) is trained first on pairs the plain method registers (untimed,
+    reported)."""
+    import numpy as np
+    import torch
+    import msgpu
+    from msgpu import warmstart as ws
+    dev = torch.device("cuda", local)
+    st = torch.cuda.current_stream(dev)
+    R, T, tgt, t_data = ws.training_set(ctx, level=LEVEL, net_level=LEVEL, num_series=WARM_TRAIN_SERIES,
+                                        frames_per_series=WARM_FPS, seed=9000 + 1000 * rank, fp64=fp64,
+                                        start_level=START)
+    net = msgpu.Net(ctx, LEVEL, seed=1)
+    _, t_train = ws.train(net, R, T, tgt, steps=WARM_STEPS, batch=WARM_BATCH, lr=WARM_LR, seed=rank)
+    del R, T, tgt
+    torch.cuda.empty_cache()
+    N = d_tmpl.shape[1]
+    nlev = LEVEL - START + 1
+    phis = torch.empty((F, 2, N), dtype=torch.float64, device=dev)
+    e = torch.empty(F, dtype=torch.float64, device=dev)
+    s = torch.empty((F, nlev), dtype=torch.int32, device=dev)
+    d_plain = torch.from_numpy(np.ascontiguousarray(plain_e)).to(dev)
+
+    def warm():
+        return ctx.register_batch_warm_device(p, net, d_ref.data_ptr(), d_tmpl.data_ptr(), F, phis.data_ptr(),
+                                              e.data_ptr(), s.data_ptr(), d_plain_energies=d_plain.data_ptr(),
+                                              rel_tol=WARM_TOL, stream=st.cuda_stream)
+
+    one = torch.empty((1, 2, N), dtype=torch.float64, device=dev)
+
+    def single():
+        for f in range(F):
+            ctx.register_batch_device(p, d_ref.data_ptr(), d_tmpl[f].data_ptr(), 1, one.data_ptr(),
+                                      stream=st.cuda_stream)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            r = fn()
+        e1.record(st)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / reps, r
+
+    t_warm, used = timed(warm, 3)
+    t_single, _ = timed(single, 1)
+    ew = e.cpu().numpy()
+    rel = (ew - plain_e) / np.abs(plain_e)
+    net.close()
+    return {
+        "plain_gpu_batched_frames_per_s": F / (plain_ms * 1e-3),
+        "plain_gpu_single_frame_frames_per_s": F / (t_single * 1e-3),
+        "warm_batched_to_energy_tol_frames_per_s": F / (t_warm * 1e-3),
+        "ratio_vs_plain_gpu_single_frame": t_single / t_warm,
+        "ratio_vs_plain_gpu_batched": plain_ms / t_warm,
+        "energy_tol_rel": WARM_TOL,
+        "frames_within_tol": int(np.sum(rel <= WARM_TOL)),
+        "fallback_frames": int(F - int(np.sum(used))),
+        "steps_per_level_warm_to_tol": [round(float(x), 1) for x in s.float().mean(0).cpu().numpy()],
+        "training": {"pairs": WARM_TRAIN_SERIES * WARM_FPS, "steps": WARM_STEPS, "seconds": t_train,
+                     "data_seconds": t_data},
+        "note": "the plain batch's final energies are the targets; frames that end above them by more than the "
+                "tolerance are registered again from the plain start inside the timed region",
+    }
+
+
 def main_warm(args, world, rank, local):
     """--warm: registration started from the learned network's prediction, to
     the stated energy tolerance: the plain batch's final energies are the
@@ -1046,6 +1119,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--fp32", action="store_true", help="FP32 bulk with FP64 reductions (outside the energy tol)")
+    ap.add_argument("--no-warm-leg", action="store_true",
+                    help="skip the metric's warm-start leg (network training + warm-started batch) of the default run")
     ap.add_argument("--autotune", action="store_true",
                     help="tune the level scheduler on the workload first (msgpu_autotune_device); writes the table "
                          "to gpurun_out/tuning.json when that folder exists")
@@ -1311,6 +1386,9 @@ def main():
                         "reference_1ulp_spread": {"max_dphi_px": sp_dphi, "max_rel_energy": sp_rel,
                                                   "perturbation": "every pixel of the reference frame "
                                                                   "+-1 ulp (random signs)"}}
+        legs = None
+        if world == 1 and not args.no_warm_leg:
+            legs = metric_legs(ctx, p, d_ref, d_tmpl, FRAMES, ms_per_step, energies, fp64, local, rank)
         psnr = syn.psnr(mean.reshape(n, n), clean_ref)
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -1339,6 +1417,7 @@ def main():
                          "steps_per_launch": statistics.mean(lvl_steps),
                          "energy_evals_per_launch": statistics.mean(lvl_evals)},
             "cpu_baseline": cpu,
+            "metric_legs": legs,
             "accuracy": accuracy,
             "reconstruction_psnr_db": psnr,
             "steps_per_level_frame0": steps_per_level[0].tolist(),

@@ -545,8 +545,9 @@ int msgpu_prepare_images_device(msgpu_context* ctx, const msgpu_params* p, const
  * plain_energies (the plain method's final energies, nullable) the frames
  * are registered to that stated energy tolerance: the warm-started solve of
  * the stop level ends as soon as a frame's energy is within
- * rel_tol * |plain energy| of (or below) its plain energy, and a frame that
- * ends above that is registered again from the plain start;
+ * rel_tol * |plain energy| of (or below) its plain energy (running up to
+ * twice maxGDIterations steps to get there), and a frame that ends above
+ * that is registered again from the plain start;
  * warm_used_out[f] (host, nullable) = 1 where the warm start was kept.
  * steps_out has the plain layout (stop-start+1 levels per frame; levels
  * below l0-1 count 0 for warm-started frames).                             */

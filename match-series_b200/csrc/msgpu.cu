@@ -860,6 +860,7 @@ struct BatchOpts {
   msgpu_net* warm = nullptr;   // learned warm start: the network's prediction is the start-level displacement
   const double* e_target = nullptr;   // device, per frame: stop the stop-level solve at this energy (+ e_tol)
   double e_tol = 0.0;
+  int max_iter_stop = 0;              // > 0: step limit of the stop level (with energy targets)
 };
 
 int warm_start_phi(msgpu_net* net, const double* pyr, const std::vector<size_t>& poff, size_t pstride, int F,
@@ -1007,6 +1008,7 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
     if (l == stop && opt.e_target) {
       a.e_target = opt.e_target;
       a.e_tol = opt.e_tol;
+      if (opt.max_iter_stop > 0) a.max_iter = opt.max_iter_stop;
     }
     const size_t prof_n = (size_t)max_level_grid(ctx->sm_count) * kPassKinds;
     if (ctx->profiling) {
@@ -4042,6 +4044,10 @@ int warm_batch(msgpu_context* ctx, const msgpu_params& p, msgpu_net* net, const 
   // of them
   opt.e_target = d_plain_e;
   opt.e_tol = rel_tol;
+  // a warm-started frame may need more steps than the plain schedule to
+  // reach its target: the stop level runs until it does, at most twice
+  // maxGDIterations steps (a frame that does not is registered again)
+  opt.max_iter_stop = d_plain_e ? 2 * p.max_gd_iterations : 0;
   if ((rc = run_batch<Real>(ctx, pw, F, io, st, opt))) return rc;
   if (d_e_out) CK(cudaMemcpyAsync(d_e_out, e, sizeof(double) * F, cudaMemcpyDeviceToDevice, st));
   if (d_s_out) {
