@@ -397,8 +397,9 @@ typedef struct {
   /* exact sums (sum order 0) per level: completed passes that added sums,
    * clock cycles of their three steps (binade predictions, chunk summaries,
    * the ordered walk; summed over the passes), chunks walked, chunks added
-   * term by term                                                            */
-  long long level_xs[16][6];
+   * term by term, cycles of those term-by-term additions and cycles of the
+   * walk (both summed over the walking warps)                               */
+  long long level_xs[16][8];
 } msgpu_stats;
 int msgpu_set_profiling(msgpu_context* ctx, int on);
 /* CUDA graphs for msgpu_register_batch_device (and the stage entry points

@@ -75,7 +75,7 @@ struct msgpu_context {
 
 namespace {
 
-constexpr int kAbiVersion = 5;
+constexpr int kAbiVersion = 6;
 // default chunking of the level scheduler: a 24th of a pass, at most 16 tiles
 constexpr int kChunkDiv = 24, kChunkMax = 16;
 
@@ -1078,7 +1078,7 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
       unsigned long long xp[8];
       CK(cudaMemcpy(xp, (unsigned long long*)ctx->prof.p + prof_n * nlev_all + 8 * k, sizeof(xp),
                     cudaMemcpyDeviceToHost));
-      for (int q = 0; q < 6; ++q) ctx->stats.level_xs[k][q] = (long long)xp[q];
+      for (int q = 0; q < 8; ++q) ctx->stats.level_xs[k][q] = (long long)xp[q];
     }
   }
   return MSGPU_OK;

@@ -333,7 +333,8 @@ __device__ __forceinline__ double xs_add_chunk(const XsSum& s, const XsGeom& g, 
 // The sequential sum 0 + t_0 + t_1 + ... of one sum, by one warp (every lane
 // returns it).  Needs the summaries of every chunk.
 __device__ double xs_drive(const XsSum& s, const XsGeom& g, unsigned long long* prof) {
-  unsigned long long slow = 0;
+  unsigned long long slow = 0, slow_cycles = 0;
+  const long long t_start = clock64();
   const int lane = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;   // lanes below this one
   const int nch = s.rows * g.nx;
@@ -378,6 +379,7 @@ __device__ double xs_drive(const XsSum& s, const XsGeom& g, unsigned long long* 
       int E;
       long long m;
       if (!xs_split(S, E, m)) {
+        const long long ts = clock64();
         if (j - jb == pf) {
           S = xs_add_terms(S, pt);
           pf = next_slow(pf + 1);
@@ -385,6 +387,7 @@ __device__ double xs_drive(const XsSum& s, const XsGeom& g, unsigned long long* 
         } else {
           S = xs_add_chunk(s, g, j, S);
         }
+        slow_cycles += (unsigned long long)(clock64() - ts);
         ++slow;
         ++j;
         continue;
@@ -429,6 +432,7 @@ __device__ double xs_drive(const XsSum& s, const XsGeom& g, unsigned long long* 
       if (j < jb + 32 && j < nch) {
         // chunk j interrupts the run (its sums leave the binade, or it has no
         // summary at this exponent): added term by term
+        const long long ts = clock64();
         if (first == pf) {
           S = xs_add_terms(S, pt);
           pf = next_slow(pf + 1);
@@ -440,6 +444,7 @@ __device__ double xs_drive(const XsSum& s, const XsGeom& g, unsigned long long* 
             if (pf >= 0) pt = xs_load_chunk(s, g, jb + pf);
           }
         }
+        slow_cycles += (unsigned long long)(clock64() - ts);
         ++slow;
         ++j;
       }
@@ -448,6 +453,8 @@ __device__ double xs_drive(const XsSum& s, const XsGeom& g, unsigned long long* 
   if (prof && (threadIdx.x & 31) == 0) {
     atomicAdd(prof + 4, (unsigned long long)nch);
     atomicAdd(prof + 5, slow);
+    atomicAdd(prof + 6, slow_cycles);
+    atomicAdd(prof + 7, (unsigned long long)(clock64() - t_start));
   }
   return S;
 }

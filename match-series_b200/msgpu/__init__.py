@@ -77,7 +77,7 @@ class Stats(ctypes.Structure):
                 ("level_ms", ctypes.c_float * 16), ("level_steps", ctypes.c_longlong * 16),
                 ("level_evals", ctypes.c_longlong * 16), ("level_cluster", ctypes.c_int * 16),
                 ("level_pass_cycles", (ctypes.c_longlong * 8) * 16), ("graph_replayed", ctypes.c_int),
-                ("level_xs", (ctypes.c_longlong * 6) * 16)]
+                ("level_xs", (ctypes.c_longlong * 8) * 16)]
 
 PASS_KINDS = ["energy0", "gradient", "vdown", "vcoarse", "vup", "ncg", "energy", "sync"]
 
@@ -714,7 +714,8 @@ class Context:
                 "level_pass_cycles": [dict(zip(PASS_KINDS, list(s.level_pass_cycles[i]))) for i in range(k)],
                 "graph_replayed": bool(s.graph_replayed),
                 "level_exact_sums": [dict(zip(["passes", "cycles_predict", "cycles_summaries", "cycles_walk",
-                                               "chunks", "chunks_term_by_term"], list(s.level_xs[i])))
+                                               "chunks", "chunks_term_by_term", "cycles_term_by_term",
+                                               "cycles_walk_warps"], list(s.level_xs[i])))
                                      for i in range(k)]}
 
     # --- single operators ------------------------------------------------
