@@ -99,6 +99,16 @@ int  msgpu_set_data_term(msgpu_context* ctx, int data_term);
 /* Order of the global sums (msgpu_params.sum_order) of the single-operator
  * entry points msgpu_energy and msgpu_gd_level of this context (default 0). */
 int  msgpu_set_sum_order(msgpu_context* ctx, int sum_order);
+/* Certified control steps with sum order 0 (default on).  A pass's sums in
+ * the reference's order differ from its parallel sums by at most
+ * 2 gamma_{N-1} sum |t| (N terms t); the level kernel takes each control
+ * decision (Armijo tests, stop rule, sigma schedule) on these bounds when
+ * they settle it, and adds the sums in order only where a decision stays
+ * open, where a value is written out (energies, logs) or enters arithmetic
+ * (the Fletcher-Reeves factor).  The results are those of the ordered sums
+ * either way; on costs six term buffers per instance (at most 16 GiB,
+ * beyond that one).  Off: every pass's sums are added in order.            */
+int  msgpu_set_certified_steps(msgpu_context* ctx, int on);
 int  msgpu_destroy(msgpu_context* ctx);
 const char* msgpu_last_error(const msgpu_context* ctx);
 
@@ -394,11 +404,12 @@ typedef struct {
   long long level_pass_cycles[16][8];
   int graph_replayed;           /* 1: the last device batch call replayed a
                                    captured CUDA graph (one launch)          */
-  /* exact sums (sum order 0) per level: completed passes that added sums,
-   * clock cycles of their three steps (binade predictions, chunk summaries,
-   * the ordered walk; summed over the passes), chunks walked, chunks added
-   * term by term, cycles of those term-by-term additions and cycles of the
-   * walk (both summed over the walking warps)                               */
+  /* exact sums (sum order 0) per level: term buffers whose sums were added
+   * in order, clock cycles of the binade predictions, control steps settled
+   * by bounded sums (certified steps), clock cycles of the ordered walks
+   * (summed over the buffers), chunks walked, chunks added term by term,
+   * cycles of those term-by-term additions and cycles of the walk (both
+   * summed over the walking warps)                                          */
   long long level_xs[16][8];
 } msgpu_stats;
 int msgpu_set_profiling(msgpu_context* ctx, int on);

@@ -44,6 +44,8 @@ struct msgpu_context {
   int data_term = 0;           // data term of the single-operator entry points
   int sum_order = 0;           // order of the global sums of the single-operator entry points
   Buf xsum;                    // exact sums: per-instance term blocks and chunk summaries
+  Buf xpart;                   // exact sums: per-tile bounds of the energy passes' sums
+  bool certified = true;       // exact sums: certified control steps (kXsBufs term buffers)
   // CUDA graph of the last device batch call (msgpu_register_batch_device):
   // captured on the second call with the same parameters and buffers, then
   // replayed as one launch while they stay the same
@@ -75,7 +77,7 @@ struct msgpu_context {
 
 namespace {
 
-constexpr int kAbiVersion = 6;
+constexpr int kAbiVersion = 7;
 // default chunking of the level scheduler: a 24th of a pass, at most 16 tiles
 constexpr int kChunkDiv = 24, kChunkMax = 16;
 
@@ -748,19 +750,37 @@ int launch_level(msgpu_context* ctx, LevelArgs<Real>& a, cudaStream_t st) {
   return MSGPU_OK;
 }
 
-// Exact sums of a level launch (FP64, SSD, sum order 0): per-instance
-// regions of XsLayout(n).stride doubles for num_inst instances; otherwise the
-// launch adds its sums in the fixed parallel order of the tile partials.
+// Exact sums of a level launch (FP64, SSD, sum order 0): per instance
+// xs_bufs term buffers of XsLayout(n).stride doubles and (xs_bufs > 1) the
+// per-tile bound sums of its energy passes.  kXsBufs buffers let a control
+// step be taken on bounded sums while the values that may still need their
+// ordered sums keep their terms (certified steps); one buffer (certified
+// steps off, or more memory than kXsCertBytes) adds every pass's sums in order
+// before its control step.  Otherwise the launch adds its sums in the fixed
+// parallel order of the tile partials.
+constexpr size_t kXsCertBytes = 16ull << 30;
 template <typename Real>
 int xs_attach(msgpu_context* ctx, LevelArgs<Real>& a, bool exact, int max_level, int num_inst) {
   a.xs = nullptr;
   a.xs_stride = 0;
+  a.xs_bufs = 1;
+  a.xpart = nullptr;
+  a.xpart_stride = 0;
   if (!exact || !std::is_same<Real, double>::value || a.ncc) return MSGPU_OK;
   int rc;
-  const size_t cap = XsLayout(lvl_n(max_level)).stride * (size_t)num_inst;
-  if ((rc = ensure(ctx, ctx->xsum, sizeof(double) * cap))) return rc;
+  const size_t stride = XsLayout(lvl_n(max_level)).stride;
+  const size_t xps = (size_t)level_max_tiles(max_level) * kXpSlots;
+  int nb = ctx->certified ? kXsBufs : 1;
+  if (nb > 1 && sizeof(double) * (stride * nb + xps) * (size_t)num_inst > kXsCertBytes) nb = 1;
+  if ((rc = ensure(ctx, ctx->xsum, sizeof(double) * stride * nb * (size_t)num_inst))) return rc;
+  if (nb > 1) {
+    if ((rc = ensure(ctx, ctx->xpart, sizeof(double) * xps * (size_t)num_inst))) return rc;
+    a.xpart = (double*)ctx->xpart.p;
+    a.xpart_stride = (size_t)level_max_tiles(a.level) * kXpSlots;
+  }
   a.xs = (double*)ctx->xsum.p;
   a.xs_stride = XsLayout(a.n).stride;
+  a.xs_bufs = nb;
   return MSGPU_OK;
 }
 
@@ -783,6 +803,7 @@ int sched_error_check(msgpu_context* ctx) {
   int h[3] = {0, 0, 0};
   if (!ctx->sched_error) return MSGPU_OK;
   CK(cudaMemcpy(h, ctx->sched_error, sizeof(h), cudaMemcpyDeviceToHost));
+  if (h[0] == 2) return fail(ctx, MSGPU_ERR_CUDA, "level kernel: exact-sum bookkeeping failed (no free term buffer)");
   if (h[0]) return fail(ctx, MSGPU_ERR_CUDA, "level kernel: a worker waited too long for work (scheduler stalled)");
   if (h[1]) return fail(ctx, MSGPU_ERR_CUDA, "composition: a grid-barrier wait timed out");
   if (h[2]) return fail(ctx, MSGPU_ERR_INVALID_ARG, "an input image holds a non-finite value (NaN or Inf)");
@@ -1750,6 +1771,13 @@ int msgpu_set_sum_order(msgpu_context* ctx, int sum_order) {
   return MSGPU_OK;
 }
 
+int msgpu_set_certified_steps(msgpu_context* ctx, int on) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  ctx->certified = on != 0;
+  ++ctx->alloc_epoch;   // a captured graph holds the old launch arguments
+  return MSGPU_OK;
+}
+
 int msgpu_set_data_term(msgpu_context* ctx, int data_term) {
   if (!ctx) return MSGPU_ERR_INVALID_ARG;
   if (data_term != 0 && data_term != 1)
@@ -1784,7 +1812,7 @@ int msgpu_destroy(msgpu_context* ctx) {
                                 &ctx->io[0], &ctx->io[1],   &ctx->io[2],    &ctx->io[3], &ctx->io[4],
                                 &ctx->io[5], &ctx->prof,    &ctx->sched,    &ctx->flags, &ctx->nccbuf,
                                 &ctx->ext,   &ctx->series,  &ctx->vals,  &ctx->xs_basis, &ctx->xs_work,
-                                &ctx->xsum};
+                                &ctx->xsum,  &ctx->xpart};
   if (ctx->graph.exec) cudaGraphExecDestroy(ctx->graph.exec);
   if (ctx->graph_stream) cudaStreamDestroy(ctx->graph_stream);
   for (auto* b : bufs)

@@ -34,6 +34,10 @@ namespace msg {
 constexpr int kThreads = 256;
 constexpr int kMaxLevel = 12;
 constexpr int kRedSlots = 4;   // partial sums reduced per pass
+// Certified control steps with exact sums: term buffers per instance, and per
+// tile of an energy pass the sums and the magnitude sums of its 5 term sets.
+constexpr int kXsBufs = 6;
+constexpr int kXpSlots = 10;
 
 // Node tiles: [x0, x0+TX) x [y0, y0+TY); the last tile of a row/column also
 // owns the final node (n-1 = 2^l is a multiple of the tile size for l >= 6).
@@ -111,6 +115,13 @@ struct LevelArgs {
   // order (msgpu_xsum.cuh); per-instance regions of xs_stride doubles, or null
   double* xs;
   size_t xs_stride;
+  // certified control steps: xs_bufs term buffers of xs_stride doubles per
+  // instance (<= 1: one, and every pass's sums are added in order before its
+  // control step); xpart (nullable): per instance xpart_stride doubles, per
+  // tile of an energy pass kXpSlots sums (the 5 sums, their magnitude sums)
+  int xs_bufs;
+  double* xpart;
+  size_t xpart_stride;
   // energy targets (nullable, per instance): the solve stops as soon as its
   // energy is <= e_target + e_tol |e_target| (registration to a stated
   // energy tolerance; no counterpart in the reference's stop rules)
@@ -271,14 +282,16 @@ struct EnergyPass {
   int nwin;
   double* part;
   Tiles tl;
-  double* xs;   // exact sums: the instance's region (Real = double), or null
+  double* xs;   // exact sums: the pass's term buffer (Real = double), or null
+  double* xp;   // certified control steps: the instance's per-tile sums, or null
 
   __device__ EnergyPass(const Inst<Real>& I_, int kind_, Real tau_, Real beta_, bool odz, const Real* phx_,
                         const Real* phy_, const Real* dx_, const Real* dy_, const Real* sx_, const Real* sy_,
                         const Real* dex_, const Real* dey_, Real* wdx_, Real* wdy_, Real* sm_, double* part_,
-                        double* xs_ = nullptr)
+                        double* xs_ = nullptr, double* xp_ = nullptr)
       : I(I_), kind(kind_), tau(tau_), beta(beta_), od_zero(odz), phx(phx_), phy(phy_), dx(dx_), dy(dy_),
-        sx(sx_), sy(sy_), dex(dex_), dey(dey_), wdx(wdx_), wdy(wdy_), sm(sm_), part(part_), tl(I_.n), xs(xs_) {
+        sx(sx_), sy(sy_), dex(dex_), dey(dey_), wdx(wdx_), wdy(wdy_), sm(sm_), part(part_), tl(I_.n), xs(xs_),
+        xp(xp_) {
     nwin = (kind == 0) ? 3 : (kind == 1 ? 5 : 7);
   }
   __device__ Real* win(int stage, int k) const { return sm + ((size_t)stage * nwin + k) * EWIN; }
@@ -312,11 +325,19 @@ struct EnergyPass {
   // position newPosition = phi + tau d (gradientDescent.h:176-178) is formed
   // on the whole window first, and E_reg = 1/2 (p_x . L p_x + p_y . L p_y)
   // is evaluated there as DisplacementLengthEnergy does (hyperelastic.h:
-  // 178-183), not by the quadratic expansion of the fast path.
+  // 178-183), not by the quadratic expansion of the fast path.  With xp the
+  // tile also stores, per term set, the sum of its terms and of their
+  // magnitudes (any order: they only bound the ordered sums).
   __device__ void compute_exact(int t, int stage) {
     int x0, x1, y0, y1;
     tl.rect(t, x0, x1, y0, y1);
     const int n = I.n;
+    __shared__ double xpw[kThreads / 32][kXpSlots];   // per warp: its rows' sums
+    const int wid = threadIdx.x >> 5;
+    if (xp && (threadIdx.x & 31) == 0) {
+#pragma unroll
+      for (int k = 0; k < kXpSlots; ++k) xpw[wid][k] = 0.0;
+    }
     Real* Wpx = win(stage, 0);
     Real* Wpy = win(stage, 1);
     const Real* Wr = win(stage, nwin - 1);
@@ -353,7 +374,7 @@ struct EnergyPass {
       const int ex1 = (x1 < n - 1) ? x1 : n - 1, ey1 = (y1 < n - 1) ? y1 : n - 1;
       const int ew = ex1 - x0, eh = ey1 - y0;
       for (int iy = ly; iy < eh; iy += kThreads / 64) {
-        double acc = 0.0;
+        double acc = 0.0, mag = 0.0;
         for (int ix = lx; ix < ew; ix += 64) {
           const int ex = x0 + ix, ey = y0 + iy;
           const int c0 = at(ex, ey);
@@ -368,9 +389,17 @@ struct EnergyPass {
           const double v = (double)element_ssd(I.T, n, I.P, I.h, ex, ey, px, py, r);
           B0[xs_at(ix, iy)] = v;
           acc += v;
+          mag += fabs(v);
         }
         acc = warp_sum(acc);
         if (lane == 0) s0.tot[((y0 + iy) * g.nx + tx) * 2 + half] = acc;
+        if (xp) {
+          mag = warp_sum(mag);
+          if (lane == 0) {
+            xpw[wid][0] += acc;
+            xpw[wid][5] += mag;
+          }
+        }
       }
     }
     // owned nodes: p . L p per component; NCG also DE . d and the direction
@@ -384,6 +413,7 @@ struct EnergyPass {
       const int nw = x1 - x0, nh = y1 - y0;
       for (int iy = ly; iy < nh; iy += kThreads / 64) {
         double a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0;
+        double m1 = 0.0, m2 = 0.0, m3 = 0.0, m4 = 0.0;
         for (int ix = lx; ix < nw; ix += 64) {
           const int x = x0 + ix, y = y0 + iy;
           const int c = at(x, y);
@@ -394,6 +424,8 @@ struct EnergyPass {
           B2[xs_at(ix, iy)] = t2;
           a1 += t1;
           a2 += t2;
+          m1 += fabs(t1);
+          m2 += fabs(t2);
           if (kind == 2) {
             const Real ddx = Wa[c], ddy = Wb[c];
             const size_t gg = (size_t)y * I.P + x;
@@ -404,6 +436,8 @@ struct EnergyPass {
             B4[xs_at(ix, iy)] = t4;
             a3 += t3;
             a4 += t4;
+            m3 += fabs(t3);
+            m4 += fabs(t4);
           }
         }
         a1 = warp_sum(a1);
@@ -421,6 +455,35 @@ struct EnergyPass {
             s4.tot[j2] = a4;
           }
         }
+        if (xp) {
+          m1 = warp_sum(m1);
+          m2 = warp_sum(m2);
+          if (kind == 2) {
+            m3 = warp_sum(m3);
+            m4 = warp_sum(m4);
+          }
+          if (lane == 0) {
+            xpw[wid][1] += a1;
+            xpw[wid][2] += a2;
+            xpw[wid][6] += m1;
+            xpw[wid][7] += m2;
+            if (kind == 2) {
+              xpw[wid][3] += a3;
+              xpw[wid][4] += a4;
+              xpw[wid][8] += m3;
+              xpw[wid][9] += m4;
+            }
+          }
+        }
+      }
+    }
+    if (xp) {
+      __syncthreads();
+      if (threadIdx.x < kXpSlots) {
+        double v = 0.0;
+#pragma unroll
+        for (int w = 0; w < kThreads / 32; ++w) v += xpw[w][threadIdx.x];
+        __stcg(xp + (size_t)t * kXpSlots + threadIdx.x, v);
       }
     }
   }
@@ -1298,6 +1361,72 @@ __host__ __device__ inline size_t level_smem_elems(int lc) {
 __device__ __forceinline__ bool finite_d(double x) { return !isnan(x) && !isinf(x); }
 
 // ---------------------------------------------------------------------------
+// Bounded values.  With exact sums a pass's sum in the reference's sequential
+// order Q differs from any other order's sum P of the same N terms by at most
+// 2 gamma_{N-1} sum |t| (both lie within gamma_{N-1} sum |t| of the real sum;
+// recursive summation bound, Higham, Accuracy and Stability of Numerical
+// Algorithms, 2nd ed., eq. 4.4), so Q is known to lie in an interval before
+// the ordered sum is formed.  Rounding to nearest is monotone, so an
+// expression of additions, subtractions, scalings and divisions (denominator
+// of fixed sign) evaluated on the ends of its operands' intervals bounds its
+// value on the exact operands; a comparison that the bounds settle is the
+// comparison of the exact values.  ex: the value is known exactly (lo = hi).
+struct Iv {
+  double lo, hi;
+  int ex;
+};
+__device__ __forceinline__ Iv ivx(double x) { return Iv{x, x, 1}; }
+__device__ __forceinline__ Iv iv_unknown() {
+  const double q = __longlong_as_double(0x7ff8000000000000ll);
+  return Iv{q, q, 0};
+}
+__device__ __forceinline__ Iv iv_add(Iv a, Iv b) {
+  if (a.ex && b.ex) return ivx(a.lo + b.lo);
+  return Iv{a.lo + b.lo, a.hi + b.hi, 0};
+}
+__device__ __forceinline__ Iv iv_sub(Iv a, Iv b) {
+  if (a.ex && b.ex) return ivx(a.lo - b.lo);
+  return Iv{a.lo - b.hi, a.hi - b.lo, 0};
+}
+__device__ __forceinline__ Iv iv_scale(Iv a, double s) {
+  if (a.ex) return ivx(a.lo * s);
+  return s >= 0.0 ? Iv{a.lo * s, a.hi * s, 0} : Iv{a.hi * s, a.lo * s, 0};
+}
+__device__ __forceinline__ Iv iv_div(Iv a, Iv b) {
+  if (a.ex && b.ex) return ivx(a.lo / b.lo);
+  if (!(b.lo > 0.0 || b.hi < 0.0)) return iv_unknown();
+  const double c1 = a.lo / b.lo, c2 = a.lo / b.hi, c3 = a.hi / b.lo, c4 = a.hi / b.hi;
+  if (isnan(c1) || isnan(c2) || isnan(c3) || isnan(c4)) return iv_unknown();
+  return Iv{fmin(fmin(c1, c2), fmin(c3, c4)), fmax(fmax(c1, c2), fmax(c3, c4)), 0};
+}
+// E_reg = 1/2 (0 + s1 + s2) and Df = 0 + s3 + s4 from a pass's sums
+__device__ __forceinline__ Iv xs_ereg(Iv s1, Iv s2) { return iv_scale(iv_add(iv_add(ivx(0.0), s1), s2), 0.5); }
+__device__ __forceinline__ Iv xs_df(Iv s3, Iv s4) { return iv_add(iv_add(ivx(0.0), s3), s4); }
+// E = (0 + E_data) + lambda E_reg, as the energy passes' totals combine
+__device__ __forceinline__ Iv xs_energy(Iv edata, Iv ereg, double lam) {
+  Iv e = ivx(0.0);
+  e = iv_add(e, edata);
+  if (lam != 1.0) e = iv_add(e, iv_scale(ereg, lam)); else e = iv_add(e, ereg);
+  return e;
+}
+
+// A value of the descent state; while it is not exact it was evaluated from
+// the bounded sums of term buffer buf (which then stays untouched) by kind.
+enum XvKind : int { XK_NONE = 0, XK_ENERGY, XK_EREG, XK_DF };
+struct XV {
+  Iv v;
+  int buf, kind;
+};
+__device__ __forceinline__ XV xv_exact(double x) { return XV{ivx(x), -1, XK_NONE}; }
+
+// Sums of a term buffer's pass: state 0 being written, 1 bounded (or not
+// known: NaN bounds), 2 exact; ns sums.
+struct XsBufState {
+  double lo[5], hi[5];
+  int state, ns;
+};
+
+// ---------------------------------------------------------------------------
 // Persistent task scheduler of the level kernel.
 //
 // A level solve of one instance is a chain of passes (initial energy,
@@ -1346,7 +1475,9 @@ struct PassDesc {
   int kind, k, cur, dcur, dn, flags;
   int ntiles, chunk;   // tiles of the pass, tiles per dispensed chunk
   int purpose;   // NCC energy subs, TK_XSUM: the pass they stand for (TK_E0, TK_GRAD, TK_TRIAL, TK_NCG, ...)
-  int xn;        // TK_XSUM: exact sums of that pass
+  int xn;        // TK_XSUM: exact sums of the buffer it adds
+  int xbuf;      // exact sums: the pass's term buffer (TK_XSUM: of the pass it stands for)
+  int xres;      // TK_XSUM: the term buffer whose sums it adds
   double t;      // trial step (NCG, TRIAL) or pending step (GRAD, FLUSH)
   double beta;   // Fletcher-Reeves factor (NCG)
   double vtau;   // tau of the V-cycle passes
@@ -1359,12 +1490,15 @@ struct InstCtl {
   int done;            // tiles of the current pass completed
   int ls;              // TRIAL role: 0 doubling, 1 halving, 2 energy at the accepted step
   int iter, evals, total_evals, attempt, rb_pos, pending, od_zero, cur, dcur;
-  double energy, energy_new, f, sigma, sigma_used, tau, og2, A, Bd, Cd, Df, t, beta, tau_p;
-  double last_ereg;    // E_reg of the last energy evaluation
-  double ereg_pos;     // E_reg at the current position (the energy log)
-  double rb_r[2];      // E_reg of the ring buffer's evaluations
-  double rb_tau[2], rb_e[2];
+  double sigma, sigma_used, tau, og2, A, Bd, Cd, t, beta, tau_p;
+  XV energy, energy_new, f, Df;
+  XV last_ereg;        // E_reg of the last energy evaluation
+  XV ereg_pos;         // E_reg at the current position (the energy log)
+  XV rb_r[2];          // E_reg of the ring buffer's evaluations
+  XV rb_e[2];
+  double rb_tau[2];
   double n1[kRedSlots];      // NCC: totals of energy sub 1 (mean, then A or Df B C)
+  XsBufState bs[kXsBufs];    // exact sums: the term buffers' sums
 };
 constexpr int kCtlWords = (int)((sizeof(InstCtl) + 7) / 8);
 constexpr int kWordStride = 16;  // dispenser words 128 bytes apart
@@ -1401,8 +1535,13 @@ __device__ __forceinline__ Inst<Real> make_inst(const LevelArgs<Real>& a, int in
 // The exact sums of a pass of kind `kind` for instance inst: slot 0 is the
 // element sum E_data for the energy passes, every other slot a node sum.
 template <typename Real>
-__device__ __forceinline__ void xs_pass_sums(const LevelArgs<Real>& a, int inst, int kind, int ns, XsSum* out) {
-  double* base = a.xs + (size_t)inst * a.xs_stride;
+__device__ __forceinline__ double* xs_buffer(const LevelArgs<Real>& a, int inst, int buf) {
+  return a.xs + ((size_t)inst * (a.xs_bufs > 1 ? a.xs_bufs : 1) + buf) * a.xs_stride;
+}
+template <typename Real>
+__device__ __forceinline__ void xs_pass_sums(const LevelArgs<Real>& a, int inst, int kind, int ns, int buf,
+                                             XsSum* out) {
+  double* base = xs_buffer(a, inst, buf);
   const bool energy = (kind == TK_E0 || kind == TK_TRIAL || kind == TK_NCG);
   for (int k = 0; k < ns; ++k) out[k] = xs_sum(base, a.n, k, energy && k == 0);
 }
@@ -1454,18 +1593,19 @@ struct TaskRunner {
     Real* phi = I.arr(a.off_phi[d.cur]);
     Real* de = I.arr(a.off_de);
     Real* s = I.arr(a.off_s);
-    double* xs = a.xs ? a.xs + (size_t)inst * a.xs_stride : nullptr;
+    double* xs = a.xs ? xs_buffer(a, inst, d.xbuf) : nullptr;
+    double* xp = a.xpart ? a.xpart + (size_t)inst * a.xpart_stride : nullptr;
     switch (d.kind) {
       case TK_E0: {
         EnergyPass<Real> ps(I, 0, Real(0), Real(0), false, phi, phi + cs, nullptr, nullptr, nullptr, nullptr, nullptr,
-                            nullptr, nullptr, nullptr, smem, part, xs);
+                            nullptr, nullptr, nullptr, smem, part, xs, xp);
         f(ps);
         break;
       }
       case TK_TRIAL: {
         const Real* dd = I.arr(a.off_d[d.dcur]);
         EnergyPass<Real> ps(I, 1, (Real)d.t, Real(0), false, phi, phi + cs, dd, dd + cs, nullptr, nullptr, nullptr,
-                            nullptr, nullptr, nullptr, smem, part, xs);
+                            nullptr, nullptr, nullptr, smem, part, xs, xp);
         f(ps);
         break;
       }
@@ -1473,7 +1613,7 @@ struct TaskRunner {
         const Real* od = I.arr(a.off_d[d.dcur]);
         Real* wd = I.arr(a.off_d[d.dn]);
         EnergyPass<Real> ps(I, 2, (Real)d.t, (Real)d.beta, (d.flags & PF_ODZERO) != 0, phi, phi + cs, od, od + cs, s,
-                            s + cs, de, de + cs, wd, wd + cs, smem, part, xs);
+                            s + cs, de, de + cs, wd, wd + cs, smem, part, xs, xp);
         f(ps);
         break;
       }
@@ -1557,7 +1697,7 @@ struct TaskRunner {
       const int k = b / ntiles;
       if (k >= d.xn) return;
       const bool energy = (d.purpose == TK_E0 || d.purpose == TK_TRIAL || d.purpose == TK_NCG);
-      const XsSum s = xs_sum(a.xs + (size_t)inst * a.xs_stride, a.n, k, energy && k == 0);
+      const XsSum s = xs_sum(xs_buffer(a, inst, d.xres), a.n, k, energy && k == 0);
       xs_summary_row(s, g, b - k * ntiles, r);
       return;
     }
@@ -1571,7 +1711,7 @@ struct TaskRunner {
       const Real* by = (L == lc) ? de + cs : bx + comp_stride(lc);
       Real* out = (L == lc) ? s : I.arr(a.off_x5[lc]);
       Real* outy = (L == lc) ? s + cs : out + comp_stride(lc);
-      double* xs = (a.xs && L == lc && a.mode != MODE_SMOOTH) ? a.xs + (size_t)inst * a.xs_stride : nullptr;
+      double* xs = (a.xs && L == lc && a.mode != MODE_SMOOTH) ? xs_buffer(a, inst, d.xbuf) : nullptr;
       coarse_vcycle<Real>(lc, d.vtau, smem, bx, by, (L == lc) ? Real(-1) : Real(1), out, outy, L == lc, part, xs);
       return;
     }
@@ -1621,40 +1761,84 @@ __device__ __forceinline__ void block_sum(const double part[kRedSlots], double (
 }
 
 // Descent control of one instance after a completed pass (run by one thread
-// on a private copy of the state).  tot[] are the pass's totals.  Fills c.desc
-// with the next pass; kind TK_DONE when the level solve is finished.
+// on a private copy of the state).  tot[] are the pass's totals; with exact
+// sums xr[] are the pass's sums in the reference's order, each known exactly
+// or (certified step) only within rigorous bounds.  Fills c.desc with the
+// next pass; kind TK_DONE when the level solve is finished.  Returns false
+// when a bounded value left a decision open (or a result to be written, or
+// an operand of arithmetic, is not exact yet): the caller then discards c
+// and has the sums added in order first.
 // Follows GradientDescentBase::applySingle with the automatic filter width
 // (gradientDescent.h:295-464, 675-691), Fletcher-Reeves NCG
 // (gradientDescent.h:200-236) and ArmijoLineSearchUsingOp
 // (ArmijoSearch.h:118-200).
 template <typename Real>
-__device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const double* tot, const double* xr) {
+__device__ bool advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const double* tot, const Iv* xr) {
   const double lam = a.lambda_inst ? a.lambda_inst[inst] : a.lambda;
   const double tau_min = 9.313225746154785e-10;  // 2^-30 (ArmijoSearch.h:77)
   const double tau_max = 33554432.0;             // 2^25  (ArmijoSearch.h:67)
   const double stop_sigma = 0.0001, sigma_tol = 0.00001;
   const int L = a.level, lc = a.lc;
   PassDesc& d = c.desc;
-  auto energy_of = [&](double edata, double ereg) {
-    double e = 0.0;
-    e += edata;
-    if (lam != 1.0) e += lam * ereg; else e += ereg;
-    return e;
+  const int xb = d.xbuf;   // term buffer of the completed pass
+  bool open = false;       // a decision the bounds do not settle
+  // comparisons: exact operands compare as doubles; bounded ones decide
+  // when the intervals do, else the step stays open
+  auto ge = [&](Iv x, Iv y) {
+    if (x.ex && y.ex) return x.lo >= y.lo;
+    if (x.lo >= y.hi) return true;
+    if (x.hi < y.lo) return false;
+    open = true;
+    return false;
   };
+  auto lt = [&](Iv x, Iv y) {
+    if (x.ex && y.ex) return x.lo < y.lo;
+    if (x.hi < y.lo) return true;
+    if (x.lo >= y.hi) return false;
+    open = true;
+    return false;
+  };
+  auto gt = [&](Iv x, Iv y) {
+    if (x.ex && y.ex) return x.lo > y.lo;
+    if (x.lo > y.hi) return true;
+    if (x.hi <= y.lo) return false;
+    open = true;
+    return false;
+  };
+  auto le = [&](Iv x, Iv y) {
+    if (x.ex && y.ex) return x.lo <= y.lo;
+    if (x.hi <= y.lo) return true;
+    if (x.lo > y.hi) return false;
+    open = true;
+    return false;
+  };
+  auto finite = [&](Iv x) {
+    if (x.ex) return finite_d(x.lo);
+    if (finite_d(x.lo) && finite_d(x.hi)) return true;
+    open = true;
+    return true;
+  };
+  auto is_nan = [&](Iv x) {
+    if (x.ex) return (bool)isnan(x.lo);
+    if (isnan(x.lo) || isnan(x.hi)) open = true;
+    return false;
+  };
+  auto need = [&](Iv x) {   // a value written out or used in arithmetic
+    if (!x.ex) open = true;
+    return (bool)x.ex;
+  };
+  // a value of the state evaluated from this pass's sums
+  auto val = [&](Iv v, int kind) { return XV{v, (xr && !v.ex) ? xb : -1, kind}; };
+  auto energy_of = [&](Iv edata, Iv ereg) { return xs_energy(edata, ereg, lam); };
   auto quad = [&](double tt) { return 0.5 * ((c.A + 2.0 * tt * c.Bd) + tt * tt * c.Cd); };
-  auto target_met = [&](double en) {
+  auto target_met = [&](Iv en) {
     if (!a.e_target) return false;
     const double tg = a.e_target[inst];
-    return en <= tg + a.e_tol * fabs(tg);
+    return le(en, ivx(tg + a.e_tol * fabs(tg)));
   };
   // exact sums (xr): E_reg = 1/2 (0 + p_x . L p_x + p_y . L p_y), the order of
   // DisplacementLengthEnergy::apply (hyperelastic.h:178-183)
-  auto ereg_exact = [&]() {
-    double dd = 0.0;
-    dd += xr[1];
-    dd += xr[2];
-    return 0.5 * dd;
-  };
+  auto ereg_exact = [&]() { return xs_ereg(xr[1], xr[2]); };
   // the next pass is an energy-type pass: with the NCC data term it starts
   // with energy sub 1 and remembers what it stands for
   auto to = [&](int kind) {
@@ -1713,7 +1897,7 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
     d.dcur = c.dcur;
     d.t = t;
   };
-  auto push_ring = [&](double t, double e) {
+  auto push_ring = [&](double t, XV e) {
     c.rb_tau[c.rb_pos] = t;
     c.rb_e[c.rb_pos] = e;
     c.rb_r[c.rb_pos] = c.last_ereg;
@@ -1723,15 +1907,16 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
   // the reference's energy log holds lambda * E_reg at the new position
   // (with a log file it evaluates the energy there again, gradientDescent.h:
   // 364-369, and writes the last evaluation's components)
-  auto log_row = [&](int row, double en) {
+  auto log_row = [&](int row, Iv en) {
     if (a.elog && row <= a.max_trace) {
+      if (!need(en) || !need(c.ereg_pos.v)) return;
       double* lg = a.elog + ((size_t)inst * (a.max_trace + 1) + row) * 3;
       lg[0] = (double)(row - 1);
-      lg[1] = lam * c.ereg_pos;
-      lg[2] = en;
+      lg[1] = lam * c.ereg_pos.v.lo;
+      lg[2] = en.lo;
     }
   };
-  auto end_iteration = [&](double en, double er) {
+  auto end_iteration = [&](XV en, XV er) {
     c.ereg_pos = er;
     if (c.tau != 0) {
       c.pending = 1;
@@ -1739,31 +1924,33 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
     }
     c.energy_new = en;
     c.total_evals += c.evals;
-    log_row(c.iter, en);
-    if (a.trace && c.iter <= a.max_trace) {
+    log_row(c.iter, en.v);
+    if (a.trace && c.iter <= a.max_trace && need(c.energy_new.v)) {
       double* tr = a.trace + ((size_t)inst * a.max_trace + (c.iter - 1)) * 4;
-      tr[0] = c.energy_new;
+      tr[0] = c.energy_new.v.lo;
       tr[1] = c.tau;
       tr[2] = c.sigma_used;
       tr[3] = c.evals;
     }
-    bool go = ((c.energy - c.energy_new) > a.stop_eps) && (c.iter < a.max_iter);
-    if ((0.5 * c.sigma > stop_sigma) && ((c.energy - c.energy_new) < sigma_tol)) {
+    const Iv dec = iv_sub(c.energy.v, c.energy_new.v);
+    bool go = (c.iter < a.max_iter) && gt(dec, ivx(a.stop_eps));
+    if ((0.5 * c.sigma > stop_sigma) && lt(dec, ivx(sigma_tol))) {
       c.sigma *= 0.5;
       c.tau = 1.;
       go = (c.sigma > stop_sigma) && (c.iter < a.max_iter);
     }
-    if (target_met(c.energy_new)) go = false;
+    if (target_met(c.energy_new.v)) go = false;
     if (go) start_iteration(); else finish();
   };
   auto step_done = [&](double acc_tau) {
     c.tau = acc_tau;
     // energy at the new position (gradientDescent.h:365-395)
-    double en = nan(""), er = c.ereg_pos;
-    if (c.rb_tau[0] == c.tau) en = c.rb_e[0], er = c.rb_r[0];
-    else if (c.rb_tau[1] == c.tau) en = c.rb_e[1], er = c.rb_r[1];
-    else if (c.tau == 0) en = c.energy;
-    if (isnan(en) && c.tau != 0) {
+    XV en = c.energy, er = c.ereg_pos;
+    bool found = false;
+    if (c.rb_tau[0] == c.tau) { en = c.rb_e[0]; er = c.rb_r[0]; found = true; }
+    else if (c.rb_tau[1] == c.tau) { en = c.rb_e[1]; er = c.rb_r[1]; found = true; }
+    else if (c.tau == 0) { en = c.energy; found = true; }
+    if ((!found || is_nan(en.v)) && c.tau != 0) {
       trial(c.tau, 2);
       return;
     }
@@ -1788,16 +1975,16 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
       for (int k = 0; k < kRedSlots; ++k) c.n1[k] = tot[k];
       d.mean = tot[0];
       d.kind = TK_N2;
-      return;
+      return true;
     case TK_N2:
       d.var = sqrt(tot[0]);
       d.kind = TK_N3;
-      return;
+      return true;
     case TK_N3:
       d.e = -(tot[0]);
       if (d.purpose == TK_GRAD) {
         d.kind = TK_NF;
-        return;
+        return true;
       }
       nt[0] = d.e;
 #pragma unroll
@@ -1814,18 +2001,18 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
   switch (d.kind) {
     case TK_E0: {
       c.A = tot[1];
-      c.last_ereg = xr ? ereg_exact() : 0.5 * c.A;
-      c.energy = energy_of(xr ? xr[0] : tot[0], c.last_ereg);
+      c.last_ereg = xr ? val(ereg_exact(), XK_EREG) : val(ivx(0.5 * c.A), XK_EREG);
+      c.energy = val(energy_of(xr ? xr[0] : ivx(tot[0]), c.last_ereg.v), XK_ENERGY);
       c.energy_new = c.energy;
       c.ereg_pos = c.last_ereg;
-      log_row(0, c.energy);
+      log_row(0, c.energy.v);
       if (a.mode == MODE_ENERGY) {
         to(TK_GRAD);
         d.cur = c.cur;
         d.dcur = c.dcur;
         d.flags = 0;
         d.t = 0;
-      } else if (a.max_iter > 0 && !target_met(c.energy)) {
+      } else if (a.max_iter > 0 && !target_met(c.energy.v)) {
         start_iteration();
       } else {
         d.kind = TK_DONE;
@@ -1861,9 +2048,10 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
       }
       double s2 = tot[0];
       if (xr) {   // 0 + s_x . s_x + s_y . s_y in the reference's order
+        if (!need(xr[0]) || !need(xr[1])) return false;
         s2 = 0.0;
-        s2 += xr[0];
-        s2 += xr[1];
+        s2 += xr[0].lo;
+        s2 += xr[1].lo;
       }
       c.beta = ((c.iter - 1) % 10) ? (s2 / c.og2) : 0.0;
       c.og2 = s2;
@@ -1873,22 +2061,19 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
     }
     case TK_NCG: {
       c.dcur = d.dn;
-      c.Df = tot[1];
+      c.Df = val(ivx(tot[1]), XK_DF);
       c.Bd = tot[2];
       c.Cd = tot[3];
-      if (xr) {   // 0 + DE_x . d_x + DE_y . d_y (ArmijoSearch.h:129-131)
-        c.Df = 0.0;
-        c.Df += xr[3];
-        c.Df += xr[4];
-      }
-      const double t = c.t, f = c.f;
-      c.last_ereg = xr ? ereg_exact() : quad(t);
-      const double fnew = energy_of(xr ? xr[0] : tot[0], c.last_ereg);
-      push_ring(t, fnew);
-      const double G = (fnew - f) / (c.Df * t);
-      if (c.Df >= 0 || !finite_d(f)) {
+      if (xr) c.Df = val(xs_df(xr[3], xr[4]), XK_DF);   // 0 + DE_x . d_x + DE_y . d_y (ArmijoSearch.h:129-131)
+      const double t = c.t;
+      const Iv f = c.f.v, Df = c.Df.v;
+      c.last_ereg = xr ? val(ereg_exact(), XK_EREG) : val(ivx(quad(t)), XK_EREG);
+      const Iv fnew = energy_of(xr ? xr[0] : ivx(tot[0]), c.last_ereg.v);
+      push_ring(t, val(fnew, XK_ENERGY));
+      const Iv G = iv_div(iv_sub(fnew, f), iv_scale(Df, t));
+      if (ge(Df, ivx(0.0)) || !finite(f)) {
         attempt_done(0.0);
-      } else if (G >= 0.5 && f >= fnew) {
+      } else if (ge(G, ivx(0.5)) && ge(f, fnew)) {
         trial(t * 2., 0);
       } else {
         trial((t > tau_min) ? t * 0.5 : t, 1);
@@ -1896,24 +2081,26 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
       break;
     }
     case TK_TRIAL: {
-      const double t = c.t, f = c.f;
-      c.last_ereg = xr ? ereg_exact() : quad(t);
-      const double fnew = energy_of(xr ? xr[0] : tot[0], c.last_ereg);
-      push_ring(t, fnew);
+      const double t = c.t;
+      const Iv f = c.f.v;
+      c.last_ereg = xr ? val(ereg_exact(), XK_EREG) : val(ivx(quad(t)), XK_EREG);
+      const Iv fnew = energy_of(xr ? xr[0] : ivx(tot[0]), c.last_ereg.v);
+      const XV fv = val(fnew, XK_ENERGY);
+      push_ring(t, fv);
       if (c.ls == 2) {
-        end_iteration(fnew, c.last_ereg);
+        end_iteration(fv, c.last_ereg);
         break;
       }
-      const double G = (fnew - f) / (c.Df * t);
+      const Iv G = iv_div(iv_sub(fnew, f), iv_scale(c.Df.v, t));
       if (c.ls == 0) {
-        if (G >= 0.5 && f >= fnew && t <= tau_max) {
+        if (ge(G, ivx(0.5)) && ge(f, fnew) && t <= tau_max) {
           trial(t * 2., 0);
         } else {
           const double tt = t * 0.5;
           attempt_done((tt > tau_min) ? tt : 0.0);
         }
       } else {
-        if ((!finite_d(fnew) || (G < 0.5 || f < fnew)) && (t > tau_min)) {
+        if ((!finite(fnew) || (lt(G, ivx(0.5)) || lt(f, fnew))) && (t > tau_min)) {
           trial((t > tau_min) ? t * 0.5 : t, 1);
         } else {
           attempt_done((t > tau_min) ? t : 0.0);
@@ -1929,6 +2116,12 @@ __device__ void advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
     }
     default: d.kind = TK_DONE; break;
   }
+  // the energy the solve reports is written out when it ends (after a flush
+  // of the pending step, or after the gradient in energy mode)
+  if ((d.kind == TK_DONE || d.kind == TK_FLUSH || (a.mode == MODE_ENERGY && d.kind == TK_GRAD)) &&
+      a.mode != MODE_SMOOTH)
+    need(c.energy_new.v);
+  return !open;
 }
 
 __device__ __forceinline__ void init_ctl_state(InstCtl& c, int cur) {
@@ -1940,6 +2133,9 @@ __device__ __forceinline__ void init_ctl_state(InstCtl& c, int cur) {
   c.og2 = 0.0;
   c.od_zero = 1;
   c.rb_tau[0] = c.rb_tau[1] = nan("");
+  c.energy = c.energy_new = c.f = c.Df = xv_exact(0.0);
+  c.last_ereg = c.ereg_pos = xv_exact(0.0);
+  c.rb_r[0] = c.rb_r[1] = c.rb_e[0] = c.rb_e[1] = xv_exact(0.0);
 }
 
 __device__ __forceinline__ void ctl_load(InstCtl& dst, const InstCtl* src) {
@@ -1953,6 +2149,143 @@ __device__ __forceinline__ void ctl_store(InstCtl* dst, const InstCtl& src) {
   for (int i = 0; i < kCtlWords; ++i) __stcg(d + i, s[i]);
 }
 
+// Exact sums a completed pass leaves to add (0: none): the energy passes
+// E_data and p . L p per component, the NCG pass also DE . d per component,
+// the top of the V-cycle |s|^2 per component.
+template <typename Real>
+__device__ __forceinline__ int xs_count(const LevelArgs<Real>& a, const PassDesc& d) {
+  if (a.mode == MODE_SMOOTH) return 0;
+  switch (d.kind) {
+    case TK_E0:
+    case TK_TRIAL: return 3;
+    case TK_NCG: return 5;
+    case TK_VUP: return d.k == a.level ? 2 : 0;
+    case TK_COARSE: return a.level == a.lc ? 2 : 0;
+    default: return 0;
+  }
+}
+
+__device__ __forceinline__ bool is_energy_kind(int kind) {
+  return kind == TK_E0 || kind == TK_TRIAL || kind == TK_NCG;
+}
+
+// Bounds of the ordered sum Q of at most N terms from another order's sum P
+// and the sum A of the terms' magnitudes, both rounded themselves:
+// |Q - P| <= 2 gamma_{N-1} A_true and A_true <= A / (1 - gamma_{N-1}); the
+// factor 3 N u (u = 2^-53) and the term 2^-50 |P| also cover the rounding of
+// the bounds.  Non-finite or huge inputs give no bounds (NaN).
+__device__ __forceinline__ void xs_bounds(double P, double A, double N, double& lo, double& hi) {
+  if (!(A < 1e300) || !(fabs(P) < 1e300)) {
+    lo = hi = __longlong_as_double(0x7ff8000000000000ll);
+    return;
+  }
+  const double B = A * (3.0 * N * 1.1102230246251565e-16) + fabs(P) * 8.881784197001252e-16;
+  lo = P - B;
+  hi = P + B;
+}
+
+// Term buffers the state holds: those of its values that are not exact yet.
+__device__ __forceinline__ unsigned xs_held(const InstCtl& c) {
+  unsigned m = 0;
+  auto hold = [&](const XV& x) {
+    if (!x.v.ex && x.buf >= 0) m |= 1u << x.buf;
+  };
+  hold(c.energy);
+  hold(c.energy_new);
+  hold(c.f);
+  hold(c.Df);
+  hold(c.last_ereg);
+  hold(c.ereg_pos);
+  hold(c.rb_r[0]);
+  hold(c.rb_r[1]);
+  hold(c.rb_e[0]);
+  hold(c.rb_e[1]);
+  return m;
+}
+
+// Buffer b's sums added in order (out[]): they are exact from now on, and so
+// are the values evaluated from them (the control step's expressions again,
+// on the exact sums); a summary pass's pending control step is taken again.
+template <typename Real>
+__device__ void xs_settle(const LevelArgs<Real>& a, int inst, InstCtl& c, int b, const double* out) {
+  XsBufState& B = c.bs[b];
+  for (int k = 0; k < B.ns; ++k) B.lo[k] = B.hi[k] = out[k];
+  B.state = 2;
+  const double lam = a.lambda_inst ? a.lambda_inst[inst] : a.lambda;
+  Iv sv[5];
+  for (int k = 0; k < 5; ++k) sv[k] = ivx(k < B.ns ? B.lo[k] : 0.0);
+  auto upd = [&](XV& x) {
+    if (x.v.ex || x.buf != b) return;
+    if (x.kind == XK_EREG) x.v = xs_ereg(sv[1], sv[2]);
+    else if (x.kind == XK_DF) x.v = xs_df(sv[3], sv[4]);
+    else if (x.kind == XK_ENERGY) x.v = xs_energy(sv[0], xs_ereg(sv[1], sv[2]), lam);
+    x.buf = -1;
+  };
+  upd(c.energy);
+  upd(c.energy_new);
+  upd(c.f);
+  upd(c.Df);
+  upd(c.last_ereg);
+  upd(c.ereg_pos);
+  upd(c.rb_r[0]);
+  upd(c.rb_r[1]);
+  upd(c.rb_e[0]);
+  upd(c.rb_e[1]);
+  if (c.desc.kind == TK_XSUM) c.desc.kind = c.desc.purpose;
+}
+
+// The buffer whose ordered sums an open control step needs next: the
+// completed pass's own, then those of the state's bounded values.
+__device__ __forceinline__ int xs_next_resolve(const InstCtl& c) {
+  const int xb = c.desc.xbuf;
+  if (xb >= 0 && c.bs[xb].state != 2) return xb;
+  const XV* order[10] = {&c.energy_new, &c.energy,    &c.f,       &c.Df,      &c.rb_e[0],
+                         &c.rb_e[1],    &c.ereg_pos,  &c.last_ereg, &c.rb_r[0], &c.rb_r[1]};
+  for (int i = 0; i < 10; ++i) {
+    const XV& x = *order[i];
+    if (!x.v.ex && x.buf >= 0 && c.bs[x.buf].state != 2) return x.buf;
+  }
+  return -1;
+}
+
+// The control step after a completed pass (thread 0; c is the CTA's copy).
+// With exact sums it is taken on the pass's sums as far as they are known:
+// bounded sums settle most steps (certified step); a step they leave open is
+// undone, and c then describes the summary pass that adds the needed
+// buffer's sums in order, whose index is returned (-1: step taken).  With a
+// single term buffer every pass's sums are added in order before its step.
+template <typename Real>
+__device__ int control_step(const LevelArgs<Real>& a, const SchedPtrs<Real>& sp, int inst, InstCtl& c,
+                            const double* tot, bool xsums) {
+  if (!xsums) {   // cannot be open: the values it writes out were exact before
+    if (!advance(a, inst, c, tot, nullptr)) atomicExch(sp.error, 2);
+    return -1;
+  }
+  const XsBufState& B = c.bs[c.desc.xbuf];
+  if (a.xs_bufs > 1 || B.state == 2) {
+    const bool bounded = B.state != 2;
+    ctl_store(sp.ctl + inst, c);   // the state before the step
+    Iv xr[5];
+    for (int k = 0; k < 5; ++k) xr[k] = bounded ? Iv{B.lo[k], B.hi[k], 0} : ivx(B.lo[k]);
+    if (advance(a, inst, c, tot, xr)) {
+      if (bounded && a.xs_prof) atomicAdd(a.xs_prof + 2, 1ull);
+      return -1;
+    }
+    ctl_load(c, sp.ctl + inst);
+  }
+  const int rb = xs_next_resolve(c);
+  if (rb < 0) {   // cannot happen: a step on exact values is never open
+    atomicExch(sp.error, 2);
+    c.desc.kind = TK_DONE;
+    return -1;
+  }
+  c.desc.purpose = c.desc.kind;
+  c.desc.kind = TK_XSUM;
+  c.desc.xres = rb;
+  c.desc.xn = c.bs[rb].ns;
+  return rb;
+}
+
 // Publishes the instance's next pass (thread 0 of the completing CTA), or
 // writes its results and counts it finished.
 template <typename Real>
@@ -1961,7 +2294,7 @@ __device__ void publish(const LevelArgs<Real>& a, const SchedPtrs<Real>& sp, int
   const unsigned long long seq = (atomicAdd(word, 0ull) >> 40) + 1;
   if (c.desc.kind == TK_DONE) {
     if (a.mode != MODE_SMOOTH) {
-      a.out_energy[inst] = c.energy_new;
+      a.out_energy[inst] = c.energy_new.v.lo;
       a.out_steps[inst] = c.iter;
       a.out_phi_buf[inst] = c.cur;
       if (a.out_evals) a.out_evals[inst] = c.total_evals;
@@ -1972,6 +2305,26 @@ __device__ void publish(const LevelArgs<Real>& a, const SchedPtrs<Real>& sp, int
     atomicExch(word, pack_word(seq, 0, 0));
     atomicAdd(sp.finished, 1);
     return;
+  }
+  // a pass with exact sums writes its terms to a buffer no bounded value holds
+  if (a.xs && c.desc.kind != TK_XSUM) {
+    const int nxs = xs_count(a, c.desc);
+    if (nxs) {
+      int b = 0;
+      if (a.xs_bufs > 1) {
+        const unsigned held = xs_held(c);
+        b = -1;
+        for (int q = 0; q < a.xs_bufs && q < kXsBufs; ++q)
+          if (!(held & (1u << q))) { b = q; break; }
+        if (b < 0) {   // cannot happen: at most 5 values are bounded at a time
+          atomicExch(sp.error, 2);
+          b = 0;
+        }
+      }
+      c.desc.xbuf = b;
+      c.bs[b].state = 0;
+      c.bs[b].ns = nxs;
+    }
   }
   c.desc.ntiles = pass_tiles(c.desc.kind, c.desc.k, a.level, a.n, c.desc.xn);
   c.desc.chunk = chunk_tiles(c.desc.ntiles, a.num_inst - *(volatile int*)sp.finished, a.chunk_div, a.chunk_max);
@@ -2047,22 +2400,6 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-// Exact sums a completed pass leaves to add (0: none): the energy passes
-// E_data and p . L p per component, the NCG pass also DE . d per component,
-// the top of the V-cycle |s|^2 per component.
-template <typename Real>
-__device__ __forceinline__ int xs_count(const LevelArgs<Real>& a, const PassDesc& d) {
-  if (a.mode == MODE_SMOOTH) return 0;
-  switch (d.kind) {
-    case TK_E0:
-    case TK_TRIAL: return 3;
-    case TK_NCG: return 5;
-    case TK_VUP: return d.k == a.level ? 2 : 0;
-    case TK_COARSE: return a.level == a.lc ? 2 : 0;
-    default: return 0;
-  }
-}
-
 template <typename Real>
 __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, SchedPtrs<Real> sp) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -2074,6 +2411,8 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
   __shared__ InstCtl cs;
   __shared__ XsSum xss[kXsSlots];
   __shared__ double xres[kXsSlots], xwtot[kThreads / 32];
+  __shared__ double xsp[12];   // bounds of a pass's sums: term sums, magnitude sums
+  __shared__ int xact;         // buffer whose ordered sums the control step needs, or -1
   PassTimer pt{a.pass_cycles ? a.pass_cycles + (size_t)blockIdx.x * kPassKinds : nullptr, 0};
   const TaskRunner<Real> run(a, smem);
 
@@ -2189,51 +2528,70 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
         for (int k = 0; k < kRedSlots; ++k) acc[k] += __ldcg(pp + (size_t)i * kRedSlots + k);
       }
       block_sum(acc, wbuf, tot);
-      // exact sums of the pass, in the reference's order: predictions here,
-      // then a summary pass over the grid, whose completing CTA walks the
-      // chunks and takes the control step of the pass it stands for
-      const int nxs = (a.xs && t.desc.kind != TK_XSUM) ? xs_count(a, t.desc) : 0;
-      // small levels: the summaries by this CTA right away (a pass of its own
-      // would cost more in latency than its work)
       const XsGeom xg(a.n);
-      const bool xs_inline = nxs && nxs * xg.nx * xg.ny * kXsBR <= 6 * kThreads;
-      if (t.desc.kind == TK_XSUM || nxs) {
-        const int kind = (t.desc.kind == TK_XSUM) ? t.desc.purpose : t.desc.kind;
-        const int ns = (t.desc.kind == TK_XSUM) ? t.desc.xn : nxs;
-        if (threadIdx.x == 0) xs_pass_sums(a, t.inst, kind, ns, xss);
-        __syncthreads();
-        if (t.desc.kind == TK_XSUM) {
-          xs_walk(xss, ns, xg, xres, a.xs_prof);
-        } else {
-          xs_predict(xss, ns, xg, xwtot, a.xs_prof);
-          if (xs_inline) {
-            const int per = xg.nx * xg.ny * kXsBR;
-            for (int job = threadIdx.x; job < ns * per; job += kThreads) {
-              const int k = job / per, rem = job - k * per;
-              xs_summary_row(xss[k], xg, rem / kXsBR, rem % kXsBR);
-            }
-            __threadfence();
-            __syncthreads();
-            xs_walk(xss, ns, xg, xres, a.xs_prof);
+      const bool xdone = (t.desc.kind == TK_XSUM);
+      const int nxs = (a.xs && !xdone) ? xs_count(a, t.desc) : 0;
+      // an energy pass with bounds: the sums of its terms and magnitudes
+      const bool cert = nxs && a.xpart && is_energy_kind(t.desc.kind);
+      if (cert) {
+        const double* xp = a.xpart + (size_t)t.inst * a.xpart_stride;
+        for (int h = 0; h < kXpSlots; h += kRedSlots) {
+          double v[kRedSlots] = {0.0, 0.0, 0.0, 0.0};
+          for (int i = threadIdx.x; i < t.desc.ntiles; i += kThreads) {
+#pragma unroll
+            for (int k = 0; k < kRedSlots; ++k)
+              if (h + k < kXpSlots) v[k] += __ldcg(xp + (size_t)i * kXpSlots + h + k);
           }
+          block_sum(v, wbuf, xsp + h);
         }
       }
-      if (threadIdx.x == 0) {
-        ctl_load(cs, sp.ctl + t.inst);
-        if (xs_inline) {
-          advance(a, t.inst, cs, tot, xres);
-        } else if (nxs) {
-          cs.desc.purpose = cs.desc.kind;
-          cs.desc.xn = nxs;
-          cs.desc.kind = TK_XSUM;
-        } else if (t.desc.kind == TK_XSUM) {
-          cs.desc.kind = cs.desc.purpose;
-          advance(a, t.inst, cs, tot, xres);
-        } else {
-          advance(a, t.inst, cs, tot, nullptr);
-        }
-        publish(a, sp, t.inst, cs);
+      // a summary pass completed: its buffer's sums in the reference's order
+      if (xdone) {
+        if (threadIdx.x == 0) xs_pass_sums(a, t.inst, t.desc.purpose, t.desc.xn, t.desc.xres, xss);
+        __syncthreads();
+        xs_walk(xss, t.desc.xn, xg, xres, a.xs_prof);
       }
+      // the control step; when it needs a buffer's ordered sums first, the
+      // predictions for them here and a summary pass over the grid (small
+      // levels: the summaries and the walk right here, then the step again)
+      for (bool first = true;; first = false) {
+        if (threadIdx.x == 0) {
+          if (first) {
+            ctl_load(cs, sp.ctl + t.inst);
+            if (xdone) {
+              xs_settle(a, t.inst, cs, t.desc.xres, xres);
+            } else if (nxs) {
+              XsBufState& B = cs.bs[cs.desc.xbuf];
+              B.ns = nxs;
+              B.state = 1;
+              const double N = (double)a.n * (double)a.n;
+              for (int k = 0; k < nxs; ++k) {
+                if (cert) xs_bounds(xsp[k], xsp[5 + k], N, B.lo[k], B.hi[k]);
+                else B.lo[k] = B.hi[k] = __longlong_as_double(0x7ff8000000000000ll);
+              }
+            }
+          }
+          xact = control_step(a, sp, t.inst, cs, tot, xdone || nxs > 0);
+        }
+        __syncthreads();
+        const int rb = xact;
+        if (rb < 0) break;
+        const int ns = cs.desc.xn;
+        if (threadIdx.x == 0) xs_pass_sums(a, t.inst, cs.desc.purpose, ns, rb, xss);
+        __syncthreads();
+        xs_predict(xss, ns, xg, xwtot, a.xs_prof);
+        if (ns * xg.nx * xg.ny * kXsBR > 6 * kThreads) break;   // summary pass published below
+        const int per = xg.nx * xg.ny * kXsBR;
+        for (int job = threadIdx.x; job < ns * per; job += kThreads) {
+          const int k = job / per, rem = job - k * per;
+          xs_summary_row(xss[k], xg, rem / kXsBR, rem % kXsBR);
+        }
+        __threadfence();
+        __syncthreads();
+        xs_walk(xss, ns, xg, xres, a.xs_prof);
+        if (threadIdx.x == 0) xs_settle(a, t.inst, cs, rb, xres);
+      }
+      if (threadIdx.x == 0) publish(a, sp, t.inst, cs);
       __syncthreads();
     }
     pt.stop(PK_REDUCE);

@@ -106,7 +106,7 @@ EXPORTS = [
     "msgpu_net_train_step_device", "msgpu_net_loss_grad", "msgpu_prepare_images_device", "msgpu_register_batch_warm",
     "msgpu_register_batch_warm_device", "msgpu_find_xshift_yconst", "msgpu_find_xshift_yconst_device",
     "msgpu_empty_lines_to_nan", "msgpu_empty_lines_to_nan_device", "msgpu_remove_empty_lines",
-    "msgpu_remove_empty_lines_device", "msgpu_set_wait_limits", "msgpu_set_sum_order", "msgpu_warp_sum_device",
+    "msgpu_remove_empty_lines_device", "msgpu_set_wait_limits", "msgpu_set_sum_order", "msgpu_set_certified_steps", "msgpu_warp_sum_device",
     "msgpu_mean_from_sums_device", "msgpu_set_graphs", "msgpu_get_tuning", "msgpu_set_tuning",
     "msgpu_autotune_device", "msgpu_gd_level_log", "msgpu_exact_sum_device",
 ]
@@ -158,6 +158,7 @@ def lib():
                                             ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
         L.msgpu_set_data_term.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.msgpu_set_sum_order.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.msgpu_set_certified_steps.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.msgpu_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(Stats)]
         L.msgpu_series_params_default.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(SeriesParams)]
         L.msgpu_series_params_default.restype = None
@@ -713,7 +714,7 @@ class Context:
                 "level_evals": list(s.level_evals[:k]), "level_cluster": list(s.level_cluster[:k]),
                 "level_pass_cycles": [dict(zip(PASS_KINDS, list(s.level_pass_cycles[i]))) for i in range(k)],
                 "graph_replayed": bool(s.graph_replayed),
-                "level_exact_sums": [dict(zip(["passes", "cycles_predict", "cycles_summaries", "cycles_walk",
+                "level_exact_sums": [dict(zip(["passes", "cycles_predict", "certified_steps", "cycles_walk",
                                                "chunks", "chunks_term_by_term", "cycles_term_by_term",
                                                "cycles_walk_warps"], list(s.level_xs[i])))
                                      for i in range(k)]}
@@ -756,6 +757,12 @@ class Context:
         """0: the reference's sequential order (default), 1: a fixed parallel
         order, for the FP64 sums of energy() and gd_level()."""
         self._check(lib().msgpu_set_sum_order(self._h, int(sum_order)))
+
+    def set_certified_steps(self, on: bool):
+        """Control steps on bounded sums where the bounds settle them (default
+        on); off: every pass's sums added in the reference's order first.
+        The results are the same either way."""
+        self._check(lib().msgpu_set_certified_steps(self._h, int(bool(on))))
 
     def gd_level(self, level, R, T, phix, phiy, lam, max_iter, stop_eps=0.0, fp64=False, max_trace=256):
         px = _f64(phix).copy()

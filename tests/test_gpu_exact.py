@@ -117,6 +117,37 @@ def test_benchmark_configuration_is_the_reference_bit_for_bit(gpu):
         assert _digest(phis[f, 0], phis[f, 1]) == str(d["digests"][f]), (f, dpx)
 
 
+def test_certified_steps_give_the_ordered_sums_results(gpu):
+    """Control steps taken on bounded sums (the default) against every pass's
+    sums added in the reference's order first: the same displacements,
+    energies and step counts, bit for bit, while most steps of the energy
+    passes are settled by the bounds alone."""
+    import msgpu
+    from msgpu import synthetic as syn
+    level = 8
+    n = (1 << level) + 1
+    fr, _, _ = syn.make_series(n, 5, syn.SQUARE_257, seed=8812)
+    p = msgpu.default_params(precision_level=level, input_level=level, start_level=4, stop_level=level,
+                             max_gd_iterations=25, use_fp64=1)
+    gpu.set_profiling(True)
+    try:
+        phis_c, e_c, s_c = gpu.register_batch(p, fr[0], fr[1:])
+        st_c = gpu.stats()
+        gpu.set_certified_steps(False)
+        phis_o, e_o, s_o = gpu.register_batch(p, fr[0], fr[1:])
+        st_o = gpu.stats()
+    finally:
+        gpu.set_certified_steps(True)
+        gpu.set_profiling(False)
+    assert np.array_equal(phis_c, phis_o)
+    assert np.array_equal(e_c, e_o) and np.array_equal(s_c, s_o)
+    cert = sum(x["certified_steps"] for x in st_c["level_exact_sums"])
+    walked_c = sum(x["passes"] for x in st_c["level_exact_sums"])
+    walked_o = sum(x["passes"] for x in st_o["level_exact_sums"])
+    assert sum(x["certified_steps"] for x in st_o["level_exact_sums"]) == 0
+    assert cert > 0 and walked_c < walked_o, (cert, walked_c, walked_o)
+
+
 def test_ragged_batch_matches_the_oracle_bit_for_bit(gpu, oracle):
     import msgpu
     from msgpu import synthetic as syn
