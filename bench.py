@@ -84,6 +84,7 @@ def workload(rank: int):
 
 
 SUM_ORDER = 0   # 0: the reference's sequential order (bit-exact); 1: parallel order (--sum-order 1)
+CERTIFIED = True   # sum order 0: control steps on bounded sums where the bounds settle them
 
 
 def params(fp64: bool):
@@ -307,6 +308,7 @@ def profile_case(level: int, iters: int, fp64: bool):
     ctx = msgpu.Context(0)
     p = msgpu.default_params(precision_level=level, input_level=level, start_level=level, stop_level=level,
                              max_gd_iterations=iters, use_fp64=int(fp64), data_term=DATA_TERM, sum_order=SUM_ORDER)
+    ctx.set_certified_steps(CERTIFIED)
     ctx.set_profiling(True)
     ctx.register_batch(p, frames[FRAMES], frames[:FRAMES])
     print(json.dumps({"profile_level": level, "frames": FRAMES, "iters": iters, "fp64": fp64,
@@ -1127,6 +1129,9 @@ def main():
     ap.add_argument("--sum-order", type=int, default=0, choices=[0, 1],
                     help="0: global sums in the reference's sequential order (bit-exact, default); "
                          "1: fixed parallel order")
+    ap.add_argument("--no-certified", action="store_true",
+                    help="with sum order 0: add every pass's sums in order before its control step (the results "
+                         "are the same; for comparisons)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ncc", action="store_true",
                     help="normalized cross-correlation data term (matchSeries' default model) instead of SSD")
@@ -1158,9 +1163,10 @@ def main():
                     help="time matchSeries' whole first stage with accumulated deformations (msgpu_match_series)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    global DATA_TERM, SUM_ORDER
+    global DATA_TERM, SUM_ORDER, CERTIFIED
     DATA_TERM = 1 if args.ncc else 0
     SUM_ORDER = args.sum_order
+    CERTIFIED = not args.no_certified
     if args.profile_level:
         return profile_case(args.profile_level, args.profile_iters, not args.fp32)
     if args.profile_compose or args.profile_series:
@@ -1238,6 +1244,7 @@ def main():
     N = n * n
     nlev = LEVEL - START + 1
     ctx = msgpu.Context(local)
+    ctx.set_certified_steps(CERTIFIED)
     dev = torch.device("cuda", local)
     d_ref = torch.from_numpy(ref).to(dev)
     d_tmpl = torch.from_numpy(tmpl).to(dev)

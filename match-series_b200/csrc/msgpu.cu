@@ -1136,11 +1136,7 @@ __global__ void k_xs_predict(XsSum s, int n) {
   xs_predict(&s, 1, XsGeom(n), wtot, nullptr);
 }
 __global__ void k_xs_summaries(XsSum s, int n) {
-  const XsGeom g(n);
-  if ((int)threadIdx.x >= kXsTilesPerTask * kXsBR) return;
-  const int b = blockIdx.x * kXsTilesPerTask + (int)threadIdx.x / kXsBR;
-  if (b >= g.nx * g.ny) return;
-  xs_summary_row(s, g, b, (int)threadIdx.x % kXsBR);
+  xs_summary_task([&](int) { return s; }, 1, XsGeom(n), (int)blockIdx.x);
 }
 __global__ void k_xs_walk(XsSum s, int n, double* out) {
   __shared__ double r[1];
@@ -1745,7 +1741,7 @@ int msgpu_exact_sum_device(msgpu_context* ctx, int level, const double* d_terms,
   k_xs_fill<<<std::min(2048, (n * n + 255) / 256), 256, 0, st>>>(d_terms, n, s);
   k_xs_totals<<<std::min(2048, (n * g.nx + 255) / 256), 256, 0, st>>>(d_terms, n, s);
   k_xs_predict<<<1, 256, 0, st>>>(s, n);
-  k_xs_summaries<<<(g.nx * g.ny + kXsTilesPerTask - 1) / kXsTilesPerTask, 256, 0, st>>>(s, n);
+  k_xs_summaries<<<xs_summary_tasks(1, n), 256, 0, st>>>(s, n);
   k_xs_walk<<<1, 32, 0, st>>>(s, n, d_out);
   CK(cudaGetLastError());
   ctx->stats.kernel_launches += 5;

@@ -284,14 +284,15 @@ struct EnergyPass {
   Tiles tl;
   double* xs;   // exact sums: the pass's term buffer (Real = double), or null
   double* xp;   // certified control steps: the instance's per-tile sums, or null
+  double (*xpw)[kXpSlots];   // with xp: per warp, the sums of its rows (shared)
 
   __device__ EnergyPass(const Inst<Real>& I_, int kind_, Real tau_, Real beta_, bool odz, const Real* phx_,
                         const Real* phy_, const Real* dx_, const Real* dy_, const Real* sx_, const Real* sy_,
                         const Real* dex_, const Real* dey_, Real* wdx_, Real* wdy_, Real* sm_, double* part_,
-                        double* xs_ = nullptr, double* xp_ = nullptr)
+                        double* xs_ = nullptr, double* xp_ = nullptr, double (*xpw_)[kXpSlots] = nullptr)
       : I(I_), kind(kind_), tau(tau_), beta(beta_), od_zero(odz), phx(phx_), phy(phy_), dx(dx_), dy(dy_),
         sx(sx_), sy(sy_), dex(dex_), dey(dey_), wdx(wdx_), wdy(wdy_), sm(sm_), part(part_), tl(I_.n), xs(xs_),
-        xp(xp_) {
+        xp(xp_), xpw(xpw_) {
     nwin = (kind == 0) ? 3 : (kind == 1 ? 5 : 7);
   }
   __device__ Real* win(int stage, int k) const { return sm + ((size_t)stage * nwin + k) * EWIN; }
@@ -326,13 +327,13 @@ struct EnergyPass {
   // on the whole window first, and E_reg = 1/2 (p_x . L p_x + p_y . L p_y)
   // is evaluated there as DisplacementLengthEnergy does (hyperelastic.h:
   // 178-183), not by the quadratic expansion of the fast path.  With xp the
-  // tile also stores, per term set, the sum of its terms and of their
-  // magnitudes (any order: they only bound the ordered sums).
+  // tile also adds up, per warp and term set, the sum of its terms and of
+  // their magnitudes (any order: they only bound the ordered sums); the
+  // task loop stores the tile's totals after its reduction barrier.
   __device__ void compute_exact(int t, int stage) {
     int x0, x1, y0, y1;
     tl.rect(t, x0, x1, y0, y1);
     const int n = I.n;
-    __shared__ double xpw[kThreads / 32][kXpSlots];   // per warp: its rows' sums
     const int wid = threadIdx.x >> 5;
     if (xp && (threadIdx.x & 31) == 0) {
 #pragma unroll
@@ -475,15 +476,6 @@ struct EnergyPass {
             }
           }
         }
-      }
-    }
-    if (xp) {
-      __syncthreads();
-      if (threadIdx.x < kXpSlots) {
-        double v = 0.0;
-#pragma unroll
-        for (int w = 0; w < kThreads / 32; ++w) v += xpw[w][threadIdx.x];
-        __stcg(xp + (size_t)t * kXpSlots + threadIdx.x, v);
       }
     }
   }
@@ -1583,7 +1575,9 @@ template <typename Real>
 struct TaskRunner {
   const LevelArgs<Real>& a;
   Real* smem;
-  __device__ TaskRunner(const LevelArgs<Real>& a_, Real* sm) : a(a_), smem(sm) {}
+  double (*xpw)[kXpSlots];   // shared: per-warp bound sums of an energy tile
+  __device__ TaskRunner(const LevelArgs<Real>& a_, Real* sm, double (*xpw_)[kXpSlots])
+      : a(a_), smem(sm), xpw(xpw_) {}
 
   template <class F>
   __device__ void with_pass(int inst, const PassDesc& d, double* part, F&& f) const {
@@ -1598,14 +1592,14 @@ struct TaskRunner {
     switch (d.kind) {
       case TK_E0: {
         EnergyPass<Real> ps(I, 0, Real(0), Real(0), false, phi, phi + cs, nullptr, nullptr, nullptr, nullptr, nullptr,
-                            nullptr, nullptr, nullptr, smem, part, xs, xp);
+                            nullptr, nullptr, nullptr, smem, part, xs, xp, xpw);
         f(ps);
         break;
       }
       case TK_TRIAL: {
         const Real* dd = I.arr(a.off_d[d.dcur]);
         EnergyPass<Real> ps(I, 1, (Real)d.t, Real(0), false, phi, phi + cs, dd, dd + cs, nullptr, nullptr, nullptr,
-                            nullptr, nullptr, nullptr, smem, part, xs, xp);
+                            nullptr, nullptr, nullptr, smem, part, xs, xp, xpw);
         f(ps);
         break;
       }
@@ -1613,7 +1607,7 @@ struct TaskRunner {
         const Real* od = I.arr(a.off_d[d.dcur]);
         Real* wd = I.arr(a.off_d[d.dn]);
         EnergyPass<Real> ps(I, 2, (Real)d.t, (Real)d.beta, (d.flags & PF_ODZERO) != 0, phi, phi + cs, od, od + cs, s,
-                            s + cs, de, de + cs, wd, wd + cs, smem, part, xs, xp);
+                            s + cs, de, de + cs, wd, wd + cs, smem, part, xs, xp, xpw);
         f(ps);
         break;
       }
@@ -1689,16 +1683,11 @@ struct TaskRunner {
 
   __device__ void compute(int inst, const PassDesc& d, int tile, int stage, double* part) const {
     if (d.kind == TK_XSUM) {
-      // thread (block b, row r) of task tile `tile`: blocks of all sums in turn
-      if ((int)threadIdx.x >= kXsTilesPerTask * kXsBR) return;
-      const XsGeom g(a.n);
-      const int ntiles = g.nx * g.ny;
-      const int b = tile * kXsTilesPerTask + (int)threadIdx.x / kXsBR, r = (int)threadIdx.x % kXsBR;
-      const int k = b / ntiles;
-      if (k >= d.xn) return;
+      // chunk and group summaries of the task tile's tile rows (all sums in turn)
       const bool energy = (d.purpose == TK_E0 || d.purpose == TK_TRIAL || d.purpose == TK_NCG);
-      const XsSum s = xs_sum(xs_buffer(a, inst, d.xres), a.n, k, energy && k == 0);
-      xs_summary_row(s, g, b - k * ntiles, r);
+      double* base = xs_buffer(a, inst, d.xres);
+      const int n = a.n;
+      xs_summary_task([&](int k) { return xs_sum(base, n, k, energy && k == 0); }, d.xn, XsGeom(n), tile);
       return;
     }
     if (d.kind == TK_COARSE) {
@@ -2414,7 +2403,8 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
   __shared__ double xsp[12];   // bounds of a pass's sums: term sums, magnitude sums
   __shared__ int xact;         // buffer whose ordered sums the control step needs, or -1
   PassTimer pt{a.pass_cycles ? a.pass_cycles + (size_t)blockIdx.x * kPassKinds : nullptr, 0};
-  const TaskRunner<Real> run(a, smem);
+  __shared__ double xpw[kThreads / 32][kXpSlots];
+  const TaskRunner<Real> run(a, smem, xpw);
 
   // publish the first pass of the instances this CTA owns
   if (threadIdx.x == 0) {
@@ -2505,6 +2495,14 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
 #pragma unroll
         for (int k = 0; k < kRedSlots; ++k) __stcg(pp + k, tot[k]);
       }
+      // an energy tile with bounds: its per-warp sums (written before the
+      // reduction's barriers) into the tile's bound sums
+      if (a.xpart && a.xs && is_energy_kind(t.desc.kind) && threadIdx.x < kXpSlots) {
+        double v = 0.0;
+#pragma unroll
+        for (int w = 0; w < kThreads / 32; ++w) v += xpw[w][threadIdx.x];
+        __stcg(a.xpart + (size_t)t.inst * a.xpart_stride + (size_t)tile * kXpSlots + threadIdx.x, v);
+      }
 #pragma unroll
       for (int k = 0; k < kRedSlots; ++k) part[k] = 0.0;
       stage ^= 1;
@@ -2580,14 +2578,9 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
         if (threadIdx.x == 0) xs_pass_sums(a, t.inst, cs.desc.purpose, ns, rb, xss);
         __syncthreads();
         xs_predict(xss, ns, xg, xwtot, a.xs_prof);
-        if (ns * xg.nx * xg.ny * kXsBR > 6 * kThreads) break;   // summary pass published below
-        const int per = xg.nx * xg.ny * kXsBR;
-        for (int job = threadIdx.x; job < ns * per; job += kThreads) {
-          const int k = job / per, rem = job - k * per;
-          xs_summary_row(xss[k], xg, rem / kXsBR, rem % kXsBR);
-        }
-        __threadfence();
-        __syncthreads();
+        const int ntask = xs_summary_tasks(ns, a.n);
+        if (ntask > 6) break;   // summary pass published below
+        for (int task = 0; task < ntask; ++task) xs_summary_task([&](int k) { return xss[k]; }, ns, xg, task);
         xs_walk(xss, ns, xg, xres, a.xs_prof);
         if (threadIdx.x == 0) xs_settle(a, t.inst, cs, rb, xres);
       }

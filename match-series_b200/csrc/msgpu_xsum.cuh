@@ -34,8 +34,9 @@
 // chunks take the slow path.
 //
 // Layout of one sum's terms: one block per tile of the pass (tile t of a grid
-// of nx x ny tiles of TX x TY items), block = (TX + 1) x (TY + 1) doubles,
-// term (k, r) (item x0 + k of row y0 + r) at k * (TY + 1) + r.  Every tile
+// of nx x ny tiles of TX x TY items), block = (TY + 1) rows of TX + 2 doubles
+// (TX + 1 items, padded to 16 bytes), term (k, r) (item x0 + k of row y0 + r)
+// at r * (TX + 2) + k: the tiles store their terms with coalesced writes.  Every tile
 // also writes two partial totals per (row, tile) chunk (the two warps of a
 // row of 64), added to predict the binades.
 #pragma once
@@ -46,7 +47,7 @@ namespace msg {
 
 constexpr int kXsSlots = 5;           // sums of one pass at most (NCG: E_data, 2 x E_reg, 2 x Df)
 constexpr int kXsBR = 9;              // rows per block: TY + 1 (the last tile row owns the final node row)
-constexpr int kXsBK = 65;             // items per block row: TX + 1
+constexpr int kXsBK = 66;             // doubles per block row: TX + 1 items, padded to 16 bytes
 constexpr int kXsBlock = kXsBR * kXsBK;
 
 // Geometry of a level's sums: element-pass tiles of 64 x 8 items.
@@ -67,7 +68,7 @@ struct XsGeom {
 // Per-instance region of the exact sums, in doubles: kXsSlots term arrays,
 // the chunk totals (2 per chunk), and the chunk summaries (struct of arrays).
 struct XsLayout {
-  size_t terms, tot, X, R, mnB, mxB, mnA, mxA, ef, stride;
+  size_t terms, tot, X, R, mnB, mxB, mnA, mxA, ef, gX, gmn, gmx, gef, stride;
   __host__ __device__ explicit XsLayout(int n) {
     const XsGeom g(n);
     const size_t nc = (size_t)g.nch, a = 32;
@@ -82,6 +83,11 @@ struct XsLayout {
     mnA = o;   o += up(kXsSlots * nc);
     mxA = o;   o += up(kXsSlots * nc);
     ef = o;    o += up((kXsSlots * nc + 1) / 2);   // ints
+    const size_t ng = (size_t)g.ny;
+    gX = o;    o += up(kXsSlots * ng);
+    gmn = o;   o += up(kXsSlots * ng);
+    gmx = o;   o += up(kXsSlots * ng);
+    gef = o;   o += up((kXsSlots * ng + 1) / 2);   // ints
     stride = o;
   }
 };
@@ -92,6 +98,8 @@ struct XsSum {
   double* tot;
   long long *X, *R, *mnB, *mxB, *mnA, *mxA;
   int* ef;
+  long long *gX, *gmn, *gmx;   // group summaries (one group per tile row)
+  int* gef;
   int rows, items;   // rows of items and items per row: n (node sums) or n - 1 (element sums)
 };
 
@@ -109,6 +117,11 @@ __host__ __device__ inline XsSum xs_sum(double* base, int n, int slot, bool elem
   s.mnA = reinterpret_cast<long long*>(base + L.mnA) + slot * nc;
   s.mxA = reinterpret_cast<long long*>(base + L.mxA) + slot * nc;
   s.ef = reinterpret_cast<int*>(base + L.ef) + slot * nc;
+  const size_t ng = (size_t)g.ny;
+  s.gX = reinterpret_cast<long long*>(base + L.gX) + slot * ng;
+  s.gmn = reinterpret_cast<long long*>(base + L.gmn) + slot * ng;
+  s.gmx = reinterpret_cast<long long*>(base + L.gmx) + slot * ng;
+  s.gef = reinterpret_cast<int*>(base + L.gef) + slot * ng;
   s.rows = elements ? n - 1 : n;
   s.items = elements ? n - 1 : n;
   return s;
@@ -116,7 +129,7 @@ __host__ __device__ inline XsSum xs_sum(double* base, int n, int slot, bool elem
 
 // Block of tile t and the place of item (k, r) in it.
 __device__ __forceinline__ double* xs_block(const XsSum& s, int tile) { return s.terms + (size_t)tile * kXsBlock; }
-__device__ __forceinline__ int xs_at(int k, int r) { return k * kXsBR + r; }
+__host__ __device__ __forceinline__ int xs_at(int k, int r) { return r * kXsBK + k; }
 
 // ---------------------------------------------------------------------------
 // Exponent arithmetic.  A finite normal double S = m 2^E with 2^52 <= |m| <
@@ -219,59 +232,6 @@ __device__ __forceinline__ bool xs_in_range(long long v, bool neg) {
   return neg ? (v >= -hi && v <= -lo) : (v >= lo && v <= hi);
 }
 
-// S + t_0 + ... + t_{cnt-1} in sequence, the terms one per lane (lane k holds
-// t_k), by the warp: at the exponent of the exact running sum every lane
-// converts its term to units of the ulp, a prefix sum over the lanes gives
-// the running mantissa after every term, and the run stops at the first term
-// whose sum leaves the binade or is a tie (or whose running sum cannot be
-// split); that one term is added in floating point, and the walk goes on
-// from the next term.  Every lane returns the same value.
-__device__ __forceinline__ double xs_add_lanes(double S, double v, int cnt) {
-  const int lane = threadIdx.x & 31;
-  int pos = 0;
-  while (pos < cnt) {
-    int E;
-    long long m;
-    if (!xs_split(S, E, m)) {
-      S = __dadd_rn(S, __shfl_sync(0xffffffffu, v, pos));
-      ++pos;
-      continue;
-    }
-    const bool act = lane >= pos && lane < cnt;
-    const double q = v * xs_pow2(-E);
-    bool ok = act && fabs(q) < 36028797018963968.0;
-    long long c = 0;
-    if (ok) {
-      c = __double2ll_rn(q);
-      ok = fabs(q - (double)c) != 0.5;
-    }
-    unsigned long long inc = act ? (unsigned long long)c : 0ull;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const unsigned long long t = __shfl_up_sync(0xffffffffu, inc, o);
-      if (lane >= o) inc += t;
-    }
-    const long long mi = m + (long long)inc;   // mantissa after this lane's term
-    const bool good = ok && xs_in_range(mi, m < 0);
-    const unsigned bad = __ballot_sync(0xffffffffu, act && !good);
-    const int first = bad ? __ffs(bad) - 1 : cnt;
-    if (first > pos) S = (double)__shfl_sync(0xffffffffu, mi, first - 1) * xs_pow2(E);
-    if (first < cnt) {
-      S = __dadd_rn(S, __shfl_sync(0xffffffffu, v, first));
-      if (first == pos) {
-        // no run at all: the sum changes binade term after term here, so
-        // the rest of the segment goes one addition after the other
-        for (int k = first + 1; k < cnt; ++k) S = __dadd_rn(S, __shfl_sync(0xffffffffu, v, k));
-        return S;
-      }
-      pos = first + 1;
-    } else {
-      pos = cnt;
-    }
-  }
-  return S;
-}
-
 // S + t_0 + ... + t_{cnt-1} one addition after the other (lane k holds t_k);
 // the shuffles do not depend on S, so they are issued ahead of the additions.
 __device__ __forceinline__ double xs_add_seq(double S, double v, int cnt) {
@@ -288,18 +248,6 @@ __device__ __forceinline__ double xs_add_seq(double S, double v, int cnt) {
   return S;
 }
 
-// One segment of up to 32 terms: where the terms are not small against the
-// running sum (its binade would change at many of them) one addition after
-// the other, else the binade runs of xs_add_lanes.
-__device__ __forceinline__ double xs_add_segment(double S, double v, int cnt) {
-  const int lane = threadIdx.x & 31;
-  double a = lane < cnt ? fabs(v) : 0.0;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-  if (!(a < fabs(S) * 0.015625)) return xs_add_seq(S, v, cnt);   // also for S = 0 and non-finite values
-  return xs_add_lanes(S, v, cnt);
-}
-
 // The terms of chunk j, lane k holding terms k, k + 32 and k + 64.
 struct XsChunkTerms {
   double v0, v1, v2;
@@ -309,20 +257,99 @@ __device__ __forceinline__ XsChunkTerms xs_load_chunk(const XsSum& s, const XsGe
   const int lane = threadIdx.x & 31;
   int tile, r, len;
   xs_chunk(s, g, j, tile, r, len);
-  const double* p = xs_block(s, tile) + r;
+  const double* p = xs_block(s, tile) + xs_at(0, r);
   XsChunkTerms c;
   c.len = len;
-  c.v0 = (lane < len) ? __ldcg(p + xs_at(lane, 0)) : 0.0;
-  c.v1 = (lane + 32 < len) ? __ldcg(p + xs_at(lane + 32, 0)) : 0.0;
-  c.v2 = (lane + 64 < len) ? __ldcg(p + xs_at(lane + 64, 0)) : 0.0;
+  c.v0 = (lane < len) ? __ldcg(p + lane) : 0.0;
+  c.v1 = (lane + 32 < len) ? __ldcg(p + lane + 32) : 0.0;
+  c.v2 = (lane + 64 < len) ? __ldcg(p + lane + 64) : 0.0;
   return c;
 }
 
+// S + t_0 + ... + t_{cnt-1} in sequence for up to 64 terms (lane k holds t_k
+// in va and t_{32+k} in vb), by the warp: at the exponent of the exact
+// running sum every lane converts its terms to units of the ulp, a prefix
+// sum over the lanes gives the running mantissa after every term, and the
+// run stops at the first term whose sum leaves the binade or is a tie (or
+// whose running sum cannot be split); that one term is added in floating
+// point, and the walk goes on from the next term.  Both halves are
+// converted and prefix-summed at once, so a run that stays in one binade
+// costs one pass over all 64 terms, and a run that crosses a binade once
+// costs two.  After two passes in a row that make no progress the rest goes
+// one addition after the other.
+__device__ __forceinline__ double xs_add_lanes64(double S, double va, double vb, int cnt) {
+  const int lane = threadIdx.x & 31;
+  auto term = [&](int t) { return __shfl_sync(0xffffffffu, t < 32 ? va : vb, t & 31); };
+  int pos = 0, stalls = 0;
+  while (pos < cnt) {
+    int E;
+    long long m;
+    if (!xs_split(S, E, m)) {
+      S = __dadd_rn(S, term(pos));
+      ++pos;
+      continue;
+    }
+    const double sc = xs_pow2(-E);
+    const bool actA = lane >= pos && lane < cnt, actB = lane + 32 >= pos && lane + 32 < cnt;
+    const double qa = va * sc, qb = vb * sc;
+    bool okA = actA && fabs(qa) < 36028797018963968.0, okB = actB && fabs(qb) < 36028797018963968.0;
+    long long ca = 0, cb = 0;
+    if (okA) {
+      ca = __double2ll_rn(qa);
+      okA = fabs(qa - (double)ca) != 0.5;
+    }
+    if (okB) {
+      cb = __double2ll_rn(qb);
+      okB = fabs(qb - (double)cb) != 0.5;
+    }
+    unsigned long long ia = actA ? (unsigned long long)ca : 0ull, ib = actB ? (unsigned long long)cb : 0ull;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long ta = __shfl_up_sync(0xffffffffu, ia, o);
+      const unsigned long long tb = __shfl_up_sync(0xffffffffu, ib, o);
+      if (lane >= o) {
+        ia += ta;
+        ib += tb;
+      }
+    }
+    const unsigned long long totA = __shfl_sync(0xffffffffu, ia, 31);
+    const long long miA = m + (long long)ia, miB = m + (long long)(totA + ib);   // mantissas after the terms
+    const bool neg = m < 0;
+    const unsigned badA = __ballot_sync(0xffffffffu, actA && !(okA && xs_in_range(miA, neg)));
+    const unsigned badB = __ballot_sync(0xffffffffu, actB && !(okB && xs_in_range(miB, neg)));
+    const int first = badA ? __ffs(badA) - 1 : (badB ? 32 + __ffs(badB) - 1 : cnt);
+    if (first > pos) {
+      const int t = first - 1;
+      S = (double)__shfl_sync(0xffffffffu, t < 32 ? miA : miB, t & 31) * xs_pow2(E);
+    }
+    if (first >= cnt) break;
+    S = __dadd_rn(S, term(first));
+    if (first == pos && ++stalls >= 2) {   // the sum changes binade term after term here
+      for (int t = first + 1; t < cnt; ++t) S = __dadd_rn(S, term(t));
+      return S;
+    }
+    if (first > pos) stalls = 0;
+    pos = first + 1;
+  }
+  return S;
+}
+
 // fl(... fl(fl(S + p_0) + p_1) ... + p_{len-1}) for a chunk's terms, by the
-// warp in segments of 32 terms (every lane returns the same value).
+// warp (every lane returns the same value): where the terms are small
+// against the running sum (its binade changes at few of them) in binade
+// runs of up to 64 terms, else one addition after the other.
 __device__ __forceinline__ double xs_add_terms(double S, const XsChunkTerms& c) {
-  S = xs_add_segment(S, c.v0, c.len < 32 ? c.len : 32);
-  if (c.len > 32) S = xs_add_segment(S, c.v1, c.len < 64 ? c.len - 32 : 32);
+  const int lane = threadIdx.x & 31;
+  const int n64 = c.len < 64 ? c.len : 64;
+  double a = (lane < n64 ? fabs(c.v0) : 0.0) + (lane + 32 < n64 ? fabs(c.v1) : 0.0);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  if (a < fabs(S) * 0.015625) {   // false for S = 0 and non-finite values
+    S = xs_add_lanes64(S, c.v0, c.v1, n64);
+  } else {
+    S = xs_add_seq(S, c.v0, c.len < 32 ? c.len : 32);
+    if (c.len > 32) S = xs_add_seq(S, c.v1, c.len < 64 ? c.len - 32 : 32);
+  }
   if (c.len > 64) S = xs_add_seq(S, c.v2, c.len - 64);
   return S;
 }
@@ -330,16 +357,19 @@ __device__ __forceinline__ double xs_add_chunk(const XsSum& s, const XsGeom& g, 
   return xs_add_terms(S, xs_load_chunk(s, g, j));
 }
 
-// The sequential sum 0 + t_0 + t_1 + ... of one sum, by one warp (every lane
-// returns it).  Needs the summaries of every chunk.
-__device__ double xs_drive(const XsSum& s, const XsGeom& g, unsigned long long* prof) {
+// Walk counters of one warp: chunks added term by term and their cycles.
+struct XsWalkCount {
+  unsigned long long chunks, slow, slow_cycles;
+};
+
+// S + the terms of chunks [j0, j1) of one sum in order, by one warp (every
+// lane returns it), from the chunk summaries: 32 chunks at a time.
+__device__ double xs_walk_chunks(const XsSum& s, const XsGeom& g, int j0, int j1, double S, XsWalkCount& wc) {
   unsigned long long slow = 0, slow_cycles = 0;
-  const long long t_start = clock64();
   const int lane = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;   // lanes below this one
-  const int nch = s.rows * g.nx;
-  double S = 0.0;
-  int j = 0;
+  const int nch = j1;
+  int j = j0;
   // the records of the next window are loaded while the current one is walked
   auto load = [&](int jn, int& ef, long long& X, long long& lo, long long& hi, long long& R, long long& loA,
                   long long& hiA) {
@@ -354,8 +384,8 @@ __device__ double xs_drive(const XsSum& s, const XsGeom& g, unsigned long long* 
   };
   int nef;
   long long nX, nlo, nhi, nR, nloA, nhiA;
-  load(lane, nef, nX, nlo, nhi, nR, nloA, nhiA);
-  for (int jb = 0; jb < nch; jb += 32) {
+  load(j0 + lane, nef, nX, nlo, nhi, nR, nloA, nhiA);
+  for (int jb = j0; jb < nch && !isnan(S); jb += 32) {
     const bool in = jb + lane < nch;
     const int ef = nef;
     const long long X = nX, lo = nlo, hi = nhi, R = nR, loA = nloA, hiA = nhiA;
@@ -375,7 +405,7 @@ __device__ double xs_drive(const XsSum& s, const XsGeom& g, unsigned long long* 
     XsChunkTerms pt;
     if (pf >= 0) pt = xs_load_chunk(s, g, jb + pf);
     while (j < jb + 32 && j < nch) {
-      if (isnan(S)) return S;
+      if (isnan(S)) break;
       int E;
       long long m;
       if (!xs_split(S, E, m)) {
@@ -450,10 +480,137 @@ __device__ double xs_drive(const XsSum& s, const XsGeom& g, unsigned long long* 
       }
     }
   }
-  if (prof && (threadIdx.x & 31) == 0) {
-    atomicAdd(prof + 4, (unsigned long long)nch);
-    atomicAdd(prof + 5, slow);
-    atomicAdd(prof + 6, slow_cycles);
+  wc.chunks += (unsigned long long)(j1 - j0);
+  wc.slow += slow;
+  wc.slow_cycles += slow_cycles;
+  return S;
+}
+
+
+// Chunk group ty of a sum: the chunks of tile row ty (rows [8 ty, 8 ty + 8),
+// the last group to the last row), a contiguous run of the walk order.
+__device__ __forceinline__ void xs_group_range(const XsSum& s, const XsGeom& g, int ty, int& j0, int& j1) {
+  j0 = ty * 8 * g.nx;
+  j1 = ((ty == g.ny - 1) ? s.rows : ty * 8 + 8) * g.nx;
+}
+
+// Summary of chunk group ty (one warp): when every chunk of it has a summary
+// at the first chunk's exponent, without a tie and with moderate sizes, the
+// sum of their c's (gX) and the smallest and largest partial sum relative to
+// the group start (gmn, gmx); else the group is marked without one (the walk
+// then takes its chunks).  Sizes below 2^53 per chunk keep the int64 sums
+// exact; a usable run never needs more (its partial sums span < 2^52).
+__device__ void xs_group_summary(const XsSum& s, const XsGeom& g, int ty) {
+  const int lane = threadIdx.x & 31;
+  int j0, j1;
+  xs_group_range(s, g, ty, j0, j1);
+  const int ef0 = __ldcg(s.ef + j0);
+  const long long lim = 1ll << 53;
+  long long carry = 0, mn = 0x7fffffffffffffffll, mx = -0x7fffffffffffffffll - 1;
+  bool ok = (ef0 & kXsValid) && !(ef0 & kXsTie);
+  for (int jb = j0; jb < j1 && ok; jb += 32) {
+    const int j = jb + lane;
+    const bool in = j < j1;
+    const int ef = in ? __ldcg(s.ef + j) : ef0;
+    const long long X = in ? __ldcg(s.X + j) : 0;
+    const long long lo = in ? __ldcg(s.mnB + j) : 0, hi = in ? __ldcg(s.mxB + j) : 0;
+    const bool bad = in && (!(ef & kXsValid) || (ef & kXsTie) || xs_exp(ef) != xs_exp(ef0) || X >= lim ||
+                            X <= -lim || lo >= lim || lo <= -lim || hi >= lim || hi <= -lim);
+    if (__any_sync(0xffffffffu, bad)) {
+      ok = false;
+      break;
+    }
+    long long inc = X;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += t;
+    }
+    const long long P = carry + inc - X;   // partial c-sum at this chunk's start
+    long long a = in ? P + lo : 0x7fffffffffffffffll, b = in ? P + hi : -0x7fffffffffffffffll - 1;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const long long ta = __shfl_xor_sync(0xffffffffu, a, o), tb = __shfl_xor_sync(0xffffffffu, b, o);
+      a = ta < a ? ta : a;
+      b = tb > b ? tb : b;
+    }
+    mn = a < mn ? a : mn;
+    mx = b > mx ? b : mx;
+    carry += __shfl_sync(0xffffffffu, inc, 31);
+  }
+  if (lane == 0) {
+    __stcg(s.gX + ty, carry);
+    __stcg(s.gmn + ty, mn);
+    __stcg(s.gmx + ty, mx);
+    __stcg(s.gef + ty, xs_pack(xs_exp(ef0), ok ? kXsValid : 0));
+  }
+}
+
+// The sequential sum 0 + t_0 + t_1 + ... of one sum, by one warp (every lane
+// returns it): 32 chunk groups at a time from their summaries (a prefix sum
+// over the lanes gives the mantissa at every group start), a group without
+// a usable summary or whose partial sums leave the binade by its chunks
+// (xs_walk_chunks).  Needs the summaries of every chunk and group.
+__device__ double xs_drive(const XsSum& s, const XsGeom& g, unsigned long long* prof) {
+  const long long t_start = clock64();
+  XsWalkCount wc{0, 0, 0};
+  const int lane = threadIdx.x & 31;
+  const int ng = g.ny;
+  double S = 0.0;
+  int q = 0;
+  auto load = [&](int qn, int& ef, long long& X, long long& lo, long long& hi) {
+    const bool in = qn < ng;
+    ef = in ? __ldcg(s.gef + qn) : 0;
+    X = in ? __ldcg(s.gX + qn) : 0;
+    lo = in ? __ldcg(s.gmn + qn) : 0;
+    hi = in ? __ldcg(s.gmx + qn) : 0;
+  };
+  int nef;
+  long long nX, nlo, nhi;
+  load(lane, nef, nX, nlo, nhi);
+  for (int qb = 0; qb < ng && !isnan(S); qb += 32) {
+    const bool in = qb + lane < ng;
+    const int ef = nef;
+    const long long X = nX, lo = nlo, hi = nhi;
+    load(qb + lane + 32, nef, nX, nlo, nhi);
+    while (q < qb + 32 && q < ng) {
+      if (isnan(S)) break;
+      int E;
+      long long m;
+      int first = q - qb;
+      if (xs_split(S, E, m)) {
+        const bool neg = m < 0;
+        const int o = q - qb;
+        const bool act = lane >= o && in;
+        const bool use = act && (ef & kXsValid) && xs_exp(ef) == E;
+        const unsigned long long delta = use ? (unsigned long long)X : 0ull;
+        unsigned long long inc = delta;
+#pragma unroll
+        for (int o2 = 1; o2 < 32; o2 <<= 1) {
+          const unsigned long long tt = __shfl_up_sync(0xffffffffu, inc, o2);
+          if (lane >= o2) inc += tt;
+        }
+        const long long mi = m + (long long)(inc - delta);   // mantissa at this group's start
+        const bool good = use && xs_in_range(mi + lo, neg) && xs_in_range(mi + hi, neg);
+        const unsigned bad = __ballot_sync(0xffffffffu, act && !good);
+        const int last = (ng - qb < 32 ? ng - qb : 32);
+        first = bad ? __ffs(bad) - 1 : last;
+        const long long mf = __shfl_sync(0xffffffffu, mi + (long long)delta, (first > 0 ? first : 1) - 1);
+        if (first > o) S = (double)mf * xs_pow2(E);
+      }
+      q = qb + first;
+      if (q < qb + 32 && q < ng) {
+        int j0, j1;
+        xs_group_range(s, g, q, j0, j1);
+        S = xs_walk_chunks(s, g, j0, j1, S, wc);
+        ++q;
+      }
+    }
+  }
+  if (prof && lane == 0) {
+    atomicAdd(prof + 4, wc.chunks);
+    atomicAdd(prof + 5, wc.slow);
+    atomicAdd(prof + 6, wc.slow_cycles);
     atomicAdd(prof + 7, (unsigned long long)(clock64() - t_start));
   }
   return S;
@@ -482,7 +639,6 @@ __device__ __forceinline__ double xs_block_excl(double v, double* wtot /* [8] sh
 // 2 (xs_summary_row, a pass of its own spread over the grid): the chunk
 // summaries at the predicted exponents, one chunk per thread.  3 (xs_walk,
 // the CTA that completed step 2): one warp per sum walks its chunks in order.
-constexpr int kXsTilesPerTask = 256 / kXsBR;   // term blocks per task tile of step 2 (9 rows each)
 
 // Profile counters (nullable): [0] passes, [1..3] cycles of the steps,
 // [4] chunks walked, [5] chunks added term by term.
@@ -552,7 +708,7 @@ __device__ __noinline__ void xs_summary_row(const XsSum& s, const XsGeom& g, int
   const int j = y * g.nx + tx;
   long long X, R, lo, hi, loA, hiA;
   int ef;
-  xs_summarise(xs_block(s, t) + r, kXsBR, len, __ldcg(s.ef + j), X, R, lo, hi, loA, hiA, ef);
+  xs_summarise(xs_block(s, t) + xs_at(0, r), 1, len, __ldcg(s.ef + j), X, R, lo, hi, loA, hiA, ef);
   __stcg(s.X + j, X);
   __stcg(s.R + j, R);
   __stcg(s.mnB + j, lo);
@@ -562,10 +718,42 @@ __device__ __noinline__ void xs_summary_row(const XsSum& s, const XsGeom& g, int
   __stcg(s.ef + j, ef);
 }
 
-// Task tiles of the summary pass.
+// Tile rows of chunk summaries per task tile of the summary pass (every
+// thread one chunk row of a term block, nx blocks per tile row), and the task
+// tiles of ns sums.
+__host__ __device__ inline int xs_rows_per_task(const XsGeom& g) {
+  const int r = 256 / (g.nx * kXsBR);
+  return r < 1 ? 1 : r;
+}
 __host__ __device__ inline int xs_summary_tasks(int ns, int n) {
   const XsGeom g(n);
-  return (ns * g.nx * g.ny + kXsTilesPerTask - 1) / kXsTilesPerTask;
+  const int rt = xs_rows_per_task(g);
+  return (ns * g.ny + rt - 1) / rt;
+}
+
+// Step 2, task tile `task` (the whole CTA of 256 threads, every thread
+// calls): the chunk summaries of its tile rows (groups), then the group
+// summaries, one warp per group.  sum(k) gives sum k of the pass.
+template <class SumOf>
+__device__ void xs_summary_task(SumOf&& sum, int ns, const XsGeom& g, int task) {
+  const int rt = xs_rows_per_task(g);
+  const int q0 = task * rt;
+  int nq = ns * g.ny - q0;
+  nq = nq < rt ? nq : rt;
+  const int per = g.nx * kXsBR;
+  for (int job = threadIdx.x; job < nq * per; job += blockDim.x) {
+    const int q = q0 + job / per, rem = job - (job / per) * per;
+    const int k = q / g.ny, ty = q - k * g.ny;
+    xs_summary_row(sum(k), g, ty * g.nx + rem / kXsBR, rem % kXsBR);
+  }
+  __threadfence();
+  __syncthreads();
+  for (int w = threadIdx.x >> 5; w < nq; w += blockDim.x >> 5) {
+    const int q = q0 + w, k = q / g.ny;
+    xs_group_summary(sum(k), g, q - k * g.ny);
+  }
+  __threadfence();
+  __syncthreads();
 }
 
 // Step 3: out[k] = the sequential sum k (one warp per sum).
