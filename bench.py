@@ -156,6 +156,8 @@ def level_traffic(fp64: bool):
     try:
         d = json.load(open(os.path.join(ROOT, "profiles", "level_kernel_traffic.json")))
         key = ("f64" if fp64 else "f32") + ("_ncc" if DATA_TERM else "")
+        if key == "f64" and SUM_ORDER == 0:
+            key = "f64_exact"   # the reference's sum order: terms stored for the ordered sums
         return d.get(key, {}).get("bytes_per_launch_513x20")
     except Exception:
         return None
