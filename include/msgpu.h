@@ -528,6 +528,11 @@ long long msgpu_net_num_params(void);
 int msgpu_net_create(msgpu_context* ctx, int input_level, unsigned long long seed, msgpu_net** out);
 int msgpu_net_destroy(msgpu_net* net);
 int msgpu_net_input_level(const msgpu_net* net);
+/* Forward convolutions on the fifth-generation tensor cores (tcgen05.mma,
+ * TMEM accumulators; default 1) or on mma.sync (0).  The data-gradient and
+ * weight-gradient convolutions of training use mma.sync either way; the two
+ * forward paths differ only in the order of the fp32 accumulation.         */
+int msgpu_net_set_tensor_cores(msgpu_net* net, int tcgen05);
 int msgpu_net_get_params(msgpu_net* net, float* out);
 int msgpu_net_set_params(msgpu_net* net, const float* in);   /* resets Adam */
 int msgpu_net_save(msgpu_net* net, const char* path);

@@ -30,6 +30,7 @@
 #include "msgpu_series.cuh"
 #include "msgpu_seismic.cuh"
 #include "msgpu_unet.cuh"
+#include "msgpu_tc.cuh"
 
 using namespace msg;
 
@@ -793,20 +794,21 @@ int sched_error_reset(msgpu_context* ctx, cudaStream_t st) {
     if ((rc = ensure(ctx, ctx->flags, 256))) return rc;
     ctx->sched_error = (int*)ctx->flags.p;
   }
-  CK(cudaMemsetAsync(ctx->sched_error, 0, 3 * sizeof(int), st));
+  CK(cudaMemsetAsync(ctx->sched_error, 0, 4 * sizeof(int), st));
   return MSGPU_OK;
 }
 
 // After the call's work has completed: reports a kernel that gave up waiting
 // and input images holding NaN or Inf (word 2, set by k_finite_check).
 int sched_error_check(msgpu_context* ctx) {
-  int h[3] = {0, 0, 0};
+  int h[4] = {0, 0, 0, 0};
   if (!ctx->sched_error) return MSGPU_OK;
   CK(cudaMemcpy(h, ctx->sched_error, sizeof(h), cudaMemcpyDeviceToHost));
   if (h[0] == 2) return fail(ctx, MSGPU_ERR_CUDA, "level kernel: exact-sum bookkeeping failed (no free term buffer)");
   if (h[0]) return fail(ctx, MSGPU_ERR_CUDA, "level kernel: a worker waited too long for work (scheduler stalled)");
   if (h[1]) return fail(ctx, MSGPU_ERR_CUDA, "composition: a grid-barrier wait timed out");
   if (h[2]) return fail(ctx, MSGPU_ERR_INVALID_ARG, "an input image holds a non-finite value (NaN or Inf)");
+  if (h[3]) return fail(ctx, MSGPU_ERR_CUDA, "tensor-core convolution: a wait for the tensor core timed out");
   return MSGPU_OK;
 }
 
@@ -3678,6 +3680,7 @@ struct msgpu_net {
   View x0, a0, a1, b0, cat1, c0, cat2, d0, d1, g0, g1, h0, h1;
   View dout, dh1, dh0, dcat1, dg1, dg0, dcat2, dd1, dd0, dc0, db0, da1, da0;
   float* out = nullptr;                  // head output, 2 floats per node of grid 1
+  bool tcgen05 = true;                   // forward convolutions on tcgen05 (else mma.sync)
 };
 
 namespace {
@@ -3758,11 +3761,86 @@ int net_kernel_attrs(msgpu_context* ctx) {
                           (int)u::conv_halo_smem_bytes<64, 16, 2>()));
   CK(cudaFuncSetAttribute(u::k_conv_halo<32, 32, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)u::conv_halo_smem_bytes<32, 32, 2>()));
+  CK(cudaFuncSetAttribute(u::k_conv_tc<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)u::conv_tc_smem_bytes<16>()));
+  CK(cudaFuncSetAttribute(u::k_conv_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)u::conv_tc_smem_bytes<32>()));
+  CK(cudaFuncSetAttribute(u::k_conv_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)u::conv_tc_smem_bytes<64>()));
+  CK(cudaFuncSetAttribute(u::k_conv_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)u::conv_tc_smem_bytes<128>()));
+  const int row_max = 200 * 1024;
+  CK(cudaFuncSetAttribute(u::k_conv_row_tc<16, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, row_max));
+  CK(cudaFuncSetAttribute(u::k_conv_row_tc<32, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, row_max));
+  CK(cudaFuncSetAttribute(u::k_conv_row_tc<64, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, row_max));
+  CK(cudaFuncSetAttribute(u::k_conv_row_tc<128, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, row_max));
+  CK(cudaFuncSetAttribute(u::k_conv_row_tc<16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, row_max));
+  CK(cudaFuncSetAttribute(u::k_conv_row_tc<32, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, row_max));
+  CK(cudaFuncSetAttribute(u::k_conv_row_tc<64, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, row_max));
+  CK(cudaFuncSetAttribute(u::k_conv_row_tc<128, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, row_max));
   return MSGPU_OK;
+}
+
+// Launches the row-tiled tensor-core convolution: the channel group G is the
+// largest of 64, 48, 32, 16 dividing cin whose two shared-memory slots fit
+// two CTAs per SM (else one); persistent CTAs over the row tiles.
+template <int BN, int S>
+void net_launch_row_tc(const msg::unet::ConvArgs& a, int rows, int sms, int* err, cudaStream_t st) {
+  namespace u = msg::unet;
+  int G = 16;
+  size_t smem = u::row_tc_smem<BN, S>(16);
+  for (int pass = 0; pass < 2; ++pass) {
+    const size_t cap = pass == 0 ? 110 * 1024 : 200 * 1024;
+    bool found = false;
+    for (int g : {64, 48, 32, 16}) {
+      if (a.cin % g || u::row_tc_smem<BN, S>(g) > cap) continue;
+      G = g;
+      smem = u::row_tc_smem<BN, S>(g);
+      found = true;
+      break;
+    }
+    if (found) break;
+  }
+  // CTAs per SM: by shared memory and by TMEM (512 columns)
+  const int per_sm = std::max(1, std::min((int)((227 * 1024) / (smem + 1024)), 512 / u::tc_cols<BN>()));
+  const int segs = (a.out_n + u::kTcBM - 1) / u::kTcBM;
+  const int tiles = (a.total / (a.out_n * a.out_n)) * a.out_n * segs;
+  const int ny = rows / BN;
+  const int gx = std::max(1, std::min(tiles, (sms * per_sm + ny - 1) / ny));
+  u::k_conv_row_tc<BN, S><<<dim3((unsigned)gx, (unsigned)ny), 128, smem, st>>>(a, G, err);
 }
 
 int net_conv_launch(msgpu_net* net, const msg::unet::ConvArgs& a, int rows, cudaStream_t st) {
   const int bn = tile_of(rows);
+  if (net->tcgen05 && a.mode == 0) {
+    // forward convolutions on the tensor cores: 128 nodes x up to 128 channels per tile
+    namespace u = msg::unet;
+    int rc;
+    if (!net->ctx->sched_error && (rc = sched_error_reset(net->ctx, st))) return rc;
+    const int tb = rows % 128 == 0 ? 128 : bn;
+    int* err = net->ctx->sched_error + 3;
+    const int sms = net->ctx->sm_count;
+    if (a.stride == 1) {
+      if (tb == 128) net_launch_row_tc<128, 1>(a, rows, sms, err, st);
+      else if (tb == 64) net_launch_row_tc<64, 1>(a, rows, sms, err, st);
+      else if (tb == 32) net_launch_row_tc<32, 1>(a, rows, sms, err, st);
+      else net_launch_row_tc<16, 1>(a, rows, sms, err, st);
+    } else if (a.stride == 2) {
+      if (tb == 128) net_launch_row_tc<128, 2>(a, rows, sms, err, st);
+      else if (tb == 64) net_launch_row_tc<64, 2>(a, rows, sms, err, st);
+      else if (tb == 32) net_launch_row_tc<32, 2>(a, rows, sms, err, st);
+      else net_launch_row_tc<16, 2>(a, rows, sms, err, st);
+    } else {
+      const dim3 grid((unsigned)((a.total + u::kTcBM - 1) / u::kTcBM), (unsigned)(rows / tb));
+      if (tb == 128) u::k_conv_tc<128><<<grid, 128, u::conv_tc_smem_bytes<128>(), st>>>(a, err);
+      else if (tb == 64) u::k_conv_tc<64><<<grid, 128, u::conv_tc_smem_bytes<64>(), st>>>(a, err);
+      else if (tb == 32) u::k_conv_tc<32><<<grid, 128, u::conv_tc_smem_bytes<32>(), st>>>(a, err);
+      else u::k_conv_tc<16><<<grid, 128, u::conv_tc_smem_bytes<16>(), st>>>(a, err);
+    }
+    NCK(cudaGetLastError());
+    ++net->ctx->stats.kernel_launches;
+    return MSGPU_OK;
+  }
   if (a.stride == 1 && (a.cin == 16 || a.cin == 32)) {
     // narrow stride-1 layers: every input node fetched once through a halo tile
     const int images = a.total / (a.out_n * a.out_n);
@@ -4195,6 +4273,12 @@ int msgpu_net_destroy(msgpu_net* net) {
 
 int msgpu_net_input_level(const msgpu_net* net) { return net ? net->level : -1; }
 
+int msgpu_net_set_tensor_cores(msgpu_net* net, int tcgen05) {
+  if (!net) return MSGPU_ERR_INVALID_ARG;
+  net->tcgen05 = tcgen05 != 0;
+  return MSGPU_OK;
+}
+
 int msgpu_net_get_params(msgpu_net* net, float* out) {
   if (!net || !out) return MSGPU_ERR_INVALID_ARG;
   int rc;
@@ -4283,6 +4367,7 @@ int msgpu_net_loss_grad(msgpu_net* net, const double* R, const double* T, const 
   msgpu_context* ctx = net->ctx;
   const cudaStream_t st = ctx->stream;
   const size_t N0 = (size_t)net->n[0] * net->n[0], N1 = (size_t)net->n[1] * net->n[1];
+  if ((rc = sched_error_reset(ctx, st))) return rc;
   if ((rc = ensure(ctx, ctx->io[0], sizeof(double) * (2 * N0 + 2 * N1) * batch))) return rc;
   double* d = (double*)ctx->io[0].p;
   CK(cudaMemcpyAsync(d, R, sizeof(double) * N0 * batch, cudaMemcpyHostToDevice, st));
@@ -4296,7 +4381,7 @@ int msgpu_net_loss_grad(msgpu_net* net, const double* R, const double* T, const 
   if (phi_out) CK(cudaMemcpyAsync(phi_out, phi, sizeof(double) * 2 * N1 * batch, cudaMemcpyDeviceToHost, st));
   if (grad_out) CK(cudaMemcpyAsync(grad_out, net->grad, sizeof(float) * net->nparams, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
-  return MSGPU_OK;
+  return sched_error_check(ctx);
 }
 
 int msgpu_prepare_images_device(msgpu_context* ctx, const msgpu_params* p, const double* d_images, int count,

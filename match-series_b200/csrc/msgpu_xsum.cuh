@@ -148,10 +148,11 @@ __device__ __forceinline__ bool xs_split(double S, int& E, long long& m) {
   return true;
 }
 
-// Packed exponent and flags of a chunk summary: bit 0 valid, bit 1 tie.
-constexpr int kXsValid = 1, kXsTie = 2;
-__device__ __forceinline__ int xs_pack(int E, int flags) { return ((E + 2048) << 2) | flags; }
-__device__ __forceinline__ int xs_exp(int ef) { return (ef >> 2) - 2048; }
+// Packed exponent and flags of a chunk summary: bit 0 valid, bit 1 tie,
+// bit 2 zero: every term of the chunk (group) is +0 or -0.
+constexpr int kXsValid = 1, kXsTie = 2, kXsZero = 4;
+__device__ __forceinline__ int xs_pack(int E, int flags) { return ((E + 2048) << 3) | flags; }
+__device__ __forceinline__ int xs_exp(int ef) { return (ef >> 3) - 2048; }
 constexpr int kXsNoExp = 0;   // no prediction: xs_exp gives -2048, never a valid exponent
 
 // Summary of one chunk (len terms at p[0], p[step], ...) for a running sum
@@ -167,11 +168,16 @@ __device__ __forceinline__ void xs_summarise(const double* p, int step, int len,
   const int E = xs_exp(ef);
   X = R = mnA = mxA = 0;
   mnB = mxB = 0;
-  if (E < -1000 || E > 1000) { out_ef = xs_pack(E < -2000 ? -2000 : E, 0); return; }
+  if (E < -1000 || E > 1000) {
+    bool zero = true;
+    for (int k = 0; k < len; ++k) zero = zero && __ldcg(p + (size_t)k * step) == 0.0;
+    out_ef = xs_pack(E < -2000 ? -2000 : E, zero ? kXsZero : 0);
+    return;
+  }
   const double sc = xs_pow2(-E);
   long long P = 0, r = 0, lo = 0x7fffffffffffffffll, hi = -0x7fffffffffffffffll - 1;
   long long loA = 0, hiA = 0;
-  bool tie = false, ok = true;
+  bool tie = false, ok = true, zero = true;
   for (int k0 = 0; k0 < len; k0 += 8) {
     double v[8];
 #pragma unroll
@@ -179,6 +185,7 @@ __device__ __forceinline__ void xs_summarise(const double* p, int step, int len,
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
       if (k0 + i >= len) break;
+      zero = zero && v[i] == 0.0;
       const double q = v[i] * sc;
       if (!(fabs(q) < 36028797018963968.0)) {   // |q| < 2^55 (NaN and Inf fail too)
         ok = false;
@@ -213,7 +220,7 @@ __device__ __forceinline__ void xs_summarise(const double* p, int step, int len,
   mxB = hi;
   mnA = loA;
   mxA = hiA;
-  out_ef = xs_pack(E, (ok ? kXsValid : 0) | (tie ? kXsTie : 0));
+  out_ef = xs_pack(E, (ok ? kXsValid : 0) | (tie ? kXsTie : 0) | (zero ? kXsZero : 0));
 }
 
 // Chunk j of a sum: its tile, row within the tile and length.
@@ -409,6 +416,11 @@ __device__ double xs_walk_chunks(const XsSum& s, const XsGeom& g, int j0, int j1
       int E;
       long long m;
       if (!xs_split(S, E, m)) {
+        // +0 plus a chunk of zeros stays +0
+        if (__double_as_longlong(S) == 0 && (__shfl_sync(0xffffffffu, ef, j - jb) & kXsZero)) {
+          ++j;
+          continue;
+        }
         const long long ts = clock64();
         if (j - jb == pf) {
           S = xs_add_terms(S, pt);
@@ -508,6 +520,11 @@ __device__ void xs_group_summary(const XsSum& s, const XsGeom& g, int ty) {
   const long long lim = 1ll << 53;
   long long carry = 0, mn = 0x7fffffffffffffffll, mx = -0x7fffffffffffffffll - 1;
   bool ok = (ef0 & kXsValid) && !(ef0 & kXsTie);
+  bool zero = true;
+  for (int jb = j0; jb < j1; jb += 32) {
+    const int j = jb + lane;
+    zero = zero && __all_sync(0xffffffffu, j >= j1 || (__ldcg(s.ef + j) & kXsZero));
+  }
   for (int jb = j0; jb < j1 && ok; jb += 32) {
     const int j = jb + lane;
     const bool in = j < j1;
@@ -542,7 +559,7 @@ __device__ void xs_group_summary(const XsSum& s, const XsGeom& g, int ty) {
     __stcg(s.gX + ty, carry);
     __stcg(s.gmn + ty, mn);
     __stcg(s.gmx + ty, mx);
-    __stcg(s.gef + ty, xs_pack(xs_exp(ef0), ok ? kXsValid : 0));
+    __stcg(s.gef + ty, xs_pack(xs_exp(ef0), (ok ? kXsValid : 0) | (zero ? kXsZero : 0)));
   }
 }
 
@@ -578,6 +595,11 @@ __device__ double xs_drive(const XsSum& s, const XsGeom& g, unsigned long long* 
       int E;
       long long m;
       int first = q - qb;
+      // +0 plus a group of zeros stays +0
+      if (__double_as_longlong(S) == 0 && (__shfl_sync(0xffffffffu, ef, q - qb) & kXsZero)) {
+        ++q;
+        continue;
+      }
       if (xs_split(S, E, m)) {
         const bool neg = m < 0;
         const int o = q - qb;

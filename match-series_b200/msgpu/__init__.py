@@ -101,7 +101,7 @@ EXPORTS = [
     "msgpu_write_displacement", "msgpu_read_arrays_start", "msgpu_io_wait", "msgpu_register_ragged",
     "msgpu_register_ragged_device", "msgpu_lineshift_energy", "msgpu_lineshift_energy_device", "msgpu_xshift_reg",
     "msgpu_xshift_reg_device", "msgpu_find_xshift", "msgpu_find_xshift_device", "msgpu_find_xshift_batch",
-    "msgpu_net_num_params", "msgpu_net_create", "msgpu_net_destroy", "msgpu_net_input_level", "msgpu_net_get_params",
+    "msgpu_net_num_params", "msgpu_net_create", "msgpu_net_destroy", "msgpu_net_input_level", "msgpu_net_set_tensor_cores", "msgpu_net_get_params",
     "msgpu_net_set_params", "msgpu_net_save", "msgpu_net_load", "msgpu_net_predict_device",
     "msgpu_net_train_step_device", "msgpu_net_loss_grad", "msgpu_prepare_images_device", "msgpu_register_batch_warm",
     "msgpu_register_batch_warm_device", "msgpu_find_xshift_yconst", "msgpu_find_xshift_yconst_device",
@@ -192,6 +192,7 @@ def lib():
         L.msgpu_net_create.argtypes = [_v, ctypes.c_int, ctypes.c_ulonglong, ctypes.POINTER(_v)]
         L.msgpu_net_destroy.argtypes = [_v]
         L.msgpu_net_input_level.argtypes = [_v]
+        L.msgpu_net_set_tensor_cores.argtypes = [_v, ctypes.c_int]
         L.msgpu_net_get_params.argtypes = [_v, _fp]
         L.msgpu_net_set_params.argtypes = [_v, _fp]
         L.msgpu_net_save.argtypes = [_v, ctypes.c_char_p]
@@ -814,6 +815,10 @@ class Net:
             self.close()
         except Exception:
             pass
+
+    def set_tensor_cores(self, on: bool):
+        """Forward convolutions on tcgen05 (default) or on mma.sync."""
+        self.ctx._check(lib().msgpu_net_set_tensor_cores(self._h, int(bool(on))))
 
     def get_params(self):
         out = np.zeros(self.num_params(), dtype=np.float32)
