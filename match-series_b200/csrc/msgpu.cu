@@ -3778,7 +3778,77 @@ int net_kernel_attrs(msgpu_context* ctx) {
   CK(cudaFuncSetAttribute(u::k_conv_row_tc<32, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, row_max));
   CK(cudaFuncSetAttribute(u::k_conv_row_tc<64, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, row_max));
   CK(cudaFuncSetAttribute(u::k_conv_row_tc<128, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, row_max));
+  const int tma_max = 200 * 1024 + 1024 + 128;
+  CK(cudaFuncSetAttribute(u::k_conv_row_tma<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, tma_max));
+  CK(cudaFuncSetAttribute(u::k_conv_row_tma<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, tma_max));
+  CK(cudaFuncSetAttribute(u::k_conv_row_tma<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, tma_max));
+  CK(cudaFuncSetAttribute(u::k_conv_row_tma<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, tma_max));
   return MSGPU_OK;
+}
+
+// The driver's tensor-map encoder, found through the runtime (no link
+// dependency on the driver library); null when the driver does not offer it.
+typedef CUresult (*TmapEncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+TmapEncodeFn tmap_encoder() {
+  static TmapEncodeFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<TmapEncodeFn>(p);
+  }
+  return fn;
+}
+
+// Stride-1 forward convolution on tcgen05 with TMA-fed operands: tensor maps
+// over the input view (channels, x, y, image; out-of-grid boxes filled with
+// zeros) and over the weight matrix (K, rows).  false: not launched (no
+// encoder, or a map the encoder refuses).
+template <int BN>
+bool net_launch_row_tma(const msg::unet::ConvArgs& a, int rows, int sms, int* err, cudaStream_t st) {
+  namespace u = msg::unet;
+  const TmapEncodeFn enc = tmap_encoder();
+  if (!enc) return false;
+  int G = 0;
+  for (int pass = 0; pass < 2 && !G; ++pass) {
+    const size_t cap = pass == 0 ? 110 * 1024 : 200 * 1024;
+    for (int g : {64, 48, 32, 16})
+      if (a.cin % g == 0 && u::row_tma_smem(BN, g) <= cap) { G = g; break; }
+  }
+  if (!G) return false;
+  const size_t smem = u::row_tma_smem(BN, G);
+  const int R = u::row_tc_rows(BN);
+  const int images = a.total / (a.out_n * a.out_n);
+  CUtensorMap tin, tw;
+  const cuuint64_t gd[4] = {(cuuint64_t)a.cin, (cuuint64_t)a.in_n, (cuuint64_t)a.in_n, (cuuint64_t)images};
+  const cuuint64_t gs[3] = {(cuuint64_t)a.in_cs * 2, (cuuint64_t)a.in_n * a.in_cs * 2, (cuuint64_t)a.in_img * 2};
+  const cuuint32_t box[4] = {8, 130, (cuuint32_t)(R + 2), 1};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  if (enc(&tin, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void*)a.in, gd, gs, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
+      CUDA_SUCCESS)
+    return false;
+  const cuuint64_t K = (cuuint64_t)9 * a.cin;
+  const cuuint64_t wd[2] = {K, (cuuint64_t)rows};
+  const cuuint64_t ws[1] = {K * 2};
+  const cuuint32_t wbox[2] = {8, (cuuint32_t)BN};
+  const cuuint32_t wes[2] = {1, 1};
+  if (enc(&tw, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)a.w, wd, ws, wbox, wes, CU_TENSOR_MAP_INTERLEAVE_NONE,
+          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
+      CUDA_SUCCESS)
+    return false;
+  const int per_sm = std::max(1, std::min((int)((227 * 1024) / (smem + 1024)), 512 / u::row_tma_cols<BN>()));
+  const int segs = (a.out_n + u::kTcBM - 1) / u::kTcBM;
+  const int tiles = images * ((a.out_n + R - 1) / R) * segs;
+  const int ny = rows / BN;
+  const int gx = std::max(1, std::min(tiles, (sms * per_sm + ny - 1) / ny));
+  u::k_conv_row_tma<BN><<<dim3((unsigned)gx, (unsigned)ny), u::kRowTmaThreads, smem, st>>>(a, G, err, tin, tw);
+  return true;
 }
 
 // Launches the row-tiled tensor-core convolution: the channel group G is the
@@ -3802,9 +3872,10 @@ void net_launch_row_tc(const msg::unet::ConvArgs& a, int rows, int sms, int* err
     if (found) break;
   }
   // CTAs per SM: by shared memory and by TMEM (512 columns)
-  const int per_sm = std::max(1, std::min((int)((227 * 1024) / (smem + 1024)), 512 / u::tc_cols<BN>()));
+  const int per_sm = std::max(1, std::min((int)((227 * 1024) / (smem + 1024)), 512 / u::row_tc_cols<BN>()));
   const int segs = (a.out_n + u::kTcBM - 1) / u::kTcBM;
-  const int tiles = (a.total / (a.out_n * a.out_n)) * a.out_n * segs;
+  const int R = u::row_tc_rows(BN);
+  const int tiles = (a.total / (a.out_n * a.out_n)) * ((a.out_n + R - 1) / R) * segs;
   const int ny = rows / BN;
   const int gx = std::max(1, std::min(tiles, (sms * per_sm + ny - 1) / ny));
   u::k_conv_row_tc<BN, S><<<dim3((unsigned)gx, (unsigned)ny), 128, smem, st>>>(a, G, err);
@@ -3812,15 +3883,27 @@ void net_launch_row_tc(const msg::unet::ConvArgs& a, int rows, int sms, int* err
 
 int net_conv_launch(msgpu_net* net, const msg::unet::ConvArgs& a, int rows, cudaStream_t st) {
   const int bn = tile_of(rows);
-  if (net->tcgen05 && a.mode == 0) {
-    // forward convolutions on the tensor cores: 128 nodes x up to 128 channels per tile
+  // forward convolutions on tcgen05 where it measured faster (B200, 8 pairs
+  // at 1025^2): stride 1 with 16 input channels, or with 64 and more input
+  // channels and at most 64 output rows; stride 2, the 32-channel layers and
+  // the 128-row layer (whose 129-node rows leave half of its second tile
+  // empty) run on the mma.sync kernels below
+  if (net->tcgen05 && a.mode == 0 && a.stride == 1 && (a.cin == 16 || (a.cin >= 64 && rows <= 64))) {
     namespace u = msg::unet;
     int rc;
     if (!net->ctx->sched_error && (rc = sched_error_reset(net->ctx, st))) return rc;
     const int tb = rows % 128 == 0 ? 128 : bn;
     int* err = net->ctx->sched_error + 3;
     const int sms = net->ctx->sm_count;
+    bool tma = false;
     if (a.stride == 1) {
+      if (tb == 128) tma = net_launch_row_tma<128>(a, rows, sms, err, st);
+      else if (tb == 64) tma = net_launch_row_tma<64>(a, rows, sms, err, st);
+      else if (tb == 32) tma = net_launch_row_tma<32>(a, rows, sms, err, st);
+      else tma = net_launch_row_tma<16>(a, rows, sms, err, st);
+    }
+    if (tma) {
+    } else if (a.stride == 1) {
       if (tb == 128) net_launch_row_tc<128, 1>(a, rows, sms, err, st);
       else if (tb == 64) net_launch_row_tc<64, 1>(a, rows, sms, err, st);
       else if (tb == 32) net_launch_row_tc<32, 1>(a, rows, sms, err, st);
