@@ -109,6 +109,15 @@ int  msgpu_set_sum_order(msgpu_context* ctx, int sum_order);
  * either way; on costs six term buffers per instance (at most 16 GiB,
  * beyond that one).  Off: every pass's sums are added in order.            */
 int  msgpu_set_certified_steps(msgpu_context* ctx, int on);
+/* findXShift's descent control (msgpu_find_xshift{,_device,_batch}) on the
+ * device (1): the descent is captured once into a CUDA graph whose step loop
+ * and Armijo searches are conditional while nodes and whose fallback attempt
+ * and energy re-evaluation are conditional if nodes, the decisions taken by
+ * one-thread kernels from the sums on the device -- one graph launch per
+ * descent.  0 (default): the same control on the host, measured faster on
+ * B200.  The two take the same decisions in the same double arithmetic:
+ * identical results.                                                       */
+int  msgpu_set_seismic_device_control(msgpu_context* ctx, int on);
 int  msgpu_destroy(msgpu_context* ctx);
 const char* msgpu_last_error(const msgpu_context* ctx);
 

@@ -73,6 +73,8 @@ struct msgpu_context {
   // seismic line-shift solve: the spectral basis of its H1 metric
   int xs_nx = 0, xs_ny = 0;
   Buf xs_basis, xs_work;
+  cudaStream_t xc_stream[4] = {nullptr, nullptr, nullptr, nullptr};   // capture streams of the findXShift graph
+  bool xs_device_control = false;                             // findXShift as a device-controlled graph
   std::vector<msgpu_context*> workers;   // contexts of the batch workers (own streams and buffers)
 };
 
@@ -1769,6 +1771,12 @@ int msgpu_set_sum_order(msgpu_context* ctx, int sum_order) {
   return MSGPU_OK;
 }
 
+int msgpu_set_seismic_device_control(msgpu_context* ctx, int on) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  ctx->xs_device_control = on != 0;
+  return MSGPU_OK;
+}
+
 int msgpu_set_certified_steps(msgpu_context* ctx, int on) {
   if (!ctx) return MSGPU_ERR_INVALID_ARG;
   ctx->certified = on != 0;
@@ -1812,6 +1820,8 @@ int msgpu_destroy(msgpu_context* ctx) {
                                 &ctx->ext,   &ctx->series,  &ctx->vals,  &ctx->xs_basis, &ctx->xs_work,
                                 &ctx->xsum,  &ctx->xpart};
   if (ctx->graph.exec) cudaGraphExecDestroy(ctx->graph.exec);
+  for (auto& xs : ctx->xc_stream)
+    if (xs) cudaStreamDestroy(xs);
   if (ctx->graph_stream) cudaStreamDestroy(ctx->graph_stream);
   for (auto* b : bufs)
     if (b->p) cudaFree(b->p);
@@ -2542,6 +2552,378 @@ int run_xshift(msgpu_context* ctx, int nx, int ny, const double* R, const double
   if (steps_out) *steps_out = iter;
   return MSGPU_OK;
 }
+
+// ---------------------------------------------------------------------------
+// findXShift with the descent control on the device: the same steps as
+// run_xshift, captured once into a CUDA graph whose loops and branches are
+// conditional nodes (the outer step loop and each Armijo search as while
+// nodes, the fallback attempt and the energy at the new position as if
+// nodes).  One-thread control kernels take every decision from the sums the
+// vector kernels leave on the device, in the same double arithmetic as the
+// host control, and set the conditions; the vector kernels read their
+// scalars (trial step, Fletcher-Reeves factor, filter width) from memory.
+// A descent is one graph launch instead of ~4,000 launches and ~3,000 host
+// round trips.  Measured on B200 (driver 580) it is the slower of the two:
+// the nodes of conditional bodies cost ~7.7 us each, more than the host round
+// trips they replace, so the host control stays the default.
+struct XsCtl {
+  double tau, sigma, energy, energy_new, f, fnew, Df, tau_ls, tw, result, beta, e_at_pos, enew;
+  double rb_tau[2], rb_e[2];
+  int rb_pos, iter, mode, go, ls_steps, guard;
+};
+constexpr double kXcTauMin = 9.313225746154785e-10;   // 2^-30 (ArmijoSearch.h:77)
+constexpr double kXcTauMax = 33554432.0;              // 2^25  (ArmijoSearch.h:67)
+
+__device__ __forceinline__ double xc_energy(const double* scal, double lambda) {
+  double v = 0.;
+  v += scal[1];
+  v += lambda * scal[2];
+  return v;
+}
+__global__ void k_xc_init(XsCtl* c, const double* scal, double lambda, int max_iter, cudaGraphConditionalHandle hgo) {
+  c->tau = 1.0;
+  c->sigma = 1.0;
+  c->energy = c->energy_new = xc_energy(scal, lambda);
+  c->rb_tau[0] = c->rb_tau[1] = __longlong_as_double(0x7ff8000000000000LL);
+  c->rb_e[0] = c->rb_e[1] = __longlong_as_double(0x7ff8000000000000LL);
+  c->rb_pos = 0;
+  c->iter = 0;
+  c->guard = 0;
+  c->go = max_iter > 0;
+  cudaGraphSetConditional(hgo, c->go ? 1u : 0u);
+}
+__global__ void k_xc_begin(XsCtl* c) {
+  c->iter++;
+  c->energy = c->energy_new;
+  c->e_at_pos = c->energy;
+}
+// beta = |d|^2 / |og|^2 except every 10th step (scal[3], scal[4])
+__global__ void k_xc_beta(XsCtl* c, const double* scal) {
+  c->beta = ((c->iter - 1) % 10) ? scal[3] / scal[4] : 0.;
+}
+// Armijo: the starting step, f at the position, the first trial step
+__global__ void k_xc_ls_init(XsCtl* c) {
+  const double t = c->tau;
+  c->tau_ls = t < kXcTauMin ? kXcTauMin : (t > kXcTauMax ? kXcTauMax : t);
+  c->f = c->e_at_pos;
+  c->tw = c->tau_ls;
+}
+// the energy at the trial point into the ring buffer
+__global__ void k_xc_eval(XsCtl* c, const double* scal, double lambda) {
+  c->fnew = xc_energy(scal, lambda);
+  c->rb_tau[c->rb_pos] = c->tw;
+  c->rb_e[c->rb_pos] = c->fnew;
+  c->rb_pos ^= 1;
+}
+// after the first trial: Df = DE . d (scal[3]); doubling (mode 1), halving
+// (mode 2) or done
+__global__ void k_xc_ls_first(XsCtl* c, const double* scal, cudaGraphConditionalHandle hls) {
+  const double sg = 0.5;
+  c->Df = scal[3];
+  const double f = c->f, fnew = c->fnew, Df = c->Df, tau = c->tau_ls;
+  const double G = (fnew - f) / (Df * tau);
+  unsigned go = 1;
+  if (Df >= 0 || !isfinite(f)) {
+    c->result = 0.;
+    go = 0;
+  } else if (G >= sg && f >= fnew) {
+    c->mode = 1;
+    c->tau_ls = tau * 2.;
+    c->tw = c->tau_ls;
+  } else {
+    c->mode = 2;
+    if (c->tau_ls > kXcTauMin) c->tau_ls *= 0.5;
+    c->tw = c->tau_ls;
+  }
+  c->ls_steps = 0;
+  cudaGraphSetConditional(hls, go);
+}
+__global__ void k_xc_ls_step(XsCtl* c, cudaGraphConditionalHandle hls) {
+  const double sg = 0.5;
+  const double f = c->f, fnew = c->fnew, Df = c->Df;
+  double tau = c->tau_ls;
+  const double G = (fnew - f) / (Df * tau);
+  unsigned go = 1;
+  if (c->mode == 1) {
+    if (G >= sg && f >= fnew && tau <= kXcTauMax) {
+      tau *= 2.;
+    } else {
+      tau *= 0.5;
+      go = 0;
+    }
+  } else {
+    if ((!isfinite(fnew) || (G < sg || f < fnew)) && (tau > kXcTauMin)) {
+      if (tau > kXcTauMin) tau *= 0.5;
+    } else {
+      go = 0;
+    }
+  }
+  c->tau_ls = tau;
+  c->tw = tau;
+  // the step range bounds a search to ~56 trials; a second bound guards the loop
+  if (++c->ls_steps > 200) {
+    c->guard = 1;
+    go = 0;
+  }
+  if (!go) c->result = (tau > kXcTauMin) ? tau : 0.;
+  cudaGraphSetConditional(hls, go);
+}
+// the search's result is the step; 0 -> the fallback attempt from the plain direction
+__global__ void k_xc_after(XsCtl* c, cudaGraphConditionalHandle hfb) {
+  c->tau = c->result;
+  cudaGraphSetConditional(hfb, c->tau == 0 ? 1u : 0u);
+}
+__global__ void k_xc_after_fallback(XsCtl* c) { c->tau = c->result; }
+// the energy at the new position from the ring buffer, or an evaluation there
+__global__ void k_xc_ring(XsCtl* c, cudaGraphConditionalHandle hne) {
+  double enew = __longlong_as_double(0x7ff8000000000000LL);
+  if (c->rb_tau[0] == c->tau) enew = c->rb_e[0];
+  else if (c->rb_tau[1] == c->tau) enew = c->rb_e[1];
+  else if (c->tau == 0) enew = c->energy;
+  c->enew = enew;
+  cudaGraphSetConditional(hne, isnan(enew) ? 1u : 0u);
+}
+__global__ void k_xc_eval_pos(XsCtl* c, const double* scal, double lambda) { c->enew = xc_energy(scal, lambda); }
+// stop rule and filter-width schedule (gradientDescent.h:416-439, 675-691)
+__global__ void k_xc_end(XsCtl* c, int max_iter, cudaGraphConditionalHandle hgo) {
+  const double stop_sigma = 0.0001, sigma_tol = 0.00001, stop_eps = 0.;
+  c->energy_new = c->enew;
+  bool go = ((c->energy - c->energy_new) > stop_eps) && (c->iter < max_iter);
+  if ((0.5 * c->sigma > stop_sigma) && ((c->energy - c->energy_new) < sigma_tol)) {
+    c->sigma *= 0.5;
+    c->tau = 1.;
+    go = (c->sigma > stop_sigma) && (c->iter < max_iter);
+  }
+  c->go = go;
+  cudaGraphSetConditional(hgo, go ? 1u : 0u);
+}
+
+// Graph capture of the descent: conditional nodes appended to the capture
+// of a stream, their bodies captured on further streams.
+struct XsGraphBuilder {
+  msgpu_context* ctx;
+  XsSolver& S;
+  XsCtl* c;
+  int max_iter;
+  cudaStream_t s[4];
+  cudaError_t err = cudaSuccess;
+
+  void check(cudaError_t e) {
+    if (e != cudaSuccess && err == cudaSuccess) err = e;
+  }
+  cudaGraphConditionalHandle handle(cudaStream_t st) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    cudaGraphConditionalHandle h = 0;
+    check(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, nullptr, nullptr));
+    if (err == cudaSuccess) check(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+    return h;
+  }
+  cudaGraph_t cond(cudaStream_t st, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    check(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
+    if (err != cudaSuccess) return nullptr;
+    cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};
+    p.conditional.handle = h;
+    p.conditional.type = type;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    check(cudaGraphAddNode(&node, g, deps, nd, &p));
+    if (err != cudaSuccess) return nullptr;
+    check(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    return p.conditional.phGraph_out[0];
+  }
+  // kernels of one energy evaluation at p: data term and regulariser into scal[1..2]
+  void parts(cudaStream_t st, const double* p, double* de) {
+    LineArgs a;
+    memset(&a, 0, sizeof(a));
+    a.nx = S.nx; a.ny = S.ny; a.img_stride = (size_t)S.N; a.R = S.R; a.T = S.T; a.phi = p;
+    a.e_line = (double*)ctx->nccbuf.p; a.de = de; a.t = S.lt;
+    a.nr_pre = S.B.nr; a.done = S.B.done; a.e_total = S.B.scal + 1;
+    k_lineshift<<<dim3(S.ny, 1), kLineThreads, sizeof(double) * 3 * (size_t)S.nx, st>>>(a);
+    const int nb = std::min(1024, (S.N + 255) / 256);
+    if (S.lapw > 0)
+      k_xshift_reg_lap<<<dim3(nb, 1), 256, 0, st>>>(S.lapt, S.nx, S.ny, (size_t)S.N, p, S.B.kphi, S.B.part,
+                                                    S.B.done + 1, S.B.scal + 2);
+    else
+      k_xshift_reg<<<dim3(nb, 1), 256, 0, st>>>(S.rt, S.nx, S.ny, (size_t)S.N, p, S.B.kphi, S.B.part, S.B.done + 1,
+                                                S.B.scal + 2);
+    check(cudaGetLastError());
+  }
+  void dot(cudaStream_t st, const double* a, const double* b, double* out) {
+    const int nb = std::min(1024, (S.N + 255) / 256);
+    k_dot_part<<<nb, 256, 0, st>>>(a, b, S.N, S.B.part);
+    k_sum_part<<<1, 256, 0, st>>>(S.B.part, nb, out);
+    check(cudaGetLastError());
+  }
+  void metric(cudaStream_t st, double* g) {
+    const XsBufs& B = S.B;
+    const int nx = S.nx, ny = S.ny, ne = (nx + 1) / 2, no = nx / 2;
+    const int gb = std::min(2048, (S.N + 255) / 256);
+    k_xfold<<<gb, 256, 0, st>>>(g, B.t1, nx, ny);
+    check(dgemm(st, true, false, ne, ny, ne, B.Ve, ne, B.t1, nx, B.t2, nx));
+    check(dgemm(st, true, false, no, ny, no, B.Vo, no, B.t1 + ne, nx, B.t2 + ne, nx));
+    check(dgemm(st, false, false, nx, ny, ny, B.t2, nx, B.Vy, ny, B.t1, nx));
+    k_spectral_scale_dev<<<gb, 256, 0, st>>>(B.t1, B.lx, B.ly, &c->sigma, nx, ny);
+    check(dgemm(st, false, true, nx, ny, ny, B.t1, nx, B.Vy, ny, B.t2, nx));
+    check(dgemm(st, false, false, ne, ny, ne, B.Ve, ne, B.t2, nx, B.t1, nx));
+    check(dgemm(st, false, false, no, ny, no, B.Vo, no, B.t2 + ne, nx, B.t1 + ne, nx));
+    k_xunfold<<<gb, 256, 0, st>>>(B.t1, g, nx, ny);
+    check(cudaGetLastError());
+  }
+  // the descent step loop's body, captured on s[1]
+  void step_body(double* phi) {
+    cudaStream_t st = s[1];
+    const XsBufs& B = S.B;
+    const int N = S.N, g1 = S.grid1();
+    k_xc_begin<<<1, 1, 0, st>>>(c);
+    parts(st, phi, B.de);
+    k_axpy<<<g1, 256, 0, st>>>(B.de, S.lambda, B.kphi, B.de, N);
+    k_mul<<<g1, 256, 0, st>>>(B.de, -1., B.d, N);
+    metric(st, B.d);
+    dot(st, B.d, B.d, B.scal + 3);
+    dot(st, B.og, B.og, B.scal + 4);
+    k_xc_beta<<<1, 1, 0, st>>>(c, B.scal);
+    check(cudaMemcpyAsync(B.og, B.d, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+    k_axpy_dev<<<g1, 256, 0, st>>>(B.d, &c->beta, B.od, B.d, N);
+    check(cudaMemcpyAsync(B.od, B.d, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+    check(cudaGetLastError());
+    // the search on the step body's stream, its loop body on s[2]
+    armijo_on(st, s[2], phi);
+    const cudaGraphConditionalHandle hfb = handle(st);
+    k_xc_after<<<1, 1, 0, st>>>(c, hfb);
+    k_scale_dev<<<g1, 256, 0, st>>>(B.d, &c->tau, N);
+    check(cudaGetLastError());
+    cudaGraph_t fb = cond(st, hfb, cudaGraphCondTypeIf);
+    if (err != cudaSuccess) return;
+    {
+      // fallback attempt: the plain direction, no memory of the old one
+      cudaStream_t sf = s[2];
+      check(cudaStreamBeginCaptureToGraph(sf, fb, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+      check(cudaMemcpyAsync(B.d, B.og, sizeof(double) * N, cudaMemcpyDeviceToDevice, sf));
+      check(cudaMemsetAsync(B.od, 0, sizeof(double) * N, sf));
+      armijo_on(sf, s[3], phi);
+      k_xc_after_fallback<<<1, 1, 0, sf>>>(c);
+      k_scale_dev<<<g1, 256, 0, sf>>>(B.d, &c->tau, N);
+      check(cudaGetLastError());
+      cudaGraph_t out = nullptr;
+      check(cudaStreamEndCapture(sf, &out));
+    }
+    const cudaGraphConditionalHandle hne = handle(st);
+    k_xc_ring<<<1, 1, 0, st>>>(c, hne);
+    k_step_dev<<<g1, 256, 0, st>>>(phi, B.d, &c->tau, N);
+    check(cudaGetLastError());
+    cudaGraph_t ne = cond(st, hne, cudaGraphCondTypeIf);
+    if (err != cudaSuccess) return;
+    {
+      cudaStream_t sn = s[2];
+      check(cudaStreamBeginCaptureToGraph(sn, ne, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+      parts(sn, phi, nullptr);
+      k_xc_eval_pos<<<1, 1, 0, sn>>>(c, B.scal, S.lambda);
+      check(cudaGetLastError());
+      cudaGraph_t out = nullptr;
+      check(cudaStreamEndCapture(sn, &out));
+    }
+    const cudaGraphConditionalHandle hgo = go_handle;
+    k_xc_end<<<1, 1, 0, st>>>(c, max_iter, hgo);
+    check(cudaGetLastError());
+  }
+  cudaGraphConditionalHandle go_handle = 0;
+  // one Armijo search captured on st, its loop body on sb
+  void armijo_on(cudaStream_t st, cudaStream_t sb, double* phi) {
+    const int g1 = S.grid1();
+    k_xc_ls_init<<<1, 1, 0, st>>>(c);
+    k_axpy_dev<<<g1, 256, 0, st>>>(phi, &c->tw, S.B.d, S.B.tx, S.N);
+    parts(st, S.B.tx, nullptr);
+    k_xc_eval<<<1, 1, 0, st>>>(c, S.B.scal, S.lambda);
+    dot(st, S.B.de, S.B.d, S.B.scal + 3);
+    const cudaGraphConditionalHandle hls = handle(st);
+    k_xc_ls_first<<<1, 1, 0, st>>>(c, S.B.scal, hls);
+    check(cudaGetLastError());
+    cudaGraph_t body = cond(st, hls, cudaGraphCondTypeWhile);
+    if (err != cudaSuccess) return;
+    check(cudaStreamBeginCaptureToGraph(sb, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    k_axpy_dev<<<g1, 256, 0, sb>>>(phi, &c->tw, S.B.d, S.B.tx, S.N);
+    parts(sb, S.B.tx, nullptr);
+    k_xc_eval<<<1, 1, 0, sb>>>(c, S.B.scal, S.lambda);
+    k_xc_ls_step<<<1, 1, 0, sb>>>(c, hls);
+    check(cudaGetLastError());
+    cudaGraph_t out = nullptr;
+    check(cudaStreamEndCapture(sb, &out));
+  }
+};
+
+int run_xshift_graph(msgpu_context* ctx, int nx, int ny, const double* R, const double* T, double lambda, double yreg,
+                     double lapw, int max_iter, double* phi, double* energy_out, int* steps_out, cudaStream_t st) {
+  XsSolver S;
+  S.ctx = ctx; S.nx = nx; S.ny = ny; S.N = nx * ny; S.R = R; S.T = T; S.lambda = lambda; S.yreg = yreg; S.st = st;
+  int rc;
+  if ((rc = xs_setup(ctx, nx, ny, S.B, st))) return rc;
+  if ((rc = ensure(ctx, ctx->nccbuf, sizeof(double) * (size_t)ny + 64))) return rc;
+  S.lt = host_line_tables(nx);
+  S.rt = host_xreg_tables(nx, ny, yreg);
+  S.lapw = lapw;
+  if (lapw > 0) S.lapt = host_xreg_lap_tables(nx, ny, yreg, lapw);
+  CK(cudaFuncSetAttribute(k_lineshift, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)(sizeof(double) * 3 * (size_t)nx)));
+  CK(cudaFuncSetAttribute(k_lineshift_prep_ref, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)(sizeof(double) * 3 * (size_t)nx)));
+  for (int k = 0; k < 4; ++k)
+    if (!ctx->xc_stream[k]) CK(cudaStreamCreateWithFlags(&ctx->xc_stream[k], cudaStreamNonBlocking));
+  XsCtl* c = reinterpret_cast<XsCtl*>(S.B.scal + 128);
+  XsGraphBuilder gb{ctx, S, c, max_iter, {ctx->xc_stream[0], ctx->xc_stream[1], ctx->xc_stream[2], ctx->xc_stream[3]}};
+  const int N = S.N, g1 = S.grid1();
+  const XsBufs& B = S.B;
+  const double scale = (double)nx / (double)(nx > ny ? nx : ny);
+  cudaStream_t s0 = gb.s[0];
+  CK(cudaStreamBeginCapture(s0, cudaStreamCaptureModeRelaxed));
+  k_lineshift_prep_ref<<<dim3(ny, 1), kLineThreads, sizeof(double) * 3 * (size_t)nx, s0>>>(R, nx, (size_t)N, S.lt,
+                                                                                         B.nr);
+  gb.check(cudaMemsetAsync(B.og, 0, sizeof(double) * N, s0));
+  gb.check(cudaMemsetAsync(B.od, 0, sizeof(double) * N, s0));
+  k_divide<<<g1, 256, 0, s0>>>(phi, scale, N);
+  gb.parts(s0, phi, nullptr);
+  gb.go_handle = gb.handle(s0);
+  k_xc_init<<<1, 1, 0, s0>>>(c, B.scal, lambda, max_iter, gb.go_handle);
+  gb.check(cudaGetLastError());
+  cudaGraph_t loop = gb.cond(s0, gb.go_handle, cudaGraphCondTypeWhile);
+  if (gb.err == cudaSuccess) {
+    gb.check(cudaStreamBeginCaptureToGraph(gb.s[1], loop, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    gb.step_body(phi);
+    cudaGraph_t out = nullptr;
+    gb.check(cudaStreamEndCapture(gb.s[1], &out));
+  }
+  k_scale<<<g1, 256, 0, s0>>>(phi, scale, N);
+  gb.check(cudaGetLastError());
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(s0, &graph);
+  if (gb.err == cudaSuccess) gb.check(ce);
+  cudaGraphExec_t exec = nullptr;
+  if (gb.err == cudaSuccess) gb.check(cudaGraphInstantiate(&exec, graph, 0));
+  if (graph) cudaGraphDestroy(graph);
+  if (gb.err != cudaSuccess) {
+    if (exec) cudaGraphExecDestroy(exec);
+    return fail(ctx, MSGPU_ERR_CUDA, "findXShift graph: %s", cudaGetErrorString(gb.err));
+  }
+  const cudaError_t le = cudaGraphLaunch(exec, st);
+  double res[2];
+  cudaError_t ce2 = le;
+  if (ce2 == cudaSuccess) ce2 = cudaMemcpyAsync(res, &c->energy_new, sizeof(double), cudaMemcpyDeviceToHost, st);
+  int it[2] = {0, 0};   // iter, guard
+  if (ce2 == cudaSuccess) ce2 = cudaMemcpyAsync(it, &c->iter, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (ce2 == cudaSuccess) ce2 = cudaMemcpyAsync(it + 1, &c->guard, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (ce2 == cudaSuccess) ce2 = cudaStreamSynchronize(st);
+  cudaGraphExecDestroy(exec);
+  CK(ce2);
+  if (it[1]) return fail(ctx, MSGPU_ERR_CUDA, "findXShift graph: a line search exceeded its trial bound");
+  ctx->stats.kernel_launches += 1;
+  if (energy_out) *energy_out = res[0];
+  if (steps_out) *steps_out = it[0];
+  return MSGPU_OK;
+}
 }  // namespace
 
 namespace {
@@ -2765,6 +3147,9 @@ int msgpu_find_xshift_device(msgpu_context* ctx, int nx, int ny, const double* d
   int rc;
   if ((rc = bind_device(ctx))) return rc;
   ctx->stats.kernel_launches = 0;
+  if (ctx->xs_device_control)
+    return run_xshift_graph(ctx, nx, ny, d_R, d_T, lambda, yreg, laplace_weight, max_iter, d_phix, energy_out,
+                            steps_out, (cudaStream_t)stream);
   return run_xshift(ctx, nx, ny, d_R, d_T, lambda, yreg, laplace_weight, max_iter, d_phix, energy_out, steps_out,
                     (cudaStream_t)stream);
 }

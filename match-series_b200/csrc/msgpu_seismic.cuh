@@ -554,6 +554,42 @@ __global__ void __launch_bounds__(256) k_sum_part(const double* part, int n, dou
   if (threadIdx.x == 0) *out = s;
 }
 // Spectral scaling of the H1 metric: z[y][x] /= 1 + tau (lx[x] + ly[y])
+// Vector kernels whose scalar lives on the device (the descent control of
+// findXShift as a graph with device-side conditions): the same arithmetic as
+// k_axpy / k_scale with the scalar read from memory.
+__global__ void k_axpy_dev(const double* a, const double* s, const double* b, double* out, int n) {
+  const double sv = *s;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double v = a[i];
+    v += sv * b[i];
+    out[i] = v;
+  }
+}
+__global__ void k_scale_dev(double* a, const double* s, int n) {
+  const double sv = *s;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] *= sv;
+}
+// phi += d when the accepted step *tau is not 0
+__global__ void k_step_dev(double* phi, const double* d, const double* tau, int n) {
+  if (*tau == 0) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double v = phi[i];
+    v += 1.0 * d[i];
+    phi[i] = v;
+  }
+}
+// the spectral scaling with tau = sigma^2 / 2 from the device's sigma
+__global__ void k_spectral_scale_dev(double* z, const double* lx, const double* ly, const double* sigma, int nx,
+                                     int ny) {
+  const double sg = *sigma;
+  const double tau = 0.5 * (sg * sg);
+  const int N = nx * ny;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    const int x = i % nx, y = i / nx;
+    z[i] /= 1.0 + tau * (lx[x] + ly[y]);
+  }
+}
+
 __global__ void k_spectral_scale(double* z, const double* lx, const double* ly, double tau, int nx, int ny) {
   const int N = nx * ny;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {

@@ -77,6 +77,25 @@ def test_find_xshift_non_square_larger_grid(gpu, oracle):
     assert np.abs(ph - rph).max() * (nx - 1) <= 1e-4
 
 
+@pytest.mark.parametrize("lapw", [0.0, 0.01])
+def test_find_xshift_device_control_equals_host_control(gpu, lapw):
+    """The descent as one device-controlled graph (conditional while/if
+    nodes) against the same descent driven from the host (the default): the
+    same steps and bit-identical shifts and energy."""
+    nx, ny = 129, 33
+    R, T = _shifted_lines(nx, ny, 1.25, 31)
+    hph, he, hsteps = gpu.find_xshift(R, T, 0.01, 1.0, 80, laplace_weight=lapw)
+    gpu.set_seismic_device_control(True)
+    try:
+        ph, e, steps = gpu.find_xshift(R, T, 0.01, 1.0, 80, laplace_weight=lapw)
+        launches = gpu.stats()["kernel_launches"]
+    finally:
+        gpu.set_seismic_device_control(False)
+    assert steps == hsteps and steps > 5
+    assert e == he and np.array_equal(ph, hph)
+    assert launches <= 2
+
+
 def test_find_xshift_batch_equals_single_calls(gpu):
     """Images spread over worker threads with their own streams: every image's
     result equals, bit for bit, its own single call."""
