@@ -85,6 +85,7 @@ def workload(rank: int):
 
 SUM_ORDER = 0   # 0: the reference's sequential order (bit-exact); 1: parallel order (--sum-order 1)
 CERTIFIED = True   # sum order 0: control steps on bounded sums where the bounds settle them
+WARM_COARSE_ITERS = 0   # warm leg: step limit below the stop level (0: maxGDIterations)
 
 
 def params(fp64: bool):
@@ -884,6 +885,8 @@ def metric_legs(ctx, p, d_ref, d_tmpl, F, plain_ms, plain_e, fp64, local, rank):
     s = torch.empty((F, nlev), dtype=torch.int32, device=dev)
     d_plain = torch.from_numpy(np.ascontiguousarray(plain_e)).to(dev)
 
+    ctx.set_warm_schedule(WARM_COARSE_ITERS)
+
     def warm():
         return ctx.register_batch_warm_device(p, net, d_ref.data_ptr(), d_tmpl.data_ptr(), F, phis.data_ptr(),
                                               e.data_ptr(), s.data_ptr(), d_plain_energies=d_plain.data_ptr(),
@@ -922,6 +925,7 @@ def metric_legs(ctx, p, d_ref, d_tmpl, F, plain_ms, plain_e, fp64, local, rank):
         "frames_within_tol": int(np.sum(rel <= WARM_TOL)),
         "fallback_frames": int(F - int(np.sum(used))),
         "steps_per_level_warm_to_tol": [round(float(x), 1) for x in s.float().mean(0).cpu().numpy()],
+        "coarse_level_step_limit": WARM_COARSE_ITERS or None,
         "training": {"pairs": WARM_TRAIN_SERIES * WARM_FPS, "steps": WARM_STEPS, "seconds": t_train,
                      "data_seconds": t_data},
         "note": "the plain batch's final energies are the targets; frames that end above them by more than the "
@@ -1134,6 +1138,8 @@ def main():
     ap.add_argument("--no-certified", action="store_true",
                     help="with sum order 0: add every pass's sums in order before its control step (the results "
                          "are the same; for comparisons)")
+    ap.add_argument("--warm-coarse-iters", type=int, default=0,
+                    help="warm leg: step limit of the levels below the stop level (0: maxGDIterations)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ncc", action="store_true",
                     help="normalized cross-correlation data term (matchSeries' default model) instead of SSD")
@@ -1165,10 +1171,11 @@ def main():
                     help="time matchSeries' whole first stage with accumulated deformations (msgpu_match_series)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    global DATA_TERM, SUM_ORDER, CERTIFIED
+    global DATA_TERM, SUM_ORDER, CERTIFIED, WARM_COARSE_ITERS
     DATA_TERM = 1 if args.ncc else 0
     SUM_ORDER = args.sum_order
     CERTIFIED = not args.no_certified
+    WARM_COARSE_ITERS = args.warm_coarse_iters
     if args.profile_level:
         return profile_case(args.profile_level, args.profile_iters, not args.fp32)
     if args.profile_compose or args.profile_series:

@@ -118,6 +118,11 @@ int  msgpu_set_certified_steps(msgpu_context* ctx, int on);
  * B200.  The two take the same decisions in the same double arithmetic:
  * identical results.                                                       */
 int  msgpu_set_seismic_device_control(msgpu_context* ctx, int on);
+/* Warm-started batches (msgpu_register_batch_warm{,_device}): the step limit
+ * of the levels between the network's output level and the stop level
+ * (0, the default: maxGDIterations).  They start near their solution; the
+ * stop level still runs to the stated energy tolerance.                    */
+int  msgpu_set_warm_schedule(msgpu_context* ctx, int coarse_iters);
 int  msgpu_destroy(msgpu_context* ctx);
 const char* msgpu_last_error(const msgpu_context* ctx);
 

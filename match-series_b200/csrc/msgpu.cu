@@ -75,6 +75,7 @@ struct msgpu_context {
   Buf xs_basis, xs_work;
   cudaStream_t xc_stream[4] = {nullptr, nullptr, nullptr, nullptr};   // capture streams of the findXShift graph
   bool xs_device_control = false;                             // findXShift as a device-controlled graph
+  int warm_coarse_iters = 0;   // warm start: step limit below the stop level (0: maxGDIterations)
   std::vector<msgpu_context*> workers;   // contexts of the batch workers (own streams and buffers)
 };
 
@@ -886,6 +887,7 @@ struct BatchOpts {
   const double* e_target = nullptr;   // device, per frame: stop the stop-level solve at this energy (+ e_tol)
   double e_tol = 0.0;
   int max_iter_stop = 0;              // > 0: step limit of the stop level (with energy targets)
+  int max_iter_below = 0;             // > 0: step limit of the levels below the stop level
 };
 
 int warm_start_phi(msgpu_net* net, const double* pyr, const std::vector<size_t>& poff, size_t pstride, int F,
@@ -1030,6 +1032,7 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
     a.out_steps = steps_all + (size_t)(l - start) * F;
     a.out_evals = evals_all + (size_t)(l - start) * F;
     a.out_phi_buf = bin;   // the level kernel updates the buffer index in place
+    if (l < stop && opt.max_iter_below > 0) a.max_iter = opt.max_iter_below;
     if (l == stop && opt.e_target) {
       a.e_target = opt.e_target;
       a.e_tol = opt.e_tol;
@@ -1768,6 +1771,14 @@ int msgpu_set_sum_order(msgpu_context* ctx, int sum_order) {
   if (!ctx) return MSGPU_ERR_INVALID_ARG;
   if (sum_order != 0 && sum_order != 1) return fail(ctx, MSGPU_ERR_INVALID_ARG, "sum_order must be 0 or 1");
   ctx->sum_order = sum_order;
+  return MSGPU_OK;
+}
+
+int msgpu_set_warm_schedule(msgpu_context* ctx, int coarse_iters) {
+  if (!ctx) return MSGPU_ERR_INVALID_ARG;
+  if (coarse_iters < 0) return fail(ctx, MSGPU_ERR_INVALID_ARG, "coarse_iters %d < 0", coarse_iters);
+  ctx->warm_coarse_iters = coarse_iters;
+  ++ctx->alloc_epoch;   // a captured graph holds the old step limits
   return MSGPU_OK;
 }
 
@@ -4618,6 +4629,9 @@ int warm_batch(msgpu_context* ctx, const msgpu_params& p, msgpu_net* net, const 
   // reach its target: the stop level runs until it does, at most twice
   // maxGDIterations steps (a frame that does not is registered again)
   opt.max_iter_stop = d_plain_e ? 2 * p.max_gd_iterations : 0;
+  // the levels between the network's output and the stop level start near
+  // their solution: optionally fewer steps there (msgpu_set_warm_schedule)
+  opt.max_iter_below = ctx->warm_coarse_iters;
   if ((rc = run_batch<Real>(ctx, pw, F, io, st, opt))) return rc;
   if (d_e_out) CK(cudaMemcpyAsync(d_e_out, e, sizeof(double) * F, cudaMemcpyDeviceToDevice, st));
   if (d_s_out) {

@@ -106,7 +106,7 @@ EXPORTS = [
     "msgpu_net_train_step_device", "msgpu_net_loss_grad", "msgpu_prepare_images_device", "msgpu_register_batch_warm",
     "msgpu_register_batch_warm_device", "msgpu_find_xshift_yconst", "msgpu_find_xshift_yconst_device",
     "msgpu_empty_lines_to_nan", "msgpu_empty_lines_to_nan_device", "msgpu_remove_empty_lines",
-    "msgpu_remove_empty_lines_device", "msgpu_set_wait_limits", "msgpu_set_sum_order", "msgpu_set_certified_steps", "msgpu_set_seismic_device_control", "msgpu_warp_sum_device",
+    "msgpu_remove_empty_lines_device", "msgpu_set_wait_limits", "msgpu_set_sum_order", "msgpu_set_certified_steps", "msgpu_set_seismic_device_control", "msgpu_set_warm_schedule", "msgpu_warp_sum_device",
     "msgpu_mean_from_sums_device", "msgpu_set_graphs", "msgpu_get_tuning", "msgpu_set_tuning",
     "msgpu_autotune_device", "msgpu_gd_level_log", "msgpu_exact_sum_device",
 ]
@@ -160,6 +160,7 @@ def lib():
         L.msgpu_set_sum_order.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.msgpu_set_certified_steps.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.msgpu_set_seismic_device_control.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.msgpu_set_warm_schedule.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.msgpu_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(Stats)]
         L.msgpu_series_params_default.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(SeriesParams)]
         L.msgpu_series_params_default.restype = None
@@ -759,6 +760,11 @@ class Context:
         """0: the reference's sequential order (default), 1: a fixed parallel
         order, for the FP64 sums of energy() and gd_level()."""
         self._check(lib().msgpu_set_sum_order(self._h, int(sum_order)))
+
+    def set_warm_schedule(self, coarse_iters: int):
+        """Warm-started batches: step limit of the levels below the stop
+        level (0: maxGDIterations)."""
+        self._check(lib().msgpu_set_warm_schedule(self._h, int(coarse_iters)))
 
     def set_seismic_device_control(self, on: bool):
         """findXShift's descent control on the device as one graph, or on
