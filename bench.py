@@ -299,9 +299,10 @@ def run_reference_arm(args, world, rank):
     return 0
 
 
-def profile_case(level: int, iters: int, fp64: bool):
+def profile_case(level: int, iters: int, fp64: bool, trace_out: str = ""):
     """One launch of the level kernel on the bench's frames generated at
     `level` (start = stop = level, `iters` steps): the case ncu captures."""
+    import numpy as np
     import msgpu
     from msgpu import build as mbuild
     from msgpu import synthetic as syn
@@ -313,9 +314,13 @@ def profile_case(level: int, iters: int, fp64: bool):
                              max_gd_iterations=iters, use_fp64=int(fp64), data_term=DATA_TERM, sum_order=SUM_ORDER)
     ctx.set_certified_steps(CERTIFIED)
     ctx.set_profiling(True)
+    if trace_out:
+        ctx.set_trace(level, 1 << 22)
     ctx.register_batch(p, frames[FRAMES], frames[:FRAMES])
     print(json.dumps({"profile_level": level, "frames": FRAMES, "iters": iters, "fp64": fp64,
                       "stats": ctx.stats()}))
+    if trace_out:
+        np.savez_compressed(trace_out, **ctx.trace())
 
 
 SERIES_SAMPLE = 3   # templates of the chain the CPU reference runs in --series
@@ -1148,6 +1153,9 @@ def main():
                     help="small case for ncu captures: one level solve of FRAMES frames at this level, "
                          "--profile-iters gradient steps, no timing")
     ap.add_argument("--profile-iters", type=int, default=5)
+    ap.add_argument("--trace-out", default="",
+                    help="with --profile-level: save the level kernel's pass timeline (msgpu_set_trace) "
+                         "to this .npz")
     ap.add_argument("--profile-compose", type=int, default=0,
                     help="small case for ncu: one displacement composition at this level, no timing")
     ap.add_argument("--profile-series", action="store_true",
@@ -1178,7 +1186,7 @@ def main():
     CERTIFIED = not args.no_certified
     WARM_COARSE_ITERS = args.warm_coarse_iters
     if args.profile_level:
-        return profile_case(args.profile_level, args.profile_iters, not args.fp32)
+        return profile_case(args.profile_level, args.profile_iters, not args.fp32, args.trace_out)
     if args.profile_compose or args.profile_series:
         return profile_series(args.profile_compose, not args.fp32)
     if args.profile_predict:

@@ -427,6 +427,23 @@ typedef struct {
   long long level_xs[16][8];
 } msgpu_stats;
 int msgpu_set_profiling(msgpu_context* ctx, int on);
+/* Pass timeline of one level's launch, recorded by profiled calls
+ * (msgpu_set_profiling on): msgpu_set_trace(ctx, level, capacity) records up
+ * to `capacity` events (at most 2^26) of the level kernel at `level` (-1:
+ * none, the default); msgpu_get_trace copies the last profiled call's events,
+ * at most `capacity`, to out (two words each) and returns how many there
+ * were (-1 on invalid arguments).  Word 0 is the GPU's global timer in ns;
+ * word 1 packs the event in bits 56-63, the CTA in bits 32-55 and a value in
+ * bits 0-31: event 1 a pass published and 2 a pass completed (value
+ * instance << 8 | pass kind: 0 initial energy, 1 gradient, 2 V-cycle down,
+ * 3 coarse V-cycle, 4 V-cycle up, 5 NCG + first trial, 6 trial, 7 flush,
+ * 8-11 NCC sub-passes, 12 summaries of exact sums, 13 instance finished),
+ * 3 a wait for work
+ * of 500 ns or more (value its length in ns, word 0 its start), 4 an ordered
+ * walk of exact sums (value its length).  Profiling aid; no counterpart in
+ * the reference (whose only tracing is a stopwatch and gprof).             */
+int msgpu_set_trace(msgpu_context* ctx, int level, unsigned int capacity);
+long long msgpu_get_trace(const msgpu_context* ctx, unsigned long long* out, long long capacity);
 /* CUDA graphs for msgpu_register_batch_device (and the stage entry points
  * built on it), default on: the second call with the same parameters and
  * buffers captures the batch's launches (per level: the level kernel, the

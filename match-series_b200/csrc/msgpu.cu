@@ -76,12 +76,19 @@ struct msgpu_context {
   cudaStream_t xc_stream[4] = {nullptr, nullptr, nullptr, nullptr};   // capture streams of the findXShift graph
   bool xs_device_control = false;                             // findXShift as a device-controlled graph
   int warm_coarse_iters = 0;   // warm start: step limit below the stop level (0: maxGDIterations)
+  // pass timeline of one level (profiling): the level, the capacity in
+  // events, the buffer (events, then the count) and the events of the last
+  // profiled call
+  int trace_level = -1;
+  unsigned trace_cap = 0;
+  Buf trace;
+  std::vector<unsigned long long> trace_host;
   std::vector<msgpu_context*> workers;   // contexts of the batch workers (own streams and buffers)
 };
 
 namespace {
 
-constexpr int kAbiVersion = 7;
+constexpr int kAbiVersion = 8;
 // default chunking of the level scheduler: a 24th of a pass, at most 16 tiles
 constexpr int kChunkDiv = 24, kChunkMax = 16;
 
@@ -1045,10 +1052,28 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
       a.xs_prof = (unsigned long long*)ctx->prof.p + prof_n * nlev_all + 8 * (l - start);
       CK(cudaMemsetAsync(a.pass_cycles, 0, sizeof(unsigned long long) * prof_n, st));
       CK(cudaMemsetAsync(a.xs_prof, 0, sizeof(unsigned long long) * 8, st));
+      if (l == ctx->trace_level && ctx->trace_cap > 0) {
+        const size_t tb = sizeof(unsigned long long) * 2 * (size_t)ctx->trace_cap;
+        if ((rc = ensure(ctx, ctx->trace, tb + 16))) return rc;
+        a.tl = (unsigned long long*)ctx->trace.p;
+        a.tl_n = (unsigned int*)((char*)ctx->trace.p + tb);
+        a.tl_cap = ctx->trace_cap;
+        CK(cudaMemsetAsync(a.tl_n, 0, 16, st));
+      }
     }
     if ((rc = xs_attach<Real>(ctx, a, p.sum_order == 0, stop, F))) return rc;
     if (ctx->profiling && l - start < 16) CK(cudaEventRecord(ctx->ev[2 * (l - start)], st));
     if ((rc = launch_level<Real>(ctx, a, st))) return rc;
+    if (a.tl) {
+      unsigned cnt = 0;
+      CK(cudaMemcpyAsync(&cnt, a.tl_n, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      cnt = std::min(cnt, a.tl_cap);
+      ctx->trace_host.resize(2 * (size_t)cnt);
+      if (cnt)
+        CK(cudaMemcpy(ctx->trace_host.data(), a.tl, sizeof(unsigned long long) * 2 * cnt,
+                      cudaMemcpyDeviceToHost));
+    }
     if (l - start < 16) ctx->stats.level_cluster[l - start] = ctx->last_grid;
     if (ctx->profiling && l - start < 16) CK(cudaEventRecord(ctx->ev[2 * (l - start) + 1], st));
     k_collect<<<1, 256, 0, st>>>(e_lvl, a.out_steps, F, (l == stop) ? io.energies_out : nullptr, io.steps_out,
@@ -3581,6 +3606,22 @@ int msgpu_set_profiling(msgpu_context* ctx, int on) {
   if (!ctx) return MSGPU_ERR_INVALID_ARG;
   ctx->profiling = (on != 0);
   return MSGPU_OK;
+}
+
+int msgpu_set_trace(msgpu_context* ctx, int level, unsigned int capacity) {
+  if (!ctx || level > kMaxLevel || capacity > (1u << 26)) return MSGPU_ERR_INVALID_ARG;
+  ctx->trace_level = level;
+  ctx->trace_cap = level < 0 ? 0u : capacity;
+  ctx->trace_host.clear();
+  return MSGPU_OK;
+}
+
+long long msgpu_get_trace(const msgpu_context* ctx, unsigned long long* out, long long capacity) {
+  if (!ctx || capacity < 0 || (capacity > 0 && !out)) return -1;
+  const long long n = (long long)(ctx->trace_host.size() / 2);
+  const long long m = std::min(n, capacity);
+  if (m > 0) std::memcpy(out, ctx->trace_host.data(), sizeof(unsigned long long) * 2 * (size_t)m);
+  return n;
 }
 
 int msgpu_get_stats(const msgpu_context* ctx, msgpu_stats* out) {

@@ -203,8 +203,17 @@ __device__ __forceinline__ void element_force(const Real* __restrict__ T, int n,
 // 259-279 order: rows j = -1..1, columns i = -1..1).  get(X, Y) reads u.
 template <typename Real, typename Get>
 __device__ __forceinline__ Real stiff_row(int x, int y, int n, Get get) {
-  const int cls = node_class(x, n) + 3 * node_class(y, n);
   Real d = Real(0);
+  if (x > 0 && x < n - 1 && y > 0 && y < n - 1) {
+    // interior node: all nine entries of its class, in the same order (the
+    // coefficients are the same for every interior node)
+#pragma unroll
+    for (int j = -1; j <= 1; ++j)
+#pragma unroll
+      for (int i = -1; i <= 1; ++i) d += Real(c_fe.st[4][j + 1][i + 1]) * get(x + i, y + j);
+    return d;
+  }
+  const int cls = node_class(x, n) + 3 * node_class(y, n);
 #pragma unroll
   for (int j = -1; j <= 1; ++j)
 #pragma unroll
@@ -219,8 +228,15 @@ __device__ __forceinline__ Real stiff_row(int x, int y, int n, Get get) {
 // hh = h^2.
 template <typename Real, typename Get>
 __device__ __forceinline__ Real mass_row(int x, int y, int n, Real hh, Get get) {
-  const int cls = node_class(x, n) + 3 * node_class(y, n);
   Real d = Real(0);
+  if (x > 0 && x < n - 1 && y > 0 && y < n - 1) {   // interior node, as in stiff_row
+#pragma unroll
+    for (int j = -1; j <= 1; ++j)
+#pragma unroll
+      for (int i = -1; i <= 1; ++i) d += (Real(c_fe.ms[4][j + 1][i + 1]) * hh) * get(x + i, y + j);
+    return d;
+  }
+  const int cls = node_class(x, n) + 3 * node_class(y, n);
 #pragma unroll
   for (int j = -1; j <= 1; ++j)
 #pragma unroll

@@ -133,7 +133,32 @@ struct LevelArgs {
   // optional profile of the exact sums: calls, cycles of their three steps,
   // chunks walked, chunks added term by term
   unsigned long long* xs_prof;
+  // optional pass timeline (profiling): up to tl_cap events of two words
+  // (global timer in ns; the packed event, trace_ev), their count at tl_n
+  unsigned long long* tl;
+  unsigned int* tl_n;
+  unsigned int tl_cap;
 };
+
+// Events of the pass timeline: a pass published (instance, kind), a pass
+// completed (its last chunk done: instance, kind), a wait for work of one
+// CTA that lasted 500 ns or more (its length), an ordered walk (its length).
+constexpr unsigned kEvPublish = 1, kEvComplete = 2, kEvIdle = 3, kEvWalk = 4;
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+template <typename Real>
+__device__ __forceinline__ void trace_ev(const LevelArgs<Real>& a, unsigned long long t, unsigned ev,
+                                         unsigned value) {
+  if (!a.tl) return;
+  const unsigned i = atomicAdd(a.tl_n, 1u);
+  if (i < a.tl_cap) {
+    a.tl[2 * (size_t)i] = t;
+    a.tl[2 * (size_t)i + 1] = ((unsigned long long)((ev << 24) | blockIdx.x) << 32) | value;
+  }
+}
 
 // A 2-component array of level k occupies 2 * comp_stride(k) elements.
 __host__ __device__ inline size_t comp_stride(int level) {
@@ -368,30 +393,30 @@ struct EnergyPass {
     const XsGeom g(n);
     const int tx = t % g.nx;
     const int lx = threadIdx.x & 63, ly = threadIdx.x >> 6, half = lx >> 5, lane = threadIdx.x & 31;
-    // elements owned by the tile: E_data terms
+    // elements owned by the tile: E_data terms.  A tile has at most 64
+    // element columns and 8 element rows, so a thread owns column lx of rows
+    // ly and ly + 4; both elements are evaluated together (independent
+    // chains), then summed row by row as one row at a time would be.
     {
       const XsSum s0 = xs_sum(xs, n, 0, true);
       double* B0 = xs_block(s0, t);
       const int ex1 = (x1 < n - 1) ? x1 : n - 1, ey1 = (y1 < n - 1) ? y1 : n - 1;
       const int ew = ex1 - x0, eh = ey1 - y0;
-      for (int iy = ly; iy < eh; iy += kThreads / 64) {
-        double acc = 0.0, mag = 0.0;
-        for (int ix = lx; ix < ew; ix += 64) {
-          const int ex = x0 + ix, ey = y0 + iy;
-          const int c0 = at(ex, ey);
-          const int idx[4] = {c0, c0 + 1, c0 + EWX, c0 + EWX + 1};
-          Real px[4], py[4], r[4];
+      const bool ein = lx < ew;
+      auto elem = [&](int ix, int iy) -> double {
+        const int ex = x0 + ix, ey = y0 + iy;
+        const int c0 = at(ex, ey);
+        const int idx[4] = {c0, c0 + 1, c0 + EWX, c0 + EWX + 1};
+        Real px[4], py[4], r[4];
 #pragma unroll
-          for (int b = 0; b < 4; ++b) {
-            r[b] = Wr[idx[b]];
-            px[b] = Wpx[idx[b]];
-            py[b] = Wpy[idx[b]];
-          }
-          const double v = (double)element_ssd(I.T, n, I.P, I.h, ex, ey, px, py, r);
-          B0[xs_at(ix, iy)] = v;
-          acc += v;
-          mag += fabs(v);
+        for (int b = 0; b < 4; ++b) {
+          r[b] = Wr[idx[b]];
+          px[b] = Wpx[idx[b]];
+          py[b] = Wpy[idx[b]];
         }
+        return (double)element_ssd(I.T, n, I.P, I.h, ex, ey, px, py, r);
+      };
+      auto row_done = [&](int iy, double acc, double mag) {
         acc = warp_sum(acc);
         if (lane == 0) s0.tot[((y0 + iy) * g.nx + tx) * 2 + half] = acc;
         if (xp) {
@@ -401,6 +426,25 @@ struct EnergyPass {
             xpw[wid][5] += mag;
           }
         }
+      };
+      if (ly < eh) {
+        const int iy = ly, iy2 = ly + 4;
+        const bool two = iy2 < eh;
+        double acc = 0.0, mag = 0.0, acc2 = 0.0, mag2 = 0.0;
+        if (ein) {
+          const double v = elem(lx, iy);
+          const double v2 = elem(lx, two ? iy2 : iy);
+          B0[xs_at(lx, iy)] = v;
+          acc += v;
+          mag += fabs(v);
+          if (two) {
+            B0[xs_at(lx, iy2)] = v2;
+            acc2 += v2;
+            mag2 += fabs(v2);
+          }
+        }
+        row_done(iy, acc, mag);
+        if (two) row_done(iy2, acc2, mag2);
       }
     }
     // owned nodes: p . L p per component; NCG also DE . d and the direction
@@ -1435,8 +1479,10 @@ struct XsBufState {
 // others.
 //
 // Tiles are handed out in chunks of consecutive tiles.  Dispenser word per
-// instance: [63:40] pass sequence number, [39:20] chunks of the pass, [19:0]
-// next chunk.  A worker reads the word and only when chunks are left takes
+// instance: [63:40] priority (an estimate of the instance's work left;
+// workers take the highest first), [39:20] chunks of the pass, [19:0] next
+// chunk.  A worker
+// reads the word and only when chunks are left takes
 // one with an atomic increment; an increment that arrives after the next pass
 // was published takes a valid chunk of that pass, whose descriptor was written
 // (and fenced) before the word.  Every wait for work is
@@ -1495,8 +1541,10 @@ struct InstCtl {
 constexpr int kCtlWords = (int)((sizeof(InstCtl) + 7) / 8);
 constexpr int kWordStride = 16;  // dispenser words 128 bytes apart
 
-__host__ __device__ inline unsigned long long pack_word(unsigned long long seq, int ntiles, int next) {
-  return ((seq & 0xFFFFFFull) << 40) | ((unsigned long long)(ntiles & 0xFFFFF) << 20) | (unsigned long long)(next & 0xFFFFF);
+// A dispenser word: the pass's priority (bits 40-63), its chunks (20-39) and
+// the chunks handed out (0-19).
+__host__ __device__ inline unsigned long long pack_word(unsigned long long prio, int ntiles, int next) {
+  return ((prio & 0xFFFFFFull) << 40) | ((unsigned long long)(ntiles & 0xFFFFF) << 20) | (unsigned long long)(next & 0xFFFFF);
 }
 
 template <typename Real>
@@ -2280,7 +2328,14 @@ __device__ int control_step(const LevelArgs<Real>& a, const SchedPtrs<Real>& sp,
 template <typename Real>
 __device__ void publish(const LevelArgs<Real>& a, const SchedPtrs<Real>& sp, int inst, InstCtl& c) {
   unsigned long long* word = sp.words + (size_t)inst * kWordStride;
-  const unsigned long long seq = (atomicAdd(word, 0ull) >> 40) + 1;
+  // priority of the pass: an estimate of the instance's work left, the
+  // gradient steps it has left at most times (3 + its energy evaluations per
+  // step so far; the other passes of a step cost about three evaluations),
+  // so that workers serve the instances furthest behind first and the
+  // batch's solves end close together (results do not depend on it)
+  const long long left = a.max_iter > c.iter ? (long long)(a.max_iter - c.iter) : 0ll;
+  const long long rate = 48 + (16ll * c.total_evals) / (c.iter > 0 ? c.iter : 1);
+  const unsigned long long prio = (unsigned long long)min(left * rate, 0xFFFFFFll);
   if (c.desc.kind == TK_DONE) {
     if (a.mode != MODE_SMOOTH) {
       a.out_energy[inst] = c.energy_new.v.lo;
@@ -2291,8 +2346,9 @@ __device__ void publish(const LevelArgs<Real>& a, const SchedPtrs<Real>& sp, int
     c.done = 0;
     ctl_store(sp.ctl + inst, c);
     __threadfence();
-    atomicExch(word, pack_word(seq, 0, 0));
+    atomicExch(word, pack_word(prio, 0, 0));
     atomicAdd(sp.finished, 1);
+    trace_ev(a, global_ns(), kEvPublish, ((unsigned)inst << 8) | (unsigned)TK_DONE);
     return;
   }
   // a pass with exact sums writes its terms to a buffer no bounded value holds
@@ -2321,7 +2377,8 @@ __device__ void publish(const LevelArgs<Real>& a, const SchedPtrs<Real>& sp, int
   c.done = 0;
   ctl_store(sp.ctl + inst, c);
   __threadfence();
-  atomicExch(word, pack_word(seq, nchunks, 0));
+  atomicExch(word, pack_word(prio, nchunks, 0));
+  trace_ev(a, global_ns(), kEvPublish, ((unsigned)inst << 8) | (unsigned)c.desc.kind);
 }
 
 // Two passes whose tiles use the same shared-memory layout (so the first
@@ -2349,14 +2406,18 @@ __device__ bool try_take(const LevelArgs<Real>& a, const SchedPtrs<Real>& sp, in
     const int inst = valid ? (start + base + lane) % a.num_inst : 0;
     unsigned long long* word = sp.words + (size_t)inst * kWordStride;
     bool avail = false;
+    unsigned prio = 0;
     if (valid) {
       const unsigned long long w = __ldcg(word);
       avail = (int)(w & 0xFFFFF) < (int)((w >> 20) & 0xFFFFF);
+      prio = (unsigned)(w >> 40);
     }
     unsigned mask = __ballot_sync(0xffffffffu, avail);
     while (mask) {
-      const int src = __ffs(mask) - 1;
-      mask &= mask - 1;
+      // the first lane (from start) among those of the highest priority
+      const unsigned top = __reduce_max_sync(0xffffffffu, ((mask >> lane) & 1u) ? prio : 0u);
+      const int src = __ffs(__ballot_sync(0xffffffffu, ((mask >> lane) & 1u) && prio == top)) - 1;
+      mask &= ~(1u << src);
       int got = 0;
       if (lane == src) {
         const unsigned long long old = atomicAdd(word, 1ull);
@@ -2383,11 +2444,6 @@ __device__ bool try_take(const LevelArgs<Real>& a, const SchedPtrs<Real>& sp, in
 // LevelArgs::idle_ns); beyond it the worker sets the error flag and every
 // worker returns.
 constexpr unsigned long long kMaxIdleNs = 4000000000ull;
-__device__ __forceinline__ unsigned long long global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
 
 template <typename Real>
 __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, SchedPtrs<Real> sp) {
@@ -2449,7 +2505,13 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
           if (stop) { code = stop; break; }
           __nanosleep(64);
         }
-        if (threadIdx.x == 0) flag_wait = code;
+        if (threadIdx.x == 0) {
+          flag_wait = code;
+          if (a.tl && code == 1) {
+            const unsigned long long w = global_ns() - t_begin;
+            if (w >= 500) trace_ev(a, t_begin, kEvIdle, (unsigned)(w < 0xffffffffull ? w : 0xffffffffull));
+          }
+        }
       }
       __syncthreads();
       pt.stop(PK_REDUCE);
@@ -2519,6 +2581,7 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
     __syncthreads();
     if (flag_last) {
       // this CTA completed the pass: totals in tile order, then the control step
+      if (threadIdx.x == 0) trace_ev(a, global_ns(), kEvComplete, ((unsigned)t.inst << 8) | (unsigned)t.desc.kind);
       double acc[kRedSlots] = {0.0, 0.0, 0.0, 0.0};
       const double* pp = sp.partials + (size_t)t.inst * sp.max_tiles * kRedSlots;
       for (int i = threadIdx.x; i < t.desc.ntiles; i += kThreads) {
@@ -2547,7 +2610,9 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
       if (xdone) {
         if (threadIdx.x == 0) xs_pass_sums(a, t.inst, t.desc.purpose, t.desc.xn, t.desc.xres, xss);
         __syncthreads();
+        const unsigned long long tw = global_ns();
         xs_walk(xss, t.desc.xn, xg, xres, a.xs_prof);
+        if (threadIdx.x == 0) trace_ev(a, tw, kEvWalk, (unsigned)(global_ns() - tw));
       }
       // the control step; when it needs a buffer's ordered sums first, the
       // predictions for them here and a summary pass over the grid (small
@@ -2581,7 +2646,9 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
         const int ntask = xs_summary_tasks(ns, a.n);
         if (ntask > 6) break;   // summary pass published below
         for (int task = 0; task < ntask; ++task) xs_summary_task([&](int k) { return xss[k]; }, ns, xg, task);
+        const unsigned long long tw = global_ns();
         xs_walk(xss, ns, xg, xres, a.xs_prof);
+        if (threadIdx.x == 0) trace_ev(a, tw, kEvWalk, (unsigned)(global_ns() - tw));
         if (threadIdx.x == 0) xs_settle(a, t.inst, cs, rb, xres);
       }
       if (threadIdx.x == 0) publish(a, sp, t.inst, cs);

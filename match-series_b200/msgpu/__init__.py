@@ -15,6 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmsgpu.so")
 
 MSGPU_OK = 0
+MSGPU_ERR_INVALID_ARG = 1
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "SIZE", 3: "CUDA", 4: "UNSUPPORTED"}
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -95,6 +96,7 @@ EXPORTS = [
     "msgpu_register_batch", "msgpu_register_batch_device", "msgpu_warp_mean", "msgpu_warp_mean_device",
     "msgpu_energy", "msgpu_smooth", "msgpu_restrict", "msgpu_prolong", "msgpu_normalize", "msgpu_gd_level",
     "msgpu_match_series_stage", "msgpu_match_series_stage_device", "msgpu_set_profiling", "msgpu_get_stats",
+    "msgpu_set_trace", "msgpu_get_trace",
     "msgpu_set_data_term", "msgpu_series_params_default", "msgpu_match_series", "msgpu_match_series_device",
     "msgpu_compose", "msgpu_compose_device", "msgpu_warp_median", "msgpu_warp_median_device",
     "msgpu_io_last_error", "msgpu_read_array", "msgpu_write_array", "msgpu_read_arrays", "msgpu_read_displacement",
@@ -151,6 +153,9 @@ def lib():
                                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                       ctypes.c_void_p, ctypes.c_void_p]
         L.msgpu_set_profiling.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.msgpu_set_trace.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint]
+        L.msgpu_get_trace.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_longlong]
+        L.msgpu_get_trace.restype = ctypes.c_longlong
         L.msgpu_set_graphs.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.msgpu_get_tuning.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(LevelTuning)]
         L.msgpu_set_tuning.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(LevelTuning)]
@@ -669,6 +674,27 @@ class Context:
 
     def set_profiling(self, on: bool):
         self._check(lib().msgpu_set_profiling(self._h, int(bool(on))))
+
+    def set_trace(self, level: int, capacity: int = 1 << 20):
+        """Record the pass timeline of the level kernel at `level` in
+        profiled calls (-1: off); read it with trace()."""
+        self._check(lib().msgpu_set_trace(self._h, int(level), int(capacity)))
+
+    def trace(self) -> dict:
+        """The pass timeline of the last profiled call: arrays t (ns, from
+        the first event), event, cta, value (event codes in msgpu.h)."""
+        n = lib().msgpu_get_trace(self._h, None, 0)
+        if n < 0:
+            raise MsgpuError(MSGPU_ERR_INVALID_ARG, "msgpu_get_trace")
+        w = np.zeros(2 * max(n, 1), dtype=np.uint64)
+        lib().msgpu_get_trace(self._h, w.ctypes.data, n)
+        w = w[:2 * n].reshape(n, 2)
+        order = np.argsort(w[:, 0], kind="stable")
+        w = w[order]
+        t = w[:, 0].astype(np.int64)
+        return {"t": t - (t[0] if n else 0), "event": (w[:, 1] >> np.uint64(56)).astype(np.int32),
+                "cta": ((w[:, 1] >> np.uint64(32)) & np.uint64(0xFFFFFF)).astype(np.int32),
+                "value": (w[:, 1] & np.uint64(0xFFFFFFFF)).astype(np.int64)}
 
     def tuning(self, fp64: bool, level: int) -> dict:
         t = LevelTuning()

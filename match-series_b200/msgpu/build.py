@@ -9,7 +9,7 @@ PKG = os.path.dirname(HERE)
 CSRC = os.path.join(PKG, "csrc")
 OUT = os.path.join(HERE, "libmsgpu.so")
 SOURCES = [os.path.join(CSRC, "msgpu.cu"), os.path.join(CSRC, "msgpu_io.cpp")]
-DEPS = SOURCES + [os.path.join(CSRC, f) for f in ("msgpu_level.cuh", "msgpu_fe.cuh", "msgpu_series.cuh", "msgpu_seismic.cuh", "msgpu_unet.cuh")] + [
+DEPS = SOURCES + sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cuh")) + [
     os.path.join(os.path.dirname(PKG), "include", "msgpu.h")]
 
 # -fmad=false: no contraction of a*b+c into FMA, so that every FP64 operation

@@ -37,7 +37,7 @@ def test_params_defaults_and_version():
     p = msgpu.default_params()
     assert (p.precision_level, p.start_level, p.stop_level, p.max_gd_iterations) == (9, 5, 9, 30)
     assert p.lambda_ == pytest.approx(0.1) and p.lambda_factor == 1.0 and p.saturation_percent == pytest.approx(0.15)
-    assert msgpu.lib().msgpu_abi_version() == 7
+    assert msgpu.lib().msgpu_abi_version() == 8
 
 
 def test_errors_are_reported_not_swallowed():

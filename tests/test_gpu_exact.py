@@ -226,3 +226,40 @@ def test_exact_sum_is_the_sequential_sum_on_hard_data(level):
                 assert got == want and np.signbit(got) == np.signbit(want), (name, got, want)
     finally:
         ctx.close()
+
+
+def test_pass_timeline_records_every_pass_and_leaves_results_unchanged(gpu):
+    """The level kernel's pass timeline (msgpu_set_trace): every published
+    pass completes once, every instance finishes once, the waits for work
+    it records are at least 500 ns, and tracing does not change a bit of
+    the results."""
+    import msgpu
+    from msgpu import synthetic as syn
+    level, F = 7, 4
+    n = (1 << level) + 1
+    fr, _, _ = syn.make_series(n, F + 1, syn.SQUARE_257, seed=8813)
+    p = msgpu.default_params(precision_level=level, input_level=level, start_level=5, stop_level=level,
+                             max_gd_iterations=12, use_fp64=1)
+    plain = gpu.register_batch(p, fr[0], fr[1:])
+    gpu.set_profiling(True)
+    gpu.set_trace(level, 1 << 18)
+    try:
+        traced = gpu.register_batch(p, fr[0], fr[1:])
+        tr = gpu.trace()
+    finally:
+        gpu.set_trace(-1, 0)
+        gpu.set_profiling(False)
+    for a, b in zip(plain, traced):
+        assert np.array_equal(a, b)
+    ev, val = tr["event"], tr["value"]
+    assert tr["t"].size > 0 and np.all(np.diff(tr["t"]) >= 0)
+    kind = val & 255
+    done = (ev == 1) & (kind == 13)
+    assert sorted((val[done] >> 8).tolist()) == list(range(F))
+    for i in range(F):
+        pub = (ev == 1) & ((val >> 8) == i) & (kind != 13)
+        com = (ev == 2) & ((val >> 8) == i)
+        assert pub.sum() == com.sum() > 0, i
+        # the passes complete in the order they were published
+        assert np.array_equal(kind[pub], kind[com]), i
+    assert np.all(val[ev == 3] >= 500)
