@@ -299,6 +299,43 @@ def run_reference_arm(args, world, rank):
     return 0
 
 
+TRACE_KINDS = {0: "energy0", 1: "gradient", 2: "vdown", 3: "vcoarse", 4: "vup", 5: "ncg", 6: "trial",
+               7: "flush", 8: "ncc1", 9: "ncc2", 10: "ncc3", 11: "ncc_var", 12: "xsum"}
+
+
+def trace_summary(tr: dict, ctas: int) -> dict:
+    """Figures of a level kernel's pass timeline (Context.trace()): CTA time
+    spent waiting for work (all of it, and after the first instance
+    finished), the ordered walks, and per pass kind the mean time from
+    publication to completion and from completion to the next publication
+    (the control step, with any ordered walk it waits for)."""
+    import numpy as np
+    t, ev, val = tr["t"], tr["event"], tr["value"]
+    span = float(t.max()) if t.size else 0.0
+    pub, com = ev == 1, ev == 2
+    fin = t[pub & ((val & 255) == 13)]
+    idle, walk = ev == 3, ev == 4
+    out = {"span_ms": span / 1e6, "ctas": ctas,
+           "idle_cta_ms": float(val[idle].sum()) / 1e6,
+           "idle_frac": float(val[idle].sum()) / (span * ctas) if span else 0.0,
+           "idle_cta_ms_after_first_finish": float(val[idle & (t >= fin.min())].sum()) / 1e6 if fin.size else 0.0,
+           "finish_ms": [float(fin.min()) / 1e6, float(np.median(fin)) / 1e6, float(fin.max()) / 1e6] if fin.size else [],
+           "walks": int(walk.sum()), "walk_us_mean": float(val[walk].mean()) / 1e3 if walk.any() else 0.0,
+           "walk_us_max": float(val[walk].max()) / 1e3 if walk.any() else 0.0}
+    dur, lat = {}, {}
+    for i in np.unique(val[pub] >> 8):
+        P = pub & ((val >> 8) == i)
+        C = com & ((val >> 8) == i)
+        tp, kp, tc = t[P], val[P] & 255, t[C]
+        for j in range(min(len(tp), len(tc))):
+            dur.setdefault(int(kp[j]), []).append(tc[j] - tp[j])
+            if j + 1 < len(tp):
+                lat.setdefault(int(kp[j]), []).append(tp[j + 1] - tc[j])
+    out["pass_us"] = {TRACE_KINDS.get(k, str(k)): [len(v), float(np.mean(v)) / 1e3] for k, v in sorted(dur.items())}
+    out["control_us"] = {TRACE_KINDS.get(k, str(k)): float(np.mean(v)) / 1e3 for k, v in sorted(lat.items())}
+    return out
+
+
 def profile_case(level: int, iters: int, fp64: bool, trace_out: str = ""):
     """One launch of the level kernel on the bench's frames generated at
     `level` (start = stop = level, `iters` steps): the case ncu captures."""
@@ -320,7 +357,9 @@ def profile_case(level: int, iters: int, fp64: bool, trace_out: str = ""):
     print(json.dumps({"profile_level": level, "frames": FRAMES, "iters": iters, "fp64": fp64,
                       "stats": ctx.stats()}))
     if trace_out:
-        np.savez_compressed(trace_out, **ctx.trace())
+        tr = ctx.trace()
+        np.savez_compressed(trace_out, **tr)
+        print(json.dumps({"trace": trace_summary(tr, ctx.stats()["level_cluster"][0])}))
 
 
 SERIES_SAMPLE = 3   # templates of the chain the CPU reference runs in --series
