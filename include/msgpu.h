@@ -440,8 +440,15 @@ int msgpu_set_profiling(msgpu_context* ctx, int on);
  * 8-11 NCC sub-passes, 12 summaries of exact sums, 13 instance finished),
  * 3 a wait for work
  * of 500 ns or more (value its length in ns, word 0 its start), 4 an ordered
- * walk of exact sums (value its length).  Profiling aid; no counterpart in
- * the reference (whose only tracing is a stopwatch and gprof).             */
+ * walk of exact sums (value its length), 5 an open control step that has a
+ * term buffer's sums added in order (value instance << 16 | buffer << 12 |
+ * reason << 8 | kind of the pass whose step is open; reason 11: a buffer
+ * the open decision was evaluated from, else 0: the pass's own sums, 1-10: a
+ * bounded value of the state, in the order energy at the new position,
+ * energy, f, Df, the two line-search energies, E_reg at the position, the
+ * last E_reg, the two line-search E_reg).  Profiling aid; no
+ * counterpart in the reference (whose only tracing is a stopwatch and
+ * gprof).                                                                  */
 int msgpu_set_trace(msgpu_context* ctx, int level, unsigned int capacity);
 long long msgpu_get_trace(const msgpu_context* ctx, unsigned long long* out, long long capacity);
 /* CUDA graphs for msgpu_register_batch_device (and the stage entry points

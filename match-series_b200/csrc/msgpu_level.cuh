@@ -142,8 +142,10 @@ struct LevelArgs {
 
 // Events of the pass timeline: a pass published (instance, kind), a pass
 // completed (its last chunk done: instance, kind), a wait for work of one
-// CTA that lasted 500 ns or more (its length), an ordered walk (its length).
-constexpr unsigned kEvPublish = 1, kEvComplete = 2, kEvIdle = 3, kEvWalk = 4;
+// CTA that lasted 500 ns or more (its length), an ordered walk (its length),
+// an open control step that has a term buffer's sums added in order
+// (instance, buffer, the kind of the pass whose step is open).
+constexpr unsigned kEvPublish = 1, kEvComplete = 2, kEvIdle = 3, kEvWalk = 4, kEvResolve = 5;
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -1407,33 +1409,36 @@ __device__ __forceinline__ bool finite_d(double x) { return !isnan(x) && !isinf(
 // of fixed sign) evaluated on the ends of its operands' intervals bounds its
 // value on the exact operands; a comparison that the bounds settle is the
 // comparison of the exact values.  ex: the value is known exactly (lo = hi).
+// m: the term buffers (bit per buffer) whose bounded sums the interval was
+// evaluated from (0 for an exact value).
 struct Iv {
   double lo, hi;
   int ex;
+  int m;
 };
-__device__ __forceinline__ Iv ivx(double x) { return Iv{x, x, 1}; }
-__device__ __forceinline__ Iv iv_unknown() {
+__device__ __forceinline__ Iv ivx(double x) { return Iv{x, x, 1, 0}; }
+__device__ __forceinline__ Iv iv_unknown(int m) {
   const double q = __longlong_as_double(0x7ff8000000000000ll);
-  return Iv{q, q, 0};
+  return Iv{q, q, 0, m};
 }
 __device__ __forceinline__ Iv iv_add(Iv a, Iv b) {
   if (a.ex && b.ex) return ivx(a.lo + b.lo);
-  return Iv{a.lo + b.lo, a.hi + b.hi, 0};
+  return Iv{a.lo + b.lo, a.hi + b.hi, 0, a.m | b.m};
 }
 __device__ __forceinline__ Iv iv_sub(Iv a, Iv b) {
   if (a.ex && b.ex) return ivx(a.lo - b.lo);
-  return Iv{a.lo - b.hi, a.hi - b.lo, 0};
+  return Iv{a.lo - b.hi, a.hi - b.lo, 0, a.m | b.m};
 }
 __device__ __forceinline__ Iv iv_scale(Iv a, double s) {
   if (a.ex) return ivx(a.lo * s);
-  return s >= 0.0 ? Iv{a.lo * s, a.hi * s, 0} : Iv{a.hi * s, a.lo * s, 0};
+  return s >= 0.0 ? Iv{a.lo * s, a.hi * s, 0, a.m} : Iv{a.hi * s, a.lo * s, 0, a.m};
 }
 __device__ __forceinline__ Iv iv_div(Iv a, Iv b) {
   if (a.ex && b.ex) return ivx(a.lo / b.lo);
-  if (!(b.lo > 0.0 || b.hi < 0.0)) return iv_unknown();
+  if (!(b.lo > 0.0 || b.hi < 0.0)) return iv_unknown(a.m | b.m);
   const double c1 = a.lo / b.lo, c2 = a.lo / b.hi, c3 = a.hi / b.lo, c4 = a.hi / b.hi;
-  if (isnan(c1) || isnan(c2) || isnan(c3) || isnan(c4)) return iv_unknown();
-  return Iv{fmin(fmin(c1, c2), fmin(c3, c4)), fmax(fmax(c1, c2), fmax(c3, c4)), 0};
+  if (isnan(c1) || isnan(c2) || isnan(c3) || isnan(c4)) return iv_unknown(a.m | b.m);
+  return Iv{fmin(fmin(c1, c2), fmin(c3, c4)), fmax(fmax(c1, c2), fmax(c3, c4)), 0, a.m | b.m};
 }
 // E_reg = 1/2 (0 + s1 + s2) and Df = 0 + s3 + s4 from a pass's sums
 __device__ __forceinline__ Iv xs_ereg(Iv s1, Iv s2) { return iv_scale(iv_add(iv_add(ivx(0.0), s1), s2), 0.5); }
@@ -1481,12 +1486,11 @@ struct XsBufState {
 // Tiles are handed out in chunks of consecutive tiles.  Dispenser word per
 // instance: [63:40] priority (an estimate of the instance's work left;
 // workers take the highest first), [39:20] chunks of the pass, [19:0] next
-// chunk.  A worker
-// reads the word and only when chunks are left takes
-// one with an atomic increment; an increment that arrives after the next pass
-// was published takes a valid chunk of that pass, whose descriptor was written
-// (and fenced) before the word.  Every wait for work is
-// bounded; a worker that gives up sets the error flag and all workers return.
+// chunk.  A worker reads the word and only when chunks are left takes one
+// with an atomic increment; an increment that arrives after the next pass was
+// published takes a valid chunk of that pass, whose descriptor was written
+// (and fenced) before the word.  Every wait for work is bounded; a worker
+// that gives up sets the error flag and all workers return.
 enum TaskKind : int {
   TK_E0 = 0, TK_GRAD, TK_VDOWN, TK_COARSE, TK_VUP, TK_NCG, TK_TRIAL, TK_FLUSH,
   TK_N1, TK_N2, TK_N3, TK_NF,   // NCC data term: energy subs 1-3, variation
@@ -1810,7 +1814,8 @@ __device__ __forceinline__ void block_sum(const double part[kRedSlots], double (
 // (gradientDescent.h:200-236) and ArmijoLineSearchUsingOp
 // (ArmijoSearch.h:118-200).
 template <typename Real>
-__device__ bool advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const double* tot, const Iv* xr) {
+__device__ bool advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const double* tot, const Iv* xr,
+                        int* open_bufs = nullptr) {
   const double lam = a.lambda_inst ? a.lambda_inst[inst] : a.lambda;
   const double tau_min = 9.313225746154785e-10;  // 2^-30 (ArmijoSearch.h:77)
   const double tau_max = 33554432.0;             // 2^25  (ArmijoSearch.h:67)
@@ -1819,49 +1824,55 @@ __device__ bool advance(const LevelArgs<Real>& a, int inst, InstCtl& c, const do
   PassDesc& d = c.desc;
   const int xb = d.xbuf;   // term buffer of the completed pass
   bool open = false;       // a decision the bounds do not settle
+  // open_bufs: the term buffers the open decisions were evaluated from
+  if (open_bufs) *open_bufs = 0;
+  auto mark = [&](int m) {
+    open = true;
+    if (open_bufs) *open_bufs |= m;
+  };
   // comparisons: exact operands compare as doubles; bounded ones decide
   // when the intervals do, else the step stays open
   auto ge = [&](Iv x, Iv y) {
     if (x.ex && y.ex) return x.lo >= y.lo;
     if (x.lo >= y.hi) return true;
     if (x.hi < y.lo) return false;
-    open = true;
+    mark(x.m | y.m);
     return false;
   };
   auto lt = [&](Iv x, Iv y) {
     if (x.ex && y.ex) return x.lo < y.lo;
     if (x.hi < y.lo) return true;
     if (x.lo >= y.hi) return false;
-    open = true;
+    mark(x.m | y.m);
     return false;
   };
   auto gt = [&](Iv x, Iv y) {
     if (x.ex && y.ex) return x.lo > y.lo;
     if (x.lo > y.hi) return true;
     if (x.hi <= y.lo) return false;
-    open = true;
+    mark(x.m | y.m);
     return false;
   };
   auto le = [&](Iv x, Iv y) {
     if (x.ex && y.ex) return x.lo <= y.lo;
     if (x.hi <= y.lo) return true;
     if (x.lo > y.hi) return false;
-    open = true;
+    mark(x.m | y.m);
     return false;
   };
   auto finite = [&](Iv x) {
     if (x.ex) return finite_d(x.lo);
     if (finite_d(x.lo) && finite_d(x.hi)) return true;
-    open = true;
+    mark(x.m);
     return true;
   };
   auto is_nan = [&](Iv x) {
     if (x.ex) return (bool)isnan(x.lo);
-    if (isnan(x.lo) || isnan(x.hi)) open = true;
+    if (isnan(x.lo) || isnan(x.hi)) mark(x.m);
     return false;
   };
   auto need = [&](Iv x) {   // a value written out or used in arithmetic
-    if (!x.ex) open = true;
+    if (!x.ex) mark(x.m);
     return (bool)x.ex;
   };
   // a value of the state evaluated from this pass's sums
@@ -2273,14 +2284,21 @@ __device__ void xs_settle(const LevelArgs<Real>& a, int inst, InstCtl& c, int b,
 
 // The buffer whose ordered sums an open control step needs next: the
 // completed pass's own, then those of the state's bounded values.
-__device__ __forceinline__ int xs_next_resolve(const InstCtl& c) {
+// why: 0 for the pass's own buffer, else 1 + the position of the value in
+// the order below (energy_new, energy, f, Df, the ring's energies, E_reg at
+// the position, the last E_reg, the ring's E_reg).
+__device__ __forceinline__ int xs_next_resolve(const InstCtl& c, int& why) {
   const int xb = c.desc.xbuf;
+  why = 0;
   if (xb >= 0 && c.bs[xb].state != 2) return xb;
   const XV* order[10] = {&c.energy_new, &c.energy,    &c.f,       &c.Df,      &c.rb_e[0],
                          &c.rb_e[1],    &c.ereg_pos,  &c.last_ereg, &c.rb_r[0], &c.rb_r[1]};
   for (int i = 0; i < 10; ++i) {
     const XV& x = *order[i];
-    if (!x.v.ex && x.buf >= 0 && c.bs[x.buf].state != 2) return x.buf;
+    if (!x.v.ex && x.buf >= 0 && c.bs[x.buf].state != 2) {
+      why = i + 1;
+      return x.buf;
+    }
   }
   return -1;
 }
@@ -2299,18 +2317,29 @@ __device__ int control_step(const LevelArgs<Real>& a, const SchedPtrs<Real>& sp,
     return -1;
   }
   const XsBufState& B = c.bs[c.desc.xbuf];
+  int obufs = 0;   // buffers the open decisions were evaluated from
   if (a.xs_bufs > 1 || B.state == 2) {
     const bool bounded = B.state != 2;
     ctl_store(sp.ctl + inst, c);   // the state before the step
     Iv xr[5];
-    for (int k = 0; k < 5; ++k) xr[k] = bounded ? Iv{B.lo[k], B.hi[k], 0} : ivx(B.lo[k]);
-    if (advance(a, inst, c, tot, xr)) {
+    for (int k = 0; k < 5; ++k) xr[k] = bounded ? Iv{B.lo[k], B.hi[k], 0, 1 << c.desc.xbuf} : ivx(B.lo[k]);
+    if (advance(a, inst, c, tot, xr, &obufs)) {
       if (bounded && a.xs_prof) atomicAdd(a.xs_prof + 2, 1ull);
       return -1;
     }
     ctl_load(c, sp.ctl + inst);
   }
-  const int rb = xs_next_resolve(c);
+  // the buffer to add in order: one the open decisions were evaluated from
+  // (the pass's own first), else the first bounded one in a fixed order
+  int why = 0, rb = -1;
+  for (int q = -1; q < kXsBufs && rb < 0; ++q) {
+    const int b = q < 0 ? c.desc.xbuf : q;
+    if (b >= 0 && ((obufs >> b) & 1) && c.bs[b].state != 2) {
+      rb = b;
+      why = 11;
+    }
+  }
+  if (rb < 0) rb = xs_next_resolve(c, why);
   if (rb < 0) {   // cannot happen: a step on exact values is never open
     atomicExch(sp.error, 2);
     c.desc.kind = TK_DONE;
@@ -2320,6 +2349,8 @@ __device__ int control_step(const LevelArgs<Real>& a, const SchedPtrs<Real>& sp,
   c.desc.kind = TK_XSUM;
   c.desc.xres = rb;
   c.desc.xn = c.bs[rb].ns;
+  trace_ev(a, global_ns(), kEvResolve,
+           ((unsigned)inst << 16) | ((unsigned)rb << 12) | ((unsigned)why << 8) | (unsigned)c.desc.purpose);
   return rb;
 }
 
