@@ -727,10 +727,13 @@ cudaError_t launch_level_core(LevelArgs<Real>& a, void* sched_mem, int* error_fl
   cudaError_t e = cudaMemsetAsync(sched_mem, 0, zb, st);
   if (e != cudaSuccess) return e;
   const size_t smem = level_smem_bytes<Real>(a.lc);
-  e = cudaFuncSetAttribute(level_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // the kernel variant that carries only the passes this launch runs
+  void (*kern)(LevelArgs<Real>, SchedPtrs<Real>) =
+      a.ncc ? level_kernel<Real, kKmAny> : (a.xs ? level_kernel<Real, kKmSsdExact> : level_kernel<Real, kKmSsd>);
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, level_kernel<Real>, kThreads, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   if (want_per_sm > 0 && want_per_sm < per_sm) per_sm = want_per_sm;
@@ -746,7 +749,7 @@ cudaError_t launch_level_core(LevelArgs<Real>& a, void* sched_mem, int* error_fl
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   if (grid_out) *grid_out = grid;
-  return cudaLaunchKernelEx(&cfg, level_kernel<Real>, a, sp);
+  return cudaLaunchKernelEx(&cfg, kern, a, sp);
 }
 
 template <typename Real>

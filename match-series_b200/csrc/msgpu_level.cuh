@@ -297,7 +297,13 @@ struct Inst {
 // Windows (EWX x EWY, origin (x0-4, y0-1)) per stage, in this order:
 //   kind 0: phx phy R ; kind 1: phx phy dx dy R ; kind 2: phx phy sx sy odx ody R
 // (kind 2 reads DE, needed at the owned nodes only, straight from L2).
-template <typename Real>
+// Variants of the level kernel, compiled separately so that each carries
+// only the passes it runs (registers are allocated for the whole kernel):
+// every pass kind (NCC data term, or any mode), the SSD data term in the
+// parallel sum order, and the SSD data term with exact sums.
+constexpr int kKmAny = 0, kKmSsd = 1, kKmSsdExact = 2;
+
+template <typename Real, int KM = kKmAny>
 struct EnergyPass {
   Inst<Real> I;
   int kind;
@@ -527,10 +533,19 @@ struct EnergyPass {
   }
 
   __device__ void compute(int t, int stage) {
-    if (xs) {
+    if constexpr (KM == kKmSsdExact) {
       compute_exact(t, stage);
       return;
+    } else {
+      if (KM == kKmAny && xs) {
+        compute_exact(t, stage);
+        return;
+      }
+      compute_parallel(t, stage);
     }
+  }
+
+  __device__ void compute_parallel(int t, int stage) {
     int x0, x1, y0, y1;
     tl.rect(t, x0, x1, y0, y1);
     const int n = I.n;
@@ -1623,13 +1638,16 @@ __device__ __forceinline__ int chunk_tiles(int ntiles, int active, int div, int 
 
 // Tiles of one pass: issue(t, stage) starts the window copies, compute(t,
 // stage) does the work and accumulates part[].
-template <typename Real>
+template <typename Real, int KM = kKmAny>
 struct TaskRunner {
   const LevelArgs<Real>& a;
   Real* smem;
   double (*xpw)[kXpSlots];   // shared: per-warp bound sums of an energy tile
   __device__ TaskRunner(const LevelArgs<Real>& a_, Real* sm, double (*xpw_)[kXpSlots])
       : a(a_), smem(sm), xpw(xpw_) {}
+  // exact sums in this launch (the host launches kKmSsdExact exactly when
+  // a.xs is set and the data term is SSD, kKmSsd when a.xs is null)
+  __device__ bool xs_on() const { return KM == kKmSsdExact ? true : (KM == kKmSsd ? false : a.xs != nullptr); }
 
   template <class F>
   __device__ void with_pass(int inst, const PassDesc& d, double* part, F&& f) const {
@@ -1639,18 +1657,18 @@ struct TaskRunner {
     Real* phi = I.arr(a.off_phi[d.cur]);
     Real* de = I.arr(a.off_de);
     Real* s = I.arr(a.off_s);
-    double* xs = a.xs ? xs_buffer(a, inst, d.xbuf) : nullptr;
-    double* xp = a.xpart ? a.xpart + (size_t)inst * a.xpart_stride : nullptr;
+    double* xs = xs_on() ? xs_buffer(a, inst, d.xbuf) : nullptr;
+    double* xp = (xs_on() && a.xpart) ? a.xpart + (size_t)inst * a.xpart_stride : nullptr;
     switch (d.kind) {
       case TK_E0: {
-        EnergyPass<Real> ps(I, 0, Real(0), Real(0), false, phi, phi + cs, nullptr, nullptr, nullptr, nullptr, nullptr,
+        EnergyPass<Real, KM> ps(I, 0, Real(0), Real(0), false, phi, phi + cs, nullptr, nullptr, nullptr, nullptr, nullptr,
                             nullptr, nullptr, nullptr, smem, part, xs, xp, xpw);
         f(ps);
         break;
       }
       case TK_TRIAL: {
         const Real* dd = I.arr(a.off_d[d.dcur]);
-        EnergyPass<Real> ps(I, 1, (Real)d.t, Real(0), false, phi, phi + cs, dd, dd + cs, nullptr, nullptr, nullptr,
+        EnergyPass<Real, KM> ps(I, 1, (Real)d.t, Real(0), false, phi, phi + cs, dd, dd + cs, nullptr, nullptr, nullptr,
                             nullptr, nullptr, nullptr, smem, part, xs, xp, xpw);
         f(ps);
         break;
@@ -1658,7 +1676,7 @@ struct TaskRunner {
       case TK_NCG: {
         const Real* od = I.arr(a.off_d[d.dcur]);
         Real* wd = I.arr(a.off_d[d.dn]);
-        EnergyPass<Real> ps(I, 2, (Real)d.t, (Real)d.beta, (d.flags & PF_ODZERO) != 0, phi, phi + cs, od, od + cs, s,
+        EnergyPass<Real, KM> ps(I, 2, (Real)d.t, (Real)d.beta, (d.flags & PF_ODZERO) != 0, phi, phi + cs, od, od + cs, s,
                             s + cs, de, de + cs, wd, wd + cs, smem, part, xs, xp, xpw);
         f(ps);
         break;
@@ -1674,6 +1692,7 @@ struct TaskRunner {
       case TK_N1:
       case TK_N2:
       case TK_N3: {
+        if constexpr (KM != kKmAny) break; else {
         const int sub = (d.kind == TK_N1) ? 1 : (d.kind == TK_N2 ? 2 : 3);
         const int mode = (d.purpose == TK_GRAD) ? NM_GRAD
                          : (d.purpose == TK_TRIAL ? NM_TRIAL : (d.purpose == TK_NCG ? NM_NCG : NM_E0));
@@ -1686,13 +1705,16 @@ struct TaskRunner {
                          s, s + cs, de, de + cs, I.normR, wd, wd + cs, nphi, nphi + cs, td, smem, part);
         f(ps);
         break;
+        }
       }
       case TK_NF: {
+        if constexpr (KM != kKmAny) break; else {
         Real* nphi = I.arr(a.off_phi[d.cur ^ 1]);
         NccForcePass<Real> ps(I, I.lambda, d.mean, d.var, d.e, nphi, nphi + cs, I.arr(a.off_td), I.normR, de, de + cs,
                               smem, part);
         f(ps);
         break;
+        }
       }
       case TK_VDOWN: {
         const int k = d.k, w = (1 << k) + 1;
@@ -1734,7 +1756,7 @@ struct TaskRunner {
   }
 
   __device__ void compute(int inst, const PassDesc& d, int tile, int stage, double* part) const {
-    if (d.kind == TK_XSUM) {
+    if (KM != kKmSsd && d.kind == TK_XSUM) {
       // chunk and group summaries of the task tile's tile rows (all sums in turn)
       const bool energy = (d.purpose == TK_E0 || d.purpose == TK_TRIAL || d.purpose == TK_NCG);
       double* base = xs_buffer(a, inst, d.xres);
@@ -1752,7 +1774,7 @@ struct TaskRunner {
       const Real* by = (L == lc) ? de + cs : bx + comp_stride(lc);
       Real* out = (L == lc) ? s : I.arr(a.off_x5[lc]);
       Real* outy = (L == lc) ? s + cs : out + comp_stride(lc);
-      double* xs = (a.xs && L == lc && a.mode != MODE_SMOOTH) ? xs_buffer(a, inst, d.xbuf) : nullptr;
+      double* xs = (xs_on() && L == lc && a.mode != MODE_SMOOTH) ? xs_buffer(a, inst, d.xbuf) : nullptr;
       coarse_vcycle<Real>(lc, d.vtau, smem, bx, by, (L == lc) ? Real(-1) : Real(1), out, outy, L == lc, part, xs);
       return;
     }
@@ -2476,7 +2498,7 @@ __device__ bool try_take(const LevelArgs<Real>& a, const SchedPtrs<Real>& sp, in
 // worker returns.
 constexpr unsigned long long kMaxIdleNs = 4000000000ull;
 
-template <typename Real>
+template <typename Real, int KM>
 __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, SchedPtrs<Real> sp) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   Real* smem = reinterpret_cast<Real*>(smem_raw);
@@ -2491,7 +2513,8 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
   __shared__ int xact;         // buffer whose ordered sums the control step needs, or -1
   PassTimer pt{a.pass_cycles ? a.pass_cycles + (size_t)blockIdx.x * kPassKinds : nullptr, 0};
   __shared__ double xpw[kThreads / 32][kXpSlots];
-  const TaskRunner<Real> run(a, smem, xpw);
+  const TaskRunner<Real, KM> run(a, smem, xpw);
+  const bool xs_on = run.xs_on();
 
   // publish the first pass of the instances this CTA owns
   if (threadIdx.x == 0) {
@@ -2590,7 +2613,7 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
       }
       // an energy tile with bounds: its per-warp sums (written before the
       // reduction's barriers) into the tile's bound sums
-      if (a.xpart && a.xs && is_energy_kind(t.desc.kind) && threadIdx.x < kXpSlots) {
+      if (xs_on && a.xpart && is_energy_kind(t.desc.kind) && threadIdx.x < kXpSlots) {
         double v = 0.0;
 #pragma unroll
         for (int w = 0; w < kThreads / 32; ++w) v += xpw[w][threadIdx.x];
@@ -2621,8 +2644,8 @@ __global__ void __launch_bounds__(kThreads, 2) level_kernel(LevelArgs<Real> a, S
       }
       block_sum(acc, wbuf, tot);
       const XsGeom xg(a.n);
-      const bool xdone = (t.desc.kind == TK_XSUM);
-      const int nxs = (a.xs && !xdone) ? xs_count(a, t.desc) : 0;
+      const bool xdone = xs_on && (t.desc.kind == TK_XSUM);
+      const int nxs = (xs_on && !xdone) ? xs_count(a, t.desc) : 0;
       // an energy pass with bounds: the sums of its terms and magnitudes
       const bool cert = nxs && a.xpart && is_energy_kind(t.desc.kind);
       if (cert) {
