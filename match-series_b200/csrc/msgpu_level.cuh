@@ -568,10 +568,12 @@ struct EnergyPass {
       if (od_zero) return Wb[i];
       return Wb[i] + beta * Woy[i];
     };
-    // elements owned by the tile
+    // elements owned by the tile (at most 64 columns and 8 rows): a thread
+    // owns column lx of rows ly and ly + 4, evaluated together and added in
+    // that order
     const int ex1 = (x1 < n - 1) ? x1 : n - 1, ey1 = (y1 < n - 1) ? y1 : n - 1;
     const int ew = ex1 - x0, eh = ey1 - y0;
-    for_2d<64>(ew, eh, [&](int ix, int iy) {
+    auto elem = [&](int ix, int iy) -> double {
       const int ex = x0 + ix, ey = y0 + iy;
       const int c0 = at(ex, ey);
       const int idx[4] = {c0, c0 + 1, c0 + EWX, c0 + EWX + 1};
@@ -591,8 +593,18 @@ struct EnergyPass {
           py[b] = vy;
         }
       }
-      part[0] += (double)element_ssd(I.T, n, I.P, I.h, ex, ey, px, py, r);
-    });
+      return (double)element_ssd(I.T, n, I.P, I.h, ex, ey, px, py, r);
+    };
+    {
+      const int lx = threadIdx.x & 63, ly = threadIdx.x >> 6;
+      if (lx < ew && ly < eh) {
+        const bool two = ly + 4 < eh;
+        const double v = elem(lx, ly);
+        const double v2 = elem(lx, two ? ly + 4 : ly);
+        part[0] += v;
+        if (two) part[0] += v2;
+      }
+    }
     if (kind == 1) return;
     // owned nodes
     const int nw = x1 - x0, nh = y1 - y0;
