@@ -424,35 +424,32 @@ struct EnergyPass {
         }
         return (double)element_ssd(I.T, n, I.P, I.h, ex, ey, px, py, r);
       };
-      auto row_done = [&](int iy, double acc, double mag) {
+      // the SSD element integrals are >= 0 (or NaN), so the sum of their
+      // magnitudes is the sum itself, added in the same order
+      auto row_done = [&](int iy, double acc) {
         acc = warp_sum(acc);
         if (lane == 0) s0.tot[((y0 + iy) * g.nx + tx) * 2 + half] = acc;
-        if (xp) {
-          mag = warp_sum(mag);
-          if (lane == 0) {
-            xpw[wid][0] += acc;
-            xpw[wid][5] += mag;
-          }
+        if (xp && lane == 0) {
+          xpw[wid][0] += acc;
+          xpw[wid][5] += acc;
         }
       };
       if (ly < eh) {
         const int iy = ly, iy2 = ly + 4;
         const bool two = iy2 < eh;
-        double acc = 0.0, mag = 0.0, acc2 = 0.0, mag2 = 0.0;
+        double acc = 0.0, acc2 = 0.0;
         if (ein) {
           const double v = elem(lx, iy);
           const double v2 = elem(lx, two ? iy2 : iy);
           B0[xs_at(lx, iy)] = v;
           acc += v;
-          mag += fabs(v);
           if (two) {
             B0[xs_at(lx, iy2)] = v2;
             acc2 += v2;
-            mag2 += fabs(v2);
           }
         }
-        row_done(iy, acc, mag);
-        if (two) row_done(iy2, acc2, mag2);
+        row_done(iy, acc);
+        if (two) row_done(iy2, acc2);
       }
     }
     // owned nodes: p . L p per component; NCG also DE . d and the direction
@@ -1703,31 +1700,29 @@ struct TaskRunner {
       }
       case TK_N1:
       case TK_N2:
-      case TK_N3: {
-        if constexpr (KM != kKmAny) break; else {
-        const int sub = (d.kind == TK_N1) ? 1 : (d.kind == TK_N2 ? 2 : 3);
-        const int mode = (d.purpose == TK_GRAD) ? NM_GRAD
-                         : (d.purpose == TK_TRIAL ? NM_TRIAL : (d.purpose == TK_NCG ? NM_NCG : NM_E0));
-        const Real* dd = I.arr(a.off_d[d.dcur]);
-        Real* wd = I.arr(a.off_d[d.dn]);
-        Real* nphi = I.arr(a.off_phi[d.cur ^ 1]);
-        Real* td = I.arr(a.off_td);
-        const bool step = (d.flags & PF_STEP) != 0, odz = (d.flags & PF_ODZERO) != 0;
-        NccPass<Real> ps(I, sub, mode, (Real)d.t, (Real)d.beta, d.mean, d.var, odz, step, phi, phi + cs, dd, dd + cs,
-                         s, s + cs, de, de + cs, I.normR, wd, wd + cs, nphi, nphi + cs, td, smem, part);
-        f(ps);
-        break;
+      case TK_N3:
+        if constexpr (KM == kKmAny) {   // the NCC passes exist in this variant only
+          const int sub = (d.kind == TK_N1) ? 1 : (d.kind == TK_N2 ? 2 : 3);
+          const int mode = (d.purpose == TK_GRAD) ? NM_GRAD
+                           : (d.purpose == TK_TRIAL ? NM_TRIAL : (d.purpose == TK_NCG ? NM_NCG : NM_E0));
+          const Real* dd = I.arr(a.off_d[d.dcur]);
+          Real* wd = I.arr(a.off_d[d.dn]);
+          Real* nphi = I.arr(a.off_phi[d.cur ^ 1]);
+          Real* td = I.arr(a.off_td);
+          const bool step = (d.flags & PF_STEP) != 0, odz = (d.flags & PF_ODZERO) != 0;
+          NccPass<Real> ps(I, sub, mode, (Real)d.t, (Real)d.beta, d.mean, d.var, odz, step, phi, phi + cs, dd,
+                           dd + cs, s, s + cs, de, de + cs, I.normR, wd, wd + cs, nphi, nphi + cs, td, smem, part);
+          f(ps);
         }
-      }
-      case TK_NF: {
-        if constexpr (KM != kKmAny) break; else {
-        Real* nphi = I.arr(a.off_phi[d.cur ^ 1]);
-        NccForcePass<Real> ps(I, I.lambda, d.mean, d.var, d.e, nphi, nphi + cs, I.arr(a.off_td), I.normR, de, de + cs,
-                              smem, part);
-        f(ps);
         break;
+      case TK_NF:
+        if constexpr (KM == kKmAny) {
+          Real* nphi = I.arr(a.off_phi[d.cur ^ 1]);
+          NccForcePass<Real> ps(I, I.lambda, d.mean, d.var, d.e, nphi, nphi + cs, I.arr(a.off_td), I.normR, de,
+                                de + cs, smem, part);
+          f(ps);
         }
-      }
+        break;
       case TK_VDOWN: {
         const int k = d.k, w = (1 << k) + 1;
         const Real hsq = (Real)(d.vtau * (double)((w - 1) * (w - 1)));
