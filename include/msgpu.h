@@ -431,28 +431,26 @@ int msgpu_set_profiling(msgpu_context* ctx, int on);
  * (msgpu_set_profiling on) that solve their levels as batches:
  * msgpu_register_batch{,_device} and the stage and series entry points
  * built on it (a call with several batches keeps the last one's events),
- * not the ragged entry points.  msgpu_set_trace(ctx, level, capacity)
- * records up
- * to `capacity` events (at most 2^26) of the level kernel at `level` (-1:
- * none, the default); msgpu_get_trace copies the last profiled call's events,
- * at most `capacity`, to out (two words each) and returns how many there
- * were (-1 on invalid arguments).  Word 0 is the GPU's global timer in ns;
- * word 1 packs the event in bits 56-63, the CTA in bits 32-55 and a value in
- * bits 0-31: event 1 a pass published and 2 a pass completed (value
- * instance << 8 | pass kind: 0 initial energy, 1 gradient, 2 V-cycle down,
- * 3 coarse V-cycle, 4 V-cycle up, 5 NCG + first trial, 6 trial, 7 flush,
- * 8-11 NCC sub-passes, 12 summaries of exact sums, 13 instance finished),
- * 3 a wait for work
- * of 500 ns or more (value its length in ns, word 0 its start), 4 an ordered
- * walk of exact sums (value its length), 5 an open control step that has a
- * term buffer's sums added in order (value instance << 16 | buffer << 12 |
- * reason << 8 | kind of the pass whose step is open; reason 11: a buffer
- * the open decision was evaluated from, else 0: the pass's own sums, 1-10: a
- * bounded value of the state, in the order energy at the new position,
- * energy, f, Df, the two line-search energies, E_reg at the position, the
- * last E_reg, the two line-search E_reg).  Profiling aid; no
- * counterpart in the reference (whose only tracing is a stopwatch and
- * gprof).                                                                  */
+ * not the ragged entry points. msgpu_set_trace(ctx, level, capacity)
+ * records up to `capacity` events (at most 2^26) of the level kernel at
+ * `level` (-1: none, the default); msgpu_get_trace copies the last profiled
+ * call's events, at most `capacity`, to out (two words each) and returns
+ * how many there were (-1 on invalid arguments). Word 0 is the GPU's global
+ * timer in ns; word 1 packs the event in bits 56-63, the CTA in bits 32-55
+ * and a value in bits 0-31: event 1 a pass published and 2 a pass completed
+ * (value instance << 8 | pass kind: 0 initial energy, 1 gradient, 2 V-cycle
+ * down, 3 coarse V-cycle, 4 V-cycle up, 5 NCG + first trial, 6 trial, 7
+ * flush, 8-11 NCC sub-passes, 12 summaries of exact sums, 13 instance
+ * finished), 3 a wait for work of 500 ns or more (value its length in ns,
+ * word 0 its start), 4 an ordered walk of exact sums (value its length), 5
+ * an open control step that has a term buffer's sums added in order (value
+ * instance << 16 | buffer << 12 | reason << 8 | kind of the pass whose step
+ * is open; reason 11: a buffer the open decision was evaluated from, else
+ * 0: the pass's own sums, 1-10: a bounded value of the state, in the order
+ * energy at the new position, energy, f, Df, the two line-search energies,
+ * E_reg at the position, the last E_reg, the two line-search E_reg).
+ * Profiling aid; no counterpart in the reference (whose only tracing is a
+ * stopwatch and gprof). */
 int msgpu_set_trace(msgpu_context* ctx, int level, unsigned int capacity);
 long long msgpu_get_trace(const msgpu_context* ctx, unsigned long long* out, long long capacity);
 /* CUDA graphs for msgpu_register_batch_device (and the stage entry points
