@@ -674,7 +674,8 @@ def main_ragged(args, world, rank, local):
     levels = [l.bit_length() - 1 for l in levels]
     F = [t.shape[0] for _, t in series]
     total = sum(F)
-    p = msgpu.default_params(start_level=4, max_gd_iterations=MAX_ITER, use_fp64=int(fp64), lambda_=LAMBDA)
+    p = msgpu.default_params(start_level=4, max_gd_iterations=MAX_ITER, use_fp64=int(fp64), lambda_=LAMBDA,
+                             sum_order=SUM_ORDER)
     ctx = msgpu.Context(local)
     use_tuning(ctx)
     dev = torch.device("cuda", local)
@@ -696,7 +697,7 @@ def main_ragged(args, world, rank, local):
     def separate():
         for d in descs:
             q = msgpu.default_params(precision_level=d.level, input_level=d.level, start_level=4, stop_level=d.level,
-                                     max_gd_iterations=MAX_ITER, use_fp64=int(fp64), lambda_=LAMBDA)
+                                     max_gd_iterations=MAX_ITER, use_fp64=int(fp64), lambda_=LAMBDA, sum_order=SUM_ORDER)
             ctx.register_batch_device(q, d.reference, d.templates, d.num_templates, d.phis_out, d.energies_out,
                                       0, 0, stream.cuda_stream)
 
@@ -748,6 +749,7 @@ def main_ragged(args, world, rank, local):
                                    f"{dict(sorted(sizes.items()))}, square/hex lattices with spacing 8-16 px and "
                                    f"Poisson peak 20-100, levels 4 to each series' finest, maxGDIterations "
                                    f"{MAX_ITER}, lambda {LAMBDA}, one level-kernel launch per level",
+                       "sum_order": "reference sequential order (bit-exact)" if SUM_ORDER == 0 else "parallel order",
                        "parallelism": f"weak, {world} ranks"},
             "e2e": {"value": world * total * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
@@ -1019,7 +1021,8 @@ def main_warm(args, world, rank, local):
     spec = syn.random_spec(np.random.default_rng(7000 + rank))
     frames = syn.make_series_torch(n, F + 1, spec, 7001 + 1000 * rank, dev).reshape(F + 1, N).contiguous()
     p = msgpu.default_params(precision_level=WARM_LEVEL, input_level=WARM_LEVEL, start_level=WARM_START,
-                             stop_level=WARM_LEVEL, max_gd_iterations=MAX_ITER, use_fp64=int(fp64), lambda_=LAMBDA)
+                             stop_level=WARM_LEVEL, max_gd_iterations=MAX_ITER, use_fp64=int(fp64), lambda_=LAMBDA,
+                             sum_order=SUM_ORDER)
     nlev = WARM_LEVEL - WARM_START + 1
     st = torch.cuda.current_stream(dev)
     outs = {k: (torch.empty((F, 2, N), dtype=torch.float64, device=dev),
