@@ -106,8 +106,9 @@ int  msgpu_set_sum_order(msgpu_context* ctx, int sum_order);
  * they settle it, and adds the sums in order only where a decision stays
  * open, where a value is written out (energies, logs) or enters arithmetic
  * (the Fletcher-Reeves factor).  The results are those of the ordered sums
- * either way; on costs six term buffers per instance (at most 16 GiB,
- * beyond that one).  Off: every pass's sums are added in order.            */
+ * either way; on costs six term buffers per instance of a level launch
+ * (at most 32 GiB per launch, beyond that one).  Off: every pass's sums
+ * are added in order.                                                      */
 int  msgpu_set_certified_steps(msgpu_context* ctx, int on);
 /* findXShift's descent control (msgpu_find_xshift{,_device,_batch}) on the
  * device (1): the descent is captured once into a CUDA graph whose step loop

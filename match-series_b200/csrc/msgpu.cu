@@ -772,7 +772,7 @@ int launch_level(msgpu_context* ctx, LevelArgs<Real>& a, cudaStream_t st) {
 // steps off, or more memory than kXsCertBytes) adds every pass's sums in order
 // before its control step.  Otherwise the launch adds its sums in the fixed
 // parallel order of the tile partials.
-constexpr size_t kXsCertBytes = 16ull << 30;
+constexpr size_t kXsCertBytes = 32ull << 30;
 template <typename Real>
 int xs_attach(msgpu_context* ctx, LevelArgs<Real>& a, bool exact, int max_level, int num_inst) {
   a.xs = nullptr;
@@ -1413,7 +1413,9 @@ int run_ragged(msgpu_context* ctx, const msgpu_params& p, std::vector<RaggedSeri
     a.out_steps = steps;
     a.out_evals = evals;
     a.out_phi_buf = bin;
-    if ((rc = xs_attach<Real>(ctx, a, p.sum_order == 0, Lmax, Ftot))) return rc;
+    // sized for this level's grid and running instances (the term buffers
+    // hold no state from one level to the next)
+    if ((rc = xs_attach<Real>(ctx, a, p.sum_order == 0, l, A))) return rc;
     if ((rc = launch_level<Real>(ctx, a, st))) return rc;
     ++launches;
     // series finishing at this level: displacements and energies out
