@@ -429,10 +429,10 @@ typedef struct {
 } msgpu_stats;
 int msgpu_set_profiling(msgpu_context* ctx, int on);
 /* Pass timeline of one level's launch, recorded by profiled calls
- * (msgpu_set_profiling on) that solve their levels as batches:
- * msgpu_register_batch{,_device} and the stage and series entry points
- * built on it (a call with several batches keeps the last one's events),
- * not the ragged entry points. msgpu_set_trace(ctx, level, capacity)
+ * (msgpu_set_profiling on) that solve their levels with the level kernel:
+ * msgpu_register_batch{,_device}, the stage and series entry points built
+ * on it (a call with several batches keeps the last one's events) and the
+ * ragged entry points. msgpu_set_trace(ctx, level, capacity)
  * records up to `capacity` events (at most 2^26) of the level kernel at
  * `level` (-1: none, the default); msgpu_get_trace copies the last profiled
  * call's events, at most `capacity`, to out (two words each) and returns

@@ -764,6 +764,33 @@ int launch_level(msgpu_context* ctx, LevelArgs<Real>& a, cudaStream_t st) {
   return MSGPU_OK;
 }
 
+// Pass timeline of a profiled level launch (msgpu_set_trace): the event
+// buffer when the launch's level is the traced one, and the events copied
+// to the host after it.
+template <typename Real>
+int trace_attach(msgpu_context* ctx, LevelArgs<Real>& a, cudaStream_t st) {
+  if (!ctx->profiling || a.level != ctx->trace_level || ctx->trace_cap == 0) return MSGPU_OK;
+  int rc;
+  const size_t tb = sizeof(unsigned long long) * 2 * (size_t)ctx->trace_cap;
+  if ((rc = ensure(ctx, ctx->trace, tb + 16))) return rc;
+  a.tl = (unsigned long long*)ctx->trace.p;
+  a.tl_n = (unsigned int*)((char*)ctx->trace.p + tb);
+  a.tl_cap = ctx->trace_cap;
+  CK(cudaMemsetAsync(a.tl_n, 0, 16, st));
+  return MSGPU_OK;
+}
+template <typename Real>
+int trace_collect(msgpu_context* ctx, const LevelArgs<Real>& a, cudaStream_t st) {
+  if (!a.tl) return MSGPU_OK;
+  unsigned cnt = 0;
+  CK(cudaMemcpyAsync(&cnt, a.tl_n, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  cnt = std::min(cnt, a.tl_cap);
+  ctx->trace_host.resize(2 * (size_t)cnt);
+  if (cnt) CK(cudaMemcpy(ctx->trace_host.data(), a.tl, sizeof(unsigned long long) * 2 * cnt, cudaMemcpyDeviceToHost));
+  return MSGPU_OK;
+}
+
 // Exact sums of a level launch (FP64, SSD, sum order 0): per instance
 // xs_bufs term buffers of XsLayout(n).stride doubles and (xs_bufs > 1) the
 // per-tile bound sums of its energy passes.  kXsBufs buffers let a control
@@ -1055,28 +1082,12 @@ int run_batch(msgpu_context* ctx, const msgpu_params& p, int F, const BatchIO& i
       a.xs_prof = (unsigned long long*)ctx->prof.p + prof_n * nlev_all + 8 * (l - start);
       CK(cudaMemsetAsync(a.pass_cycles, 0, sizeof(unsigned long long) * prof_n, st));
       CK(cudaMemsetAsync(a.xs_prof, 0, sizeof(unsigned long long) * 8, st));
-      if (l == ctx->trace_level && ctx->trace_cap > 0) {
-        const size_t tb = sizeof(unsigned long long) * 2 * (size_t)ctx->trace_cap;
-        if ((rc = ensure(ctx, ctx->trace, tb + 16))) return rc;
-        a.tl = (unsigned long long*)ctx->trace.p;
-        a.tl_n = (unsigned int*)((char*)ctx->trace.p + tb);
-        a.tl_cap = ctx->trace_cap;
-        CK(cudaMemsetAsync(a.tl_n, 0, 16, st));
-      }
+      if ((rc = trace_attach<Real>(ctx, a, st))) return rc;
     }
     if ((rc = xs_attach<Real>(ctx, a, p.sum_order == 0, stop, F))) return rc;
     if (ctx->profiling && l - start < 16) CK(cudaEventRecord(ctx->ev[2 * (l - start)], st));
     if ((rc = launch_level<Real>(ctx, a, st))) return rc;
-    if (a.tl) {
-      unsigned cnt = 0;
-      CK(cudaMemcpyAsync(&cnt, a.tl_n, sizeof(cnt), cudaMemcpyDeviceToHost, st));
-      CK(cudaStreamSynchronize(st));
-      cnt = std::min(cnt, a.tl_cap);
-      ctx->trace_host.resize(2 * (size_t)cnt);
-      if (cnt)
-        CK(cudaMemcpy(ctx->trace_host.data(), a.tl, sizeof(unsigned long long) * 2 * cnt,
-                      cudaMemcpyDeviceToHost));
-    }
+    if ((rc = trace_collect<Real>(ctx, a, st))) return rc;
     if (l - start < 16) ctx->stats.level_cluster[l - start] = ctx->last_grid;
     if (ctx->profiling && l - start < 16) CK(cudaEventRecord(ctx->ev[2 * (l - start) + 1], st));
     k_collect<<<1, 256, 0, st>>>(e_lvl, a.out_steps, F, (l == stop) ? io.energies_out : nullptr, io.steps_out,
@@ -1416,7 +1427,9 @@ int run_ragged(msgpu_context* ctx, const msgpu_params& p, std::vector<RaggedSeri
     // sized for this level's grid and running instances (the term buffers
     // hold no state from one level to the next)
     if ((rc = xs_attach<Real>(ctx, a, p.sum_order == 0, l, A))) return rc;
+    if ((rc = trace_attach<Real>(ctx, a, st))) return rc;
     if ((rc = launch_level<Real>(ctx, a, st))) return rc;
+    if ((rc = trace_collect<Real>(ctx, a, st))) return rc;
     ++launches;
     // series finishing at this level: displacements and energies out
     for (int s = 0; s < ns; ++s) {

@@ -263,3 +263,36 @@ def test_pass_timeline_records_every_pass_and_leaves_results_unchanged(gpu):
         # the passes complete in the order they were published
         assert np.array_equal(kind[pub], kind[com]), i
     assert np.all(val[ev == 3] >= 500)
+
+
+def test_pass_timeline_of_a_ragged_batch(gpu):
+    """The ragged entry point records the timeline too: at a level that two
+    series of different sizes both pass, every instance of both finishes
+    once and every pass it published completes."""
+    import msgpu
+    from msgpu import synthetic as syn
+    p = msgpu.default_params(start_level=4, max_gd_iterations=8, use_fp64=1)
+    series = []
+    for level, F, seed in ((7, 2, 9801), (6, 3, 9802)):
+        n = (1 << level) + 1
+        fr, _, _ = syn.make_series(n, F + 1, syn.SQUARE_257, seed=seed)
+        series.append((fr[0], fr[1:]))
+    plain = gpu.register_ragged(p, series)
+    gpu.set_profiling(True)
+    gpu.set_trace(6, 1 << 18)
+    try:
+        traced = gpu.register_ragged(p, series)
+        tr = gpu.trace()
+    finally:
+        gpu.set_trace(-1, 0)
+        gpu.set_profiling(False)
+    for (pa, ea), (pb, eb) in zip(plain, traced):
+        assert np.array_equal(pa, pb) and np.array_equal(ea, eb)
+    ev, val = tr["event"], tr["value"]
+    kind = val & 255
+    done = (ev == 1) & (kind == 13)
+    assert sorted((val[done] >> 8).tolist()) == list(range(5))
+    for i in range(5):
+        pub = (ev == 1) & ((val >> 8) == i) & (kind != 13)
+        com = (ev == 2) & ((val >> 8) == i)
+        assert pub.sum() == com.sum() > 0, i
